@@ -1,0 +1,156 @@
+"""ctypes mirror of the plain-data types in include/aprl_gpu.h.
+
+Only data layouts live here; the loader for the CUDA library is in
+aprl_b200/native.py.
+"""
+import ctypes as C
+
+APRL_OK = 0
+APRL_ERR_INVALID_ARGUMENT = 1
+APRL_ERR_OUT_OF_RANGE = 2
+APRL_ERR_RUNTIME = 3
+APRL_ERR_NOT_CONVERGED = 4
+APRL_ERR_CUDA = 5
+APRL_ERR_UNSUPPORTED = 6
+
+STATUS_NAMES = {
+    APRL_OK: "ok",
+    APRL_ERR_INVALID_ARGUMENT: "invalid_argument",
+    APRL_ERR_OUT_OF_RANGE: "out_of_range",
+    APRL_ERR_RUNTIME: "runtime_error",
+    APRL_ERR_NOT_CONVERGED: "not_converged",
+    APRL_ERR_CUDA: "cuda_error",
+    APRL_ERR_UNSUPPORTED: "unsupported",
+}
+
+SHAPE_LINEAR_BINOMIAL3 = 0
+SHAPE_QUINTIC_COMPENSATED = 1
+SHAPES = {"linear-binomial3": SHAPE_LINEAR_BINOMIAL3,
+          "quintic-compensated": SHAPE_QUINTIC_COMPENSATED}
+
+MAGNET_PLANAR_UNDULATOR = 0
+MAGNET_UNIFORM_DIPOLE = 1
+MAGNET_QUADRUPOLE = 2
+MAX_MAGNETS = 4
+
+# Field component order of the ABI: Ex Ey Ez Bx By Bz Jx Jy Jz.
+COMPONENTS = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz")
+
+
+class Magnet(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("gaussian_fringe", C.c_int32),
+        ("center", C.c_double * 3),
+        ("length", C.c_double),
+        ("period", C.c_double),
+        ("peak_field", C.c_double),
+        ("polarization_angle", C.c_double),
+        ("fringe_relative_cutoff", C.c_double),
+        ("quadrupole_gradient", C.c_double),
+        ("wave_number", C.c_double),
+        ("fringe_extent", C.c_double),
+        ("cos_angle", C.c_double),
+        ("sin_angle", C.c_double),
+    ]
+
+
+class RunConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("dt", C.c_double),
+        ("cpml_cells_x", C.c_uint64), ("cpml_cells_y", C.c_uint64),
+        ("cpml_polynomial_order", C.c_double),
+        ("cpml_target_reflection", C.c_double),
+        ("cpml_kappa_max", C.c_double),
+        ("cpml_alpha_fraction", C.c_double),
+        ("shape", C.c_int32),
+        ("substeps", C.c_uint32),
+        ("max_trials", C.c_uint32),
+        ("reserved0", C.c_uint32),
+        ("force_tolerance", C.c_double),
+        ("work_tolerance", C.c_double),
+        ("boost_gamma", C.c_double), ("boost_beta", C.c_double),
+        ("boost_gamma_beta", C.c_double),
+        ("lab_time_origin", C.c_double), ("lab_z_origin", C.c_double),
+        ("box_z_origin", C.c_double),
+        ("reference_origin", C.c_double * 3),
+        ("initial_offset", C.c_int64),
+        ("reference_nz", C.c_uint64),
+        ("translation_beta", C.c_double),
+        ("exit_lab_z", C.c_double),
+        ("n_magnets", C.c_uint32),
+        ("reserved1", C.c_uint32),
+        ("magnets", Magnet * MAX_MAGNETS),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("step", C.c_uint64),
+        ("iterations", C.c_uint32),
+        ("max_iterations", C.c_uint32),
+        ("total_iterations", C.c_uint64),
+        ("force", C.c_double),
+        ("work", C.c_double),
+        ("particles", C.c_uint64),
+        ("carriers", C.c_uint64),
+        ("exits", C.c_uint64),
+        ("exit_charge", C.c_double),
+        ("cpml_entries", C.c_uint64 * 6),
+        ("cpml_entry_charge", C.c_double * 6),
+        ("carrier_outer", C.c_uint64 * 6),
+        ("carrier_outer_charge", C.c_double * 6),
+        ("cropped_carriers", C.c_uint64),
+        ("cropped_charge", C.c_double),
+        ("window_offset", C.c_int64),
+        ("origin_z", C.c_double),
+        ("time_box", C.c_double),
+        ("device_error", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            value = getattr(self, name)
+            if isinstance(value, C.Array):
+                value = list(value)
+            out[name] = value
+        return out
+
+
+def field_shape(config, component):
+    """Yee extents (nx_c, ny_c, nz_c) of an ABI component (x fastest)."""
+    cells = (config.nx, config.ny, config.nz)
+    electric = component < 3 or component >= 6
+    axis = component % 3
+    return tuple(cells[d] + ((d != axis) if electric else (d == axis))
+                 for d in range(3))
+
+
+def reference_shape(config, component):
+    """Extents of one prepared-reference component over reference_nz cells."""
+    nx_c, ny_c, _ = field_shape(config, component)
+    return (nx_c, ny_c,
+            config.reference_nz + (1 if component in (0, 1, 5) else 0))
+
+
+def history_shape(config, index):
+    """(slots, layers, row) of CPML history `index` (0..11), or None when the
+    term is inactive (z-derivative histories under the moving window)."""
+    pairs = ((0, 1), (0, 2), (1, 2), (1, 0), (2, 0), (2, 1))
+    comp, der = pairs[index % 6]
+    if der == 2:
+        return None
+    electric = index >= 6
+    shape = field_shape(config, comp if electric else 3 + comp)
+    cells = config.cpml_cells_x if der == 0 else config.cpml_cells_y
+    # makeProfile marks 2*cells active points on each derivative axis
+    # (cells on each side) for magnetic (half-integer) positions and
+    # 2*cells (+0) for electric nodes: the node at the thickness edge has
+    # zero depth and is inactive.
+    slots = 2 * cells
+    row = shape[1] if der == 0 else shape[0]
+    return (slots, shape[2], row)

@@ -1,0 +1,320 @@
+"""ctypes binding of the C ABI (include/aprl_gpu.h) and a thin Python handle.
+
+`load()` opens the in-tree CUDA library aprl_b200/libaprl_b200.so and fails
+loudly when it is missing: there is no CPU fallback.  `bind()` declares the
+ABI signatures on any library that exports them under a given prefix, and
+`Run` drives one handle through the reference-shaped operator sequence.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libaprl_b200.so")
+
+_D = C.POINTER(C.c_double)
+_U64 = C.POINTER(C.c_uint64)
+_I32 = C.POINTER(C.c_int32)
+_I64 = C.POINTER(C.c_int64)
+_SZ = C.POINTER(C.c_size_t)
+
+# name -> (restype, argtypes) with the handle type as `H`.
+_H = object()
+_SIGNATURES = {
+    "last_error": (C.c_char_p, []),
+    "magnet_prepare": (C.c_int, [C.POINTER(abi.Magnet)]),
+    "cowan_coefficients": (C.c_int, [C.c_double, C.c_double, C.c_double, _D]),
+    "run_destroy": (C.c_int, [_H]),
+    "run_set_reference": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_set_field": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_get_field": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_history_length": (C.c_int, [_H, C.c_uint, _U64]),
+    "run_set_history": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_get_history": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_set_particles": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D,
+                                    _D, _D, _U64, C.c_int]),
+    "run_particle_count": (C.c_int, [_H, _SZ]),
+    "run_get_particles": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D,
+                                    _D, _D, _U64, _SZ]),
+    "run_carrier_count": (C.c_int, [_H, _SZ]),
+    "run_get_carriers": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _SZ]),
+    "run_set_carriers": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D]),
+    "run_advance_magnetic": (C.c_int, [_H]),
+    "run_preview_electric": (C.c_int, [_H]),
+    "run_coupling_trial": (C.c_int, [_H, _D]),
+    "run_commit_electric": (C.c_int, [_H]),
+    "run_shift": (C.c_int, [_H]),
+    "run_step": (C.c_int, [_H, C.c_uint32]),
+    "run_get_stats": (C.c_int, [_H, C.POINTER(abi.StepStats)]),
+    "run_get_slot_fields": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _SZ]),
+    "run_sample_field_plane": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
+                                         C.POINTER(C.c_int)]),
+}
+_PRODUCT_ONLY = {
+    "abi_version": (C.c_int, []),
+    "run_synchronize": (C.c_int, [_H]),
+    "run_profile_enable": (C.c_int, [_H, C.c_int]),
+    "run_profile_read": (C.c_int, [_H, _D, _U64, C.c_uint, C.POINTER(C.c_uint)]),
+    "kernel_name": (C.c_char_p, [C.c_uint]),
+    "run_launch_count": (C.c_int, [_H, _U64]),
+    "run_reset_iteration_stats": (C.c_int, [_H]),
+}
+
+
+class AprlError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Binding:
+    """The ABI functions of one library, keyed by their unprefixed names."""
+
+    def __init__(self, lib, prefix, product):
+        self.lib = lib
+        self.prefix = prefix
+        self.product = product
+        self.fn = {}
+        sigs = dict(_SIGNATURES)
+        if product:
+            sigs.update(_PRODUCT_ONLY)
+        for name, (res, args) in sigs.items():
+            f = getattr(lib, prefix + name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = [C.c_void_p if a is _H else a for a in args]
+            self.fn[name] = f
+        create = getattr(lib, prefix + "run_create")
+        create.restype = C.c_int
+        if product:
+            create.argtypes = [C.POINTER(abi.RunConfig), C.c_void_p,
+                               C.POINTER(C.c_void_p)]
+        else:
+            create.argtypes = [C.POINTER(abi.RunConfig), C.POINTER(C.c_void_p)]
+        self.fn["run_create"] = create
+
+    def error(self):
+        msg = self.fn["last_error"]()
+        return msg.decode() if msg else ""
+
+    def check(self, status):
+        if status != abi.APRL_OK:
+            raise AprlError(status, self.error())
+
+    def __call__(self, name, *args):
+        self.check(self.fn[name](*args))
+
+
+def bind(lib, prefix, product=False):
+    return Binding(lib, prefix, product)
+
+
+_PRODUCT = None
+
+
+def load():
+    """The product library; raises when it has not been built."""
+    global _PRODUCT
+    if _PRODUCT is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise ImportError(
+                f"aprl_b200 CUDA library not built: {LIBRARY_PATH} is missing "
+                "(run `python -m aprl_b200.build`); there is no CPU fallback")
+        _PRODUCT = bind(C.CDLL(LIBRARY_PATH), "aprl_", product=True)
+    return _PRODUCT
+
+
+def _ptr(array, ctype=C.c_double):
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+class Run:
+    """One aprl_run (or a checker's run) driven through the ABI."""
+
+    def __init__(self, binding, config, stream=None):
+        self.b = binding
+        self.config = config
+        handle = C.c_void_p()
+        if binding.product:
+            binding.check(binding.fn["run_create"](C.byref(config),
+                                                   C.c_void_p(stream or 0),
+                                                   C.byref(handle)))
+        else:
+            binding.check(binding.fn["run_create"](C.byref(config),
+                                                   C.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            self.b("run_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ----------------------------------------------------------
+    def set_reference(self, tables):
+        for a, t in enumerate(tables):
+            t = np.ascontiguousarray(t, dtype=np.float64)
+            self.b("run_set_reference", self.handle, a, _ptr(t), t.size)
+
+    def set_field(self, component, array):
+        a = np.ascontiguousarray(array, dtype=np.float64)
+        self.b("run_set_field", self.handle, component, _ptr(a), a.size)
+
+    def get_field(self, component):
+        shape = abi.field_shape(self.config, component)
+        out = np.empty(shape[::-1])
+        self.b("run_get_field", self.handle, component, _ptr(out), out.size)
+        return out
+
+    def history_length(self, index):
+        n = C.c_uint64()
+        self.b("run_history_length", self.handle, index, C.byref(n))
+        return n.value
+
+    def get_history(self, index):
+        out = np.empty(self.history_length(index))
+        if out.size:
+            self.b("run_get_history", self.handle, index, _ptr(out), out.size)
+        return out
+
+    def set_history(self, index, array):
+        a = np.ascontiguousarray(array, dtype=np.float64)
+        self.b("run_set_history", self.handle, index, _ptr(a), a.size)
+
+    def set_particles(self, p, reset_carriers=True):
+        cols = [np.ascontiguousarray(p[k], dtype=np.float64)
+                for k in ("x", "y", "z", "ux", "uy", "uz", "charge", "mass")]
+        ids = np.ascontiguousarray(p["id"], dtype=np.uint64)
+        self.b("run_set_particles", self.handle, ids.size,
+               *[_ptr(c) for c in cols], _ptr(ids, C.c_uint64),
+               1 if reset_carriers else 0)
+
+    def particle_count(self):
+        n = C.c_size_t()
+        self.b("run_particle_count", self.handle, C.byref(n))
+        return n.value
+
+    def get_particles(self):
+        n = self.particle_count()
+        out = {k: np.empty(n) for k in ("x", "y", "z", "ux", "uy", "uz",
+                                        "charge", "mass")}
+        out["id"] = np.empty(n, dtype=np.uint64)
+        count = C.c_size_t()
+        self.b("run_get_particles", self.handle, n,
+               *[_ptr(out[k]) for k in ("x", "y", "z", "ux", "uy", "uz",
+                                        "charge", "mass")],
+               _ptr(out["id"], C.c_uint64), C.byref(count))
+        return out
+
+    def carrier_count(self):
+        n = C.c_size_t()
+        self.b("run_carrier_count", self.handle, C.byref(n))
+        return n.value
+
+    def get_carriers(self):
+        n = self.carrier_count()
+        out = {"position": np.empty((n, 3)), "velocity": np.empty((n, 3)),
+               "charge": np.empty(n), "weight": np.empty(n)}
+        count = C.c_size_t()
+        self.b("run_get_carriers", self.handle, n, _ptr(out["position"]),
+               _ptr(out["velocity"]), _ptr(out["charge"]),
+               _ptr(out["weight"]), C.byref(count))
+        return out
+
+    def set_carriers(self, c):
+        pos = np.ascontiguousarray(c["position"], dtype=np.float64)
+        vel = np.ascontiguousarray(c["velocity"], dtype=np.float64)
+        q = np.ascontiguousarray(c["charge"], dtype=np.float64)
+        w = np.ascontiguousarray(c["weight"], dtype=np.float64)
+        self.b("run_set_carriers", self.handle, q.size, _ptr(pos), _ptr(vel),
+               _ptr(q), _ptr(w))
+
+    def load_workload(self, workload):
+        self.set_reference(workload.reference)
+        for a, f in enumerate(workload.fields):
+            self.set_field(a, f)
+        self.set_particles(workload.particles)
+        return self
+
+    # -- operators ------------------------------------------------------
+    def advance_magnetic(self):
+        self.b("run_advance_magnetic", self.handle)
+
+    def preview_electric(self):
+        self.b("run_preview_electric", self.handle)
+
+    def coupling_trial(self):
+        res = (C.c_double * 4)()
+        self.b("run_coupling_trial", self.handle, res)
+        return list(res)
+
+    def commit_electric(self):
+        self.b("run_commit_electric", self.handle)
+
+    def shift(self):
+        self.b("run_shift", self.handle)
+
+    def step(self, steps=1):
+        self.b("run_step", self.handle, steps)
+
+    def stats(self):
+        s = abi.StepStats()
+        self.b("run_get_stats", self.handle, C.byref(s))
+        return s.as_dict()
+
+    def slot_fields(self):
+        n = self.particle_count_slots()
+        out = {k: np.empty((n, 3)) for k in ("used_e", "used_b", "next_e",
+                                             "next_b")}
+        count = C.c_size_t()
+        self.b("run_get_slot_fields", self.handle, n, _ptr(out["used_e"]),
+               _ptr(out["used_b"]), _ptr(out["next_e"]), _ptr(out["next_b"]),
+               C.byref(count))
+        return out
+
+    def particle_count_slots(self):
+        """Slots are sized by the particle list at the last preview; with all
+        output pointers NULL the call only reports that count."""
+        count = C.c_size_t()
+        self.b("run_get_slot_fields", self.handle, 0, None, None, None, None,
+               C.byref(count))
+        return count.value
+
+    def sample_field_plane(self, lab_z):
+        cfg = self.config
+        out = np.empty((cfg.ny, cfg.nx, 6))
+        inside = C.c_int()
+        self.b("run_sample_field_plane", self.handle, lab_z, _ptr(out),
+               out.size, C.byref(inside))
+        return out if inside.value else None
+
+    # -- product-only ---------------------------------------------------
+    def synchronize(self):
+        self.b("run_synchronize", self.handle)
+
+    def profile_enable(self, enabled=True):
+        self.b("run_profile_enable", self.handle, 1 if enabled else 0)
+
+    def profile_read(self):
+        cap = 64
+        ms = (C.c_double * cap)()
+        launches = (C.c_uint64 * cap)()
+        n = C.c_uint()
+        self.b("run_profile_read", self.handle, ms, launches, cap, C.byref(n))
+        names = [self.b.fn["kernel_name"](i).decode() for i in range(n.value)]
+        return {names[i]: (ms[i], launches[i]) for i in range(n.value)
+                if launches[i]}
+
+    def launch_count(self):
+        n = C.c_uint64()
+        self.b("run_launch_count", self.handle, C.byref(n))
+        return n.value

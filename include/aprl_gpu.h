@@ -1,0 +1,302 @@
+/*
+ * aprl_gpu.h -- C ABI of the B200 (sm_100a) implementation of APRL's
+ * per-timestep particle-in-cell loop: Cowan-z E/B update, CFS-CPML, the
+ * conservative-source (Lapenta-Markidis) gather/push with its implicit
+ * fixed-point trials, wide-shape charge-conserving deposition, CPML current
+ * carriers and the moving-window shift.
+ *
+ * The reference has no FFI layer: its seams are C++ classes called directly
+ * by Simulation.  Each entry point below names the reference interface it
+ * replaces (paths are relative to the APRL source tree).  Plain pointers and
+ * sizes only; no C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *   - Every entry point returns an aprl_status.  On failure a message is kept
+ *     in thread-local storage and returned by aprl_last_error(); the reference
+ *     throws std::invalid_argument / std::out_of_range / std::runtime_error in
+ *     the same situations (APRL_ERR_INVALID_ARGUMENT / _OUT_OF_RANGE /
+ *     _RUNTIME).  Device-side failures never trap: kernels raise a flag that
+ *     the host reads after the step.
+ *   - Field arrays use the reference's Yee layout: component extents
+ *     Ex(nx,ny+1,nz+1) Ey(nx+1,ny,nz+1) Ez(nx+1,ny+1,nz) Bx(nx+1,ny,nz)
+ *     By(nx,ny+1,nz) Bz(nx,ny,nz+1), J collocated with E, x fastest:
+ *     index (k*ny_c + j)*nx_c + i (src/eb_field.h:134-141, eb_field.cpp:217-225).
+ *   - SI units throughout, as in the reference E/B core (src/eb_field.h:16-23).
+ *   - A handle is not reentrant: one host thread drives one aprl_run.
+ */
+#ifndef APRL_GPU_H
+#define APRL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define APRL_GPU_ABI_VERSION 1
+
+typedef enum {
+  APRL_OK = 0,
+  APRL_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  APRL_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range (particle/stencil outside the grid) */
+  APRL_ERR_RUNTIME = 3,          /* std::runtime_error (non-finite, crossing budget) */
+  APRL_ERR_NOT_CONVERGED = 4,    /* coupling fixed point exhausted its trials */
+  APRL_ERR_CUDA = 5,             /* CUDA runtime failure */
+  APRL_ERR_UNSUPPORTED = 6       /* valid in the reference, not built here */
+} aprl_status;
+
+/* mesh.longitudinal_shape (src/config.cpp:1097-1112).  linear-binomial3
+ * implies transverseXBinomial3 (the F3 x-z product) in the production code. */
+typedef enum {
+  APRL_SHAPE_LINEAR_BINOMIAL3 = 0,
+  APRL_SHAPE_QUINTIC_COMPENSATED = 1
+} aprl_shape;
+
+/* SIMagnetType (src/eb_sources.h:97-102). */
+typedef enum {
+  APRL_MAGNET_PLANAR_UNDULATOR = 0,
+  APRL_MAGNET_UNIFORM_DIPOLE = 1,
+  APRL_MAGNET_QUADRUPOLE = 2
+} aprl_magnet_type;
+
+/* SIMagneticElement (src/eb_sources.h:103-140).  The derived constants
+ * (wave number, fringe extent, cos/sin of the polarisation angle) are filled
+ * by aprl_magnet_prepare, the counterpart of SIMagneticElement::prepare. */
+typedef struct {
+  int32_t type;                  /* aprl_magnet_type */
+  int32_t gaussian_fringe;       /* planar undulator only */
+  double center[3];              /* m; center[2] is the entrance */
+  double length;                 /* m */
+  double period;                 /* m, planar undulator */
+  double peak_field;             /* T */
+  double polarization_angle;     /* rad from +x */
+  double fringe_relative_cutoff; /* raw Gaussian at the compact edge */
+  double quadrupole_gradient;    /* T/m */
+  /* derived by aprl_magnet_prepare */
+  double wave_number;
+  double fringe_extent;
+  double cos_angle;
+  double sin_angle;
+} aprl_magnet;
+
+#define APRL_MAX_MAGNETS 4
+
+/* Everything a single-GPU run needs.  Mirrors EBGridGeometry (solver fixed to
+ * CowanZ), EBCPMLParameters (z CPML must be 0 under the moving window,
+ * src/config.cpp:2064-2071), BoostFrameTransform, the moving-window state of
+ * Simulation and the coupling tolerances of solveConservativeSourceStep. */
+typedef struct {
+  /* EBGridGeometry (src/eb_field.h:54-70); requires c*dt = dz */
+  uint64_t nx, ny, nz;
+  double dx, dy, dz, dt;
+  /* EBCPMLParameters (src/eb_cpml.h:12-24) for x and y */
+  uint64_t cpml_cells_x, cpml_cells_y;
+  double cpml_polynomial_order;   /* 3 */
+  double cpml_target_reflection;  /* 1e-8 */
+  double cpml_kappa_max;          /* 8 */
+  double cpml_alpha_fraction;     /* 0 */
+  /* particle coupling */
+  int32_t shape;                  /* aprl_shape */
+  uint32_t substeps;              /* particleSubsteps_ (src/simulation.cpp:2623-2685) */
+  uint32_t max_trials;            /* 64 (src/simulation_source_coupling.cpp:40) */
+  uint32_t reserved0;
+  double force_tolerance;         /* 1e-13 (src/simulation_source_coupling.cpp:50) */
+  double work_tolerance;          /* 1e-8 */
+  /* BoostFrameTransform (src/boostframe.h:8-17) */
+  double boost_gamma, boost_beta, boost_gamma_beta;
+  double lab_time_origin, lab_z_origin, box_z_origin;
+  /* moving window (src/simulation_moving_window.cpp:53-117, 275-379) */
+  double reference_origin[3];     /* box-frame origin of the prepared reference */
+  int64_t initial_offset;         /* window start cell in reference native z */
+  uint64_t reference_nz;          /* prepared reference cells in z */
+  double translation_beta;        /* inlet lerp speed, in cells per step */
+  double exit_lab_z;              /* fixed-lab particle exit plane */
+  /* prescribed lab magnets (SIFieldSourceSet::addPrescribedLabMagnet) */
+  uint32_t n_magnets;
+  uint32_t reserved1;
+  aprl_magnet magnets[APRL_MAX_MAGNETS];
+} aprl_run_config;
+
+/* Per-step results of the coupled step (SourceCoupling log row,
+ * src/source_coupling.cpp:189, plus the particle boundary counters of
+ * Simulation, src/simulation.cpp:4841-4901). */
+typedef struct {
+  uint64_t step;                 /* completed steps */
+  uint32_t iterations;           /* fixed-point trials of the last step */
+  uint32_t max_iterations;       /* over all steps since the last reset */
+  uint64_t total_iterations;     /* sum over steps since the last reset */
+  double force;                  /* last converged self-force defect */
+  double work;                   /* last relative work defect */
+  uint64_t particles;            /* active particles after the step */
+  uint64_t carriers;             /* CPML carriers after the step */
+  uint64_t exits;                /* cumulative moving-window exits */
+  double exit_charge;
+  uint64_t cpml_entries[6];      /* cumulative CPML entries by face */
+  double cpml_entry_charge[6];
+  uint64_t carrier_outer[6];     /* carriers leaving through outer faces */
+  double carrier_outer_charge[6];
+  uint64_t cropped_carriers;     /* carriers beyond the window upper edge */
+  double cropped_charge;
+  int64_t window_offset;         /* current window offset (reference cells) */
+  double origin_z;               /* current box-frame window origin z */
+  double time_box;               /* box time after the last step */
+  uint32_t device_error;         /* first device error code seen (0 = none) */
+  uint32_t reserved;
+} aprl_step_stats;
+
+typedef struct aprl_run aprl_run;
+
+/* ---------------------------------------------------------------------- */
+const char* aprl_last_error(void);
+int aprl_abi_version(void);
+
+/* SIMagneticElement::prepare (src/eb_sources.cpp:313-350). */
+aprl_status aprl_magnet_prepare(aprl_magnet* magnet);
+
+/* Cowan-z smoothing coefficients, EBCowanCoefficients::forZDispersion
+ * (src/eb_field.cpp:33-73).  out: alpha[3], beta[3], deltaXY, deltaYZ,
+ * deltaZX, ratio[3] (12 doubles). */
+aprl_status aprl_cowan_coefficients(double dx, double dy, double dz,
+                                    double out[12]);
+
+/* EBFieldGrid(EBGridGeometry) + EBConvolutionalPML + MovingWindowFields +
+ * ConservativeSourceCoupling construction (src/eb_field.cpp:211-229,
+ * src/eb_cpml.cpp:296-372, src/moving_window_fields.cpp:327-360,
+ * src/source_coupling.cpp:62-68).  `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  Allocates all device state of the run. */
+aprl_status aprl_run_create(const aprl_run_config* config, void* stream,
+                            aprl_run** out);
+aprl_status aprl_run_destroy(aprl_run* run);
+
+/* The prepared inlet reference (MovingWindowReference, src/moving_window_fields.h:15-20,
+ * served by Simulation::movingWindowFieldValue, src/simulation_moving_window.cpp:280-294).
+ * `component` 0..5 = Ex,Ey,Ez,Bx,By,Bz in the native layout of a grid with
+ * (nx, ny, reference_nz) cells.  Copied to the device once. */
+aprl_status aprl_run_set_reference(aprl_run* run, unsigned component,
+                                   const double* host, size_t count);
+
+/* EBFieldGrid component accessors (src/eb_field.h:211-229).  component
+ * 0..8 = Ex,Ey,Ez,Bx,By,Bz,Jx,Jy,Jz, logical (window) indexing. */
+aprl_status aprl_run_set_field(aprl_run* run, unsigned component,
+                               const double* host, size_t count);
+aprl_status aprl_run_get_field(aprl_run* run, unsigned component,
+                               double* host, size_t count);
+/* Yee component extents {nx_c, ny_c, nz_c}. */
+aprl_status aprl_run_field_shape(const aprl_run* run, unsigned component,
+                                 uint64_t shape[3]);
+
+/* EBConvolutionalPML::checkpointHistory (src/eb_cpml.cpp:568-596): index
+ * 0..11, magnetic then electric, pairs (0,1),(0,2),(1,2),(1,0),(2,0),(2,1),
+ * in the reference's [slot][k][row] order.  Histories of inactive
+ * (z-derivative) terms have length 0. */
+aprl_status aprl_run_history_length(const aprl_run* run, unsigned index,
+                                    uint64_t* length);
+aprl_status aprl_run_set_history(aprl_run* run, unsigned index,
+                                 const double* host, size_t count);
+aprl_status aprl_run_get_history(aprl_run* run, unsigned index,
+                                 double* host, size_t count);
+
+/* Active particles: RelativisticParticleSI (src/eb_particles.h:12-25) as SoA.
+ * position in m (box frame), proper velocity u = gamma v / c, charge and
+ * mass of the macro-particle (weight already applied), id.  Replaces the
+ * particle list, and resets the carrier list when reset_carriers != 0. */
+aprl_status aprl_run_set_particles(aprl_run* run, size_t count,
+                                   const double* x, const double* y,
+                                   const double* z, const double* ux,
+                                   const double* uy, const double* uz,
+                                   const double* charge, const double* mass,
+                                   const uint64_t* id, int reset_carriers);
+aprl_status aprl_run_particle_count(const aprl_run* run, size_t* count);
+aprl_status aprl_run_get_particles(aprl_run* run, size_t capacity,
+                                   double* x, double* y, double* z,
+                                   double* ux, double* uy, double* uz,
+                                   double* charge, double* mass,
+                                   uint64_t* id, size_t* count);
+/* ParticleCPMLCarrier (src/particle_boundary.h:76-84): position, velocity
+ * (m/s), charge, currentWeight. */
+aprl_status aprl_run_carrier_count(const aprl_run* run, size_t* count);
+aprl_status aprl_run_get_carriers(aprl_run* run, size_t capacity,
+                                  double* position /* 3*count */,
+                                  double* velocity /* 3*count */,
+                                  double* charge, double* weight,
+                                  size_t* count);
+aprl_status aprl_run_set_carriers(aprl_run* run, size_t count,
+                                  const double* position,
+                                  const double* velocity,
+                                  const double* charge, const double* weight);
+
+/* ---- per-operator seams (one step = begin, magnetic, preview, trials,
+ *      commit, shift; aprl_run_step runs them all) ---------------------- */
+
+/* MovingWindowFields::beginStep + physicalElectricHalos + EBFieldGrid::
+ * advanceMagnetic(halo) with the CPML afterMagneticUpdate
+ * (src/simulation.cpp:518-524, src/moving_window_fields.cpp:192-227,
+ * src/eb_field.cpp:488-558, src/eb_cpml.cpp:406-468). */
+aprl_status aprl_run_advance_magnetic(aprl_run* run);
+/* previewElectricBoundary(true) + advanceElectric() with J = 0 + the
+ * boundary preview (src/simulation_source_coupling.cpp:18-24,
+ * src/eb_field.cpp:582-627, src/moving_window_fields.cpp:168-186). */
+aprl_status aprl_run_preview_electric(aprl_run* run);
+/* One fixed-point trial: clearCurrent, restore, carrier advance, push +
+ * deposit of every active particle, and localResidual
+ * (src/simulation_source_coupling.cpp:43-48, src/simulation.cpp:4167-5368,
+ * src/source_coupling.cpp:90-159).  residual = {force, defect, scale, calls}. */
+aprl_status aprl_run_coupling_trial(aprl_run* run, double residual[4]);
+/* Replay + commitConservativeElectric: adopt the last trial's particle and
+ * carrier states and E^{n+1} = E* - dt/eps0 J
+ * (src/simulation_source_coupling.cpp:56-65). */
+aprl_status aprl_run_commit_electric(aprl_run* run);
+/* finishMovingWindowStep (src/simulation_moving_window.cpp:341-379):
+ * MovingWindowFields::shift (src/moving_window_fields.cpp:439-518) as a
+ * z ring-buffer rotation, origin update, carrier crop. */
+aprl_status aprl_run_shift(aprl_run* run);
+
+/* Whole steps: Simulation::solve's loop body for one rank with the moving
+ * window and conservative-source coupling (src/simulation.cpp:493-613). */
+aprl_status aprl_run_step(aprl_run* run, uint32_t steps);
+
+aprl_status aprl_run_get_stats(const aprl_run* run, aprl_step_stats* stats);
+aprl_status aprl_run_reset_iteration_stats(aprl_run* run);
+
+/* Gathered fields of the particles after the last trial: usedE/usedB of the
+ * last push and nextE/nextB of the last residual (Slot,
+ * src/source_coupling.cpp:19), 3*count doubles each; any pointer may be NULL,
+ * and with all four NULL the call only stores the slot count. */
+aprl_status aprl_run_get_slot_fields(aprl_run* run, size_t capacity,
+                                     double* used_e, double* used_b,
+                                     double* next_e, double* next_b,
+                                     size_t* count);
+
+/* Detector field plane at a fixed lab z: LabDetectorManager::sampleFieldPlanes
+ * + samplePlane (src/lab_detectors.cpp:2426-2490, 2836-2905) without the HDF5
+ * writer and without background subtraction.  The plane's box z at the
+ * current box time is boxZFromLabZAndBoxT; each pixel (i,j) at the cell
+ * centre is interpolated per Yee component (src/lab_detectors.cpp:39-99) and
+ * transformed with fieldsBoxToLab.  out: 6*nx*ny doubles, pixel (i,j) ->
+ * out[6*(j*nx+i) + {Ex,Ey,Ez,Bx,By,Bz}] (lab frame).  *inside is 0 (and out
+ * untouched) when the plane lies outside the window. */
+aprl_status aprl_run_sample_field_plane(aprl_run* run, double plane_lab_z,
+                                        double* out, size_t count,
+                                        int* inside);
+
+/* Synchronise the run's stream. */
+aprl_status aprl_run_synchronize(aprl_run* run);
+
+/* Stage timers (the GPU counterpart of APRL_PROFILE_INTERVAL stages,
+ * src/simulation.cpp:5748-5825): CUDA events around every kernel launch on
+ * the run's stream.  aprl_run_profile_read returns, per kernel id, the summed
+ * milliseconds and launch count since enable; names via aprl_kernel_name. */
+aprl_status aprl_run_profile_enable(aprl_run* run, int enabled);
+aprl_status aprl_run_profile_read(aprl_run* run, double* milliseconds,
+                                  uint64_t* launches, unsigned capacity,
+                                  unsigned* kernels);
+const char* aprl_kernel_name(unsigned kernel);
+/* Number of kernels this library launched on the run since creation. */
+aprl_status aprl_run_launch_count(const aprl_run* run, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APRL_GPU_H */

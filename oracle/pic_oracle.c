@@ -1,0 +1,2393 @@
+/*
+ * pic_oracle.c -- CPU oracle (TEST INFRASTRUCTURE ONLY, never part of the
+ * product path) for APRL 2.1's one-rank step with the moving window and the
+ * conservative-source coupling.
+ *
+ * A serial plain-C restatement of the reference algorithm.  Every function
+ * names the reference lines it follows (paths relative to the APRL tree).
+ * Arithmetic keeps the reference's operation order and compiles without
+ * floating-point contraction (-ffp-contract=off), so field updates agree
+ * bit for bit with the reference's own translation units; the reference's
+ * long double work sums are kept as long double.  Exceptions of the
+ * reference become status codes with the same message text.
+ */
+#include "pic_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- SI constants (src/eb_field.cpp:13-20) ---------------------------- */
+#define SI_C 299792458.0
+#define SI_EPSILON0 8.8541878128e-12
+#define SI_MU0 1.25663706212e-6
+#define SI_E 1.602176634e-19
+#define SI_ME 9.1093837139e-31
+#define K_PI 3.14159265358979323846
+#define K_TWO_PI (2.0 * K_PI)
+
+static __thread char g_error[512];
+
+static aprl_status fail(aprl_status status, const char* format, ...) {
+  va_list args;
+  va_start(args, format);
+  vsnprintf(g_error, sizeof g_error, format, args);
+  va_end(args);
+  return status;
+}
+
+const char* oracle_last_error(void) { return g_error; }
+
+/* ---- storage ---------------------------------------------------------- */
+typedef struct {
+  size_t nx, ny, nz;
+  double* v;
+} comp_t;
+
+static inline size_t cidx(const comp_t* c, size_t i, size_t j, size_t k) {
+  return (k * c->ny + j) * c->nx + i;
+}
+#define AT(c, i, j, k) ((c)->v[cidx((c), (i), (j), (k))])
+
+typedef struct {
+  double inverse_kappa_minus_one, decay, drive;
+  int active;
+} cpml_point;
+
+typedef struct {
+  unsigned axis;
+  size_t count;
+  cpml_point* point;
+  size_t* active;  /* activeIndices */
+  size_t nactive;
+} cpml_profile;
+
+typedef struct {
+  unsigned axis;
+  size_t dims[3];
+  size_t* base;  /* baseByAxisIndex, SIZE_MAX = inactive */
+  double* history;
+  size_t length;
+} cpml_term;
+
+typedef struct {
+  double pos[3], u[3];
+  double q, m;
+  uint64_t id;
+} particle_t;
+
+typedef struct {
+  double pos[3], vel[3];
+  double q, w;
+} carrier_t;
+
+typedef struct {
+  particle_t first, last;
+  double guess[3], used_e[3], used_b[3], next_e[3], next_b[3];
+  int seen, initialized, replayed, next_ready;
+  double time, dt;
+  long double abs_grid_work; /* sum over substeps of |BorisWork::gridWork| */
+} slot_t;
+
+typedef struct {
+  unsigned axis;
+  size_t index;
+  double value;
+} preview_delta_t;
+
+struct oracle_run {
+  aprl_run_config cfg;
+  double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
+  comp_t f[9];    /* Ex Ey Ez Bx By Bz Jx Jy Jz */
+  comp_t old[3];  /* ConservativeSourceCoupling::Impl::old */
+  cpml_profile mprof[3], eprof[3];
+  cpml_term mterm[3][3], eterm[3][3];
+  int has_mterm[3][3], has_eterm[3][3];
+  double max_rate[3]; /* ParticleCPMLRegion maximumRate_ */
+  double* lower[3];
+  double* upper[3];
+  preview_delta_t* delta;
+  size_t ndelta, delta_cap;
+  int preview_present;
+  comp_t ref[6];
+  int ref_set[6];
+  /* window / time state */
+  uint64_t step;
+  int64_t offset;
+  double time;
+  double origin[3]; /* globalOriginBox_ == localOriginBox_ at one rank */
+  /* particles and carriers */
+  particle_t* p;
+  size_t np, pcap;
+  carrier_t* c;
+  size_t nc, ccap;
+  slot_t* slot;
+  size_t nslot;
+  /* step-trial scratch */
+  particle_t* retained;
+  size_t nretained, rcap;
+  carrier_t* rcarrier;
+  size_t nrcarrier, rccap;
+  /* counters */
+  uint64_t exits;
+  double exit_charge;
+  uint64_t cpml_entries[6];
+  double cpml_entry_charge[6];
+  uint64_t direct_outer[6];
+  double direct_outer_charge[6];
+  uint64_t carrier_outer[6];
+  double carrier_outer_charge[6];
+  uint64_t cropped_carriers;
+  double cropped_charge;
+  uint32_t last_iterations, max_iterations;
+  uint64_t total_iterations;
+  double last_force, last_work;
+  int replay;
+  int stage; /* 0 idle, 1 magnetic done, 2 preview done, 3 trial done */
+  uint32_t trials_this_step;
+  /* saved state of the step (solveConservativeSourceStep restore()) */
+  particle_t* saved_p;
+  size_t saved_np;
+  carrier_t* saved_c;
+  size_t saved_nc;
+  uint64_t saved_exits;
+  double saved_exit_charge;
+  uint64_t saved_counts[3][6];
+  double saved_charges[3][6];
+};
+
+static void* xrealloc(void* p, size_t bytes) {
+  void* q = realloc(p, bytes ? bytes : 1);
+  if (!q) {
+    fprintf(stderr, "oracle: out of memory\n");
+    abort();
+  }
+  return q;
+}
+
+/* ---- Cowan coefficients: EBCowanCoefficients::forZDispersion
+ *      (src/eb_field.cpp:33-73) ----------------------------------------- */
+aprl_status oracle_cowan_coefficients(double dx, double dy, double dz,
+                                      double out[12]) {
+  if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0) || !isfinite(dx) ||
+      !isfinite(dy) || !isfinite(dz))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Cowan-z grid spacing must be positive and finite");
+  const double tolerance =
+      64.0 * DBL_EPSILON * fmax(dx, fmax(dy, dz));
+  if (dx + tolerance < dz || dy + tolerance < dz)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Cowan-z requires dz to be the smallest grid spacing");
+  double ratio[3];
+  ratio[0] = (dz / dx) * (dz / dx);
+  ratio[1] = (dz / dy) * (dz / dy);
+  ratio[2] = 1.0;
+  const double rx = ratio[0], ry = ratio[1], rz = ratio[2];
+  const double denominator = rx * ry + ry * rz + rz * rx;
+  if (!(denominator > 0.0) || !isfinite(denominator))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid Cowan-z aspect ratios");
+  const double product_fraction = rx * ry * rz / denominator;
+  double beta[3], alpha[3];
+  beta[0] = rx * (1.0 - product_fraction) / 8.0;
+  beta[1] = ry * (1.0 - product_fraction) / 8.0;
+  beta[2] = rz * (1.0 - product_fraction) / 8.0;
+  const double delta_xy = rx * ry * (1.0 / 16.0 - rx * ry / (8.0 * denominator));
+  const double delta_yz = ry * rz * (1.0 / 16.0 - ry * rz / (8.0 * denominator));
+  const double delta_zx = rz * rx * (1.0 / 16.0 - rz * rx / (8.0 * denominator));
+  alpha[0] = 1.0 - 2.0 * beta[1] - 2.0 * beta[2] - 4.0 * delta_yz;
+  alpha[1] = 1.0 - 2.0 * beta[2] - 2.0 * beta[0] - 4.0 * delta_zx;
+  alpha[2] = 1.0 - 2.0 * beta[0] - 2.0 * beta[1] - 4.0 * delta_xy;
+  out[0] = alpha[0]; out[1] = alpha[1]; out[2] = alpha[2];
+  out[3] = beta[0]; out[4] = beta[1]; out[5] = beta[2];
+  out[6] = delta_xy; out[7] = delta_yz; out[8] = delta_zx;
+  out[9] = ratio[0]; out[10] = ratio[1]; out[11] = ratio[2];
+  return APRL_OK;
+}
+
+/* ---- SIMagneticElement::prepare (src/eb_sources.cpp:313-350) ----------- */
+aprl_status oracle_magnet_prepare(aprl_magnet* m) {
+  if (!isfinite(m->center[0]) || !isfinite(m->center[1]) ||
+      !isfinite(m->center[2]) || !(m->length >= 0.0) || !isfinite(m->length) ||
+      !isfinite(m->peak_field) || !isfinite(m->polarization_angle))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI magnetic element");
+  if (m->type == APRL_MAGNET_PLANAR_UNDULATOR &&
+      (!(m->period > 0.0) || !isfinite(m->period)))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Undulator period must be positive");
+  if (m->type == APRL_MAGNET_PLANAR_UNDULATOR && m->gaussian_fringe &&
+      (!(m->fringe_relative_cutoff > 0.0) ||
+       !(m->fringe_relative_cutoff < 1.0) || !isfinite(m->fringe_relative_cutoff)))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Undulator fringe_relative_cutoff must be in (0,1)");
+  if (m->type == APRL_MAGNET_UNIFORM_DIPOLE && !(m->length > 0.0))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Dipole length must be positive");
+  if (m->type == APRL_MAGNET_QUADRUPOLE &&
+      (!(m->length > 0.0) || !isfinite(m->quadrupole_gradient)))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Quadrupole length/gradient is invalid");
+  m->wave_number = m->type == APRL_MAGNET_PLANAR_UNDULATOR ? K_TWO_PI / m->period : 0.0;
+  m->fringe_extent = m->type == APRL_MAGNET_PLANAR_UNDULATOR && m->gaussian_fringe
+      ? sqrt(-2.0 * log(m->fringe_relative_cutoff)) / m->wave_number
+      : 0.0;
+  m->cos_angle = cos(m->polarization_angle);
+  m->sin_angle = sin(m->polarization_angle);
+  return APRL_OK;
+}
+
+/* SIMagneticElement::fieldsLab (src/eb_sources.cpp:352-447), magnetic only;
+ * internal end ramps and undulator phase are not modelled (zero defaults). */
+static void magnet_fields_lab(const aprl_magnet* m, const double pos[3],
+                              double b[3]) {
+  b[0] = b[1] = b[2] = 0.0;
+  double rel[3] = {pos[0] - m->center[0], pos[1] - m->center[1],
+                   pos[2] - m->center[2]};
+  const double z = rel[2];
+  if (m->type == APRL_MAGNET_QUADRUPOLE) {
+    if (z >= 0.0 && z <= m->length) {
+      const double x = rel[0] * m->cos_angle + rel[1] * m->sin_angle;
+      const double y = -rel[0] * m->sin_angle + rel[1] * m->cos_angle;
+      const double bx = m->quadrupole_gradient * y;
+      const double by = m->quadrupole_gradient * x;
+      b[0] = bx * m->cos_angle - by * m->sin_angle;
+      b[1] = bx * m->sin_angle + by * m->cos_angle;
+    }
+    return;
+  }
+  if (m->type == APRL_MAGNET_UNIFORM_DIPOLE) {
+    if (z >= 0.0 && z <= m->length) {
+      b[0] = m->peak_field * m->cos_angle;
+      b[1] = m->peak_field * m->sin_angle;
+    }
+    return;
+  }
+  double transverse_shape = 0.0, longitudinal_shape = 0.0;
+  const double k = m->wave_number;
+  if (z >= 0.0 && z <= m->length) {
+    transverse_shape = sin(k * z);
+    longitudinal_shape = cos(k * z);
+  } else if (m->gaussian_fringe) {
+    const double fringe_coordinate = z < 0.0 ? z : z - m->length;
+    const double distance = fabs(fringe_coordinate);
+    if (distance >= m->fringe_extent) return;
+    const double q = distance / m->fringe_extent;
+    const double q2 = q * q, q3 = q2 * q, q4 = q3 * q, q5 = q4 * q;
+    const double taper = 1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5;
+    const double taper_derivative =
+        (-30.0 * q2 + 60.0 * q3 - 30.0 * q4) / m->fringe_extent;
+    const double gaussian = exp(-0.5 * pow(k * distance, 2.0));
+    longitudinal_shape = gaussian * taper;
+    const double derivative_by_distance =
+        gaussian * (taper_derivative - k * k * distance * taper);
+    transverse_shape = z < 0.0 ? derivative_by_distance / k
+                               : -derivative_by_distance / k;
+  } else {
+    return;
+  }
+  const double tc = rel[0] * m->cos_angle + rel[1] * m->sin_angle;
+  const double transverse_field = m->peak_field * cosh(k * tc) * transverse_shape;
+  b[0] = transverse_field * m->cos_angle;
+  b[1] = transverse_field * m->sin_angle;
+  b[2] = m->peak_field * sinh(k * tc) * longitudinal_shape;
+}
+
+/* BoostFrameTransform::boxToLab (src/boostframe.cpp:221-229). */
+static void box_to_lab(const aprl_run_config* g, double t_box, double z_box,
+                       double* t_lab, double* z_lab) {
+  const double z_shift = z_box - g->box_z_origin;
+  *z_lab = g->lab_z_origin + fma(g->boost_gamma_beta * SI_C, t_box,
+                                 g->boost_gamma * z_shift);
+  *t_lab = g->lab_time_origin + fma(g->boost_gamma_beta / SI_C, z_shift,
+                                    g->boost_gamma * t_box);
+}
+
+/* BoostFrameTransform::labZFromBoxZT (src/boostframe.cpp:241-245). */
+static double lab_z_from_box_zt(const aprl_run_config* g, double z_box,
+                                double t_box) {
+  return g->lab_z_origin +
+         fma(g->boost_gamma_beta * SI_C, t_box, g->boost_gamma * (z_box - g->box_z_origin));
+}
+
+/* BoostFrameTransform::boxZFromLabZAndBoxT (src/boostframe.cpp:231-235). */
+static double box_z_from_lab_z_and_box_t(const aprl_run_config* g, double z_lab,
+                                         double t_box) {
+  return g->box_z_origin + (z_lab - g->lab_z_origin) / g->boost_gamma -
+         g->boost_beta * SI_C * t_box;
+}
+
+/* fieldsLabToBox / fieldsBoxToLab (src/boostframe.cpp:262-285). */
+static void fields_lab_to_box(const aprl_run_config* g, const double el[3],
+                              const double bl[3], double eb[3], double bb[3]) {
+  const double gb = g->boost_gamma_beta, ga = g->boost_gamma;
+  eb[0] = fma(-gb * SI_C, bl[1], ga * el[0]);
+  eb[1] = fma(gb * SI_C, bl[0], ga * el[1]);
+  eb[2] = el[2];
+  bb[0] = fma(gb / SI_C, el[1], ga * bl[0]);
+  bb[1] = fma(-gb / SI_C, el[0], ga * bl[1]);
+  bb[2] = bl[2];
+}
+
+static void fields_box_to_lab(const aprl_run_config* g, const double eb[3],
+                              const double bb[3], double el[3], double bl[3]) {
+  const double gb = g->boost_gamma_beta, ga = g->boost_gamma;
+  el[0] = fma(gb * SI_C, bb[1], ga * eb[0]);
+  el[1] = fma(-gb * SI_C, bb[0], ga * eb[1]);
+  el[2] = eb[2];
+  bl[0] = fma(-gb / SI_C, eb[1], ga * bb[0]);
+  bl[1] = fma(gb / SI_C, eb[0], ga * bb[1]);
+  bl[2] = bb[2];
+}
+
+/* SIFieldSourceSet::addPrescribedBox -> transformSampleToBox
+ * (src/eb_sources.cpp:537-582): lab magnets only. */
+static void add_prescribed_box(const aprl_run_config* g, const double pos[3],
+                               double t_box, double e[3], double b[3]) {
+  if (g->n_magnets == 0) return;
+  double pos_lab[3] = {pos[0], pos[1], pos[2]};
+  double t_lab = 0.0;
+  box_to_lab(g, t_box, pos[2], &t_lab, &pos_lab[2]);
+  double el[3] = {0.0, 0.0, 0.0}, bl[3] = {0.0, 0.0, 0.0};
+  for (uint32_t n = 0; n < g->n_magnets; ++n) {
+    double contribution[3];
+    magnet_fields_lab(&g->magnets[n], pos_lab, contribution);
+    for (int a = 0; a < 3; ++a) bl[a] += contribution[a];
+  }
+  double ebx[3], bbx[3];
+  fields_lab_to_box(g, el, bl, ebx, bbx);
+  for (int a = 0; a < 3; ++a) {
+    e[a] += ebx[a];
+    b[a] += bbx[a];
+  }
+}
+
+aprl_status oracle_prescribed_box(const aprl_run_config* config,
+                                  const double position[3], double time,
+                                  double e[3], double b[3]) {
+  e[0] = e[1] = e[2] = b[0] = b[1] = b[2] = 0.0;
+  add_prescribed_box(config, position, time, e, b);
+  return APRL_OK;
+}
+
+/* BoostFrameTransform::gammaFromProperVelocity (src/boostframe.cpp:74-87). */
+static double gamma_u(const double u[3]) {
+  const double scale = fmax(1.0, fmax(fabs(u[0]), fmax(fabs(u[1]), fabs(u[2]))));
+  const double inverse_scale = 1.0 / scale;
+  const double ux = u[0] * inverse_scale, uy = u[1] * inverse_scale,
+               uz = u[2] * inverse_scale;
+  return scale * sqrt(inverse_scale * inverse_scale + ux * ux + uy * uy + uz * uz);
+}
+
+double oracle_gamma(const double u[3]) { return gamma_u(u); }
+
+static inline double dot3(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+static inline void cross3(const double l[3], const double r[3], double o[3]) {
+  o[0] = l[1] * r[2] - l[2] * r[1];
+  o[1] = l[2] * r[0] - l[0] * r[2];
+  o[2] = l[0] * r[1] - l[1] * r[0];
+}
+
+/* source_coupling_math::momentum: Lapenta-Markidis mean-gamma Newton solve
+ * (src/source_coupling_math.h:272-293).  Returns iterations+1, or -1 for a
+ * nonphysical root, -2 for no convergence. */
+int oracle_momentum(double u[3], const double e[3], const double magnetic[3],
+                    double q, double m, double h, double known_gamma) {
+  const double before[3] = {u[0], u[1], u[2]};
+  const double g0 = known_gamma > 0.0 ? known_gamma : gamma_u(before);
+  const double ks = q * h / (2 * m * SI_C);
+  const double bs = q * h / (2 * m);
+  double kick[3], b[3], a[3], axb[3];
+  for (int i = 0; i < 3; ++i) {
+    kick[i] = e[i] * ks;
+    b[i] = magnetic[i] * bs;
+  }
+  for (int i = 0; i < 3; ++i) a[i] = before[i] + kick[i];
+  cross3(a, b, axb);
+  const double b2 = dot3(b, b), ka = dot3(kick, a), kb = dot3(kick, b),
+               ab = dot3(a, b), kcross = dot3(kick, axb);
+  const double first = dot3(kick, before) / g0;
+  double G = g0 + first + (dot3(kick, kick) + kcross / g0 - first * first) / g0;
+  G = fmax(G, .5 * (g0 + 1.));
+  unsigned iteration = 0;
+  for (; iteration < 12; ++iteration) {
+    const double den = G * G + b2, numerator = G * G * ka + G * kcross + ab * kb;
+    const double f = G * (G - g0) - numerator / den;
+    const double derivative =
+        2 * G - g0 - ((2 * G * ka + kcross) * den - 2 * G * numerator) / (den * den);
+    const double correction = f / derivative;
+    const double next = G - correction;
+    if (!isfinite(next) || next < .5 * (g0 + 1.) - 1e-13) return -1;
+    G = fmax(next, .5 * (g0 + 1.));
+    if (fabs(correction) <= 8 * DBL_EPSILON * fmax(1., G)) break;
+  }
+  if (iteration == 12) return -2;
+  const double den = G * G + b2;
+  for (int k = 0; k < 3; ++k)
+    u[k] = 2 * (G * G * a[k] + ab * b[k] + G * axb[k]) / den - before[k];
+  return (int)iteration + 1;
+}
+
+/* source_coupling_math::chargeWork (src/source_coupling_math.h:24-26). */
+static long double charge_work(double q, const double e[3], const double x[3],
+                               const double y[3]) {
+  long double s = 0;
+  for (int a = 0; a < 3; ++a)
+    s += (long double)q * e[a] * ((long double)y[a] - x[a]);
+  return s;
+}
+
+/* ---- longitudinal shapes (src/longitudinal_shape.h:15-117,
+ *      src/transverse_source_shape.h:8-10) ------------------------------ */
+typedef struct {
+  long long first;
+  unsigned count;
+  double v[12];
+} basis_t;
+
+static void node_weights(double f, double w[4]) {
+  w[0] = 0.25 * (1. - f);
+  w[1] = 0.5 - 0.25 * f;
+  w[2] = 0.25 + 0.25 * f;
+  w[3] = 0.25 * f;
+}
+
+/* basis() for the two production shapes (src/longitudinal_shape.h:25-55). */
+static basis_t shape_basis(double z, int edge, int shape) {
+  basis_t r;
+  if (shape == APRL_SHAPE_LINEAR_BINOMIAL3) {
+    const double cell = floor(z), f = z - cell;
+    const double c[3] = {.25, .5, .25};
+    r.first = (long long)cell - 1;
+    r.count = edge ? 3 : 4;
+    for (int n = 0; n < 12; ++n) r.v[n] = 0.;
+    for (int k = -1; k <= 1; ++k) {
+      const double w = c[k + 1];
+      if (edge)
+        r.v[k + 1] += w;
+      else {
+        r.v[k + 1] += w * (1. - f);
+        r.v[k + 2] += w * f;
+      }
+    }
+    return r;
+  }
+  const unsigned degree = edge ? 4 : 5;
+  const double cell = floor(z), f = z - cell;
+  double n[6] = {1., 0., 0., 0., 0., 0.};
+  for (unsigned j = 1; j <= degree; ++j) {
+    double saved = 0.;
+    for (unsigned k = 0; k < j; ++k) {
+      const double t = n[k] / j;
+      n[k] = saved + (k + 1 - f) * t;
+      saved = (f + j - k - 1) * t;
+    }
+    n[j] = saved;
+  }
+  const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
+               d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
+  const double c[7] = {-d / 64., b / 16. + 3 * d / 32., -a / 4. - b / 4. - 15 * d / 64.,
+                       1 + a / 2. + 3 * b / 8. + 5 * d / 16.,
+                       -a / 4. - b / 4. - 15 * d / 64., b / 16. + 3 * d / 32., -d / 64.};
+  r.first = (long long)cell - 5;
+  r.count = degree + 7;
+  for (int q = 0; q < 12; ++q) r.v[q] = 0.;
+  for (unsigned j = 0; j <= degree; ++j)
+    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
+  return r;
+}
+
+/* Visitor interface of longitudinal_shape::weights. */
+typedef struct visitor visitor_t;
+struct visitor {
+  void (*visit)(visitor_t*, unsigned axis, long long i, long long j,
+                long long k, double w);
+};
+
+/* binomialXZSegment (src/longitudinal_shape.h:61-94). */
+static void binomial_xz_segment(const aprl_run_config* g, const double start[3],
+                                const double delta[3], double first,
+                                double last, visitor_t* visit) {
+  const double width = last - first;
+  const double mid = (first + last) * 0.5;
+  const double x = start[0] + mid * delta[0], y = start[1] + mid * delta[1],
+               z = start[2] + mid * delta[2];
+  long long i = (long long)floor(x), j = (long long)floor(y);
+  const long long k = (long long)floor(z);
+  if (i == (long long)g->nx) --i;
+  if (j == (long long)g->ny) --j;
+  double wx[4], wz[4];
+  node_weights(x - i, wx);
+  node_weights(z - k, wz);
+  const double wy[2] = {1. - (y - j), y - j};
+  const double edge[3] = {0.25, 0.5, 0.25};
+  const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
+  const double sy[2] = {-1., 1.};
+  const double curvature = width * width / 12.;
+  const double xy = curvature * delta[0] * delta[1];
+  const double xz = curvature * delta[0] * delta[2];
+  const double yz = curvature * delta[1] * delta[2];
+  for (unsigned c = 0; c < 4; ++c) {
+    for (unsigned b = 0; b < 2; ++b) {
+      const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+      for (unsigned a = 0; a < 3; ++a)
+        visit->visit(visit, 0, i - 1 + a, j + b, k - 1 + c, weight * edge[a]);
+    }
+    for (unsigned a = 0; a < 4; ++a)
+      visit->visit(visit, 1, i - 1 + a, j, k - 1 + c,
+                   width * (wx[a] * wz[c] + xz * slope[a] * slope[c]));
+  }
+  for (unsigned b = 0; b < 2; ++b)
+    for (unsigned a = 0; a < 4; ++a) {
+      const double weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+      for (unsigned c = 0; c < 3; ++c)
+        visit->visit(visit, 2, i - 1 + a, j + b, k - 1 + c, weight * edge[c]);
+    }
+}
+
+static int cmp_double(const void* a, const void* b) {
+  const double x = *(const double*)a, y = *(const double*)b;
+  return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* longitudinal_shape::weights (src/longitudinal_shape.h:97-117), with
+ * smoothX = (shape == linear-binomial3) as in production
+ * (src/config.cpp:1097-1112).  Returns segments, or -1 on crossing budget. */
+static int shape_weights(const aprl_run_config* g, const double origin[3],
+                         const double begin[3], const double end[3],
+                         visitor_t* visit) {
+  const double h[3] = {g->dx, g->dy, g->dz};
+  double x[3], v[3], cuts[64];
+  unsigned count = 2;
+  cuts[0] = 0.;
+  cuts[1] = 1.;
+  for (unsigned a = 0; a < 3; ++a) {
+    x[a] = (begin[a] - origin[a]) / h[a];
+    v[a] = (end[a] - begin[a]) / h[a];
+    if (v[a] != 0.)
+      for (long long j = (long long)floor(fmin(x[a], x[a] + v[a])) + 1;
+           j < fmax(x[a], x[a] + v[a]); ++j) {
+        if (count == 64) return -1;
+        cuts[count++] = (j - x[a]) / v[a];
+      }
+  }
+  qsort(cuts, count, sizeof(double), cmp_double);
+  const double q[4] = {-.8611363115940525752, -.3399810435848562648,
+                       .3399810435848562648, .8611363115940525752};
+  const double qw[4] = {.3478548451374538574, .6521451548625461426,
+                        .6521451548625461426, .3478548451374538574};
+  int segments = 0;
+  for (unsigned s = 1; s < count; ++s) {
+    const double width = cuts[s] - cuts[s - 1];
+    if (width <= 0.) continue;
+    ++segments;
+    if (g->shape == APRL_SHAPE_LINEAR_BINOMIAL3) {
+      binomial_xz_segment(g, x, v, cuts[s - 1], cuts[s], visit);
+      continue;
+    }
+    for (unsigned t = 0; t < 4; ++t) {
+      const double node = q[t], weight = qw[t];
+      const double u = .5 * (cuts[s] + cuts[s - 1] + width * node),
+                   factor = .5 * width * weight, xx = x[0] + u * v[0],
+                   yy = x[1] + u * v[1], zz = x[2] + u * v[2];
+      long long i = (long long)floor(xx), j = (long long)floor(yy);
+      if (i == (long long)g->nx) --i;
+      if (j == (long long)g->ny) --j;
+      const double fx = xx - i, fy = yy - j;
+      const basis_t nodes = shape_basis(zz, 0, g->shape),
+                    edge = shape_basis(zz, 1, g->shape);
+      for (unsigned k = 0; k < nodes.count; ++k) {
+        const double w = factor * nodes.v[k];
+        if (w == 0.) continue;
+        for (unsigned b = 0; b < 2; ++b)
+          visit->visit(visit, 0, i, j + b, nodes.first + k, w * (b ? fy : 1. - fy));
+        for (unsigned a = 0; a < 2; ++a)
+          visit->visit(visit, 1, i + a, j, nodes.first + k, w * (a ? fx : 1. - fx));
+      }
+      for (unsigned k = 0; k < edge.count; ++k) {
+        const double w = factor * edge.v[k];
+        if (w == 0.) continue;
+        for (unsigned b = 0; b < 2; ++b)
+          for (unsigned a = 0; a < 2; ++a)
+            visit->visit(visit, 2, i + a, j + b, edge.first + k,
+                         w * (a ? fx : 1. - fx) * (b ? fy : 1. - fy));
+      }
+    }
+  }
+  return segments;
+}
+
+typedef struct {
+  visitor_t base;
+  int32_t* axis;
+  int64_t* index;
+  double* weight;
+  long count, capacity;
+} record_visitor;
+
+static void record_visit(visitor_t* v, unsigned axis, long long i, long long j,
+                         long long k, double w) {
+  record_visitor* r = (record_visitor*)v;
+  if (r->count < r->capacity) {
+    r->axis[r->count] = (int32_t)axis;
+    r->index[3 * r->count] = i;
+    r->index[3 * r->count + 1] = j;
+    r->index[3 * r->count + 2] = k;
+    r->weight[r->count] = w;
+  }
+  ++r->count;
+}
+
+long oracle_shape_weights(const aprl_run_config* config, const double origin[3],
+                          const double begin[3], const double end[3],
+                          int32_t* axis, int64_t* index, double* weight,
+                          long capacity) {
+  record_visitor r;
+  r.base.visit = record_visit;
+  r.axis = axis;
+  r.index = index;
+  r.weight = weight;
+  r.count = 0;
+  r.capacity = capacity;
+  if (shape_weights(config, origin, begin, end, &r.base) < 0) {
+    fail(APRL_ERR_RUNTIME, "Quintic orbit exceeds crossing budget");
+    return -1;
+  }
+  return r.count;
+}
+
+/* ---- run construction -------------------------------------------------- */
+static void comp_shape(const aprl_run_config* g, unsigned a, size_t s[3]) {
+  /* moving_window_fields.cpp shape(): electric and current components are
+   * node-centred off their own axis, magnetic ones on it. */
+  const int electric = a < 3 || a >= 6;
+  const unsigned axis = a % 3;
+  const size_t cells[3] = {g->nx, g->ny, g->nz};
+  for (unsigned d = 0; d < 3; ++d)
+    s[d] = cells[d] + (electric ? (d != axis) : (d == axis));
+}
+
+static void comp_alloc(comp_t* c, const size_t s[3]) {
+  c->nx = s[0];
+  c->ny = s[1];
+  c->nz = s[2];
+  c->v = (double*)calloc((s[0] * s[1] * s[2]) ? s[0] * s[1] * s[2] : 1, sizeof(double));
+}
+
+/* EBCPMLParameters::maximumConductivityRate (src/eb_cpml.cpp:277-294). */
+static double maximum_rate(const aprl_run_config* g, unsigned axis) {
+  const size_t cells = axis == 0 ? g->cpml_cells_x : (axis == 1 ? g->cpml_cells_y : 0);
+  if (cells == 0) return 0.0;
+  const double spacing = axis == 0 ? g->dx : (axis == 1 ? g->dy : g->dz);
+  const double thickness = (double)cells * spacing;
+  return -(g->cpml_polynomial_order + 1.0) * SI_C *
+         log(g->cpml_target_reflection) / (2.0 * thickness);
+}
+
+/* makeProfile (src/eb_cpml.cpp:195-248) at one rank (z offset 0). */
+static void make_profile(const aprl_run_config* g, unsigned axis, int electric,
+                         cpml_profile* r) {
+  r->axis = axis;
+  const size_t local_cells = axis == 0 ? g->nx : (axis == 1 ? g->ny : g->nz);
+  const size_t count = local_cells + (electric ? 1 : 0);
+  r->count = count;
+  r->point = (cpml_point*)calloc(count, sizeof(cpml_point));
+  r->active = (size_t*)calloc(count, sizeof(size_t));
+  r->nactive = 0;
+  const size_t thickness_cells =
+      axis == 0 ? g->cpml_cells_x : (axis == 1 ? g->cpml_cells_y : 0);
+  if (thickness_cells == 0) return;
+  const double thickness = (double)thickness_cells;
+  const double sigma_rate_maximum = maximum_rate(g, axis);
+  for (size_t local = 0; local < count; ++local) {
+    const double position = (double)local + (electric ? 0.0 : 0.5);
+    double depth = 0.0;
+    if (position < thickness) depth = (thickness - position) / thickness;
+    const double upper_start = (double)(local_cells - thickness_cells);
+    if (position > upper_start) depth = fmax(depth, (position - upper_start) / thickness);
+    if (!(depth > 0.0)) continue;
+    depth = fmin(1.0, depth);
+    const double graded = pow(depth, g->cpml_polynomial_order);
+    const double sigma_rate = sigma_rate_maximum * graded;
+    const double kappa = 1.0 + (g->cpml_kappa_max - 1.0) * graded;
+    const double alpha_rate = g->cpml_alpha_fraction * sigma_rate_maximum * (1.0 - depth);
+    cpml_point* c = &r->point[local];
+    c->inverse_kappa_minus_one = 1.0 / kappa - 1.0;
+    c->decay = exp(-(sigma_rate / kappa + alpha_rate) * g->dt);
+    const double denominator = sigma_rate * kappa + alpha_rate * kappa * kappa;
+    c->drive = denominator > 0.0 ? sigma_rate * (c->decay - 1.0) / denominator : 0.0;
+    c->active = 1;
+    r->active[r->nactive++] = local;
+  }
+}
+
+/* CPMLMemoryTerm (src/eb_cpml.cpp:42-96). */
+static void make_term(unsigned derivative, const size_t shape[3],
+                      const cpml_profile* profile, cpml_term* t) {
+  t->axis = derivative;
+  for (int d = 0; d < 3; ++d) t->dims[d] = shape[d];
+  t->base = (size_t*)malloc(sizeof(size_t) * (shape[derivative] ? shape[derivative] : 1));
+  for (size_t n = 0; n < shape[derivative]; ++n) t->base[n] = SIZE_MAX;
+  const size_t cross = derivative == 0 ? shape[1] * shape[2]
+                       : (derivative == 1 ? shape[0] * shape[2] : shape[0] * shape[1]);
+  t->length = profile->nactive * cross;
+  t->history = (double*)calloc(t->length ? t->length : 1, sizeof(double));
+  for (size_t o = 0; o < profile->nactive; ++o) t->base[profile->active[o]] = o * cross;
+}
+
+static inline double* term_value(cpml_term* t, size_t i, size_t j, size_t k) {
+  const size_t axis_index = t->axis == 0 ? i : (t->axis == 1 ? j : k);
+  const size_t base = t->base[axis_index];
+  const size_t cross = t->axis == 0 ? k * t->dims[1] + j
+                       : (t->axis == 1 ? k * t->dims[0] + i : j * t->dims[0] + i);
+  return &t->history[base + cross];
+}
+
+static aprl_status validate_config(const aprl_run_config* g) {
+  if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "E/B staggered grid needs at least two cells in every direction");
+  if (!(g->dx > 0.0) || !(g->dy > 0.0) || !(g->dz > 0.0) || !(g->dt > 0.0) ||
+      !isfinite(g->dx) || !isfinite(g->dy) || !isfinite(g->dz) || !isfinite(g->dt))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "E/B grid spacing and time step must be positive finite SI values");
+  if (fabs(SI_C * g->dt - g->dz) > 64 * DBL_EPSILON * g->dz)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Moving-window requires c*dt=dz");
+  if (g->cpml_cells_x < 2 || g->cpml_cells_y < 2 || 2 * g->cpml_cells_x >= g->nx ||
+      2 * g->cpml_cells_y >= g->ny)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Moving-window requires valid Cowan integer z slabs, xy-only CPML and an inlet reference");
+  if (!(g->cpml_polynomial_order > 0.0) ||
+      !(g->cpml_target_reflection > 0.0 && g->cpml_target_reflection < 1.0) ||
+      !(g->cpml_kappa_max >= 1.0) || !(g->cpml_alpha_fraction >= 0.0))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid CPML grading parameters");
+  if (g->shape != APRL_SHAPE_LINEAR_BINOMIAL3 && g->shape != APRL_SHAPE_QUINTIC_COMPENSATED)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "APRL 2.1 longitudinal_shape must be linear-binomial3 or quintic-compensated");
+  if (g->substeps < 1 || g->max_trials < 1 || g->max_trials > 64)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid substep or trial count");
+  if (!(g->boost_gamma >= 1.0) || !isfinite(g->boost_gamma))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Lorentz gamma must be finite and >= 1");
+  if (g->n_magnets > APRL_MAX_MAGNETS)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Too many prescribed magnets");
+  return APRL_OK;
+}
+
+aprl_status oracle_run_create(const aprl_run_config* config, oracle_run** out) {
+  aprl_status s = validate_config(config);
+  if (s != APRL_OK) return s;
+  oracle_run* r = (oracle_run*)calloc(1, sizeof(oracle_run));
+  r->cfg = *config;
+  double co[12];
+  s = oracle_cowan_coefficients(config->dx, config->dy, config->dz, co);
+  if (s != APRL_OK) {
+    free(r);
+    return s;
+  }
+  for (int a = 0; a < 3; ++a) {
+    r->alpha[a] = co[a];
+    r->beta[a] = co[3 + a];
+  }
+  r->delta_xy = co[6];
+  r->delta_yz = co[7];
+  r->delta_zx = co[8];
+  for (unsigned a = 0; a < 9; ++a) {
+    size_t sh[3];
+    comp_shape(config, a, sh);
+    comp_alloc(&r->f[a], sh);
+    if (a < 3) comp_alloc(&r->old[a], sh);
+    if (a < 6) {
+      size_t rs[3] = {sh[0], sh[1], config->reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0)};
+      r->ref[a].nx = rs[0];
+      r->ref[a].ny = rs[1];
+      r->ref[a].nz = rs[2];
+      r->ref[a].v = NULL;
+    }
+  }
+  for (unsigned axis = 0; axis < 3; ++axis) {
+    make_profile(config, axis, 0, &r->mprof[axis]);
+    make_profile(config, axis, 1, &r->eprof[axis]);
+    r->max_rate[axis] = maximum_rate(config, axis);
+  }
+  const unsigned pairs[6][2] = {{0, 1}, {0, 2}, {1, 2}, {1, 0}, {2, 0}, {2, 1}};
+  for (unsigned pair = 0; pair < 6; ++pair) {
+    const unsigned comp = pairs[pair][0], der = pairs[pair][1];
+    size_t sh[3];
+    comp_shape(config, 3 + comp, sh);
+    make_term(der, sh, &r->mprof[der], &r->mterm[comp][der]);
+    r->has_mterm[comp][der] = 1;
+    comp_shape(config, comp, sh);
+    make_term(der, sh, &r->eprof[der], &r->eterm[comp][der]);
+    r->has_eterm[comp][der] = 1;
+  }
+  for (unsigned a = 0; a < 3; ++a) {
+    const size_t n = r->f[a].nx * r->f[a].ny;
+    r->lower[a] = (double*)calloc(n, sizeof(double));
+    r->upper[a] = (double*)calloc(n, sizeof(double));
+  }
+  r->offset = config->initial_offset;
+  r->origin[0] = config->reference_origin[0];
+  r->origin[1] = config->reference_origin[1];
+  r->origin[2] = fma((double)config->initial_offset, config->dz, config->reference_origin[2]);
+  *out = r;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_destroy(oracle_run* r) {
+  if (!r) return APRL_OK;
+  for (int a = 0; a < 9; ++a) free(r->f[a].v);
+  for (int a = 0; a < 3; ++a) {
+    free(r->old[a].v);
+    free(r->lower[a]);
+    free(r->upper[a]);
+  }
+  for (int a = 0; a < 6; ++a) free(r->ref[a].v);
+  for (int a = 0; a < 3; ++a) {
+    free(r->mprof[a].point); free(r->mprof[a].active);
+    free(r->eprof[a].point); free(r->eprof[a].active);
+    for (int d = 0; d < 3; ++d) {
+      if (r->has_mterm[a][d]) { free(r->mterm[a][d].base); free(r->mterm[a][d].history); }
+      if (r->has_eterm[a][d]) { free(r->eterm[a][d].base); free(r->eterm[a][d].history); }
+    }
+  }
+  free(r->delta); free(r->p); free(r->c); free(r->slot); free(r->retained);
+  free(r->rcarrier); free(r->saved_p); free(r->saved_c);
+  free(r);
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_reference(oracle_run* r, unsigned a, const double* host,
+                                     size_t count) {
+  if (a >= 6) return fail(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
+  const size_t n = r->ref[a].nx * r->ref[a].ny * r->ref[a].nz;
+  if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
+  free(r->ref[a].v);
+  r->ref[a].v = (double*)malloc(n * sizeof(double));
+  memcpy(r->ref[a].v, host, n * sizeof(double));
+  r->ref_set[a] = 1;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_field_shape(const oracle_run* r, unsigned a, uint64_t s[3]) {
+  if (a >= 9) return fail(APRL_ERR_OUT_OF_RANGE, "Field component");
+  s[0] = r->f[a].nx;
+  s[1] = r->f[a].ny;
+  s[2] = r->f[a].nz;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_field(oracle_run* r, unsigned a, const double* host, size_t count) {
+  if (a >= 9) return fail(APRL_ERR_OUT_OF_RANGE, "Field component");
+  const size_t n = r->f[a].nx * r->f[a].ny * r->f[a].nz;
+  if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Field component size mismatch");
+  memcpy(r->f[a].v, host, n * sizeof(double));
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_field(oracle_run* r, unsigned a, double* host, size_t count) {
+  if (a >= 9) return fail(APRL_ERR_OUT_OF_RANGE, "Field component");
+  const size_t n = r->f[a].nx * r->f[a].ny * r->f[a].nz;
+  if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Field component size mismatch");
+  memcpy(host, r->f[a].v, n * sizeof(double));
+  return APRL_OK;
+}
+
+static cpml_term* history_term(oracle_run* r, unsigned index) {
+  const unsigned pairs[6][2] = {{0, 1}, {0, 2}, {1, 2}, {1, 0}, {2, 0}, {2, 1}};
+  const unsigned comp = pairs[index % 6][0], der = pairs[index % 6][1];
+  return index < 6 ? &r->mterm[comp][der] : &r->eterm[comp][der];
+}
+
+aprl_status oracle_run_history_length(const oracle_run* r, unsigned index, uint64_t* length) {
+  if (index >= 12) return fail(APRL_ERR_OUT_OF_RANGE, "CPML checkpoint history index is out of range");
+  *length = history_term((oracle_run*)r, index)->length;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_history(oracle_run* r, unsigned index, const double* host, size_t count) {
+  if (index >= 12) return fail(APRL_ERR_OUT_OF_RANGE, "CPML checkpoint history index is out of range");
+  cpml_term* t = history_term(r, index);
+  if (count != t->length) return fail(APRL_ERR_INVALID_ARGUMENT, "CPML history size mismatch");
+  memcpy(t->history, host, count * sizeof(double));
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_history(oracle_run* r, unsigned index, double* host, size_t count) {
+  if (index >= 12) return fail(APRL_ERR_OUT_OF_RANGE, "CPML checkpoint history index is out of range");
+  cpml_term* t = history_term(r, index);
+  if (count != t->length) return fail(APRL_ERR_INVALID_ARGUMENT, "CPML history size mismatch");
+  memcpy(host, t->history, count * sizeof(double));
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_particles(oracle_run* r, size_t n, const double* x, const double* y,
+                                     const double* z, const double* ux, const double* uy,
+                                     const double* uz, const double* q, const double* m,
+                                     const uint64_t* id, int reset_carriers) {
+  if (n > r->pcap) {
+    r->pcap = n;
+    r->p = (particle_t*)xrealloc(r->p, n * sizeof(particle_t));
+  }
+  for (size_t i = 0; i < n; ++i) {
+    particle_t* p = &r->p[i];
+    p->pos[0] = x[i]; p->pos[1] = y[i]; p->pos[2] = z[i];
+    p->u[0] = ux[i]; p->u[1] = uy[i]; p->u[2] = uz[i];
+    p->q = q[i]; p->m = m[i]; p->id = id[i];
+  }
+  r->np = n;
+  if (reset_carriers) r->nc = 0;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_particle_count(const oracle_run* r, size_t* count) {
+  *count = r->np;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_particles(oracle_run* r, size_t capacity, double* x, double* y,
+                                     double* z, double* ux, double* uy, double* uz,
+                                     double* q, double* m, uint64_t* id, size_t* count) {
+  if (capacity < r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  for (size_t i = 0; i < r->np; ++i) {
+    const particle_t* p = &r->p[i];
+    if (x) x[i] = p->pos[0];
+    if (y) y[i] = p->pos[1];
+    if (z) z[i] = p->pos[2];
+    if (ux) ux[i] = p->u[0];
+    if (uy) uy[i] = p->u[1];
+    if (uz) uz[i] = p->u[2];
+    if (q) q[i] = p->q;
+    if (m) m[i] = p->m;
+    if (id) id[i] = p->id;
+  }
+  *count = r->np;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_carrier_count(const oracle_run* r, size_t* count) {
+  *count = r->nc;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_carriers(oracle_run* r, size_t capacity, double* pos, double* vel,
+                                    double* q, double* w, size_t* count) {
+  if (capacity < r->nc) return fail(APRL_ERR_INVALID_ARGUMENT, "Carrier buffer too small");
+  for (size_t i = 0; i < r->nc; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      if (pos) pos[3 * i + a] = r->c[i].pos[a];
+      if (vel) vel[3 * i + a] = r->c[i].vel[a];
+    }
+    if (q) q[i] = r->c[i].q;
+    if (w) w[i] = r->c[i].w;
+  }
+  *count = r->nc;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_carriers(oracle_run* r, size_t n, const double* pos,
+                                    const double* vel, const double* q, const double* w) {
+  if (n > r->ccap) {
+    r->ccap = n;
+    r->c = (carrier_t*)xrealloc(r->c, n * sizeof(carrier_t));
+  }
+  for (size_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      r->c[i].pos[a] = pos[3 * i + a];
+      r->c[i].vel[a] = vel[3 * i + a];
+    }
+    r->c[i].q = q[i];
+    r->c[i].w = w[i];
+  }
+  r->nc = n;
+  return APRL_OK;
+}
+
+/* ---- moving-window reference lookup: Simulation::movingWindowFieldValue
+ *      (src/simulation_moving_window.cpp:280-294) ------------------------ */
+static aprl_status reference_value(oracle_run* r, unsigned a, size_t i, size_t j,
+                                   long long k, uint64_t step, double* out) {
+  if (!r->ref_set[a]) return fail(APRL_ERR_INVALID_ARGUMENT, "Missing moving-window inlet reference");
+  const double z = (double)k - r->cfg.translation_beta * (double)step;
+  const size_t count = r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0);
+  if (a >= 6 || !isfinite(z) || z < 0. || z > (double)(count - 1))
+    return fail(APRL_ERR_OUT_OF_RANGE, "Moving reference query outside prepared native field");
+  const size_t lo = (size_t)floor(z), hi = lo + 1 < count - 1 ? lo + 1 : count - 1;
+  const double f = z - (double)lo;
+  const comp_t* c = &r->ref[a];
+  const double lower = c->v[(lo * c->ny + j) * c->nx + i];
+  double v = f == 0. ? lower : (1. - f) * lower + f * c->v[(hi * c->ny + j) * c->nx + i];
+  if (!isfinite(v)) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
+  *out = v;
+  return APRL_OK;
+}
+
+/* ---- Cowan-z Faraday (src/eb_field.cpp:350-558) ------------------------ */
+/* electricValue with the moving window's halo planes (both present at one
+ * rank: lower = inlet reference, upper = zero plane). */
+static double electric_value(const oracle_run* r, unsigned comp, long long i,
+                             long long j, long long k) {
+  const comp_t* c = &r->f[comp];
+  long long coord[3] = {i, j, k};
+  const long long size[3] = {(long long)c->nx, (long long)c->ny, (long long)c->nz};
+  double sign = 1.0;
+  for (unsigned axis = 0; axis < 2; ++axis) {
+    if (coord[axis] < 0) {
+      if (comp == axis)
+        coord[axis] = 0;
+      else {
+        coord[axis] = -coord[axis];
+        sign = -sign;
+      }
+    } else if (coord[axis] >= size[axis]) {
+      if (comp == axis)
+        coord[axis] = size[axis] - 1;
+      else {
+        coord[axis] = 2 * (size[axis] - 1) - coord[axis];
+        sign = -sign;
+      }
+    }
+  }
+  if (coord[2] < 0 || coord[2] >= size[2]) {
+    const double* plane = coord[2] < 0 ? r->lower[comp] : r->upper[comp];
+    return sign * plane[(size_t)coord[1] * c->nx + (size_t)coord[0]];
+  }
+  return sign * AT(c, (size_t)coord[0], (size_t)coord[1], (size_t)coord[2]);
+}
+
+/* smoothedElectric (src/eb_field.cpp:419-486); one path, same order. */
+static double smoothed_electric(const oracle_run* r, unsigned comp,
+                                unsigned derivative, long long i, long long j,
+                                long long k) {
+  const unsigned ta = (derivative + 1) % 3, tb = (derivative + 2) % 3;
+  const double delta = derivative == 0 ? r->delta_yz
+                       : (derivative == 1 ? r->delta_zx : r->delta_xy);
+  long long base[3] = {i, j, k};
+  double result = r->alpha[derivative] * electric_value(r, comp, i, j, k);
+  for (int direction = -1; direction <= 1; direction += 2) {
+    long long pa[3] = {base[0], base[1], base[2]};
+    long long pb[3] = {base[0], base[1], base[2]};
+    pa[ta] += direction;
+    pb[tb] += direction;
+    result += r->beta[ta] * electric_value(r, comp, pa[0], pa[1], pa[2]);
+    result += r->beta[tb] * electric_value(r, comp, pb[0], pb[1], pb[2]);
+  }
+  for (int da = -1; da <= 1; da += 2)
+    for (int db = -1; db <= 1; db += 2) {
+      long long p[3] = {base[0], base[1], base[2]};
+      p[ta] += da;
+      p[tb] += db;
+      result += delta * electric_value(r, comp, p[0], p[1], p[2]);
+    }
+  return result;
+}
+
+/* advanceMagneticCowan (src/eb_field.cpp:488-558). */
+static void advance_magnetic_cowan(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  const double dtdx = g->dt / g->dx, dtdy = g->dt / g->dy, dtdz = g->dt / g->dz;
+  comp_t* bx = &r->f[3];
+  comp_t* by = &r->f[4];
+  comp_t* bz = &r->f[5];
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 0; j < g->ny; ++j)
+      for (size_t i = 0; i <= g->nx; ++i) {
+        const double dEzDy = smoothed_electric(r, 2, 1, i, j + 1, k) -
+                             smoothed_electric(r, 2, 1, i, j, k);
+        const double dEyDz = smoothed_electric(r, 1, 2, i, j, k + 1) -
+                             smoothed_electric(r, 1, 2, i, j, k);
+        AT(bx, i, j, k) -= dtdy * dEzDy - dtdz * dEyDz;
+      }
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 0; j <= g->ny; ++j) {
+      double previous = smoothed_electric(r, 2, 0, 0, j, k);
+      for (size_t i = 0; i < g->nx; ++i) {
+        const double dExDz = smoothed_electric(r, 0, 2, i, j, k + 1) -
+                             smoothed_electric(r, 0, 2, i, j, k);
+        const double next = smoothed_electric(r, 2, 0, i + 1, j, k);
+        const double dEzDx = next - previous;
+        AT(by, i, j, k) -= dtdz * dExDz - dtdx * dEzDx;
+        previous = next;
+      }
+    }
+  for (size_t k = 0; k <= g->nz; ++k)
+    for (size_t j = 0; j < g->ny; ++j) {
+      double previous = smoothed_electric(r, 1, 0, 0, j, k);
+      for (size_t i = 0; i < g->nx; ++i) {
+        const double next = smoothed_electric(r, 1, 0, i + 1, j, k);
+        const double dEyDx = next - previous;
+        const double dExDy = smoothed_electric(r, 0, 1, i, j + 1, k) -
+                             smoothed_electric(r, 0, 1, i, j, k);
+        AT(bz, i, j, k) -= dtdx * dEyDx - dtdy * dExDy;
+        previous = next;
+      }
+    }
+}
+
+/* forActivePoints order (src/eb_cpml.cpp:140-193), serial. */
+typedef void (*point_op)(oracle_run*, void*, size_t, size_t, size_t);
+static void for_active_points(oracle_run* r, const cpml_profile* profile,
+                              const size_t begin[3], const size_t end[3],
+                              point_op op, void* ctx) {
+  if (profile->axis == 0) {
+    for (size_t k = begin[2]; k < end[2]; ++k)
+      for (size_t j = begin[1]; j < end[1]; ++j)
+        for (size_t o = 0; o < profile->nactive; ++o) {
+          const size_t i = profile->active[o];
+          if (i >= begin[0] && i < end[0]) op(r, ctx, i, j, k);
+        }
+  } else if (profile->axis == 1) {
+    for (size_t k = begin[2]; k < end[2]; ++k)
+      for (size_t o = 0; o < profile->nactive; ++o) {
+        const size_t j = profile->active[o];
+        if (j < begin[1] || j >= end[1]) continue;
+        for (size_t i = begin[0]; i < end[0]; ++i) op(r, ctx, i, j, k);
+      }
+  } else {
+    for (size_t o = 0; o < profile->nactive; ++o)
+      for (size_t j = begin[1]; j < end[1]; ++j) {
+        const size_t k = profile->active[o];
+        if (k < begin[2] || k >= end[2]) continue;
+        for (size_t i = begin[0]; i < end[0]; ++i) op(r, ctx, i, j, k);
+      }
+  }
+}
+
+typedef struct {
+  unsigned target, source, derivative;
+  double sign, scale;
+  cpml_term* term;
+  const cpml_profile* profile;
+} correct_ctx;
+
+static void magnetic_correct_point(oracle_run* r, void* vctx, size_t i, size_t j, size_t k) {
+  correct_ctx* c = (correct_ctx*)vctx;
+  long long plus[3] = {(long long)i, (long long)j, (long long)k};
+  ++plus[c->derivative];
+  const double difference =
+      smoothed_electric(r, c->source, c->derivative, plus[0], plus[1], plus[2]) -
+      smoothed_electric(r, c->source, c->derivative, i, j, k);
+  double* history = term_value(c->term, i, j, k);
+  const cpml_point* coefficient =
+      &c->profile->point[c->derivative == 0 ? i : (c->derivative == 1 ? j : k)];
+  *history = coefficient->decay * *history + coefficient->drive * difference;
+  const double correction = coefficient->inverse_kappa_minus_one * difference + *history;
+  AT(&r->f[3 + c->target], i, j, k) += c->sign * c->scale * correction;
+}
+
+/* EBConvolutionalPML::afterMagneticUpdate (src/eb_cpml.cpp:406-468). */
+static void cpml_after_magnetic(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  const double scale[3] = {g->dt / g->dx, g->dt / g->dy, g->dt / g->dz};
+  const int terms[6][3] = {{0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {1, 2, 0}, {2, 1, 0}, {2, 0, 1}};
+  const double signs[6] = {-1.0, 1.0, -1.0, 1.0, -1.0, 1.0};
+  for (int t = 0; t < 6; ++t) {
+    const unsigned target = terms[t][0], source = terms[t][1], der = terms[t][2];
+    const cpml_profile* profile = &r->mprof[der];
+    if (profile->nactive == 0) continue;
+    correct_ctx c = {target, source, der, signs[t], scale[der], &r->mterm[target][der], profile};
+    const comp_t* tc = &r->f[3 + target];
+    const size_t begin[3] = {0, 0, 0}, end[3] = {tc->nx, tc->ny, tc->nz};
+    for_active_points(r, profile, begin, end, magnetic_correct_point, &c);
+  }
+}
+
+static void electric_correct_point(oracle_run* r, void* vctx, size_t i, size_t j, size_t k) {
+  correct_ctx* c = (correct_ctx*)vctx;
+  const comp_t* s = &r->f[3 + c->source];
+  const double difference =
+      c->derivative == 0 ? AT(s, i, j, k) - AT(s, i - 1, j, k)
+      : (c->derivative == 1 ? AT(s, i, j, k) - AT(s, i, j - 1, k)
+                            : AT(s, i, j, k) - AT(s, i, j, k - 1));
+  double* history = term_value(c->term, i, j, k);
+  const cpml_point* coefficient =
+      &c->profile->point[c->derivative == 0 ? i : (c->derivative == 1 ? j : k)];
+  *history = coefficient->decay * *history + coefficient->drive * difference;
+  const double correction = coefficient->inverse_kappa_minus_one * difference + *history;
+  AT(&r->f[c->target], i, j, k) += c->sign * c->scale * correction;
+}
+
+/* PerfectElectricConductorBoundary::afterElectricUpdate with both z faces
+ * non-physical (src/eb_field.cpp:151-209). */
+static void pec_termination(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  comp_t* ex = &r->f[0];
+  comp_t* ey = &r->f[1];
+  comp_t* ez = &r->f[2];
+  for (size_t k = 0; k <= g->nz; ++k)
+    for (size_t i = 0; i < g->nx; ++i) {
+      AT(ex, i, 0, k) = 0.0;
+      AT(ex, i, g->ny, k) = 0.0;
+    }
+  for (size_t k = 0; k <= g->nz; ++k)
+    for (size_t j = 0; j < g->ny; ++j) {
+      AT(ey, 0, j, k) = 0.0;
+      AT(ey, g->nx, j, k) = 0.0;
+    }
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 0; j <= g->ny; ++j) {
+      AT(ez, 0, j, k) = 0.0;
+      AT(ez, g->nx, j, k) = 0.0;
+    }
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t i = 0; i <= g->nx; ++i) {
+      AT(ez, i, 0, k) = 0.0;
+      AT(ez, i, g->ny, k) = 0.0;
+    }
+}
+
+/* EBConvolutionalPML::afterElectricUpdate (src/eb_cpml.cpp:470-539) with
+ * lowerZPhysical = upperZPhysical = false (moving-window Boundary). */
+static void cpml_after_electric(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  const double curl_scale = g->dt / (SI_MU0 * SI_EPSILON0);
+  const double scale[3] = {curl_scale / g->dx, curl_scale / g->dy, curl_scale / g->dz};
+  const int terms[6][3] = {{0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {1, 2, 0}, {2, 1, 0}, {2, 0, 1}};
+  const double signs[6] = {1.0, -1.0, 1.0, -1.0, 1.0, -1.0};
+  for (int t = 0; t < 6; ++t) {
+    const unsigned target = terms[t][0], source = terms[t][1], der = terms[t][2];
+    const cpml_profile* profile = &r->eprof[der];
+    if (profile->nactive == 0) continue;
+    correct_ctx c = {target, source, der, signs[t], scale[der], &r->eterm[target][der], profile};
+    const comp_t* tc = &r->f[target];
+    size_t begin[3] = {0, 0, 0}, end[3] = {tc->nx, tc->ny, tc->nz};
+    if (target == 0) {
+      begin[1] = 1; end[1] = g->ny;
+      begin[2] = 0; end[2] = g->nz + 1;
+    } else if (target == 1) {
+      begin[0] = 1; end[0] = g->nx;
+      begin[2] = 0; end[2] = g->nz + 1;
+    } else {
+      begin[0] = 1; end[0] = g->nx;
+      begin[1] = 1; end[1] = g->ny;
+    }
+    for_active_points(r, profile, begin, end, electric_correct_point, &c);
+  }
+  pec_termination(r);
+}
+
+/* advanceElectric curl + current part (src/eb_field.cpp:582-627). */
+static void advance_electric_curl(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  const double curl_scale = g->dt / (SI_MU0 * SI_EPSILON0);
+  const double current_scale = g->dt / SI_EPSILON0;
+  const double cx = curl_scale / g->dx, cy = curl_scale / g->dy, cz = curl_scale / g->dz;
+  comp_t *ex = &r->f[0], *ey = &r->f[1], *ez = &r->f[2];
+  comp_t *bx = &r->f[3], *by = &r->f[4], *bz = &r->f[5];
+  comp_t *jx = &r->f[6], *jy = &r->f[7], *jz = &r->f[8];
+  for (size_t k = 1; k < g->nz; ++k)
+    for (size_t j = 1; j < g->ny; ++j)
+      for (size_t i = 0; i < g->nx; ++i)
+        AT(ex, i, j, k) += cy * (AT(bz, i, j, k) - AT(bz, i, j - 1, k)) -
+                           cz * (AT(by, i, j, k) - AT(by, i, j, k - 1)) -
+                           current_scale * AT(jx, i, j, k);
+  for (size_t k = 1; k < g->nz; ++k)
+    for (size_t j = 0; j < g->ny; ++j)
+      for (size_t i = 1; i < g->nx; ++i)
+        AT(ey, i, j, k) += cz * (AT(bx, i, j, k) - AT(bx, i, j, k - 1)) -
+                           cx * (AT(bz, i, j, k) - AT(bz, i - 1, j, k)) -
+                           current_scale * AT(jy, i, j, k);
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 1; j < g->ny; ++j)
+      for (size_t i = 1; i < g->nx; ++i)
+        AT(ez, i, j, k) += cx * (AT(by, i, j, k) - AT(by, i - 1, j, k)) -
+                           cy * (AT(bx, i, j, k) - AT(bx, i, j - 1, k)) -
+                           current_scale * AT(jz, i, j, k);
+}
+
+/* Boundary::afterElectricUpdate inlet overwrite (src/moving_window_fields.cpp:278-282). */
+static aprl_status inlet_overwrite(oracle_run* r) {
+  for (unsigned a = 0; a < 2; ++a) {
+    comp_t* c = &r->f[a];
+    for (size_t j = 0; j < c->ny; ++j)
+      for (size_t i = 0; i < c->nx; ++i) {
+        double v;
+        aprl_status s = reference_value(r, a, i, j, r->offset, r->step + 1, &v);
+        if (s != APRL_OK) return s;
+        AT(c, i, j, 0) = v;
+      }
+  }
+  return APRL_OK;
+}
+
+/* ---- step stages -------------------------------------------------------- */
+/* clearCurrent (src/eb_field.cpp:271-295). */
+static void clear_current(oracle_run* r) {
+  for (int a = 6; a < 9; ++a)
+    memset(r->f[a].v, 0, r->f[a].nx * r->f[a].ny * r->f[a].nz * sizeof(double));
+}
+
+aprl_status oracle_run_advance_magnetic(oracle_run* r) {
+  /* Simulation::solve (src/simulation.cpp:518-524): clearCurrent, then
+   * Boundary::begin (src/moving_window_fields.cpp:192-216) fills the lower
+   * halo planes from the reference at (offset-1, step); the upper planes are
+   * the zero vectors of the last rank. */
+  clear_current(r);
+  for (unsigned a = 0; a < 3; ++a) {
+    const comp_t* c = &r->f[a];
+    for (size_t j = 0; j < c->ny; ++j)
+      for (size_t i = 0; i < c->nx; ++i) {
+        double v;
+        aprl_status s = reference_value(r, a, i, j, r->offset - 1, r->step, &v);
+        if (s != APRL_OK) return s;
+        r->lower[a][j * c->nx + i] = v;
+      }
+  }
+  advance_magnetic_cowan(r);
+  cpml_after_magnetic(r);
+  r->stage = 1;
+  return APRL_OK;
+}
+
+static int in_preview_region(const oracle_run* r, unsigned a, size_t i, size_t j, size_t k) {
+  const comp_t* v = &r->f[a];
+  const size_t c0 = r->cfg.cpml_cells_x, c1 = r->cfg.cpml_cells_y;
+  return i <= c0 + 2 || i + c0 + 3 >= v->nx || j <= c1 + 2 || j + c1 + 3 >= v->ny ||
+         (a < 2 && k == 0);
+}
+
+aprl_status oracle_run_preview_electric(oracle_run* r) {
+  if (r->stage != 1) return fail(APRL_ERR_RUNTIME, "Moving-window electric phase mismatch");
+  /* ConservativeSourceCoupling::begin (src/source_coupling.cpp:71): snapshot
+   * E^n and reset the per-particle slots. */
+  for (int a = 0; a < 3; ++a)
+    memcpy(r->old[a].v, r->f[a].v, r->f[a].nx * r->f[a].ny * r->f[a].nz * sizeof(double));
+  if (r->np > r->nslot) r->slot = (slot_t*)xrealloc(r->slot, r->np * sizeof(slot_t));
+  r->nslot = r->np;
+  memset(r->slot, 0, r->nslot * sizeof(slot_t));
+  /* advanceElectric with J = 0 and the reversible boundary preview
+   * (src/simulation_source_coupling.cpp:20-24, src/moving_window_fields.cpp:168-186). */
+  advance_electric_curl(r);
+  r->ndelta = 0;
+  for (unsigned a = 0; a < 3; ++a) {
+    const comp_t* v = &r->f[a];
+    for (size_t k = 0; k < v->nz; ++k)
+      for (size_t j = 0; j < v->ny; ++j)
+        for (size_t i = 0; i < v->nx; ++i)
+          if (in_preview_region(r, a, i, j, k)) {
+            if (r->ndelta == r->delta_cap) {
+              r->delta_cap = r->delta_cap ? 2 * r->delta_cap : 4096;
+              r->delta = (preview_delta_t*)xrealloc(r->delta, r->delta_cap * sizeof(preview_delta_t));
+            }
+            r->delta[r->ndelta].axis = a;
+            r->delta[r->ndelta].index = cidx(v, i, j, k);
+            r->delta[r->ndelta].value = AT(v, i, j, k);
+            ++r->ndelta;
+          }
+  }
+  double* saved[6];
+  for (unsigned h = 6; h < 12; ++h) {
+    cpml_term* t = history_term(r, h);
+    saved[h - 6] = (double*)malloc((t->length ? t->length : 1) * sizeof(double));
+    memcpy(saved[h - 6], t->history, t->length * sizeof(double));
+  }
+  cpml_after_electric(r);
+  aprl_status s = inlet_overwrite(r);
+  for (size_t n = 0; n < r->ndelta; ++n)
+    r->delta[n].value = r->f[r->delta[n].axis].v[r->delta[n].index] - r->delta[n].value;
+  for (unsigned h = 6; h < 12; ++h) {
+    cpml_term* t = history_term(r, h);
+    memcpy(t->history, saved[h - 6], t->length * sizeof(double));
+    free(saved[h - 6]);
+  }
+  if (s != APRL_OK) return s;
+  r->preview_present = 1;
+  /* solveConservativeSourceStep saves the particle/carrier/counter state for
+   * the transactional trials (src/simulation_source_coupling.cpp:26-35). */
+  r->saved_p = (particle_t*)xrealloc(r->saved_p, (r->np ? r->np : 1) * sizeof(particle_t));
+  memcpy(r->saved_p, r->p, r->np * sizeof(particle_t));
+  r->saved_np = r->np;
+  r->saved_c = (carrier_t*)xrealloc(r->saved_c, (r->nc ? r->nc : 1) * sizeof(carrier_t));
+  memcpy(r->saved_c, r->c, r->nc * sizeof(carrier_t));
+  r->saved_nc = r->nc;
+  r->saved_exits = r->exits;
+  r->saved_exit_charge = r->exit_charge;
+  memcpy(r->saved_counts[0], r->cpml_entries, sizeof r->cpml_entries);
+  memcpy(r->saved_counts[1], r->direct_outer, sizeof r->direct_outer);
+  memcpy(r->saved_counts[2], r->carrier_outer, sizeof r->carrier_outer);
+  memcpy(r->saved_charges[0], r->cpml_entry_charge, sizeof r->cpml_entry_charge);
+  memcpy(r->saved_charges[1], r->direct_outer_charge, sizeof r->direct_outer_charge);
+  memcpy(r->saved_charges[2], r->carrier_outer_charge, sizeof r->carrier_outer_charge);
+  r->trials_this_step = 0;
+  r->stage = 2;
+  return APRL_OK;
+}
+
+/* ConservativeSourceCoupling::applyCurrentSource (src/source_coupling.cpp:84-89). */
+static void apply_current_source(oracle_run* r, double sign) {
+  const aprl_run_config* g = &r->cfg;
+  for (unsigned a = 0; a < 3; ++a) {
+    comp_t* e = &r->f[a];
+    const comp_t* jc = &r->f[6 + a];
+    for (size_t k = 0; k < e->nz; ++k)
+      for (size_t y = 0; y < e->ny; ++y)
+        for (size_t x = 0; x < e->nx; ++x) {
+          const int applied =
+              a == 0 ? (y > 0 && y < g->ny && k != 0 && k != g->nz)
+              : (a == 1 ? (x > 0 && x < g->nx && k != 0 && k != g->nz)
+                        : (x > 0 && x < g->nx && y > 0 && y < g->ny));
+          if (applied) {
+            const size_t n = (k * e->ny + y) * e->nx + x;
+            if (jc->v[n] != 0.) e->v[n] += sign * g->dt / SI_EPSILON0 * jc->v[n];
+          }
+        }
+  }
+}
+
+static void restore_state(oracle_run* r) {
+  if (r->saved_np > r->pcap) {
+    r->pcap = r->saved_np;
+    r->p = (particle_t*)xrealloc(r->p, r->pcap * sizeof(particle_t));
+  }
+  memcpy(r->p, r->saved_p, r->saved_np * sizeof(particle_t));
+  r->np = r->saved_np;
+  if (r->saved_nc > r->ccap) {
+    r->ccap = r->saved_nc;
+    r->c = (carrier_t*)xrealloc(r->c, r->ccap * sizeof(carrier_t));
+  }
+  memcpy(r->c, r->saved_c, r->saved_nc * sizeof(carrier_t));
+  r->nc = r->saved_nc;
+  r->exits = r->saved_exits;
+  r->exit_charge = r->saved_exit_charge;
+  memcpy(r->cpml_entries, r->saved_counts[0], sizeof r->cpml_entries);
+  memcpy(r->direct_outer, r->saved_counts[1], sizeof r->direct_outer);
+  memcpy(r->carrier_outer, r->saved_counts[2], sizeof r->carrier_outer);
+  memcpy(r->cpml_entry_charge, r->saved_charges[0], sizeof r->cpml_entry_charge);
+  memcpy(r->direct_outer_charge, r->saved_charges[1], sizeof r->direct_outer_charge);
+  memcpy(r->carrier_outer_charge, r->saved_charges[2], sizeof r->carrier_outer_charge);
+}
+
+/* ---- gathers (src/source_coupling.cpp:31-51, source_coupling_math.h) ---- */
+typedef struct {
+  double first, last;
+  double begin[3], end[3];
+  int valid;
+} open_orbit;
+
+/* clipOpenOrbit at one rank (src/source_coupling_math.h:234-250). */
+static aprl_status clip_open_orbit(const oracle_run* r, const double begin[3],
+                                   const double end[3], open_orbit* o) {
+  const aprl_run_config* g = &r->cfg;
+  const double ds[3] = {g->dx, g->dy, g->dz};
+  const size_t size[3] = {g->nx, g->ny, g->nz};
+  o->first = 0.;
+  o->last = 1.;
+  o->valid = 1;
+  for (int a = 0; a < 3; ++a) {
+    o->begin[a] = begin[a];
+    o->end[a] = end[a];
+  }
+  for (int a = 0; a < 3; ++a) {
+    const double x = (begin[a] - r->origin[a]) / ds[a], d = (end[a] - begin[a]) / ds[a];
+    if (!isfinite(x) || !isfinite(d)) return fail(APRL_ERR_RUNTIME, "Nonfinite open coupling orbit");
+    if (d == 0.) {
+      if (x < 0. || x > (double)size[a]) o->valid = 0;
+      continue;
+    }
+    {
+      const double t = -x / d;
+      if (d > 0.) o->first = fmax(o->first, t);
+      else o->last = fmin(o->last, t);
+    }
+    {
+      const double t = ((double)size[a] - x) / d;
+      if (d > 0.) o->last = fmin(o->last, t);
+      else o->first = fmax(o->first, t);
+    }
+  }
+  o->valid = o->valid && o->last >= o->first;
+  if (o->valid)
+    for (int a = 0; a < 3; ++a) {
+      const double d = end[a] - begin[a];
+      if (o->first != 0.) o->begin[a] = begin[a] + o->first * d;
+      if (o->last != 1.) o->end[a] = begin[a] + o->last * d;
+    }
+  return APRL_OK;
+}
+
+typedef struct {
+  visitor_t base;
+  const oracle_run* r;
+  double result[3];
+} electric_visitor;
+
+static void electric_visit(visitor_t* v, unsigned d, long long i, long long j,
+                           long long k, double w) {
+  electric_visitor* ev = (electric_visitor*)v;
+  const comp_t* c = &ev->r->f[d];
+  if (i < 0 || j < 0 || i >= (long long)c->nx || j >= (long long)c->ny) return;
+  if (k < 0 || k >= (long long)c->nz) return; /* no native halo at one rank */
+  const size_t n = cidx(c, (size_t)i, (size_t)j, (size_t)k);
+  ev->result[d] += .5 * w * (c->v[n] + ev->r->old[d].v[n]);
+}
+
+/* Impl::electric(a,b,open=true) for wide shapes (src/source_coupling.cpp:31-39). */
+static aprl_status gather_electric(const oracle_run* r, const double a[3],
+                                   const double b[3], double out[3]) {
+  open_orbit path;
+  aprl_status s = clip_open_orbit(r, a, b, &path);
+  if (s != APRL_OK) return s;
+  if (!path.valid) return fail(APRL_ERR_OUT_OF_RANGE, "Quintic active orbit outside domain");
+  electric_visitor ev;
+  ev.base.visit = electric_visit;
+  ev.r = r;
+  ev.result[0] = ev.result[1] = ev.result[2] = 0.0;
+  if (shape_weights(&r->cfg, r->origin, path.begin, path.end, &ev.base) < 0)
+    return fail(APRL_ERR_RUNTIME, "Quintic orbit exceeds crossing budget");
+  const double fraction = path.last - path.first;
+  for (int d = 0; d < 3; ++d) out[d] = ev.result[d] * fraction;
+  return APRL_OK;
+}
+
+/* NativeHalo::openMagneticValue at one rank (src/source_coupling_math.h:113-119). */
+static double open_magnetic_value(const comp_t* v, long long i, long long j, long long k) {
+  if (i < 0) i = 0;
+  if (i > (long long)v->nx - 1) i = (long long)v->nx - 1;
+  if (j < 0) j = 0;
+  if (j > (long long)v->ny - 1) j = (long long)v->ny - 1;
+  if (k < 0) k = 0;
+  if (k >= (long long)v->nz) k = (long long)v->nz - 1;
+  return v->v[cidx(v, (size_t)i, (size_t)j, (size_t)k)];
+}
+
+/* binomialXZMagneticSample (src/source_coupling_math.h:142-167). */
+static void binomial_xz_magnetic(const oracle_run* r, const double point[3], double value[3]) {
+  const aprl_run_config* g = &r->cfg;
+  const double h[3] = {g->dx, g->dy, g->dz};
+  for (unsigned a = 0; a < 3; ++a) {
+    long long cell[3];
+    double fraction[3];
+    for (unsigned d = 0; d < 3; ++d) {
+      const double pos = (point[d] - r->origin[d]) / h[d] - (a == d ? 0. : 0.5);
+      cell[d] = (long long)floor(pos);
+      fraction[d] = pos - cell[d];
+    }
+    double wx[4], wz[4];
+    node_weights(fraction[0], wx);
+    node_weights(fraction[2], wz);
+    const double wy[2] = {1. - fraction[1], fraction[1]};
+    value[a] = 0.;
+    const comp_t* f = &r->f[3 + a];
+    for (unsigned k = 0; k < 4; ++k)
+      for (unsigned j = 0; j < 2; ++j) {
+        double row = 0.;
+        for (unsigned i = 0; i < 4; ++i)
+          row += wx[i] * open_magnetic_value(f, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
+        value[a] += wz[k] * wy[j] * row;
+      }
+  }
+}
+
+/* magneticSample(bounds=false, halo, openFaces=true) (src/source_coupling_math.h:122-138). */
+static void trilinear_magnetic(const oracle_run* r, const double position[3], double value[3]) {
+  const aprl_run_config* g = &r->cfg;
+  const double ds[3] = {g->dx, g->dy, g->dz};
+  int cell[2][3];
+  double fraction[2][3];
+  for (unsigned half = 0; half < 2; ++half)
+    for (unsigned d = 0; d < 3; ++d) {
+      const double x = (position[d] - r->origin[d]) / ds[d] - .5 * half;
+      cell[half][d] = (int)floor(x);
+      fraction[half][d] = x - cell[half][d];
+    }
+  for (unsigned axis = 0; axis < 3; ++axis) {
+    const unsigned hx = axis == 0 ? 0 : 1, hy = axis == 1 ? 0 : 1, hz = axis == 2 ? 0 : 1;
+    value[axis] = 0.;
+    const comp_t* f = &r->f[3 + axis];
+    for (unsigned k = 0; k < 2; ++k)
+      for (unsigned j = 0; j < 2; ++j)
+        for (unsigned i = 0; i < 2; ++i) {
+          const double x = i ? fraction[hx][0] : 1 - fraction[hx][0],
+                       y = j ? fraction[hy][1] : 1 - fraction[hy][1],
+                       z = k ? fraction[hz][2] : 1 - fraction[hz][2];
+          const double b = open_magnetic_value(f, cell[hx][0] + (int)i, cell[hy][1] + (int)j,
+                                               cell[hz][2] + (int)k);
+          value[axis] += x * y * z * b;
+        }
+  }
+}
+
+/* Impl::magnetic (src/source_coupling.cpp:40-51): F3 x-z tensor at the
+ * clipped-chord midpoint for binomial3, trilinear for quintic. */
+static aprl_status gather_magnetic(const oracle_run* r, const double a[3],
+                                   const double b[3], double out[3]) {
+  open_orbit path;
+  aprl_status s = clip_open_orbit(r, a, b, &path);
+  if (s != APRL_OK) return s;
+  if (!path.valid)
+    return fail(APRL_ERR_OUT_OF_RANGE,
+                r->cfg.shape == APRL_SHAPE_LINEAR_BINOMIAL3
+                    ? "Notch magnetic orbit outside domain"
+                    : "Active coupling magnetic orbit has no in-domain portion");
+  double middle[3];
+  for (int d = 0; d < 3; ++d) middle[d] = (path.begin[d] + path.end[d]) * .5;
+  if (r->cfg.shape == APRL_SHAPE_LINEAR_BINOMIAL3)
+    binomial_xz_magnetic(r, middle, out);
+  else
+    trilinear_magnetic(r, middle, out);
+  return APRL_OK;
+}
+
+/* ---- deposition: longitudinal_shape::Current::deposit at one rank
+ *      (src/longitudinal_shape.h:175-187) -------------------------------- */
+typedef struct {
+  visitor_t base;
+  oracle_run* r;
+  double scale[3];
+  int error;
+} deposit_visitor;
+
+static void deposit_visit(visitor_t* v, unsigned a, long long i, long long j,
+                          long long k, double w) {
+  deposit_visitor* dv = (deposit_visitor*)v;
+  if (dv->scale[a] == 0.) return;
+  comp_t* c = &dv->r->f[6 + a];
+  if (i < 0 || i >= (long long)c->nx) {
+    if (dv->r->cfg.shape == APRL_SHAPE_LINEAR_BINOMIAL3) return;
+    dv->error = 1;
+    return;
+  }
+  if (j < 0 || j >= (long long)c->ny) {
+    dv->error = 2;
+    return;
+  }
+  const double value = dv->scale[a] * w;
+  if (k >= 0 && k < (long long)c->nz) AT(c, (size_t)i, (size_t)j, (size_t)k) += value;
+}
+
+/* ChargeConservingCurrentDepositor::depositSegment -> Current::deposit. */
+static aprl_status deposit_segment(oracle_run* r, const double begin[3],
+                                   const double end[3], double charge) {
+  const aprl_run_config* g = &r->cfg;
+  /* validatePosition (src/eb_deposition.cpp:228-250). */
+  const double extent[3] = {(double)g->nx * g->dx, (double)g->ny * g->dy, (double)g->nz * g->dz};
+  const double* pts[2] = {begin, end};
+  for (int n = 0; n < 2; ++n)
+    for (int a = 0; a < 3; ++a) {
+      const double rel = pts[n][a] - r->origin[a];
+      const double tol = 64.0 * DBL_EPSILON * fmax(1.0, fmax(fabs(r->origin[a]), extent[a]));
+      if (!isfinite(pts[n][a]) || rel < -tol || rel > extent[a] + tol)
+        return fail(APRL_ERR_OUT_OF_RANGE, "Particle trajectory endpoint is outside the E/B domain");
+    }
+  if (!isfinite(charge)) return fail(APRL_ERR_INVALID_ARGUMENT, "Deposited particle charge must be finite");
+  deposit_visitor dv;
+  dv.base.visit = deposit_visit;
+  dv.r = r;
+  dv.error = 0;
+  for (int a = 0; a < 3; ++a)
+    dv.scale[a] = charge * (end[a] - begin[a]) / (g->dx * g->dy * g->dz * g->dt);
+  if (shape_weights(g, r->origin, begin, end, &dv.base) < 0)
+    return fail(APRL_ERR_RUNTIME, "Quintic orbit exceeds crossing budget");
+  if (dv.error == 1) return fail(APRL_ERR_OUT_OF_RANGE, "Transverse current support outside x grid");
+  if (dv.error == 2) return fail(APRL_ERR_OUT_OF_RANGE, "Transverse current support outside y grid");
+  return APRL_OK;
+}
+
+/* ---- particle boundaries (src/particle_boundary.cpp) -------------------- */
+typedef struct {
+  double position[3];
+  double fraction;
+  int face;
+} boundary_hit;
+
+static double coordinate_tolerance(double lower, double upper) {
+  return 64.0 * DBL_EPSILON * fmax(1.0, fmax(fabs(lower), fabs(upper)));
+}
+
+typedef struct {
+  double outer_lower[3], outer_upper[3], physical_lower[3], physical_upper[3], tolerance[3];
+} cpml_region;
+
+/* ParticleCPMLRegion constructor (src/particle_boundary.cpp:56-85) on the
+ * global window geometry and origin. */
+static void make_cpml_region(const oracle_run* r, cpml_region* c) {
+  const aprl_run_config* g = &r->cfg;
+  const double spacing[3] = {g->dx, g->dy, g->dz};
+  const size_t cells[3] = {g->nx, g->ny, g->nz};
+  const size_t pc[3] = {g->cpml_cells_x, g->cpml_cells_y, 0};
+  for (int a = 0; a < 3; ++a) {
+    c->outer_lower[a] = r->origin[a];
+    c->outer_upper[a] = r->origin[a] + (double)cells[a] * spacing[a];
+    c->physical_lower[a] = c->outer_lower[a] + (double)pc[a] * spacing[a];
+    c->physical_upper[a] = c->outer_upper[a] - (double)pc[a] * spacing[a];
+    c->tolerance[a] = coordinate_tolerance(c->outer_lower[a], c->outer_upper[a]);
+  }
+}
+
+/* ParticleCPMLRegion::firstEntry (src/particle_boundary.cpp:104-174). */
+static aprl_status cpml_first_entry(const oracle_run* r, const cpml_region* c,
+                                    const double start[3], const double end[3],
+                                    boundary_hit* hit, int* entered_out) {
+  const size_t pc[3] = {r->cfg.cpml_cells_x, r->cfg.cpml_cells_y, 0};
+  double best = INFINITY;
+  int best_face = 0, entered = 0;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!isfinite(start[axis]) || !isfinite(end[axis]))
+      return fail(APRL_ERR_RUNTIME, "Particle CPML trajectory contains a non-finite coordinate");
+    if (start[axis] < c->physical_lower[axis] - c->tolerance[axis] ||
+        start[axis] > c->physical_upper[axis] + c->tolerance[axis])
+      return fail(APRL_ERR_OUT_OF_RANGE, "Active particle starts inside the non-physical CPML region");
+    if (pc[axis] == 0) continue;
+    double candidate = 0.0;
+    int face = 0, hit_axis = 0;
+    if (end[axis] < c->physical_lower[axis]) {
+      candidate = (c->physical_lower[axis] - start[axis]) / (end[axis] - start[axis]);
+      face = 2 * axis;
+      hit_axis = 1;
+    } else if (end[axis] > c->physical_upper[axis]) {
+      candidate = (c->physical_upper[axis] - start[axis]) / (end[axis] - start[axis]);
+      face = 2 * axis + 1;
+      hit_axis = 1;
+    }
+    if (hit_axis && candidate < best) {
+      best = candidate;
+      best_face = face;
+      entered = 1;
+    }
+  }
+  *entered_out = entered;
+  if (!entered) return APRL_OK;
+  const double ft = 64.0 * DBL_EPSILON;
+  if (!isfinite(best) || best < -ft || best > 1.0 + ft)
+    return fail(APRL_ERR_RUNTIME, "Cannot locate the first particle entry into CPML");
+  hit->fraction = fmax(0.0, fmin(1.0, best));
+  hit->face = best_face;
+  for (int a = 0; a < 3; ++a) {
+    hit->position[a] = start[a] + hit->fraction * (end[a] - start[a]);
+    hit->position[a] = fmax(c->outer_lower[a], fmin(c->outer_upper[a], hit->position[a]));
+  }
+  const int normal = best_face / 2;
+  hit->position[normal] = (best_face % 2) != 0 ? c->physical_upper[normal] : c->physical_lower[normal];
+  return APRL_OK;
+}
+
+/* ParticleCPMLRegion::conductivityRate / currentDampingFactor
+ * (src/particle_boundary.cpp:176-240). */
+static double conductivity_rate(const oracle_run* r, const cpml_region* c, const double pos[3]) {
+  const aprl_run_config* g = &r->cfg;
+  const double spacing[3] = {g->dx, g->dy, g->dz};
+  const size_t pc[3] = {g->cpml_cells_x, g->cpml_cells_y, 0};
+  double rate = 0.0;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (pc[axis] == 0) continue;
+    const double thickness = (double)pc[axis] * spacing[axis];
+    double depth = 0.0;
+    if (pos[axis] < c->physical_lower[axis])
+      depth = (c->physical_lower[axis] - pos[axis]) / thickness;
+    else if (pos[axis] > c->physical_upper[axis])
+      depth = (pos[axis] - c->physical_upper[axis]) / thickness;
+    depth = fmax(0.0, fmin(1.0, depth));
+    rate += r->max_rate[axis] * pow(depth, g->cpml_polynomial_order);
+  }
+  return rate;
+}
+
+static double current_damping_factor(const oracle_run* r, const cpml_region* c,
+                                     const double start[3], const double end[3],
+                                     double duration) {
+  if (duration == 0.0) return 1.0;
+  const double abscissa = sqrt(3.0 / 5.0);
+  const double node[3] = {0.5 * (1.0 - abscissa), 0.5, 0.5 * (1.0 + abscissa)};
+  const double weight[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
+  double average = 0.0;
+  for (int s = 0; s < 3; ++s) {
+    double pos[3];
+    for (int a = 0; a < 3; ++a) pos[a] = start[a] + node[s] * (end[a] - start[a]);
+    average += weight[s] * conductivity_rate(r, c, pos);
+  }
+  const double exponent = -duration * average;
+  return exponent < log(DBL_MIN) ? 0.0 : exp(exponent);
+}
+
+/* ParticleOpenBoundary::firstExit (src/particle_boundary.cpp:303-373) on
+ * the global window. */
+static aprl_status outer_first_exit(const oracle_run* r, const double start[3],
+                                    const double end[3], boundary_hit* hit, int* out) {
+  const aprl_run_config* g = &r->cfg;
+  const double spacing[3] = {g->dx, g->dy, g->dz};
+  const size_t cells[3] = {g->nx, g->ny, g->nz};
+  double lo[3], hi[3], tol[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = r->origin[a];
+    hi[a] = fma((double)cells[a], spacing[a], r->origin[a]);
+    tol[a] = coordinate_tolerance(lo[a], hi[a]);
+  }
+  double best = INFINITY;
+  int best_face = 0, escaped = 0;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!isfinite(start[axis]) || !isfinite(end[axis]))
+      return fail(APRL_ERR_RUNTIME, "Particle trajectory contains a non-finite coordinate");
+    if (start[axis] < lo[axis] - tol[axis] || start[axis] > hi[axis] + tol[axis])
+      return fail(APRL_ERR_OUT_OF_RANGE, "Particle trajectory starts outside the global E/B domain");
+    double candidate = 0.0;
+    int face = 0, e = 0;
+    if (end[axis] < lo[axis]) {
+      candidate = (lo[axis] - start[axis]) / (end[axis] - start[axis]);
+      face = 2 * axis;
+      e = 1;
+    } else if (end[axis] > hi[axis]) {
+      candidate = (hi[axis] - start[axis]) / (end[axis] - start[axis]);
+      face = 2 * axis + 1;
+      e = 1;
+    }
+    if (e && candidate < best) {
+      best = candidate;
+      best_face = face;
+      escaped = 1;
+    }
+  }
+  *out = escaped;
+  if (!escaped) return APRL_OK;
+  const double ft = 64.0 * DBL_EPSILON;
+  if (best < -ft || best > 1.0 + ft || !isfinite(best))
+    return fail(APRL_ERR_RUNTIME, "Cannot locate the first particle-domain exit");
+  hit->fraction = fmax(0.0, fmin(1.0, best));
+  hit->face = best_face;
+  for (int a = 0; a < 3; ++a) {
+    hit->position[a] = start[a] + hit->fraction * (end[a] - start[a]);
+    hit->position[a] = fmax(lo[a], fmin(hi[a], hit->position[a]));
+  }
+  const int normal = best_face / 2;
+  hit->position[normal] = (best_face % 2) ? hi[normal] : lo[normal];
+  return APRL_OK;
+}
+
+/* Simulation::firstMovingWindowEntry (src/simulation_moving_window.cpp:380-395). */
+static aprl_status moving_window_entry(const oracle_run* r, const cpml_region* c,
+                                       const double start[3], const double end[3],
+                                       double start_fraction, boundary_hit* hit, int* present) {
+  aprl_status s = cpml_first_entry(r, c, start, end, hit, present);
+  if (s != APRL_OK) return s;
+  const double a = lab_z_from_box_zt(&r->cfg, start[2], r->time + start_fraction * r->cfg.dt) -
+                   r->cfg.exit_lab_z;
+  const double b = lab_z_from_box_zt(&r->cfg, end[2], r->time + r->cfg.dt) - r->cfg.exit_lab_z;
+  if (a >= 0.) return fail(APRL_ERR_RUNTIME, "Active particle started beyond trusted moving-window exit");
+  if (b >= 0. && b > a) {
+    const double fraction = -a / (b - a);
+    if (!*present || fraction < hit->fraction) {
+      for (int d = 0; d < 3; ++d) hit->position[d] = start[d] + fraction * (end[d] - start[d]);
+      hit->fraction = fraction;
+      hit->face = 5;
+      *present = 1;
+    }
+  }
+  return APRL_OK;
+}
+
+/* ---- the particle part of one trial ------------------------------------ */
+static void push_retained(oracle_run* r, const particle_t* p) {
+  if (r->nretained == r->rcap) {
+    r->rcap = r->rcap ? 2 * r->rcap : 1024;
+    r->retained = (particle_t*)xrealloc(r->retained, r->rcap * sizeof(particle_t));
+  }
+  r->retained[r->nretained++] = *p;
+}
+
+static void push_rcarrier(oracle_run* r, const carrier_t* c) {
+  if (r->nrcarrier == r->rccap) {
+    r->rccap = r->rccap ? 2 * r->rccap : 256;
+    r->rcarrier = (carrier_t*)xrealloc(r->rcarrier, r->rccap * sizeof(carrier_t));
+  }
+  r->rcarrier[r->nrcarrier++] = *c;
+}
+
+/* processCarrierSegment at one rank (src/simulation.cpp:4310-4407). */
+static aprl_status process_carrier_segment(oracle_run* r, const cpml_region* reg,
+                                           carrier_t carrier, const double seg_start[3],
+                                           double seg_start_fraction) {
+  const double cutoff = 64.0 * DBL_EPSILON;
+  if (!(seg_start_fraction >= 0.0 && seg_start_fraction <= 1.0) || !isfinite(seg_start_fraction))
+    return fail(APRL_ERR_RUNTIME, "Invalid CPML-carrier segment time fraction");
+  if (!(carrier.w >= 0.0) || !isfinite(carrier.w))
+    return fail(APRL_ERR_RUNTIME, "Invalid CPML carrier current weight");
+  if (carrier.w <= cutoff) return APRL_OK;
+  boundary_hit outer;
+  int exits = 0;
+  aprl_status s = outer_first_exit(r, seg_start, carrier.pos, &outer, &exits);
+  if (s != APRL_OK) return s;
+  double local_end = 1.0;
+  double seg_end[3] = {carrier.pos[0], carrier.pos[1], carrier.pos[2]};
+  int remove = 0;
+  if (exits) {
+    local_end = outer.fraction;
+    for (int a = 0; a < 3; ++a) seg_end[a] = outer.position[a];
+    remove = 1;
+  }
+  const double global_end = seg_start_fraction + local_end * (1.0 - seg_start_fraction);
+  const double duration = (global_end - seg_start_fraction) * r->cfg.dt;
+  double midpoint[3];
+  for (int a = 0; a < 3; ++a) midpoint[a] = 0.5 * (seg_start[a] + seg_end[a]);
+  const double mid_damping = current_damping_factor(r, reg, seg_start, midpoint, 0.5 * duration);
+  const double end_damping = current_damping_factor(r, reg, seg_start, seg_end, duration);
+  const double deposited = carrier.w * mid_damping;
+  const double end_weight = carrier.w * end_damping;
+  s = deposit_segment(r, seg_start, seg_end, carrier.q * deposited);
+  if (s != APRL_OK) return s;
+  if (remove) {
+    ++r->carrier_outer[outer.face];
+    r->carrier_outer_charge[outer.face] += carrier.q * end_weight;
+    return APRL_OK;
+  }
+  if (end_weight <= cutoff) return APRL_OK;
+  carrier.w = end_weight;
+  for (int a = 0; a < 3; ++a) carrier.pos[a] = seg_end[a];
+  push_rcarrier(r, &carrier);
+  return APRL_OK;
+}
+
+/* ConservativeSourceCoupling::push (src/source_coupling.cpp:90-104). */
+static aprl_status coupling_push(oracle_run* r, particle_t* p, slot_t* q) {
+  const aprl_run_config* g = &r->cfg;
+  const double dt = g->dt, time = r->time;
+  const unsigned steps = g->substeps;
+  if (r->replay) {
+    if (!q->seen || q->time != time || q->dt != dt)
+      return fail(APRL_ERR_RUNTIME, "Missing converged particle replay");
+    for (int a = 0; a < 3; ++a)
+      if (q->first.pos[a] != p->pos[a] || q->first.u[a] != p->u[a])
+        return fail(APRL_ERR_RUNTIME, "Release state changed during coupled replay");
+    q->replayed = 1;
+    *p = q->last;
+    return APRL_OK;
+  }
+  if (!q->initialized) {
+    for (int a = 0; a < 3; ++a) q->guess[a] = p->pos[a];
+    const double gamma = gamma_u(p->u);
+    const double s = dt * SI_C / gamma;
+    for (int a = 0; a < 3; ++a) q->guess[a] += s * p->u[a];
+    q->initialized = 1;
+  }
+  q->first = *p;
+  q->time = time;
+  q->dt = dt;
+  q->seen = 1;
+  if (q->next_ready) {
+    for (int a = 0; a < 3; ++a) {
+      q->used_e[a] = q->next_e[a];
+      q->used_b[a] = q->next_b[a];
+    }
+  } else {
+    aprl_status s = gather_electric(r, p->pos, q->guess, q->used_e);
+    if (s != APRL_OK) return s;
+    s = gather_magnetic(r, p->pos, q->guess, q->used_b);
+    if (s != APRL_OK) return s;
+  }
+  q->abs_grid_work = 0;
+  const double h = dt / steps;
+  for (unsigned n = 0; n < steps; ++n) {
+    const particle_t before = *p;
+    const double g0 = gamma_u(p->u);
+    double point[3];
+    const double ps = .5 * h * SI_C / g0;
+    for (int a = 0; a < 3; ++a) point[a] = p->pos[a] + ps * p->u[a];
+    double ee[3] = {0., 0., 0.}, bb[3] = {0., 0., 0.};
+    add_prescribed_box(g, point, time + (n + .5) * h, ee, bb);
+    double e[3], b[3];
+    for (int a = 0; a < 3; ++a) {
+      e[a] = q->used_e[a] + ee[a];
+      b[a] = q->used_b[a] + bb[a];
+    }
+    const int it = oracle_momentum(p->u, e, b, p->q, p->m, h, g0);
+    if (it == -1) return fail(APRL_ERR_RUNTIME, "Nonphysical local mean-gamma root");
+    if (it == -2) return fail(APRL_ERR_RUNTIME, "Local mean-gamma root did not converge");
+    const double g1 = gamma_u(p->u);
+    double mean[3];
+    for (int a = 0; a < 3; ++a) mean[a] = before.u[a] + p->u[a];
+    const double xs = h * SI_C / (g0 + g1);
+    for (int a = 0; a < 3; ++a) p->pos[a] += xs * mean[a];
+    const long double grid_work = charge_work(p->q, q->used_e, before.pos, p->pos);
+    q->abs_grid_work += fabsl(grid_work);
+  }
+  q->last = *p;
+  for (int a = 0; a < 3; ++a) q->guess[a] = p->pos[a];
+  return APRL_OK;
+}
+
+/* pushDepositAndMigrate at one rank for active particles and CPML carriers
+ * (src/simulation.cpp:4167-5368, processActiveSegment 4555-4917). */
+static aprl_status push_deposit(oracle_run* r) {
+  const double crossing_tolerance = 64.0 * DBL_EPSILON;
+  cpml_region reg;
+  make_cpml_region(r, &reg);
+  r->nretained = 0;
+  r->nrcarrier = 0;
+  for (size_t n = 0; n < r->nc; ++n) {
+    carrier_t c = r->c[n];
+    const double start[3] = {c.pos[0], c.pos[1], c.pos[2]};
+    for (int a = 0; a < 3; ++a) c.pos[a] += r->cfg.dt * c.vel[a];
+    aprl_status s = process_carrier_segment(r, &reg, c, start, 0.0);
+    if (s != APRL_OK) return s;
+  }
+  for (size_t n = 0; n < r->np; ++n) {
+    particle_t p = r->p[n];
+    const double start[3] = {p.pos[0], p.pos[1], p.pos[2]};
+    if (start[2] < r->origin[2])
+      return fail(APRL_ERR_RUNTIME,
+                  "An active particle is upstream of the moving window; the inlet guard did not contain its release event");
+    aprl_status s = coupling_push(r, &p, &r->slot[n]);
+    if (s != APRL_OK) return s;
+    boundary_hit cpml_hit, outer_hit;
+    int enters = 0, exits = 0;
+    s = moving_window_entry(r, &reg, start, p.pos, 0.0, &cpml_hit, &enters);
+    if (s != APRL_OK) return s;
+    s = outer_first_exit(r, start, p.pos, &outer_hit, &exits);
+    if (s != APRL_OK) return s;
+    int action = 0; /* 0 retain, 1 enter CPML, 2 exit outer */
+    double local_end = 1.0, seg_end[3] = {p.pos[0], p.pos[1], p.pos[2]};
+    boundary_hit selected;
+    if (enters && (!exits || cpml_hit.fraction <= outer_hit.fraction + crossing_tolerance)) {
+      action = 1;
+      local_end = cpml_hit.fraction;
+      selected = cpml_hit;
+    } else if (exits) {
+      action = 2;
+      local_end = outer_hit.fraction;
+      selected = outer_hit;
+    }
+    if (action) for (int a = 0; a < 3; ++a) seg_end[a] = selected.position[a];
+    s = deposit_segment(r, start, seg_end, p.q);
+    if (s != APRL_OK) return s;
+    const double global_end = 0.0 + local_end * (1.0 - 0.0);
+    if (action == 1) {
+      if (selected.face == 5) {
+        ++r->exits;
+        r->exit_charge += p.q;
+      } else {
+        ++r->cpml_entries[selected.face];
+        r->cpml_entry_charge[selected.face] += p.q;
+      }
+      carrier_t c;
+      for (int a = 0; a < 3; ++a) c.pos[a] = p.pos[a];
+      const double gamma = gamma_u(p.u);
+      for (int a = 0; a < 3; ++a) c.vel[a] = p.u[a] * (SI_C / gamma);
+      c.q = p.q;
+      c.w = 1.0;
+      s = process_carrier_segment(r, &reg, c, selected.position, global_end);
+      if (s != APRL_OK) return s;
+    } else if (action == 2) {
+      ++r->direct_outer[selected.face];
+      r->direct_outer_charge[selected.face] += p.q;
+    } else {
+      push_retained(r, &p);
+    }
+  }
+  /* particles_ <- retained, pmlCarriers_ <- retainedCarriers. */
+  if (r->nretained > r->pcap) {
+    r->pcap = r->nretained;
+    r->p = (particle_t*)xrealloc(r->p, r->pcap * sizeof(particle_t));
+  }
+  memcpy(r->p, r->retained, r->nretained * sizeof(particle_t));
+  r->np = r->nretained;
+  if (r->nrcarrier > r->ccap) {
+    r->ccap = r->nrcarrier;
+    r->c = (carrier_t*)xrealloc(r->c, r->ccap * sizeof(carrier_t));
+  }
+  memcpy(r->c, r->rcarrier, r->nrcarrier * sizeof(carrier_t));
+  r->nc = r->nrcarrier;
+  return APRL_OK;
+}
+
+/* ConservativeSourceCoupling::localResidual (src/source_coupling.cpp:105-159). */
+static aprl_status local_residual(oracle_run* r, double out[4]) {
+  double force = 0., defect = 0., scale = 0., calls = 0.;
+  for (size_t n = 0; n < r->nslot; ++n) {
+    slot_t* q = &r->slot[n];
+    if (!q->seen) continue;
+    calls += 1;
+    aprl_status s = gather_electric(r, q->first.pos, q->last.pos, q->next_e);
+    if (s != APRL_OK) return s;
+    s = gather_magnetic(r, q->first.pos, q->last.pos, q->next_b);
+    if (s != APRL_OK) return s;
+    q->next_ready = 1;
+    double de[3], db[3];
+    for (int a = 0; a < 3; ++a) {
+      de[a] = q->next_e[a] - q->used_e[a];
+      db[a] = q->next_b[a] - q->used_b[a];
+    }
+    force = fmax(force, fabs(q->first.q / q->first.m) * q->dt / SI_C *
+                            (sqrt(dot3(de, de)) + SI_C * sqrt(dot3(db, db))));
+    defect += fabsl(charge_work(q->first.q, de, q->first.pos, q->last.pos));
+    scale += q->abs_grid_work;
+    scale += fabsl(charge_work(q->first.q, q->next_e, q->first.pos, q->last.pos));
+  }
+  out[0] = force;
+  out[1] = defect;
+  out[2] = scale;
+  out[3] = calls;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_coupling_trial(oracle_run* r, double residual[4]) {
+  if (r->stage != 2 && r->stage != 3)
+    return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
+  /* Loop body of solveConservativeSourceStep (src/simulation_source_coupling.cpp:43-48). */
+  if (r->trials_this_step) apply_current_source(r, 1.);
+  clear_current(r);
+  restore_state(r);
+  for (size_t n = 0; n < r->nslot; ++n) r->slot[n].seen = 0; /* beginTrial */
+  r->replay = 0;
+  aprl_status s = push_deposit(r);
+  if (s != APRL_OK) return s;
+  apply_current_source(r, -1.);
+  s = local_residual(r, residual);
+  if (s != APRL_OK) return s;
+  ++r->trials_this_step;
+  r->stage = 3;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_commit_electric(oracle_run* r) {
+  if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
+  /* Remove the trial current, replay against E^n, then commit
+   * (src/simulation_source_coupling.cpp:58-65). */
+  apply_current_source(r, 1.);
+  clear_current(r);
+  restore_state(r);
+  for (int a = 0; a < 3; ++a) {
+    double* t = r->f[a].v;
+    r->f[a].v = r->old[a].v;
+    r->old[a].v = t;
+  }
+  r->replay = 1;
+  aprl_status s = push_deposit(r);
+  r->replay = 0;
+  if (s != APRL_OK) return s;
+  for (int a = 0; a < 3; ++a) {
+    double* t = r->f[a].v;
+    r->f[a].v = r->old[a].v;
+    r->old[a].v = t;
+  }
+  if (!r->preview_present) return fail(APRL_ERR_RUNTIME, "Missing electric boundary preview");
+  for (size_t n = 0; n < r->ndelta; ++n)
+    r->f[r->delta[n].axis].v[r->delta[n].index] -= r->delta[n].value;
+  r->preview_present = 0;
+  apply_current_source(r, -1.);
+  cpml_after_electric(r);
+  s = inlet_overwrite(r);
+  if (s != APRL_OK) return s;
+  r->stage = 4;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_shift(oracle_run* r) {
+  if (r->stage != 4) return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
+  const aprl_run_config* g = &r->cfg;
+  r->time += g->dt;
+  r->step += 1;
+  r->offset = g->initial_offset - (int64_t)r->step;
+  /* MovingWindowFields::Impl::shift (src/moving_window_fields.cpp:439-518). */
+  for (unsigned a = 0; a < 6; ++a) {
+    comp_t* c = &r->f[a];
+    const size_t plane = c->nx * c->ny;
+    double* fresh = (double*)malloc(plane * sizeof(double));
+    for (size_t j = 0; j < c->ny; ++j)
+      for (size_t i = 0; i < c->nx; ++i) {
+        aprl_status s = reference_value(r, a, i, j, r->offset, r->step, &fresh[j * c->nx + i]);
+        if (s != APRL_OK) {
+          free(fresh);
+          return s;
+        }
+      }
+    memmove(c->v + plane, c->v, (c->nz - 1) * plane * sizeof(double));
+    memcpy(c->v, fresh, plane * sizeof(double));
+    free(fresh);
+  }
+  clear_current(r);
+  for (unsigned h = 0; h < 12; ++h) {
+    cpml_term* t = history_term(r, h);
+    if (t->length == 0) continue;
+    const size_t layers = t->dims[2];
+    const size_t row = t->dims[t->axis == 0 ? 1 : 0];
+    const size_t slots = t->length / (layers * row);
+    for (size_t slot = 0; slot < slots; ++slot) {
+      double* base = t->history + slot * layers * row;
+      memmove(base + row, base, (layers - 1) * row * sizeof(double));
+      memset(base, 0, row * sizeof(double));
+    }
+  }
+  /* finishMovingWindowStep particle part (src/simulation_moving_window.cpp:352-371). */
+  r->origin[2] = fma((double)r->offset, g->dz, g->reference_origin[2]);
+  for (size_t n = 0; n < r->np; ++n)
+    if (r->p[n].pos[2] < r->origin[2])
+      return fail(APRL_ERR_RUNTIME, "Active particle fell behind moving inlet");
+  const double upper = fma((double)g->nz, g->dz, r->origin[2]);
+  size_t kept = 0;
+  for (size_t n = 0; n < r->nc; ++n) {
+    const carrier_t* c = &r->c[n];
+    if (c->pos[2] >= upper) {
+      ++r->cropped_carriers;
+      r->cropped_charge += c->q * c->w;
+    } else if (c->pos[2] < r->origin[2]) {
+      return fail(APRL_ERR_RUNTIME, "Current carrier fell behind moving inlet");
+    } else {
+      r->c[kept++] = *c;
+    }
+  }
+  r->nc = kept;
+  r->stage = 0;
+  return APRL_OK;
+}
+
+/* Simulation::solve loop body (src/simulation.cpp:493-613) with
+ * solveConservativeSourceStep (src/simulation_source_coupling.cpp:16-60). */
+aprl_status oracle_run_step(oracle_run* r, uint32_t steps) {
+  for (uint32_t n = 0; n < steps; ++n) {
+    aprl_status s = oracle_run_advance_magnetic(r);
+    if (s != APRL_OK) return s;
+    s = oracle_run_preview_electric(r);
+    if (s != APRL_OK) return s;
+    int converged = 0;
+    unsigned iterations = 0;
+    double force = 0., work = 0.;
+    for (unsigned t = 0; t < r->cfg.max_trials; ++t) {
+      double res[4];
+      s = oracle_run_coupling_trial(r, res);
+      if (s != APRL_OK) return s;
+      force = res[0];
+      work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
+      iterations = t + 1;
+      if (iterations >= (res[3] > 0. ? 2u : 1u) && force < r->cfg.force_tolerance &&
+          work < r->cfg.work_tolerance) {
+        converged = 1;
+        break;
+      }
+    }
+    if (!converged)
+      return fail(APRL_ERR_NOT_CONVERGED,
+                  "Conservative source coupling failed at step %llu: force=%g work=%g iterations=%u",
+                  (unsigned long long)(r->step + 1), force, work, iterations);
+    r->last_iterations = iterations;
+    if (iterations > r->max_iterations) r->max_iterations = iterations;
+    r->total_iterations += iterations;
+    r->last_force = force;
+    r->last_work = work;
+    s = oracle_run_commit_electric(r);
+    if (s != APRL_OK) return s;
+    s = oracle_run_shift(r);
+    if (s != APRL_OK) return s;
+  }
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_stats(const oracle_run* r, aprl_step_stats* st) {
+  memset(st, 0, sizeof *st);
+  st->step = r->step;
+  st->iterations = r->last_iterations;
+  st->max_iterations = r->max_iterations;
+  st->total_iterations = r->total_iterations;
+  st->force = r->last_force;
+  st->work = r->last_work;
+  st->particles = r->np;
+  st->carriers = r->nc;
+  st->exits = r->exits;
+  st->exit_charge = r->exit_charge;
+  for (int f = 0; f < 6; ++f) {
+    st->cpml_entries[f] = r->cpml_entries[f];
+    st->cpml_entry_charge[f] = r->cpml_entry_charge[f];
+    st->carrier_outer[f] = r->carrier_outer[f];
+    st->carrier_outer_charge[f] = r->carrier_outer_charge[f];
+  }
+  st->cropped_carriers = r->cropped_carriers;
+  st->cropped_charge = r->cropped_charge;
+  st->window_offset = r->offset;
+  st->origin_z = r->origin[2];
+  st->time_box = r->time;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_get_slot_fields(oracle_run* r, size_t capacity, double* used_e,
+                                       double* used_b, double* next_e, double* next_b,
+                                       size_t* count) {
+  *count = r->nslot;
+  if (!used_e && !used_b && !next_e && !next_b) return APRL_OK;
+  if (capacity < r->nslot) return fail(APRL_ERR_INVALID_ARGUMENT, "Slot buffer too small");
+  for (size_t n = 0; n < r->nslot; ++n)
+    for (int a = 0; a < 3; ++a) {
+      if (used_e) used_e[3 * n + a] = r->slot[n].used_e[a];
+      if (used_b) used_b[3 * n + a] = r->slot[n].used_b[a];
+      if (next_e) next_e[3 * n + a] = r->slot[n].next_e[a];
+      if (next_b) next_b[3 * n + a] = r->slot[n].next_b[a];
+    }
+  *count = r->nslot;
+  return APRL_OK;
+}
+
+/* ---- detector field plane (src/lab_detectors.cpp:39-99, 2426-2490,
+ *      2836-2905) ----------------------------------------------------------- */
+typedef struct {
+  size_t lower;
+  double fraction;
+} interp_axis;
+
+static interp_axis interpolation_axis(double lattice, size_t size) {
+  interp_axis r;
+  if (lattice <= 0.0) {
+    r.lower = 0;
+    r.fraction = 0.0;
+  } else if (lattice >= (double)(size - 1)) {
+    r.lower = size - 2;
+    r.fraction = 1.0;
+  } else {
+    r.lower = (size_t)floor(lattice);
+    r.fraction = lattice - (double)r.lower;
+  }
+  return r;
+}
+
+static double sample_detector_component(const comp_t* c, double lx, double ly,
+                                        const interp_axis* z) {
+  const interp_axis x = interpolation_axis(lx, c->nx), y = interpolation_axis(ly, c->ny);
+  double value = 0.0;
+  for (unsigned cz = 0; cz < 2; ++cz) {
+    const double wz = cz ? z->fraction : 1.0 - z->fraction;
+    if (wz == 0.0) continue;
+    const size_t k = z->lower + cz;
+    for (unsigned b = 0; b < 2; ++b)
+      for (unsigned a = 0; a < 2; ++a) {
+        const double wx = a ? x.fraction : 1.0 - x.fraction;
+        const double wy = b ? y.fraction : 1.0 - y.fraction;
+        value += wx * wy * wz * AT(c, x.lower + a, y.lower + b, k);
+      }
+  }
+  return value;
+}
+
+aprl_status oracle_run_sample_field_plane(oracle_run* r, double plane_lab_z, double* out,
+                                          size_t count, int* inside) {
+  const aprl_run_config* g = &r->cfg;
+  if (count != 6 * g->nx * g->ny) return fail(APRL_ERR_INVALID_ARGUMENT, "Detector buffer size mismatch");
+  const double box_z = box_z_from_lab_z_and_box_t(g, plane_lab_z, r->time);
+  const double coordinate = (box_z - r->origin[2]) / g->dz;
+  /* ownerRank (src/simulation.cpp:4068-4085): upstream of the window maps
+   * to rank 0; beyond the upper face nothing samples. */
+  const double tolerance = 64.0 * DBL_EPSILON * fmax(1.0, fabs(coordinate));
+  if (!(box_z < r->origin[2]) && coordinate > (double)g->nz + tolerance) {
+    *inside = 0;
+    return APRL_OK;
+  }
+  *inside = 1;
+  const interp_axis vertex_z = interpolation_axis(coordinate, g->nz + 1);
+  const interp_axis half_z = interpolation_axis(coordinate - 0.5, g->nz);
+  for (size_t j = 0; j < g->ny; ++j) {
+    const double py = g->reference_origin[1] + ((double)j + 0.5) * g->dy;
+    const double y = (py - g->reference_origin[1]) / g->dy;
+    for (size_t i = 0; i < g->nx; ++i) {
+      const double px = g->reference_origin[0] + ((double)i + 0.5) * g->dx;
+      const double x = (px - g->reference_origin[0]) / g->dx;
+      double eb[3], bb[3], el[3], bl[3];
+      eb[0] = sample_detector_component(&r->f[0], x - 0.5, y, &vertex_z);
+      eb[1] = sample_detector_component(&r->f[1], x, y - 0.5, &vertex_z);
+      eb[2] = sample_detector_component(&r->f[2], x, y, &half_z);
+      bb[0] = sample_detector_component(&r->f[3], x, y - 0.5, &half_z);
+      bb[1] = sample_detector_component(&r->f[4], x - 0.5, y, &half_z);
+      bb[2] = sample_detector_component(&r->f[5], x - 0.5, y - 0.5, &vertex_z);
+      fields_box_to_lab(g, eb, bb, el, bl);
+      double* o = out + 6 * (j * g->nx + i);
+      for (int a = 0; a < 3; ++a) {
+        o[a] = el[a];
+        o[3 + a] = bl[a];
+      }
+    }
+  }
+  return APRL_OK;
+}

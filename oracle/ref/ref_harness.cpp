@@ -1,0 +1,696 @@
+// ref_harness.cpp -- drives the reference's OWN hot-path classes, compiled
+// from the APRL sources by oracle/build_oracle.py into oracle/_ref/.
+// TEST INFRASTRUCTURE ONLY: it pins the plain-C oracle (oracle/pic_oracle.c)
+// to the reference arithmetic and times the reference CPU path for the
+// benchmark's CPU-baseline leg.  The product never loads it.
+//
+// The numerical operators are the reference's: EBFieldGrid (Cowan-z),
+// EBConvolutionalPML through MovingWindowFields' boundary, the moving-window
+// shift, ConservativeSourceCoupling (gather, Lapenta-Markidis push,
+// residual, E +/- J), ChargeConservingCurrentDepositor with
+// longitudinal_shape::Current, ParticleCPMLRegion, ParticleOpenBoundary,
+// BoostFrameTransform and SIFieldSourceSet.  Only the one-rank driver of
+// Simulation (src/simulation.cpp:493-613, 4167-5605,
+// src/simulation_source_coupling.cpp:16-65,
+// src/simulation_moving_window.cpp:280-379), which lives in translation
+// units that need HDF5/yaml/FFTW, is restated here for active particles and
+// CPML carriers.  The exported functions mirror include/aprl_gpu.h with the
+// prefix ref_.
+#include <mpi.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <unistd.h>
+
+#include "aprl_gpu.h"
+#include "boostframe.h"
+#include "compute_threads.h"
+#include "eb_cpml.h"
+#include "eb_deposition.h"
+#include "eb_field.h"
+#include "eb_particles.h"
+#include "eb_sources.h"
+#include "longitudinal_shape.h"
+#include "moving_window_fields.h"
+#include "particle_boundary.h"
+#include "source_coupling.h"
+#include "source_coupling_math.h"
+
+using namespace aprl;
+typedef FieldVector<Double> Vec;
+
+namespace {
+thread_local std::string g_error;
+
+aprl_status failWith(aprl_status s, const std::string& m) {
+  g_error = m;
+  return s;
+}
+
+template <class F>
+aprl_status guarded(F f) {
+  try {
+    f();
+    return APRL_OK;
+  } catch (const std::invalid_argument& e) {
+    return failWith(APRL_ERR_INVALID_ARGUMENT, e.what());
+  } catch (const std::out_of_range& e) {
+    return failWith(APRL_ERR_OUT_OF_RANGE, e.what());
+  } catch (const std::exception& e) {
+    return failWith(APRL_ERR_RUNTIME, e.what());
+  }
+}
+}  // namespace
+
+struct ref_run {
+  aprl_run_config cfg;
+  EBGridGeometry geometry;
+  EBCPMLParameters cpml;
+  std::unique_ptr<EBFieldGrid> fields;
+  std::unique_ptr<MovingWindowFields> window;
+  std::unique_ptr<ConservativeSourceCoupling> coupling;
+  BoostFrameTransform frame;
+  SIFieldSourceSet sources;
+  std::vector<double> reference[6];
+  std::size_t referenceShape[6][3];
+  std::vector<RelativisticParticleSI> particles, savedParticles;
+  std::vector<ParticleCPMLCarrier> carriers, savedCarriers;
+  std::size_t step = 0;
+  std::ptrdiff_t offset = 0;
+  double time = 0.;
+  Vec origin;
+  unsigned long long exits = 0, savedExits = 0;
+  double exitCharge = 0., savedExitCharge = 0.;
+  unsigned long long counts[3][6] = {}, savedCounts[3][6] = {};
+  double charges[3][6] = {}, savedCharges[3][6] = {};
+  unsigned long long croppedCarriers = 0;
+  double croppedCharge = 0.;
+  unsigned lastIterations = 0, maxIterations = 0;
+  unsigned long long totalIterations = 0;
+  double lastForce = 0., lastWork = 0.;
+  unsigned trials = 0;
+  int stage = 0;
+  std::string directory;
+};
+
+namespace {
+// Simulation::movingWindowFieldValue (src/simulation_moving_window.cpp:280-294)
+// over the supplied in-memory reference table.
+Double referenceValue(void* context, unsigned a, std::size_t i, std::size_t j,
+                      std::ptrdiff_t k, std::size_t step) {
+  const ref_run& r = *static_cast<ref_run*>(context);
+  const double z = static_cast<double>(k) - r.cfg.translation_beta * step;
+  const std::size_t count = r.cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0);
+  if (a >= 6 || !std::isfinite(z) || z < 0. || z > count - 1)
+    throw std::out_of_range("Moving reference query outside prepared native field");
+  const auto lo = static_cast<std::size_t>(std::floor(z)), hi = std::min(lo + 1, count - 1);
+  const auto& s = r.referenceShape[a];
+  const double f = z - lo, lower = r.reference[a].at((lo * s[1] + j) * s[0] + i);
+  return f == 0. ? lower : (1. - f) * lower + f * r.reference[a].at((hi * s[1] + j) * s[0] + i);
+}
+
+YeeComponent& component(EBFieldGrid& f, unsigned a) {
+  switch (a) {
+    case 0: return f.ex(); case 1: return f.ey(); case 2: return f.ez();
+    case 3: return f.bx(); case 4: return f.by(); case 5: return f.bz();
+    case 6: return f.jx(); case 7: return f.jy(); default: return f.jz();
+  }
+}
+
+void save(ref_run& r) {
+  r.savedParticles = r.particles;
+  r.savedCarriers = r.carriers;
+  r.savedExits = r.exits;
+  r.savedExitCharge = r.exitCharge;
+  std::memcpy(r.savedCounts, r.counts, sizeof r.counts);
+  std::memcpy(r.savedCharges, r.charges, sizeof r.charges);
+}
+
+void restore(ref_run& r) {
+  r.particles = r.savedParticles;
+  r.carriers = r.savedCarriers;
+  r.exits = r.savedExits;
+  r.exitCharge = r.savedExitCharge;
+  std::memcpy(r.counts, r.savedCounts, sizeof r.counts);
+  std::memcpy(r.charges, r.savedCharges, sizeof r.charges);
+}
+
+// Simulation::firstMovingWindowEntry (src/simulation_moving_window.cpp:380-395).
+bool firstMovingWindowEntry(const ref_run& r, const ParticleCPMLRegion& cpml,
+                            const Vec& start, const Vec& end, Double startFraction,
+                            ParticleBoundaryHit& hit) {
+  bool present = cpml.firstEntry(start, end, hit);
+  const double a = r.frame.labZFromBoxZT(start[2], r.time + startFraction * r.cfg.dt) - r.cfg.exit_lab_z;
+  const double b = r.frame.labZFromBoxZT(end[2], r.time + r.cfg.dt) - r.cfg.exit_lab_z;
+  if (a >= 0.) throw std::runtime_error("Active particle started beyond trusted moving-window exit");
+  if (b >= 0. && b > a) {
+    const double fraction = -a / (b - a);
+    if (!present || fraction < hit.fraction) {
+      for (unsigned d = 0; d < 3; ++d) hit.position[d] = start[d] + fraction * (end[d] - start[d]);
+      hit.fraction = fraction;
+      hit.face = ParticleBoundaryFace::UpperZ;
+      present = true;
+    }
+  }
+  return present;
+}
+
+// pushDepositAndMigrate for one rank, active particles and CPML carriers
+// (src/simulation.cpp:4167-5368; processCarrierSegment 4310-4407,
+// processActiveSegment 4555-4917).
+void pushDepositAndMigrate(ref_run& r) {
+  ChargeConservingCurrentDepositor depositor(*r.fields, r.origin, r.coupling->longitudinalCurrent());
+  ParticleCPMLRegion cpml(r.geometry, r.origin, r.cpml);
+  ParticleOpenBoundary boundary(r.geometry, r.origin, r.geometry, r.origin, 0);
+  const Double crossingTolerance = 64.0 * std::numeric_limits<Double>::epsilon();
+  const Double carrierCutoff = 64.0 * std::numeric_limits<Double>::epsilon();
+  std::vector<RelativisticParticleSI> retained;
+  std::vector<ParticleCPMLCarrier> retainedCarriers;
+  retained.reserve(r.particles.size());
+  const auto processCarrierSegment = [&](ParticleCPMLCarrier carrier, const Vec& segmentStart,
+                                         Double segmentStartFraction) {
+    if (!(carrier.currentWeight >= 0.0) || !std::isfinite(carrier.currentWeight))
+      throw std::runtime_error("Invalid CPML carrier current weight");
+    if (carrier.currentWeight <= carrierCutoff) return;
+    ParticleBoundaryHit outerHit;
+    const bool exitsOuter = boundary.firstExit(segmentStart, carrier.position, outerHit);
+    Double localEndFraction = 1.0;
+    Vec segmentEnd(carrier.position);
+    bool remove = false;
+    if (exitsOuter) {
+      localEndFraction = outerHit.fraction;
+      segmentEnd = outerHit.position;
+      remove = true;
+    }
+    const Double globalEndFraction = segmentStartFraction + localEndFraction * (1.0 - segmentStartFraction);
+    const Double duration = (globalEndFraction - segmentStartFraction) * r.cfg.dt;
+    Vec midpoint(0.0);
+    for (unsigned a = 0; a < 3; ++a) midpoint[a] = 0.5 * (segmentStart[a] + segmentEnd[a]);
+    const Double midpointDamping = cpml.currentDampingFactor(segmentStart, midpoint, 0.5 * duration);
+    const Double endDamping = cpml.currentDampingFactor(segmentStart, segmentEnd, duration);
+    const Double depositedWeight = carrier.currentWeight * midpointDamping;
+    const Double endWeight = carrier.currentWeight * endDamping;
+    depositor.depositSegment(segmentStart, segmentEnd, carrier.charge * depositedWeight);
+    if (remove) {
+      const std::size_t face = static_cast<std::size_t>(outerHit.face);
+      ++r.counts[2][face];
+      r.charges[2][face] += carrier.charge * endWeight;
+      return;
+    }
+    if (endWeight <= carrierCutoff) return;
+    carrier.currentWeight = endWeight;
+    carrier.position = segmentEnd;
+    retainedCarriers.push_back(carrier);
+  };
+  for (std::size_t n = 0; n < r.carriers.size(); ++n) {
+    ParticleCPMLCarrier carrier = r.carriers[n];
+    const Vec start(carrier.position);
+    carrier.position.pmv(r.cfg.dt, carrier.velocity);
+    processCarrierSegment(carrier, start, 0.0);
+  }
+  for (std::size_t n = 0; n < r.particles.size(); ++n) {
+    RelativisticParticleSI particle = r.particles[n];
+    const Vec start(particle.position);
+    if (start[2] < r.origin[2] && !particle.frozen)
+      throw std::runtime_error("An active particle is upstream of the moving window; the inlet guard did not contain its release event");
+    r.coupling->push(particle, r.sources, r.frame, r.time, r.cfg.dt, r.cfg.substeps, 0, 0, 0);
+    ParticleBoundaryHit cpmlHit, outerHit;
+    const bool entersCpml = firstMovingWindowEntry(r, cpml, start, particle.position, 0.0, cpmlHit);
+    const bool exitsOuter = boundary.firstExit(start, particle.position, outerHit);
+    int action = 0;
+    Double localEndFraction = 1.0;
+    Vec segmentEnd(particle.position);
+    ParticleBoundaryHit selected;
+    if (entersCpml && (!exitsOuter || cpmlHit.fraction <= outerHit.fraction + crossingTolerance)) {
+      action = 1;
+      localEndFraction = cpmlHit.fraction;
+      segmentEnd = cpmlHit.position;
+      selected = cpmlHit;
+    } else if (exitsOuter) {
+      action = 2;
+      localEndFraction = outerHit.fraction;
+      segmentEnd = outerHit.position;
+      selected = outerHit;
+    }
+    depositor.depositSegment(start, segmentEnd, particle.charge);
+    const Double globalEndFraction = 0.0 + localEndFraction * (1.0 - 0.0);
+    if (action == 1) {
+      const std::size_t face = static_cast<std::size_t>(selected.face);
+      if (selected.face == ParticleBoundaryFace::UpperZ) {
+        ++r.exits;
+        r.exitCharge += particle.charge;
+      } else {
+        ++r.counts[0][face];
+        r.charges[0][face] += particle.charge;
+      }
+      ParticleCPMLCarrier carrier;
+      carrier.position = particle.position;
+      const Double gamma = BoostFrameTransform::gammaFromProperVelocity(particle.properVelocity);
+      carrier.velocity = particle.properVelocity;
+      carrier.velocity *= SI::c / gamma;
+      carrier.charge = particle.charge;
+      carrier.currentWeight = 1.0;
+      processCarrierSegment(carrier, selected.position, globalEndFraction);
+    } else if (action == 2) {
+      const std::size_t face = static_cast<std::size_t>(selected.face);
+      ++r.counts[1][face];
+      r.charges[1][face] += particle.charge;
+    } else {
+      retained.push_back(particle);
+    }
+  }
+  r.particles.swap(retained);
+  r.carriers.swap(retainedCarriers);
+}
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+aprl_status ref_run_create(const aprl_run_config* config, ref_run** out) {
+  auto run = std::unique_ptr<ref_run>(new ref_run());
+  ref_run& r = *run;
+  r.cfg = *config;
+  return guarded([&] {
+    r.geometry = EBGridGeometry(config->nx, config->ny, config->nz, config->dx, config->dy,
+                                config->dz, config->dt, EBMaxwellSolver::CowanZ);
+    r.cpml.cells[0] = config->cpml_cells_x;
+    r.cpml.cells[1] = config->cpml_cells_y;
+    r.cpml.cells[2] = 0;
+    r.cpml.polynomialOrder = config->cpml_polynomial_order;
+    r.cpml.targetReflection = config->cpml_target_reflection;
+    r.cpml.kappaMax = config->cpml_kappa_max;
+    r.cpml.alphaFraction = config->cpml_alpha_fraction;
+    r.fields.reset(new EBFieldGrid(r.geometry));
+    for (unsigned a = 0; a < 6; ++a) {
+      const YeeComponent& c = component(*r.fields, a);
+      r.referenceShape[a][0] = c.nx();
+      r.referenceShape[a][1] = c.ny();
+      r.referenceShape[a][2] = config->reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0);
+    }
+    MovingWindowReference reference;
+    reference.context = &r;
+    reference.value = &referenceValue;
+    r.window.reset(new MovingWindowFields(r.geometry, config->nz, 0, MPI_COMM_WORLD, r.cpml, reference));
+    r.window->installBoundary(*r.fields);
+    char pattern[] = "/tmp/aprl_ref_XXXXXX";
+    const char* dir = mkdtemp(pattern);
+    if (!dir) throw std::runtime_error("Cannot create coupling log directory");
+    r.directory = dir;
+    const bool binomial = config->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+    r.coupling.reset(new ConservativeSourceCoupling(MPI_COMM_WORLD, r.directory, !binomial, false,
+                                                    binomial, false, false, binomial));
+    r.frame.setOriginsFromGamma(config->boost_gamma, SI::c, config->lab_time_origin,
+                                config->lab_z_origin, config->box_z_origin);
+    for (unsigned m = 0; m < config->n_magnets; ++m) {
+      const aprl_magnet& g = config->magnets[m];
+      SIMagneticElement e;
+      e.type = g.type == APRL_MAGNET_PLANAR_UNDULATOR ? SIMagnetType::PlanarUndulator
+               : (g.type == APRL_MAGNET_UNIFORM_DIPOLE ? SIMagnetType::UniformDipole
+                                                       : SIMagnetType::Quadrupole);
+      for (unsigned a = 0; a < 3; ++a) e.center[a] = g.center[a];
+      e.length = g.length;
+      e.period = g.period;
+      e.peakMagneticField = g.peak_field;
+      e.polarizationAngle = g.polarization_angle;
+      e.gaussianFringe = g.gaussian_fringe != 0;
+      e.fringeRelativeCutoff = g.fringe_relative_cutoff;
+      e.quadrupoleGradient = g.quadrupole_gradient;
+      e.prepare();
+      r.sources.addPrescribedLabMagnet(e);
+    }
+    r.offset = config->initial_offset;
+    r.origin[0] = config->reference_origin[0];
+    r.origin[1] = config->reference_origin[1];
+    r.origin[2] = std::fma(static_cast<double>(config->initial_offset), config->dz,
+                           config->reference_origin[2]);
+    *out = run.release();
+  });
+}
+
+aprl_status ref_run_destroy(ref_run* r) {
+  if (r) {
+    const std::string dir = r->directory;
+    delete r;
+    if (!dir.empty()) {
+      std::string command = "rm -rf '" + dir + "'";
+      if (std::system(command.c_str()) != 0) return failWith(APRL_ERR_RUNTIME, "cannot remove log directory");
+    }
+  }
+  return APRL_OK;
+}
+
+aprl_status ref_set_threads(unsigned threads) {
+  return guarded([&] { configureComputeThreads(MPI_THREAD_FUNNELED, static_cast<int>(threads)); });
+}
+
+aprl_status ref_run_set_reference(ref_run* r, unsigned a, const double* host, size_t count) {
+  if (a >= 6) return failWith(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
+  const auto& s = r->referenceShape[a];
+  if (count != s[0] * s[1] * s[2]) return failWith(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
+  r->reference[a].assign(host, host + count);
+  return APRL_OK;
+}
+
+aprl_status ref_run_set_field(ref_run* r, unsigned a, const double* host, size_t count) {
+  if (a >= 9) return failWith(APRL_ERR_OUT_OF_RANGE, "Field component");
+  YeeComponent& c = component(*r->fields, a);
+  if (count != c.size()) return failWith(APRL_ERR_INVALID_ARGUMENT, "Field component size mismatch");
+  std::copy(host, host + count, c.data());
+  return APRL_OK;
+}
+
+aprl_status ref_run_get_field(ref_run* r, unsigned a, double* host, size_t count) {
+  if (a >= 9) return failWith(APRL_ERR_OUT_OF_RANGE, "Field component");
+  YeeComponent& c = component(*r->fields, a);
+  if (count != c.size()) return failWith(APRL_ERR_INVALID_ARGUMENT, "Field component size mismatch");
+  std::copy(c.data(), c.data() + count, host);
+  return APRL_OK;
+}
+
+aprl_status ref_run_history_length(ref_run* r, unsigned index, uint64_t* length) {
+  return guarded([&] {
+    EBConvolutionalPML& p = dynamic_cast<EBConvolutionalPML&>(r->fields->boundary());
+    *length = p.checkpointHistory(index).size();
+  });
+}
+
+aprl_status ref_run_set_history(ref_run* r, unsigned index, const double* host, size_t count) {
+  return guarded([&] {
+    EBConvolutionalPML& p = dynamic_cast<EBConvolutionalPML&>(r->fields->boundary());
+    std::vector<Double>& h = p.checkpointHistory(index);
+    if (h.size() != count) throw std::invalid_argument("CPML history size mismatch");
+    std::copy(host, host + count, h.begin());
+  });
+}
+
+aprl_status ref_run_get_history(ref_run* r, unsigned index, double* host, size_t count) {
+  return guarded([&] {
+    EBConvolutionalPML& p = dynamic_cast<EBConvolutionalPML&>(r->fields->boundary());
+    const std::vector<Double>& h = p.checkpointHistory(index);
+    if (h.size() != count) throw std::invalid_argument("CPML history size mismatch");
+    std::copy(h.begin(), h.end(), host);
+  });
+}
+
+aprl_status ref_run_set_particles(ref_run* r, size_t n, const double* x, const double* y,
+                                  const double* z, const double* ux, const double* uy,
+                                  const double* uz, const double* q, const double* m,
+                                  const uint64_t* id, int resetCarriers) {
+  r->particles.assign(n, RelativisticParticleSI());
+  for (size_t i = 0; i < n; ++i) {
+    RelativisticParticleSI& p = r->particles[i];
+    p.position[0] = x[i]; p.position[1] = y[i]; p.position[2] = z[i];
+    p.properVelocity[0] = ux[i]; p.properVelocity[1] = uy[i]; p.properVelocity[2] = uz[i];
+    p.charge = q[i]; p.mass = m[i]; p.weight = 1.0; p.id = id[i]; p.sourceId = id[i];
+    p.frozen = false; p.frozenBetaZ = 0.0;
+  }
+  if (resetCarriers) r->carriers.clear();
+  return APRL_OK;
+}
+
+aprl_status ref_run_particle_count(ref_run* r, size_t* count) {
+  *count = r->particles.size();
+  return APRL_OK;
+}
+
+aprl_status ref_run_get_particles(ref_run* r, size_t capacity, double* x, double* y, double* z,
+                                  double* ux, double* uy, double* uz, double* q, double* m,
+                                  uint64_t* id, size_t* count) {
+  if (capacity < r->particles.size()) return failWith(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  for (size_t i = 0; i < r->particles.size(); ++i) {
+    const RelativisticParticleSI& p = r->particles[i];
+    if (x) x[i] = p.position[0];
+    if (y) y[i] = p.position[1];
+    if (z) z[i] = p.position[2];
+    if (ux) ux[i] = p.properVelocity[0];
+    if (uy) uy[i] = p.properVelocity[1];
+    if (uz) uz[i] = p.properVelocity[2];
+    if (q) q[i] = p.charge;
+    if (m) m[i] = p.mass;
+    if (id) id[i] = p.id;
+  }
+  *count = r->particles.size();
+  return APRL_OK;
+}
+
+aprl_status ref_run_carrier_count(ref_run* r, size_t* count) {
+  *count = r->carriers.size();
+  return APRL_OK;
+}
+
+aprl_status ref_run_get_carriers(ref_run* r, size_t capacity, double* pos, double* vel,
+                                 double* q, double* w, size_t* count) {
+  if (capacity < r->carriers.size()) return failWith(APRL_ERR_INVALID_ARGUMENT, "Carrier buffer too small");
+  for (size_t i = 0; i < r->carriers.size(); ++i) {
+    const ParticleCPMLCarrier& c = r->carriers[i];
+    for (unsigned a = 0; a < 3; ++a) {
+      if (pos) pos[3 * i + a] = c.position[a];
+      if (vel) vel[3 * i + a] = c.velocity[a];
+    }
+    if (q) q[i] = c.charge;
+    if (w) w[i] = c.currentWeight;
+  }
+  *count = r->carriers.size();
+  return APRL_OK;
+}
+
+aprl_status ref_run_set_carriers(ref_run* r, size_t n, const double* pos, const double* vel,
+                                 const double* q, const double* w) {
+  r->carriers.assign(n, ParticleCPMLCarrier());
+  for (size_t i = 0; i < n; ++i) {
+    for (unsigned a = 0; a < 3; ++a) {
+      r->carriers[i].position[a] = pos[3 * i + a];
+      r->carriers[i].velocity[a] = vel[3 * i + a];
+    }
+    r->carriers[i].charge = q[i];
+    r->carriers[i].currentWeight = w[i];
+  }
+  return APRL_OK;
+}
+
+aprl_status ref_run_advance_magnetic(ref_run* r) {
+  return guarded([&] {
+    r->fields->clearCurrent();
+    r->window->beginStep(*r->fields, r->step, r->offset);
+    const EBElectricHaloView halo = r->window->physicalElectricHalos(*r->fields, r->step);
+    r->fields->advanceMagnetic(halo);
+    r->stage = 1;
+  });
+}
+
+aprl_status ref_run_preview_electric(ref_run* r) {
+  return guarded([&] {
+    if (r->stage != 1) throw std::logic_error("Moving-window electric phase mismatch");
+    r->coupling->begin(*r->fields, r->origin, r->particles, r->cfg.cpml_cells_x, r->cfg.cpml_cells_y);
+    r->window->previewElectricBoundary(true);
+    r->fields->advanceElectric();
+    r->window->previewElectricBoundary(false);
+    save(*r);
+    r->trials = 0;
+    r->stage = 2;
+  });
+}
+
+aprl_status ref_run_coupling_trial(ref_run* r, double residual[4]) {
+  return guarded([&] {
+    if (r->stage != 2 && r->stage != 3) throw std::logic_error("Coupling trial requires a previewed electric field");
+    if (r->trials) r->coupling->applyCurrentSource(1.);
+    r->fields->clearCurrent();
+    restore(*r);
+    r->coupling->beginTrial();
+    r->coupling->exchangeCandidate();
+    pushDepositAndMigrate(*r);
+    r->coupling->completeCurrent();
+    r->coupling->applyCurrentSource(-1.);
+    r->coupling->exchangeCandidate();
+    const auto res = r->coupling->localResidual();
+    for (int i = 0; i < 4; ++i) residual[i] = res[i];
+    ++r->trials;
+    r->stage = 3;
+  });
+}
+
+aprl_status ref_run_commit_electric(ref_run* r) {
+  return guarded([&] {
+    if (r->stage != 3) throw std::logic_error("Commit requires a completed coupling trial");
+    r->coupling->applyCurrentSource(1.);
+    r->fields->clearCurrent();
+    restore(*r);
+    r->coupling->swapElectric();
+    r->coupling->setReplay(true);
+    pushDepositAndMigrate(*r);
+    r->coupling->completeCurrent();
+    r->coupling->setReplay(false);
+    r->coupling->finish(r->step + 1, r->lastIterations, r->lastForce, r->lastWork);
+    r->coupling->swapElectric();
+    r->window->undoPreviewElectricBoundary(*r->fields);
+    r->coupling->applyCurrentSource(-1.);
+    r->window->commitPreparedElectricBoundary(*r->fields);
+    r->stage = 4;
+  });
+}
+
+aprl_status ref_run_shift(ref_run* r) {
+  return guarded([&] {
+    if (r->stage != 4) throw std::logic_error("Moving-window requires one left shift after each complete step");
+    r->time += r->cfg.dt;
+    ++r->step;
+    r->offset = r->cfg.initial_offset - static_cast<std::ptrdiff_t>(r->step);
+    r->window->shift(*r->fields, r->step, r->offset);
+    r->origin[2] = std::fma(static_cast<double>(r->offset), r->cfg.dz, r->cfg.reference_origin[2]);
+    for (const auto& p : r->particles)
+      if (p.position[2] < r->origin[2] && !p.frozen)
+        throw std::runtime_error("Active particle fell behind moving inlet");
+    const double upper = std::fma(static_cast<double>(r->cfg.nz), r->cfg.dz, r->origin[2]);
+    std::size_t kept = 0;
+    for (const auto& c : r->carriers) {
+      if (c.position[2] >= upper) {
+        ++r->croppedCarriers;
+        r->croppedCharge += c.charge * c.currentWeight;
+      } else if (c.position[2] < r->origin[2]) {
+        throw std::runtime_error("Current carrier fell behind moving inlet");
+      } else {
+        r->carriers[kept++] = c;
+      }
+    }
+    r->carriers.resize(kept);
+    r->stage = 0;
+  });
+}
+
+aprl_status ref_run_step(ref_run* r, uint32_t steps) {
+  for (uint32_t n = 0; n < steps; ++n) {
+    aprl_status s = ref_run_advance_magnetic(r);
+    if (s != APRL_OK) return s;
+    s = ref_run_preview_electric(r);
+    if (s != APRL_OK) return s;
+    bool converged = false;
+    unsigned iterations = 0;
+    double force = 0., work = 0.;
+    for (unsigned t = 0; t < r->cfg.max_trials; ++t) {
+      double res[4];
+      s = ref_run_coupling_trial(r, res);
+      if (s != APRL_OK) return s;
+      force = res[0];
+      work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
+      iterations = t + 1;
+      if (iterations >= (res[3] > 0. ? 2u : 1u) && force < r->cfg.force_tolerance &&
+          work < r->cfg.work_tolerance) {
+        converged = true;
+        break;
+      }
+    }
+    if (!converged) return failWith(APRL_ERR_NOT_CONVERGED, "Conservative source coupling failed");
+    r->lastIterations = iterations;
+    r->maxIterations = std::max(r->maxIterations, iterations);
+    r->totalIterations += iterations;
+    r->lastForce = force;
+    r->lastWork = work;
+    s = ref_run_commit_electric(r);
+    if (s != APRL_OK) return s;
+    s = ref_run_shift(r);
+    if (s != APRL_OK) return s;
+  }
+  return APRL_OK;
+}
+
+aprl_status ref_run_get_stats(ref_run* r, aprl_step_stats* st) {
+  std::memset(st, 0, sizeof *st);
+  st->step = r->step;
+  st->iterations = r->lastIterations;
+  st->max_iterations = r->maxIterations;
+  st->total_iterations = r->totalIterations;
+  st->force = r->lastForce;
+  st->work = r->lastWork;
+  st->particles = r->particles.size();
+  st->carriers = r->carriers.size();
+  st->exits = r->exits;
+  st->exit_charge = r->exitCharge;
+  for (int f = 0; f < 6; ++f) {
+    st->cpml_entries[f] = r->counts[0][f];
+    st->cpml_entry_charge[f] = r->charges[0][f];
+    st->carrier_outer[f] = r->counts[2][f];
+    st->carrier_outer_charge[f] = r->charges[2][f];
+  }
+  st->cropped_carriers = r->croppedCarriers;
+  st->cropped_charge = r->croppedCharge;
+  st->window_offset = r->offset;
+  st->origin_z = r->origin[2];
+  st->time_box = r->time;
+  return APRL_OK;
+}
+
+// Direct operator probes on the reference's own kernels.
+long ref_shape_weights(const aprl_run_config* config, const double origin[3], const double begin[3],
+                       const double end[3], int32_t* axis, int64_t* index, double* weight,
+                       long capacity) {
+  try {
+    EBGridGeometry g(config->nx, config->ny, config->nz, config->dx, config->dy, config->dz,
+                     config->dt, EBMaxwellSolver::CowanZ);
+    Vec o, b, e;
+    for (unsigned a = 0; a < 3; ++a) { o[a] = origin[a]; b[a] = begin[a]; e[a] = end[a]; }
+    long count = 0;
+    const bool binomial = config->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+    longitudinal_shape::weights(g, o, b, e, [&](unsigned d, long long i, long long j, long long k, double w) {
+      if (count < capacity) {
+        axis[count] = static_cast<int32_t>(d);
+        index[3 * count] = i; index[3 * count + 1] = j; index[3 * count + 2] = k;
+        weight[count] = w;
+      }
+      ++count;
+    }, binomial ? longitudinal_shape::Shape::LinearBinomial3 : longitudinal_shape::Shape::QuinticCompensated, binomial);
+    return count;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+int ref_momentum(double u[3], const double e[3], const double b[3], double q, double m, double h,
+                 double knownGamma) {
+  try {
+    Vec uu, ee, bb;
+    for (unsigned a = 0; a < 3; ++a) { uu[a] = u[a]; ee[a] = e[a]; bb[a] = b[a]; }
+    const unsigned it = source_coupling_math::momentum(uu, ee, bb, q, m, h, knownGamma);
+    for (unsigned a = 0; a < 3; ++a) u[a] = uu[a];
+    return static_cast<int>(it);
+  } catch (const std::exception& ex) {
+    g_error = ex.what();
+    return -1;
+  }
+}
+
+double ref_gamma(const double u[3]) {
+  Vec uu;
+  for (unsigned a = 0; a < 3; ++a) uu[a] = u[a];
+  return BoostFrameTransform::gammaFromProperVelocity(uu);
+}
+
+aprl_status ref_prescribed_box(ref_run* r, const double position[3], double time, double e[3],
+                               double b[3]) {
+  return guarded([&] {
+    Vec p, ee(0.), bb(0.);
+    for (unsigned a = 0; a < 3; ++a) p[a] = position[a];
+    r->sources.addPrescribedBox(p, time, r->frame, ee, bb);
+    for (unsigned a = 0; a < 3; ++a) { e[a] = ee[a]; b[a] = bb[a]; }
+  });
+}
+
+aprl_status ref_cowan_coefficients(double dx, double dy, double dz, double out[12]) {
+  return guarded([&] {
+    const EBCowanCoefficients c = EBCowanCoefficients::forZDispersion(dx, dy, dz);
+    for (int a = 0; a < 3; ++a) { out[a] = c.alpha[a]; out[3 + a] = c.beta[a]; out[9 + a] = c.ratio[a]; }
+    out[6] = c.deltaXY; out[7] = c.deltaYZ; out[8] = c.deltaZX;
+  });
+}
+
+}  // extern "C"

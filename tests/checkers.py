@@ -1,0 +1,119 @@
+"""Loaders for the CPU checkers under oracle/ (test infrastructure only).
+
+The plain-C oracle (oracle/libpic_oracle.so) and, where it was built, the
+reference's own translation units (oracle/_ref/libaprl_ref.so) export the
+same ABI as the product under the prefixes `oracle_` and `ref_`.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+from aprl_b200 import abi, native  # noqa: E402
+
+ORACLE_PATH = os.path.join(REPO, "oracle", "libpic_oracle.so")
+REFERENCE_PATH = os.path.join(REPO, "oracle", "_ref", "libaprl_ref.so")
+
+_oracle = None
+_reference = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_PATH):
+            subprocess.check_call([sys.executable,
+                                   os.path.join(REPO, "oracle", "build_oracle.py")])
+        lib = C.CDLL(ORACLE_PATH)
+        _oracle = native.bind(lib, "oracle_")
+        f = lib.oracle_shape_weights
+        f.restype = C.c_long
+        f.argtypes = [C.POINTER(abi.RunConfig), C.POINTER(C.c_double),
+                      C.POINTER(C.c_double), C.POINTER(C.c_double),
+                      C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                      C.POINTER(C.c_double), C.c_long]
+        f = lib.oracle_momentum
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(C.c_double)] * 3 + [C.c_double] * 4
+        f = lib.oracle_gamma
+        f.restype = C.c_double
+        f.argtypes = [C.POINTER(C.c_double)]
+    return _oracle
+
+
+def reference_available():
+    return os.path.exists(REFERENCE_PATH)
+
+
+def reference():
+    global _reference
+    if _reference is None:
+        lib = C.CDLL(REFERENCE_PATH)
+        _reference = native.bind(lib, "ref_")
+        f = lib.ref_shape_weights
+        f.restype = C.c_long
+        f.argtypes = [C.POINTER(abi.RunConfig), C.POINTER(C.c_double),
+                      C.POINTER(C.c_double), C.POINTER(C.c_double),
+                      C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                      C.POINTER(C.c_double), C.c_long]
+        f = lib.ref_momentum
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(C.c_double)] * 3 + [C.c_double] * 4
+        f = lib.ref_gamma
+        f.restype = C.c_double
+        f.argtypes = [C.POINTER(C.c_double)]
+        f = lib.ref_set_threads
+        f.restype = C.c_int
+        f.argtypes = [C.c_uint]
+    return _reference
+
+
+def shape_weights(binding, config, origin, begin, end, capacity=8192):
+    axis = np.empty(capacity, dtype=np.int32)
+    index = np.empty((capacity, 3), dtype=np.int64)
+    weight = np.empty(capacity)
+    f = getattr(binding.lib, binding.prefix + "shape_weights")
+    d = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+    n = f(C.byref(config), d(origin), d(begin), d(end),
+          axis.ctypes.data_as(C.POINTER(C.c_int32)),
+          index.ctypes.data_as(C.POINTER(C.c_int64)),
+          weight.ctypes.data_as(C.POINTER(C.c_double)), capacity)
+    if n < 0:
+        raise native.AprlError(abi.APRL_ERR_RUNTIME, binding.error())
+    return axis[:n], index[:n], weight[:n]
+
+
+def run(binding, workload):
+    return native.Run(binding, workload.config).load_workload(workload)
+
+
+def state(run_handle, histories=True):
+    """Everything observable after a step, as numpy arrays."""
+    out = {"fields": [run_handle.get_field(a) for a in range(6)],
+           "particles": run_handle.get_particles(),
+           "carriers": run_handle.get_carriers(),
+           "stats": run_handle.stats()}
+    if histories:
+        out["histories"] = [run_handle.get_history(h) for h in range(12)]
+    return out
+
+
+def max_relative(a, b):
+    """max |a-b| / max |b| (0 when both vanish)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.shape != b.shape:
+        raise AssertionError(f"shape mismatch {a.shape} vs {b.shape}")
+    if a.size == 0:
+        return 0.0
+    scale = np.max(np.abs(b))
+    diff = np.max(np.abs(a - b))
+    if scale == 0.0:
+        return float(diff)
+    return float(diff / scale)
