@@ -1,0 +1,66 @@
+"""Build the in-tree CUDA library aprl_b200/libaprl_b200.so for sm_100a.
+
+The FP64 drop-in kernels are compiled without FMA contraction
+(--fmad=false) so their arithmetic follows the reference's operation order.
+
+Usage: python -m aprl_b200.build [--force]
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUTPUT = os.path.join(HERE, "libaprl_b200.so")
+SOURCES = ["run.cu", "fields.cu", "particles.cu"]
+HEADERS = ["common.cuh", "fields.cuh", "particles.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc():
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(path):
+        raise RuntimeError("nvcc not found")
+    return path
+
+
+def flags():
+    return ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler",
+            "-fPIC", "-I", os.path.join(REPO, "include")] + ARCH
+
+
+def build(force=False, verbose=True):
+    deps = ([os.path.join(CSRC, s) for s in SOURCES + HEADERS] +
+            [os.path.join(REPO, "include", "aprl_gpu.h")])
+    if (not force and os.path.exists(OUTPUT) and
+            all(os.path.getmtime(d) <= os.path.getmtime(OUTPUT) for d in deps)):
+        return OUTPUT
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objects = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = [nvcc(), "-rdc=false", "-c", os.path.join(CSRC, src), "-o", obj] + flags()
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+        objects.append(obj)
+    cmd = [nvcc(), "-shared", "-o", OUTPUT] + objects + ARCH + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return OUTPUT
+
+
+def main(argv=None):
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--force", action="store_true")
+    args = parser.parse_args(argv)
+    build(force=args.force)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

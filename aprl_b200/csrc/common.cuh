@@ -1,0 +1,149 @@
+// common.cuh -- device-side views, constants and helpers shared by the field
+// and particle kernels of the B200 PIC step.
+//
+// Memory layout in HBM (one run):
+//   * Yee components in the reference's SoA layout, x fastest,
+//     index (k*ny_c + j)*nx_c + i (src/eb_field.h:134-141), but E and B are
+//     z RING BUFFERS: logical plane k lives at physical plane
+//     (k + zbase_c) mod nz_c.  The moving-window shift
+//     (src/moving_window_fields.cpp:439-518) then only decrements zbase and
+//     rewrites the one inserted plane instead of moving the volume.
+//   * Two E buffers: E^n ("old", read by the orbit-averaged gather) and
+//     E* ("star", the zero-current preview with its boundary applied).  The
+//     trial candidate E* - dt/eps0 J is never stored: every gather forms it
+//     from E* and J, so a fixed-point trial touches the grid only through J.
+//   * J is not ring-buffered: it is cleared before every trial.
+//   * CPML convolution histories keep the reference's [slot][k][row] order
+//     (src/eb_cpml.cpp:42-96) with the same z ring as their component.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace aprl_gpu {
+
+constexpr double kC = 299792458.0;          // src/eb_field.cpp:15-19
+constexpr double kEpsilon0 = 8.8541878128e-12;
+constexpr double kMu0 = 1.25663706212e-6;
+constexpr double kEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+constexpr double kDblMin = 2.2250738585072013830903e-308;
+constexpr double kPi = 3.14159265358979323846;
+
+// Device error codes (first error wins; the host maps them to statuses).
+enum DeviceError : unsigned {
+  kErrNone = 0,
+  kErrCrossingBudget = 1,     // weights(): more than 64 cuts
+  kErrOrbitOutside = 2,       // clipOpenOrbit found no in-domain part
+  kErrDepositOutside = 3,     // depositor endpoint outside the E/B domain
+  kErrSupportX = 4,           // quintic transverse support outside x grid
+  kErrSupportY = 5,           // transverse support outside y grid
+  kErrRootNonphysical = 6,    // momentum(): nonphysical mean-gamma root
+  kErrRootNoConvergence = 7,  // momentum(): 12 Newton steps exhausted
+  kErrNonFinite = 8,          // non-finite particle coordinate
+  kErrStartInCpml = 9,        // active particle starts in the CPML region
+  kErrStartOutside = 10,      // trajectory starts outside the domain
+  kErrBeyondExit = 11,        // active particle started beyond the exit
+  kErrUpstream = 12,          // active particle upstream of the inlet
+  kErrCarrierWeight = 13,     // invalid carrier weight
+  kErrFellBehind = 14,        // particle/carrier behind the moving inlet
+  kErrReferenceRange = 15,    // inlet reference query outside the table
+  kErrHitLocate = 16,         // boundary hit fraction outside [0,1]
+  kErrCount
+};
+
+struct DeviceStatus {
+  unsigned code;
+  unsigned long long where;  // particle or element index of the first error
+};
+
+__device__ __forceinline__ void raise_error(DeviceStatus* s, unsigned code,
+                                            unsigned long long where) {
+  if (atomicCAS(&s->code, 0u, code) == 0u) s->where = where;
+}
+
+// One magnet of SIFieldSourceSet (src/eb_sources.h:103-140).
+struct DMagnet {
+  int type;  // 0 undulator, 1 dipole, 2 quadrupole
+  int gaussian_fringe;
+  double center[3];
+  double length, period, peak_field;
+  double quadrupole_gradient, wave_number, fringe_extent;
+  double cos_angle, sin_angle;
+};
+
+struct DFrame {  // BoostFrameTransform
+  double gamma, beta, gamma_beta;
+  double lab_time_origin, lab_z_origin, box_z_origin;
+};
+
+// Everything the kernels need about the grid; passed by value.
+struct DGrid {
+  int nx, ny, nz;
+  double dx, dy, dz, dt;
+  double origin[3];      // localOriginBox_ of the current window
+  double* e_old[3];      // E^n  (ring)
+  double* e_star[3];     // E*   (ring)
+  double* b[3];          // B    (ring)
+  double* j[3];          // J    (plain)
+  int zb_e[3];           // ring bases of Ex Ey Ez
+  int zb_b[3];           // ring bases of Bx By Bz
+  double jcoef;          // (-1*dt)/eps0, applyCurrentSource(-1) scale
+};
+
+__device__ __forceinline__ int e_nx(const DGrid& g, int c) { return g.nx + (c != 0); }
+__device__ __forceinline__ int e_ny(const DGrid& g, int c) { return g.ny + (c != 1); }
+__device__ __forceinline__ int e_nz(const DGrid& g, int c) { return g.nz + (c != 2); }
+__device__ __forceinline__ int b_nx(const DGrid& g, int c) { return g.nx + (c == 0); }
+__device__ __forceinline__ int b_ny(const DGrid& g, int c) { return g.ny + (c == 1); }
+__device__ __forceinline__ int b_nz(const DGrid& g, int c) { return g.nz + (c == 2); }
+
+__device__ __forceinline__ int ring(int k, int base, int n) {
+  int p = k + base;
+  return p >= n ? p - n : p;
+}
+
+__device__ __forceinline__ size_t e_index(const DGrid& g, int c, int i, int j, int k) {
+  const int nzc = e_nz(g, c);
+  return ((size_t)ring(k, g.zb_e[c], nzc) * e_ny(g, c) + j) * e_nx(g, c) + i;
+}
+
+__device__ __forceinline__ size_t b_index(const DGrid& g, int c, int i, int j, int k) {
+  const int nzc = b_nz(g, c);
+  return ((size_t)ring(k, g.zb_b[c], nzc) * b_ny(g, c) + j) * b_nx(g, c) + i;
+}
+
+__device__ __forceinline__ size_t j_index(const DGrid& g, int c, int i, int j, int k) {
+  return ((size_t)k * e_ny(g, c) + j) * e_nx(g, c) + i;
+}
+
+// applyCurrentSource's interior mask (src/source_coupling.cpp:87) at one rank.
+__device__ __forceinline__ bool current_mask(const DGrid& g, int c, int i, int j, int k) {
+  if (c == 0) return j > 0 && j < g.ny && k != 0 && k != g.nz;
+  if (c == 1) return i > 0 && i < g.nx && k != 0 && k != g.nz;
+  return i > 0 && i < g.nx && j > 0 && j < g.ny;
+}
+
+// Trial candidate E* - dt/eps0 J at a native node (applyCurrentSource(-1)).
+__device__ __forceinline__ double e_candidate(const DGrid& g, int c, int i, int j, int k) {
+  double v = g.e_star[c][e_index(g, c, i, j, k)];
+  if (current_mask(g, c, i, j, k)) {
+    const double jc = g.j[c][j_index(g, c, i, j, k)];
+    if (jc != 0.) v += g.jcoef * jc;
+  }
+  return v;
+}
+
+// BoostFrameTransform::gammaFromProperVelocity (src/boostframe.cpp:74-87).
+__device__ __forceinline__ double gamma_u(double ux, double uy, double uz) {
+  const double scale = fmax(1.0, fmax(fabs(ux), fmax(fabs(uy), fabs(uz))));
+  const double inv = 1.0 / scale;
+  const double a = ux * inv, b = uy * inv, c = uz * inv;
+  return scale * sqrt(inv * inv + a * a + b * b + c * c);
+}
+
+// labZFromBoxZT (src/boostframe.cpp:241-245).
+__device__ __forceinline__ double lab_z_from_box_zt(const DFrame& f, double z, double t) {
+  return f.lab_z_origin + fma(f.gamma_beta * kC, t, f.gamma * (z - f.box_z_origin));
+}
+
+}  // namespace aprl_gpu

@@ -1,0 +1,334 @@
+// fields.cu -- grid kernels of the step: Cowan-z Faraday with the CPML
+// magnetic correction, the zero-current Ampere preview with the CPML
+// electric correction, PEC termination and inlet overwrite, the commit
+// E^{n+1} = E* - dt/eps0 J, and the moving-window plane insertion.
+//
+// FP64 drop-in arithmetic: every expression keeps the reference's operation
+// order and the library is compiled without FMA contraction, so these
+// kernels reproduce the reference's translation units bit for bit.
+#include "common.cuh"
+#include "fields.cuh"
+
+namespace aprl_gpu {
+
+// electricValue (src/eb_field.cpp:350-417) under the moving window: x/y
+// PEC parity extension, z halo planes (lower = inlet reference plane,
+// upper = the last rank's zero plane).
+__device__ __forceinline__ double electric_value(const CowanArgs& a, int c, int i,
+                                                 int j, int k) {
+  const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1), nzc = a.g.nz + (c != 2);
+  double sign = 1.0;
+  if (i < 0) {
+    if (c == 0) i = 0; else { i = -i; sign = -sign; }
+  } else if (i >= nxc) {
+    if (c == 0) i = nxc - 1; else { i = 2 * (nxc - 1) - i; sign = -sign; }
+  }
+  if (j < 0) {
+    if (c == 1) j = 0; else { j = -j; sign = -sign; }
+  } else if (j >= nyc) {
+    if (c == 1) j = nyc - 1; else { j = 2 * (nyc - 1) - j; sign = -sign; }
+  }
+  if (k < 0) return sign * a.lower[c][(size_t)j * nxc + i];
+  if (k >= nzc) return sign * 0.0;
+  return sign * a.e[c][((size_t)ring(k, a.g.zb_e[c], nzc) * nyc + j) * nxc + i];
+}
+
+// smoothedElectric (src/eb_field.cpp:419-486): alpha*centre, then the four
+// beta edge samples, then the four delta corners, in the reference order.
+__device__ __forceinline__ double smoothed(const CowanArgs& a, int c, int d, int i,
+                                           int j, int k) {
+  const int ta = (d + 1) % 3, tb = (d + 2) % 3;
+  const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
+  const int p[3] = {i, j, k};
+  double result = a.alpha[d] * electric_value(a, c, i, j, k);
+  for (int dir = -1; dir <= 1; dir += 2) {
+    int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
+    qa[ta] += dir;
+    qb[tb] += dir;
+    result += a.beta[ta] * electric_value(a, c, qa[0], qa[1], qa[2]);
+    result += a.beta[tb] * electric_value(a, c, qb[0], qb[1], qb[2]);
+  }
+  for (int da = -1; da <= 1; da += 2)
+    for (int db = -1; db <= 1; db += 2) {
+      int q[3] = {p[0], p[1], p[2]};
+      q[ta] += da;
+      q[tb] += db;
+      result += delta * electric_value(a, c, q[0], q[1], q[2]);
+    }
+  return result;
+}
+
+// transformedCorrection (src/eb_cpml.cpp:131-138).
+__device__ __forceinline__ double cpml_correction(const CpmlAxis& ax, int index,
+                                                  double difference, double* history) {
+  const double psi = ax.decay[index] * *history + ax.drive[index] * difference;
+  *history = psi;
+  return ax.inverse_kappa_minus_one[index] * difference + psi;
+}
+
+__device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, int k,
+                                              int zbase, int row_index) {
+  return h.data + ((size_t)slot * h.layers + ring(k, zbase, h.layers)) * h.row + row_index;
+}
+
+// advanceMagneticCowan (src/eb_field.cpp:488-558) fused with
+// EBConvolutionalPML::afterMagneticUpdate (src/eb_cpml.cpp:406-468): each B
+// node is updated by the curl, then by its CPML terms in the reference's
+// term order (0,2,1), (1,2,0), (2,1,0), (2,0,1); the CPML difference is the
+// same smoothed difference the curl used.
+__global__ void cowan_magnetic_kernel(CowanArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const DGrid& g = a.g;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
+  if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
+    const double dEzDy = smoothed(a, 2, 1, i, j + 1, k) - smoothed(a, 2, 1, i, j, k);
+    const double dEyDz = smoothed(a, 1, 2, i, j, k + 1) - smoothed(a, 1, 2, i, j, k);
+    double* bx = &g.b[0][b_index(g, 0, i, j, k)];
+    double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
+    const int s = a.my.ordinal[j];
+    if (s >= 0) {
+      const double corr = cpml_correction(a.my, j, dEzDy,
+                                          history_at(a.h[0], s, k, g.zb_b[0], i));
+      v += -1.0 * dtdy * corr;
+    }
+    *bx = v;
+  }
+  if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
+    const double dExDz = smoothed(a, 0, 2, i, j, k + 1) - smoothed(a, 0, 2, i, j, k);
+    const double dEzDx = smoothed(a, 2, 0, i + 1, j, k) - smoothed(a, 2, 0, i, j, k);
+    double* by = &g.b[1][b_index(g, 1, i, j, k)];
+    double v = *by - (dtdz * dExDz - dtdx * dEzDx);
+    const int s = a.mx.ordinal[i];
+    if (s >= 0) {
+      const double corr = cpml_correction(a.mx, i, dEzDx,
+                                          history_at(a.h[1], s, k, g.zb_b[1], j));
+      v += 1.0 * dtdx * corr;
+    }
+    *by = v;
+  }
+  if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
+    const double dEyDx = smoothed(a, 1, 0, i + 1, j, k) - smoothed(a, 1, 0, i, j, k);
+    const double dExDy = smoothed(a, 0, 1, i, j + 1, k) - smoothed(a, 0, 1, i, j, k);
+    double* bz = &g.b[2][b_index(g, 2, i, j, k)];
+    double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
+    const int sx = a.mx.ordinal[i];
+    if (sx >= 0) {
+      const double corr = cpml_correction(a.mx, i, dEyDx,
+                                          history_at(a.h[2], sx, k, g.zb_b[2], j));
+      v += -1.0 * dtdx * corr;
+    }
+    const int sy = a.my.ordinal[j];
+    if (sy >= 0) {
+      const double corr = cpml_correction(a.my, j, dExDy,
+                                          history_at(a.h[3], sy, k, g.zb_b[2], i));
+      v += 1.0 * dtdy * corr;
+    }
+    *bz = v;
+  }
+}
+
+__device__ __forceinline__ double bval(const DGrid& g, int c, int i, int j, int k) {
+  return g.b[c][b_index(g, c, i, j, k)];
+}
+
+// advanceElectric with J = 0 (src/eb_field.cpp:582-627) followed by the
+// moving-window boundary (src/moving_window_fields.cpp:254-293): the CPML
+// electric terms (src/eb_cpml.cpp:470-539; the convolution histories are
+// advanced here once, exactly as the later commit would advance them from
+// the same B), PEC on the x/y faces, and the inlet Ex/Ey overwrite at k=0.
+// Reads E^n from e_old, writes E* to e_star.
+__global__ void electric_preview_kernel(PreviewArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const DGrid& g = a.g;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  const double curl = g.dt / (kMu0 * kEpsilon0);
+  const double cx = curl / g.dx, cy = curl / g.dy, cz = curl / g.dz;
+  if (i < g.nx) {  // Ex (nx, ny+1, nz+1)
+    const size_t n = e_index(g, 0, i, j, k);
+    double v = g.e_old[0][n];
+    if (k >= 1 && k < g.nz && j >= 1 && j < g.ny)
+      v += cy * (bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k)) -
+           cz * (bval(g, 1, i, j, k) - bval(g, 1, i, j, k - 1));
+    if (j >= 1 && j < g.ny) {
+      const int s = a.ey_prof.ordinal[j];
+      if (s >= 0) {
+        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
+        v += 1.0 * cy * cpml_correction(a.ey_prof, j, diff,
+                                        history_at(a.h[0], s, k, g.zb_e[0], i));
+      }
+    }
+    if (j == 0 || j == g.ny) v = 0.0;
+    if (k == 0) v = inlet_value(a.inlet, 0, i, j);
+    g.e_star[0][n] = v;
+  }
+  if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
+    const size_t n = e_index(g, 1, i, j, k);
+    double v = g.e_old[1][n];
+    if (k >= 1 && k < g.nz && i >= 1 && i < g.nx)
+      v += cz * (bval(g, 0, i, j, k) - bval(g, 0, i, j, k - 1)) -
+           cx * (bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k));
+    if (i >= 1 && i < g.nx) {
+      const int s = a.ex_prof.ordinal[i];
+      if (s >= 0) {
+        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
+        v += -1.0 * cx * cpml_correction(a.ex_prof, i, diff,
+                                         history_at(a.h[1], s, k, g.zb_e[1], j));
+      }
+    }
+    if (i == 0 || i == g.nx) v = 0.0;
+    if (k == 0) v = inlet_value(a.inlet, 1, i, j);
+    g.e_star[1][n] = v;
+  }
+  if (k < g.nz) {  // Ez (nx+1, ny+1, nz)
+    const size_t n = e_index(g, 2, i, j, k);
+    double v = g.e_old[2][n];
+    const bool inner = i >= 1 && i < g.nx && j >= 1 && j < g.ny;
+    if (inner)
+      v += cx * (bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k)) -
+           cy * (bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k));
+    if (inner) {
+      const int sx = a.ex_prof.ordinal[i];
+      if (sx >= 0) {
+        const double diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
+        v += 1.0 * cx * cpml_correction(a.ex_prof, i, diff,
+                                        history_at(a.h[2], sx, k, g.zb_e[2], j));
+      }
+      const int sy = a.ey_prof.ordinal[j];
+      if (sy >= 0) {
+        const double diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
+        v += -1.0 * cy * cpml_correction(a.ey_prof, j, diff,
+                                         history_at(a.h[3], sy, k, g.zb_e[2], i));
+      }
+    }
+    if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
+    g.e_star[2][n] = v;
+  }
+}
+
+// commitConservativeElectric (src/simulation_source_coupling.cpp:61-65): the
+// previewed boundary already holds the committed CPML/PEC/inlet values, so
+// E^{n+1} = E* - dt/eps0 J on the applyCurrentSource mask, in place.
+__global__ void electric_commit_kernel(DGrid g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  for (int c = 0; c < 3; ++c) {
+    if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
+    if (!current_mask(g, c, i, j, k)) continue;
+    const double jc = g.j[c][j_index(g, c, i, j, k)];
+    if (jc != 0.) g.e_star[c][e_index(g, c, i, j, k)] += g.jcoef * jc;
+  }
+}
+
+// Boundary::begin lower halo planes (src/moving_window_fields.cpp:206-210):
+// reference(a, i, j, offset-1, step) for Ex, Ey, Ez.
+__global__ void inlet_lower_kernel(InletPlaneArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  const int nxc = a.nx + (c != 0), nyc = a.ny + (c != 1);
+  if (i >= nxc || j >= nyc) return;
+  a.out[c][(size_t)j * nxc + i] = inlet_value(a.inlet, c, i, j);
+}
+
+// MovingWindowFields::shift plane insertion (src/moving_window_fields.cpp:
+// 470-517) on the ring: after the bases moved down by one, logical plane 0
+// (the dropped upper plane's storage) receives reference(a, i, j, offset,
+// step) for E and B, and every CPML history gets a zero layer at k = 0.
+__global__ void shift_insert_kernel(ShiftArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;  // 0..5 fields, 6..13 histories
+  const DGrid& g = a.g;
+  if (c < 3) {
+    const int nxc = e_nx(g, c), nyc = e_ny(g, c);
+    if (i >= nxc || j >= nyc) return;
+    g.e_old[c][e_index(g, c, i, j, 0)] = inlet_value(a.inlet, c, i, j);
+  } else if (c < 6) {
+    const int b = c - 3;
+    const int nxc = b_nx(g, b), nyc = b_ny(g, b);
+    if (i >= nxc || j >= nyc) return;
+    g.b[b][b_index(g, b, i, j, 0)] = inlet_value(a.inlet, c, i, j);
+  } else {
+    const CpmlHistory& h = a.h[c - 6];
+    // i runs over the row, j over the slots.
+    if (i >= h.row || j >= h.slots) return;
+    *history_at(h, j, 0, a.history_base[c - 6], i) = 0.0;
+  }
+}
+
+// Lab detector field plane (src/lab_detectors.cpp:39-99, 2836-2905).
+__device__ __forceinline__ void interp_axis(double lattice, int size, int* lower,
+                                            double* fraction) {
+  if (lattice <= 0.0) {
+    *lower = 0;
+    *fraction = 0.0;
+  } else if (lattice >= (double)(size - 1)) {
+    *lower = size - 2;
+    *fraction = 1.0;
+  } else {
+    *lower = (int)floor(lattice);
+    *fraction = lattice - (double)*lower;
+  }
+}
+
+__device__ double detector_component(const DGrid& g, int comp, double lx, double ly,
+                                     int zl, double zf) {
+  const bool electric = comp < 3;
+  const int c = comp % 3;
+  const int nxc = electric ? e_nx(g, c) : b_nx(g, c);
+  const int nyc = electric ? e_ny(g, c) : b_ny(g, c);
+  int xl, yl;
+  double xf, yf;
+  interp_axis(lx, nxc, &xl, &xf);
+  interp_axis(ly, nyc, &yl, &yf);
+  double value = 0.0;
+  for (int cz = 0; cz < 2; ++cz) {
+    const double wz = cz ? zf : 1.0 - zf;
+    if (wz == 0.0) continue;
+    for (int b = 0; b < 2; ++b)
+      for (int a = 0; a < 2; ++a) {
+        const double wx = a ? xf : 1.0 - xf;
+        const double wy = b ? yf : 1.0 - yf;
+        const double v = electric ? g.e_old[c][e_index(g, c, xl + a, yl + b, zl + cz)]
+                                  : g.b[c][b_index(g, c, xl + a, yl + b, zl + cz)];
+        value += wx * wy * wz * v;
+      }
+  }
+  return value;
+}
+
+__global__ void detector_plane_kernel(DetectorArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const DGrid& g = a.g;
+  if (i >= g.nx || j >= g.ny) return;
+  const double py = a.origin_xy[1] + ((double)j + 0.5) * g.dy;
+  const double y = (py - a.origin_xy[1]) / g.dy;
+  const double px = a.origin_xy[0] + ((double)i + 0.5) * g.dx;
+  const double x = (px - a.origin_xy[0]) / g.dx;
+  double eb[3], bb[3];
+  eb[0] = detector_component(g, 0, x - 0.5, y, a.vertex_lower, a.vertex_fraction);
+  eb[1] = detector_component(g, 1, x, y - 0.5, a.vertex_lower, a.vertex_fraction);
+  eb[2] = detector_component(g, 2, x, y, a.half_lower, a.half_fraction);
+  bb[0] = detector_component(g, 3, x, y - 0.5, a.half_lower, a.half_fraction);
+  bb[1] = detector_component(g, 4, x - 0.5, y, a.half_lower, a.half_fraction);
+  bb[2] = detector_component(g, 5, x - 0.5, y - 0.5, a.vertex_lower, a.vertex_fraction);
+  // fieldsBoxToLab (src/boostframe.cpp:275-285)
+  const DFrame& f = a.frame;
+  double* o = a.out + 6 * ((size_t)j * g.nx + i);
+  o[0] = fma(f.gamma_beta * kC, bb[1], f.gamma * eb[0]);
+  o[1] = fma(-f.gamma_beta * kC, bb[0], f.gamma * eb[1]);
+  o[2] = eb[2];
+  o[3] = fma(-f.gamma_beta / kC, eb[1], f.gamma * bb[0]);
+  o[4] = fma(f.gamma_beta / kC, eb[0], f.gamma * bb[1]);
+  o[5] = bb[2];
+}
+
+}  // namespace aprl_gpu

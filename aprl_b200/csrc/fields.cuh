@@ -1,0 +1,87 @@
+// fields.cuh -- argument blocks of the grid kernels (fields.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace aprl_gpu {
+
+// One CPML profile axis (makeProfile, src/eb_cpml.cpp:195-248) on device:
+// per native index the coefficients and the history slot (-1 inactive).
+struct CpmlAxis {
+  const double* inverse_kappa_minus_one;
+  const double* decay;
+  const double* drive;
+  const int* ordinal;
+};
+
+// One active convolution history in [slot][k][row] order.
+struct CpmlHistory {
+  double* data;
+  int slots, layers, row;
+};
+
+// The prepared inlet reference sampled at one (k, step): the lerp weights of
+// Simulation::movingWindowFieldValue (src/simulation_moving_window.cpp:
+// 284-293) are the same for every (i, j), so the host evaluates them once.
+struct InletTable {
+  const double* table[6];
+  int nxc[6], nyc[6];
+  int lo[6], hi[6];
+  double fraction;
+};
+
+__device__ __forceinline__ double inlet_value(const InletTable& t, int c, int i, int j) {
+  const size_t plane = (size_t)t.nyc[c] * t.nxc[c];
+  const size_t cell = (size_t)j * t.nxc[c] + i;
+  const double lower = t.table[c][(size_t)t.lo[c] * plane + cell];
+  return t.fraction == 0. ? lower
+                          : (1. - t.fraction) * lower +
+                                t.fraction * t.table[c][(size_t)t.hi[c] * plane + cell];
+}
+
+struct CowanArgs {
+  DGrid g;               // B (ring) is updated in place
+  const double* e[3];    // E^n (ring)
+  const double* lower[3];  // inlet lower halo planes
+  double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
+  CpmlAxis mx, my;       // magnetic profiles (half-integer positions)
+  CpmlHistory h[4];      // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
+};
+
+struct PreviewArgs {
+  DGrid g;               // e_old = E^n, e_star = E* (written)
+  CpmlAxis ex_prof, ey_prof;  // electric profiles (integer positions)
+  CpmlHistory h[4];      // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
+  InletTable inlet;      // reference(a, i, j, offset, step+1)
+};
+
+struct InletPlaneArgs {
+  int nx, ny;
+  double* out[3];
+  InletTable inlet;      // reference(a, i, j, offset-1, step)
+};
+
+struct ShiftArgs {
+  DGrid g;               // e_old = the committed E (ring, bases already moved)
+  InletTable inlet;      // reference(a, i, j, offset, step) after the shift
+  CpmlHistory h[8];      // magnetic 0,3,4,5 then electric 6,9,10,11
+  int history_base[8];
+};
+
+struct DetectorArgs {
+  DGrid g;               // e_old = committed E
+  DFrame frame;
+  double origin_xy[2];
+  int vertex_lower, half_lower;
+  double vertex_fraction, half_fraction;
+  double* out;
+};
+
+__global__ void cowan_magnetic_kernel(CowanArgs a);
+__global__ void electric_preview_kernel(PreviewArgs a);
+__global__ void electric_commit_kernel(DGrid g);
+__global__ void inlet_lower_kernel(InletPlaneArgs a);
+__global__ void shift_insert_kernel(ShiftArgs a);
+__global__ void detector_plane_kernel(DetectorArgs a);
+
+}  // namespace aprl_gpu

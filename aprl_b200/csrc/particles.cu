@@ -1,0 +1,1041 @@
+// particles.cu -- per-particle kernels of the conservative-source step:
+// the wide-shape weights, the orbit-averaged electric gather and the F3 x-z
+// (or trilinear) magnetic gather, the Lapenta-Markidis push with prescribed
+// lab magnets, charge-conserving deposition, particle-boundary events with
+// CPML current carriers, the fixed-point residual, and stable compaction.
+//
+// One thread owns one particle; its gathers and weights run in the
+// reference's visit order, so in FP64 (no FMA contraction) the per-particle
+// arithmetic matches the reference.  Deposition accumulates with FP64
+// atomics into J; only the summation order of J differs from the reference.
+#include "common.cuh"
+#include "particles.cuh"
+
+namespace aprl_gpu {
+
+// ---------------------------------------------------------------------------
+// shapes (src/longitudinal_shape.h:15-117, src/transverse_source_shape.h:8-10)
+__device__ __forceinline__ void node_weights(double f, double w[4]) {
+  w[0] = 0.25 * (1. - f);
+  w[1] = 0.5 - 0.25 * f;
+  w[2] = 0.25 + 0.25 * f;
+  w[3] = 0.25 * f;
+}
+
+struct Basis {
+  long long first;
+  int count;
+  double v[12];
+};
+
+// basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54).
+__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis& r) {
+  const unsigned degree = edge ? 4 : 5;
+  const double cell = floor(z), f = z - cell;
+  double n[6] = {1., 0., 0., 0., 0., 0.};
+  for (unsigned j = 1; j <= degree; ++j) {
+    double saved = 0.;
+    for (unsigned k = 0; k < j; ++k) {
+      const double t = n[k] / j;
+      n[k] = saved + (k + 1 - f) * t;
+      saved = (f + j - k - 1) * t;
+    }
+    n[j] = saved;
+  }
+  const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
+               d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
+  const double c[7] = {-d / 64., b / 16. + 3 * d / 32., -a / 4. - b / 4. - 15 * d / 64.,
+                       1 + a / 2. + 3 * b / 8. + 5 * d / 16.,
+                       -a / 4. - b / 4. - 15 * d / 64., b / 16. + 3 * d / 32., -d / 64.};
+  r.first = (long long)cell - 5;
+  r.count = degree + 7;
+  for (int q = 0; q < 12; ++q) r.v[q] = 0.;
+  for (unsigned j = 0; j <= degree; ++j)
+    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
+}
+
+// binomialXZSegment (src/longitudinal_shape.h:61-94).
+template <class V>
+__device__ __forceinline__ void binomial_xz_segment(const DGrid& g, const double s[3],
+                                                    const double d[3], double first,
+                                                    double last, V& visit) {
+  const double width = last - first;
+  const double mid = (first + last) * 0.5;
+  const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
+  long long i = (long long)floor(x), j = (long long)floor(y);
+  const long long k = (long long)floor(z);
+  if (i == (long long)g.nx) --i;
+  if (j == (long long)g.ny) --j;
+  double wx[4], wz[4];
+  node_weights(x - i, wx);
+  node_weights(z - k, wz);
+  const double wy[2] = {1. - (y - j), y - j};
+  const double edge[3] = {0.25, 0.5, 0.25};
+  const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
+  const double sy[2] = {-1., 1.};
+  const double curvature = width * width / 12.;
+  const double xy = curvature * d[0] * d[1];
+  const double xz = curvature * d[0] * d[2];
+  const double yz = curvature * d[1] * d[2];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) visit(0, i - 1 + a, j + b, k - 1 + c, weight * edge[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+      visit(1, i - 1 + a, j, k - 1 + c, width * (wx[a] * wz[c] + xz * slope[a] * slope[c]));
+  }
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const double weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) visit(2, i - 1 + a, j + b, k - 1 + c, weight * edge[c]);
+    }
+}
+
+// longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
+// smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
+// when the chord exceeds the 64-cut crossing budget.
+template <class V>
+__device__ int shape_weights(const DGrid& g, int shape, const double begin[3],
+                             const double end[3], V& visit) {
+  const double h[3] = {g.dx, g.dy, g.dz};
+  double x[3], v[3], cuts[64];
+  int count = 2;
+  cuts[0] = 0.;
+  cuts[1] = 1.;
+  for (int a = 0; a < 3; ++a) {
+    x[a] = (begin[a] - g.origin[a]) / h[a];
+    v[a] = (end[a] - begin[a]) / h[a];
+    if (v[a] != 0.)
+      for (long long j = (long long)floor(fmin(x[a], x[a] + v[a])) + 1;
+           j < fmax(x[a], x[a] + v[a]); ++j) {
+        if (count == 64) return -1;
+        cuts[count++] = (j - x[a]) / v[a];
+      }
+  }
+  // insertion sort (the cut count is tiny)
+  for (int s = 1; s < count; ++s) {
+    const double key = cuts[s];
+    int t = s - 1;
+    while (t >= 0 && cuts[t] > key) {
+      cuts[t + 1] = cuts[t];
+      --t;
+    }
+    cuts[t + 1] = key;
+  }
+  int segments = 0;
+  for (int s = 1; s < count; ++s) {
+    const double width = cuts[s] - cuts[s - 1];
+    if (width <= 0.) continue;
+    ++segments;
+    if (shape == 0) {
+      binomial_xz_segment(g, x, v, cuts[s - 1], cuts[s], visit);
+      continue;
+    }
+    const double q[4] = {-.8611363115940525752, -.3399810435848562648,
+                         .3399810435848562648, .8611363115940525752};
+    const double qw[4] = {.3478548451374538574, .6521451548625461426,
+                          .6521451548625461426, .3478548451374538574};
+    for (int t = 0; t < 4; ++t) {
+      const double u = .5 * (cuts[s] + cuts[s - 1] + width * q[t]),
+                   factor = .5 * width * qw[t], xx = x[0] + u * v[0],
+                   yy = x[1] + u * v[1], zz = x[2] + u * v[2];
+      long long i = (long long)floor(xx), j = (long long)floor(yy);
+      if (i == (long long)g.nx) --i;
+      if (j == (long long)g.ny) --j;
+      const double fx = xx - i, fy = yy - j;
+      Basis nodes, edge;
+      quintic_basis(zz, false, nodes);
+      quintic_basis(zz, true, edge);
+      for (int k = 0; k < nodes.count; ++k) {
+        const double w = factor * nodes.v[k];
+        if (w == 0.) continue;
+        for (int b = 0; b < 2; ++b) visit(0, i, j + b, nodes.first + k, w * (b ? fy : 1. - fy));
+        for (int a = 0; a < 2; ++a) visit(1, i + a, j, nodes.first + k, w * (a ? fx : 1. - fx));
+      }
+      for (int k = 0; k < edge.count; ++k) {
+        const double w = factor * edge.v[k];
+        if (w == 0.) continue;
+        for (int b = 0; b < 2; ++b)
+          for (int a = 0; a < 2; ++a)
+            visit(2, i + a, j + b, edge.first + k, w * (a ? fx : 1. - fx) * (b ? fy : 1. - fy));
+      }
+    }
+  }
+  return segments;
+}
+
+// ---------------------------------------------------------------------------
+// gathers (src/source_coupling.cpp:31-51, src/source_coupling_math.h:122-250)
+struct OpenOrbit {
+  double first, last;
+  double begin[3], end[3];
+  bool valid;
+};
+
+// clipOpenOrbit at one rank (src/source_coupling_math.h:234-250).
+__device__ __forceinline__ bool clip_open_orbit(const DGrid& g, const double b[3],
+                                                const double e[3], OpenOrbit& o) {
+  const double ds[3] = {g.dx, g.dy, g.dz};
+  const double size[3] = {(double)g.nx, (double)g.ny, (double)g.nz};
+  o.first = 0.;
+  o.last = 1.;
+  o.valid = true;
+  for (int a = 0; a < 3; ++a) {
+    o.begin[a] = b[a];
+    o.end[a] = e[a];
+  }
+  for (int a = 0; a < 3; ++a) {
+    const double x = (b[a] - g.origin[a]) / ds[a], d = (e[a] - b[a]) / ds[a];
+    if (!isfinite(x) || !isfinite(d)) return false;
+    if (d == 0.) {
+      if (x < 0. || x > size[a]) o.valid = false;
+      continue;
+    }
+    {
+      const double t = -x / d;
+      if (d > 0.) o.first = fmax(o.first, t);
+      else o.last = fmin(o.last, t);
+    }
+    {
+      const double t = (size[a] - x) / d;
+      if (d > 0.) o.last = fmin(o.last, t);
+      else o.first = fmax(o.first, t);
+    }
+  }
+  o.valid = o.valid && o.last >= o.first;
+  if (o.valid)
+    for (int a = 0; a < 3; ++a) {
+      const double d = e[a] - b[a];
+      if (o.first != 0.) o.begin[a] = b[a] + o.first * d;
+      if (o.last != 1.) o.end[a] = b[a] + o.last * d;
+    }
+  return true;
+}
+
+// Orbit average of 1/2 (E_new + E^n) with the shape weights.  with_current
+// selects E_new = E* - dt/eps0 J (residual) or E* (first-trial guess, when
+// the grid still holds the zero-current preview).
+struct ElectricVisitor {
+  const DGrid* g;
+  bool with_current;
+  double r[3];
+  __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k,
+                                             double w) {
+    const DGrid& G = *g;
+    if (i < 0 || j < 0 || i >= e_nx(G, d) || j >= e_ny(G, d)) return;
+    if (k < 0 || k >= e_nz(G, d)) return;
+    const int ii = (int)i, jj = (int)j, kk = (int)k;
+    const size_t n = e_index(G, d, ii, jj, kk);
+    const double vn = with_current ? e_candidate(G, d, ii, jj, kk) : G.e_star[d][n];
+    r[d] += .5 * w * (vn + G.e_old[d][n]);
+  }
+};
+
+__device__ __forceinline__ double open_b(const DGrid& g, int a, long long i, long long j,
+                                         long long k) {
+  const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
+  if (i < 0) i = 0;
+  if (i > nxc - 1) i = nxc - 1;
+  if (j < 0) j = 0;
+  if (j > nyc - 1) j = nyc - 1;
+  if (k < 0) k = 0;
+  if (k >= nzc) k = nzc - 1;
+  return g.b[a][b_index(g, a, (int)i, (int)j, (int)k)];
+}
+
+// binomialXZMagneticSample (src/source_coupling_math.h:142-167).
+__device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const double p[3],
+                                                     double value[3]) {
+  const double h[3] = {g.dx, g.dy, g.dz};
+  for (int a = 0; a < 3; ++a) {
+    long long cell[3];
+    double fraction[3];
+    for (int d = 0; d < 3; ++d) {
+      const double pos = (p[d] - g.origin[d]) / h[d] - (a == d ? 0. : 0.5);
+      cell[d] = (long long)floor(pos);
+      fraction[d] = pos - cell[d];
+    }
+    double wx[4], wz[4];
+    node_weights(fraction[0], wx);
+    node_weights(fraction[2], wz);
+    const double wy[2] = {1. - fraction[1], fraction[1]};
+    double v = 0.;
+    for (int k = 0; k < 4; ++k)
+      for (int j = 0; j < 2; ++j) {
+        double row = 0.;
+        for (int i = 0; i < 4; ++i)
+          row += wx[i] * open_b(g, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
+        v += wz[k] * wy[j] * row;
+      }
+    value[a] = v;
+  }
+}
+
+// magneticSample(bounds=false, halo, openFaces=true) (src/source_coupling_math.h:122-138).
+__device__ __forceinline__ void trilinear_magnetic(const DGrid& g, const double p[3],
+                                                   double value[3]) {
+  const double ds[3] = {g.dx, g.dy, g.dz};
+  int cell[2][3];
+  double fraction[2][3];
+  for (int half = 0; half < 2; ++half)
+    for (int d = 0; d < 3; ++d) {
+      const double x = (p[d] - g.origin[d]) / ds[d] - .5 * half;
+      cell[half][d] = (int)floor(x);
+      fraction[half][d] = x - cell[half][d];
+    }
+  for (int axis = 0; axis < 3; ++axis) {
+    const int hx = axis == 0 ? 0 : 1, hy = axis == 1 ? 0 : 1, hz = axis == 2 ? 0 : 1;
+    double v = 0.;
+    for (int k = 0; k < 2; ++k)
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+          const double x = i ? fraction[hx][0] : 1 - fraction[hx][0],
+                       y = j ? fraction[hy][1] : 1 - fraction[hy][1],
+                       z = k ? fraction[hz][2] : 1 - fraction[hz][2];
+          v += x * y * z *
+               open_b(g, axis, cell[hx][0] + i, cell[hy][1] + j, cell[hz][2] + k);
+        }
+    value[axis] = v;
+  }
+}
+
+// Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
+__device__ __forceinline__ unsigned gather_electric(const DGrid& g, int shape,
+                                                    const double a[3], const double b[3],
+                                                    bool with_current, double out[3]) {
+  OpenOrbit path;
+  if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
+  if (!path.valid) return kErrOrbitOutside;
+  ElectricVisitor v{&g, with_current, {0., 0., 0.}};
+  if (shape_weights(g, shape, path.begin, path.end, v) < 0) return kErrCrossingBudget;
+  const double fraction = path.last - path.first;
+  for (int d = 0; d < 3; ++d) out[d] = v.r[d] * fraction;
+  return kErrNone;
+}
+
+// Impl::magnetic (src/source_coupling.cpp:40-51).
+__device__ __forceinline__ unsigned gather_magnetic(const DGrid& g, int shape,
+                                                    const double a[3], const double b[3],
+                                                    double out[3]) {
+  OpenOrbit path;
+  if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
+  if (!path.valid) return kErrOrbitOutside;
+  double middle[3];
+  for (int d = 0; d < 3; ++d) middle[d] = (path.begin[d] + path.end[d]) * .5;
+  if (shape == 0)
+    binomial_xz_magnetic(g, middle, out);
+  else
+    trilinear_magnetic(g, middle, out);
+  return kErrNone;
+}
+
+// ---------------------------------------------------------------------------
+// deposition: Current::deposit at one rank (src/longitudinal_shape.h:175-187)
+struct DepositVisitor {
+  const DGrid* g;
+  double scale[3];
+  bool smooth_x;
+  unsigned error;
+  __device__ __forceinline__ void operator()(int a, long long i, long long j, long long k,
+                                             double w) {
+    if (scale[a] == 0.) return;
+    const DGrid& G = *g;
+    if (i < 0 || i >= e_nx(G, a)) {
+      if (!smooth_x) error = kErrSupportX;
+      return;
+    }
+    if (j < 0 || j >= e_ny(G, a)) {
+      error = kErrSupportY;
+      return;
+    }
+    if (k < 0 || k >= e_nz(G, a)) return;
+    atomicAdd(&G.j[a][j_index(G, a, (int)i, (int)j, (int)k)], scale[a] * w);
+  }
+};
+
+// ChargeConservingCurrentDepositor::depositSegment (src/eb_deposition.cpp:41-51,
+// validatePosition 228-246).
+__device__ unsigned deposit_segment(const DGrid& g, int shape, const double b[3],
+                                    const double e[3], double charge) {
+  const double extent[3] = {(double)g.nx * g.dx, (double)g.ny * g.dy, (double)g.nz * g.dz};
+  for (int a = 0; a < 3; ++a) {
+    const double tol = 64.0 * kEpsilon * fmax(1.0, fmax(fabs(g.origin[a]), extent[a]));
+    const double rb = b[a] - g.origin[a], re = e[a] - g.origin[a];
+    if (!isfinite(b[a]) || rb < -tol || rb > extent[a] + tol) return kErrDepositOutside;
+    if (!isfinite(e[a]) || re < -tol || re > extent[a] + tol) return kErrDepositOutside;
+  }
+  if (!isfinite(charge)) return kErrNonFinite;
+  DepositVisitor v;
+  v.g = &g;
+  v.smooth_x = shape == 0;
+  v.error = kErrNone;
+  for (int a = 0; a < 3; ++a)
+    v.scale[a] = charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt);
+  if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
+  return v.error;
+}
+
+// ---------------------------------------------------------------------------
+// push (src/source_coupling_math.h:272-293, src/source_coupling.cpp:90-104)
+
+// source_coupling_math::momentum.  Returns 0 or an error code.
+__device__ unsigned momentum(double u[3], const double e[3], const double mag[3],
+                             double q, double m, double h, double g0) {
+  const double before[3] = {u[0], u[1], u[2]};
+  const double ks = q * h / (2 * m * kC);
+  const double bs = q * h / (2 * m);
+  double kick[3], b[3], a[3], axb[3];
+  for (int i = 0; i < 3; ++i) {
+    kick[i] = e[i] * ks;
+    b[i] = mag[i] * bs;
+  }
+  for (int i = 0; i < 3; ++i) a[i] = before[i] + kick[i];
+  axb[0] = a[1] * b[2] - a[2] * b[1];
+  axb[1] = a[2] * b[0] - a[0] * b[2];
+  axb[2] = a[0] * b[1] - a[1] * b[0];
+  const double b2 = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+  const double ka = kick[0] * a[0] + kick[1] * a[1] + kick[2] * a[2];
+  const double kb = kick[0] * b[0] + kick[1] * b[1] + kick[2] * b[2];
+  const double ab = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+  const double kcross = kick[0] * axb[0] + kick[1] * axb[1] + kick[2] * axb[2];
+  const double first = (kick[0] * before[0] + kick[1] * before[1] + kick[2] * before[2]) / g0;
+  const double kk = kick[0] * kick[0] + kick[1] * kick[1] + kick[2] * kick[2];
+  double G = g0 + first + (kk + kcross / g0 - first * first) / g0;
+  G = fmax(G, .5 * (g0 + 1.));
+  int iteration = 0;
+  for (; iteration < 12; ++iteration) {
+    const double den = G * G + b2, numerator = G * G * ka + G * kcross + ab * kb;
+    const double f = G * (G - g0) - numerator / den;
+    const double derivative =
+        2 * G - g0 - ((2 * G * ka + kcross) * den - 2 * G * numerator) / (den * den);
+    const double correction = f / derivative;
+    const double next = G - correction;
+    if (!isfinite(next) || next < .5 * (g0 + 1.) - 1e-13) return kErrRootNonphysical;
+    G = fmax(next, .5 * (g0 + 1.));
+    if (fabs(correction) <= 8 * kEpsilon * fmax(1., G)) break;
+  }
+  if (iteration == 12) return kErrRootNoConvergence;
+  const double den = G * G + b2;
+  for (int k = 0; k < 3; ++k) u[k] = 2 * (G * G * a[k] + ab * b[k] + G * axb[k]) / den - before[k];
+  return kErrNone;
+}
+
+// SIMagneticElement::fieldsLab, magnetic part (src/eb_sources.cpp:352-447).
+__device__ void magnet_lab(const DMagnet& m, const double pos[3], double b[3]) {
+  b[0] = b[1] = b[2] = 0.0;
+  const double rel[3] = {pos[0] - m.center[0], pos[1] - m.center[1], pos[2] - m.center[2]};
+  const double z = rel[2];
+  if (m.type == 2) {
+    if (z >= 0.0 && z <= m.length) {
+      const double x = rel[0] * m.cos_angle + rel[1] * m.sin_angle;
+      const double y = -rel[0] * m.sin_angle + rel[1] * m.cos_angle;
+      const double bx = m.quadrupole_gradient * y, by = m.quadrupole_gradient * x;
+      b[0] = bx * m.cos_angle - by * m.sin_angle;
+      b[1] = bx * m.sin_angle + by * m.cos_angle;
+    }
+    return;
+  }
+  if (m.type == 1) {
+    if (z >= 0.0 && z <= m.length) {
+      b[0] = m.peak_field * m.cos_angle;
+      b[1] = m.peak_field * m.sin_angle;
+    }
+    return;
+  }
+  const double k = m.wave_number;
+  double ts = 0.0, ls = 0.0;
+  if (z >= 0.0 && z <= m.length) {
+    ts = sin(k * z);
+    ls = cos(k * z);
+  } else if (m.gaussian_fringe) {
+    const double fc = z < 0.0 ? z : z - m.length;
+    const double distance = fabs(fc);
+    if (distance >= m.fringe_extent) return;
+    const double q = distance / m.fringe_extent;
+    const double q2 = q * q, q3 = q2 * q, q4 = q3 * q, q5 = q4 * q;
+    const double taper = 1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5;
+    const double taper_derivative = (-30.0 * q2 + 60.0 * q3 - 30.0 * q4) / m.fringe_extent;
+    const double gaussian = exp(-0.5 * pow(k * distance, 2.0));
+    ls = gaussian * taper;
+    const double dbd = gaussian * (taper_derivative - k * k * distance * taper);
+    ts = z < 0.0 ? dbd / k : -dbd / k;
+  } else {
+    return;
+  }
+  const double tc = rel[0] * m.cos_angle + rel[1] * m.sin_angle;
+  const double tf = m.peak_field * cosh(k * tc) * ts;
+  b[0] = tf * m.cos_angle;
+  b[1] = tf * m.sin_angle;
+  b[2] = m.peak_field * sinh(k * tc) * ls;
+}
+
+// SIFieldSourceSet::addPrescribedBox (src/eb_sources.cpp:537-582) with lab
+// magnets only: box event -> lab event, sum of magnets, lab -> box fields.
+__device__ void add_prescribed_box(const PushArgs& a, const double pos[3], double t_box,
+                                   double e[3], double b[3]) {
+  if (a.n_magnets == 0) return;
+  const DFrame& f = a.frame;
+  const double z_shift = pos[2] - f.box_z_origin;
+  const double pos_lab[3] = {pos[0], pos[1],
+                             f.lab_z_origin + fma(f.gamma_beta * kC, t_box, f.gamma * z_shift)};
+  double bl[3] = {0., 0., 0.};
+  for (int n = 0; n < a.n_magnets; ++n) {
+    double c[3];
+    magnet_lab(a.magnets[n], pos_lab, c);
+    for (int d = 0; d < 3; ++d) bl[d] += c[d];
+  }
+  // fieldsLabToBox with zero lab E (src/boostframe.cpp:262-273)
+  const double el[3] = {0., 0., 0.};
+  const double ebx[3] = {fma(-f.gamma_beta * kC, bl[1], f.gamma * el[0]),
+                         fma(f.gamma_beta * kC, bl[0], f.gamma * el[1]), el[2]};
+  const double bbx[3] = {fma(f.gamma_beta / kC, el[1], f.gamma * bl[0]),
+                         fma(-f.gamma_beta / kC, el[0], f.gamma * bl[1]), bl[2]};
+  for (int d = 0; d < 3; ++d) {
+    e[d] += ebx[d];
+    b[d] += bbx[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// particle boundaries (src/particle_boundary.cpp)
+struct Hit {
+  double position[3];
+  double fraction;
+  int face;
+};
+
+// ParticleCPMLRegion::firstEntry (src/particle_boundary.cpp:104-174).
+__device__ unsigned cpml_first_entry(const DRegion& r, const double s[3], const double e[3],
+                                     Hit& hit, bool& entered) {
+  double best = INFINITY;
+  int best_face = 0;
+  entered = false;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!isfinite(s[axis]) || !isfinite(e[axis])) return kErrNonFinite;
+    if (s[axis] < r.physical_lower[axis] - r.tolerance[axis] ||
+        s[axis] > r.physical_upper[axis] + r.tolerance[axis])
+      return kErrStartInCpml;
+    if (r.cells[axis] == 0) continue;
+    double candidate = 0.0;
+    int face = 0;
+    bool h = false;
+    if (e[axis] < r.physical_lower[axis]) {
+      candidate = (r.physical_lower[axis] - s[axis]) / (e[axis] - s[axis]);
+      face = 2 * axis;
+      h = true;
+    } else if (e[axis] > r.physical_upper[axis]) {
+      candidate = (r.physical_upper[axis] - s[axis]) / (e[axis] - s[axis]);
+      face = 2 * axis + 1;
+      h = true;
+    }
+    if (h && candidate < best) {
+      best = candidate;
+      best_face = face;
+      entered = true;
+    }
+  }
+  if (!entered) return kErrNone;
+  const double ft = 64.0 * kEpsilon;
+  if (!isfinite(best) || best < -ft || best > 1.0 + ft) return kErrHitLocate;
+  hit.fraction = fmax(0.0, fmin(1.0, best));
+  hit.face = best_face;
+  for (int a = 0; a < 3; ++a) {
+    hit.position[a] = s[a] + hit.fraction * (e[a] - s[a]);
+    hit.position[a] = fmax(r.outer_lower[a], fmin(r.outer_upper[a], hit.position[a]));
+  }
+  const int normal = best_face / 2;
+  hit.position[normal] = (best_face % 2) ? r.physical_upper[normal] : r.physical_lower[normal];
+  return kErrNone;
+}
+
+// ParticleOpenBoundary::firstExit (src/particle_boundary.cpp:303-373).
+__device__ unsigned outer_first_exit(const DRegion& r, const double s[3], const double e[3],
+                                     Hit& hit, bool& escaped) {
+  double best = INFINITY;
+  int best_face = 0;
+  escaped = false;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!isfinite(s[axis]) || !isfinite(e[axis])) return kErrNonFinite;
+    if (s[axis] < r.global_lower[axis] - r.global_tolerance[axis] ||
+        s[axis] > r.global_upper[axis] + r.global_tolerance[axis])
+      return kErrStartOutside;
+    double candidate = 0.0;
+    int face = 0;
+    bool h = false;
+    if (e[axis] < r.global_lower[axis]) {
+      candidate = (r.global_lower[axis] - s[axis]) / (e[axis] - s[axis]);
+      face = 2 * axis;
+      h = true;
+    } else if (e[axis] > r.global_upper[axis]) {
+      candidate = (r.global_upper[axis] - s[axis]) / (e[axis] - s[axis]);
+      face = 2 * axis + 1;
+      h = true;
+    }
+    if (h && candidate < best) {
+      best = candidate;
+      best_face = face;
+      escaped = true;
+    }
+  }
+  if (!escaped) return kErrNone;
+  const double ft = 64.0 * kEpsilon;
+  if (best < -ft || best > 1.0 + ft || !isfinite(best)) return kErrHitLocate;
+  hit.fraction = fmax(0.0, fmin(1.0, best));
+  hit.face = best_face;
+  for (int a = 0; a < 3; ++a) {
+    hit.position[a] = s[a] + hit.fraction * (e[a] - s[a]);
+    hit.position[a] = fmax(r.global_lower[a], fmin(r.global_upper[a], hit.position[a]));
+  }
+  const int normal = best_face / 2;
+  hit.position[normal] = (best_face % 2) ? r.global_upper[normal] : r.global_lower[normal];
+  return kErrNone;
+}
+
+// ParticleCPMLRegion::conductivityRate / currentDampingFactor
+// (src/particle_boundary.cpp:176-240).
+__device__ double conductivity_rate(const DRegion& r, const double p[3]) {
+  double rate = 0.0;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (r.cells[axis] == 0) continue;
+    double depth = 0.0;
+    if (p[axis] < r.physical_lower[axis])
+      depth = (r.physical_lower[axis] - p[axis]) / r.thickness[axis];
+    else if (p[axis] > r.physical_upper[axis])
+      depth = (p[axis] - r.physical_upper[axis]) / r.thickness[axis];
+    depth = fmax(0.0, fmin(1.0, depth));
+    rate += r.max_rate[axis] * pow(depth, r.order);
+  }
+  return rate;
+}
+
+__device__ double damping_factor(const DRegion& r, const double s[3], const double e[3],
+                                 double duration) {
+  if (duration == 0.0) return 1.0;
+  const double abscissa = sqrt(3.0 / 5.0);
+  const double node[3] = {0.5 * (1.0 - abscissa), 0.5, 0.5 * (1.0 + abscissa)};
+  const double weight[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
+  double average = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    double p[3];
+    for (int a = 0; a < 3; ++a) p[a] = s[a] + node[k] * (e[a] - s[a]);
+    average += weight[k] * conductivity_rate(r, p);
+  }
+  const double exponent = -duration * average;
+  return exponent < log(kDblMin) ? 0.0 : exp(exponent);
+}
+
+struct CarrierState {
+  double pos[3], vel[3], q, w;
+};
+
+// processCarrierSegment at one rank (src/simulation.cpp:4310-4407).
+// Returns an error code; *kept tells whether the carrier survives.
+__device__ unsigned carrier_segment(const DGrid& g, int shape, const DRegion& r,
+                                    CarrierState& c, const double seg_start[3],
+                                    double seg_start_fraction, TrialCounters* counters,
+                                    bool& kept) {
+  const double cutoff = 64.0 * kEpsilon;
+  kept = false;
+  if (!(c.w >= 0.0) || !isfinite(c.w)) return kErrCarrierWeight;
+  if (c.w <= cutoff) return kErrNone;
+  Hit outer;
+  bool exits = false;
+  unsigned err = outer_first_exit(r, seg_start, c.pos, outer, exits);
+  if (err) return err;
+  double local_end = 1.0;
+  double seg_end[3] = {c.pos[0], c.pos[1], c.pos[2]};
+  if (exits) {
+    local_end = outer.fraction;
+    for (int a = 0; a < 3; ++a) seg_end[a] = outer.position[a];
+  }
+  const double global_end = seg_start_fraction + local_end * (1.0 - seg_start_fraction);
+  const double duration = (global_end - seg_start_fraction) * g.dt;
+  double midpoint[3];
+  for (int a = 0; a < 3; ++a) midpoint[a] = 0.5 * (seg_start[a] + seg_end[a]);
+  const double mid_damping = damping_factor(r, seg_start, midpoint, 0.5 * duration);
+  const double end_damping = damping_factor(r, seg_start, seg_end, duration);
+  const double deposited = c.w * mid_damping;
+  const double end_weight = c.w * end_damping;
+  err = deposit_segment(g, shape, seg_start, seg_end, c.q * deposited);
+  if (err) return err;
+  if (exits) {
+    atomicAdd(&counters->carrier_outer[outer.face], 1ull);
+    atomicAdd(&counters->carrier_outer_charge[outer.face], c.q * end_weight);
+    return kErrNone;
+  }
+  if (end_weight <= cutoff) return kErrNone;
+  c.w = end_weight;
+  for (int a = 0; a < 3; ++a) c.pos[a] = seg_end[a];
+  kept = true;
+  return kErrNone;
+}
+
+// ---------------------------------------------------------------------------
+// Existing CPML carriers: ballistic step, damped deposit, outer exit
+// (src/simulation.cpp:4531-4537).  Carriers deposit with the run's shape,
+// like every ChargeConservingCurrentDepositor call.
+__global__ void carrier_kernel(CarrierArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.count) return;
+  CarrierState c;
+  c.pos[0] = a.in.px[n]; c.pos[1] = a.in.py[n]; c.pos[2] = a.in.pz[n];
+  c.vel[0] = a.in.vx[n]; c.vel[1] = a.in.vy[n]; c.vel[2] = a.in.vz[n];
+  c.q = a.in.q[n];
+  c.w = a.in.w[n];
+  const double start[3] = {c.pos[0], c.pos[1], c.pos[2]};
+  for (int d = 0; d < 3; ++d) c.pos[d] += a.g.dt * c.vel[d];
+  bool kept = false;
+  const unsigned err = carrier_segment(a.g, a.shape, a.region, c, start, 0.0, a.counters, kept);
+  if (err) raise_error(a.status, err, (unsigned long long)n);
+  a.keep[n] = kept ? 1 : 0;
+  a.out.px[n] = c.pos[0]; a.out.py[n] = c.pos[1]; a.out.pz[n] = c.pos[2];
+  a.out.vx[n] = c.vel[0]; a.out.vy[n] = c.vel[1]; a.out.vz[n] = c.vel[2];
+  a.out.q[n] = c.q;
+  a.out.w[n] = c.w;
+}
+
+// One fixed-point trial of one active particle: ConservativeSourceCoupling::
+// push (src/source_coupling.cpp:90-104) from the step-start state, then the
+// boundary events and deposition of processActiveSegment
+// (src/simulation.cpp:4760-4917) with Simulation::firstMovingWindowEntry
+// (src/simulation_moving_window.cpp:380-395).
+__global__ void push_deposit_kernel(PushArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.count) return;
+  const DGrid& g = a.g;
+  const double dt = g.dt;
+  double pos[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
+  double u[3] = {a.p.ux[n], a.p.uy[n], a.p.uz[n]};
+  const double q = a.p.q[n], m = a.p.m[n];
+  const double start[3] = {pos[0], pos[1], pos[2]};
+  unsigned err = kErrNone;
+  if (start[2] < g.origin[2]) err = kErrUpstream;
+  double used_e[3], used_b[3];
+  if (!err) {
+    if (a.first_trial) {
+      const double gamma = gamma_u(u[0], u[1], u[2]);
+      const double s = dt * kC / gamma;
+      const double guess[3] = {pos[0] + s * u[0], pos[1] + s * u[1], pos[2] + s * u[2]};
+      err = gather_electric(g, a.shape, pos, guess, false, used_e);
+      if (!err) err = gather_magnetic(g, a.shape, pos, guess, used_b);
+    } else {
+      for (int d = 0; d < 3; ++d) {
+        used_e[d] = a.next_e[3 * n + d];
+        used_b[d] = a.next_b[3 * n + d];
+      }
+    }
+  }
+  double abs_work = 0.0;
+  if (!err) {
+    const double h = dt / a.substeps;
+    for (int s = 0; s < a.substeps && !err; ++s) {
+      const double before_pos[3] = {pos[0], pos[1], pos[2]};
+      const double before_u[3] = {u[0], u[1], u[2]};
+      const double g0 = gamma_u(u[0], u[1], u[2]);
+      const double ps = .5 * h * kC / g0;
+      const double point[3] = {pos[0] + ps * u[0], pos[1] + ps * u[1], pos[2] + ps * u[2]};
+      double ee[3] = {0., 0., 0.}, bb[3] = {0., 0., 0.};
+      add_prescribed_box(a, point, a.time + (s + .5) * h, ee, bb);
+      double e[3], b[3];
+      for (int d = 0; d < 3; ++d) {
+        e[d] = used_e[d] + ee[d];
+        b[d] = used_b[d] + bb[d];
+      }
+      err = momentum(u, e, b, q, m, h, g0);
+      if (err) break;
+      const double g1 = gamma_u(u[0], u[1], u[2]);
+      const double xs = h * kC / (g0 + g1);
+      for (int d = 0; d < 3; ++d) pos[d] += xs * (before_u[d] + u[d]);
+      // |BorisWork::gridWork| of this substep (chargeWork, evaluated in
+      // binary64 here; the reference keeps long double).
+      double w = 0.0;
+      for (int d = 0; d < 3; ++d) w += q * used_e[d] * (pos[d] - before_pos[d]);
+      abs_work += fabs(w);
+    }
+  }
+  unsigned char action = 0;
+  bool born_kept = false;
+  CarrierState born;
+  if (!err) {
+    // firstMovingWindowEntry = CPML first entry + fixed-lab exit plane
+    Hit cpml_hit, outer_hit;
+    bool enters = false, exits = false;
+    err = cpml_first_entry(a.region, start, pos, cpml_hit, enters);
+    if (!err) {
+      const double za = lab_z_from_box_zt(a.frame, start[2], a.time + 0.0 * dt) - a.exit_lab_z;
+      const double zb = lab_z_from_box_zt(a.frame, pos[2], a.time + dt) - a.exit_lab_z;
+      if (za >= 0.) err = kErrBeyondExit;
+      else if (zb >= 0. && zb > za) {
+        const double fraction = -za / (zb - za);
+        if (!enters || fraction < cpml_hit.fraction) {
+          for (int d = 0; d < 3; ++d) cpml_hit.position[d] = start[d] + fraction * (pos[d] - start[d]);
+          cpml_hit.fraction = fraction;
+          cpml_hit.face = 5;
+          enters = true;
+        }
+      }
+    }
+    if (!err) err = outer_first_exit(a.region, start, pos, outer_hit, exits);
+    if (!err) {
+      const double crossing = 64.0 * kEpsilon;
+      double seg_end[3] = {pos[0], pos[1], pos[2]};
+      double local_end = 1.0;
+      Hit selected;
+      if (enters && (!exits || cpml_hit.fraction <= outer_hit.fraction + crossing)) {
+        action = 1;
+        selected = cpml_hit;
+      } else if (exits) {
+        action = 2;
+        selected = outer_hit;
+      }
+      if (action) {
+        local_end = selected.fraction;
+        for (int d = 0; d < 3; ++d) seg_end[d] = selected.position[d];
+      }
+      err = deposit_segment(g, a.shape, start, seg_end, q);
+      const double global_end = 0.0 + local_end * (1.0 - 0.0);
+      if (!err && action == 1) {
+        if (selected.face == 5) {
+          atomicAdd(&a.counters->exits, 1ull);
+          atomicAdd(&a.counters->exit_charge, q);
+        } else {
+          atomicAdd(&a.counters->cpml[selected.face], 1ull);
+          atomicAdd(&a.counters->cpml_charge[selected.face], q);
+        }
+        for (int d = 0; d < 3; ++d) born.pos[d] = pos[d];
+        const double gamma = gamma_u(u[0], u[1], u[2]);
+        const double sv = kC / gamma;
+        for (int d = 0; d < 3; ++d) born.vel[d] = u[d] * sv;
+        born.q = q;
+        born.w = 1.0;
+        err = carrier_segment(g, a.shape, a.region, born, selected.position, global_end,
+                              a.counters, born_kept);
+      } else if (!err && action == 2) {
+        atomicAdd(&a.counters->direct[selected.face], 1ull);
+        atomicAdd(&a.counters->direct_charge[selected.face], q);
+      }
+    }
+  }
+  if (err) raise_error(a.status, err, (unsigned long long)n);
+  a.x1[n] = pos[0]; a.y1[n] = pos[1]; a.z1[n] = pos[2];
+  a.ux1[n] = u[0]; a.uy1[n] = u[1]; a.uz1[n] = u[2];
+  for (int d = 0; d < 3; ++d) {
+    a.used_e[3 * n + d] = used_e[d];
+    a.used_b[3 * n + d] = used_b[d];
+  }
+  a.abs_grid_work[n] = abs_work;
+  a.action[n] = action;
+  a.born_keep[n] = born_kept ? 1 : 0;
+  if (born_kept) {
+    a.born.px[n] = born.pos[0]; a.born.py[n] = born.pos[1]; a.born.pz[n] = born.pos[2];
+    a.born.vx[n] = born.vel[0]; a.born.vy[n] = born.vel[1]; a.born.vz[n] = born.vel[2];
+    a.born.q[n] = born.q;
+    a.born.w[n] = born.w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ConservativeSourceCoupling::localResidual (src/source_coupling.cpp:105-159):
+// re-gather along the actual chord, then force = max, defect and scale =
+// sums.  Block reduction with warp shuffles, one atomic per block.
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void residual_kernel(ResidualArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double force = 0.0, defect = 0.0, scale = 0.0;
+  if (n < a.count) {
+    const double first[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
+    const double last[3] = {a.x1[n], a.y1[n], a.z1[n]};
+    double ne[3], nb[3];
+    unsigned err = gather_electric(a.g, a.shape, first, last, true, ne);
+    if (!err) err = gather_magnetic(a.g, a.shape, first, last, nb);
+    if (err) {
+      raise_error(a.status, err, (unsigned long long)n);
+      for (int d = 0; d < 3; ++d) ne[d] = nb[d] = 0.0;
+    }
+    double de[3], db[3];
+    for (int d = 0; d < 3; ++d) {
+      a.next_e[3 * n + d] = ne[d];
+      a.next_b[3 * n + d] = nb[d];
+      de[d] = ne[d] - a.used_e[3 * n + d];
+      db[d] = nb[d] - a.used_b[3 * n + d];
+    }
+    const double q = a.p.q[n], m = a.p.m[n];
+    force = fabs(q / m) * a.g.dt / kC *
+            (sqrt(de[0] * de[0] + de[1] * de[1] + de[2] * de[2]) +
+             kC * sqrt(db[0] * db[0] + db[1] * db[1] + db[2] * db[2]));
+    double wd = 0.0, wn = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      wd += q * de[d] * (last[d] - first[d]);
+      wn += q * ne[d] * (last[d] - first[d]);
+    }
+    defect = fabs(wd);
+    scale = a.abs_grid_work[n] + fabs(wn);
+  }
+  __shared__ double s_force[32], s_defect[32], s_scale[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  force = warp_max(force);
+  defect = warp_sum(defect);
+  scale = warp_sum(scale);
+  if (lane == 0) {
+    s_force[warp] = force;
+    s_defect[warp] = defect;
+    s_scale[warp] = scale;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int warps = blockDim.x >> 5;
+    force = lane < warps ? s_force[lane] : 0.0;
+    defect = lane < warps ? s_defect[lane] : 0.0;
+    scale = lane < warps ? s_scale[lane] : 0.0;
+    force = warp_max(force);
+    defect = warp_sum(defect);
+    scale = warp_sum(scale);
+    if (lane == 0) {
+      atomicMax(&a.sums->force_bits, (unsigned long long)__double_as_longlong(force));
+      atomicAdd(&a.sums->defect, defect);
+      atomicAdd(&a.sums->scale, scale);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stable compaction: the retained list keeps the reference's push_back
+// order (src/simulation.cpp:4916, 5581).
+__global__ void flag_count_kernel(const unsigned char* flag, unsigned char want, long long n,
+                                  unsigned* block_count) {
+  const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+  const bool f = i < n && flag[i] == want;
+  const unsigned ballot = __ballot_sync(0xffffffffu, f);
+  __shared__ unsigned warp_count[kScanBlock / 32];
+  if ((threadIdx.x & 31) == 0) warp_count[threadIdx.x >> 5] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned s = 0;
+    for (int w = 0; w < kScanBlock / 32; ++w) s += warp_count[w];
+    block_count[blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of the per-block counts by one block of 1024 threads.
+__global__ void block_offset_scan_kernel(const unsigned* block_count, int blocks,
+                                         unsigned* block_offset,
+                                         unsigned long long* total) {
+  __shared__ unsigned partial[1024];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < blocks; base += 1024) {
+    const int i = base + threadIdx.x;
+    const unsigned v = i < blocks ? block_count[i] : 0u;
+    partial[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      const unsigned add = threadIdx.x >= off ? partial[threadIdx.x - off] : 0u;
+      __syncthreads();
+      partial[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (i < blocks) block_offset[i] = (unsigned)(carry + partial[threadIdx.x] - v);
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += partial[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__device__ __forceinline__ long long compact_slot(const unsigned char* flag, unsigned char want,
+                                                  long long n, const unsigned* block_offset,
+                                                  bool& selected) {
+  const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+  selected = i < n && flag[i] == want;
+  const unsigned ballot = __ballot_sync(0xffffffffu, selected);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ unsigned warp_base[kScanBlock / 32];
+  if (lane == 0) warp_base[warp] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned s = 0;
+    for (int w = 0; w < kScanBlock / 32; ++w) {
+      const unsigned c = warp_base[w];
+      warp_base[w] = s;
+      s += c;
+    }
+  }
+  __syncthreads();
+  return (long long)block_offset[blockIdx.x] + warp_base[warp] +
+         __popc(ballot & ((1u << lane) - 1u));
+}
+
+__global__ void gather_particles_kernel(DParticles out, DParticles src, const double* x1,
+                                        const double* y1, const double* z1,
+                                        const double* ux1, const double* uy1,
+                                        const double* uz1, const unsigned char* flag,
+                                        unsigned char want, long long n,
+                                        const unsigned* block_offset) {
+  bool selected;
+  const long long slot = compact_slot(flag, want, n, block_offset, selected);
+  const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+  if (!selected) return;
+  out.x[slot] = x1[i]; out.y[slot] = y1[i]; out.z[slot] = z1[i];
+  out.ux[slot] = ux1[i]; out.uy[slot] = uy1[i]; out.uz[slot] = uz1[i];
+  out.q[slot] = src.q[i];
+  out.m[slot] = src.m[i];
+  out.id[slot] = src.id[i];
+}
+
+__global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsigned char* flag,
+                                       unsigned char want, long long n,
+                                       const unsigned* block_offset,
+                                       unsigned long long base) {
+  bool selected;
+  const long long slot = compact_slot(flag, want, n, block_offset, selected) + (long long)base;
+  const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+  if (!selected) return;
+  out.px[slot] = src.px[i]; out.py[slot] = src.py[i]; out.pz[slot] = src.pz[i];
+  out.vx[slot] = src.vx[i]; out.vy[slot] = src.vy[i]; out.vz[slot] = src.vz[i];
+  out.q[slot] = src.q[i];
+  out.w[slot] = src.w[i];
+}
+
+// finishMovingWindowStep carrier crop (src/simulation_moving_window.cpp:363-368).
+__global__ void crop_flags_kernel(DCarriers c, long long n, double upper, double lower,
+                                  unsigned char* keep, TrialCounters* counters,
+                                  DeviceStatus* status) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double z = c.pz[i];
+  unsigned char k = 1;
+  if (z >= upper) {
+    k = 0;
+    atomicAdd(&counters->cropped, 1ull);
+    atomicAdd(&counters->cropped_charge, c.q[i] * c.w[i]);
+  } else if (z < lower) {
+    raise_error(status, kErrFellBehind, (unsigned long long)i);
+  }
+  keep[i] = k;
+}
+
+// migrateWindowObjects' inlet guard (src/simulation_moving_window.cpp:355-358).
+__global__ void inlet_check_kernel(const double* z, long long n, double origin,
+                                   DeviceStatus* status) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && z[i] < origin) raise_error(status, kErrFellBehind, (unsigned long long)i);
+}
+
+}  // namespace aprl_gpu

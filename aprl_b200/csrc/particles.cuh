@@ -1,0 +1,134 @@
+// particles.cuh -- argument blocks of the particle kernels (particles.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace aprl_gpu {
+
+constexpr int kMaxMagnets = 4;
+
+// ParticleCPMLRegion + ParticleOpenBoundary geometry of the current window
+// (src/particle_boundary.cpp:56-85, 251-283), evaluated on the host.
+struct DRegion {
+  double outer_lower[3], outer_upper[3];
+  double physical_lower[3], physical_upper[3], tolerance[3];
+  double max_rate[3];     // maximumConductivityRate per axis
+  double thickness[3];    // cells*spacing per axis (0 when no CPML)
+  int cells[3];
+  double global_lower[3], global_upper[3], global_tolerance[3];
+  double order;           // polynomial order of the grading
+};
+
+// Particle SoA (RelativisticParticleSI without the diagnostics).
+struct DParticles {
+  double *x, *y, *z, *ux, *uy, *uz, *q, *m;
+  unsigned long long* id;
+};
+
+struct DCarriers {
+  double *px, *py, *pz, *vx, *vy, *vz, *q, *w;
+};
+
+// Per-trial counters of the boundary bookkeeping (src/simulation.cpp:
+// 4841-4901, 4375-4383); cumulative counters live on the host.
+struct TrialCounters {
+  unsigned long long exits;
+  double exit_charge;
+  unsigned long long cpml[6];
+  double cpml_charge[6];
+  unsigned long long direct[6];
+  double direct_charge[6];
+  unsigned long long carrier_outer[6];
+  double carrier_outer_charge[6];
+  unsigned long long cropped;     // carriers beyond the window upper edge
+  double cropped_charge;
+};
+
+struct ResidualSums {
+  unsigned long long force_bits;  // max over particles (non-negative double bits)
+  double defect;
+  double scale;
+  double calls;
+};
+
+struct PushArgs {
+  DGrid g;
+  DFrame frame;
+  DRegion region;
+  DMagnet magnets[kMaxMagnets];
+  int n_magnets;
+  int shape;
+  int substeps;
+  int first_trial;       // 1: gather along the ballistic guess chord
+  double time;           // box time at the start of the step
+  double exit_lab_z;
+  long long count;
+  DParticles p;          // state at the start of the step (read only)
+  double *x1, *y1, *z1, *ux1, *uy1, *uz1;  // state after the trial push
+  double* used_e;        // 3*count, written
+  double* used_b;
+  const double* next_e;  // 3*count, from the previous residual
+  const double* next_b;
+  double* abs_grid_work; // sum over substeps of |grid work|
+  unsigned char* action; // 0 retain, 1 CPML/exit carrier, 2 outer exit
+  DCarriers born;        // carrier created by a CPML entry (when kept)
+  unsigned char* born_keep;
+  TrialCounters* counters;
+  DeviceStatus* status;
+};
+
+struct CarrierArgs {
+  DGrid g;
+  DRegion region;
+  int shape;
+  long long count;
+  DCarriers in;          // carriers at the start of the step
+  DCarriers out;         // after this step's segment
+  unsigned char* keep;
+  TrialCounters* counters;
+  DeviceStatus* status;
+};
+
+struct ResidualArgs {
+  DGrid g;
+  int shape;
+  long long count;
+  DParticles p;
+  const double *x1, *y1, *z1;
+  const double* used_e;
+  const double* used_b;
+  double* next_e;
+  double* next_b;
+  const double* abs_grid_work;
+  ResidualSums* sums;
+  DeviceStatus* status;
+};
+
+__global__ void push_deposit_kernel(PushArgs a);
+__global__ void carrier_kernel(CarrierArgs a);
+__global__ void residual_kernel(ResidualArgs a);
+
+// Stable compaction helpers (warp ballot + block scan + block-offset scan).
+constexpr int kScanBlock = 256;
+__global__ void flag_count_kernel(const unsigned char* flag, unsigned char want,
+                                  long long n, unsigned* block_count);
+__global__ void block_offset_scan_kernel(const unsigned* block_count, int blocks,
+                                         unsigned* block_offset,
+                                         unsigned long long* total);
+__global__ void gather_particles_kernel(DParticles out, DParticles src,
+                                        const double* x1, const double* y1,
+                                        const double* z1, const double* ux1,
+                                        const double* uy1, const double* uz1,
+                                        const unsigned char* flag, unsigned char want,
+                                        long long n, const unsigned* block_offset);
+__global__ void gather_carriers_kernel(DCarriers out, DCarriers src,
+                                       const unsigned char* flag, unsigned char want,
+                                       long long n, const unsigned* block_offset,
+                                       unsigned long long base);
+__global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
+                                  double lower, unsigned char* keep,
+                                  TrialCounters* counters, DeviceStatus* status);
+__global__ void inlet_check_kernel(const double* z, long long n, double origin,
+                                   DeviceStatus* status);
+
+}  // namespace aprl_gpu

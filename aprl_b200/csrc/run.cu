@@ -1,0 +1,1415 @@
+// run.cu -- host runtime and C ABI of the B200 PIC step (include/aprl_gpu.h).
+//
+// An aprl_run owns all device state of one moving-window run and drives the
+// kernels of fields.cu and particles.cu on its stream in the reference's
+// step order (src/simulation.cpp:493-613,
+// src/simulation_source_coupling.cpp:16-65): inlet halos and the Cowan B
+// update, the zero-current E preview, fixed-point trials (carriers, push +
+// deposit, residual) until force < 1e-13 and work < 1e-8 after at least two
+// trials, the commit E^{n+1} = E* - dt/eps0 J with stable particle/carrier
+// compaction, and the ring-buffer window shift.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/aprl_gpu.h"
+#include "common.cuh"
+#include "fields.cuh"
+#include "particles.cuh"
+
+using namespace aprl_gpu;
+
+namespace {
+
+thread_local std::string g_error;
+
+aprl_status fail(aprl_status s, const char* format, ...) {
+  char buffer[640];
+  va_list args;
+  va_start(args, format);
+  vsnprintf(buffer, sizeof buffer, format, args);
+  va_end(args);
+  g_error = buffer;
+  return s;
+}
+
+#define CUDA_TRY(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess)                                                      \
+      return fail(APRL_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));      \
+  } while (0)
+
+enum Kernel : unsigned {
+  kInletLower, kCowanMagnetic, kElectricPreview, kCarrier, kPushDeposit,
+  kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
+  kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
+  kKernelCount
+};
+
+const char* kKernelNames[kKernelCount] = {
+  "inlet_lower", "cowan_magnetic", "electric_preview", "carrier",
+  "push_deposit", "residual", "electric_commit", "flag_count",
+  "block_offset_scan", "gather_particles", "gather_carriers",
+  "shift_insert", "crop_flags", "inlet_check", "detector_plane"};
+
+const char* device_error_text(unsigned code) {
+  switch (code) {
+    case kErrCrossingBudget: return "Quintic orbit exceeds crossing budget";
+    case kErrOrbitOutside: return "Active coupling orbit has no in-domain portion";
+    case kErrDepositOutside: return "Particle trajectory endpoint is outside the E/B domain";
+    case kErrSupportX: return "Transverse current support outside x grid";
+    case kErrSupportY: return "Transverse current support outside y grid";
+    case kErrRootNonphysical: return "Nonphysical local mean-gamma root";
+    case kErrRootNoConvergence: return "Local mean-gamma root did not converge";
+    case kErrNonFinite: return "Particle trajectory contains a non-finite coordinate";
+    case kErrStartInCpml: return "Active particle starts inside the non-physical CPML region";
+    case kErrStartOutside: return "Particle trajectory starts outside the global E/B domain";
+    case kErrBeyondExit: return "Active particle started beyond trusted moving-window exit";
+    case kErrUpstream: return "An active particle is upstream of the moving window";
+    case kErrCarrierWeight: return "Invalid CPML carrier current weight";
+    case kErrFellBehind: return "Active particle fell behind moving inlet";
+    case kErrReferenceRange: return "Moving reference query outside prepared native field";
+    case kErrHitLocate: return "Cannot locate the first particle boundary crossing";
+  }
+  return "unknown device error";
+}
+
+aprl_status device_error_status(unsigned code) {
+  switch (code) {
+    case kErrOrbitOutside: case kErrDepositOutside: case kErrSupportX:
+    case kErrSupportY: case kErrStartInCpml: case kErrStartOutside:
+    case kErrReferenceRange:
+      return APRL_ERR_OUT_OF_RANGE;
+    default:
+      return APRL_ERR_RUNTIME;
+  }
+}
+
+template <class T>
+aprl_status device_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
+  return APRL_OK;
+}
+
+// EBCowanCoefficients::forZDispersion (src/eb_field.cpp:33-73).
+aprl_status cowan(double dx, double dy, double dz, double out[12]) {
+  if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0) || !std::isfinite(dx) ||
+      !std::isfinite(dy) || !std::isfinite(dz))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Cowan-z grid spacing must be positive and finite");
+  const double tolerance = 64.0 * DBL_EPSILON * std::max(dx, std::max(dy, dz));
+  if (dx + tolerance < dz || dy + tolerance < dz)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Cowan-z requires dz to be the smallest grid spacing");
+  const double rx = (dz / dx) * (dz / dx), ry = (dz / dy) * (dz / dy), rz = 1.0;
+  const double den = rx * ry + ry * rz + rz * rx;
+  if (!(den > 0.0) || !std::isfinite(den))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid Cowan-z aspect ratios");
+  const double pf = rx * ry * rz / den;
+  double beta[3] = {rx * (1.0 - pf) / 8.0, ry * (1.0 - pf) / 8.0, rz * (1.0 - pf) / 8.0};
+  const double dxy = rx * ry * (1.0 / 16.0 - rx * ry / (8.0 * den));
+  const double dyz = ry * rz * (1.0 / 16.0 - ry * rz / (8.0 * den));
+  const double dzx = rz * rx * (1.0 / 16.0 - rz * rx / (8.0 * den));
+  out[0] = 1.0 - 2.0 * beta[1] - 2.0 * beta[2] - 4.0 * dyz;
+  out[1] = 1.0 - 2.0 * beta[2] - 2.0 * beta[0] - 4.0 * dzx;
+  out[2] = 1.0 - 2.0 * beta[0] - 2.0 * beta[1] - 4.0 * dxy;
+  out[3] = beta[0]; out[4] = beta[1]; out[5] = beta[2];
+  out[6] = dxy; out[7] = dyz; out[8] = dzx;
+  out[9] = rx; out[10] = ry; out[11] = rz;
+  return APRL_OK;
+}
+
+struct HostProfile {  // makeProfile result for one axis
+  std::vector<double> ikm1, decay, drive;
+  std::vector<int> ordinal;
+  int active = 0;
+};
+
+// EBCPMLParameters::maximumConductivityRate (src/eb_cpml.cpp:277-294).
+double maximum_rate(const aprl_run_config& g, int axis) {
+  const uint64_t cells = axis == 0 ? g.cpml_cells_x : (axis == 1 ? g.cpml_cells_y : 0);
+  if (cells == 0) return 0.0;
+  const double spacing = axis == 0 ? g.dx : (axis == 1 ? g.dy : g.dz);
+  const double thickness = static_cast<double>(cells) * spacing;
+  return -(g.cpml_polynomial_order + 1.0) * kC * std::log(g.cpml_target_reflection) /
+         (2.0 * thickness);
+}
+
+// makeProfile (src/eb_cpml.cpp:195-248) at one rank.
+HostProfile make_profile(const aprl_run_config& g, int axis, bool electric) {
+  HostProfile r;
+  const size_t local = axis == 0 ? g.nx : g.ny;
+  const size_t count = local + (electric ? 1 : 0);
+  r.ikm1.assign(count, 0.0);
+  r.decay.assign(count, 0.0);
+  r.drive.assign(count, 0.0);
+  r.ordinal.assign(count, -1);
+  const size_t thickness_cells = axis == 0 ? g.cpml_cells_x : g.cpml_cells_y;
+  if (thickness_cells == 0) return r;
+  const double thickness = static_cast<double>(thickness_cells);
+  const double sigma_max = maximum_rate(g, axis);
+  for (size_t index = 0; index < count; ++index) {
+    const double position = static_cast<double>(index) + (electric ? 0.0 : 0.5);
+    double depth = 0.0;
+    if (position < thickness) depth = (thickness - position) / thickness;
+    const double upper_start = static_cast<double>(local - thickness_cells);
+    if (position > upper_start) depth = std::max(depth, (position - upper_start) / thickness);
+    if (!(depth > 0.0)) continue;
+    depth = std::min(1.0, depth);
+    const double graded = std::pow(depth, g.cpml_polynomial_order);
+    const double sigma = sigma_max * graded;
+    const double kappa = 1.0 + (g.cpml_kappa_max - 1.0) * graded;
+    const double alpha = g.cpml_alpha_fraction * sigma_max * (1.0 - depth);
+    r.ikm1[index] = 1.0 / kappa - 1.0;
+    r.decay[index] = std::exp(-(sigma / kappa + alpha) * g.dt);
+    const double den = sigma * kappa + alpha * kappa * kappa;
+    r.drive[index] = den > 0.0 ? sigma * (r.decay[index] - 1.0) / den : 0.0;
+    r.ordinal[index] = r.active++;
+  }
+  return r;
+}
+
+struct DeviceProfile {
+  double *ikm1 = nullptr, *decay = nullptr, *drive = nullptr;
+  int* ordinal = nullptr;
+  int active = 0;
+  CpmlAxis view() const { return CpmlAxis{ikm1, decay, drive, ordinal}; }
+};
+
+// One of the 8 active histories.  component: ABI index (0..5); derivative
+// axis 0/1; the history's k ring follows its component's ring.
+struct HistoryBuffer {
+  double* data = nullptr;
+  int slots = 0, layers = 0, row = 0;
+  int component = 0;
+  int abi_index = 0;
+  size_t length() const { return (size_t)slots * layers * row; }
+  CpmlHistory view() const { return CpmlHistory{data, slots, layers, row}; }
+};
+
+struct Timing {
+  cudaEvent_t start, stop;
+  unsigned kernel;
+};
+
+}  // namespace
+
+struct aprl_run {
+  aprl_run_config cfg{};
+  cudaStream_t stream = nullptr;
+  double coeff[12]{};
+  double* e[2][3]{};
+  int cur = 0;  // e[cur] = E^n (committed), e[1-cur] = E*
+  double* b[3]{};
+  double* jc[3]{};
+  double* lower[3]{};
+  int zb_e[3]{}, zb_b[3]{};
+  double* ref[6]{};
+  bool ref_set[6]{};
+  DeviceProfile mprof[2], eprof[2];
+  HistoryBuffer hist[8];  // ABI indices 0,3,4,5,6,9,10,11
+  double max_rate[3]{};
+  // particles
+  size_t np = 0, pcap = 0;
+  DParticles p{}, p_alt{};
+  double *x1 = nullptr, *y1 = nullptr, *z1 = nullptr, *ux1 = nullptr, *uy1 = nullptr,
+         *uz1 = nullptr;
+  double *used_e = nullptr, *used_b = nullptr, *next_e = nullptr, *next_b = nullptr;
+  double* abs_work = nullptr;
+  unsigned char* action = nullptr;
+  DCarriers born{};
+  unsigned char* born_keep = nullptr;
+  size_t nslot = 0;
+  // carriers
+  size_t nc = 0, ccap = 0;
+  DCarriers c{}, c_alt{}, c_out{};
+  unsigned char* c_keep = nullptr;
+  // reductions, counters, status, scan scratch
+  TrialCounters* d_counters = nullptr;
+  ResidualSums* d_sums = nullptr;
+  DeviceStatus* d_status = nullptr;
+  unsigned* scan_count = nullptr;
+  unsigned* scan_offset = nullptr;
+  unsigned long long* scan_total = nullptr;
+  size_t scan_cap = 0;
+  // pinned host mirrors
+  ResidualSums* h_sums = nullptr;
+  DeviceStatus* h_status = nullptr;
+  TrialCounters* h_counters = nullptr;
+  unsigned long long* h_total = nullptr;
+  TrialCounters cumulative{};
+  // window state
+  uint64_t step = 0;
+  int64_t offset = 0;
+  double time = 0.0;
+  double origin[3]{};
+  int stage = 0;
+  unsigned trials = 0;
+  uint32_t last_iterations = 0, max_iterations = 0;
+  uint64_t total_iterations = 0;
+  double last_force = 0.0, last_work = 0.0;
+  // detector scratch
+  double* d_detector = nullptr;
+  size_t detector_cap = 0;
+  // profiling
+  bool profile = false;
+  std::vector<Timing> pending;
+  std::vector<cudaEvent_t> event_pool;
+  double kernel_ms[kKernelCount]{};
+  uint64_t kernel_launches[kKernelCount]{};
+  uint64_t launches = 0;
+};
+
+namespace {
+
+size_t e_count(const aprl_run_config& g, int c) {
+  return (size_t)(g.nx + (c != 0)) * (g.ny + (c != 1)) * (g.nz + (c != 2));
+}
+size_t b_count(const aprl_run_config& g, int c) {
+  return (size_t)(g.nx + (c == 0)) * (g.ny + (c == 1)) * (g.nz + (c == 2));
+}
+void comp_shape(const aprl_run_config& g, unsigned a, size_t s[3]) {
+  const bool electric = a < 3 || a >= 6;
+  const unsigned axis = a % 3;
+  const size_t cells[3] = {g.nx, g.ny, g.nz};
+  for (unsigned d = 0; d < 3; ++d) s[d] = cells[d] + (electric ? (d != axis) : (d == axis));
+}
+
+cudaEvent_t take_event(aprl_run* r) {
+  if (!r->event_pool.empty()) {
+    cudaEvent_t e = r->event_pool.back();
+    r->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+aprl_status drain_timings(aprl_run* r) {
+  for (auto& t : r->pending) {
+    CUDA_TRY(cudaEventSynchronize(t.stop));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, t.start, t.stop));
+    r->kernel_ms[t.kernel] += ms;
+    r->event_pool.push_back(t.start);
+    r->event_pool.push_back(t.stop);
+  }
+  r->pending.clear();
+  return APRL_OK;
+}
+
+// Launch with optional stage timing on the run's stream.
+template <class K, class... Args>
+aprl_status launch(aprl_run* r, unsigned id, K kernel, dim3 grid, dim3 block, Args... args) {
+  if (grid.x == 0 || grid.y == 0 || grid.z == 0) return APRL_OK;
+  Timing t{};
+  if (r->profile) {
+    t.start = take_event(r);
+    t.stop = take_event(r);
+    t.kernel = id;
+    CUDA_TRY(cudaEventRecord(t.start, r->stream));
+  }
+  kernel<<<grid, block, 0, r->stream>>>(args...);
+  CUDA_TRY(cudaGetLastError());
+  if (r->profile) {
+    CUDA_TRY(cudaEventRecord(t.stop, r->stream));
+    r->pending.push_back(t);
+  }
+  ++r->kernel_launches[id];
+  ++r->launches;
+  return APRL_OK;
+}
+
+#define TRY(expr)                    \
+  do {                               \
+    aprl_status s_ = (expr);         \
+    if (s_ != APRL_OK) return s_;    \
+  } while (0)
+
+DGrid make_grid(const aprl_run* r) {
+  DGrid g{};
+  g.nx = (int)r->cfg.nx;
+  g.ny = (int)r->cfg.ny;
+  g.nz = (int)r->cfg.nz;
+  g.dx = r->cfg.dx;
+  g.dy = r->cfg.dy;
+  g.dz = r->cfg.dz;
+  g.dt = r->cfg.dt;
+  for (int a = 0; a < 3; ++a) {
+    g.origin[a] = r->origin[a];
+    g.e_old[a] = r->e[r->cur][a];
+    g.e_star[a] = r->e[1 - r->cur][a];
+    g.b[a] = r->b[a];
+    g.j[a] = r->jc[a];
+    g.zb_e[a] = r->zb_e[a];
+    g.zb_b[a] = r->zb_b[a];
+  }
+  g.jcoef = -1. * r->cfg.dt / kEpsilon0;
+  return g;
+}
+
+DFrame make_frame(const aprl_run_config& c) {
+  return DFrame{c.boost_gamma, c.boost_beta, c.boost_gamma_beta,
+                c.lab_time_origin, c.lab_z_origin, c.box_z_origin};
+}
+
+// Simulation::movingWindowFieldValue's lerp weights for (k, step)
+// (src/simulation_moving_window.cpp:284-293).
+aprl_status inlet_table(const aprl_run* r, int64_t k, uint64_t step, InletTable& t) {
+  const double z = static_cast<double>(k) - r->cfg.translation_beta * static_cast<double>(step);
+  for (int a = 0; a < 6; ++a) {
+    if (!r->ref_set[a])
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Missing moving-window inlet reference component %d", a);
+    const size_t count = r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0);
+    if (!std::isfinite(z) || z < 0. || z > static_cast<double>(count - 1))
+      return fail(APRL_ERR_OUT_OF_RANGE, "Moving reference query outside prepared native field");
+    const size_t lo = static_cast<size_t>(std::floor(z));
+    const size_t hi = std::min(lo + 1, count - 1);
+    size_t s[3];
+    comp_shape(r->cfg, a, s);
+    t.table[a] = r->ref[a];
+    t.nxc[a] = (int)s[0];
+    t.nyc[a] = (int)s[1];
+    t.lo[a] = (int)lo;
+    t.hi[a] = (int)hi;
+    t.fraction = z - static_cast<double>(lo);
+  }
+  return APRL_OK;
+}
+
+// ParticleCPMLRegion / ParticleOpenBoundary on the current window.
+DRegion make_region(const aprl_run* r) {
+  const aprl_run_config& g = r->cfg;
+  DRegion d{};
+  const double spacing[3] = {g.dx, g.dy, g.dz};
+  const size_t cells[3] = {g.nx, g.ny, g.nz};
+  const size_t pc[3] = {g.cpml_cells_x, g.cpml_cells_y, 0};
+  for (int a = 0; a < 3; ++a) {
+    d.outer_lower[a] = r->origin[a];
+    d.outer_upper[a] = r->origin[a] + static_cast<double>(cells[a]) * spacing[a];
+    d.physical_lower[a] = d.outer_lower[a] + static_cast<double>(pc[a]) * spacing[a];
+    d.physical_upper[a] = d.outer_upper[a] - static_cast<double>(pc[a]) * spacing[a];
+    d.tolerance[a] = 64.0 * DBL_EPSILON *
+                     std::max(1.0, std::max(std::abs(d.outer_lower[a]), std::abs(d.outer_upper[a])));
+    d.max_rate[a] = r->max_rate[a];
+    d.thickness[a] = static_cast<double>(pc[a]) * spacing[a];
+    d.cells[a] = (int)pc[a];
+    d.global_lower[a] = r->origin[a];
+    d.global_upper[a] = std::fma(static_cast<double>(cells[a]), spacing[a], r->origin[a]);
+    d.global_tolerance[a] = 64.0 * DBL_EPSILON *
+        std::max(1.0, std::max(std::abs(d.global_lower[a]), std::abs(d.global_upper[a])));
+  }
+  d.order = g.cpml_polynomial_order;
+  return d;
+}
+
+aprl_status validate(const aprl_run_config& g) {
+  if (g.nx < 2 || g.ny < 2 || g.nz < 2)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "E/B staggered grid needs at least two cells in every direction");
+  if (g.nx > (1u << 20) || g.ny > (1u << 20) || g.nz > (1u << 24))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Grid extent exceeds the supported index range");
+  if (!(g.dx > 0.0) || !(g.dy > 0.0) || !(g.dz > 0.0) || !(g.dt > 0.0) || !std::isfinite(g.dx) ||
+      !std::isfinite(g.dy) || !std::isfinite(g.dz) || !std::isfinite(g.dt))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "E/B grid spacing and time step must be positive finite SI values");
+  if (std::abs(kC * g.dt - g.dz) > 64 * DBL_EPSILON * g.dz)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Moving-window requires c*dt=dz");
+  if (g.cpml_cells_x < 2 || g.cpml_cells_y < 2 || 2 * g.cpml_cells_x >= g.nx || 2 * g.cpml_cells_y >= g.ny)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Moving-window requires valid Cowan integer z slabs, xy-only CPML and an inlet reference");
+  if (!(g.cpml_polynomial_order > 0.0) ||
+      !(g.cpml_target_reflection > 0.0 && g.cpml_target_reflection < 1.0) ||
+      !(g.cpml_kappa_max >= 1.0) || !(g.cpml_alpha_fraction >= 0.0))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid CPML grading parameters");
+  if (g.shape != APRL_SHAPE_LINEAR_BINOMIAL3 && g.shape != APRL_SHAPE_QUINTIC_COMPENSATED)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "APRL 2.1 longitudinal_shape must be linear-binomial3 or quintic-compensated");
+  if (g.substeps < 1 || g.max_trials < 1 || g.max_trials > 64)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid substep or trial count");
+  if (!(g.boost_gamma >= 1.0) || !std::isfinite(g.boost_gamma))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Lorentz gamma must be finite and >= 1");
+  if (g.n_magnets > APRL_MAX_MAGNETS)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Too many prescribed magnets");
+  return APRL_OK;
+}
+
+aprl_status ensure_scan(aprl_run* r, size_t n) {
+  const size_t blocks = (n + kScanBlock - 1) / kScanBlock + 1;
+  if (blocks <= r->scan_cap) return APRL_OK;
+  cudaFree(r->scan_count);
+  cudaFree(r->scan_offset);
+  TRY(device_alloc(&r->scan_count, blocks));
+  TRY(device_alloc(&r->scan_offset, blocks));
+  r->scan_cap = blocks;
+  return APRL_OK;
+}
+
+aprl_status alloc_particles(DParticles& p, size_t n) {
+  TRY(device_alloc(&p.x, n)); TRY(device_alloc(&p.y, n)); TRY(device_alloc(&p.z, n));
+  TRY(device_alloc(&p.ux, n)); TRY(device_alloc(&p.uy, n)); TRY(device_alloc(&p.uz, n));
+  TRY(device_alloc(&p.q, n)); TRY(device_alloc(&p.m, n)); TRY(device_alloc(&p.id, n));
+  return APRL_OK;
+}
+void free_particles(DParticles& p) {
+  cudaFree(p.x); cudaFree(p.y); cudaFree(p.z); cudaFree(p.ux); cudaFree(p.uy);
+  cudaFree(p.uz); cudaFree(p.q); cudaFree(p.m); cudaFree(p.id);
+  p = DParticles{};
+}
+aprl_status alloc_carriers(DCarriers& c, size_t n) {
+  TRY(device_alloc(&c.px, n)); TRY(device_alloc(&c.py, n)); TRY(device_alloc(&c.pz, n));
+  TRY(device_alloc(&c.vx, n)); TRY(device_alloc(&c.vy, n)); TRY(device_alloc(&c.vz, n));
+  TRY(device_alloc(&c.q, n)); TRY(device_alloc(&c.w, n));
+  return APRL_OK;
+}
+void free_carriers(DCarriers& c) {
+  cudaFree(c.px); cudaFree(c.py); cudaFree(c.pz); cudaFree(c.vx); cudaFree(c.vy);
+  cudaFree(c.vz); cudaFree(c.q); cudaFree(c.w);
+  c = DCarriers{};
+}
+
+// Particle capacity: state (two copies for compaction), trial outputs,
+// slots, newborn carriers.  Existing contents of p are preserved.
+aprl_status reserve_particles(aprl_run* r, size_t n) {
+  if (n <= r->pcap) return APRL_OK;
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  DParticles np{};
+  TRY(alloc_particles(np, n));
+  if (r->np) {
+    CUDA_TRY(cudaMemcpy(np.x, r->p.x, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.y, r->p.y, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.z, r->p.z, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.ux, r->p.ux, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.uy, r->p.uy, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.uz, r->p.uz, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.q, r->p.q, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.m, r->p.m, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.id, r->p.id, r->np * 8, cudaMemcpyDeviceToDevice));
+  }
+  free_particles(r->p);
+  free_particles(r->p_alt);
+  r->p = np;
+  TRY(alloc_particles(r->p_alt, n));
+  double** trial[] = {&r->x1, &r->y1, &r->z1, &r->ux1, &r->uy1, &r->uz1, &r->abs_work};
+  for (double** t : trial) {
+    cudaFree(*t);
+    TRY(device_alloc(t, n));
+  }
+  double** slot[] = {&r->used_e, &r->used_b, &r->next_e, &r->next_b};
+  for (double** t : slot) {
+    cudaFree(*t);
+    TRY(device_alloc(t, 3 * n));
+  }
+  cudaFree(r->action);
+  cudaFree(r->born_keep);
+  TRY(device_alloc(&r->action, n));
+  TRY(device_alloc(&r->born_keep, n));
+  free_carriers(r->born);
+  TRY(alloc_carriers(r->born, n));
+  r->pcap = n;
+  return ensure_scan(r, n);
+}
+
+aprl_status copy_carriers(DCarriers& dst, const DCarriers& src, size_t n) {
+  if (!n) return APRL_OK;
+  const double* s[] = {src.px, src.py, src.pz, src.vx, src.vy, src.vz, src.q, src.w};
+  double* d[] = {dst.px, dst.py, dst.pz, dst.vx, dst.vy, dst.vz, dst.q, dst.w};
+  for (int k = 0; k < 8; ++k)
+    CUDA_TRY(cudaMemcpy(d[k], s[k], n * 8, cudaMemcpyDeviceToDevice));
+  return APRL_OK;
+}
+
+// Carrier capacity.  The current list and the per-step outputs (c_out,
+// c_keep) of the `nc` existing carriers survive a reallocation.
+aprl_status reserve_carriers(aprl_run* r, size_t n) {
+  if (n <= r->ccap) return APRL_OK;
+  n = std::max(n, 2 * r->ccap);
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  DCarriers nc{}, nout{};
+  unsigned char* nkeep = nullptr;
+  TRY(alloc_carriers(nc, n));
+  TRY(alloc_carriers(nout, n));
+  TRY(device_alloc(&nkeep, n));
+  TRY(copy_carriers(nc, r->c, r->nc));
+  TRY(copy_carriers(nout, r->c_out, r->nc));
+  if (r->nc) CUDA_TRY(cudaMemcpy(nkeep, r->c_keep, r->nc, cudaMemcpyDeviceToDevice));
+  free_carriers(r->c);
+  free_carriers(r->c_alt);
+  free_carriers(r->c_out);
+  cudaFree(r->c_keep);
+  r->c = nc;
+  r->c_out = nout;
+  r->c_keep = nkeep;
+  TRY(alloc_carriers(r->c_alt, n));
+  r->ccap = n;
+  return ensure_scan(r, n);
+}
+
+// Rotate between logical (window) and physical (ring) plane order.
+aprl_status copy_ring(aprl_run* r, double* device, const double* host_in, double* host_out,
+                      size_t plane, size_t layers, int base, size_t slots = 1) {
+  for (size_t s = 0; s < slots; ++s) {
+    const size_t slot_offset = s * layers * plane;
+    for (size_t k = 0; k < layers; ++k) {
+      const size_t pk = (k + base) % layers;
+      double* d = device + slot_offset + pk * plane;
+      if (host_in)
+        CUDA_TRY(cudaMemcpyAsync(d, host_in + slot_offset + k * plane, plane * 8,
+                                 cudaMemcpyHostToDevice, r->stream));
+      else
+        CUDA_TRY(cudaMemcpyAsync(host_out + slot_offset + k * plane, d, plane * 8,
+                                 cudaMemcpyDeviceToHost, r->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status check_device(aprl_run* r) {
+  CUDA_TRY(cudaMemcpyAsync(r->h_status, r->d_status, sizeof(DeviceStatus),
+                           cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (r->h_status->code)
+    return fail(device_error_status(r->h_status->code), "%s (element %llu)",
+                device_error_text(r->h_status->code), r->h_status->where);
+  return APRL_OK;
+}
+
+dim3 grid3(const aprl_run_config& g, dim3 block) {
+  return dim3((unsigned)((g.nx + 1 + block.x - 1) / block.x),
+              (unsigned)((g.ny + 1 + block.y - 1) / block.y), (unsigned)(g.nz + 1));
+}
+
+unsigned blocks_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+void add_counters(TrialCounters& to, const TrialCounters& from) {
+  to.exits += from.exits;
+  to.exit_charge += from.exit_charge;
+  for (int f = 0; f < 6; ++f) {
+    to.cpml[f] += from.cpml[f];
+    to.cpml_charge[f] += from.cpml_charge[f];
+    to.direct[f] += from.direct[f];
+    to.direct_charge[f] += from.direct_charge[f];
+    to.carrier_outer[f] += from.carrier_outer[f];
+    to.carrier_outer_charge[f] += from.carrier_outer_charge[f];
+  }
+  to.cropped += from.cropped;
+  to.cropped_charge += from.cropped_charge;
+}
+
+// Stable compaction of `n` flagged elements; returns the kept count.
+aprl_status compact_count(aprl_run* r, const unsigned char* flag, unsigned char want, size_t n,
+                          unsigned long long* kept) {
+  *kept = 0;
+  if (n == 0) return APRL_OK;
+  TRY(ensure_scan(r, n));
+  const unsigned blocks = blocks_for(n, kScanBlock);
+  TRY(launch(r, kFlagCount, flag_count_kernel, dim3(blocks), dim3(kScanBlock), flag, want,
+             (long long)n, r->scan_count));
+  TRY(launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
+             (const unsigned*)r->scan_count, (int)blocks, r->scan_offset, r->scan_total));
+  CUDA_TRY(cudaMemcpyAsync(r->h_total, r->scan_total, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  *kept = *r->h_total;
+  return APRL_OK;
+}
+
+aprl_status do_advance_magnetic(aprl_run* r) {
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
+  const aprl_run_config& c = r->cfg;
+  for (int a = 0; a < 3; ++a)
+    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream));
+  InletPlaneArgs ia{};
+  ia.nx = (int)c.nx;
+  ia.ny = (int)c.ny;
+  for (int a = 0; a < 3; ++a) ia.out[a] = r->lower[a];
+  TRY(inlet_table(r, r->offset - 1, r->step, ia.inlet));
+  TRY(launch(r, kInletLower, inlet_lower_kernel,
+             dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), 3), dim3(32, 8), ia));
+  CowanArgs ca{};
+  ca.g = make_grid(r);
+  for (int a = 0; a < 3; ++a) {
+    ca.e[a] = r->e[r->cur][a];
+    ca.lower[a] = r->lower[a];
+    ca.alpha[a] = r->coeff[a];
+    ca.beta[a] = r->coeff[3 + a];
+  }
+  ca.delta_xy = r->coeff[6];
+  ca.delta_yz = r->coeff[7];
+  ca.delta_zx = r->coeff[8];
+  ca.mx = r->mprof[0].view();
+  ca.my = r->mprof[1].view();
+  for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
+  const dim3 block(32, 4);
+  TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel, grid3(c, block), block, ca));
+  r->stage = 1;
+  return APRL_OK;
+}
+
+aprl_status do_preview_electric(aprl_run* r) {
+  if (r->stage != 1) return fail(APRL_ERR_RUNTIME, "Moving-window electric phase mismatch");
+  const aprl_run_config& c = r->cfg;
+  PreviewArgs pa{};
+  pa.g = make_grid(r);
+  pa.ex_prof = r->eprof[0].view();
+  pa.ey_prof = r->eprof[1].view();
+  for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view();
+  TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
+  const dim3 block(32, 4);
+  TRY(launch(r, kElectricPreview, electric_preview_kernel, grid3(c, block), block, pa));
+  r->nslot = r->np;
+  r->trials = 0;
+  r->stage = 2;
+  return APRL_OK;
+}
+
+aprl_status do_trial(aprl_run* r, double residual[4]) {
+  if (r->stage != 2 && r->stage != 3)
+    return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
+  const aprl_run_config& c = r->cfg;
+  for (int a = 0; a < 3; ++a)
+    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
+  CUDA_TRY(cudaMemsetAsync(r->d_sums, 0, sizeof(ResidualSums), r->stream));
+  const DGrid g = make_grid(r);
+  const DRegion region = make_region(r);
+  if (r->nc) {
+    CarrierArgs ca{};
+    ca.g = g;
+    ca.region = region;
+    ca.shape = c.shape;
+    ca.count = (long long)r->nc;
+    ca.in = r->c;
+    ca.out = r->c_out;
+    ca.keep = r->c_keep;
+    ca.counters = r->d_counters;
+    ca.status = r->d_status;
+    TRY(launch(r, kCarrier, carrier_kernel, dim3(blocks_for(r->nc, 128)), dim3(128), ca));
+  }
+  if (r->np) {
+    PushArgs pa{};
+    pa.g = g;
+    pa.frame = make_frame(c);
+    pa.region = region;
+    pa.n_magnets = (int)c.n_magnets;
+    for (uint32_t m = 0; m < c.n_magnets; ++m) {
+      const aprl_magnet& s = c.magnets[m];
+      DMagnet& d = pa.magnets[m];
+      d.type = s.type == APRL_MAGNET_PLANAR_UNDULATOR ? 0 : (s.type == APRL_MAGNET_UNIFORM_DIPOLE ? 1 : 2);
+      d.gaussian_fringe = s.gaussian_fringe;
+      for (int a = 0; a < 3; ++a) d.center[a] = s.center[a];
+      d.length = s.length;
+      d.period = s.period;
+      d.peak_field = s.peak_field;
+      d.quadrupole_gradient = s.quadrupole_gradient;
+      d.wave_number = s.wave_number;
+      d.fringe_extent = s.fringe_extent;
+      d.cos_angle = s.cos_angle;
+      d.sin_angle = s.sin_angle;
+    }
+    pa.shape = c.shape;
+    pa.substeps = (int)c.substeps;
+    pa.first_trial = r->trials == 0 ? 1 : 0;
+    pa.time = r->time;
+    pa.exit_lab_z = c.exit_lab_z;
+    pa.count = (long long)r->np;
+    pa.p = r->p;
+    pa.x1 = r->x1; pa.y1 = r->y1; pa.z1 = r->z1;
+    pa.ux1 = r->ux1; pa.uy1 = r->uy1; pa.uz1 = r->uz1;
+    pa.used_e = r->used_e;
+    pa.used_b = r->used_b;
+    pa.next_e = r->next_e;
+    pa.next_b = r->next_b;
+    pa.abs_grid_work = r->abs_work;
+    pa.action = r->action;
+    pa.born = r->born;
+    pa.born_keep = r->born_keep;
+    pa.counters = r->d_counters;
+    pa.status = r->d_status;
+    TRY(launch(r, kPushDeposit, push_deposit_kernel, dim3(blocks_for(r->np, 128)), dim3(128), pa));
+    ResidualArgs ra{};
+    ra.g = g;
+    ra.shape = c.shape;
+    ra.count = (long long)r->np;
+    ra.p = r->p;
+    ra.x1 = r->x1; ra.y1 = r->y1; ra.z1 = r->z1;
+    ra.used_e = r->used_e;
+    ra.used_b = r->used_b;
+    ra.next_e = r->next_e;
+    ra.next_b = r->next_b;
+    ra.abs_grid_work = r->abs_work;
+    ra.sums = r->d_sums;
+    ra.status = r->d_status;
+    TRY(launch(r, kResidual, residual_kernel, dim3(blocks_for(r->np, 128)), dim3(128), ra));
+  }
+  CUDA_TRY(cudaMemcpyAsync(r->h_sums, r->d_sums, sizeof(ResidualSums), cudaMemcpyDeviceToHost,
+                           r->stream));
+  TRY(check_device(r));
+  double force;
+  const unsigned long long bits = r->h_sums->force_bits;
+  std::memcpy(&force, &bits, sizeof force);
+  residual[0] = force;
+  residual[1] = r->h_sums->defect;
+  residual[2] = r->h_sums->scale;
+  residual[3] = static_cast<double>(r->np);
+  ++r->trials;
+  r->stage = 3;
+  return APRL_OK;
+}
+
+aprl_status do_commit(aprl_run* r) {
+  if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
+  const aprl_run_config& c = r->cfg;
+  const DGrid g = make_grid(r);
+  const dim3 block(32, 4);
+  TRY(launch(r, kElectricCommit, electric_commit_kernel, grid3(c, block), block, g));
+  r->cur = 1 - r->cur;
+  // Counters of the converged trial become cumulative.
+  CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
+                           cudaMemcpyDeviceToHost, r->stream));
+  // Carriers: surviving old carriers, then carriers born this step, in
+  // particle order (retainedCarriers, src/simulation.cpp:4401-4405).
+  unsigned long long kept_old = 0, kept_born = 0;
+  TRY(compact_count(r, r->c_keep, 1, r->nc, &kept_old));
+  TRY(compact_count(r, r->born_keep, 1, r->np, &kept_born));
+  TRY(reserve_carriers(r, kept_old + kept_born));
+  if (r->nc) {
+    TRY(compact_count(r, r->c_keep, 1, r->nc, &kept_old));
+    TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->nc, kScanBlock)),
+               dim3(kScanBlock), r->c_alt, r->c_out, (const unsigned char*)r->c_keep,
+               (unsigned char)1, (long long)r->nc, (const unsigned*)r->scan_offset, 0ull));
+  }
+  if (r->np) {
+    TRY(compact_count(r, r->born_keep, 1, r->np, &kept_born));
+    TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->np, kScanBlock)),
+               dim3(kScanBlock), r->c_alt, r->born, (const unsigned char*)r->born_keep,
+               (unsigned char)1, (long long)r->np, (const unsigned*)r->scan_offset,
+               (unsigned long long)kept_old));
+  }
+  std::swap(r->c, r->c_alt);
+  r->nc = kept_old + kept_born;
+  // Particles: the retained list in order (src/simulation.cpp:4916, 5581).
+  if (r->np) {
+    unsigned long long kept = 0;
+    TRY(compact_count(r, r->action, 0, r->np, &kept));
+    TRY(launch(r, kGatherParticles, gather_particles_kernel, dim3(blocks_for(r->np, kScanBlock)),
+               dim3(kScanBlock), r->p_alt, r->p, (const double*)r->x1, (const double*)r->y1,
+               (const double*)r->z1, (const double*)r->ux1, (const double*)r->uy1,
+               (const double*)r->uz1, (const unsigned char*)r->action, (unsigned char)0,
+               (long long)r->np, (const unsigned*)r->scan_offset));
+    std::swap(r->p, r->p_alt);
+    r->np = kept;
+  }
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  add_counters(r->cumulative, *r->h_counters);
+  r->stage = 4;
+  return APRL_OK;
+}
+
+aprl_status do_shift(aprl_run* r) {
+  if (r->stage != 4)
+    return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
+  const aprl_run_config& c = r->cfg;
+  r->time += c.dt;
+  r->step += 1;
+  r->offset = c.initial_offset - static_cast<int64_t>(r->step);
+  for (int a = 0; a < 3; ++a) {
+    const int nze = (int)(c.nz + (a != 2)), nzb = (int)(c.nz + (a == 2));
+    r->zb_e[a] = (r->zb_e[a] + nze - 1) % nze;
+    r->zb_b[a] = (r->zb_b[a] + nzb - 1) % nzb;
+  }
+  ShiftArgs sa{};
+  sa.g = make_grid(r);
+  TRY(inlet_table(r, r->offset, r->step, sa.inlet));
+  for (int h = 0; h < 8; ++h) {
+    sa.h[h] = r->hist[h].view();
+    const int comp = r->hist[h].component;
+    sa.history_base[h] = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
+  }
+  int max_row = (int)std::max(c.nx, c.ny) + 1, max_slots = 1;
+  for (int h = 0; h < 8; ++h) max_slots = std::max(max_slots, r->hist[h].slots);
+  const int ydim = std::max(max_slots, (int)c.ny + 1);
+  TRY(launch(r, kShiftInsert, shift_insert_kernel,
+             dim3(blocks_for(max_row, 32), blocks_for(ydim, 8), 14), dim3(32, 8), sa));
+  r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
+  if (r->np)
+    TRY(launch(r, kInletCheck, inlet_check_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
+               (const double*)r->p.z, (long long)r->np, r->origin[2], r->d_status));
+  if (r->nc) {
+    const double upper = std::fma(static_cast<double>(c.nz), c.dz, r->origin[2]);
+    CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
+    TRY(launch(r, kCropFlags, crop_flags_kernel, dim3(blocks_for(r->nc, 256)), dim3(256), r->c,
+               (long long)r->nc, upper, r->origin[2], r->c_keep, r->d_counters, r->d_status));
+    unsigned long long kept = 0;
+    TRY(compact_count(r, r->c_keep, 1, r->nc, &kept));
+    TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->nc, kScanBlock)),
+               dim3(kScanBlock), r->c_alt, r->c, (const unsigned char*)r->c_keep,
+               (unsigned char)1, (long long)r->nc, (const unsigned*)r->scan_offset, 0ull));
+    std::swap(r->c, r->c_alt);
+    r->nc = kept;
+    CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
+                             cudaMemcpyDeviceToHost, r->stream));
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    r->cumulative.cropped += r->h_counters->cropped;
+    r->cumulative.cropped_charge += r->h_counters->cropped_charge;
+  }
+  TRY(check_device(r));
+  r->stage = 0;
+  return APRL_OK;
+}
+
+HistoryBuffer* find_history(aprl_run* r, unsigned index) {
+  for (auto& h : r->hist)
+    if ((unsigned)h.abi_index == index) return &h;
+  return nullptr;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* aprl_last_error(void) { return g_error.c_str(); }
+int aprl_abi_version(void) { return APRL_GPU_ABI_VERSION; }
+
+const char* aprl_kernel_name(unsigned kernel) {
+  return kernel < kKernelCount ? kKernelNames[kernel] : "";
+}
+
+aprl_status aprl_cowan_coefficients(double dx, double dy, double dz, double out[12]) {
+  return cowan(dx, dy, dz, out);
+}
+
+aprl_status aprl_magnet_prepare(aprl_magnet* m) {
+  if (!m) return fail(APRL_ERR_INVALID_ARGUMENT, "null magnet");
+  if (!std::isfinite(m->center[0]) || !std::isfinite(m->center[1]) || !std::isfinite(m->center[2]) ||
+      !(m->length >= 0.0) || !std::isfinite(m->length) || !std::isfinite(m->peak_field) ||
+      !std::isfinite(m->polarization_angle))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI magnetic element");
+  if (m->type == APRL_MAGNET_PLANAR_UNDULATOR && (!(m->period > 0.0) || !std::isfinite(m->period)))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Undulator period must be positive");
+  if (m->type == APRL_MAGNET_PLANAR_UNDULATOR && m->gaussian_fringe &&
+      (!(m->fringe_relative_cutoff > 0.0) || !(m->fringe_relative_cutoff < 1.0)))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Undulator fringe_relative_cutoff must be in (0,1)");
+  if (m->type == APRL_MAGNET_UNIFORM_DIPOLE && !(m->length > 0.0))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Dipole length must be positive");
+  if (m->type == APRL_MAGNET_QUADRUPOLE && (!(m->length > 0.0) || !std::isfinite(m->quadrupole_gradient)))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Quadrupole length/gradient is invalid");
+  m->wave_number = m->type == APRL_MAGNET_PLANAR_UNDULATOR ? 2.0 * kPi / m->period : 0.0;
+  m->fringe_extent = m->type == APRL_MAGNET_PLANAR_UNDULATOR && m->gaussian_fringe
+                         ? std::sqrt(-2.0 * std::log(m->fringe_relative_cutoff)) / m->wave_number
+                         : 0.0;
+  m->cos_angle = std::cos(m->polarization_angle);
+  m->sin_angle = std::sin(m->polarization_angle);
+  return APRL_OK;
+}
+
+aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_run** out) {
+  if (!config || !out) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  TRY(validate(*config));
+  aprl_run* r = new (std::nothrow) aprl_run();
+  if (!r) return fail(APRL_ERR_RUNTIME, "out of host memory");
+  r->cfg = *config;
+  r->stream = static_cast<cudaStream_t>(stream);
+  aprl_status s = cowan(config->dx, config->dy, config->dz, r->coeff);
+  auto cleanup = [&](aprl_status st) {
+    aprl_run_destroy(r);
+    return st;
+  };
+  if (s != APRL_OK) return cleanup(s);
+  const aprl_run_config& c = *config;
+  for (int a = 0; a < 3; ++a) {
+    for (int k = 0; k < 2; ++k) {
+      if ((s = device_alloc(&r->e[k][a], e_count(c, a))) != APRL_OK) return cleanup(s);
+      cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * 8, r->stream);
+    }
+    if ((s = device_alloc(&r->b[a], b_count(c, a))) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(r->b[a], 0, b_count(c, a) * 8, r->stream);
+    if ((s = device_alloc(&r->jc[a], e_count(c, a))) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream);
+    const size_t plane = (size_t)(c.nx + (a != 0)) * (c.ny + (a != 1));
+    if ((s = device_alloc(&r->lower[a], plane)) != APRL_OK) return cleanup(s);
+    r->max_rate[a] = maximum_rate(c, a);
+  }
+  // CPML profiles (x, y) for magnetic (half-integer) and electric nodes.
+  for (int axis = 0; axis < 2; ++axis) {
+    for (int electric = 0; electric < 2; ++electric) {
+      const HostProfile hp = make_profile(c, axis, electric != 0);
+      DeviceProfile& dp = electric ? r->eprof[axis] : r->mprof[axis];
+      const size_t n = hp.ikm1.size();
+      if ((s = device_alloc(&dp.ikm1, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(&dp.decay, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(&dp.drive, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(&dp.ordinal, n)) != APRL_OK) return cleanup(s);
+      cudaMemcpy(dp.ikm1, hp.ikm1.data(), n * 8, cudaMemcpyHostToDevice);
+      cudaMemcpy(dp.decay, hp.decay.data(), n * 8, cudaMemcpyHostToDevice);
+      cudaMemcpy(dp.drive, hp.drive.data(), n * 8, cudaMemcpyHostToDevice);
+      cudaMemcpy(dp.ordinal, hp.ordinal.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+      dp.active = hp.active;
+    }
+  }
+  // Active histories: ABI index, component (ABI), derivative axis.
+  const int defs[8][3] = {{0, 3, 1}, {3, 4, 0}, {4, 5, 0}, {5, 5, 1},
+                          {6, 0, 1}, {9, 1, 0}, {10, 2, 0}, {11, 2, 1}};
+  for (int h = 0; h < 8; ++h) {
+    HistoryBuffer& hb = r->hist[h];
+    hb.abi_index = defs[h][0];
+    hb.component = defs[h][1];
+    const int der = defs[h][2];
+    size_t sh[3];
+    comp_shape(c, (unsigned)hb.component, sh);
+    const DeviceProfile& prof = hb.component < 3 ? r->eprof[der] : r->mprof[der];
+    hb.slots = prof.active;
+    hb.layers = (int)sh[2];
+    hb.row = (int)(der == 0 ? sh[1] : sh[0]);
+    if ((s = device_alloc(&hb.data, hb.length())) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * 8, r->stream);
+  }
+  if ((s = device_alloc(&r->d_counters, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->d_sums, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->d_status, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->scan_total, 1)) != APRL_OK) return cleanup(s);
+  cudaMemsetAsync(r->d_status, 0, sizeof(DeviceStatus), r->stream);
+  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums), sizeof(ResidualSums)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_status), sizeof(DeviceStatus)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters), sizeof(TrialCounters)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_total), sizeof(unsigned long long)) != cudaSuccess)
+    return cleanup(fail(APRL_ERR_CUDA, "cudaMallocHost failed"));
+  r->offset = c.initial_offset;
+  r->origin[0] = c.reference_origin[0];
+  r->origin[1] = c.reference_origin[1];
+  r->origin[2] = std::fma(static_cast<double>(c.initial_offset), c.dz, c.reference_origin[2]);
+  if (cudaStreamSynchronize(r->stream) != cudaSuccess)
+    return cleanup(fail(APRL_ERR_CUDA, "stream synchronise failed at creation"));
+  *out = r;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_destroy(aprl_run* r) {
+  if (!r) return APRL_OK;
+  if (r->stream) cudaStreamSynchronize(r->stream); else cudaDeviceSynchronize();
+  for (auto& t : r->pending) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  for (auto e : r->event_pool) cudaEventDestroy(e);
+  for (int a = 0; a < 3; ++a) {
+    cudaFree(r->e[0][a]); cudaFree(r->e[1][a]); cudaFree(r->b[a]); cudaFree(r->jc[a]);
+    cudaFree(r->lower[a]);
+  }
+  for (int a = 0; a < 6; ++a) cudaFree(r->ref[a]);
+  for (int a = 0; a < 2; ++a) {
+    for (DeviceProfile* dp : {&r->mprof[a], &r->eprof[a]}) {
+      cudaFree(dp->ikm1); cudaFree(dp->decay); cudaFree(dp->drive); cudaFree(dp->ordinal);
+    }
+  }
+  for (auto& h : r->hist) cudaFree(h.data);
+  free_particles(r->p);
+  free_particles(r->p_alt);
+  double* singles[] = {r->x1, r->y1, r->z1, r->ux1, r->uy1, r->uz1, r->used_e, r->used_b,
+                       r->next_e, r->next_b, r->abs_work, r->d_detector};
+  for (double* d : singles) cudaFree(d);
+  cudaFree(r->action);
+  cudaFree(r->born_keep);
+  free_carriers(r->born);
+  free_carriers(r->c);
+  free_carriers(r->c_alt);
+  free_carriers(r->c_out);
+  cudaFree(r->c_keep);
+  cudaFree(r->d_counters);
+  cudaFree(r->d_sums);
+  cudaFree(r->d_status);
+  cudaFree(r->scan_count);
+  cudaFree(r->scan_offset);
+  cudaFree(r->scan_total);
+  cudaFreeHost(r->h_sums);
+  cudaFreeHost(r->h_status);
+  cudaFreeHost(r->h_counters);
+  cudaFreeHost(r->h_total);
+  delete r;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_set_reference(aprl_run* r, unsigned a, const double* host, size_t count) {
+  if (!r || a >= 6) return fail(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
+  size_t s[3];
+  comp_shape(r->cfg, a, s);
+  const size_t n = s[0] * s[1] * (r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0));
+  if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
+  if (host)
+    for (size_t i = 0; i < n; ++i)
+      if (!std::isfinite(host[i])) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  cudaFree(r->ref[a]);
+  r->ref[a] = nullptr;
+  TRY(device_alloc(&r->ref[a], n));
+  if (host)
+    CUDA_TRY(cudaMemcpy(r->ref[a], host, n * 8, cudaMemcpyHostToDevice));
+  else
+    CUDA_TRY(cudaMemset(r->ref[a], 0, n * 8));
+  r->ref_set[a] = true;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_set_reference_planes(aprl_run* r, unsigned a, uint64_t first, uint64_t planes,
+                                          const double* host) {
+  if (!r || a >= 6) return fail(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
+  if (!r->ref_set[a]) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component not allocated");
+  size_t s[3];
+  comp_shape(r->cfg, a, s);
+  const uint64_t layers = r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0);
+  if (!host || first > layers || planes > layers - first)
+    return fail(APRL_ERR_OUT_OF_RANGE, "Reference planes outside the prepared native field");
+  const size_t plane = s[0] * s[1];
+  for (size_t i = 0; i < planes * plane; ++i)
+    if (!std::isfinite(host[i])) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
+  CUDA_TRY(cudaMemcpyAsync(r->ref[a] + first * plane, host, planes * plane * 8,
+                           cudaMemcpyHostToDevice, r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_field_shape(const aprl_run* r, unsigned a, uint64_t shape[3]) {
+  if (!r || a >= 9) return fail(APRL_ERR_OUT_OF_RANGE, "Field component");
+  size_t s[3];
+  comp_shape(r->cfg, a, s);
+  for (int d = 0; d < 3; ++d) shape[d] = s[d];
+  return APRL_OK;
+}
+
+static aprl_status field_io(aprl_run* r, unsigned a, const double* in, double* out, size_t count) {
+  if (!r || a >= 9) return fail(APRL_ERR_OUT_OF_RANGE, "Field component");
+  size_t s[3];
+  comp_shape(r->cfg, a, s);
+  if (count != s[0] * s[1] * s[2] || (!in && !out))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Field component size mismatch");
+  if (r->stage != 0 && r->stage != 4 && in)
+    return fail(APRL_ERR_RUNTIME, "Fields can only be replaced between steps");
+  const size_t plane = s[0] * s[1];
+  if (a >= 6)
+    return copy_ring(r, r->jc[a - 6], in, out, plane, s[2], 0);
+  if (a < 3) return copy_ring(r, r->e[r->cur][a], in, out, plane, s[2], r->zb_e[a]);
+  return copy_ring(r, r->b[a - 3], in, out, plane, s[2], r->zb_b[a - 3]);
+}
+
+aprl_status aprl_run_set_field(aprl_run* r, unsigned a, const double* host, size_t count) {
+  return field_io(r, a, host, nullptr, count);
+}
+
+aprl_status aprl_run_get_field(aprl_run* r, unsigned a, double* host, size_t count) {
+  return field_io(r, a, nullptr, host, count);
+}
+
+aprl_status aprl_run_history_length(const aprl_run* r, unsigned index, uint64_t* length) {
+  if (!r || index >= 12) return fail(APRL_ERR_OUT_OF_RANGE, "CPML checkpoint history index is out of range");
+  HistoryBuffer* h = find_history(const_cast<aprl_run*>(r), index);
+  *length = h ? h->length() : 0;
+  return APRL_OK;
+}
+
+static aprl_status history_io(aprl_run* r, unsigned index, const double* in, double* out, size_t count) {
+  if (!r || index >= 12) return fail(APRL_ERR_OUT_OF_RANGE, "CPML checkpoint history index is out of range");
+  HistoryBuffer* h = find_history(r, index);
+  const size_t length = h ? h->length() : 0;
+  if (count != length) return fail(APRL_ERR_INVALID_ARGUMENT, "CPML history size mismatch");
+  if (!length) return APRL_OK;
+  const int comp = h->component;
+  const int base = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
+  return copy_ring(r, h->data, in, out, (size_t)h->row, (size_t)h->layers, base, (size_t)h->slots);
+}
+
+aprl_status aprl_run_set_history(aprl_run* r, unsigned index, const double* host, size_t count) {
+  return history_io(r, index, host, nullptr, count);
+}
+
+aprl_status aprl_run_get_history(aprl_run* r, unsigned index, double* host, size_t count) {
+  return history_io(r, index, nullptr, host, count);
+}
+
+aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const double* y,
+                                   const double* z, const double* ux, const double* uy,
+                                   const double* uz, const double* q, const double* m,
+                                   const uint64_t* id, int reset_carriers) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Particles can only be replaced between steps");
+  if (n && (!x || !y || !z || !ux || !uy || !uz || !q || !m || !id))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "null particle array");
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]) ||
+        !std::isfinite(ux[i]) || !std::isfinite(uy[i]) || !std::isfinite(uz[i]) ||
+        !std::isfinite(q[i]) || !(m[i] > 0.0))
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Particle %zu has a non-finite state or nonpositive mass", i);
+  TRY(reserve_particles(r, n));
+  r->np = 0;
+  const double* src[] = {x, y, z, ux, uy, uz, q, m};
+  double* dst[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
+  for (int k = 0; k < 8; ++k)
+    CUDA_TRY(cudaMemcpy(dst[k], src[k], n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(r->p.id, id, n * 8, cudaMemcpyHostToDevice));
+  r->np = n;
+  if (reset_carriers) r->nc = 0;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_particle_count(const aprl_run* r, size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  *count = r->np;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_get_particles(aprl_run* r, size_t capacity, double* x, double* y, double* z,
+                                   double* ux, double* uy, double* uz, double* q, double* m,
+                                   uint64_t* id, size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (capacity < r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  double* dst[] = {x, y, z, ux, uy, uz, q, m};
+  const double* src[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
+  for (int k = 0; k < 8; ++k)
+    if (dst[k] && r->np) CUDA_TRY(cudaMemcpy(dst[k], src[k], r->np * 8, cudaMemcpyDeviceToHost));
+  if (id && r->np) CUDA_TRY(cudaMemcpy(id, r->p.id, r->np * 8, cudaMemcpyDeviceToHost));
+  *count = r->np;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_carrier_count(const aprl_run* r, size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  *count = r->nc;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_get_carriers(aprl_run* r, size_t capacity, double* pos, double* vel,
+                                  double* q, double* w, size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (capacity < r->nc) return fail(APRL_ERR_INVALID_ARGUMENT, "Carrier buffer too small");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const size_t n = r->nc;
+  std::vector<double> t(n);
+  const double* comps[] = {r->c.px, r->c.py, r->c.pz, r->c.vx, r->c.vy, r->c.vz};
+  for (int k = 0; k < 6; ++k) {
+    double* dst = k < 3 ? pos : vel;
+    if (!dst || !n) continue;
+    CUDA_TRY(cudaMemcpy(t.data(), comps[k], n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) dst[3 * i + (k % 3)] = t[i];
+  }
+  if (q && n) CUDA_TRY(cudaMemcpy(q, r->c.q, n * 8, cudaMemcpyDeviceToHost));
+  if (w && n) CUDA_TRY(cudaMemcpy(w, r->c.w, n * 8, cudaMemcpyDeviceToHost));
+  *count = n;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_set_carriers(aprl_run* r, size_t n, const double* pos, const double* vel,
+                                  const double* q, const double* w) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Carriers can only be replaced between steps");
+  TRY(reserve_carriers(r, n));
+  std::vector<double> t(n);
+  double* comps[] = {r->c.px, r->c.py, r->c.pz, r->c.vx, r->c.vy, r->c.vz};
+  for (int k = 0; k < 6; ++k) {
+    const double* src = k < 3 ? pos : vel;
+    for (size_t i = 0; i < n; ++i) t[i] = src[3 * i + (k % 3)];
+    if (n) CUDA_TRY(cudaMemcpy(comps[k], t.data(), n * 8, cudaMemcpyHostToDevice));
+  }
+  if (n) CUDA_TRY(cudaMemcpy(r->c.q, q, n * 8, cudaMemcpyHostToDevice));
+  if (n) CUDA_TRY(cudaMemcpy(r->c.w, w, n * 8, cudaMemcpyHostToDevice));
+  r->nc = n;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_advance_magnetic(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(do_advance_magnetic(r));
+  return check_device(r);
+}
+
+aprl_status aprl_run_preview_electric(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(do_preview_electric(r));
+  return check_device(r);
+}
+
+aprl_status aprl_run_coupling_trial(aprl_run* r, double residual[4]) {
+  if (!r || !residual) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  return do_trial(r, residual);
+}
+
+aprl_status aprl_run_commit_electric(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(do_commit(r));
+  return check_device(r);
+}
+
+aprl_status aprl_run_shift(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  return do_shift(r);
+}
+
+aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  for (uint32_t n = 0; n < steps; ++n) {
+    TRY(do_advance_magnetic(r));
+    TRY(do_preview_electric(r));
+    bool converged = false;
+    unsigned iterations = 0;
+    double force = 0.0, work = 0.0;
+    for (unsigned t = 0; t < r->cfg.max_trials; ++t) {
+      double res[4];
+      TRY(do_trial(r, res));
+      force = res[0];
+      work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
+      iterations = t + 1;
+      // src/simulation_source_coupling.cpp:50
+      if (iterations >= (res[3] > 0. ? 2u : 1u) && force < r->cfg.force_tolerance &&
+          work < r->cfg.work_tolerance) {
+        converged = true;
+        break;
+      }
+    }
+    if (!converged)
+      return fail(APRL_ERR_NOT_CONVERGED,
+                  "Conservative source coupling failed at step %llu: force=%g work=%g iterations=%u",
+                  (unsigned long long)(r->step + 1), force, work, iterations);
+    r->last_iterations = iterations;
+    r->max_iterations = std::max(r->max_iterations, iterations);
+    r->total_iterations += iterations;
+    r->last_force = force;
+    r->last_work = work;
+    TRY(do_commit(r));
+    TRY(do_shift(r));
+  }
+  return APRL_OK;
+}
+
+aprl_status aprl_run_get_stats(const aprl_run* r, aprl_step_stats* st) {
+  if (!r || !st) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  std::memset(st, 0, sizeof *st);
+  st->step = r->step;
+  st->iterations = r->last_iterations;
+  st->max_iterations = r->max_iterations;
+  st->total_iterations = r->total_iterations;
+  st->force = r->last_force;
+  st->work = r->last_work;
+  st->particles = r->np;
+  st->carriers = r->nc;
+  st->exits = r->cumulative.exits;
+  st->exit_charge = r->cumulative.exit_charge;
+  for (int f = 0; f < 6; ++f) {
+    st->cpml_entries[f] = r->cumulative.cpml[f];
+    st->cpml_entry_charge[f] = r->cumulative.cpml_charge[f];
+    st->carrier_outer[f] = r->cumulative.carrier_outer[f];
+    st->carrier_outer_charge[f] = r->cumulative.carrier_outer_charge[f];
+  }
+  st->cropped_carriers = r->cumulative.cropped;
+  st->cropped_charge = r->cumulative.cropped_charge;
+  st->window_offset = r->offset;
+  st->origin_z = r->origin[2];
+  st->time_box = r->time;
+  st->device_error = r->h_status ? r->h_status->code : 0;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_reset_iteration_stats(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  r->max_iterations = 0;
+  r->total_iterations = 0;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_get_slot_fields(aprl_run* r, size_t capacity, double* used_e, double* used_b,
+                                     double* next_e, double* next_b, size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  *count = r->nslot;
+  if (!used_e && !used_b && !next_e && !next_b) return APRL_OK;
+  if (capacity < r->nslot) return fail(APRL_ERR_INVALID_ARGUMENT, "Slot buffer too small");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  double* dst[] = {used_e, used_b, next_e, next_b};
+  const double* src[] = {r->used_e, r->used_b, r->next_e, r->next_b};
+  for (int k = 0; k < 4; ++k)
+    if (dst[k] && r->nslot) CUDA_TRY(cudaMemcpy(dst[k], src[k], 3 * r->nslot * 8, cudaMemcpyDeviceToHost));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double* out, size_t count,
+                                        int* inside) {
+  if (!r || !out || !inside) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  const aprl_run_config& c = r->cfg;
+  if (count != 6 * c.nx * c.ny) return fail(APRL_ERR_INVALID_ARGUMENT, "Detector buffer size mismatch");
+  // boxZFromLabZAndBoxT (src/boostframe.cpp:231-235) and ownerRank
+  // (src/simulation.cpp:4068-4085).
+  const double box_z = c.box_z_origin + (plane_lab_z - c.lab_z_origin) / c.boost_gamma -
+                       c.boost_beta * kC * r->time;
+  const double coordinate = (box_z - r->origin[2]) / c.dz;
+  const double tolerance = 64.0 * DBL_EPSILON * std::max(1.0, std::abs(coordinate));
+  if (!(box_z < r->origin[2]) && coordinate > static_cast<double>(c.nz) + tolerance) {
+    *inside = 0;
+    return APRL_OK;
+  }
+  *inside = 1;
+  auto axis = [](double lattice, size_t size, int* lower, double* fraction) {
+    if (lattice <= 0.0) { *lower = 0; *fraction = 0.0; }
+    else if (lattice >= static_cast<double>(size - 1)) { *lower = (int)size - 2; *fraction = 1.0; }
+    else { *lower = (int)std::floor(lattice); *fraction = lattice - static_cast<double>(*lower); }
+  };
+  DetectorArgs da{};
+  da.g = make_grid(r);
+  da.frame = make_frame(c);
+  da.origin_xy[0] = c.reference_origin[0];
+  da.origin_xy[1] = c.reference_origin[1];
+  axis(coordinate, c.nz + 1, &da.vertex_lower, &da.vertex_fraction);
+  axis(coordinate - 0.5, c.nz, &da.half_lower, &da.half_fraction);
+  if (r->detector_cap < count) {
+    cudaFree(r->d_detector);
+    TRY(device_alloc(&r->d_detector, count));
+    r->detector_cap = count;
+  }
+  da.out = r->d_detector;
+  TRY(launch(r, kDetectorPlane, detector_plane_kernel,
+             dim3(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), dim3(32, 8), da));
+  CUDA_TRY(cudaMemcpyAsync(out, r->d_detector, count * 8, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_synchronize(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_profile_enable(aprl_run* r, int enabled) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(drain_timings(r));
+  r->profile = enabled != 0;
+  for (unsigned k = 0; k < kKernelCount; ++k) {
+    r->kernel_ms[k] = 0.0;
+    r->kernel_launches[k] = 0;
+  }
+  return APRL_OK;
+}
+
+aprl_status aprl_run_profile_read(aprl_run* r, double* ms, uint64_t* launches, unsigned capacity,
+                                  unsigned* kernels) {
+  if (!r || !kernels) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  TRY(drain_timings(r));
+  *kernels = kKernelCount;
+  for (unsigned k = 0; k < kKernelCount && k < capacity; ++k) {
+    if (ms) ms[k] = r->kernel_ms[k];
+    if (launches) launches[k] = r->kernel_launches[k];
+  }
+  return APRL_OK;
+}
+
+aprl_status aprl_run_launch_count(const aprl_run* r, uint64_t* launches) {
+  if (!r || !launches) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  *launches = r->launches;
+  return APRL_OK;
+}
+
+}  // extern "C"

@@ -29,6 +29,7 @@ _SIGNATURES = {
     "cowan_coefficients": (C.c_int, [C.c_double, C.c_double, C.c_double, _D]),
     "run_destroy": (C.c_int, [_H]),
     "run_set_reference": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
+    "run_set_reference_planes": (C.c_int, [_H, C.c_uint, C.c_uint64, C.c_uint64, _D]),
     "run_set_field": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
     "run_get_field": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
     "run_history_length": (C.c_int, [_H, C.c_uint, _U64]),
@@ -164,6 +165,18 @@ class Run:
         for a, t in enumerate(tables):
             t = np.ascontiguousarray(t, dtype=np.float64)
             self.b("run_set_reference", self.handle, a, _ptr(t), t.size)
+
+    def allocate_reference(self):
+        """Zero-filled device table, to be streamed with set_reference_planes."""
+        for a in range(6):
+            n = int(np.prod(abi.reference_shape(self.config, a)))
+            self.b("run_set_reference", self.handle, a, None, n)
+
+    def set_reference_planes(self, component, first, planes):
+        """planes: array (count, ny_c, nx_c) of native planes from `first`."""
+        a = np.ascontiguousarray(planes, dtype=np.float64)
+        self.b("run_set_reference_planes", self.handle, component, first,
+               a.shape[0], _ptr(a))
 
     def set_field(self, component, array):
         a = np.ascontiguousarray(array, dtype=np.float64)

@@ -195,11 +195,15 @@ def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
     z_hi = 2.0 * cfg.dz + z_fraction[1] * (exit_box - 2.0 * cfg.dz)
     z_center = 0.5 * (z_lo + z_hi)
 
+    if not (x_lo < x_hi and y_lo < y_hi and z_lo < z_hi):
+        raise ValueError("the trusted particle region of this window is empty")
     kept = []
     total = 0
     index = np.uint64(0)
     block = max(4 * count, 4096)
-    while total < count:
+    for _ in range(64):
+        if total >= count:
+            break
         ids = np.arange(int(index), int(index) + block, dtype=np.uint64)
         index = np.uint64(int(index) + block)
         x = sigma_xy * gaussian(seed, ids, 0)
@@ -215,6 +219,8 @@ def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
         sel = np.nonzero(ok)[0][: count - total]
         kept.append((ids[sel], x[sel], y[sel], z[sel], ux[sel], uy[sel], uz[sel]))
         total += sel.size
+    if total < count:
+        raise ValueError("the bunch barely overlaps the trusted particle region")
     cols = [np.concatenate(c) for c in zip(*kept)]
     ids, x, y, z, ux, uy, uz = cols
     u_lab = np.stack([ux, uy, uz], axis=1)

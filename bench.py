@@ -1,0 +1,380 @@
+"""Benchmark of the B200 PIC step on the dipole-radiation workload.
+
+`python bench.py --gpus N --steps K --warmup W` runs one independent run per
+GPU (replicas: a moving-window run does not shard without z-slab halos), W
+untimed steps, then K timed steps bracketed by a barrier and a device
+synchronise, timed with CUDA events on the run's stream; rank 0 prints one
+JSON line.  `--impl reference` times the reference's own CPU translation
+units (oracle/_ref, built from the APRL sources) on the host cores instead.
+
+Workload: 128x128x512 cells (dx = dy = 5 um, dz = 2 um, c dt = dz), 10-cell
+transverse CPML, linear-binomial3, a uniform 1 T lab dipole seen in a
+gamma = 10 boosted frame, and a seeded 1 GeV, 100 pC Gaussian bunch of 1M
+macro-particles (sigma_xy = 50 um, sigma_z = 20 um lab, 1 um emittance,
+1e-4 energy spread) truncated to the window's trusted region.  Fields start
+at zero; the inlet reference is a smooth seeded analytic table.
+"""
+import argparse
+import contextlib
+import csv
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+from aprl_b200 import abi, native, workloads  # noqa: E402
+
+METRIC = "particle-steps/s"
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--particles", type=int, default=1_000_000)
+    p.add_argument("--shape", default="linear-binomial3")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    return p.parse_args(argv)
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+@contextlib.contextmanager
+def clock_sampler(index):
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    proc = None
+    try:
+        proc = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={fields}",
+                                 "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=out, stderr=subprocess.DEVNULL)
+    except OSError:
+        proc = None
+    result = {}
+    try:
+        yield result
+    finally:
+        if proc is not None:
+            proc.terminate()
+            try:
+                proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                proc.kill()
+        out.flush()
+        out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(out.read())) if len(r) >= 9]
+        out.close()
+        os.unlink(out.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, value in zip(names, r[5:9]):
+                if value.strip().lower() == "active":
+                    reasons.add(name)
+        result.update({"sm_mhz": statistics.median(sm) if sm else None,
+                       "sm_max_mhz": max(mx) if mx else None,
+                       "reasons": sorted(reasons), "samples": len(sm)})
+
+
+def algorithmic_bytes(kernel, cfg, particles, carriers):
+    """Unique-state bytes one launch must move (FP64).  Gather/deposit
+    stencil traffic is not counted: it is cache traffic for cell-local
+    particles."""
+    n_cells = cfg.nx * cfg.ny * cfg.nz
+    if kernel == "cowan_magnetic":      # read 3 E, read+write 3 B
+        return 9 * 8 * n_cells
+    if kernel == "electric_preview":    # read 3 E^n and 3 B, write 3 E*
+        return 9 * 8 * n_cells
+    if kernel == "electric_commit":     # read E* and J, write E
+        return 9 * 8 * n_cells
+    if kernel == "push_deposit":        # read x,u,q,m,nextE/B; write x1,u1,usedE/B,work,flags
+        return particles * (64 + 48 + 48 + 48 + 8 + 2)
+    if kernel == "residual":            # read x0,x1,q,m,usedE/B,work; write nextE/B
+        return particles * (48 + 16 + 48 + 8 + 48)
+    if kernel == "carrier":             # read + write 8 words
+        return carriers * 128
+    return None
+
+
+# ---------------------------------------------------------------------------
+def reference_planes_for_step(cfg, step):
+    """Native reference z planes the inlet queries of one step touch:
+    begin (offset-1, step), preview (offset, step+1), shift (offset-1, step+1)."""
+    offset = cfg.initial_offset - step
+    zs = [offset - 1 - cfg.translation_beta * step,
+          offset - cfg.translation_beta * (step + 1),
+          offset - 1 - cfg.translation_beta * (step + 1)]
+    lo = max(0, int(math.floor(min(zs))))
+    hi = int(math.floor(max(zs))) + 1
+    return lo, hi
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    K, W = args.steps, args.warmup
+    total_steps = W + 2 * K + 4
+    w = workloads.dipole_c2(steps=total_steps, particles=args.particles, shape=args.shape,
+                            seed=17 + rank)
+    cfg = w.config
+    lib = native.load()
+    run = native.Run(lib, cfg, stream=stream.cuda_stream)
+    run.set_reference(w.reference)
+    run.set_particles(w.particles)
+
+    for _ in range(W):
+        run.step(1)
+    run.synchronize()
+    run.b("run_reset_iteration_stats", run.handle)
+
+    # ---- device-resident timed region ------------------------------------
+    launches0 = run.launch_count()
+    run.profile_enable(True)
+    particle_steps = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clock_sampler(local) as clocks:
+        start.record(stream)
+        for _ in range(K):
+            particle_steps += run.particle_count()
+            run.step(1)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    elapsed_ms = start.elapsed_time(stop)
+    if world > 1:
+        dist.barrier()
+    profile = run.profile_read()
+    run.profile_enable(False)
+    launches = run.launch_count() - launches0
+    stats = run.stats()
+
+    # ---- end to end through the C ABI with host buffers -------------------
+    pinned = {}
+    for a in range(6):
+        nx_c, ny_c, _ = abi.reference_shape(cfg, a)
+        pinned[a] = torch.empty((4, ny_c, nx_c), dtype=torch.float64, pin_memory=True).numpy()
+    detector = torch.empty((cfg.ny, cfg.nx, 6), dtype=torch.float64, pin_memory=True).numpy()
+    detector_lab_z = cfg.boost_gamma * (0.5 * cfg.nz * cfg.dz)
+    e2e_particle_steps, h2d, d2h = 0, 0, 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    e_start.record(stream)
+    for _ in range(K):
+        step = run.stats()["step"]
+        lo, hi = reference_planes_for_step(cfg, step)
+        for a in range(6):
+            planes = w.reference[a][lo:hi + 1]
+            buf = pinned[a][:planes.shape[0]]
+            np.copyto(buf, planes)
+            run.set_reference_planes(a, lo, buf)
+            h2d += buf.nbytes
+        e2e_particle_steps += run.particle_count()
+        run.step(1)
+        out = np.empty(cfg.nx * cfg.ny * 6)
+        inside = __import__("ctypes").c_int()
+        run.b("run_sample_field_plane", run.handle, detector_lab_z,
+              detector.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)),
+              detector.size, __import__("ctypes").byref(inside))
+        d2h += detector.nbytes + 8 * 24  # plane + stats block
+        run.stats()
+    e_stop.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e_start.elapsed_time(e_stop)
+    e2e_wall_ms = (time.perf_counter() - wall0) * 1e3
+
+    # max over ranks, totals over ranks
+    vals = torch.tensor([elapsed_ms, e2e_ms, float(particle_steps), float(e2e_particle_steps)],
+                        dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = vals.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = vals.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        elapsed_ms, e2e_ms = mx[0].item(), mx[1].item()
+        particle_steps, e2e_particle_steps = int(sm[2].item()), int(sm[3].item())
+    run.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    value = particle_steps / (elapsed_ms * 1e-3)
+    e2e_value = e2e_particle_steps / (e2e_ms * 1e-3)
+    peak, peak_kind = measured_peaks()
+    dominant = max(profile.items(), key=lambda kv: kv[1][0]) if profile else None
+    roofline = None
+    if dominant:
+        name, (ms, count) = dominant
+        per_launch_ms = ms / max(count, 1)
+        mean_particles = particle_steps / max(K, 1)
+        algo = algorithmic_bytes(name, cfg, mean_particles, stats["carriers"])
+        achieved = algo / (per_launch_ms * 1e-3) / 1e9 if algo else None
+        roofline = {"bound": "hbm", "kernel": name,
+                    "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": (achieved / peak) if achieved else None,
+                    "peak_source": peak_kind, "traffic": None,
+                    "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
+                    "launches": count}
+    kernels = {k: {"ms": v[0], "launches": v[1],
+                   "share": v[0] / max(sum(x[0] for x in profile.values()), 1e-12)}
+               for k, v in profile.items()}
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": elapsed_ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian bunch, analytic inlet reference)",
+        "config": {"workload": w.name, "cells": [cfg.nx, cfg.ny, cfg.nz],
+                   "particles": args.particles, "shape": args.shape,
+                   "precision": "fp64-drop-in", "magnet": "uniform 1 T lab dipole",
+                   "boost_gamma": cfg.boost_gamma, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (fields + particles > 126 MB)"},
+        "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
+                               "max": stats["max_iterations"]},
+        "particles_end": stats["particles"], "carriers_end": stats["carriers"],
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": h2d // max(K, 1),
+                "d2h_bytes_per_step": d2h // max(K, 1),
+                "wall_ms_per_step": e2e_wall_ms / K},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "kernels": kernels,
+        "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
+                   "reasons": clocks.get("reasons", [])},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def reference_sample_workload(args, steps, seed=17):
+    """A bounded slice of the benchmark workload for the CPU: the full
+    transverse grid and 1/8 of the window length with 1/8 of the particles
+    (same particles per cell)."""
+    cfg = workloads.make_config(128, 128, 64, 5e-6, 5e-6, 2e-6, 10, 10.0, args.shape,
+                                steps, magnets=[workloads.dipole(1.0)], right_margin=8)
+    bunch = workloads.gaussian_bunch(cfg, max(args.particles // 8, 1), 100e-12 / 8, 1e9,
+                                     50e-6, 20e-6, 1e-6, 1e-4, seed=seed,
+                                     z_fraction=(0.05, 0.95))
+    return workloads.Workload("dipole-slice-128x128x64", cfg, bunch,
+                              workloads.synthetic_reference(cfg), steps=steps)
+
+
+def _cpu_checker():
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import checkers
+    if checkers.reference_available():
+        b = checkers.reference()
+        b.lib.ref_set_threads(os.cpu_count() or 1)
+        return b, "reference", os.cpu_count() or 1
+    return checkers.oracle(), "port", 1
+
+
+def cpu_baseline(args):
+    binding, kind, cores = _cpu_checker()
+    steps = 3
+    w = reference_sample_workload(args, steps + 1)
+    run = native.Run(binding, w.config).load_workload(w)
+    done, ps, t0 = 0, 0, time.perf_counter()
+    while done < steps:
+        ps += run.particle_count()
+        run.step(1)
+        done += 1
+        if time.perf_counter() - t0 > args.cpu_sample_seconds:
+            break
+    elapsed = time.perf_counter() - t0
+    run.close()
+    return {"value": ps / elapsed, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{done} steps of a 128x128x64-cell slice with "
+                      f"{w.particles['x'].size} particles (1/8 of the window and bunch)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    binding, kind, cores = _cpu_checker()
+    K, W = args.steps, args.warmup
+    w = reference_sample_workload(args, K + W + 2)
+    run = native.Run(binding, w.config).load_workload(w)
+    for _ in range(W):
+        run.step(1)
+    ps = 0
+    t0 = time.perf_counter()
+    for _ in range(K):
+        ps += run.particle_count()
+        run.step(1)
+    elapsed = time.perf_counter() - t0
+    stats = run.stats()
+    run.close()
+    value = ps / elapsed
+    sample = (f"each step: one reference step of a 128x128x64-cell slice with "
+              f"{w.particles['x'].size} particles (1/8 of the window and bunch)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K, "warmup": W,
+        "ms_per_step": elapsed * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "dipole-128x128x512", "sample": w.name,
+                   "shape": args.shape, "precision": "fp64"},
+        "fixed_point_trials": {"mean": stats["total_iterations"] / max(K + W, 1),
+                               "max": stats["max_iterations"]},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -175,6 +175,14 @@ aprl_status aprl_run_destroy(aprl_run* run);
  * (nx, ny, reference_nz) cells.  Copied to the device once. */
 aprl_status aprl_run_set_reference(aprl_run* run, unsigned component,
                                    const double* host, size_t count);
+/* Streaming form of the same supply, the counterpart of the reference's
+ * bounded block reader (src/blocked_cowan_reference.h:59-98): when
+ * aprl_run_set_reference was given host == NULL the table is allocated
+ * zero-filled, and this call overwrites `planes` native z planes starting at
+ * `first_plane` of one component (host holds planes*nx_c*ny_c doubles). */
+aprl_status aprl_run_set_reference_planes(aprl_run* run, unsigned component,
+                                          uint64_t first_plane, uint64_t planes,
+                                          const double* host);
 
 /* EBFieldGrid component accessors (src/eb_field.h:211-229).  component
  * 0..8 = Ex,Ey,Ez,Bx,By,Bz,Jx,Jy,Jz, logical (window) indexing. */
