@@ -19,11 +19,17 @@ struct DRegion {
   double order;           // polynomial order of the grading
 };
 
-// Particle SoA (RelativisticParticleSI without the diagnostics).
+// Particle SoA (RelativisticParticleSI without the diagnostics).  Storage
+// is sorted by 4x4x4 cell tiles for gather/deposit locality; `order` keeps
+// each particle's rank in the reference's list order, which the ABI
+// restores on read-out.
 struct DParticles {
   double *x, *y, *z, *ux, *uy, *uz, *q, *m;
   unsigned long long* id;
+  unsigned long long* order;
 };
+
+constexpr int kTileShift = 2;  // 4 cells per tile edge
 
 struct DCarriers {
   double *px, *py, *pz, *vx, *vy, *vz, *q, *w;
@@ -125,6 +131,17 @@ __global__ void gather_carriers_kernel(DCarriers out, DCarriers src,
                                        const unsigned char* flag, unsigned char want,
                                        long long n, const unsigned* block_offset,
                                        unsigned long long base);
+// Counting sort of the particle storage by cell tile.
+__global__ void tile_count_kernel(DParticles p, long long n, DGrid g, int tiles_x,
+                                  int tiles_y, int tiles_z, unsigned* tile_count,
+                                  unsigned* tile_of, unsigned* rank_in_tile);
+__global__ void chunk_scan_kernel(const unsigned* in, long long n, unsigned* out,
+                                  unsigned* chunk_sum);
+__global__ void chunk_add_kernel(unsigned* data, long long n, const unsigned* chunk_offset);
+__global__ void scatter_particles_kernel(DParticles out, DParticles src, long long n,
+                                         const unsigned* tile_of,
+                                         const unsigned* rank_in_tile,
+                                         const unsigned* tile_offset);
 __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
                                   double lower, unsigned char* keep,
                                   TrialCounters* counters, DeviceStatus* status);

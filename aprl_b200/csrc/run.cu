@@ -52,6 +52,7 @@ enum Kernel : unsigned {
   kInletLower, kCowanMagnetic, kElectricPreview, kCarrier, kPushDeposit,
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
+  kTileCount, kChunkScan, kChunkAdd, kScatterParticles,
   kKernelCount
 };
 
@@ -59,7 +60,8 @@ const char* kKernelNames[kKernelCount] = {
   "inlet_lower", "cowan_magnetic", "electric_preview", "carrier",
   "push_deposit", "residual", "electric_commit", "flag_count",
   "block_offset_scan", "gather_particles", "gather_carriers",
-  "shift_insert", "crop_flags", "inlet_check", "detector_plane"};
+  "shift_insert", "crop_flags", "inlet_check", "detector_plane",
+  "tile_count", "chunk_scan", "chunk_add", "scatter_particles"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -229,6 +231,13 @@ struct aprl_run {
   DCarriers born{};
   unsigned char* born_keep = nullptr;
   size_t nslot = 0;
+  unsigned long long* slot_order = nullptr;  // p.order at the last preview
+  unsigned long long next_order = 0;
+  // tile sort scratch
+  unsigned *tile_count = nullptr, *tile_offset = nullptr, *tile_of = nullptr,
+           *tile_rank = nullptr, *chunk_sum = nullptr, *chunk_offset = nullptr;
+  size_t ntiles = 0;
+  int tiles[3]{};
   // carriers
   size_t nc = 0, ccap = 0;
   DCarriers c{}, c_alt{}, c_out{};
@@ -455,11 +464,12 @@ aprl_status alloc_particles(DParticles& p, size_t n) {
   TRY(device_alloc(&p.x, n)); TRY(device_alloc(&p.y, n)); TRY(device_alloc(&p.z, n));
   TRY(device_alloc(&p.ux, n)); TRY(device_alloc(&p.uy, n)); TRY(device_alloc(&p.uz, n));
   TRY(device_alloc(&p.q, n)); TRY(device_alloc(&p.m, n)); TRY(device_alloc(&p.id, n));
+  TRY(device_alloc(&p.order, n));
   return APRL_OK;
 }
 void free_particles(DParticles& p) {
   cudaFree(p.x); cudaFree(p.y); cudaFree(p.z); cudaFree(p.ux); cudaFree(p.uy);
-  cudaFree(p.uz); cudaFree(p.q); cudaFree(p.m); cudaFree(p.id);
+  cudaFree(p.uz); cudaFree(p.q); cudaFree(p.m); cudaFree(p.id); cudaFree(p.order);
   p = DParticles{};
 }
 aprl_status alloc_carriers(DCarriers& c, size_t n) {
@@ -491,6 +501,7 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
     CUDA_TRY(cudaMemcpy(np.q, r->p.q, r->np * 8, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.m, r->p.m, r->np * 8, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.id, r->p.id, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice));
   }
   free_particles(r->p);
   free_particles(r->p_alt);
@@ -508,8 +519,14 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   }
   cudaFree(r->action);
   cudaFree(r->born_keep);
+  cudaFree(r->slot_order);
+  cudaFree(r->tile_of);
+  cudaFree(r->tile_rank);
   TRY(device_alloc(&r->action, n));
   TRY(device_alloc(&r->born_keep, n));
+  TRY(device_alloc(&r->slot_order, n));
+  TRY(device_alloc(&r->tile_of, n));
+  TRY(device_alloc(&r->tile_rank, n));
   free_carriers(r->born);
   TRY(alloc_carriers(r->born, n));
   r->pcap = n;
@@ -621,6 +638,29 @@ aprl_status compact_count(aprl_run* r, const unsigned char* flag, unsigned char 
   return APRL_OK;
 }
 
+// Counting sort of the particle storage by 4x4x4 cell tiles
+// (tile_count -> chunked exclusive scan -> scatter).
+aprl_status sort_particles(aprl_run* r) {
+  if (r->np == 0) return APRL_OK;
+  const long long n = (long long)r->np;
+  const DGrid g = make_grid(r);
+  CUDA_TRY(cudaMemsetAsync(r->tile_count, 0, r->ntiles * sizeof(unsigned), r->stream));
+  TRY(launch(r, kTileCount, tile_count_kernel, dim3(blocks_for(r->np, 256)), dim3(256), r->p, n, g,
+             r->tiles[0], r->tiles[1], r->tiles[2], r->tile_count, r->tile_of, r->tile_rank));
+  const unsigned chunks = blocks_for(r->ntiles, 1024);
+  TRY(launch(r, kChunkScan, chunk_scan_kernel, dim3(chunks), dim3(1024),
+             (const unsigned*)r->tile_count, (long long)r->ntiles, r->tile_offset, r->chunk_sum));
+  TRY(launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
+             (const unsigned*)r->chunk_sum, (int)chunks, r->chunk_offset, r->scan_total));
+  TRY(launch(r, kChunkAdd, chunk_add_kernel, dim3(chunks), dim3(1024), r->tile_offset,
+             (long long)r->ntiles, (const unsigned*)r->chunk_offset));
+  TRY(launch(r, kScatterParticles, scatter_particles_kernel, dim3(blocks_for(r->np, 256)),
+             dim3(256), r->p_alt, r->p, n, (const unsigned*)r->tile_of,
+             (const unsigned*)r->tile_rank, (const unsigned*)r->tile_offset));
+  std::swap(r->p, r->p_alt);
+  return APRL_OK;
+}
+
 aprl_status do_advance_magnetic(aprl_run* r) {
   if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
   const aprl_run_config& c = r->cfg;
@@ -664,6 +704,9 @@ aprl_status do_preview_electric(aprl_run* r) {
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel, grid3(c, block), block, pa));
+  if (r->np)
+    CUDA_TRY(cudaMemcpyAsync(r->slot_order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice,
+                             r->stream));
   r->nslot = r->np;
   r->trials = 0;
   r->stage = 2;
@@ -806,6 +849,7 @@ aprl_status do_commit(aprl_run* r) {
                (long long)r->np, (const unsigned*)r->scan_offset));
     std::swap(r->p, r->p_alt);
     r->np = kept;
+    TRY(sort_particles(r));
   }
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   add_counters(r->cumulative, *r->h_counters);
@@ -973,6 +1017,15 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     if ((s = device_alloc(&hb.data, hb.length())) != APRL_OK) return cleanup(s);
     cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * 8, r->stream);
   }
+  for (int a = 0; a < 3; ++a) {
+    const uint64_t cells = a == 0 ? c.nx : (a == 1 ? c.ny : c.nz);
+    r->tiles[a] = (int)((cells + (1u << kTileShift) - 1) >> kTileShift);
+  }
+  r->ntiles = (size_t)r->tiles[0] * r->tiles[1] * r->tiles[2];
+  if ((s = device_alloc(&r->tile_count, r->ntiles)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->tile_offset, r->ntiles)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->chunk_sum, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(&r->chunk_offset, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(&r->d_counters, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(&r->d_sums, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(&r->d_status, 1)) != APRL_OK) return cleanup(s);
@@ -1019,6 +1072,13 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   for (double* d : singles) cudaFree(d);
   cudaFree(r->action);
   cudaFree(r->born_keep);
+  cudaFree(r->slot_order);
+  cudaFree(r->tile_of);
+  cudaFree(r->tile_rank);
+  cudaFree(r->tile_count);
+  cudaFree(r->tile_offset);
+  cudaFree(r->chunk_sum);
+  cudaFree(r->chunk_offset);
   free_carriers(r->born);
   free_carriers(r->c);
   free_carriers(r->c_alt);
@@ -1153,8 +1213,14 @@ aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const
   for (int k = 0; k < 8; ++k)
     CUDA_TRY(cudaMemcpy(dst[k], src[k], n * 8, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(r->p.id, id, n * 8, cudaMemcpyHostToDevice));
+  std::vector<unsigned long long> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = i;
+  if (n) CUDA_TRY(cudaMemcpy(r->p.order, order.data(), n * 8, cudaMemcpyHostToDevice));
+  r->next_order = n;
   r->np = n;
   if (reset_carriers) r->nc = 0;
+  TRY(sort_particles(r));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;
 }
 
@@ -1164,18 +1230,40 @@ aprl_status aprl_run_particle_count(const aprl_run* r, size_t* count) {
   return APRL_OK;
 }
 
+// Storage is tile-sorted; read-out restores the reference's list order.
+static aprl_status storage_permutation(aprl_run* r, const unsigned long long* device_order,
+                                       size_t n, std::vector<size_t>& perm) {
+  std::vector<unsigned long long> order(n);
+  if (n) CUDA_TRY(cudaMemcpy(order.data(), device_order, n * 8, cudaMemcpyDeviceToHost));
+  perm.resize(n);
+  for (size_t i = 0; i < n; ++i) perm[i] = i;
+  std::sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return order[a] < order[b]; });
+  return APRL_OK;
+}
+
 aprl_status aprl_run_get_particles(aprl_run* r, size_t capacity, double* x, double* y, double* z,
                                    double* ux, double* uy, double* uz, double* q, double* m,
                                    uint64_t* id, size_t* count) {
   if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
   if (capacity < r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const size_t n = r->np;
+  std::vector<size_t> perm;
+  TRY(storage_permutation(r, r->p.order, n, perm));
+  std::vector<double> t(n);
   double* dst[] = {x, y, z, ux, uy, uz, q, m};
   const double* src[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
-  for (int k = 0; k < 8; ++k)
-    if (dst[k] && r->np) CUDA_TRY(cudaMemcpy(dst[k], src[k], r->np * 8, cudaMemcpyDeviceToHost));
-  if (id && r->np) CUDA_TRY(cudaMemcpy(id, r->p.id, r->np * 8, cudaMemcpyDeviceToHost));
-  *count = r->np;
+  for (int k = 0; k < 8; ++k) {
+    if (!dst[k] || !n) continue;
+    CUDA_TRY(cudaMemcpy(t.data(), src[k], n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) dst[k][i] = t[perm[i]];
+  }
+  if (id && n) {
+    std::vector<uint64_t> ids(n);
+    CUDA_TRY(cudaMemcpy(ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) id[i] = ids[perm[i]];
+  }
+  *count = n;
   return APRL_OK;
 }
 
@@ -1329,10 +1417,18 @@ aprl_status aprl_run_get_slot_fields(aprl_run* r, size_t capacity, double* used_
   if (!used_e && !used_b && !next_e && !next_b) return APRL_OK;
   if (capacity < r->nslot) return fail(APRL_ERR_INVALID_ARGUMENT, "Slot buffer too small");
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const size_t n = r->nslot;
+  std::vector<size_t> perm;
+  TRY(storage_permutation(r, r->slot_order, n, perm));
+  std::vector<double> t(3 * n);
   double* dst[] = {used_e, used_b, next_e, next_b};
   const double* src[] = {r->used_e, r->used_b, r->next_e, r->next_b};
-  for (int k = 0; k < 4; ++k)
-    if (dst[k] && r->nslot) CUDA_TRY(cudaMemcpy(dst[k], src[k], 3 * r->nslot * 8, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 4; ++k) {
+    if (!dst[k] || !n) continue;
+    CUDA_TRY(cudaMemcpy(t.data(), src[k], 3 * n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) dst[k][3 * i + d] = t[3 * perm[i] + d];
+  }
   return APRL_OK;
 }
 
