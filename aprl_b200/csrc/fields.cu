@@ -72,61 +72,132 @@ __device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, in
 }
 
 // advanceMagneticCowan (src/eb_field.cpp:488-558) fused with
-// EBConvolutionalPML::afterMagneticUpdate (src/eb_cpml.cpp:406-468): each B
-// node is updated by the curl, then by its CPML terms in the reference's
-// term order (0,2,1), (1,2,0), (2,1,0), (2,0,1); the CPML difference is the
-// same smoothed difference the curl used.
-__global__ void cowan_magnetic_kernel(CowanArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+// EBConvolutionalPML::afterMagneticUpdate (src/eb_cpml.cpp:406-468).
+//
+// A block owns a TX x TY tile of (i, j) columns and marches a chunk of z
+// planes.  The three E components of planes k-1, k, k+1 live in a shared
+// memory ring, one (TX+2) x (TY+2) tile each, loaded once per plane through
+// electricValue's parity/halo rules.  Every smoothed difference is then
+// evaluated from shared memory with the reference's 9-point order, so the
+// update is bit-identical to the reference.  Each B node is updated by the
+// curl, then by its CPML terms in the reference's term order (0,2,1),
+// (1,2,0), (2,1,0), (2,0,1), reusing the curl's smoothed difference.
+constexpr int kTX = 32, kTY = 8, kKChunk = 16;
+
+struct ETile {
+  double v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
+};
+
+__device__ __forceinline__ int plane_slot(int k) { return ((k % 3) + 3) % 3; }
+
+__device__ __forceinline__ double tile_at(const ETile& t, int c, int i, int j, int k,
+                                          int i0, int j0) {
+  return t.v[c][plane_slot(k)][j - j0 + 1][i - i0 + 1];
+}
+
+__device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs& a, int c,
+                                                int d, int i, int j, int k, int i0, int j0) {
+  const int ta = (d + 1) % 3, tb = (d + 2) % 3;
+  const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
+  const int p[3] = {i, j, k};
+  double result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
+#pragma unroll
+  for (int dir = -1; dir <= 1; dir += 2) {
+    int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
+    qa[ta] += dir;
+    qb[tb] += dir;
+    result += a.beta[ta] * tile_at(t, c, qa[0], qa[1], qa[2], i0, j0);
+    result += a.beta[tb] * tile_at(t, c, qb[0], qb[1], qb[2], i0, j0);
+  }
+#pragma unroll
+  for (int da = -1; da <= 1; da += 2)
+#pragma unroll
+    for (int db = -1; db <= 1; db += 2) {
+      int q[3] = {p[0], p[1], p[2]};
+      q[ta] += da;
+      q[tb] += db;
+      result += delta * tile_at(t, c, q[0], q[1], q[2], i0, j0);
+    }
+  return result;
+}
+
+// Fills one plane of the tile.  Only coordinates within one cell of a
+// component's index range are ever read by the smoothing (the reference's
+// own reach); tile points farther out, which exist only where a small grid
+// ends inside a tile, are stored as zero and never used.
+__device__ __forceinline__ void load_plane(ETile& t, const CowanArgs& a, int k, int i0, int j0) {
+  const int slot = plane_slot(k);
+  constexpr int W = kTX + 2, H = kTY + 2, N = W * H;
+  for (int c = 0; c < 3; ++c) {
+    const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1);
+    for (int n = threadIdx.y * kTX + threadIdx.x; n < N; n += kTX * kTY) {
+      const int ii = n % W, jj = n / W;
+      const int i = i0 - 1 + ii, j = j0 - 1 + jj;
+      t.v[c][slot][jj][ii] = (i < -1 || i > nxc || j < -1 || j > nyc)
+                                 ? 0.0 : electric_value(a, c, i, j, k);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs a) {
+  __shared__ ETile t;
   const DGrid& g = a.g;
-  if (i > g.nx || j > g.ny || k > g.nz) return;
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kKChunk;
+  const int k1 = min(k0 + kKChunk, g.nz + 1);
   const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
-  if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
-    const double dEzDy = smoothed(a, 2, 1, i, j + 1, k) - smoothed(a, 2, 1, i, j, k);
-    const double dEyDz = smoothed(a, 1, 2, i, j, k + 1) - smoothed(a, 1, 2, i, j, k);
-    double* bx = &g.b[0][b_index(g, 0, i, j, k)];
-    double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
-    const int s = a.my.ordinal[j];
-    if (s >= 0) {
-      const double corr = cpml_correction(a.my, j, dEzDy,
-                                          history_at(a.h[0], s, k, g.zb_b[0], i));
-      v += -1.0 * dtdy * corr;
+  load_plane(t, a, k0 - 1, i0, j0);
+  load_plane(t, a, k0, i0, j0);
+  for (int k = k0; k < k1; ++k) {
+    load_plane(t, a, k + 1, i0, j0);
+    __syncthreads();
+    if (i <= g.nx && j <= g.ny) {
+      if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
+        const double dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
+                             tile_smoothed(t, a, 2, 1, i, j, k, i0, j0);
+        const double dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
+                             tile_smoothed(t, a, 1, 2, i, j, k, i0, j0);
+        double* bx = &g.b[0][b_index(g, 0, i, j, k)];
+        double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
+        const int s = a.my.ordinal[j];
+        if (s >= 0)
+          v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
+                                             history_at(a.h[0], s, k, g.zb_b[0], i));
+        *bx = v;
+      }
+      if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
+        const double dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
+                             tile_smoothed(t, a, 0, 2, i, j, k, i0, j0);
+        const double dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
+                             tile_smoothed(t, a, 2, 0, i, j, k, i0, j0);
+        double* by = &g.b[1][b_index(g, 1, i, j, k)];
+        double v = *by - (dtdz * dExDz - dtdx * dEzDx);
+        const int s = a.mx.ordinal[i];
+        if (s >= 0)
+          v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
+                                            history_at(a.h[1], s, k, g.zb_b[1], j));
+        *by = v;
+      }
+      if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
+        const double dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
+                             tile_smoothed(t, a, 1, 0, i, j, k, i0, j0);
+        const double dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
+                             tile_smoothed(t, a, 0, 1, i, j, k, i0, j0);
+        double* bz = &g.b[2][b_index(g, 2, i, j, k)];
+        double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
+        const int sx = a.mx.ordinal[i];
+        if (sx >= 0)
+          v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,
+                                             history_at(a.h[2], sx, k, g.zb_b[2], j));
+        const int sy = a.my.ordinal[j];
+        if (sy >= 0)
+          v += 1.0 * dtdy * cpml_correction(a.my, j, dExDy,
+                                            history_at(a.h[3], sy, k, g.zb_b[2], i));
+        *bz = v;
+      }
     }
-    *bx = v;
-  }
-  if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
-    const double dExDz = smoothed(a, 0, 2, i, j, k + 1) - smoothed(a, 0, 2, i, j, k);
-    const double dEzDx = smoothed(a, 2, 0, i + 1, j, k) - smoothed(a, 2, 0, i, j, k);
-    double* by = &g.b[1][b_index(g, 1, i, j, k)];
-    double v = *by - (dtdz * dExDz - dtdx * dEzDx);
-    const int s = a.mx.ordinal[i];
-    if (s >= 0) {
-      const double corr = cpml_correction(a.mx, i, dEzDx,
-                                          history_at(a.h[1], s, k, g.zb_b[1], j));
-      v += 1.0 * dtdx * corr;
-    }
-    *by = v;
-  }
-  if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
-    const double dEyDx = smoothed(a, 1, 0, i + 1, j, k) - smoothed(a, 1, 0, i, j, k);
-    const double dExDy = smoothed(a, 0, 1, i, j + 1, k) - smoothed(a, 0, 1, i, j, k);
-    double* bz = &g.b[2][b_index(g, 2, i, j, k)];
-    double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
-    const int sx = a.mx.ordinal[i];
-    if (sx >= 0) {
-      const double corr = cpml_correction(a.mx, i, dEyDx,
-                                          history_at(a.h[2], sx, k, g.zb_b[2], j));
-      v += -1.0 * dtdx * corr;
-    }
-    const int sy = a.my.ordinal[j];
-    if (sy >= 0) {
-      const double corr = cpml_correction(a.my, j, dExDy,
-                                          history_at(a.h[3], sy, k, g.zb_b[2], i));
-      v += 1.0 * dtdy * corr;
-    }
-    *bz = v;
+    __syncthreads();
   }
 }
 

@@ -700,6 +700,7 @@ __global__ void carrier_kernel(CarrierArgs a) {
   a.out.vx[n] = c.vel[0]; a.out.vy[n] = c.vel[1]; a.out.vz[n] = c.vel[2];
   a.out.q[n] = c.q;
   a.out.w[n] = c.w;
+  a.out.key[n] = a.in.key[n];
 }
 
 // One fixed-point trial of one active particle: ConservativeSourceCoupling::
@@ -839,6 +840,7 @@ __global__ void push_deposit_kernel(PushArgs a) {
     a.born.vx[n] = born.vel[0]; a.born.vy[n] = born.vel[1]; a.born.vz[n] = born.vel[2];
     a.born.q[n] = born.q;
     a.born.w[n] = born.w;
+    a.born.key[n] = a.key_base | (a.p.order[n] & 0xffffffffull);
   }
 }
 
@@ -1012,6 +1014,7 @@ __global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsig
   out.vx[slot] = src.vx[i]; out.vy[slot] = src.vy[i]; out.vz[slot] = src.vz[i];
   out.q[slot] = src.q[i];
   out.w[slot] = src.w[i];
+  out.key[slot] = src.key[i];
 }
 
 // ---------------------------------------------------------------------------

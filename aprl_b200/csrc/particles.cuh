@@ -31,8 +31,13 @@ struct DParticles {
 
 constexpr int kTileShift = 2;  // 4 cells per tile edge
 
+// CPML carriers.  `key` = (birth step + 1) << 32 | rank of the parent in
+// the particle list, so sorting by key restores the reference's carrier
+// order (survivors first, then newborns in particle order); storage order
+// is free.
 struct DCarriers {
   double *px, *py, *pz, *vx, *vy, *vz, *q, *w;
+  unsigned long long* key;
 };
 
 // Per-trial counters of the boundary bookkeeping (src/simulation.cpp:
@@ -78,6 +83,7 @@ struct PushArgs {
   double* abs_grid_work; // sum over substeps of |grid work|
   unsigned char* action; // 0 retain, 1 CPML/exit carrier, 2 outer exit
   DCarriers born;        // carrier created by a CPML entry (when kept)
+  unsigned long long key_base;  // (step + 1) << 32 for newborn carrier keys
   unsigned char* born_keep;
   TrialCounters* counters;
   DeviceStatus* status;

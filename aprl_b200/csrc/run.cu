@@ -475,12 +475,12 @@ void free_particles(DParticles& p) {
 aprl_status alloc_carriers(DCarriers& c, size_t n) {
   TRY(device_alloc(&c.px, n)); TRY(device_alloc(&c.py, n)); TRY(device_alloc(&c.pz, n));
   TRY(device_alloc(&c.vx, n)); TRY(device_alloc(&c.vy, n)); TRY(device_alloc(&c.vz, n));
-  TRY(device_alloc(&c.q, n)); TRY(device_alloc(&c.w, n));
+  TRY(device_alloc(&c.q, n)); TRY(device_alloc(&c.w, n)); TRY(device_alloc(&c.key, n));
   return APRL_OK;
 }
 void free_carriers(DCarriers& c) {
   cudaFree(c.px); cudaFree(c.py); cudaFree(c.pz); cudaFree(c.vx); cudaFree(c.vy);
-  cudaFree(c.vz); cudaFree(c.q); cudaFree(c.w);
+  cudaFree(c.vz); cudaFree(c.q); cudaFree(c.w); cudaFree(c.key);
   c = DCarriers{};
 }
 
@@ -539,6 +539,7 @@ aprl_status copy_carriers(DCarriers& dst, const DCarriers& src, size_t n) {
   double* d[] = {dst.px, dst.py, dst.pz, dst.vx, dst.vy, dst.vz, dst.q, dst.w};
   for (int k = 0; k < 8; ++k)
     CUDA_TRY(cudaMemcpy(d[k], s[k], n * 8, cudaMemcpyDeviceToDevice));
+  CUDA_TRY(cudaMemcpy(dst.key, src.key, n * 8, cudaMemcpyDeviceToDevice));
   return APRL_OK;
 }
 
@@ -687,8 +688,10 @@ aprl_status do_advance_magnetic(aprl_run* r) {
   ca.mx = r->mprof[0].view();
   ca.my = r->mprof[1].view();
   for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
-  const dim3 block(32, 4);
-  TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel, grid3(c, block), block, ca));
+  // 32x8 column tiles, 16-plane z chunks (kTX, kTY, kKChunk in fields.cu).
+  const dim3 cblock(32, 8);
+  const dim3 cgrid(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), blocks_for(c.nz + 1, 16));
+  TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel, cgrid, cblock, ca));
   r->stage = 1;
   return APRL_OK;
 }
@@ -774,6 +777,7 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     pa.action = r->action;
     pa.born = r->born;
     pa.born_keep = r->born_keep;
+    pa.key_base = (unsigned long long)(r->step + 1) << 32;
     pa.counters = r->d_counters;
     pa.status = r->d_status;
     TRY(launch(r, kPushDeposit, push_deposit_kernel, dim3(blocks_for(r->np, 128)), dim3(128), pa));
@@ -1279,16 +1283,23 @@ aprl_status aprl_run_get_carriers(aprl_run* r, size_t capacity, double* pos, dou
   if (capacity < r->nc) return fail(APRL_ERR_INVALID_ARGUMENT, "Carrier buffer too small");
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   const size_t n = r->nc;
+  std::vector<size_t> perm;
+  TRY(storage_permutation(r, r->c.key, n, perm));
   std::vector<double> t(n);
   const double* comps[] = {r->c.px, r->c.py, r->c.pz, r->c.vx, r->c.vy, r->c.vz};
   for (int k = 0; k < 6; ++k) {
     double* dst = k < 3 ? pos : vel;
     if (!dst || !n) continue;
     CUDA_TRY(cudaMemcpy(t.data(), comps[k], n * 8, cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < n; ++i) dst[3 * i + (k % 3)] = t[i];
+    for (size_t i = 0; i < n; ++i) dst[3 * i + (k % 3)] = t[perm[i]];
   }
-  if (q && n) CUDA_TRY(cudaMemcpy(q, r->c.q, n * 8, cudaMemcpyDeviceToHost));
-  if (w && n) CUDA_TRY(cudaMemcpy(w, r->c.w, n * 8, cudaMemcpyDeviceToHost));
+  double* scalars[] = {q, w};
+  const double* ssrc[] = {r->c.q, r->c.w};
+  for (int k = 0; k < 2; ++k) {
+    if (!scalars[k] || !n) continue;
+    CUDA_TRY(cudaMemcpy(t.data(), ssrc[k], n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) scalars[k][i] = t[perm[i]];
+  }
   *count = n;
   return APRL_OK;
 }
@@ -1307,6 +1318,9 @@ aprl_status aprl_run_set_carriers(aprl_run* r, size_t n, const double* pos, cons
   }
   if (n) CUDA_TRY(cudaMemcpy(r->c.q, q, n * 8, cudaMemcpyHostToDevice));
   if (n) CUDA_TRY(cudaMemcpy(r->c.w, w, n * 8, cudaMemcpyHostToDevice));
+  std::vector<unsigned long long> keys(n);
+  for (size_t i = 0; i < n; ++i) keys[i] = i;
+  if (n) CUDA_TRY(cudaMemcpy(r->c.key, keys.data(), n * 8, cudaMemcpyHostToDevice));
   r->nc = n;
   return APRL_OK;
 }
