@@ -136,7 +136,10 @@ __device__ int shape_weights(const DGrid& g, int shape, const double begin[3],
     if (width <= 0.) continue;
     ++segments;
     if (shape == 0) {
-      binomial_xz_segment(g, x, v, cuts[s - 1], cuts[s], visit);
+      if constexpr (V::kF3Segment)
+        visit.f3_segment(g, x, v, cuts[s - 1], cuts[s]);
+      else
+        binomial_xz_segment(g, x, v, cuts[s - 1], cuts[s], visit);
       continue;
     }
     const double q[4] = {-.8611363115940525752, -.3399810435848562648,
@@ -224,6 +227,7 @@ __device__ __forceinline__ bool clip_open_orbit(const DGrid& g, const double b[3
 // selects E_new = E* - dt/eps0 J (residual) or E* (first-trial guess, when
 // the grid still holds the zero-current preview).
 struct ElectricVisitor {
+  static constexpr bool kF3Segment = true;
   const DGrid* g;
   bool with_current;
   double r[3];
@@ -236,6 +240,100 @@ struct ElectricVisitor {
     const size_t n = e_index(G, d, ii, jj, kk);
     const double vn = with_current ? e_candidate(G, d, ii, jj, kk) : G.e_star[d][n];
     r[d] += .5 * w * (vn + G.e_old[d][n]);
+  }
+
+  // One accumulation .5*w*(E_new + E^n) at ring/plain offsets (n, jn) of a
+  // node whose applyCurrentSource mask is known to be true.
+  __device__ __forceinline__ double term(int d, size_t n, size_t jn, double w) const {
+    const DGrid& G = *g;
+    double vn = G.e_star[d][n];
+    if (with_current) {
+      const double jc = G.j[d][jn];
+      if (jc != 0.) vn += G.jcoef * jc;
+    }
+    return .5 * w * (vn + G.e_old[d][n]);
+  }
+
+  // binomialXZSegment specialised for the gather.  When the whole 4x2x4
+  // stencil is inside every component and inside the current mask (true
+  // for particles away from the PEC faces and the window ends), each stencil
+  // row is addressed once and its nodes read back to back; otherwise the
+  // generic visits run.  Per component the accumulation order is the
+  // reference's (Ex: k, y, x; Ey: k, x; Ez: y, x, k).
+  __device__ __forceinline__ void f3_segment(const DGrid& G, const double s[3],
+                                             const double d[3], double first, double last) {
+    const double width = last - first;
+    const double mid = (first + last) * 0.5;
+    const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
+    long long i = (long long)floor(x), j = (long long)floor(y);
+    const long long k = (long long)floor(z);
+    if (i == (long long)G.nx) --i;
+    if (j == (long long)G.ny) --j;
+    if (!(i >= 2 && i <= G.nx - 3 && j >= 1 && j <= G.ny - 2 && k >= 2 && k <= G.nz - 3)) {
+      binomial_xz_segment(G, s, d, first, last, *this);
+      return;
+    }
+    double wx[4], wz[4];
+    node_weights(x - i, wx);
+    node_weights(z - k, wz);
+    const double wy[2] = {1. - (y - j), y - j};
+    const double edge[3] = {0.25, 0.5, 0.25};
+    const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
+    const double sy[2] = {-1., 1.};
+    const double curvature = width * width / 12.;
+    const double xy = curvature * d[0] * d[1];
+    const double xz = curvature * d[0] * d[2];
+    const double yz = curvature * d[1] * d[2];
+    const int I = (int)i, J = (int)j, K = (int)k;
+    // Ex (nx, ny+1, nz+1): nodes x I-1..I+1, y J..J+1, z K-1..K+2
+    {
+      const int nxc = G.nx, nyc = G.ny + 1, nzc = G.nz + 1;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const size_t plane = (size_t)ring(K - 1 + c, G.zb_e[0], nzc) * nyc;
+        const size_t jplane = (size_t)(K - 1 + c) * nyc;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+          const size_t n0 = (plane + J + b) * nxc + (I - 1);
+          const size_t j0 = (jplane + J + b) * nxc + (I - 1);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) r[0] += term(0, n0 + a, j0 + a, weight * edge[a]);
+        }
+      }
+    }
+    // Ey (nx+1, ny, nz+1): nodes x I-1..I+2, y J, z K-1..K+2
+    {
+      const int nxc = G.nx + 1, nyc = G.ny, nzc = G.nz + 1;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const size_t n0 = ((size_t)ring(K - 1 + c, G.zb_e[1], nzc) * nyc + J) * nxc + (I - 1);
+        const size_t j0 = ((size_t)(K - 1 + c) * nyc + J) * nxc + (I - 1);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          r[1] += term(1, n0 + a, j0 + a, width * (wx[a] * wz[c] + xz * slope[a] * slope[c]));
+      }
+    }
+    // Ez (nx+1, ny+1, nz): nodes x I-1..I+2, y J..J+1, z K-1..K+1
+    {
+      const int nxc = G.nx + 1, nyc = G.ny + 1, nzc = G.nz;
+      size_t plane[3], jplane[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        plane[c] = (size_t)ring(K - 1 + c, G.zb_e[2], nzc) * nyc;
+        jplane[c] = (size_t)(K - 1 + c) * nyc;
+      }
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const double weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            r[2] += term(2, (plane[c] + J + b) * nxc + (I - 1 + a),
+                         (jplane[c] + J + b) * nxc + (I - 1 + a), weight * edge[c]);
+        }
+    }
   }
 };
 
@@ -251,10 +349,13 @@ __device__ __forceinline__ double open_b(const DGrid& g, int a, long long i, lon
   return g.b[a][b_index(g, a, (int)i, (int)j, (int)k)];
 }
 
-// binomialXZMagneticSample (src/source_coupling_math.h:142-167).
+// binomialXZMagneticSample (src/source_coupling_math.h:142-167).  Rows of
+// the 4x2x4 stencil that lie inside the component are read without the
+// open-face clamps; the clamped form runs otherwise.  Same order either way.
 __device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const double p[3],
                                                      double value[3]) {
   const double h[3] = {g.dx, g.dy, g.dz};
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
     long long cell[3];
     double fraction[3];
@@ -267,14 +368,32 @@ __device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const doubl
     node_weights(fraction[0], wx);
     node_weights(fraction[2], wz);
     const double wy[2] = {1. - fraction[1], fraction[1]};
+    const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
     double v = 0.;
-    for (int k = 0; k < 4; ++k)
-      for (int j = 0; j < 2; ++j) {
-        double row = 0.;
-        for (int i = 0; i < 4; ++i)
-          row += wx[i] * open_b(g, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
-        v += wz[k] * wy[j] * row;
+    if (cell[0] >= 1 && cell[0] + 2 <= nxc - 1 && cell[1] >= 0 && cell[1] + 1 <= nyc - 1 &&
+        cell[2] >= 1 && cell[2] + 2 <= nzc - 1) {
+      const double* base = g.b[a];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const size_t plane = (size_t)ring((int)cell[2] - 1 + k, g.zb_b[a], (int)nzc) * nyc;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const double* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
+          double r = 0.;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) r += wx[i] * row[i];
+          v += wz[k] * wy[j] * r;
+        }
       }
+    } else {
+      for (int k = 0; k < 4; ++k)
+        for (int j = 0; j < 2; ++j) {
+          double row = 0.;
+          for (int i = 0; i < 4; ++i)
+            row += wx[i] * open_b(g, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
+          v += wz[k] * wy[j] * row;
+        }
+    }
     value[a] = v;
   }
 }
@@ -340,6 +459,7 @@ __device__ __forceinline__ unsigned gather_magnetic(const DGrid& g, int shape,
 // ---------------------------------------------------------------------------
 // deposition: Current::deposit at one rank (src/longitudinal_shape.h:175-187)
 struct DepositVisitor {
+  static constexpr bool kF3Segment = false;
   const DGrid* g;
   double scale[3];
   bool smooth_x;

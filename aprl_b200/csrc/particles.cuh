@@ -20,7 +20,7 @@ struct DRegion {
 };
 
 // Particle SoA (RelativisticParticleSI without the diagnostics).  Storage
-// is sorted by 4x4x4 cell tiles for gather/deposit locality; `order` keeps
+// is sorted by cell (x fastest) for gather/deposit locality; `order` keeps
 // each particle's rank in the reference's list order, which the ABI
 // restores on read-out.
 struct DParticles {
@@ -29,7 +29,7 @@ struct DParticles {
   unsigned long long* order;
 };
 
-constexpr int kTileShift = 2;  // 4 cells per tile edge
+constexpr int kTileShift = 0;  // sort granularity: single cells (2^0)
 
 // CPML carriers.  `key` = (birth step + 1) << 32 | rank of the parent in
 // the particle list, so sorting by key restores the reference's carrier
