@@ -80,6 +80,8 @@ class RunConfig(C.Structure):
         ("reference_nz", C.c_uint64),
         ("translation_beta", C.c_double),
         ("exit_lab_z", C.c_double),
+        ("activation_plane_lab_z", C.c_double),
+        ("maximum_step", C.c_uint64),
         ("n_magnets", C.c_uint32),
         ("reserved1", C.c_uint32),
         ("magnets", Magnet * MAX_MAGNETS),
@@ -109,6 +111,10 @@ class StepStats(C.Structure):
         ("time_box", C.c_double),
         ("device_error", C.c_uint32),
         ("reserved", C.c_uint32),
+        ("pending", C.c_uint64),
+        ("admitted", C.c_uint64),
+        ("activations", C.c_uint64),
+        ("held", C.c_uint64),
     ]
 
     def as_dict(self):

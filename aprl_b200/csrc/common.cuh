@@ -18,6 +18,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace aprl_gpu {
@@ -48,6 +49,9 @@ enum DeviceError : unsigned {
   kErrFellBehind = 14,        // particle/carrier behind the moving inlet
   kErrReferenceRange = 15,    // inlet reference query outside the table
   kErrHitLocate = 16,         // boundary hit fraction outside [0,1]
+  kErrEarlyRelease = 17,      // held particle released before entering the window
+  kErrAdmission = 18,         // invalid upstream admission of a held particle
+  kErrHeldBoundary = 19,      // held segment crossed a particle boundary
   kErrCount
 };
 
@@ -139,6 +143,78 @@ __device__ __forceinline__ double gamma_u(double ux, double uy, double uz) {
   const double inv = 1.0 / scale;
   const double a = ux * inv, b = uy * inv, c = uz * inv;
   return scale * sqrt(inv * inv + a * a + b * b + c * c);
+}
+
+// repeatHeldAddition (src/pending_particle_queue.cpp:38-88): `count`
+// separately rounded binary64 additions, with runs of constant spacing
+// skipped by integer ULP arithmetic.  Host and device share this code.
+__host__ __device__ __forceinline__ unsigned long long held_bits(double v) {
+#ifdef __CUDA_ARCH__
+  return (unsigned long long)__double_as_longlong(v);
+#else
+  unsigned long long b;
+  memcpy(&b, &v, 8);
+  return b;
+#endif
+}
+__host__ __device__ __forceinline__ double held_from_bits(unsigned long long b) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)b);
+#else
+  double v;
+  memcpy(&v, &b, 8);
+  return v;
+#endif
+}
+__host__ __device__ __forceinline__ unsigned long long held_ordered(unsigned long long v) {
+  return (v & 0x8000000000000000ull) ? ~v : v ^ 0x8000000000000000ull;
+}
+__host__ __device__ __forceinline__ double held_from_ordered(unsigned long long v) {
+  return held_from_bits((v & 0x8000000000000000ull) ? v ^ 0x8000000000000000ull : ~v);
+}
+__host__ __device__ __forceinline__ bool held_same_spacing(unsigned long long a,
+                                                           unsigned long long b) {
+  const unsigned long long m = 0x8000000000000000ull | 0x7ff0000000000000ull;
+  return (a & m) == (b & m);
+}
+__host__ __device__ __forceinline__ double held_repeat_positive(double x, double increment,
+                                                                unsigned long long count) {
+  while (count) {
+    const double y = x + increment;
+    if (!isfinite(y)) return y;
+    if (count == 1 || y == x) return y;
+    const double z = y + increment;
+    const unsigned long long bx = held_bits(x), by = held_bits(y), bz = held_bits(z);
+    if (isfinite(z) && held_same_spacing(bx, by) && held_same_spacing(by, bz)) {
+      const unsigned long long ox = held_ordered(bx), oy = held_ordered(by), oz = held_ordered(bz);
+      const unsigned long long stride = oy - ox;
+      if (stride && oz - oy == stride) {
+        const unsigned long long last_bits =
+            (bx & 0x8000000000000000ull) ? bx & (0x8000000000000000ull | 0x7ff0000000000000ull)
+                                         : bx | 0x000fffffffffffffull;
+        const unsigned long long available = (held_ordered(last_bits) - ox) / stride;
+        const unsigned long long safe = available ? available - 1 : 0;
+        const unsigned long long jump = safe < count ? safe : count;
+        if (jump) {
+          x = held_from_ordered(ox + jump * stride);
+          count -= jump;
+          continue;
+        }
+      }
+    }
+    x = y;
+    --count;
+  }
+  return x;
+}
+__host__ __device__ __forceinline__ double repeat_held_addition(double initial, double increment,
+                                                                unsigned long long count) {
+  if (!count) return initial;
+  if (increment < 0.) {
+    const double result = -held_repeat_positive(-initial, -increment, count);
+    return result == 0. ? 0. : result;
+  }
+  return held_repeat_positive(initial, increment, count);
 }
 
 // labZFromBoxZT (src/boostframe.cpp:241-245).

@@ -823,76 +823,187 @@ __global__ void carrier_kernel(CarrierArgs a) {
   a.out.key[n] = a.in.key[n];
 }
 
-// One fixed-point trial of one active particle: ConservativeSourceCoupling::
-// push (src/source_coupling.cpp:90-104) from the step-start state, then the
-// boundary events and deposition of processActiveSegment
-// (src/simulation.cpp:4760-4917) with Simulation::firstMovingWindowEntry
+// ConservativeSourceCoupling::push of one slot (src/source_coupling.cpp:90-104):
+// the first trial gathers along the ballistic guess chord from the slot's
+// start, later trials take the previous residual's re-gathered fields; then
+// `substeps` Lapenta-Markidis substeps with the prescribed magnets.
+__device__ unsigned coupling_push(const PushArgs& a, long long n, double pos[3], double u[3],
+                                  double q, double m, double time, double dt, double used_e[3],
+                                  double used_b[3], double& abs_work) {
+  const DGrid& g = a.g;
+  unsigned err = kErrNone;
+  if (a.first_trial) {
+    const double gamma = gamma_u(u[0], u[1], u[2]);
+    const double s = dt * kC / gamma;
+    const double guess[3] = {pos[0] + s * u[0], pos[1] + s * u[1], pos[2] + s * u[2]};
+    err = gather_electric(g, a.shape, pos, guess, false, used_e);
+    if (!err) err = gather_magnetic(g, a.shape, pos, guess, used_b);
+  } else {
+    for (int d = 0; d < 3; ++d) {
+      used_e[d] = a.next_e[3 * n + d];
+      used_b[d] = a.next_b[3 * n + d];
+    }
+  }
+  abs_work = 0.0;
+  if (err) return err;
+  const double h = dt / a.substeps;
+  for (int s = 0; s < a.substeps; ++s) {
+    const double before_pos[3] = {pos[0], pos[1], pos[2]};
+    const double before_u[3] = {u[0], u[1], u[2]};
+    const double g0 = gamma_u(u[0], u[1], u[2]);
+    const double ps = .5 * h * kC / g0;
+    const double point[3] = {pos[0] + ps * u[0], pos[1] + ps * u[1], pos[2] + ps * u[2]};
+    double ee[3] = {0., 0., 0.}, bb[3] = {0., 0., 0.};
+    add_prescribed_box(a, point, time + (s + .5) * h, ee, bb);
+    double e[3], b[3];
+    for (int d = 0; d < 3; ++d) {
+      e[d] = used_e[d] + ee[d];
+      b[d] = used_b[d] + bb[d];
+    }
+    err = momentum(u, e, b, q, m, h, g0);
+    if (err) return err;
+    const double g1 = gamma_u(u[0], u[1], u[2]);
+    const double xs = h * kC / (g0 + g1);
+    for (int d = 0; d < 3; ++d) pos[d] += xs * (before_u[d] + u[d]);
+    // |BorisWork::gridWork| of this substep (chargeWork, evaluated in
+    // binary64 here; the reference keeps long double).
+    double w = 0.0;
+    for (int d = 0; d < 3; ++d) w += q * used_e[d] * (pos[d] - before_pos[d]);
+    abs_work += fabs(w);
+  }
+  return kErrNone;
+}
+
+// Longitudinal-shape Current::deposit without the depositor's endpoint
+// validation (src/longitudinal_shape.h:175-187): the upstream part of an
+// admitted held particle and the frozen source support
+// (src/source_coupling.cpp:73-78) deposit this way.
+__device__ unsigned deposit_current(const DGrid& g, int shape, const double b[3],
+                                    const double e[3], double charge) {
+  DepositVisitor v;
+  v.g = &g;
+  v.smooth_x = shape == 0;
+  v.error = kErrNone;
+  for (int a = 0; a < 3; ++a)
+    v.scale[a] = charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt);
+  if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
+  return v.error;
+}
+
+// One fixed-point trial of one particle of the list: prepareParticle
+// (src/simulation.cpp:4919-5035; held advance at c*frozenBetaZ, activation-
+// plane crossing with the push of the remaining fraction of the step, or
+// ConservativeSourceCoupling::push from the step start), then the deposit
+// and boundary pass (src/simulation.cpp:5083-5368): upstream admission
+// clip, the frozen-to-active kink (4684-4756) and processActiveSegment
+// (4760-4917) with Simulation::firstMovingWindowEntry
 // (src/simulation_moving_window.cpp:380-395).
 __global__ void push_deposit_kernel(PushArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   const DGrid& g = a.g;
-  const double dt = g.dt;
+  const double t = a.time, dt = g.dt;
   double pos[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
   double u[3] = {a.p.ux[n], a.p.uy[n], a.p.uz[n]};
   const double q = a.p.q[n], m = a.p.m[n];
-  const double start[3] = {pos[0], pos[1], pos[2]};
+  const bool frozen0 = a.p.frozen[n] != 0;
+  bool frozen1 = frozen0;
+  double start[3] = {pos[0], pos[1], pos[2]};
   unsigned err = kErrNone;
-  if (start[2] < g.origin[2]) err = kErrUpstream;
-  double used_e[3], used_b[3];
-  if (!err) {
-    if (a.first_trial) {
-      const double gamma = gamma_u(u[0], u[1], u[2]);
-      const double s = dt * kC / gamma;
-      const double guess[3] = {pos[0] + s * u[0], pos[1] + s * u[1], pos[2] + s * u[2]};
-      err = gather_electric(g, a.shape, pos, guess, false, used_e);
-      if (!err) err = gather_magnetic(g, a.shape, pos, guess, used_b);
-    } else {
-      for (int d = 0; d < 3; ++d) {
-        used_e[d] = a.next_e[3 * n + d];
-        used_b[d] = a.next_b[3 * n + d];
-      }
-    }
-  }
+  if (start[2] < g.origin[2] && !frozen0) err = kErrUpstream;
+  bool has_active = !frozen0;
+  double active_time = t;
+  double kink[3] = {start[0], start[1], start[2]};
+  unsigned char seen = 0;
+  double slot_dt = dt;
+  double used_e[3] = {0., 0., 0.}, used_b[3] = {0., 0., 0.};
   double abs_work = 0.0;
   if (!err) {
-    const double h = dt / a.substeps;
-    for (int s = 0; s < a.substeps && !err; ++s) {
-      const double before_pos[3] = {pos[0], pos[1], pos[2]};
-      const double before_u[3] = {u[0], u[1], u[2]};
-      const double g0 = gamma_u(u[0], u[1], u[2]);
-      const double ps = .5 * h * kC / g0;
-      const double point[3] = {pos[0] + ps * u[0], pos[1] + ps * u[1], pos[2] + ps * u[2]};
-      double ee[3] = {0., 0., 0.}, bb[3] = {0., 0., 0.};
-      add_prescribed_box(a, point, a.time + (s + .5) * h, ee, bb);
-      double e[3], b[3];
-      for (int d = 0; d < 3; ++d) {
-        e[d] = used_e[d] + ee[d];
-        b[d] = used_b[d] + bb[d];
+    if (frozen0) {
+      const double beta = a.p.beta[n];
+      const double start_lab = lab_z_from_box_zt(a.frame, start[2], t);
+      pos[2] += kC * dt * beta;
+      const double end_lab = lab_z_from_box_zt(a.frame, pos[2], t + dt);
+      const double plane = a.activation_plane_lab_z;
+      if (end_lab >= plane) {
+        if (start[2] < g.origin[2]) {
+          err = kErrEarlyRelease;
+        } else {
+          const double crossing =
+              start_lab >= plane
+                  ? 0.0
+                  : fmax(0.0, fmin(1.0, (plane - start_lab) / (end_lab - start_lab)));
+          for (int d = 0; d < 3; ++d) pos[d] = start[d];
+          pos[2] += kC * crossing * dt * beta;
+          frozen1 = false;
+          has_active = true;
+          for (int d = 0; d < 3; ++d) kink[d] = pos[d];
+          active_time = t + crossing * dt;
+          const double remaining = (1.0 - crossing) * dt;
+          if (remaining > 0.0) {
+            err = coupling_push(a, n, pos, u, q, m, active_time, remaining, used_e, used_b,
+                                abs_work);
+            seen = 2;
+            slot_dt = remaining;
+          }
+        }
       }
-      err = momentum(u, e, b, q, m, h, g0);
-      if (err) break;
-      const double g1 = gamma_u(u[0], u[1], u[2]);
-      const double xs = h * kC / (g0 + g1);
-      for (int d = 0; d < 3; ++d) pos[d] += xs * (before_u[d] + u[d]);
-      // |BorisWork::gridWork| of this substep (chargeWork, evaluated in
-      // binary64 here; the reference keeps long double).
-      double w = 0.0;
-      for (int d = 0; d < 3; ++d) w += q * used_e[d] * (pos[d] - before_pos[d]);
-      abs_work += fabs(w);
+    } else {
+      err = coupling_push(a, n, pos, u, q, m, t, dt, used_e, used_b, abs_work);
+      seen = 1;
     }
   }
+  if (!err && frozen0 && has_active) atomicAdd(&a.counters->activations, 1ull);
   unsigned char action = 0;
   bool born_kept = false;
   CarrierState born;
-  if (!err) {
+  double seg_frac = 0.0;
+  bool upstream_only = false;
+  if (!err && start[2] < g.origin[2]) {
+    // Upstream admission of an unreleased held particle: the part before
+    // the inlet deposits without validation, the rest is an ordinary
+    // segment starting at the admission fraction.
+    if (!frozen0 || !frozen1 || has_active) {
+      err = kErrAdmission;
+    } else if (pos[2] < g.origin[2]) {
+      err = deposit_current(g, a.shape, start, pos, q);
+      upstream_only = true;
+    } else {
+      const double fraction = (g.origin[2] - start[2]) / (pos[2] - start[2]);
+      if (!(fraction >= 0.0 && fraction <= 1.0) || !isfinite(fraction)) {
+        err = kErrAdmission;
+      } else {
+        double clipped[3];
+        for (int d = 0; d < 3; ++d) clipped[d] = start[d] + fraction * (pos[d] - start[d]);
+        clipped[2] = g.origin[2];
+        seg_frac = fraction;
+        err = deposit_current(g, a.shape, start, clipped, q);
+        for (int d = 0; d < 3; ++d) start[d] = clipped[d];
+      }
+    }
+  }
+  if (!err && !upstream_only) {
+    if (frozen0 && has_active && active_time > t && active_time < t + dt) {
+      // The frozen part of the step up to the activation kink may not
+      // cross a particle boundary.
+      Hit hc, ho;
+      bool enters = false, exits = false;
+      err = cpml_first_entry(a.region, start, kink, hc, enters);
+      if (!err) err = outer_first_exit(a.region, start, kink, ho, exits);
+      if (!err && (enters || exits)) err = kErrHeldBoundary;
+      if (!err) err = deposit_segment(g, a.shape, start, kink, q);
+      for (int d = 0; d < 3; ++d) start[d] = kink[d];
+      seg_frac = (active_time - t) / dt;
+    }
+  }
+  if (!err && !upstream_only) {
     // firstMovingWindowEntry = CPML first entry + fixed-lab exit plane
     Hit cpml_hit, outer_hit;
     bool enters = false, exits = false;
     err = cpml_first_entry(a.region, start, pos, cpml_hit, enters);
     if (!err) {
-      const double za = lab_z_from_box_zt(a.frame, start[2], a.time + 0.0 * dt) - a.exit_lab_z;
-      const double zb = lab_z_from_box_zt(a.frame, pos[2], a.time + dt) - a.exit_lab_z;
+      const double za = lab_z_from_box_zt(a.frame, start[2], t + seg_frac * dt) - a.exit_lab_z;
+      const double zb = lab_z_from_box_zt(a.frame, pos[2], t + dt) - a.exit_lab_z;
       if (za >= 0.) err = kErrBeyondExit;
       else if (zb >= 0. && zb > za) {
         const double fraction = -za / (zb - za);
@@ -922,7 +1033,7 @@ __global__ void push_deposit_kernel(PushArgs a) {
         for (int d = 0; d < 3; ++d) seg_end[d] = selected.position[d];
       }
       err = deposit_segment(g, a.shape, start, seg_end, q);
-      const double global_end = 0.0 + local_end * (1.0 - 0.0);
+      const double global_end = seg_frac + local_end * (1.0 - seg_frac);
       if (!err && action == 1) {
         if (selected.face == 5) {
           atomicAdd(&a.counters->exits, 1ull);
@@ -946,8 +1057,22 @@ __global__ void push_deposit_kernel(PushArgs a) {
     }
   }
   if (err) raise_error(a.status, err, (unsigned long long)n);
+  // Held particles retained by this trial, one atomic per converged group.
+  const bool held = !err && action == 0 && frozen1;
+  const unsigned group = __activemask();
+  const unsigned held_ballot = __ballot_sync(group, held);
+  if (held_ballot && (threadIdx.x & 31) == __ffs(group) - 1)
+    atomicAdd(&a.counters->held, (unsigned long long)__popc(held_ballot));
   a.x1[n] = pos[0]; a.y1[n] = pos[1]; a.z1[n] = pos[2];
   a.ux1[n] = u[0]; a.uy1[n] = u[1]; a.uz1[n] = u[2];
+  a.frozen1[n] = frozen1 ? 1 : 0;
+  a.slot.seen[n] = seen;
+  if (seen == 2) {
+    a.slot.x0[n] = kink[0];
+    a.slot.y0[n] = kink[1];
+    a.slot.z0[n] = kink[2];
+    a.slot.dt[n] = slot_dt;
+  }
   for (int d = 0; d < 3; ++d) {
     a.used_e[3 * n + d] = used_e[d];
     a.used_b[3 * n + d] = used_b[d];
@@ -980,8 +1105,17 @@ __device__ __forceinline__ double warp_max(double v) {
 __global__ void residual_kernel(ResidualArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double force = 0.0, defect = 0.0, scale = 0.0;
-  if (n < a.count) {
-    const double first[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
+  const unsigned char seen = n < a.count ? a.slot.seen[n] : 0;
+  if (seen) {
+    // Slot start: the step start, or the activation kink of a held
+    // particle released during the step (seen == 2).
+    double first[3], dt = a.g.dt;
+    if (seen == 2) {
+      first[0] = a.slot.x0[n]; first[1] = a.slot.y0[n]; first[2] = a.slot.z0[n];
+      dt = a.slot.dt[n];
+    } else {
+      first[0] = a.p.x[n]; first[1] = a.p.y[n]; first[2] = a.p.z[n];
+    }
     const double last[3] = {a.x1[n], a.y1[n], a.z1[n]};
     double ne[3], nb[3];
     unsigned err = gather_electric(a.g, a.shape, first, last, true, ne);
@@ -998,7 +1132,7 @@ __global__ void residual_kernel(ResidualArgs a) {
       db[d] = nb[d] - a.used_b[3 * n + d];
     }
     const double q = a.p.q[n], m = a.p.m[n];
-    force = fabs(q / m) * a.g.dt / kC *
+    force = fabs(q / m) * dt / kC *
             (sqrt(de[0] * de[0] + de[1] * de[1] + de[2] * de[2]) +
              kC * sqrt(db[0] * db[0] + db[1] * db[1] + db[2] * db[2]));
     double wd = 0.0, wn = 0.0;
@@ -1009,6 +1143,8 @@ __global__ void residual_kernel(ResidualArgs a) {
     defect = fabs(wd);
     scale = a.abs_grid_work[n] + fabs(wn);
   }
+  __shared__ unsigned s_calls[32];
+  const unsigned calls = __popc(__ballot_sync(0xffffffffu, seen != 0));
   __shared__ double s_force[32], s_defect[32], s_scale[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   force = warp_max(force);
@@ -1018,6 +1154,7 @@ __global__ void residual_kernel(ResidualArgs a) {
     s_force[warp] = force;
     s_defect[warp] = defect;
     s_scale[warp] = scale;
+    s_calls[warp] = calls;
   }
   __syncthreads();
   if (warp == 0) {
@@ -1025,13 +1162,16 @@ __global__ void residual_kernel(ResidualArgs a) {
     force = lane < warps ? s_force[lane] : 0.0;
     defect = lane < warps ? s_defect[lane] : 0.0;
     scale = lane < warps ? s_scale[lane] : 0.0;
+    unsigned block_calls = lane < warps ? s_calls[lane] : 0u;
     force = warp_max(force);
     defect = warp_sum(defect);
     scale = warp_sum(scale);
+    for (int o = 16; o > 0; o >>= 1) block_calls += __shfl_xor_sync(0xffffffffu, block_calls, o);
     if (lane == 0) {
       atomicMax(&a.sums->force_bits, (unsigned long long)__double_as_longlong(force));
       atomicAdd(&a.sums->defect, defect);
       atomicAdd(&a.sums->scale, scale);
+      if (block_calls) atomicAdd(&a.sums->calls, (unsigned long long)block_calls);
     }
   }
 }
@@ -1107,9 +1247,9 @@ __device__ __forceinline__ long long compact_slot(const unsigned char* flag, uns
 __global__ void gather_particles_kernel(DParticles out, DParticles src, const double* x1,
                                         const double* y1, const double* z1,
                                         const double* ux1, const double* uy1,
-                                        const double* uz1, const unsigned char* flag,
-                                        unsigned char want, long long n,
-                                        const unsigned* block_offset) {
+                                        const double* uz1, const unsigned char* frozen1,
+                                        const unsigned char* flag, unsigned char want,
+                                        long long n, const unsigned* block_offset) {
   bool selected;
   const long long slot = compact_slot(flag, want, n, block_offset, selected);
   const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
@@ -1120,6 +1260,8 @@ __global__ void gather_particles_kernel(DParticles out, DParticles src, const do
   out.m[slot] = src.m[i];
   out.id[slot] = src.id[i];
   out.order[slot] = src.order[i];
+  out.frozen[slot] = frozen1[i];
+  out.beta[slot] = src.beta[i];
 }
 
 __global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsigned char* flag,
@@ -1193,6 +1335,48 @@ __global__ void scatter_particles_kernel(DParticles out, DParticles src, long lo
   out.m[d] = src.m[i];
   out.id[d] = src.id[i];
   out.order[d] = src.order[i];
+  out.frozen[d] = src.frozen[i];
+  out.beta[d] = src.beta[i];
+}
+
+// PendingParticleQueue::admit (src/pending_particle_queue.cpp:163-186): the
+// queue entries [begin, begin+count) join the end of the list with their
+// held z advanced by `steps` separately rounded additions of
+// (c*dt)*frozenBetaZ.
+__global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
+                             long long begin, long long count, unsigned long long steps,
+                             double held_distance_per_beta, unsigned long long first_order) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const long long k = begin + i, d = first_slot + i;
+  const double beta = src.beta[k];
+  out.x[d] = src.x[k];
+  out.y[d] = src.y[k];
+  out.z[d] = repeat_held_addition(src.z[k], held_distance_per_beta * beta, steps);
+  out.ux[d] = src.ux[k]; out.uy[d] = src.uy[k]; out.uz[d] = src.uz[k];
+  out.q[d] = src.q[k];
+  out.m[d] = src.m[k];
+  out.id[d] = src.id[k];
+  out.order[d] = first_order + (unsigned long long)i;
+  out.frozen[d] = 1;
+  out.beta[d] = beta;
+}
+
+// Frozen source support of the queue entries due within the next steps
+// (PendingParticleQueue::visitNear + depositFrozenSourceSupport,
+// src/simulation.cpp:4170-4172, src/source_coupling.cpp:73-78): each
+// deposits its held chord of this step without endpoint validation.
+__global__ void frozen_support_kernel(SupportArgs a) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.count) return;
+  const long long k = a.begin + i;
+  const double beta = a.src.beta[k];
+  const double increment = a.held_distance_per_beta * beta;
+  const double start[3] = {a.src.x[k], a.src.y[k],
+                           repeat_held_addition(a.src.z[k], increment, a.steps)};
+  const double stop[3] = {start[0], start[1], start[2] + increment};
+  const unsigned err = deposit_current(a.g, a.shape, start, stop, a.src.q[k]);
+  if (err) raise_error(a.status, err, (unsigned long long)k);
 }
 
 // finishMovingWindowStep carrier crop (src/simulation_moving_window.cpp:363-368).
@@ -1214,10 +1398,11 @@ __global__ void crop_flags_kernel(DCarriers c, long long n, double upper, double
 }
 
 // migrateWindowObjects' inlet guard (src/simulation_moving_window.cpp:355-358).
-__global__ void inlet_check_kernel(const double* z, long long n, double origin,
-                                   DeviceStatus* status) {
+__global__ void inlet_check_kernel(const double* z, const unsigned char* frozen, long long n,
+                                   double origin, DeviceStatus* status) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && z[i] < origin) raise_error(status, kErrFellBehind, (unsigned long long)i);
+  if (i < n && z[i] < origin && !frozen[i])
+    raise_error(status, kErrFellBehind, (unsigned long long)i);
 }
 
 }  // namespace aprl_gpu

@@ -27,6 +27,8 @@ struct DParticles {
   double *x, *y, *z, *ux, *uy, *uz, *q, *m;
   unsigned long long* id;
   unsigned long long* order;
+  unsigned char* frozen;  // held lab-plane injection state
+  double* beta;           // frozenBetaZ
 };
 
 constexpr int kTileShift = 0;  // sort granularity: single cells (2^0)
@@ -53,13 +55,25 @@ struct TrialCounters {
   double carrier_outer_charge[6];
   unsigned long long cropped;     // carriers beyond the window upper edge
   double cropped_charge;
+  unsigned long long activations; // held particles crossing the activation plane
+  unsigned long long held;        // held particles retained by the trial
 };
 
 struct ResidualSums {
   unsigned long long force_bits;  // max over particles (non-negative double bits)
   double defect;
   double scale;
-  double calls;
+  unsigned long long calls;       // pushed (seen) slots
+};
+
+// Per-slot record of one trial push (ConservativeSourceCoupling::Impl::Slot,
+// src/source_coupling.cpp:19): where and when the push started and its dt
+// (a held particle released mid-step is pushed from its activation kink for
+// the remaining fraction of the step).
+struct DSlots {
+  double *x0, *y0, *z0;
+  double* dt;
+  unsigned char* seen;
 };
 
 struct PushArgs {
@@ -73,9 +87,12 @@ struct PushArgs {
   int first_trial;       // 1: gather along the ballistic guess chord
   double time;           // box time at the start of the step
   double exit_lab_z;
+  double activation_plane_lab_z;
   long long count;
   DParticles p;          // state at the start of the step (read only)
   double *x1, *y1, *z1, *ux1, *uy1, *uz1;  // state after the trial push
+  unsigned char* frozen1;                  // held state after the trial
+  DSlots slot;
   double* used_e;        // 3*count, written
   double* used_b;
   const double* next_e;  // 3*count, from the previous residual
@@ -106,6 +123,7 @@ struct ResidualArgs {
   int shape;
   long long count;
   DParticles p;
+  DSlots slot;
   const double *x1, *y1, *z1;
   const double* used_e;
   const double* used_b;
@@ -131,6 +149,7 @@ __global__ void gather_particles_kernel(DParticles out, DParticles src,
                                         const double* x1, const double* y1,
                                         const double* z1, const double* ux1,
                                         const double* uy1, const double* uz1,
+                                        const unsigned char* frozen1,
                                         const unsigned char* flag, unsigned char want,
                                         long long n, const unsigned* block_offset);
 __global__ void gather_carriers_kernel(DCarriers out, DCarriers src,
@@ -148,10 +167,31 @@ __global__ void scatter_particles_kernel(DParticles out, DParticles src, long lo
                                          const unsigned* tile_of,
                                          const unsigned* rank_in_tile,
                                          const unsigned* tile_offset);
+// Pending queue (PendingParticleQueue) on the device: particles sorted by
+// their due step, initial state.
+struct DPending {
+  double *x, *y, *z, *ux, *uy, *uz, *q, *m, *beta;
+  unsigned long long* id;
+};
+__global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
+                             long long begin, long long count, unsigned long long steps,
+                             double held_distance_per_beta, unsigned long long first_order);
+struct SupportArgs {
+  DGrid g;
+  int shape;
+  DPending src;
+  long long begin, count;
+  unsigned long long steps;      // step - initial step
+  double held_distance_per_beta; // c*dt
+  DeviceStatus* status;
+};
+__global__ void frozen_support_kernel(SupportArgs a);
 __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
                                   double lower, unsigned char* keep,
                                   TrialCounters* counters, DeviceStatus* status);
-__global__ void inlet_check_kernel(const double* z, long long n, double origin,
-                                   DeviceStatus* status);
+// finishMovingWindowStep's guard (src/simulation_moving_window.cpp:358-359):
+// an active particle may not fall behind the inlet; held ones may.
+__global__ void inlet_check_kernel(const double* z, const unsigned char* frozen, long long n,
+                                   double origin, DeviceStatus* status);
 
 }  // namespace aprl_gpu

@@ -52,7 +52,7 @@ enum Kernel : unsigned {
   kInletLower, kCowanMagnetic, kElectricPreview, kCarrier, kPushDeposit,
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
-  kTileCount, kChunkScan, kChunkAdd, kScatterParticles,
+  kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
   kKernelCount
 };
 
@@ -61,7 +61,8 @@ const char* kKernelNames[kKernelCount] = {
   "push_deposit", "residual", "electric_commit", "flag_count",
   "block_offset_scan", "gather_particles", "gather_carriers",
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
-  "tile_count", "chunk_scan", "chunk_add", "scatter_particles"};
+  "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
+  "frozen_support"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -81,6 +82,12 @@ const char* device_error_text(unsigned code) {
     case kErrFellBehind: return "Active particle fell behind moving inlet";
     case kErrReferenceRange: return "Moving reference query outside prepared native field";
     case kErrHitLocate: return "Cannot locate the first particle boundary crossing";
+    case kErrEarlyRelease:
+      return "A pending upstream held particle would release before a complete in-window step";
+    case kErrAdmission:
+      return "Moving-window upstream admission requires an unreleased held particle on rank zero";
+    case kErrHeldBoundary:
+      return "Held-transverse activation crossed a particle boundary during the frozen part of a field step";
   }
   return "unknown device error";
 }
@@ -233,6 +240,18 @@ struct aprl_run {
   size_t nslot = 0;
   unsigned long long* slot_order = nullptr;  // p.order at the last preview
   unsigned long long next_order = 0;
+  unsigned char* frozen1 = nullptr;           // held state after a trial
+  DSlots slots{};                             // per-slot push start (kinks)
+  // held lab-plane injection: PendingParticleQueue at one rank
+  struct Queue {
+    bool extracted = false;
+    uint64_t initial_step = 0, last_step = 0, maximum_step = 0, next_due = 0;
+    size_t n = 0, cursor = 0;
+    std::vector<size_t> offsets;  // bucket b = due step - initial_step
+    DPending d{};                 // entries in due order
+  } queue;
+  uint64_t admitted = 0;
+  uint64_t held = 0;              // frozen particles in the list
   // tile sort scratch
   unsigned *tile_count = nullptr, *tile_offset = nullptr, *tile_of = nullptr,
            *tile_rank = nullptr, *chunk_sum = nullptr, *chunk_offset = nullptr;
@@ -465,12 +484,19 @@ aprl_status alloc_particles(DParticles& p, size_t n) {
   TRY(device_alloc(&p.ux, n)); TRY(device_alloc(&p.uy, n)); TRY(device_alloc(&p.uz, n));
   TRY(device_alloc(&p.q, n)); TRY(device_alloc(&p.m, n)); TRY(device_alloc(&p.id, n));
   TRY(device_alloc(&p.order, n));
+  TRY(device_alloc(&p.frozen, n)); TRY(device_alloc(&p.beta, n));
   return APRL_OK;
 }
 void free_particles(DParticles& p) {
   cudaFree(p.x); cudaFree(p.y); cudaFree(p.z); cudaFree(p.ux); cudaFree(p.uy);
   cudaFree(p.uz); cudaFree(p.q); cudaFree(p.m); cudaFree(p.id); cudaFree(p.order);
+  cudaFree(p.frozen); cudaFree(p.beta);
   p = DParticles{};
+}
+void free_pending(DPending& d) {
+  cudaFree(d.x); cudaFree(d.y); cudaFree(d.z); cudaFree(d.ux); cudaFree(d.uy);
+  cudaFree(d.uz); cudaFree(d.q); cudaFree(d.m); cudaFree(d.beta); cudaFree(d.id);
+  d = DPending{};
 }
 aprl_status alloc_carriers(DCarriers& c, size_t n) {
   TRY(device_alloc(&c.px, n)); TRY(device_alloc(&c.py, n)); TRY(device_alloc(&c.pz, n));
@@ -502,12 +528,16 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
     CUDA_TRY(cudaMemcpy(np.m, r->p.m, r->np * 8, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.id, r->p.id, r->np * 8, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.frozen, r->p.frozen, r->np, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(cudaMemcpy(np.beta, r->p.beta, r->np * 8, cudaMemcpyDeviceToDevice));
   }
   free_particles(r->p);
   free_particles(r->p_alt);
   r->p = np;
   TRY(alloc_particles(r->p_alt, n));
-  double** trial[] = {&r->x1, &r->y1, &r->z1, &r->ux1, &r->uy1, &r->uz1, &r->abs_work};
+  double** trial[] = {&r->x1,       &r->y1,       &r->z1,       &r->ux1,     &r->uy1,
+                      &r->uz1,      &r->abs_work, &r->slots.x0, &r->slots.y0, &r->slots.z0,
+                      &r->slots.dt};
   for (double** t : trial) {
     cudaFree(*t);
     TRY(device_alloc(t, n));
@@ -522,6 +552,10 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   cudaFree(r->slot_order);
   cudaFree(r->tile_of);
   cudaFree(r->tile_rank);
+  cudaFree(r->frozen1);
+  cudaFree(r->slots.seen);
+  TRY(device_alloc(&r->frozen1, n));
+  TRY(device_alloc(&r->slots.seen, n));
   TRY(device_alloc(&r->action, n));
   TRY(device_alloc(&r->born_keep, n));
   TRY(device_alloc(&r->slot_order, n));
@@ -619,6 +653,7 @@ void add_counters(TrialCounters& to, const TrialCounters& from) {
   }
   to.cropped += from.cropped;
   to.cropped_charge += from.cropped_charge;
+  to.activations += from.activations;
 }
 
 // Stable compaction of `n` flagged elements; returns the kept count.
@@ -662,8 +697,90 @@ aprl_status sort_particles(aprl_run* r) {
   return APRL_OK;
 }
 
+// ---- held lab-plane injection: PendingParticleQueue at one rank
+// (src/pending_particle_queue.cpp).  The queue's bookkeeping lives on the
+// host; its entries live on the device in due order, so one admission is
+// one contiguous range.
+double held_distance_per_beta(const aprl_run_config& c) { return kC * c.dt; }
+
+// PendingParticleQueue::origin (src/pending_particle_queue.cpp:106-111).
+double pending_origin(const aprl_run_config& c, uint64_t step) {
+  const int64_t offset = c.initial_offset - static_cast<int64_t>(step);
+  return std::fma(static_cast<double>(offset), c.dz, c.reference_origin[2]);
+}
+
+// participates (src/pending_particle_queue.cpp:113-117): the held chord of
+// `step` ends at or beyond that step's inlet.
+bool participates(const aprl_run* r, double z, double beta, uint64_t step) {
+  const double end = repeat_held_addition(z, held_distance_per_beta(r->cfg) * beta,
+                                          step - r->queue.initial_step + 1);
+  return end >= pending_origin(r->cfg, step);
+}
+
+// firstDue (src/pending_particle_queue.cpp:119-126): extended-precision
+// estimate, confirmed or replaced by bisection over participates.
+uint64_t first_due(const aprl_run* r, double z, double beta) {
+  const auto& q = r->queue;
+  const double increment = held_distance_per_beta(r->cfg) * beta;
+  const long double distance = static_cast<long double>(pending_origin(r->cfg, q.initial_step)) -
+                               static_cast<long double>(z) - static_cast<long double>(increment);
+  const long double estimate = std::ceil(
+      distance / (static_cast<long double>(r->cfg.dz) + static_cast<long double>(increment)));
+  const uint64_t sentinel = q.maximum_step + 1;
+  const long double steps_left = static_cast<long double>(q.maximum_step - q.initial_step);
+  const uint64_t guess =
+      estimate > steps_left
+          ? sentinel
+          : q.initial_step + static_cast<uint64_t>(estimate > 1.L ? estimate : 1.L);
+  if (guess <= q.maximum_step && participates(r, z, beta, guess) &&
+      !participates(r, z, beta, guess - 1))
+    return guess;
+  if (guess == sentinel && !participates(r, z, beta, q.maximum_step)) return sentinel;
+  uint64_t lower = q.initial_step + 1, upper = sentinel;
+  while (lower < upper) {
+    const uint64_t middle = lower + (upper - lower) / 2;
+    if (participates(r, z, beta, middle)) upper = middle;
+    else lower = middle + 1;
+  }
+  return lower;
+}
+
+void advance_next_due(aprl_run::Queue& q) {
+  while (q.next_due <= q.maximum_step && q.offsets[q.next_due - q.initial_step + 1] <= q.cursor)
+    ++q.next_due;
+}
+
+// PendingParticleQueue::admit (src/pending_particle_queue.cpp:163-186),
+// called by admitMovingWindowParticles at the start of the step
+// (src/simulation.cpp:513).
+aprl_status admit_pending(aprl_run* r) {
+  auto& q = r->queue;
+  if (!q.extracted) return APRL_OK;
+  const uint64_t step = r->step;
+  if (step < q.last_step || step > q.maximum_step || step > q.next_due)
+    return fail(APRL_ERR_RUNTIME, "Pending admission skipped an event or exceeds its horizon");
+  q.last_step = step;
+  const size_t end = q.offsets[step - q.initial_step + 1];
+  const size_t k = end - q.cursor;
+  if (k) {
+    TRY(reserve_particles(r, r->np + k));
+    TRY(launch(r, kAdmit, admit_kernel, dim3(blocks_for(k, 256)), dim3(256), r->p,
+               (long long)r->np, q.d, (long long)q.cursor, (long long)k,
+               (unsigned long long)(step - q.initial_step), held_distance_per_beta(r->cfg),
+               (unsigned long long)r->next_order));
+    r->np += k;
+    r->next_order += k;
+    q.cursor = end;
+    r->admitted += k;
+    r->held += k;
+  }
+  advance_next_due(q);
+  return APRL_OK;
+}
+
 aprl_status do_advance_magnetic(aprl_run* r) {
   if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
+  TRY(admit_pending(r));
   const aprl_run_config& c = r->cfg;
   for (int a = 0; a < 3; ++a)
     CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream));
@@ -726,6 +843,26 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
   CUDA_TRY(cudaMemsetAsync(r->d_sums, 0, sizeof(ResidualSums), r->stream));
   const DGrid g = make_grid(r);
   const DRegion region = make_region(r);
+  if (r->queue.extracted) {
+    // Frozen source support of the entries due within min(8, horizon) steps.
+    const auto& q = r->queue;
+    const uint64_t room = q.maximum_step - r->step;
+    const uint64_t until = r->step + std::min<uint64_t>(8, room);
+    const size_t end = q.offsets[until - q.initial_step + 1];
+    if (end > q.cursor) {
+      SupportArgs sa{};
+      sa.g = g;
+      sa.shape = c.shape;
+      sa.src = q.d;
+      sa.begin = (long long)q.cursor;
+      sa.count = (long long)(end - q.cursor);
+      sa.steps = r->step - q.initial_step;
+      sa.held_distance_per_beta = held_distance_per_beta(c);
+      sa.status = r->d_status;
+      TRY(launch(r, kFrozenSupport, frozen_support_kernel, dim3(blocks_for(end - q.cursor, 128)),
+                 dim3(128), sa));
+    }
+  }
   if (r->nc) {
     CarrierArgs ca{};
     ca.g = g;
@@ -765,10 +902,13 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     pa.first_trial = r->trials == 0 ? 1 : 0;
     pa.time = r->time;
     pa.exit_lab_z = c.exit_lab_z;
+    pa.activation_plane_lab_z = c.activation_plane_lab_z;
     pa.count = (long long)r->np;
     pa.p = r->p;
     pa.x1 = r->x1; pa.y1 = r->y1; pa.z1 = r->z1;
     pa.ux1 = r->ux1; pa.uy1 = r->uy1; pa.uz1 = r->uz1;
+    pa.frozen1 = r->frozen1;
+    pa.slot = r->slots;
     pa.used_e = r->used_e;
     pa.used_b = r->used_b;
     pa.next_e = r->next_e;
@@ -786,6 +926,7 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     ra.shape = c.shape;
     ra.count = (long long)r->np;
     ra.p = r->p;
+    ra.slot = r->slots;
     ra.x1 = r->x1; ra.y1 = r->y1; ra.z1 = r->z1;
     ra.used_e = r->used_e;
     ra.used_b = r->used_b;
@@ -805,7 +946,7 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
   residual[0] = force;
   residual[1] = r->h_sums->defect;
   residual[2] = r->h_sums->scale;
-  residual[3] = static_cast<double>(r->np);
+  residual[3] = static_cast<double>(r->h_sums->calls);
   ++r->trials;
   r->stage = 3;
   return APRL_OK;
@@ -849,14 +990,16 @@ aprl_status do_commit(aprl_run* r) {
     TRY(launch(r, kGatherParticles, gather_particles_kernel, dim3(blocks_for(r->np, kScanBlock)),
                dim3(kScanBlock), r->p_alt, r->p, (const double*)r->x1, (const double*)r->y1,
                (const double*)r->z1, (const double*)r->ux1, (const double*)r->uy1,
-               (const double*)r->uz1, (const unsigned char*)r->action, (unsigned char)0,
-               (long long)r->np, (const unsigned*)r->scan_offset));
+               (const double*)r->uz1, (const unsigned char*)r->frozen1,
+               (const unsigned char*)r->action, (unsigned char)0, (long long)r->np,
+               (const unsigned*)r->scan_offset));
     std::swap(r->p, r->p_alt);
     r->np = kept;
     TRY(sort_particles(r));
   }
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   add_counters(r->cumulative, *r->h_counters);
+  r->held = r->h_counters->held;
   r->stage = 4;
   return APRL_OK;
 }
@@ -889,7 +1032,8 @@ aprl_status do_shift(aprl_run* r) {
   r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
   if (r->np)
     TRY(launch(r, kInletCheck, inlet_check_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
-               (const double*)r->p.z, (long long)r->np, r->origin[2], r->d_status));
+               (const double*)r->p.z, (const unsigned char*)r->p.frozen, (long long)r->np,
+               r->origin[2], r->d_status));
   if (r->nc) {
     const double upper = std::fma(static_cast<double>(c.nz), c.dz, r->origin[2]);
     CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
@@ -1071,9 +1215,14 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   for (auto& h : r->hist) cudaFree(h.data);
   free_particles(r->p);
   free_particles(r->p_alt);
-  double* singles[] = {r->x1, r->y1, r->z1, r->ux1, r->uy1, r->uz1, r->used_e, r->used_b,
-                       r->next_e, r->next_b, r->abs_work, r->d_detector};
+  double* singles[] = {r->x1,       r->y1,       r->z1,       r->ux1,        r->uy1,
+                       r->uz1,      r->used_e,   r->used_b,   r->next_e,     r->next_b,
+                       r->abs_work, r->slots.x0, r->slots.y0, r->slots.z0,   r->slots.dt,
+                       r->d_detector};
   for (double* d : singles) cudaFree(d);
+  cudaFree(r->slots.seen);
+  cudaFree(r->frozen1);
+  free_pending(r->queue.d);
   cudaFree(r->action);
   cudaFree(r->born_keep);
   cudaFree(r->slot_order);
@@ -1220,8 +1369,13 @@ aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const
   std::vector<unsigned long long> order(n);
   for (size_t i = 0; i < n; ++i) order[i] = i;
   if (n) CUDA_TRY(cudaMemcpy(r->p.order, order.data(), n * 8, cudaMemcpyHostToDevice));
+  if (n) {
+    CUDA_TRY(cudaMemset(r->p.frozen, 0, n));
+    CUDA_TRY(cudaMemset(r->p.beta, 0, n * 8));
+  }
   r->next_order = n;
   r->np = n;
+  r->held = 0;
   if (reset_carriers) r->nc = 0;
   TRY(sort_particles(r));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
@@ -1266,6 +1420,136 @@ aprl_status aprl_run_get_particles(aprl_run* r, size_t capacity, double* x, doub
     std::vector<uint64_t> ids(n);
     CUDA_TRY(cudaMemcpy(ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) id[i] = ids[perm[i]];
+  }
+  *count = n;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, const double* beta) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Held state can only be set between steps");
+  if (n != r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Held state must cover the particle list");
+  if (n && (!frozen || !beta)) return fail(APRL_ERR_INVALID_ARGUMENT, "null held array");
+  auto& q = r->queue;
+  if (q.extracted) return fail(APRL_ERR_RUNTIME, "Pending queue can only be initialized once");
+  const aprl_run_config& c = r->cfg;
+  q.initial_step = r->step;
+  q.last_step = r->step;
+  q.maximum_step = c.maximum_step;
+  q.next_due = r->step;
+  if (!(c.dz > 0.) || q.initial_step > q.maximum_step)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid pending-window geometry/horizon");
+  // The list in reference order.
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  std::vector<size_t> perm;
+  TRY(storage_permutation(r, r->p.order, n, perm));
+  std::vector<double> v[8];
+  const double* dsrc[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
+  for (int k = 0; k < 8; ++k) {
+    std::vector<double> t(n);
+    if (n) CUDA_TRY(cudaMemcpy(t.data(), dsrc[k], n * 8, cudaMemcpyDeviceToHost));
+    v[k].resize(n);
+    for (size_t i = 0; i < n; ++i) v[k][i] = t[perm[i]];
+  }
+  std::vector<unsigned long long> ids(n), id(n);
+  if (n) CUDA_TRY(cudaMemcpy(ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; ++i) id[i] = ids[perm[i]];
+  // PendingParticleQueue::extract (src/pending_particle_queue.cpp:128-154).
+  const size_t buckets = static_cast<size_t>(q.maximum_step - q.initial_step + 2);
+  q.offsets.assign(buckets + 1, 0);
+  const double inlet = pending_origin(c, q.initial_step);
+  std::vector<size_t> kept, queued, due;
+  for (size_t i = 0; i < n; ++i) {
+    const double z = v[2][i];
+    if (frozen[i] && z < inlet && beta[i] >= 0. && !participates(r, z, beta[i], q.initial_step)) {
+      const uint64_t event = first_due(r, z, beta[i]);
+      due.push_back(static_cast<size_t>(event - q.initial_step));
+      ++q.offsets[event - q.initial_step + 1];
+      queued.push_back(i);
+    } else {
+      kept.push_back(i);
+    }
+  }
+  for (size_t b = 1; b < buckets + 1; ++b) q.offsets[b] += q.offsets[b - 1];
+  std::vector<size_t> slot(queued.size());
+  {
+    std::vector<size_t> insertion(q.offsets);
+    for (size_t j = 0; j < queued.size(); ++j) slot[insertion[due[j]]++] = j;
+  }
+  // Queue entries on the device, in due order.
+  free_pending(q.d);
+  const size_t nq = queued.size();
+  q.n = nq;
+  q.cursor = 0;
+  if (nq) {
+    double** qd[] = {&q.d.x, &q.d.y, &q.d.z, &q.d.ux, &q.d.uy, &q.d.uz, &q.d.q, &q.d.m};
+    std::vector<double> t(nq);
+    for (int k = 0; k < 8; ++k) {
+      TRY(device_alloc(qd[k], nq));
+      for (size_t s = 0; s < nq; ++s) t[s] = v[k][queued[slot[s]]];
+      CUDA_TRY(cudaMemcpy(*qd[k], t.data(), nq * 8, cudaMemcpyHostToDevice));
+    }
+    TRY(device_alloc(&q.d.beta, nq));
+    for (size_t s = 0; s < nq; ++s) t[s] = beta[queued[slot[s]]];
+    CUDA_TRY(cudaMemcpy(q.d.beta, t.data(), nq * 8, cudaMemcpyHostToDevice));
+    std::vector<unsigned long long> qi(nq);
+    for (size_t s = 0; s < nq; ++s) qi[s] = id[queued[slot[s]]];
+    TRY(device_alloc(&q.d.id, nq));
+    CUDA_TRY(cudaMemcpy(q.d.id, qi.data(), nq * 8, cudaMemcpyHostToDevice));
+  }
+  // The retained list, in order, with its held state.
+  const size_t nk = kept.size();
+  if (nk) {
+    double* pd[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
+    std::vector<double> t(nk);
+    for (int k = 0; k < 8; ++k) {
+      for (size_t s = 0; s < nk; ++s) t[s] = v[k][kept[s]];
+      CUDA_TRY(cudaMemcpy(pd[k], t.data(), nk * 8, cudaMemcpyHostToDevice));
+    }
+    for (size_t s = 0; s < nk; ++s) t[s] = beta[kept[s]];
+    CUDA_TRY(cudaMemcpy(r->p.beta, t.data(), nk * 8, cudaMemcpyHostToDevice));
+    std::vector<unsigned long long> ki(nk), ko(nk);
+    std::vector<unsigned char> kf(nk);
+    uint64_t held = 0;
+    for (size_t s = 0; s < nk; ++s) {
+      ki[s] = id[kept[s]];
+      ko[s] = s;
+      kf[s] = frozen[kept[s]] ? 1 : 0;
+      held += kf[s];
+    }
+    CUDA_TRY(cudaMemcpy(r->p.id, ki.data(), nk * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(r->p.order, ko.data(), nk * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(r->p.frozen, kf.data(), nk, cudaMemcpyHostToDevice));
+    r->held = held;
+  } else {
+    r->held = 0;
+  }
+  r->np = nk;
+  r->next_order = nk;
+  q.extracted = true;
+  advance_next_due(q);
+  TRY(sort_particles(r));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_get_held(aprl_run* r, size_t capacity, uint8_t* frozen, double* beta,
+                              size_t* count) {
+  if (!r || !count) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (capacity < r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const size_t n = r->np;
+  std::vector<size_t> perm;
+  TRY(storage_permutation(r, r->p.order, n, perm));
+  if (frozen && n) {
+    std::vector<unsigned char> f(n);
+    CUDA_TRY(cudaMemcpy(f.data(), r->p.frozen, n, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) frozen[i] = f[perm[i]];
+  }
+  if (beta && n) {
+    std::vector<double> b(n);
+    CUDA_TRY(cudaMemcpy(b.data(), r->p.beta, n * 8, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) beta[i] = b[perm[i]];
   }
   *count = n;
   return APRL_OK;
@@ -1414,6 +1698,10 @@ aprl_status aprl_run_get_stats(const aprl_run* r, aprl_step_stats* st) {
   st->origin_z = r->origin[2];
   st->time_box = r->time;
   st->device_error = r->h_status ? r->h_status->code : 0;
+  st->pending = r->queue.extracted ? r->queue.n - r->queue.cursor : 0;
+  st->admitted = r->admitted;
+  st->activations = r->cumulative.activations;
+  st->held = r->held;
   return APRL_OK;
 }
 

@@ -38,6 +38,8 @@ _SIGNATURES = {
     "run_set_particles": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D,
                                     _D, _D, _U64, C.c_int]),
     "run_particle_count": (C.c_int, [_H, _SZ]),
+    "run_set_held": (C.c_int, [_H, C.c_size_t, C.POINTER(C.c_uint8), _D]),
+    "run_get_held": (C.c_int, [_H, C.c_size_t, C.POINTER(C.c_uint8), _D, _SZ]),
     "run_get_particles": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D,
                                     _D, _D, _U64, _SZ]),
     "run_carrier_count": (C.c_int, [_H, _SZ]),
@@ -211,6 +213,21 @@ class Run:
                *[_ptr(c) for c in cols], _ptr(ids, C.c_uint64),
                1 if reset_carriers else 0)
 
+    def set_held(self, frozen, beta):
+        """Frozen flags + held speeds for the current list, then the
+        pending-queue extraction."""
+        f = np.ascontiguousarray(frozen, dtype=np.uint8)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        self.b("run_set_held", self.handle, f.size, _ptr(f, C.c_uint8), _ptr(b))
+
+    def get_held(self):
+        n = self.particle_count()
+        f = np.empty(n, dtype=np.uint8)
+        b = np.empty(n)
+        count = C.c_size_t()
+        self.b("run_get_held", self.handle, n, _ptr(f, C.c_uint8), _ptr(b), C.byref(count))
+        return f, b
+
     def particle_count(self):
         n = C.c_size_t()
         self.b("run_particle_count", self.handle, C.byref(n))
@@ -256,6 +273,9 @@ class Run:
         for a, f in enumerate(workload.fields):
             self.set_field(a, f)
         self.set_particles(workload.particles)
+        held = getattr(workload, "held", None)
+        if held is not None:
+            self.set_held(held, workload.particles["beta_held"])
         return self
 
     # -- operators ------------------------------------------------------

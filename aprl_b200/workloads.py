@@ -96,7 +96,7 @@ class Workload:
 
 def make_config(nx, ny, nz, dx, dy, dz, cpml_cells, boost_gamma, shape,
                 steps, substeps=1, magnets=(), right_margin=None,
-                translation_beta=1.0):
+                translation_beta=1.0, release_cells=6):
     """Run configuration of a moving window with `steps` of inlet reference."""
     cfg = abi.RunConfig()
     cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
@@ -134,6 +134,11 @@ def make_config(nx, ny, nz, dx, dy, dz, cpml_cells, boost_gamma, shape,
     safe_exit = (nz - right_margin) * dz          # box z at t = 0
     # labZFromBoxZT(safe_exit, 0) = labZOrigin + gamma*(z - boxZOrigin)
     cfg.exit_lab_z = cfg.lab_z_origin + boost_gamma * (safe_exit - cfg.box_z_origin)
+    # Held particles release at a fixed lab plane `release_cells` above the
+    # window inlet at t = 0 (startCell = release - lowerGuardCells,
+    # src/simulation_moving_window.cpp:83).
+    cfg.activation_plane_lab_z = cfg.lab_z_origin + boost_gamma * (release_cells * dz)
+    cfg.maximum_step = steps
     cfg.n_magnets = len(magnets)
     for n, m in enumerate(magnets):
         cfg.magnets[n] = m
@@ -174,9 +179,21 @@ def planar_undulator(k_parameter, period, entrance_z, periods, angle=0.0):
     return m
 
 
+def held_beta_z(u_lab, boost_gamma):
+    """BoostFrameTransform::heldLongitudinalBetaZ for a lab proper velocity:
+    keep only lab u_z, boost it, beta = u/hypot(1, u)
+    (src/boostframe.cpp:96-107)."""
+    gb = gamma_beta_from_gamma(boost_gamma)
+    uz = u_lab[:, 2]
+    g = np.sqrt(1.0 + uz * uz)
+    positive = np.where(uz >= 0.0, g + uz, 1.0 / (g - uz)) / (boost_gamma + gb)
+    u_box = 0.5 * (positive - 1.0 / positive)
+    return u_box / np.hypot(1.0, u_box)
+
+
 def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
                    emittance_n, energy_spread, seed=17, margin_cells=3,
-                   z_fraction=(0.05, 0.95)):
+                   z_fraction=(0.05, 0.95), z_range=None):
     """Box-frame snapshot of a lab-frame Gaussian electron bunch, truncated
     to the moving window's trusted particle region (inside the transverse
     CPML by `margin_cells`, above the inlet guard, below the exit plane)."""
@@ -193,6 +210,8 @@ def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
     exit_box = cfg.exit_lab_z / boost
     z_lo = 2.0 * cfg.dz + z_fraction[0] * (exit_box - 2.0 * cfg.dz)
     z_hi = 2.0 * cfg.dz + z_fraction[1] * (exit_box - 2.0 * cfg.dz)
+    if z_range is not None:
+        z_lo, z_hi = z_range
     z_center = 0.5 * (z_lo + z_hi)
 
     if not (x_lo < x_hi and y_lo < y_hi and z_lo < z_hi):
@@ -227,7 +246,9 @@ def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
     u_box = proper_velocity_lab_to_box(u_lab, boost)
     electrons = charge_c / ELEMENTARY_CHARGE
     per = electrons / count
+    beta_held = held_beta_z(u_lab, boost)
     return {
+        "beta_held": np.ascontiguousarray(beta_held),
         "x": np.ascontiguousarray(x), "y": np.ascontiguousarray(y),
         "z": np.ascontiguousarray(z),
         "ux": np.ascontiguousarray(u_box[:, 0]),
@@ -304,6 +325,35 @@ def dipole_c2(steps=2000, particles=1_000_000, shape="linear-binomial3",
                     description={"cells": [128, 128, 512], "particles": particles,
                                  "shape": shape, "boost_gamma": 10.0,
                                  "dipole_T": 1.0})
+
+
+def split_held(cfg, bunch):
+    """Frozen flags for held lab-plane injection: particles below the
+    activation plane's box position at t = 0 are held (src/eb_bunch.cpp)."""
+    release_box = (cfg.activation_plane_lab_z - cfg.lab_z_origin) / cfg.boost_gamma
+    return (bunch["z"] < release_box).astype(np.uint8)
+
+
+def streaming_case(nx=16, ny=16, nz=40, particles=600, steps=12,
+                   shape="linear-binomial3", magnets=None, seed=5, cpml=4,
+                   upstream_cells=24, margin_cells=2):
+    """A bunch straddling the inlet: pending upstream, held between the
+    inlet and the activation plane, active above it."""
+    if magnets is None:
+        magnets = [dipole(1.0)]
+    cfg = make_config(nx, ny, nz, 5e-6, 5e-6, 2e-6, cpml, 10.0, shape, steps,
+                      magnets=magnets)
+    exit_box = cfg.exit_lab_z / cfg.boost_gamma
+    z_range = (-upstream_cells * cfg.dz, 0.8 * exit_box)
+    bunch = gaussian_bunch(cfg, particles, 20e-12, 1e9, 12e-6, 10e-6, 1e-6,
+                           1e-4, seed=seed, z_range=z_range,
+                           margin_cells=margin_cells)
+    w = Workload(f"stream-{nx}x{ny}x{nz}", cfg, bunch, synthetic_reference(cfg),
+                 synthetic_fields(cfg), steps=steps,
+                 description={"cells": [nx, ny, nz], "particles": particles,
+                              "shape": shape, "held_injection": True})
+    w.held = split_held(cfg, bunch)
+    return w
 
 
 def small_case(nx=16, ny=16, nz=40, particles=400, steps=6,

@@ -112,6 +112,10 @@ typedef struct {
   uint64_t reference_nz;          /* prepared reference cells in z */
   double translation_beta;        /* inlet lerp speed, in cells per step */
   double exit_lab_z;              /* fixed-lab particle exit plane */
+  /* held lab-plane injection (src/config.cpp:2072-2076): held particles move
+   * along z at c*frozenBetaZ until they cross this fixed lab plane */
+  double activation_plane_lab_z;
+  uint64_t maximum_step;          /* pending-queue horizon (PendingWindowGeometry) */
   /* prescribed lab magnets (SIFieldSourceSet::addPrescribedLabMagnet) */
   uint32_t n_magnets;
   uint32_t reserved1;
@@ -143,6 +147,10 @@ typedef struct {
   double time_box;               /* box time after the last step */
   uint32_t device_error;         /* first device error code seen (0 = none) */
   uint32_t reserved;
+  uint64_t pending;              /* held particles still upstream in the queue */
+  uint64_t admitted;             /* cumulative PendingParticleQueue::admit count */
+  uint64_t activations;          /* cumulative activation-plane crossings */
+  uint64_t held;                 /* held (frozen) particles in the list */
 } aprl_step_stats;
 
 typedef struct aprl_run aprl_run;
@@ -216,6 +224,16 @@ aprl_status aprl_run_set_particles(aprl_run* run, size_t count,
                                    const double* charge, const double* mass,
                                    const uint64_t* id, int reset_carriers);
 aprl_status aprl_run_particle_count(const aprl_run* run, size_t* count);
+/* Held lab-plane injection state of the current list: frozen flag and held
+ * speed frozenBetaZ per particle (src/eb_particles.h:21-22), followed by
+ * PendingParticleQueue::extract (src/pending_particle_queue.cpp:128-154):
+ * held particles upstream of the inlet that do not take part in the first
+ * step leave the list for the queue, in their order; the rest stay. */
+aprl_status aprl_run_set_held(aprl_run* run, size_t count, const uint8_t* frozen,
+                              const double* frozen_beta_z);
+/* Frozen flags and held speeds of the current list (reference order). */
+aprl_status aprl_run_get_held(aprl_run* run, size_t capacity, uint8_t* frozen,
+                              double* frozen_beta_z, size_t* count);
 aprl_status aprl_run_get_particles(aprl_run* run, size_t capacity,
                                    double* x, double* y, double* z,
                                    double* ux, double* uy, double* uz,

@@ -24,7 +24,7 @@ DEFAULT_REFERENCE_SRC = "/root/reference/src"
 REFERENCE_UNITS = [
     "eb_field", "eb_cpml", "eb_deposition", "eb_particles", "boostframe",
     "eb_sources", "compute_threads", "source_coupling",
-    "moving_window_fields", "particle_boundary",
+    "moving_window_fields", "particle_boundary", "pending_particle_queue",
 ]
 
 

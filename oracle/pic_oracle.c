@@ -77,7 +77,21 @@ typedef struct {
   double pos[3], u[3];
   double q, m;
   uint64_t id;
+  int frozen;      /* RelativisticParticleSI::frozen */
+  double beta;     /* RelativisticParticleSI::frozenBetaZ */
 } particle_t;
+
+/* PendingParticleQueue (src/pending_particle_queue.h:24-76) at one rank. */
+typedef struct {
+  particle_t* p;        /* pending_: initial states, extraction order */
+  size_t n;
+  size_t* order;        /* order_: indices sorted by due step (stable) */
+  size_t* offsets;      /* offsets_: buckets + 1 prefix counts */
+  size_t buckets;
+  size_t cursor;
+  uint64_t next_due, last_step, initial_step, maximum_step;
+  int extracted;
+} pending_t;
 
 typedef struct {
   double pos[3], vel[3];
@@ -148,16 +162,21 @@ struct oracle_run {
   int replay;
   int stage; /* 0 idle, 1 magnetic done, 2 preview done, 3 trial done */
   uint32_t trials_this_step;
+  pending_t pending;
+  uint64_t admitted, activations;
   /* saved state of the step (solveConservativeSourceStep restore()) */
   particle_t* saved_p;
   size_t saved_np;
   carrier_t* saved_c;
   size_t saved_nc;
-  uint64_t saved_exits;
+  uint64_t saved_exits, saved_activations;
   double saved_exit_charge;
   uint64_t saved_counts[3][6];
   double saved_charges[3][6];
 };
+
+static aprl_status pending_extract(oracle_run* r);
+static aprl_status pending_admit(oracle_run* r);
 
 static void* xrealloc(void* p, size_t bytes) {
   void* q = realloc(p, bytes ? bytes : 1);
@@ -851,6 +870,7 @@ aprl_status oracle_run_destroy(oracle_run* r) {
       if (r->has_eterm[a][d]) { free(r->eterm[a][d].base); free(r->eterm[a][d].history); }
     }
   }
+  free(r->pending.p); free(r->pending.order); free(r->pending.offsets);
   free(r->delta); free(r->p); free(r->c); free(r->slot); free(r->retained);
   free(r->rcarrier); free(r->saved_p); free(r->saved_c);
   free(r);
@@ -934,9 +954,31 @@ aprl_status oracle_run_set_particles(oracle_run* r, size_t n, const double* x, c
     p->pos[0] = x[i]; p->pos[1] = y[i]; p->pos[2] = z[i];
     p->u[0] = ux[i]; p->u[1] = uy[i]; p->u[2] = uz[i];
     p->q = q[i]; p->m = m[i]; p->id = id[i];
+    p->frozen = 0; p->beta = 0.0;
   }
   r->np = n;
   if (reset_carriers) r->nc = 0;
+  return APRL_OK;
+}
+
+aprl_status oracle_run_set_held(oracle_run* r, size_t n, const uint8_t* frozen,
+                                const double* beta) {
+  if (n != r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Held state must cover the particle list");
+  for (size_t i = 0; i < n; ++i) {
+    r->p[i].frozen = frozen[i] ? 1 : 0;
+    r->p[i].beta = beta[i];
+  }
+  return pending_extract(r);
+}
+
+aprl_status oracle_run_get_held(oracle_run* r, size_t capacity, uint8_t* frozen, double* beta,
+                                size_t* count) {
+  if (capacity < r->np) return fail(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  for (size_t i = 0; i < r->np; ++i) {
+    if (frozen) frozen[i] = (uint8_t)r->p[i].frozen;
+    if (beta) beta[i] = r->p[i].beta;
+  }
+  *count = r->np;
   return APRL_OK;
 }
 
@@ -1318,6 +1360,10 @@ static void clear_current(oracle_run* r) {
 }
 
 aprl_status oracle_run_advance_magnetic(oracle_run* r) {
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
+  /* admitMovingWindowParticles (src/simulation.cpp:513). */
+  aprl_status admitted = pending_admit(r);
+  if (admitted != APRL_OK) return admitted;
   /* Simulation::solve (src/simulation.cpp:518-524): clearCurrent, then
    * Boundary::begin (src/moving_window_fields.cpp:192-216) fills the lower
    * halo planes from the reference at (offset-1, step); the upper planes are
@@ -1401,6 +1447,7 @@ aprl_status oracle_run_preview_electric(oracle_run* r) {
   memcpy(r->saved_c, r->c, r->nc * sizeof(carrier_t));
   r->saved_nc = r->nc;
   r->saved_exits = r->exits;
+  r->saved_activations = r->activations;
   r->saved_exit_charge = r->exit_charge;
   memcpy(r->saved_counts[0], r->cpml_entries, sizeof r->cpml_entries);
   memcpy(r->saved_counts[1], r->direct_outer, sizeof r->direct_outer);
@@ -1448,6 +1495,7 @@ static void restore_state(oracle_run* r) {
   memcpy(r->c, r->saved_c, r->saved_nc * sizeof(carrier_t));
   r->nc = r->saved_nc;
   r->exits = r->saved_exits;
+  r->activations = r->saved_activations;
   r->exit_charge = r->saved_exit_charge;
   memcpy(r->cpml_entries, r->saved_counts[0], sizeof r->cpml_entries);
   memcpy(r->direct_outer, r->saved_counts[1], sizeof r->direct_outer);
@@ -1653,6 +1701,25 @@ static void deposit_visit(visitor_t* v, unsigned a, long long i, long long j,
   }
   const double value = dv->scale[a] * w;
   if (k >= 0 && k < (long long)c->nz) AT(c, (size_t)i, (size_t)j, (size_t)k) += value;
+}
+
+/* longitudinal_shape::Current::deposit without the depositor's endpoint
+ * validation: ConservativeSourceCoupling::depositFrozenSourceSupport
+ * (src/source_coupling.cpp:73-78) deposits held sources this way. */
+static aprl_status deposit_current(oracle_run* r, const double begin[3], const double end[3],
+                                   double charge) {
+  const aprl_run_config* g = &r->cfg;
+  deposit_visitor dv;
+  dv.base.visit = deposit_visit;
+  dv.r = r;
+  dv.error = 0;
+  for (int a = 0; a < 3; ++a)
+    dv.scale[a] = charge * (end[a] - begin[a]) / (g->dx * g->dy * g->dz * g->dt);
+  if (shape_weights(g, r->origin, begin, end, &dv.base) < 0)
+    return fail(APRL_ERR_RUNTIME, "Quintic orbit exceeds crossing budget");
+  if (dv.error == 1) return fail(APRL_ERR_OUT_OF_RANGE, "Transverse current support outside x grid");
+  if (dv.error == 2) return fail(APRL_ERR_OUT_OF_RANGE, "Transverse current support outside y grid");
+  return APRL_OK;
 }
 
 /* ChargeConservingCurrentDepositor::depositSegment -> Current::deposit. */
@@ -1935,10 +2002,11 @@ static aprl_status process_carrier_segment(oracle_run* r, const cpml_region* reg
   return APRL_OK;
 }
 
-/* ConservativeSourceCoupling::push (src/source_coupling.cpp:90-104). */
-static aprl_status coupling_push(oracle_run* r, particle_t* p, slot_t* q) {
+/* ConservativeSourceCoupling::push (src/source_coupling.cpp:90-104) for a
+ * push of `dt` starting at box time `time`. */
+static aprl_status coupling_push(oracle_run* r, particle_t* p, slot_t* q, double time,
+                                 double dt) {
   const aprl_run_config* g = &r->cfg;
-  const double dt = g->dt, time = r->time;
   const unsigned steps = g->substeps;
   if (r->replay) {
     if (!q->seen || q->time != time || q->dt != dt)
@@ -2003,73 +2071,379 @@ static aprl_status coupling_push(oracle_run* r, particle_t* p, slot_t* q) {
   return APRL_OK;
 }
 
-/* pushDepositAndMigrate at one rank for active particles and CPML carriers
- * (src/simulation.cpp:4167-5368, processActiveSegment 4555-4917). */
-static aprl_status push_deposit(oracle_run* r) {
+/* ---- held lab-plane injection (src/pending_particle_queue.cpp,
+ *      src/simulation.cpp:4919-5035, 5083-5160) --------------------------- */
+static uint64_t dbits(double v) { uint64_t b; memcpy(&b, &v, 8); return b; }
+static double dfrom(uint64_t b) { double v; memcpy(&v, &b, 8); return v; }
+static uint64_t ordered_bits(uint64_t v) {
+  return (v & 0x8000000000000000ull) ? ~v : v ^ 0x8000000000000000ull;
+}
+static double from_ordered(uint64_t v) {
+  return dfrom((v & 0x8000000000000000ull) ? v ^ 0x8000000000000000ull : ~v);
+}
+static int same_spacing(uint64_t a, uint64_t b) {
+  const uint64_t m = 0x8000000000000000ull | 0x7ff0000000000000ull;
+  return (a & m) == (b & m);
+}
+
+/* repeatPositive (src/pending_particle_queue.cpp:38-71): `count` separately
+ * rounded additions, skipping constant-spacing runs with integer ULP steps. */
+static double repeat_positive(double x, double increment, size_t count, int* overflow) {
+  while (count) {
+    const double y = x + increment;
+    if (!isfinite(y)) { *overflow = 1; return y; }
+    if (count == 1 || y == x) return y;
+    const double z = y + increment;
+    const uint64_t bx = dbits(x), by = dbits(y), bz = dbits(z);
+    if (isfinite(z) && same_spacing(bx, by) && same_spacing(by, bz)) {
+      const uint64_t ox = ordered_bits(bx), oy = ordered_bits(by), oz = ordered_bits(bz);
+      const uint64_t stride = oy - ox;
+      if (stride && oz - oy == stride) {
+        const uint64_t last_bits = (bx & 0x8000000000000000ull)
+                                       ? bx & (0x8000000000000000ull | 0x7ff0000000000000ull)
+                                       : bx | 0x000fffffffffffffull;
+        const uint64_t available = (ordered_bits(last_bits) - ox) / stride;
+        const uint64_t safe = available ? available - 1 : 0;
+        const size_t jump = (size_t)(safe < count ? safe : count);
+        if (jump) {
+          x = from_ordered(ox + (uint64_t)jump * stride);
+          count -= jump;
+          continue;
+        }
+      }
+    }
+    x = y;
+    --count;
+  }
+  return x;
+}
+
+/* repeatHeldAddition (src/pending_particle_queue.cpp:73-88). */
+static double repeat_held_addition(double initial, double increment, size_t count) {
+  int overflow = 0;
+  if (!count) return initial;
+  if (increment < 0.) {
+    const double result = -repeat_positive(-initial, -increment, count, &overflow);
+    return result == 0. ? 0. : result;
+  }
+  return repeat_positive(initial, increment, count, &overflow);
+}
+
+static double held_increment(const oracle_run* r, const particle_t* p) {
+  return SI_C * r->cfg.dt * p->beta;  /* heldDistancePerBeta * frozenBetaZ */
+}
+
+/* PendingParticleQueue::origin (src/pending_particle_queue.cpp:106-111). */
+static double pending_origin(const oracle_run* r, uint64_t step) {
+  const int64_t offset = r->cfg.initial_offset - (int64_t)step;
+  return fma((double)offset, r->cfg.dz, r->cfg.reference_origin[2]);
+}
+
+/* participates (src/pending_particle_queue.cpp:113-117). */
+static int participates(const oracle_run* r, const particle_t* p, uint64_t step) {
+  const double end = repeat_held_addition(p->pos[2], held_increment(r, p),
+                                          step - r->pending.initial_step + 1);
+  return end >= pending_origin(r, step);
+}
+
+/* firstDue (src/pending_particle_queue.cpp:119-126). */
+static uint64_t first_due(const oracle_run* r, const particle_t* p) {
+  const pending_t* q = &r->pending;
+  const double increment = held_increment(r, p);
+  const long double distance = (long double)pending_origin(r, q->initial_step) -
+                               (long double)p->pos[2] - (long double)increment;
+  const long double estimate = ceill(distance / ((long double)r->cfg.dz + (long double)increment));
+  const uint64_t sentinel = q->maximum_step + 1;
+  const long double steps_left = (long double)(q->maximum_step - q->initial_step);
+  const uint64_t guess = estimate > steps_left
+                             ? sentinel
+                             : q->initial_step + (uint64_t)(estimate > 1.L ? estimate : 1.L);
+  if (guess <= q->maximum_step && participates(r, p, guess) && !participates(r, p, guess - 1))
+    return guess;
+  if (guess == sentinel && !participates(r, p, q->maximum_step)) return sentinel;
+  uint64_t lower = q->initial_step + 1, upper = sentinel;
+  while (lower < upper) {
+    const uint64_t middle = lower + (upper - lower) / 2;
+    if (participates(r, p, middle)) upper = middle;
+    else lower = middle + 1;
+  }
+  return lower;
+}
+
+static void advance_next_due(pending_t* q) {
+  while (q->next_due <= q->maximum_step &&
+         q->offsets[q->next_due - q->initial_step + 1] <= q->cursor)
+    ++q->next_due;
+}
+
+/* PendingParticleQueue::extract (src/pending_particle_queue.cpp:128-154). */
+static aprl_status pending_extract(oracle_run* r) {
+  pending_t* q = &r->pending;
+  if (q->extracted) return fail(APRL_ERR_RUNTIME, "Pending queue can only be initialized once");
+  q->initial_step = r->step;
+  q->last_step = r->step;
+  q->maximum_step = r->cfg.maximum_step;
+  q->next_due = r->step;
+  if (!(r->cfg.dz > 0.) || q->initial_step > q->maximum_step)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid pending-window geometry/horizon");
+  q->buckets = (size_t)(q->maximum_step - q->initial_step + 2);
+  q->offsets = (size_t*)calloc(q->buckets + 1, sizeof(size_t));
+  q->p = (particle_t*)malloc((r->np ? r->np : 1) * sizeof(particle_t));
+  size_t* due = (size_t*)malloc((r->np ? r->np : 1) * sizeof(size_t));
+  const double inlet = pending_origin(r, q->initial_step);
+  size_t retained = 0;
+  q->n = 0;
+  for (size_t i = 0; i < r->np; ++i) {
+    const particle_t particle = r->p[i];
+    if (particle.frozen && particle.pos[2] < inlet && particle.beta >= 0. &&
+        !participates(r, &particle, q->initial_step)) {
+      const uint64_t event = first_due(r, &particle);
+      due[q->n] = (size_t)(event - q->initial_step);
+      ++q->offsets[event - q->initial_step + 1];
+      q->p[q->n++] = particle;
+    } else {
+      r->p[retained++] = particle;
+    }
+  }
+  r->np = retained;
+  for (size_t i = 1; i < q->buckets + 1; ++i) q->offsets[i] += q->offsets[i - 1];
+  q->order = (size_t*)malloc((q->n ? q->n : 1) * sizeof(size_t));
+  size_t* insertion = (size_t*)malloc((q->buckets + 1) * sizeof(size_t));
+  memcpy(insertion, q->offsets, (q->buckets + 1) * sizeof(size_t));
+  for (size_t i = 0; i < q->n; ++i) q->order[insertion[due[i]]++] = i;
+  free(insertion);
+  free(due);
+  q->extracted = 1;
+  advance_next_due(q);
+  return APRL_OK;
+}
+
+/* PendingParticleQueue::admit (src/pending_particle_queue.cpp:163-186). */
+static aprl_status pending_admit(oracle_run* r) {
+  pending_t* q = &r->pending;
+  if (!q->extracted) return APRL_OK;
+  const uint64_t step = r->step;
+  if (step < q->last_step || step > q->maximum_step || step > q->next_due)
+    return fail(APRL_ERR_RUNTIME, "Pending admission skipped an event or exceeds its horizon");
+  q->last_step = step;
+  const size_t end = q->offsets[step - q->initial_step + 1];
+  const size_t need = r->np + (end - q->cursor);
+  if (need > r->pcap) {
+    r->pcap = need;
+    r->p = (particle_t*)xrealloc(r->p, r->pcap * sizeof(particle_t));
+  }
+  while (q->cursor < end) {
+    particle_t particle = q->p[q->order[q->cursor]];
+    particle.pos[2] = repeat_held_addition(particle.pos[2], held_increment(r, &particle),
+                                           step - q->initial_step);
+    r->p[r->np++] = particle;
+    ++q->cursor;
+    ++r->admitted;
+  }
+  advance_next_due(q);
+  return APRL_OK;
+}
+
+/* Frozen source support of the pending particles due within 8 steps
+ * (visitNear + depositFrozenSourceSupport, src/simulation.cpp:4170-4172). */
+static aprl_status pending_support(oracle_run* r) {
+  const pending_t* q = &r->pending;
+  if (!q->extracted) return APRL_OK;
+  const uint64_t step = r->step;
+  const uint64_t room = q->maximum_step - step;
+  const uint64_t until = step + (8 < room ? 8 : room);
+  const size_t end = q->offsets[until - q->initial_step + 1];
+  for (size_t n = q->cursor; n < end; ++n) {
+    particle_t p = q->p[q->order[n]];
+    p.pos[2] = repeat_held_addition(p.pos[2], held_increment(r, &p), step - q->initial_step);
+    double stop[3] = {p.pos[0], p.pos[1], p.pos[2]};
+    stop[2] += SI_C * r->cfg.dt * p.beta;
+    aprl_status s = deposit_current(r, p.pos, stop, p.q);
+    if (s != APRL_OK) return s;
+  }
+  return APRL_OK;
+}
+
+/* processActiveSegment at one rank (src/simulation.cpp:4555-4917), with the
+ * held-activation kink (src/simulation.cpp:4684-4756); `cached` holds the
+ * diagnostic boundary hits when the segment has no kink. */
+typedef struct {
+  boundary_hit cpml_hit, outer_hit;
+  int enters, exits;
+} segment_hits;
+
+static aprl_status process_active_segment(oracle_run* r, const cpml_region* reg,
+                                          particle_t particle, double seg_start[3],
+                                          double seg_start_fraction, const double* kink,
+                                          double kink_fraction, const segment_hits* cached) {
   const double crossing_tolerance = 64.0 * DBL_EPSILON;
+  aprl_status s;
+  if (kink) {
+    boundary_hit ch, oh;
+    int e1 = 0, e2 = 0;
+    s = cpml_first_entry(r, reg, seg_start, kink, &ch, &e1);
+    if (s != APRL_OK) return s;
+    s = outer_first_exit(r, seg_start, kink, &oh, &e2);
+    if (s != APRL_OK) return s;
+    if (e1 || e2)
+      return fail(APRL_ERR_RUNTIME,
+                  "Held-transverse activation crossed a particle boundary during the frozen part of a field step");
+    s = deposit_segment(r, seg_start, kink, particle.q);
+    if (s != APRL_OK) return s;
+    for (int a = 0; a < 3; ++a) seg_start[a] = kink[a];
+    seg_start_fraction = kink_fraction;
+  }
+  segment_hits computed;
+  if (!cached) {
+    s = moving_window_entry(r, reg, seg_start, particle.pos, seg_start_fraction,
+                            &computed.cpml_hit, &computed.enters);
+    if (s != APRL_OK) return s;
+    s = outer_first_exit(r, seg_start, particle.pos, &computed.outer_hit, &computed.exits);
+    if (s != APRL_OK) return s;
+    cached = &computed;
+  }
+  int action = 0;
+  double local_end = 1.0, seg_end[3] = {particle.pos[0], particle.pos[1], particle.pos[2]};
+  boundary_hit selected;
+  if (cached->enters &&
+      (!cached->exits || cached->cpml_hit.fraction <= cached->outer_hit.fraction + crossing_tolerance)) {
+    action = 1;
+    selected = cached->cpml_hit;
+  } else if (cached->exits) {
+    action = 2;
+    selected = cached->outer_hit;
+  }
+  if (action) {
+    local_end = selected.fraction;
+    for (int a = 0; a < 3; ++a) seg_end[a] = selected.position[a];
+  }
+  s = deposit_segment(r, seg_start, seg_end, particle.q);
+  if (s != APRL_OK) return s;
+  const double global_end = seg_start_fraction + local_end * (1.0 - seg_start_fraction);
+  if (action == 1) {
+    if (selected.face == 5) {
+      ++r->exits;
+      r->exit_charge += particle.q;
+    } else {
+      ++r->cpml_entries[selected.face];
+      r->cpml_entry_charge[selected.face] += particle.q;
+    }
+    carrier_t c;
+    for (int a = 0; a < 3; ++a) c.pos[a] = particle.pos[a];
+    const double gamma = gamma_u(particle.u);
+    for (int a = 0; a < 3; ++a) c.vel[a] = particle.u[a] * (SI_C / gamma);
+    c.q = particle.q;
+    c.w = 1.0;
+    return process_carrier_segment(r, reg, c, selected.position, global_end);
+  }
+  if (action == 2) {
+    ++r->direct_outer[selected.face];
+    r->direct_outer_charge[selected.face] += particle.q;
+    return APRL_OK;
+  }
+  push_retained(r, &particle);
+  return APRL_OK;
+}
+
+/* pushDepositAndMigrate at one rank (src/simulation.cpp:4167-5368): frozen
+ * source support of the pending queue, CPML carriers, then every particle:
+ * prepareParticle (held advance, activation crossing, coupled push) and the
+ * serial deposit / boundary pass in list order. */
+static aprl_status push_deposit(oracle_run* r) {
   cpml_region reg;
   make_cpml_region(r, &reg);
   r->nretained = 0;
   r->nrcarrier = 0;
+  aprl_status s = pending_support(r);
+  if (s != APRL_OK) return s;
   for (size_t n = 0; n < r->nc; ++n) {
     carrier_t c = r->c[n];
     const double start[3] = {c.pos[0], c.pos[1], c.pos[2]};
     for (int a = 0; a < 3; ++a) c.pos[a] += r->cfg.dt * c.vel[a];
-    aprl_status s = process_carrier_segment(r, &reg, c, start, 0.0);
+    s = process_carrier_segment(r, &reg, c, start, 0.0);
     if (s != APRL_OK) return s;
   }
+  const double t = r->time, dt = r->cfg.dt;
   for (size_t n = 0; n < r->np; ++n) {
-    particle_t p = r->p[n];
-    const double start[3] = {p.pos[0], p.pos[1], p.pos[2]};
-    if (start[2] < r->origin[2])
+    const particle_t original = r->p[n];
+    particle_t particle = original;
+    double start[3] = {original.pos[0], original.pos[1], original.pos[2]};
+    if (start[2] < r->origin[2] && !particle.frozen)
       return fail(APRL_ERR_RUNTIME,
                   "An active particle is upstream of the moving window; the inlet guard did not contain its release event");
-    aprl_status s = coupling_push(r, &p, &r->slot[n]);
-    if (s != APRL_OK) return s;
-    boundary_hit cpml_hit, outer_hit;
-    int enters = 0, exits = 0;
-    s = moving_window_entry(r, &reg, start, p.pos, 0.0, &cpml_hit, &enters);
-    if (s != APRL_OK) return s;
-    s = outer_first_exit(r, start, p.pos, &outer_hit, &exits);
-    if (s != APRL_OK) return s;
-    int action = 0; /* 0 retain, 1 enter CPML, 2 exit outer */
-    double local_end = 1.0, seg_end[3] = {p.pos[0], p.pos[1], p.pos[2]};
-    boundary_hit selected;
-    if (enters && (!exits || cpml_hit.fraction <= outer_hit.fraction + crossing_tolerance)) {
-      action = 1;
-      local_end = cpml_hit.fraction;
-      selected = cpml_hit;
-    } else if (exits) {
-      action = 2;
-      local_end = outer_hit.fraction;
-      selected = outer_hit;
-    }
-    if (action) for (int a = 0; a < 3; ++a) seg_end[a] = selected.position[a];
-    s = deposit_segment(r, start, seg_end, p.q);
-    if (s != APRL_OK) return s;
-    const double global_end = 0.0 + local_end * (1.0 - 0.0);
-    if (action == 1) {
-      if (selected.face == 5) {
-        ++r->exits;
-        r->exit_charge += p.q;
-      } else {
-        ++r->cpml_entries[selected.face];
-        r->cpml_entry_charge[selected.face] += p.q;
+    /* prepareParticle (src/simulation.cpp:4919-5035), holdTransverse. */
+    particle_t active_start = particle;
+    double active_start_time = t;
+    int has_active = !particle.frozen;
+    if (particle.frozen) {
+      const double beta_held = particle.beta;
+      const double start_lab_z = lab_z_from_box_zt(&r->cfg, start[2], t);
+      particle.pos[2] += SI_C * dt * beta_held;
+      const double end_lab_z = lab_z_from_box_zt(&r->cfg, particle.pos[2], t + dt);
+      if (end_lab_z >= r->cfg.activation_plane_lab_z) {
+        if (start[2] < r->origin[2])
+          return fail(APRL_ERR_RUNTIME,
+                      "A pending upstream held particle would release before a complete in-window step");
+        const double plane = r->cfg.activation_plane_lab_z;
+        const double crossing = start_lab_z >= plane
+                                    ? 0.0
+                                    : fmax(0.0, fmin(1.0, (plane - start_lab_z) / (end_lab_z - start_lab_z)));
+        for (int a = 0; a < 3; ++a) particle.pos[a] = start[a];
+        particle.pos[2] += SI_C * crossing * dt * beta_held;
+        particle.frozen = 0;
+        has_active = 1;
+        active_start = particle;
+        active_start_time = t + crossing * dt;
+        const double remaining = (1.0 - crossing) * dt;
+        if (remaining > 0.0) {
+          s = coupling_push(r, &particle, &r->slot[n], active_start_time, remaining);
+          if (s != APRL_OK) return s;
+        }
       }
-      carrier_t c;
-      for (int a = 0; a < 3; ++a) c.pos[a] = p.pos[a];
-      const double gamma = gamma_u(p.u);
-      for (int a = 0; a < 3; ++a) c.vel[a] = p.u[a] * (SI_C / gamma);
-      c.q = p.q;
-      c.w = 1.0;
-      s = process_carrier_segment(r, &reg, c, selected.position, global_end);
-      if (s != APRL_OK) return s;
-    } else if (action == 2) {
-      ++r->direct_outer[selected.face];
-      r->direct_outer_charge[selected.face] += p.q;
     } else {
-      push_retained(r, &p);
+      s = coupling_push(r, &particle, &r->slot[n], t, dt);
+      if (s != APRL_OK) return s;
     }
+    if (original.frozen && has_active) ++r->activations;
+    /* deposit and boundary pass (src/simulation.cpp:5083-5368) */
+    double seg_start_fraction = 0.0;
+    if (start[2] < r->origin[2]) {
+      if (!original.frozen || !particle.frozen || has_active)
+        return fail(APRL_ERR_RUNTIME,
+                    "Moving-window upstream admission requires an unreleased held particle on rank zero");
+      if (particle.pos[2] < r->origin[2]) {
+        s = deposit_current(r, start, particle.pos, particle.q);
+        if (s != APRL_OK) return s;
+        push_retained(r, &particle);
+        continue;
+      }
+      const double fraction = (r->origin[2] - start[2]) / (particle.pos[2] - start[2]);
+      if (!(fraction >= 0.0 && fraction <= 1.0) || !isfinite(fraction))
+        return fail(APRL_ERR_RUNTIME, "Invalid moving-window admission fraction");
+      double clipped[3];
+      for (int a = 0; a < 3; ++a) clipped[a] = start[a] + fraction * (particle.pos[a] - start[a]);
+      clipped[2] = r->origin[2];
+      seg_start_fraction = fraction;
+      s = deposit_current(r, original.pos, clipped, particle.q);
+      if (s != APRL_OK) return s;
+      for (int a = 0; a < 3; ++a) start[a] = clipped[a];
+    }
+    const int has_kink = original.frozen && has_active && active_start_time > t &&
+                         active_start_time < t + dt;
+    const double kink_fraction = (active_start_time - t) / dt;
+    if (has_kink) {
+      s = process_active_segment(r, &reg, particle, start, seg_start_fraction,
+                                 active_start.pos, kink_fraction, NULL);
+    } else {
+      segment_hits hits;
+      s = moving_window_entry(r, &reg, start, particle.pos, seg_start_fraction,
+                              &hits.cpml_hit, &hits.enters);
+      if (s != APRL_OK) return s;
+      s = outer_first_exit(r, start, particle.pos, &hits.outer_hit, &hits.exits);
+      if (s != APRL_OK) return s;
+      s = process_active_segment(r, &reg, particle, start, seg_start_fraction, NULL, 0.0, &hits);
+    }
+    if (s != APRL_OK) return s;
   }
   /* particles_ <- retained, pmlCarriers_ <- retainedCarriers. */
   if (r->nretained > r->pcap) {
@@ -2208,7 +2582,7 @@ aprl_status oracle_run_shift(oracle_run* r) {
   /* finishMovingWindowStep particle part (src/simulation_moving_window.cpp:352-371). */
   r->origin[2] = fma((double)r->offset, g->dz, g->reference_origin[2]);
   for (size_t n = 0; n < r->np; ++n)
-    if (r->p[n].pos[2] < r->origin[2])
+    if (r->p[n].pos[2] < r->origin[2] && !r->p[n].frozen)
       return fail(APRL_ERR_RUNTIME, "Active particle fell behind moving inlet");
   const double upper = fma((double)g->nz, g->dz, r->origin[2]);
   size_t kept = 0;
@@ -2292,6 +2666,10 @@ aprl_status oracle_run_get_stats(const oracle_run* r, aprl_step_stats* st) {
   st->window_offset = r->offset;
   st->origin_z = r->origin[2];
   st->time_box = r->time;
+  st->pending = r->pending.extracted ? r->pending.n - r->pending.cursor : 0;
+  st->admitted = r->admitted;
+  st->activations = r->activations;
+  for (size_t i = 0; i < r->np; ++i) st->held += r->p[i].frozen ? 1 : 0;
   return APRL_OK;
 }
 

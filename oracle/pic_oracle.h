@@ -49,6 +49,10 @@ aprl_status oracle_run_set_particles(oracle_run* run, size_t count,
                                      const double* charge, const double* mass,
                                      const uint64_t* id, int reset_carriers);
 aprl_status oracle_run_particle_count(const oracle_run* run, size_t* count);
+aprl_status oracle_run_set_held(oracle_run* run, size_t count, const uint8_t* frozen,
+                                const double* frozen_beta_z);
+aprl_status oracle_run_get_held(oracle_run* run, size_t capacity, uint8_t* frozen,
+                                double* frozen_beta_z, size_t* count);
 aprl_status oracle_run_get_particles(oracle_run* run, size_t capacity,
                                      double* x, double* y, double* z,
                                      double* ux, double* uy, double* uz,

@@ -40,6 +40,7 @@
 #include "longitudinal_shape.h"
 #include "moving_window_fields.h"
 #include "particle_boundary.h"
+#include "pending_particle_queue.h"
 #include "source_coupling.h"
 #include "source_coupling_math.h"
 
@@ -98,6 +99,8 @@ struct ref_run {
   unsigned trials = 0;
   int stage = 0;
   std::string directory;
+  std::unique_ptr<PendingParticleQueue> pending;
+  unsigned long long admitted = 0, activations = 0, savedActivations = 0;
 };
 
 namespace {
@@ -125,6 +128,7 @@ YeeComponent& component(EBFieldGrid& f, unsigned a) {
 }
 
 void save(ref_run& r) {
+  r.savedActivations = r.activations;
   r.savedParticles = r.particles;
   r.savedCarriers = r.carriers;
   r.savedExits = r.exits;
@@ -134,6 +138,7 @@ void save(ref_run& r) {
 }
 
 void restore(ref_run& r) {
+  r.activations = r.savedActivations;
   r.particles = r.savedParticles;
   r.carriers = r.savedCarriers;
   r.exits = r.savedExits;
@@ -209,38 +214,62 @@ void pushDepositAndMigrate(ref_run& r) {
     carrier.position = segmentEnd;
     retainedCarriers.push_back(carrier);
   };
+  if (r.pending)
+    r.pending->visitNear(r.step, 8, [&](const RelativisticParticleSI& p) {
+      auto end = p.position;
+      end[2] += SI::c * r.cfg.dt * p.frozenBetaZ;
+      r.coupling->depositFrozenSourceSupport(p.position, end, p.charge, false);
+    });
   for (std::size_t n = 0; n < r.carriers.size(); ++n) {
     ParticleCPMLCarrier carrier = r.carriers[n];
     const Vec start(carrier.position);
     carrier.position.pmv(r.cfg.dt, carrier.velocity);
     processCarrierSegment(carrier, start, 0.0);
   }
-  for (std::size_t n = 0; n < r.particles.size(); ++n) {
-    RelativisticParticleSI particle = r.particles[n];
-    const Vec start(particle.position);
-    if (start[2] < r.origin[2] && !particle.frozen)
-      throw std::runtime_error("An active particle is upstream of the moving window; the inlet guard did not contain its release event");
-    r.coupling->push(particle, r.sources, r.frame, r.time, r.cfg.dt, r.cfg.substeps, 0, 0, 0);
+  struct Hits {
     ParticleBoundaryHit cpmlHit, outerHit;
-    const bool entersCpml = firstMovingWindowEntry(r, cpml, start, particle.position, 0.0, cpmlHit);
-    const bool exitsOuter = boundary.firstExit(start, particle.position, outerHit);
+    bool entersCpml = false, exitsOuter = false;
+  };
+  // processActiveSegment (src/simulation.cpp:4555-4917) at one rank.
+  const auto processActiveSegment = [&](RelativisticParticleSI particle, Vec segmentStart,
+                                        Double segmentStartFraction, const Vec* kink,
+                                        Double kinkFraction, const Hits* cached) {
+    if (kink) {
+      ParticleBoundaryHit cpmlHit, outerHit;
+      const bool entersCpml = cpml.firstEntry(segmentStart, *kink, cpmlHit);
+      const bool exitsOuter = boundary.firstExit(segmentStart, *kink, outerHit);
+      if (entersCpml || exitsOuter)
+        throw std::runtime_error("Held-transverse activation crossed a particle boundary during the frozen part of a field step");
+      depositor.depositSegment(segmentStart, *kink, particle.charge);
+      segmentStart = *kink;
+      segmentStartFraction = kinkFraction;
+    }
+    Hits computed;
+    if (!cached) {
+      computed.entersCpml = firstMovingWindowEntry(r, cpml, segmentStart, particle.position,
+                                                   segmentStartFraction, computed.cpmlHit);
+      computed.exitsOuter = boundary.firstExit(segmentStart, particle.position, computed.outerHit);
+      cached = &computed;
+    }
     int action = 0;
     Double localEndFraction = 1.0;
     Vec segmentEnd(particle.position);
     ParticleBoundaryHit selected;
-    if (entersCpml && (!exitsOuter || cpmlHit.fraction <= outerHit.fraction + crossingTolerance)) {
+    if (cached->entersCpml &&
+        (!cached->exitsOuter ||
+         cached->cpmlHit.fraction <= cached->outerHit.fraction + crossingTolerance)) {
       action = 1;
-      localEndFraction = cpmlHit.fraction;
-      segmentEnd = cpmlHit.position;
-      selected = cpmlHit;
-    } else if (exitsOuter) {
+      localEndFraction = cached->cpmlHit.fraction;
+      segmentEnd = cached->cpmlHit.position;
+      selected = cached->cpmlHit;
+    } else if (cached->exitsOuter) {
       action = 2;
-      localEndFraction = outerHit.fraction;
-      segmentEnd = outerHit.position;
-      selected = outerHit;
+      localEndFraction = cached->outerHit.fraction;
+      segmentEnd = cached->outerHit.position;
+      selected = cached->outerHit;
     }
-    depositor.depositSegment(start, segmentEnd, particle.charge);
-    const Double globalEndFraction = 0.0 + localEndFraction * (1.0 - 0.0);
+    depositor.depositSegment(segmentStart, segmentEnd, particle.charge);
+    const Double globalEndFraction = segmentStartFraction + localEndFraction * (1.0 - segmentStartFraction);
     if (action == 1) {
       const std::size_t face = static_cast<std::size_t>(selected.face);
       if (selected.face == ParticleBoundaryFace::UpperZ) {
@@ -264,6 +293,75 @@ void pushDepositAndMigrate(ref_run& r) {
       r.charges[1][face] += particle.charge;
     } else {
       retained.push_back(particle);
+    }
+  };
+  const Double dt = r.cfg.dt, t = r.time;
+  for (std::size_t n = 0; n < r.particles.size(); ++n) {
+    const RelativisticParticleSI original = r.particles[n];
+    RelativisticParticleSI particle = original;
+    Vec start(particle.position);
+    if (start[2] < r.origin[2] && !particle.frozen)
+      throw std::runtime_error("An active particle is upstream of the moving window; the inlet guard did not contain its release event");
+    // prepareParticle (src/simulation.cpp:4919-5035) with holdTransverse.
+    RelativisticParticleSI activeStart = particle;
+    Double activeStartTime = t;
+    bool hasActiveSegment = !particle.frozen;
+    if (particle.frozen) {
+      const Double betaHeld = particle.frozenBetaZ;
+      const Double startLabZ = r.frame.labZFromBoxZT(start[2], t);
+      particle.position[2] += SI::c * dt * betaHeld;
+      const Double endLabZ = r.frame.labZFromBoxZT(particle.position[2], t + dt);
+      if (endLabZ >= r.cfg.activation_plane_lab_z) {
+        if (start[2] < r.origin[2])
+          throw std::runtime_error("A pending upstream held particle would release before a complete in-window step");
+        const Double plane = r.cfg.activation_plane_lab_z;
+        const Double crossingFraction = startLabZ >= plane ? 0.0 :
+          std::max(0.0, std::min(1.0, (plane - startLabZ) / (endLabZ - startLabZ)));
+        particle.position = start;
+        particle.position[2] += SI::c * crossingFraction * dt * betaHeld;
+        particle.frozen = false;
+        hasActiveSegment = true;
+        activeStart = particle;
+        activeStartTime = t + crossingFraction * dt;
+        const Double remaining = (1.0 - crossingFraction) * dt;
+        if (remaining > 0.0)
+          r.coupling->push(particle, r.sources, r.frame, activeStartTime, remaining,
+                           r.cfg.substeps, 0, 0, 0);
+      }
+    } else {
+      r.coupling->push(particle, r.sources, r.frame, t, dt, r.cfg.substeps, 0, 0, 0);
+    }
+    if (original.frozen && hasActiveSegment) ++r.activations;
+    Double segmentStartFraction = 0.0;
+    if (start[2] < r.origin[2]) {
+      if (!original.frozen || !particle.frozen || hasActiveSegment)
+        throw std::runtime_error("Moving-window upstream admission requires an unreleased held particle on rank zero");
+      if (particle.position[2] < r.origin[2]) {
+        r.coupling->depositFrozenSourceSupport(start, particle.position, particle.charge, false);
+        retained.push_back(particle);
+        continue;
+      }
+      const Double fraction = (r.origin[2] - start[2]) / (particle.position[2] - start[2]);
+      if (!(fraction >= 0.0 && fraction <= 1.0) || !std::isfinite(fraction))
+        throw std::runtime_error("Invalid moving-window admission fraction");
+      for (unsigned axis = 0; axis < 3; ++axis)
+        start[axis] += fraction * (particle.position[axis] - start[axis]);
+      start[2] = r.origin[2];
+      segmentStartFraction = fraction;
+      r.coupling->depositFrozenSourceSupport(original.position, start, particle.charge, false);
+    }
+    const bool hasActivationKink = original.frozen && hasActiveSegment &&
+                                   activeStartTime > t && activeStartTime < t + dt;
+    const Double activationKinkFraction = (activeStartTime - t) / dt;
+    if (hasActivationKink) {
+      processActiveSegment(particle, start, segmentStartFraction, &activeStart.position,
+                           activationKinkFraction, nullptr);
+    } else {
+      Hits hits;
+      hits.entersCpml = firstMovingWindowEntry(r, cpml, start, particle.position,
+                                               segmentStartFraction, hits.cpmlHit);
+      hits.exitsOuter = boundary.firstExit(start, particle.position, hits.outerHit);
+      processActiveSegment(particle, start, segmentStartFraction, nullptr, 0.0, &hits);
     }
   }
   r.particles.swap(retained);
@@ -417,6 +515,35 @@ aprl_status ref_run_set_particles(ref_run* r, size_t n, const double* x, const d
   return APRL_OK;
 }
 
+aprl_status ref_run_set_held(ref_run* r, size_t n, const uint8_t* frozen, const double* beta) {
+  return guarded([&] {
+    if (n != r->particles.size()) throw std::invalid_argument("Held state must cover the particle list");
+    for (size_t i = 0; i < n; ++i) {
+      r->particles[i].frozen = frozen[i] != 0;
+      r->particles[i].frozenBetaZ = beta[i];
+    }
+    PendingWindowGeometry geometry;
+    geometry.referenceOriginZ = r->cfg.reference_origin[2];
+    geometry.initialOffset = r->cfg.initial_offset;
+    geometry.dz = r->cfg.dz;
+    geometry.heldDistancePerBeta = SI::c * r->cfg.dt;
+    geometry.maximumStep = r->cfg.maximum_step;
+    r->pending.reset(new PendingParticleQueue(geometry, r->step));
+    r->pending->extract(r->particles);
+  });
+}
+
+aprl_status ref_run_get_held(ref_run* r, size_t capacity, uint8_t* frozen, double* beta,
+                             size_t* count) {
+  if (capacity < r->particles.size()) return failWith(APRL_ERR_INVALID_ARGUMENT, "Particle buffer too small");
+  for (size_t i = 0; i < r->particles.size(); ++i) {
+    if (frozen) frozen[i] = r->particles[i].frozen ? 1 : 0;
+    if (beta) beta[i] = r->particles[i].frozenBetaZ;
+  }
+  *count = r->particles.size();
+  return APRL_OK;
+}
+
 aprl_status ref_run_particle_count(ref_run* r, size_t* count) {
   *count = r->particles.size();
   return APRL_OK;
@@ -479,6 +606,8 @@ aprl_status ref_run_set_carriers(ref_run* r, size_t n, const double* pos, const 
 
 aprl_status ref_run_advance_magnetic(ref_run* r) {
   return guarded([&] {
+    if (r->stage != 0) throw std::logic_error("Moving-window beginStep phase/origin mismatch");
+    if (r->pending) r->admitted += r->pending->admit(r->step, r->particles);
     r->fields->clearCurrent();
     r->window->beginStep(*r->fields, r->step, r->offset);
     const EBElectricHaloView halo = r->window->physicalElectricHalos(*r->fields, r->step);
@@ -626,6 +755,10 @@ aprl_status ref_run_get_stats(ref_run* r, aprl_step_stats* st) {
   st->window_offset = r->offset;
   st->origin_z = r->origin[2];
   st->time_box = r->time;
+  st->pending = r->pending ? r->pending->size() : 0;
+  st->admitted = r->admitted;
+  st->activations = r->activations;
+  for (const auto& p : r->particles) st->held += p.frozen ? 1 : 0;
   return APRL_OK;
 }
 

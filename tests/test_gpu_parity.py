@@ -107,3 +107,38 @@ def test_detector_plane_matches_oracle():
     dg, do = g.sample_field_plane(lab_z), o.sample_field_plane(lab_z)
     assert dg is not None and do is not None
     assert checkers.max_relative(dg, do) <= RTOL
+
+
+@pytest.mark.parametrize("shape", ["linear-binomial3", "quintic-compensated"])
+def test_held_injection_matches_oracle(shape):
+    """Held lab-plane injection: queue extraction, admission, frozen source
+    support, activation kinks and upstream admission clips, 12 steps."""
+    w = workloads.streaming_case(shape=shape, steps=12)
+    g, o = gpu_run(w), checkers.run(checkers.oracle(), w)
+    assert g.stats()["pending"] == o.stats()["pending"] > 0
+    for _ in range(w.steps):
+        g.step(1)
+        o.step(1)
+        stg, sto = g.stats(), o.stats()
+        for k in ("pending", "admitted", "activations", "held", "particles"):
+            assert stg[k] == sto[k], k
+    compare_state(g, o)
+    fg, bg = g.get_held()
+    fo, bo = o.get_held()
+    np.testing.assert_array_equal(fg, fo)
+    np.testing.assert_array_equal(bg, bo)
+    assert o.stats()["admitted"] > 0 and o.stats()["activations"] > 0
+
+
+def test_held_trial_residual_counts_pushed_slots():
+    """The residual's call count is the number of pushed slots: held
+    particles that stay frozen are not pushed."""
+    w = workloads.streaming_case(steps=3)
+    g, o = gpu_run(w), checkers.run(checkers.oracle(), w)
+    for r in (g, o):
+        r.advance_magnetic()
+        r.preview_electric()
+    rg, ro = g.coupling_trial(), o.coupling_trial()
+    assert rg[3] == ro[3] < g.particle_count()
+    for x, y in zip(rg[:3], ro[:3]):
+        assert abs(x - y) <= 1e-12 * max(abs(y), 1e-300)

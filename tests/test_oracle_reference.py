@@ -146,3 +146,22 @@ def test_momentum_identical():
         assert io == ir
         assert list(uo) == list(ur)
         assert lib_o.oracle_gamma(d(u)) == lib_r.ref_gamma(d(u))
+
+
+@pytest.mark.parametrize("shape", ["linear-binomial3", "quintic-compensated"])
+def test_held_injection_bit_identical(shape):
+    """Pending extraction, admission, frozen source support, activation kinks
+    and upstream admission clips against the reference's
+    PendingParticleQueue and prepareParticle path."""
+    w = workloads.streaming_case(shape=shape, steps=12)
+    o = checkers.run(checkers.oracle(), w)
+    r = checkers.run(checkers.reference(), w)
+    assert o.stats()["pending"] == r.stats()["pending"] > 0
+    for _ in range(w.steps):
+        o.step(1)
+        r.step(1)
+        assert_states_identical(checkers.state(o), checkers.state(r))
+        for x, y in zip(o.get_held(), r.get_held()):
+            np.testing.assert_array_equal(x, y)
+    s = o.stats()
+    assert s["admitted"] > 0 and s["activations"] > 0
