@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -1807,6 +1808,90 @@ aprl_status aprl_run_profile_read(aprl_run* r, double* ms, uint64_t* launches, u
 aprl_status aprl_run_launch_count(const aprl_run* r, uint64_t* launches) {
   if (!r || !launches) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
   *launches = r->launches;
+  return APRL_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Detector plane without device allocation.
+//
+// The plane is staged in this fixed array instead of the run's lazily
+// allocated detector buffer.  In host code `g_plane_scratch` names a host-side
+// stand-in, not device memory, so the kernel receives the address that
+// cudaGetSymbolAddress reports for the current device.
+static __device__ __align__(256) double g_plane_scratch[APRL_NOALLOC_PLANE_MAX_VALUES];
+
+namespace {
+
+constexpr int kPlaneScratchDevices = 64;
+std::atomic<double*> g_plane_scratch_address[kPlaneScratchDevices];
+
+// Device address of g_plane_scratch on the current device; looked up once
+// per device, with that device current.
+aprl_status plane_scratch(double** out) {
+  int device = 0;
+  CUDA_TRY(cudaGetDevice(&device));
+  if (device < 0 || device >= kPlaneScratchDevices)
+    return fail(APRL_ERR_UNSUPPORTED, "Device ordinal %d is beyond the %d devices of the fixed detector scratch",
+                device, kPlaneScratchDevices);
+  double* ptr = g_plane_scratch_address[device].load(std::memory_order_acquire);
+  if (!ptr) {
+    CUDA_TRY(cudaGetSymbolAddress((void**)&ptr, g_plane_scratch));
+    g_plane_scratch_address[device].store(ptr, std::memory_order_release);
+  }
+  *out = ptr;
+  return APRL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* r, double plane_lab_z, double* out,
+                                                size_t count, int* inside) {
+  if (!r || !out || !inside) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  const aprl_run_config& c = r->cfg;
+  if (count != 6 * c.nx * c.ny) return fail(APRL_ERR_INVALID_ARGUMENT, "Detector buffer size mismatch");
+  if (count > APRL_NOALLOC_PLANE_MAX_VALUES)
+    return fail(APRL_ERR_OUT_OF_RANGE,
+                "Detector plane of %zu values exceeds the fixed %u-value scratch of "
+                "aprl_run_sample_field_plane_noalloc; use aprl_run_sample_field_plane",
+                count, APRL_NOALLOC_PLANE_MAX_VALUES);
+  double* scratch = nullptr;
+  TRY(plane_scratch(&scratch));
+  // boxZFromLabZAndBoxT (src/boostframe.cpp:231-235) and the window test,
+  // as in aprl_run_sample_field_plane.
+  const double box_z = c.box_z_origin + (plane_lab_z - c.lab_z_origin) / c.boost_gamma -
+                       c.boost_beta * kC * r->time;
+  const double coordinate = (box_z - r->origin[2]) / c.dz;
+  const double tolerance = 64.0 * DBL_EPSILON * std::max(1.0, std::abs(coordinate));
+  if (!(box_z < r->origin[2]) && coordinate > static_cast<double>(c.nz) + tolerance) {
+    *inside = 0;
+    return APRL_OK;
+  }
+  *inside = 1;
+  auto axis = [](double lattice, size_t size, int* lower, double* fraction) {
+    if (lattice <= 0.0) { *lower = 0; *fraction = 0.0; }
+    else if (lattice >= static_cast<double>(size - 1)) { *lower = (int)size - 2; *fraction = 1.0; }
+    else { *lower = (int)std::floor(lattice); *fraction = lattice - static_cast<double>(*lower); }
+  };
+  DetectorArgs da{};
+  da.g = make_grid(r);
+  da.frame = make_frame(c);
+  da.origin_xy[0] = c.reference_origin[0];
+  da.origin_xy[1] = c.reference_origin[1];
+  axis(coordinate, c.nz + 1, &da.vertex_lower, &da.vertex_fraction);
+  axis(coordinate - 0.5, c.nz, &da.half_lower, &da.half_fraction);
+  da.out = scratch;
+  // A direct launch: no timing events are created on this path.
+  const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
+  detector_plane_kernel<<<grid, block, 0, r->stream>>>(da);
+  CUDA_TRY(cudaGetLastError());
+  ++r->kernel_launches[kDetectorPlane];
+  ++r->launches;
+  CUDA_TRY(cudaMemcpyAsync(out, scratch, count * 8, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;
 }
 

@@ -64,6 +64,8 @@ _PRODUCT_ONLY = {
     "kernel_name": (C.c_char_p, [C.c_uint]),
     "run_launch_count": (C.c_int, [_H, _U64]),
     "run_reset_iteration_stats": (C.c_int, [_H]),
+    "run_sample_field_plane_noalloc": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
+                                                 C.POINTER(C.c_int)]),
 }
 
 

@@ -306,6 +306,35 @@ aprl_status aprl_run_sample_field_plane(aprl_run* run, double plane_lab_z,
                                         double* out, size_t count,
                                         int* inside);
 
+/* Largest plane (count = 6*nx*ny values) that
+ * aprl_run_sample_field_plane_noalloc accepts: 6*256*256 doubles, i.e. a
+ * fixed 3 MiB device array that every GPU which loads this library keeps
+ * until the process exits. */
+#define APRL_NOALLOC_PLANE_MAX_VALUES 393216u
+
+/* The detector plane of aprl_run_sample_field_plane (same arguments, same
+ * values, same *inside rule), for callers that cannot allocate device memory
+ * in the middle of a run.  There is no counterpart of this call in the
+ * reference.  Such callers are, for example, a host framework whose caching
+ * allocator has already reserved the free device memory, so that a direct
+ * cudaMalloc may fail even though the framework holds unused blocks, or a
+ * stepping loop that must not take the device-wide synchronisation which
+ * cudaFree brings.  aprl_run_sample_field_plane stages the plane in a device
+ * buffer that the run allocates on first use; this call stages it in a fixed
+ * array built into the library and calls no cudaMalloc or cudaFree.
+ *   - count above APRL_NOALLOC_PLANE_MAX_VALUES is rejected with
+ *     APRL_ERR_OUT_OF_RANGE; use aprl_run_sample_field_plane there.
+ *   - The first call on each device looks up the array's device address, with
+ *     that device current.  Make that first call before any stream capture.
+ *   - Every call on a device uses the same array.  The call waits for its copy
+ *     to the host before it returns, but calls that overlap on the GPU (from
+ *     several host threads or runs at once) race for the array.
+ *   - The kernel writes every value of the plane, so nothing left over from
+ *     an earlier call needs clearing. */
+aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* run, double plane_lab_z,
+                                                double* out, size_t count,
+                                                int* inside);
+
 /* Synchronise the run's stream. */
 aprl_status aprl_run_synchronize(aprl_run* run);
 
