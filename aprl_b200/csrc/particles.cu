@@ -102,75 +102,97 @@ __device__ __forceinline__ void binomial_xz_segment(const DGrid& g, const double
 // longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
 // smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
 // when the chord exceeds the 64-cut crossing budget.
+// Four-point Gauss quadrature of the quintic-compensated shape over one cut
+// piece of the chord (the quintic branch of longitudinal_shape::weights).
+template <class V>
+__device__ __forceinline__ void quintic_segment(const DGrid& g, const double x[3],
+                                                const double v[3], double lower,
+                                                double upper, double width, V& visit) {
+  const double q[4] = {-.8611363115940525752, -.3399810435848562648,
+                       .3399810435848562648, .8611363115940525752};
+  const double qw[4] = {.3478548451374538574, .6521451548625461426,
+                        .6521451548625461426, .3478548451374538574};
+  for (int t = 0; t < 4; ++t) {
+    const double u = .5 * (upper + lower + width * q[t]),
+                 factor = .5 * width * qw[t], xx = x[0] + u * v[0],
+                 yy = x[1] + u * v[1], zz = x[2] + u * v[2];
+    long long i = (long long)floor(xx), j = (long long)floor(yy);
+    if (i == (long long)g.nx) --i;
+    if (j == (long long)g.ny) --j;
+    const double fx = xx - i, fy = yy - j;
+    Basis nodes, edge;
+    quintic_basis(zz, false, nodes);
+    quintic_basis(zz, true, edge);
+    for (int k = 0; k < nodes.count; ++k) {
+      const double w = factor * nodes.v[k];
+      if (w == 0.) continue;
+      for (int b = 0; b < 2; ++b) visit(0, i, j + b, nodes.first + k, w * (b ? fy : 1. - fy));
+      for (int a = 0; a < 2; ++a) visit(1, i + a, j, nodes.first + k, w * (a ? fx : 1. - fx));
+    }
+    for (int k = 0; k < edge.count; ++k) {
+      const double w = factor * edge.v[k];
+      if (w == 0.) continue;
+      for (int b = 0; b < 2; ++b)
+        for (int a = 0; a < 2; ++a)
+          visit(2, i + a, j + b, edge.first + k, w * (a ? fx : 1. - fx) * (b ? fy : 1. - fy));
+    }
+  }
+}
+
 template <class V>
 __device__ int shape_weights(const DGrid& g, int shape, const double begin[3],
                              const double end[3], V& visit) {
   const double h[3] = {g.dx, g.dy, g.dz};
-  double x[3], v[3], cuts[64];
-  int count = 2;
-  cuts[0] = 0.;
-  cuts[1] = 1.;
+  // The cell-boundary cuts of the chord, ascending.  Along each axis the cuts
+  // (j - x)/v of the crossed lattice planes j are already monotone, so a
+  // three-way merge yields the sorted cut sequence of the reference (same
+  // values, ties give zero-width pieces) without a cut array.
+  double x[3], v[3], next[3];
+  long long plane[3], left[3];
+  int dir[3];
+  long long total = 0;
   for (int a = 0; a < 3; ++a) {
     x[a] = (begin[a] - g.origin[a]) / h[a];
     v[a] = (end[a] - begin[a]) / h[a];
-    if (v[a] != 0.)
-      for (long long j = (long long)floor(fmin(x[a], x[a] + v[a])) + 1;
-           j < fmax(x[a], x[a] + v[a]); ++j) {
-        if (count == 64) return -1;
-        cuts[count++] = (j - x[a]) / v[a];
-      }
-  }
-  // insertion sort (the cut count is tiny)
-  for (int s = 1; s < count; ++s) {
-    const double key = cuts[s];
-    int t = s - 1;
-    while (t >= 0 && cuts[t] > key) {
-      cuts[t + 1] = cuts[t];
-      --t;
+    left[a] = 0;
+    if (v[a] != 0.) {
+      const double lo = fmin(x[a], x[a] + v[a]), hi = fmax(x[a], x[a] + v[a]);
+      const long long first = (long long)floor(lo) + 1, last = (long long)ceil(hi) - 1;
+      left[a] = last >= first ? last - first + 1 : 0;
+      dir[a] = v[a] > 0. ? 1 : -1;
+      plane[a] = v[a] > 0. ? first : last;
+      if (left[a]) next[a] = (plane[a] - x[a]) / v[a];
     }
-    cuts[t + 1] = key;
+    total += left[a];
   }
+  if (total > 62) return -1;  // more than 64 cuts with the chord ends
   int segments = 0;
-  for (int s = 1; s < count; ++s) {
-    const double width = cuts[s] - cuts[s - 1];
-    if (width <= 0.) continue;
-    ++segments;
-    if (shape == 0) {
-      if constexpr (V::kF3Segment)
-        visit.f3_segment(g, x, v, cuts[s - 1], cuts[s]);
-      else
-        binomial_xz_segment(g, x, v, cuts[s - 1], cuts[s], visit);
-      continue;
+  double lower = 0.;
+  for (;;) {
+    int axis = -1;
+    for (int a = 0; a < 3; ++a)
+      if (left[a] && (axis < 0 || next[a] < next[axis])) axis = a;
+    double upper = 1.;
+    if (axis >= 0) {
+      upper = next[axis];
+      plane[axis] += dir[axis];
+      if (--left[axis]) next[axis] = (plane[axis] - x[axis]) / v[axis];
     }
-    const double q[4] = {-.8611363115940525752, -.3399810435848562648,
-                         .3399810435848562648, .8611363115940525752};
-    const double qw[4] = {.3478548451374538574, .6521451548625461426,
-                          .6521451548625461426, .3478548451374538574};
-    for (int t = 0; t < 4; ++t) {
-      const double u = .5 * (cuts[s] + cuts[s - 1] + width * q[t]),
-                   factor = .5 * width * qw[t], xx = x[0] + u * v[0],
-                   yy = x[1] + u * v[1], zz = x[2] + u * v[2];
-      long long i = (long long)floor(xx), j = (long long)floor(yy);
-      if (i == (long long)g.nx) --i;
-      if (j == (long long)g.ny) --j;
-      const double fx = xx - i, fy = yy - j;
-      Basis nodes, edge;
-      quintic_basis(zz, false, nodes);
-      quintic_basis(zz, true, edge);
-      for (int k = 0; k < nodes.count; ++k) {
-        const double w = factor * nodes.v[k];
-        if (w == 0.) continue;
-        for (int b = 0; b < 2; ++b) visit(0, i, j + b, nodes.first + k, w * (b ? fy : 1. - fy));
-        for (int a = 0; a < 2; ++a) visit(1, i + a, j, nodes.first + k, w * (a ? fx : 1. - fx));
-      }
-      for (int k = 0; k < edge.count; ++k) {
-        const double w = factor * edge.v[k];
-        if (w == 0.) continue;
-        for (int b = 0; b < 2; ++b)
-          for (int a = 0; a < 2; ++a)
-            visit(2, i + a, j + b, edge.first + k, w * (a ? fx : 1. - fx) * (b ? fy : 1. - fy));
+    const double width = upper - lower;
+    const double piece_lower = lower;
+    lower = upper;
+    if (width > 0.) {
+      ++segments;
+      if (shape == 0) {
+        if constexpr (V::kF3Segment)
+          visit.f3_segment(g, x, v, piece_lower, upper);
+        else
+          binomial_xz_segment(g, x, v, piece_lower, upper, visit);
+      } else {
+        quintic_segment(g, x, v, piece_lower, upper, width, visit);
       }
     }
+    if (axis < 0) break;
   }
   return segments;
 }
@@ -824,28 +846,17 @@ __global__ void carrier_kernel(CarrierArgs a) {
 }
 
 // ConservativeSourceCoupling::push of one slot (src/source_coupling.cpp:90-104):
-// the first trial gathers along the ballistic guess chord from the slot's
-// start, later trials take the previous residual's re-gathered fields; then
-// `substeps` Lapenta-Markidis substeps with the prescribed magnets.
+// `substeps` Lapenta-Markidis substeps with the prescribed magnets, using the
+// slot's gathered fields (the ballistic-guess gather of the first trial, or
+// the previous residual's re-gather).
 __device__ unsigned coupling_push(const PushArgs& a, long long n, double pos[3], double u[3],
                                   double q, double m, double time, double dt, double used_e[3],
                                   double used_b[3], double& abs_work) {
-  const DGrid& g = a.g;
-  unsigned err = kErrNone;
-  if (a.first_trial) {
-    const double gamma = gamma_u(u[0], u[1], u[2]);
-    const double s = dt * kC / gamma;
-    const double guess[3] = {pos[0] + s * u[0], pos[1] + s * u[1], pos[2] + s * u[2]};
-    err = gather_electric(g, a.shape, pos, guess, false, used_e);
-    if (!err) err = gather_magnetic(g, a.shape, pos, guess, used_b);
-  } else {
-    for (int d = 0; d < 3; ++d) {
-      used_e[d] = a.next_e[3 * n + d];
-      used_b[d] = a.next_b[3 * n + d];
-    }
+  for (int d = 0; d < 3; ++d) {
+    used_e[d] = a.next_e[3 * n + d];
+    used_b[d] = a.next_b[3 * n + d];
   }
   abs_work = 0.0;
-  if (err) return err;
   const double h = dt / a.substeps;
   for (int s = 0; s < a.substeps; ++s) {
     const double before_pos[3] = {pos[0], pos[1], pos[2]};
@@ -860,7 +871,7 @@ __device__ unsigned coupling_push(const PushArgs& a, long long n, double pos[3],
       e[d] = used_e[d] + ee[d];
       b[d] = used_b[d] + bb[d];
     }
-    err = momentum(u, e, b, q, m, h, g0);
+    const unsigned err = momentum(u, e, b, q, m, h, g0);
     if (err) return err;
     const double g1 = gamma_u(u[0], u[1], u[2]);
     const double xs = h * kC / (g0 + g1);
@@ -890,171 +901,214 @@ __device__ unsigned deposit_current(const DGrid& g, int shape, const double b[3]
   return v.error;
 }
 
+// Where the coupled push of one particle starts this step: prepareParticle
+// with hold_transverse_until_activation (src/simulation.cpp:4919-5035).  An
+// active particle is pushed from the step start over dt; a held particle
+// advances along z at c*frozenBetaZ and, when its chord reaches the fixed lab
+// activation plane, is released there and pushed over the rest of the step.
+struct SlotPlan {
+  double start[3];     // push start: the step start or the activation kink
+  double time, dt;     // push time and duration
+  double held_z;       // z after the held advance (held for the whole step)
+  unsigned char seen;  // 0 no push, 1 push from the step start, 2 from the kink
+  bool released;       // held at the step start, active at its end
+  unsigned err;
+};
+
+__device__ __forceinline__ SlotPlan plan_slot(const DGrid& g, const DFrame& f, double plane,
+                                              double t, const double start[3], bool frozen,
+                                              double beta) {
+  SlotPlan s;
+  for (int d = 0; d < 3; ++d) s.start[d] = start[d];
+  s.time = t;
+  s.dt = g.dt;
+  s.held_z = start[2];
+  s.seen = 0;
+  s.released = false;
+  s.err = kErrNone;
+  if (!frozen) {
+    if (start[2] < g.origin[2]) s.err = kErrUpstream;
+    else s.seen = 1;
+    return s;
+  }
+  const double dt = g.dt;
+  const double start_lab = lab_z_from_box_zt(f, start[2], t);
+  s.held_z = start[2] + kC * dt * beta;
+  const double end_lab = lab_z_from_box_zt(f, s.held_z, t + dt);
+  if (!(end_lab >= plane)) return s;
+  if (start[2] < g.origin[2]) {
+    s.err = kErrEarlyRelease;
+    return s;
+  }
+  const double crossing =
+      start_lab >= plane ? 0.0 : fmax(0.0, fmin(1.0, (plane - start_lab) / (end_lab - start_lab)));
+  s.start[2] = start[2] + kC * crossing * dt * beta;
+  s.released = true;
+  s.time = t + crossing * dt;
+  s.dt = (1.0 - crossing) * dt;
+  if (s.dt > 0.0) s.seen = 2;
+  return s;
+}
+
+// First trial: the fields along each slot's ballistic guess chord
+// (Impl::Slot::guess, src/source_coupling.cpp:92-95), gathered from E*
+// before any current of the trial is deposited; the push reads them as the
+// previous residual's fields.
+__global__ void guess_gather_kernel(PushArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.count) return;
+  const double start[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
+  const bool frozen = a.p.frozen[n] != 0;
+  const SlotPlan s = plan_slot(a.g, a.frame, a.activation_plane_lab_z, a.time, start, frozen,
+                               frozen ? a.p.beta[n] : 0.0);
+  if (s.err || !s.seen) return;  // the push reports the error
+  const double u[3] = {a.p.ux[n], a.p.uy[n], a.p.uz[n]};
+  const double gamma = gamma_u(u[0], u[1], u[2]);
+  const double sc = s.dt * kC / gamma;
+  const double guess[3] = {s.start[0] + sc * u[0], s.start[1] + sc * u[1],
+                           s.start[2] + sc * u[2]};
+  double ne[3], nb[3];
+  unsigned err = gather_electric(a.g, a.shape, s.start, guess, false, ne);
+  if (!err) err = gather_magnetic(a.g, a.shape, s.start, guess, nb);
+  if (err) raise_error(a.status, err, (unsigned long long)n);
+  double* next_e = const_cast<double*>(a.next_e);
+  double* next_b = const_cast<double*>(a.next_b);
+  for (int d = 0; d < 3; ++d) {
+    next_e[3 * n + d] = ne[d];
+    next_b[3 * n + d] = nb[d];
+  }
+}
+
 // One fixed-point trial of one particle of the list: prepareParticle
-// (src/simulation.cpp:4919-5035; held advance at c*frozenBetaZ, activation-
-// plane crossing with the push of the remaining fraction of the step, or
-// ConservativeSourceCoupling::push from the step start), then the deposit
-// and boundary pass (src/simulation.cpp:5083-5368): upstream admission
-// clip, the frozen-to-active kink (4684-4756) and processActiveSegment
-// (4760-4917) with Simulation::firstMovingWindowEntry
+// (src/simulation.cpp:4919-5035), then the deposit and boundary pass
+// (src/simulation.cpp:5083-5368): upstream admission clip, the frozen part
+// up to an activation kink (4684-4756) and processActiveSegment (4760-4917)
+// with Simulation::firstMovingWindowEntry
 // (src/simulation_moving_window.cpp:380-395).
-__global__ void push_deposit_kernel(PushArgs a) {
+__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   const DGrid& g = a.g;
   const double t = a.time, dt = g.dt;
-  double pos[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
+  double start[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
   double u[3] = {a.p.ux[n], a.p.uy[n], a.p.uz[n]};
   const double q = a.p.q[n], m = a.p.m[n];
   const bool frozen0 = a.p.frozen[n] != 0;
-  bool frozen1 = frozen0;
-  double start[3] = {pos[0], pos[1], pos[2]};
-  unsigned err = kErrNone;
-  if (start[2] < g.origin[2] && !frozen0) err = kErrUpstream;
-  bool has_active = !frozen0;
-  double active_time = t;
-  double kink[3] = {start[0], start[1], start[2]};
-  unsigned char seen = 0;
-  double slot_dt = dt;
+  const SlotPlan s = plan_slot(g, a.frame, a.activation_plane_lab_z, t, start, frozen0,
+                               frozen0 ? a.p.beta[n] : 0.0);
+  unsigned err = s.err;
+  const bool frozen1 = frozen0 && !s.released;
+  double pos[3] = {s.start[0], s.start[1], frozen1 ? s.held_z : s.start[2]};
   double used_e[3] = {0., 0., 0.}, used_b[3] = {0., 0., 0.};
   double abs_work = 0.0;
-  if (!err) {
-    if (frozen0) {
-      const double beta = a.p.beta[n];
-      const double start_lab = lab_z_from_box_zt(a.frame, start[2], t);
-      pos[2] += kC * dt * beta;
-      const double end_lab = lab_z_from_box_zt(a.frame, pos[2], t + dt);
-      const double plane = a.activation_plane_lab_z;
-      if (end_lab >= plane) {
-        if (start[2] < g.origin[2]) {
-          err = kErrEarlyRelease;
-        } else {
-          const double crossing =
-              start_lab >= plane
-                  ? 0.0
-                  : fmax(0.0, fmin(1.0, (plane - start_lab) / (end_lab - start_lab)));
-          for (int d = 0; d < 3; ++d) pos[d] = start[d];
-          pos[2] += kC * crossing * dt * beta;
-          frozen1 = false;
-          has_active = true;
-          for (int d = 0; d < 3; ++d) kink[d] = pos[d];
-          active_time = t + crossing * dt;
-          const double remaining = (1.0 - crossing) * dt;
-          if (remaining > 0.0) {
-            err = coupling_push(a, n, pos, u, q, m, active_time, remaining, used_e, used_b,
-                                abs_work);
-            seen = 2;
-            slot_dt = remaining;
-          }
-        }
-      }
-    } else {
-      err = coupling_push(a, n, pos, u, q, m, t, dt, used_e, used_b, abs_work);
-      seen = 1;
-    }
-  }
-  if (!err && frozen0 && has_active) atomicAdd(&a.counters->activations, 1ull);
-  unsigned char action = 0;
-  bool born_kept = false;
-  CarrierState born;
+  if (!err && s.seen)
+    err = coupling_push(a, n, pos, u, q, m, s.time, s.dt, used_e, used_b, abs_work);
+  if (!err && s.released) atomicAdd(&a.counters->activations, 1ull);
+  // An optional leading piece, then the main segment: the upstream part of
+  // an admitted held particle (deposited without validation), or the frozen
+  // part up to an activation kink (which may not cross a boundary).
   double seg_frac = 0.0;
-  bool upstream_only = false;
+  bool has_pre = false, pre_validate = false, has_main = true;
+  double pre_end[3] = {pos[0], pos[1], pos[2]};
+  double pre_start[3] = {start[0], start[1], start[2]};
   if (!err && start[2] < g.origin[2]) {
-    // Upstream admission of an unreleased held particle: the part before
-    // the inlet deposits without validation, the rest is an ordinary
-    // segment starting at the admission fraction.
-    if (!frozen0 || !frozen1 || has_active) {
+    if (!frozen0 || !frozen1) {
       err = kErrAdmission;
     } else if (pos[2] < g.origin[2]) {
-      err = deposit_current(g, a.shape, start, pos, q);
-      upstream_only = true;
+      has_pre = true;
+      has_main = false;
     } else {
       const double fraction = (g.origin[2] - start[2]) / (pos[2] - start[2]);
       if (!(fraction >= 0.0 && fraction <= 1.0) || !isfinite(fraction)) {
         err = kErrAdmission;
       } else {
-        double clipped[3];
-        for (int d = 0; d < 3; ++d) clipped[d] = start[d] + fraction * (pos[d] - start[d]);
-        clipped[2] = g.origin[2];
+        for (int d = 0; d < 3; ++d) pre_end[d] = start[d] + fraction * (pos[d] - start[d]);
+        pre_end[2] = g.origin[2];
+        has_pre = true;
         seg_frac = fraction;
-        err = deposit_current(g, a.shape, start, clipped, q);
-        for (int d = 0; d < 3; ++d) start[d] = clipped[d];
+        for (int d = 0; d < 3; ++d) start[d] = pre_end[d];
       }
     }
-  }
-  if (!err && !upstream_only) {
-    if (frozen0 && has_active && active_time > t && active_time < t + dt) {
-      // The frozen part of the step up to the activation kink may not
-      // cross a particle boundary.
-      Hit hc, ho;
-      bool enters = false, exits = false;
-      err = cpml_first_entry(a.region, start, kink, hc, enters);
-      if (!err) err = outer_first_exit(a.region, start, kink, ho, exits);
-      if (!err && (enters || exits)) err = kErrHeldBoundary;
-      if (!err) err = deposit_segment(g, a.shape, start, kink, q);
-      for (int d = 0; d < 3; ++d) start[d] = kink[d];
-      seg_frac = (active_time - t) / dt;
-    }
-  }
-  if (!err && !upstream_only) {
-    // firstMovingWindowEntry = CPML first entry + fixed-lab exit plane
-    Hit cpml_hit, outer_hit;
+  } else if (!err && s.released && s.time > t && s.time < t + dt) {
+    Hit hc, ho;
     bool enters = false, exits = false;
-    err = cpml_first_entry(a.region, start, pos, cpml_hit, enters);
-    if (!err) {
-      const double za = lab_z_from_box_zt(a.frame, start[2], t + seg_frac * dt) - a.exit_lab_z;
-      const double zb = lab_z_from_box_zt(a.frame, pos[2], t + dt) - a.exit_lab_z;
-      if (za >= 0.) err = kErrBeyondExit;
-      else if (zb >= 0. && zb > za) {
-        const double fraction = -za / (zb - za);
-        if (!enters || fraction < cpml_hit.fraction) {
-          for (int d = 0; d < 3; ++d) cpml_hit.position[d] = start[d] + fraction * (pos[d] - start[d]);
-          cpml_hit.fraction = fraction;
-          cpml_hit.face = 5;
-          enters = true;
+    err = cpml_first_entry(a.region, start, s.start, hc, enters);
+    if (!err) err = outer_first_exit(a.region, start, s.start, ho, exits);
+    if (!err && (enters || exits)) err = kErrHeldBoundary;
+    for (int d = 0; d < 3; ++d) pre_end[d] = s.start[d];
+    has_pre = true;
+    pre_validate = true;
+    for (int d = 0; d < 3; ++d) start[d] = s.start[d];
+    seg_frac = (s.time - t) / dt;
+  }
+  unsigned char action = 0;
+  Hit selected;
+  for (int piece = has_pre ? 0 : 1; piece < (has_main ? 2 : 1) && !err; ++piece) {
+    double b[3], e[3];
+    bool validate = true;
+    if (piece == 0) {
+      for (int d = 0; d < 3; ++d) {
+        b[d] = pre_start[d];
+        e[d] = pre_end[d];
+      }
+      validate = pre_validate;
+    } else {
+      // firstMovingWindowEntry = CPML first entry + fixed-lab exit plane
+      Hit cpml_hit, outer_hit;
+      bool enters = false, exits = false;
+      err = cpml_first_entry(a.region, start, pos, cpml_hit, enters);
+      if (!err) {
+        const double za = lab_z_from_box_zt(a.frame, start[2], t + seg_frac * dt) - a.exit_lab_z;
+        const double zb = lab_z_from_box_zt(a.frame, pos[2], t + dt) - a.exit_lab_z;
+        if (za >= 0.) err = kErrBeyondExit;
+        else if (zb >= 0. && zb > za) {
+          const double fraction = -za / (zb - za);
+          if (!enters || fraction < cpml_hit.fraction) {
+            for (int d = 0; d < 3; ++d) cpml_hit.position[d] = start[d] + fraction * (pos[d] - start[d]);
+            cpml_hit.fraction = fraction;
+            cpml_hit.face = 5;
+            enters = true;
+          }
         }
       }
-    }
-    if (!err) err = outer_first_exit(a.region, start, pos, outer_hit, exits);
-    if (!err) {
-      const double crossing = 64.0 * kEpsilon;
-      double seg_end[3] = {pos[0], pos[1], pos[2]};
-      double local_end = 1.0;
-      Hit selected;
-      if (enters && (!exits || cpml_hit.fraction <= outer_hit.fraction + crossing)) {
+      if (!err) err = outer_first_exit(a.region, start, pos, outer_hit, exits);
+      if (err) break;
+      if (enters && (!exits || cpml_hit.fraction <= outer_hit.fraction + 64.0 * kEpsilon)) {
         action = 1;
         selected = cpml_hit;
       } else if (exits) {
         action = 2;
         selected = outer_hit;
       }
-      if (action) {
-        local_end = selected.fraction;
-        for (int d = 0; d < 3; ++d) seg_end[d] = selected.position[d];
-      }
-      err = deposit_segment(g, a.shape, start, seg_end, q);
-      const double global_end = seg_frac + local_end * (1.0 - seg_frac);
-      if (!err && action == 1) {
-        if (selected.face == 5) {
-          atomicAdd(&a.counters->exits, 1ull);
-          atomicAdd(&a.counters->exit_charge, q);
-        } else {
-          atomicAdd(&a.counters->cpml[selected.face], 1ull);
-          atomicAdd(&a.counters->cpml_charge[selected.face], q);
-        }
-        for (int d = 0; d < 3; ++d) born.pos[d] = pos[d];
-        const double gamma = gamma_u(u[0], u[1], u[2]);
-        const double sv = kC / gamma;
-        for (int d = 0; d < 3; ++d) born.vel[d] = u[d] * sv;
-        born.q = q;
-        born.w = 1.0;
-        err = carrier_segment(g, a.shape, a.region, born, selected.position, global_end,
-                              a.counters, born_kept);
-      } else if (!err && action == 2) {
-        atomicAdd(&a.counters->direct[selected.face], 1ull);
-        atomicAdd(&a.counters->direct_charge[selected.face], q);
+      for (int d = 0; d < 3; ++d) {
+        b[d] = start[d];
+        e[d] = action ? selected.position[d] : pos[d];
       }
     }
+    err = validate ? deposit_segment(g, a.shape, b, e, q) : deposit_current(g, a.shape, b, e, q);
+  }
+  bool born_kept = false;
+  CarrierState born;
+  if (!err && has_main && action == 1) {
+    if (selected.face == 5) {
+      atomicAdd(&a.counters->exits, 1ull);
+      atomicAdd(&a.counters->exit_charge, q);
+    } else {
+      atomicAdd(&a.counters->cpml[selected.face], 1ull);
+      atomicAdd(&a.counters->cpml_charge[selected.face], q);
+    }
+    for (int d = 0; d < 3; ++d) born.pos[d] = pos[d];
+    const double gamma = gamma_u(u[0], u[1], u[2]);
+    const double sv = kC / gamma;
+    for (int d = 0; d < 3; ++d) born.vel[d] = u[d] * sv;
+    born.q = q;
+    born.w = 1.0;
+    const double global_end = seg_frac + selected.fraction * (1.0 - seg_frac);
+    err = carrier_segment(g, a.shape, a.region, born, selected.position, global_end, a.counters,
+                          born_kept);
+  } else if (!err && has_main && action == 2) {
+    atomicAdd(&a.counters->direct[selected.face], 1ull);
+    atomicAdd(&a.counters->direct_charge[selected.face], q);
   }
   if (err) raise_error(a.status, err, (unsigned long long)n);
   // Held particles retained by this trial, one atomic per converged group.
@@ -1066,12 +1120,12 @@ __global__ void push_deposit_kernel(PushArgs a) {
   a.x1[n] = pos[0]; a.y1[n] = pos[1]; a.z1[n] = pos[2];
   a.ux1[n] = u[0]; a.uy1[n] = u[1]; a.uz1[n] = u[2];
   a.frozen1[n] = frozen1 ? 1 : 0;
-  a.slot.seen[n] = seen;
-  if (seen == 2) {
-    a.slot.x0[n] = kink[0];
-    a.slot.y0[n] = kink[1];
-    a.slot.z0[n] = kink[2];
-    a.slot.dt[n] = slot_dt;
+  a.slot.seen[n] = s.seen;
+  if (s.seen == 2) {
+    a.slot.x0[n] = s.start[0];
+    a.slot.y0[n] = s.start[1];
+    a.slot.z0[n] = s.start[2];
+    a.slot.dt[n] = s.dt;
   }
   for (int d = 0; d < 3; ++d) {
     a.used_e[3 * n + d] = used_e[d];
@@ -1102,7 +1156,7 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-__global__ void residual_kernel(ResidualArgs a) {
+__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double force = 0.0, defect = 0.0, scale = 0.0;
   const unsigned char seen = n < a.count ? a.slot.seen[n] : 0;

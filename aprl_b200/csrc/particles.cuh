@@ -84,7 +84,6 @@ struct PushArgs {
   int n_magnets;
   int shape;
   int substeps;
-  int first_trial;       // 1: gather along the ballistic guess chord
   double time;           // box time at the start of the step
   double exit_lab_z;
   double activation_plane_lab_z;
@@ -134,9 +133,29 @@ struct ResidualArgs {
   DeviceStatus* status;
 };
 
-__global__ void push_deposit_kernel(PushArgs a);
+// Occupancy knobs of the two hot particle kernels (blocks of 128 threads
+// that must fit one SM; 0 leaves the register count to the compiler).
+#ifndef APRL_PUSH_MIN_BLOCKS
+#define APRL_PUSH_MIN_BLOCKS 4
+#endif
+#ifndef APRL_RESIDUAL_MIN_BLOCKS
+#define APRL_RESIDUAL_MIN_BLOCKS 4
+#endif
+#if APRL_PUSH_MIN_BLOCKS > 0
+#define APRL_PUSH_BOUNDS __launch_bounds__(128, APRL_PUSH_MIN_BLOCKS)
+#else
+#define APRL_PUSH_BOUNDS
+#endif
+#if APRL_RESIDUAL_MIN_BLOCKS > 0
+#define APRL_RESIDUAL_BOUNDS __launch_bounds__(128, APRL_RESIDUAL_MIN_BLOCKS)
+#else
+#define APRL_RESIDUAL_BOUNDS
+#endif
+
+__global__ void guess_gather_kernel(PushArgs a);
+__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs a);
 __global__ void carrier_kernel(CarrierArgs a);
-__global__ void residual_kernel(ResidualArgs a);
+__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs a);
 
 // Stable compaction helpers (warp ballot + block scan + block-offset scan).
 constexpr int kScanBlock = 256;

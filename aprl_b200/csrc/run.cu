@@ -54,7 +54,7 @@ enum Kernel : unsigned {
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
-  kKernelCount
+  kGuessGather, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -63,7 +63,7 @@ const char* kKernelNames[kKernelCount] = {
   "block_offset_scan", "gather_particles", "gather_carriers",
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
-  "frozen_support"};
+  "frozen_support", "guess_gather"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -900,7 +900,6 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     }
     pa.shape = c.shape;
     pa.substeps = (int)c.substeps;
-    pa.first_trial = r->trials == 0 ? 1 : 0;
     pa.time = r->time;
     pa.exit_lab_z = c.exit_lab_z;
     pa.activation_plane_lab_z = c.activation_plane_lab_z;
@@ -921,6 +920,9 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     pa.key_base = (unsigned long long)(r->step + 1) << 32;
     pa.counters = r->d_counters;
     pa.status = r->d_status;
+    if (r->trials == 0)
+      TRY(launch(r, kGuessGather, guess_gather_kernel, dim3(blocks_for(r->np, 128)), dim3(128),
+                 pa));
     TRY(launch(r, kPushDeposit, push_deposit_kernel, dim3(blocks_for(r->np, 128)), dim3(128), pa));
     ResidualArgs ra{};
     ra.g = g;

@@ -120,6 +120,8 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
         return particles * (64 + 48 + 48 + 48 + 8 + 2)
     if kernel == "residual":            # read x0,x1,q,m,usedE/B,work; write nextE/B
         return particles * (48 + 16 + 48 + 8 + 48)
+    if kernel == "guess_gather":        # read x,u,flags; write nextE/B
+        return particles * (48 + 1 + 48)
     if kernel == "carrier":             # read + write 8 words
         return carriers * 128
     return None
