@@ -28,6 +28,10 @@ SHAPE_QUINTIC_COMPENSATED = 1
 SHAPES = {"linear-binomial3": SHAPE_LINEAR_BINOMIAL3,
           "quintic-compensated": SHAPE_QUINTIC_COMPENSATED}
 
+PRECISION_FP64 = 0
+PRECISION_FP32_MIXED = 1
+PRECISIONS = {"fp64": PRECISION_FP64, "fp32-mixed": PRECISION_FP32_MIXED}
+
 MAGNET_PLANAR_UNDULATOR = 0
 MAGNET_UNIFORM_DIPOLE = 1
 MAGNET_QUADRUPOLE = 2
@@ -68,7 +72,7 @@ class RunConfig(C.Structure):
         ("shape", C.c_int32),
         ("substeps", C.c_uint32),
         ("max_trials", C.c_uint32),
-        ("reserved0", C.c_uint32),
+        ("precision", C.c_uint32),
         ("force_tolerance", C.c_double),
         ("work_tolerance", C.c_double),
         ("boost_gamma", C.c_double), ("boost_beta", C.c_double),

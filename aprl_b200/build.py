@@ -28,8 +28,11 @@ def nvcc():
 
 
 def flags():
+    # Kernel templates are instantiated in fields.cu / particles.cu and
+    # launched from run.cu: keep their host stubs externally visible.
     return ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler",
-            "-fPIC", "-I", os.path.join(REPO, "include")] + ARCH
+            "-fPIC", "-static-global-template-stub=false",
+            "-I", os.path.join(REPO, "include")] + ARCH
 
 
 def build(force=False, verbose=True):

@@ -80,59 +80,74 @@ struct DFrame {  // BoostFrameTransform
   double lab_time_origin, lab_z_origin, box_z_origin;
 };
 
-// Everything the kernels need about the grid; passed by value.
-struct DGrid {
+// Everything the kernels need about the grid; passed by value.  F is the
+// field element type: double for the FP64 drop-in, float for the FP32-mixed
+// mode (geometry, origin and time stay binary64 in both).
+template <class F>
+struct GridT {
   int nx, ny, nz;
   double dx, dy, dz, dt;
   double origin[3];      // localOriginBox_ of the current window
-  double* e_old[3];      // E^n  (ring)
-  double* e_star[3];     // E*   (ring)
-  double* b[3];          // B    (ring)
-  double* j[3];          // J    (plain)
+  F* e_old[3];           // E^n  (ring)
+  F* e_star[3];          // E*   (ring)
+  F* b[3];               // B    (ring)
+  F* j[3];               // J    (plain)
   int zb_e[3];           // ring bases of Ex Ey Ez
   int zb_b[3];           // ring bases of Bx By Bz
-  double jcoef;          // (-1*dt)/eps0, applyCurrentSource(-1) scale
+  F jcoef;               // (-1*dt)/eps0, applyCurrentSource(-1) scale
 };
+using DGrid = GridT<double>;
 
-__device__ __forceinline__ int e_nx(const DGrid& g, int c) { return g.nx + (c != 0); }
-__device__ __forceinline__ int e_ny(const DGrid& g, int c) { return g.ny + (c != 1); }
-__device__ __forceinline__ int e_nz(const DGrid& g, int c) { return g.nz + (c != 2); }
-__device__ __forceinline__ int b_nx(const DGrid& g, int c) { return g.nx + (c == 0); }
-__device__ __forceinline__ int b_ny(const DGrid& g, int c) { return g.ny + (c == 1); }
-__device__ __forceinline__ int b_nz(const DGrid& g, int c) { return g.nz + (c == 2); }
+template <class F>
+__device__ __forceinline__ int e_nx(const GridT<F>& g, int c) { return g.nx + (c != 0); }
+template <class F>
+__device__ __forceinline__ int e_ny(const GridT<F>& g, int c) { return g.ny + (c != 1); }
+template <class F>
+__device__ __forceinline__ int e_nz(const GridT<F>& g, int c) { return g.nz + (c != 2); }
+template <class F>
+__device__ __forceinline__ int b_nx(const GridT<F>& g, int c) { return g.nx + (c == 0); }
+template <class F>
+__device__ __forceinline__ int b_ny(const GridT<F>& g, int c) { return g.ny + (c == 1); }
+template <class F>
+__device__ __forceinline__ int b_nz(const GridT<F>& g, int c) { return g.nz + (c == 2); }
 
 __device__ __forceinline__ int ring(int k, int base, int n) {
   int p = k + base;
   return p >= n ? p - n : p;
 }
 
-__device__ __forceinline__ size_t e_index(const DGrid& g, int c, int i, int j, int k) {
+template <class F>
+__device__ __forceinline__ size_t e_index(const GridT<F>& g, int c, int i, int j, int k) {
   const int nzc = e_nz(g, c);
   return ((size_t)ring(k, g.zb_e[c], nzc) * e_ny(g, c) + j) * e_nx(g, c) + i;
 }
 
-__device__ __forceinline__ size_t b_index(const DGrid& g, int c, int i, int j, int k) {
+template <class F>
+__device__ __forceinline__ size_t b_index(const GridT<F>& g, int c, int i, int j, int k) {
   const int nzc = b_nz(g, c);
   return ((size_t)ring(k, g.zb_b[c], nzc) * b_ny(g, c) + j) * b_nx(g, c) + i;
 }
 
-__device__ __forceinline__ size_t j_index(const DGrid& g, int c, int i, int j, int k) {
+template <class F>
+__device__ __forceinline__ size_t j_index(const GridT<F>& g, int c, int i, int j, int k) {
   return ((size_t)k * e_ny(g, c) + j) * e_nx(g, c) + i;
 }
 
 // applyCurrentSource's interior mask (src/source_coupling.cpp:87) at one rank.
-__device__ __forceinline__ bool current_mask(const DGrid& g, int c, int i, int j, int k) {
+template <class F>
+__device__ __forceinline__ bool current_mask(const GridT<F>& g, int c, int i, int j, int k) {
   if (c == 0) return j > 0 && j < g.ny && k != 0 && k != g.nz;
   if (c == 1) return i > 0 && i < g.nx && k != 0 && k != g.nz;
   return i > 0 && i < g.nx && j > 0 && j < g.ny;
 }
 
 // Trial candidate E* - dt/eps0 J at a native node (applyCurrentSource(-1)).
-__device__ __forceinline__ double e_candidate(const DGrid& g, int c, int i, int j, int k) {
-  double v = g.e_star[c][e_index(g, c, i, j, k)];
+template <class F>
+__device__ __forceinline__ F e_candidate(const GridT<F>& g, int c, int i, int j, int k) {
+  F v = g.e_star[c][e_index(g, c, i, j, k)];
   if (current_mask(g, c, i, j, k)) {
-    const double jc = g.j[c][j_index(g, c, i, j, k)];
-    if (jc != 0.) v += g.jcoef * jc;
+    const F jc = g.j[c][j_index(g, c, i, j, k)];
+    if (jc != F(0.)) v += g.jcoef * jc;
   }
   return v;
 }

@@ -3,9 +3,11 @@
 // electric correction, PEC termination and inlet overwrite, the commit
 // E^{n+1} = E* - dt/eps0 J, and the moving-window plane insertion.
 //
-// FP64 drop-in arithmetic: every expression keeps the reference's operation
-// order and the library is compiled without FMA contraction, so these
-// kernels reproduce the reference's translation units bit for bit.
+// Every kernel is templated on the field element type F.  With F = double
+// (the FP64 drop-in) every expression keeps the reference's operation order
+// and the library is compiled without FMA contraction, so these kernels
+// reproduce the reference's translation units bit for bit; F = float is the
+// FP32-mixed mode (coefficients computed in binary64, then rounded once).
 #include "common.cuh"
 #include "fields.cuh"
 
@@ -14,10 +16,10 @@ namespace aprl_gpu {
 // electricValue (src/eb_field.cpp:350-417) under the moving window: x/y
 // PEC parity extension, z halo planes (lower = inlet reference plane,
 // upper = the last rank's zero plane).
-__device__ __forceinline__ double electric_value(const CowanArgs& a, int c, int i,
-                                                 int j, int k) {
+template <class F>
+__device__ __forceinline__ F electric_value(const CowanArgs<F>& a, int c, int i, int j, int k) {
   const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1), nzc = a.g.nz + (c != 2);
-  double sign = 1.0;
+  F sign = F(1.0);
   if (i < 0) {
     if (c == 0) i = 0; else { i = -i; sign = -sign; }
   } else if (i >= nxc) {
@@ -29,45 +31,22 @@ __device__ __forceinline__ double electric_value(const CowanArgs& a, int c, int 
     if (c == 1) j = nyc - 1; else { j = 2 * (nyc - 1) - j; sign = -sign; }
   }
   if (k < 0) return sign * a.lower[c][(size_t)j * nxc + i];
-  if (k >= nzc) return sign * 0.0;
+  if (k >= nzc) return sign * F(0.0);
   return sign * a.e[c][((size_t)ring(k, a.g.zb_e[c], nzc) * nyc + j) * nxc + i];
 }
 
-// smoothedElectric (src/eb_field.cpp:419-486): alpha*centre, then the four
-// beta edge samples, then the four delta corners, in the reference order.
-__device__ __forceinline__ double smoothed(const CowanArgs& a, int c, int d, int i,
-                                           int j, int k) {
-  const int ta = (d + 1) % 3, tb = (d + 2) % 3;
-  const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
-  const int p[3] = {i, j, k};
-  double result = a.alpha[d] * electric_value(a, c, i, j, k);
-  for (int dir = -1; dir <= 1; dir += 2) {
-    int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
-    qa[ta] += dir;
-    qb[tb] += dir;
-    result += a.beta[ta] * electric_value(a, c, qa[0], qa[1], qa[2]);
-    result += a.beta[tb] * electric_value(a, c, qb[0], qb[1], qb[2]);
-  }
-  for (int da = -1; da <= 1; da += 2)
-    for (int db = -1; db <= 1; db += 2) {
-      int q[3] = {p[0], p[1], p[2]};
-      q[ta] += da;
-      q[tb] += db;
-      result += delta * electric_value(a, c, q[0], q[1], q[2]);
-    }
-  return result;
-}
-
 // transformedCorrection (src/eb_cpml.cpp:131-138).
-__device__ __forceinline__ double cpml_correction(const CpmlAxis& ax, int index,
-                                                  double difference, double* history) {
-  const double psi = ax.decay[index] * *history + ax.drive[index] * difference;
+template <class F>
+__device__ __forceinline__ F cpml_correction(const CpmlAxis& ax, int index, F difference,
+                                             F* history) {
+  const F psi = F(ax.decay[index]) * *history + F(ax.drive[index]) * difference;
   *history = psi;
-  return ax.inverse_kappa_minus_one[index] * difference + psi;
+  return F(ax.inverse_kappa_minus_one[index]) * difference + psi;
 }
 
-__device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, int k,
-                                              int zbase, int row_index) {
+template <class F>
+__device__ __forceinline__ F* history_at(const CpmlHistoryT<F>& h, int slot, int k, int zbase,
+                                         int row_index) {
   return h.data + ((size_t)slot * h.layers + ring(k, zbase, h.layers)) * h.row + row_index;
 }
 
@@ -77,30 +56,35 @@ __device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, in
 // A block owns a TX x TY tile of (i, j) columns and marches a chunk of z
 // planes.  The three E components of planes k-1, k, k+1 live in a shared
 // memory ring, one (TX+2) x (TY+2) tile each, loaded once per plane through
-// electricValue's parity/halo rules.  Every smoothed difference is then
-// evaluated from shared memory with the reference's 9-point order, so the
-// update is bit-identical to the reference.  Each B node is updated by the
+// electricValue's parity/halo rules.  Every smoothed difference (the
+// 9-point smoothedElectric of src/eb_field.cpp:419-486: alpha*centre, the
+// four beta edge samples, the four delta corners) is then evaluated from
+// shared memory in the reference's order, so the FP64 update is
+// bit-identical to the reference.  Each B node is updated by the
 // curl, then by its CPML terms in the reference's term order (0,2,1),
 // (1,2,0), (2,1,0), (2,0,1), reusing the curl's smoothed difference.
 constexpr int kTX = 32, kTY = 8, kKChunk = 16;
 
+template <class F>
 struct ETile {
-  double v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
+  F v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
 };
 
 __device__ __forceinline__ int plane_slot(int k) { return ((k % 3) + 3) % 3; }
 
-__device__ __forceinline__ double tile_at(const ETile& t, int c, int i, int j, int k,
-                                          int i0, int j0) {
+template <class F>
+__device__ __forceinline__ F tile_at(const ETile<F>& t, int c, int i, int j, int k, int i0,
+                                     int j0) {
   return t.v[c][plane_slot(k)][j - j0 + 1][i - i0 + 1];
 }
 
-__device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs& a, int c,
-                                                int d, int i, int j, int k, int i0, int j0) {
+template <class F>
+__device__ __forceinline__ F tile_smoothed(const ETile<F>& t, const CowanArgs<F>& a, int c,
+                                           int d, int i, int j, int k, int i0, int j0) {
   const int ta = (d + 1) % 3, tb = (d + 2) % 3;
-  const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
+  const F delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
   const int p[3] = {i, j, k};
-  double result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
+  F result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
 #pragma unroll
   for (int dir = -1; dir <= 1; dir += 2) {
     int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
@@ -125,7 +109,9 @@ __device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs&
 // component's index range are ever read by the smoothing (the reference's
 // own reach); tile points farther out, which exist only where a small grid
 // ends inside a tile, are stored as zero and never used.
-__device__ __forceinline__ void load_plane(ETile& t, const CowanArgs& a, int k, int i0, int j0) {
+template <class F>
+__device__ __forceinline__ void load_plane(ETile<F>& t, const CowanArgs<F>& a, int k, int i0,
+                                           int j0) {
   const int slot = plane_slot(k);
   constexpr int W = kTX + 2, H = kTY + 2, N = W * H;
   for (int c = 0; c < 3; ++c) {
@@ -134,19 +120,20 @@ __device__ __forceinline__ void load_plane(ETile& t, const CowanArgs& a, int k, 
       const int ii = n % W, jj = n / W;
       const int i = i0 - 1 + ii, j = j0 - 1 + jj;
       t.v[c][slot][jj][ii] = (i < -1 || i > nxc || j < -1 || j > nyc)
-                                 ? 0.0 : electric_value(a, c, i, j, k);
+                                 ? F(0.0) : electric_value(a, c, i, j, k);
     }
   }
 }
 
-__global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs a) {
-  __shared__ ETile t;
-  const DGrid& g = a.g;
+template <class F>
+__global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> a) {
+  __shared__ ETile<F> t;
+  const GridT<F>& g = a.g;
   const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
   const int k0 = blockIdx.z * kKChunk;
   const int k1 = min(k0 + kKChunk, g.nz + 1);
-  const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
+  const F dtdx = F(g.dt / g.dx), dtdy = F(g.dt / g.dy), dtdz = F(g.dt / g.dz);
   load_plane(t, a, k0 - 1, i0, j0);
   load_plane(t, a, k0, i0, j0);
   for (int k = k0; k < k1; ++k) {
@@ -154,45 +141,45 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs a) 
     __syncthreads();
     if (i <= g.nx && j <= g.ny) {
       if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
-        const double dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
+        const F dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
                              tile_smoothed(t, a, 2, 1, i, j, k, i0, j0);
-        const double dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
+        const F dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
                              tile_smoothed(t, a, 1, 2, i, j, k, i0, j0);
-        double* bx = &g.b[0][b_index(g, 0, i, j, k)];
-        double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
+        F* bx = &g.b[0][b_index(g, 0, i, j, k)];
+        F v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
         const int s = a.my.ordinal[j];
         if (s >= 0)
-          v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
+          v += F(-1.0) * dtdy * cpml_correction(a.my, j, dEzDy,
                                              history_at(a.h[0], s, k, g.zb_b[0], i));
         *bx = v;
       }
       if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
-        const double dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
+        const F dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
                              tile_smoothed(t, a, 0, 2, i, j, k, i0, j0);
-        const double dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
+        const F dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
                              tile_smoothed(t, a, 2, 0, i, j, k, i0, j0);
-        double* by = &g.b[1][b_index(g, 1, i, j, k)];
-        double v = *by - (dtdz * dExDz - dtdx * dEzDx);
+        F* by = &g.b[1][b_index(g, 1, i, j, k)];
+        F v = *by - (dtdz * dExDz - dtdx * dEzDx);
         const int s = a.mx.ordinal[i];
         if (s >= 0)
-          v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
+          v += F(1.0) * dtdx * cpml_correction(a.mx, i, dEzDx,
                                             history_at(a.h[1], s, k, g.zb_b[1], j));
         *by = v;
       }
       if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
-        const double dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
+        const F dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
                              tile_smoothed(t, a, 1, 0, i, j, k, i0, j0);
-        const double dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
+        const F dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
                              tile_smoothed(t, a, 0, 1, i, j, k, i0, j0);
-        double* bz = &g.b[2][b_index(g, 2, i, j, k)];
-        double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
+        F* bz = &g.b[2][b_index(g, 2, i, j, k)];
+        F v = *bz - (dtdx * dEyDx - dtdy * dExDy);
         const int sx = a.mx.ordinal[i];
         if (sx >= 0)
-          v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,
+          v += F(-1.0) * dtdx * cpml_correction(a.mx, i, dEyDx,
                                              history_at(a.h[2], sx, k, g.zb_b[2], j));
         const int sy = a.my.ordinal[j];
         if (sy >= 0)
-          v += 1.0 * dtdy * cpml_correction(a.my, j, dExDy,
+          v += F(1.0) * dtdy * cpml_correction(a.my, j, dExDy,
                                             history_at(a.h[3], sy, k, g.zb_b[2], i));
         *bz = v;
       }
@@ -201,7 +188,8 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs a) 
   }
 }
 
-__device__ __forceinline__ double bval(const DGrid& g, int c, int i, int j, int k) {
+template <class F>
+__device__ __forceinline__ F bval(const GridT<F>& g, int c, int i, int j, int k) {
   return g.b[c][b_index(g, c, i, j, k)];
 }
 
@@ -211,53 +199,54 @@ __device__ __forceinline__ double bval(const DGrid& g, int c, int i, int j, int 
 // advanced here once, exactly as the later commit would advance them from
 // the same B), PEC on the x/y faces, and the inlet Ex/Ey overwrite at k=0.
 // Reads E^n from e_old, writes E* to e_star.
-__global__ void electric_preview_kernel(PreviewArgs a) {
+template <class F>
+__global__ void electric_preview_kernel(PreviewArgs<F> a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
-  const DGrid& g = a.g;
+  const GridT<F>& g = a.g;
   if (i > g.nx || j > g.ny || k > g.nz) return;
   const double curl = g.dt / (kMu0 * kEpsilon0);
-  const double cx = curl / g.dx, cy = curl / g.dy, cz = curl / g.dz;
+  const F cx = F(curl / g.dx), cy = F(curl / g.dy), cz = F(curl / g.dz);
   if (i < g.nx) {  // Ex (nx, ny+1, nz+1)
     const size_t n = e_index(g, 0, i, j, k);
-    double v = g.e_old[0][n];
+    F v = g.e_old[0][n];
     if (k >= 1 && k < g.nz && j >= 1 && j < g.ny)
       v += cy * (bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k)) -
            cz * (bval(g, 1, i, j, k) - bval(g, 1, i, j, k - 1));
     if (j >= 1 && j < g.ny) {
       const int s = a.ey_prof.ordinal[j];
       if (s >= 0) {
-        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
-        v += 1.0 * cy * cpml_correction(a.ey_prof, j, diff,
+        const F diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
+        v += F(1.0) * cy * cpml_correction(a.ey_prof, j, diff,
                                         history_at(a.h[0], s, k, g.zb_e[0], i));
       }
     }
-    if (j == 0 || j == g.ny) v = 0.0;
-    if (k == 0) v = inlet_value(a.inlet, 0, i, j);
+    if (j == 0 || j == g.ny) v = F(0.0);
+    if (k == 0) v = F(inlet_value(a.inlet, 0, i, j));
     g.e_star[0][n] = v;
   }
   if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
     const size_t n = e_index(g, 1, i, j, k);
-    double v = g.e_old[1][n];
+    F v = g.e_old[1][n];
     if (k >= 1 && k < g.nz && i >= 1 && i < g.nx)
       v += cz * (bval(g, 0, i, j, k) - bval(g, 0, i, j, k - 1)) -
            cx * (bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k));
     if (i >= 1 && i < g.nx) {
       const int s = a.ex_prof.ordinal[i];
       if (s >= 0) {
-        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
-        v += -1.0 * cx * cpml_correction(a.ex_prof, i, diff,
+        const F diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
+        v += F(-1.0) * cx * cpml_correction(a.ex_prof, i, diff,
                                          history_at(a.h[1], s, k, g.zb_e[1], j));
       }
     }
-    if (i == 0 || i == g.nx) v = 0.0;
-    if (k == 0) v = inlet_value(a.inlet, 1, i, j);
+    if (i == 0 || i == g.nx) v = F(0.0);
+    if (k == 0) v = F(inlet_value(a.inlet, 1, i, j));
     g.e_star[1][n] = v;
   }
   if (k < g.nz) {  // Ez (nx+1, ny+1, nz)
     const size_t n = e_index(g, 2, i, j, k);
-    double v = g.e_old[2][n];
+    F v = g.e_old[2][n];
     const bool inner = i >= 1 && i < g.nx && j >= 1 && j < g.ny;
     if (inner)
       v += cx * (bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k)) -
@@ -265,18 +254,18 @@ __global__ void electric_preview_kernel(PreviewArgs a) {
     if (inner) {
       const int sx = a.ex_prof.ordinal[i];
       if (sx >= 0) {
-        const double diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
-        v += 1.0 * cx * cpml_correction(a.ex_prof, i, diff,
+        const F diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
+        v += F(1.0) * cx * cpml_correction(a.ex_prof, i, diff,
                                         history_at(a.h[2], sx, k, g.zb_e[2], j));
       }
       const int sy = a.ey_prof.ordinal[j];
       if (sy >= 0) {
-        const double diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
-        v += -1.0 * cy * cpml_correction(a.ey_prof, j, diff,
+        const F diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
+        v += F(-1.0) * cy * cpml_correction(a.ey_prof, j, diff,
                                          history_at(a.h[3], sy, k, g.zb_e[2], i));
       }
     }
-    if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
+    if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = F(0.0);
     g.e_star[2][n] = v;
   }
 }
@@ -284,7 +273,8 @@ __global__ void electric_preview_kernel(PreviewArgs a) {
 // commitConservativeElectric (src/simulation_source_coupling.cpp:61-65): the
 // previewed boundary already holds the committed CPML/PEC/inlet values, so
 // E^{n+1} = E* - dt/eps0 J on the applyCurrentSource mask, in place.
-__global__ void electric_commit_kernel(DGrid g) {
+template <class F>
+__global__ void electric_commit_kernel(GridT<F> g) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -292,45 +282,47 @@ __global__ void electric_commit_kernel(DGrid g) {
   for (int c = 0; c < 3; ++c) {
     if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
     if (!current_mask(g, c, i, j, k)) continue;
-    const double jc = g.j[c][j_index(g, c, i, j, k)];
-    if (jc != 0.) g.e_star[c][e_index(g, c, i, j, k)] += g.jcoef * jc;
+    const F jc = g.j[c][j_index(g, c, i, j, k)];
+    if (jc != F(0.)) g.e_star[c][e_index(g, c, i, j, k)] += g.jcoef * jc;
   }
 }
 
 // Boundary::begin lower halo planes (src/moving_window_fields.cpp:206-210):
 // reference(a, i, j, offset-1, step) for Ex, Ey, Ez.
-__global__ void inlet_lower_kernel(InletPlaneArgs a) {
+template <class F>
+__global__ void inlet_lower_kernel(InletPlaneArgs<F> a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int c = blockIdx.z;
   const int nxc = a.nx + (c != 0), nyc = a.ny + (c != 1);
   if (i >= nxc || j >= nyc) return;
-  a.out[c][(size_t)j * nxc + i] = inlet_value(a.inlet, c, i, j);
+  a.out[c][(size_t)j * nxc + i] = F(inlet_value(a.inlet, c, i, j));
 }
 
 // MovingWindowFields::shift plane insertion (src/moving_window_fields.cpp:
 // 470-517) on the ring: after the bases moved down by one, logical plane 0
 // (the dropped upper plane's storage) receives reference(a, i, j, offset,
 // step) for E and B, and every CPML history gets a zero layer at k = 0.
-__global__ void shift_insert_kernel(ShiftArgs a) {
+template <class F>
+__global__ void shift_insert_kernel(ShiftArgs<F> a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int c = blockIdx.z;  // 0..5 fields, 6..13 histories
-  const DGrid& g = a.g;
+  const GridT<F>& g = a.g;
   if (c < 3) {
     const int nxc = e_nx(g, c), nyc = e_ny(g, c);
     if (i >= nxc || j >= nyc) return;
-    g.e_old[c][e_index(g, c, i, j, 0)] = inlet_value(a.inlet, c, i, j);
+    g.e_old[c][e_index(g, c, i, j, 0)] = F(inlet_value(a.inlet, c, i, j));
   } else if (c < 6) {
     const int b = c - 3;
     const int nxc = b_nx(g, b), nyc = b_ny(g, b);
     if (i >= nxc || j >= nyc) return;
-    g.b[b][b_index(g, b, i, j, 0)] = inlet_value(a.inlet, c, i, j);
+    g.b[b][b_index(g, b, i, j, 0)] = F(inlet_value(a.inlet, c, i, j));
   } else {
-    const CpmlHistory& h = a.h[c - 6];
+    const CpmlHistoryT<F>& h = a.h[c - 6];
     // i runs over the row, j over the slots.
     if (i >= h.row || j >= h.slots) return;
-    *history_at(h, j, 0, a.history_base[c - 6], i) = 0.0;
+    *history_at(h, j, 0, a.history_base[c - 6], i) = F(0.0);
   }
 }
 
@@ -349,8 +341,9 @@ __device__ __forceinline__ void interp_axis(double lattice, int size, int* lower
   }
 }
 
-__device__ double detector_component(const DGrid& g, int comp, double lx, double ly,
-                                     int zl, double zf) {
+template <class F>
+__device__ double detector_component(const GridT<F>& g, int comp, double lx, double ly, int zl,
+                                     double zf) {
   const bool electric = comp < 3;
   const int c = comp % 3;
   const int nxc = electric ? e_nx(g, c) : b_nx(g, c);
@@ -367,18 +360,19 @@ __device__ double detector_component(const DGrid& g, int comp, double lx, double
       for (int a = 0; a < 2; ++a) {
         const double wx = a ? xf : 1.0 - xf;
         const double wy = b ? yf : 1.0 - yf;
-        const double v = electric ? g.e_old[c][e_index(g, c, xl + a, yl + b, zl + cz)]
-                                  : g.b[c][b_index(g, c, xl + a, yl + b, zl + cz)];
+        const double v = electric ? double(g.e_old[c][e_index(g, c, xl + a, yl + b, zl + cz)])
+                                  : double(g.b[c][b_index(g, c, xl + a, yl + b, zl + cz)]);
         value += wx * wy * wz * v;
       }
   }
   return value;
 }
 
-__global__ void detector_plane_kernel(DetectorArgs a) {
+template <class F>
+__global__ void detector_plane_kernel(DetectorArgs<F> a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const DGrid& g = a.g;
+  const GridT<F>& g = a.g;
   if (i >= g.nx || j >= g.ny) return;
   const double py = a.origin_xy[1] + ((double)j + 0.5) * g.dy;
   const double y = (py - a.origin_xy[1]) / g.dy;
@@ -401,5 +395,17 @@ __global__ void detector_plane_kernel(DetectorArgs a) {
   o[4] = fma(f.gamma_beta / kC, eb[0], f.gamma * bb[1]);
   o[5] = bb[2];
 }
+
+// Both element types are built: FP64 drop-in and FP32-mixed.
+#define APRL_FIELD_KERNELS(F)                                                  \
+  template __global__ void cowan_magnetic_kernel<F>(CowanArgs<F>);            \
+  template __global__ void electric_preview_kernel<F>(PreviewArgs<F>);        \
+  template __global__ void electric_commit_kernel<F>(GridT<F>);               \
+  template __global__ void inlet_lower_kernel<F>(InletPlaneArgs<F>);          \
+  template __global__ void shift_insert_kernel<F>(ShiftArgs<F>);              \
+  template __global__ void detector_plane_kernel<F>(DetectorArgs<F>);
+APRL_FIELD_KERNELS(double)
+APRL_FIELD_KERNELS(float)
+#undef APRL_FIELD_KERNELS
 
 }  // namespace aprl_gpu

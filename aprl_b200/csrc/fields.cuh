@@ -15,8 +15,9 @@ struct CpmlAxis {
 };
 
 // One active convolution history in [slot][k][row] order.
-struct CpmlHistory {
-  double* data;
+template <class F>
+struct CpmlHistoryT {
+  F* data;
   int slots, layers, row;
 };
 
@@ -39,37 +40,43 @@ __device__ __forceinline__ double inlet_value(const InletTable& t, int c, int i,
                                 t.fraction * t.table[c][(size_t)t.hi[c] * plane + cell];
 }
 
+// Argument blocks, templated on the field element type F (double or float).
+template <class F>
 struct CowanArgs {
-  DGrid g;               // B (ring) is updated in place
-  const double* e[3];    // E^n (ring)
-  const double* lower[3];  // inlet lower halo planes
-  double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
+  GridT<F> g;            // B (ring) is updated in place
+  const F* e[3];         // E^n (ring)
+  const F* lower[3];     // inlet lower halo planes
+  F alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
   CpmlAxis mx, my;       // magnetic profiles (half-integer positions)
-  CpmlHistory h[4];      // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
+  CpmlHistoryT<F> h[4];  // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
 };
 
+template <class F>
 struct PreviewArgs {
-  DGrid g;               // e_old = E^n, e_star = E* (written)
+  GridT<F> g;            // e_old = E^n, e_star = E* (written)
   CpmlAxis ex_prof, ey_prof;  // electric profiles (integer positions)
-  CpmlHistory h[4];      // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
+  CpmlHistoryT<F> h[4];  // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
   InletTable inlet;      // reference(a, i, j, offset, step+1)
 };
 
+template <class F>
 struct InletPlaneArgs {
   int nx, ny;
-  double* out[3];
+  F* out[3];
   InletTable inlet;      // reference(a, i, j, offset-1, step)
 };
 
+template <class F>
 struct ShiftArgs {
-  DGrid g;               // e_old = the committed E (ring, bases already moved)
+  GridT<F> g;            // e_old = the committed E (ring, bases already moved)
   InletTable inlet;      // reference(a, i, j, offset, step) after the shift
-  CpmlHistory h[8];      // magnetic 0,3,4,5 then electric 6,9,10,11
+  CpmlHistoryT<F> h[8];  // magnetic 0,3,4,5 then electric 6,9,10,11
   int history_base[8];
 };
 
+template <class F>
 struct DetectorArgs {
-  DGrid g;               // e_old = committed E
+  GridT<F> g;            // e_old = committed E
   DFrame frame;
   double origin_xy[2];
   int vertex_lower, half_lower;
@@ -77,11 +84,11 @@ struct DetectorArgs {
   double* out;
 };
 
-__global__ void cowan_magnetic_kernel(CowanArgs a);
-__global__ void electric_preview_kernel(PreviewArgs a);
-__global__ void electric_commit_kernel(DGrid g);
-__global__ void inlet_lower_kernel(InletPlaneArgs a);
-__global__ void shift_insert_kernel(ShiftArgs a);
-__global__ void detector_plane_kernel(DetectorArgs a);
+template <class F> __global__ void cowan_magnetic_kernel(CowanArgs<F> a);
+template <class F> __global__ void electric_preview_kernel(PreviewArgs<F> a);
+template <class F> __global__ void electric_commit_kernel(GridT<F> g);
+template <class F> __global__ void inlet_lower_kernel(InletPlaneArgs<F> a);
+template <class F> __global__ void shift_insert_kernel(ShiftArgs<F> a);
+template <class F> __global__ void detector_plane_kernel(DetectorArgs<F> a);
 
 }  // namespace aprl_gpu

@@ -6,8 +6,13 @@
 //
 // One thread owns one particle; its gathers and weights run in the
 // reference's visit order, so in FP64 (no FMA contraction) the per-particle
-// arithmetic matches the reference.  Deposition accumulates with FP64
-// atomics into J; only the summation order of J differs from the reference.
+// arithmetic matches the reference.  Deposition accumulates with atomics into
+// J; only the summation order of J differs from the reference.
+//
+// The walkers are templated on the field element type F.  Positions, chord
+// cuts and cell indices are always binary64; the weights are evaluated in F
+// from the cell-relative offsets, and the fields are read and accumulated in
+// F.  F = double is the FP64 drop-in, F = float the FP32-mixed mode.
 #include "common.cuh"
 #include "particles.cuh"
 
@@ -15,73 +20,79 @@ namespace aprl_gpu {
 
 // ---------------------------------------------------------------------------
 // shapes (src/longitudinal_shape.h:15-117, src/transverse_source_shape.h:8-10)
-__device__ __forceinline__ void node_weights(double f, double w[4]) {
-  w[0] = 0.25 * (1. - f);
-  w[1] = 0.5 - 0.25 * f;
-  w[2] = 0.25 + 0.25 * f;
-  w[3] = 0.25 * f;
+template <class F>
+__device__ __forceinline__ void node_weights(F f, F w[4]) {
+  w[0] = F(0.25) * (F(1.) - f);
+  w[1] = F(0.5) - F(0.25) * f;
+  w[2] = F(0.25) + F(0.25) * f;
+  w[3] = F(0.25) * f;
 }
 
+template <class F>
 struct Basis {
   long long first;
   int count;
-  double v[12];
+  F v[12];
 };
 
-// basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54).
-__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis& r) {
+// basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54): the
+// cell in binary64, the B-spline and compensation arithmetic in F on the
+// cell-relative offset.
+template <class F>
+__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) {
   const unsigned degree = edge ? 4 : 5;
-  const double cell = floor(z), f = z - cell;
-  double n[6] = {1., 0., 0., 0., 0., 0.};
+  const double cell = floor(z);
+  const F f = F(z - cell);
+  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
   for (unsigned j = 1; j <= degree; ++j) {
-    double saved = 0.;
+    F saved = F(0.);
     for (unsigned k = 0; k < j; ++k) {
-      const double t = n[k] / j;
-      n[k] = saved + (k + 1 - f) * t;
-      saved = (f + j - k - 1) * t;
+      const F t = n[k] / F(j);
+      n[k] = saved + (F(k + 1) - f) * t;
+      saved = (f + F(j) - F(k) - F(1)) * t;
     }
     n[j] = saved;
   }
   const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
                d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
-  const double c[7] = {-d / 64., b / 16. + 3 * d / 32., -a / 4. - b / 4. - 15 * d / 64.,
-                       1 + a / 2. + 3 * b / 8. + 5 * d / 16.,
-                       -a / 4. - b / 4. - 15 * d / 64., b / 16. + 3 * d / 32., -d / 64.};
+  const F c[7] = {F(-d / 64.), F(b / 16. + 3 * d / 32.), F(-a / 4. - b / 4. - 15 * d / 64.),
+                  F(1 + a / 2. + 3 * b / 8. + 5 * d / 16.),
+                  F(-a / 4. - b / 4. - 15 * d / 64.), F(b / 16. + 3 * d / 32.), F(-d / 64.)};
   r.first = (long long)cell - 5;
   r.count = degree + 7;
-  for (int q = 0; q < 12; ++q) r.v[q] = 0.;
+  for (int q = 0; q < 12; ++q) r.v[q] = F(0.);
   for (unsigned j = 0; j <= degree; ++j)
     for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
 }
 
 // binomialXZSegment (src/longitudinal_shape.h:61-94).
-template <class V>
-__device__ __forceinline__ void binomial_xz_segment(const DGrid& g, const double s[3],
+template <class F, class V>
+__device__ __forceinline__ void binomial_xz_segment(const GridT<F>& g, const double s[3],
                                                     const double d[3], double first,
                                                     double last, V& visit) {
-  const double width = last - first;
+  const F width = F(last - first);
   const double mid = (first + last) * 0.5;
   const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
   long long i = (long long)floor(x), j = (long long)floor(y);
   const long long k = (long long)floor(z);
   if (i == (long long)g.nx) --i;
   if (j == (long long)g.ny) --j;
-  double wx[4], wz[4];
-  node_weights(x - i, wx);
-  node_weights(z - k, wz);
-  const double wy[2] = {1. - (y - j), y - j};
-  const double edge[3] = {0.25, 0.5, 0.25};
-  const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
-  const double sy[2] = {-1., 1.};
-  const double curvature = width * width / 12.;
-  const double xy = curvature * d[0] * d[1];
-  const double xz = curvature * d[0] * d[2];
-  const double yz = curvature * d[1] * d[2];
+  F wx[4], wz[4];
+  node_weights(F(x - i), wx);
+  node_weights(F(z - k), wz);
+  const F wy[2] = {F(1.) - F(y - j), F(y - j)};
+  const F edge[3] = {F(0.25), F(0.5), F(0.25)};
+  const F slope[4] = {F(-0.25), F(-0.25), F(0.25), F(0.25)};
+  const F sy[2] = {F(-1.), F(1.)};
+  const F curvature = width * width / F(12.);
+  const F xy = curvature * F(d[0]) * F(d[1]);
+  const F xz = curvature * F(d[0]) * F(d[2]);
+  const F yz = curvature * F(d[1]) * F(d[2]);
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+      const F weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
 #pragma unroll
       for (int a = 0; a < 3; ++a) visit(0, i - 1 + a, j + b, k - 1 + c, weight * edge[a]);
     }
@@ -93,19 +104,16 @@ __device__ __forceinline__ void binomial_xz_segment(const DGrid& g, const double
   for (int b = 0; b < 2; ++b)
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-      const double weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+      const F weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
 #pragma unroll
       for (int c = 0; c < 3; ++c) visit(2, i - 1 + a, j + b, k - 1 + c, weight * edge[c]);
     }
 }
 
-// longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
-// smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
-// when the chord exceeds the 64-cut crossing budget.
 // Four-point Gauss quadrature of the quintic-compensated shape over one cut
 // piece of the chord (the quintic branch of longitudinal_shape::weights).
-template <class V>
-__device__ __forceinline__ void quintic_segment(const DGrid& g, const double x[3],
+template <class F, class V>
+__device__ __forceinline__ void quintic_segment(const GridT<F>& g, const double x[3],
                                                 const double v[3], double lower,
                                                 double upper, double width, V& visit) {
   const double q[4] = {-.8611363115940525752, -.3399810435848562648,
@@ -113,34 +121,38 @@ __device__ __forceinline__ void quintic_segment(const DGrid& g, const double x[3
   const double qw[4] = {.3478548451374538574, .6521451548625461426,
                         .6521451548625461426, .3478548451374538574};
   for (int t = 0; t < 4; ++t) {
-    const double u = .5 * (upper + lower + width * q[t]),
-                 factor = .5 * width * qw[t], xx = x[0] + u * v[0],
+    const double u = .5 * (upper + lower + width * q[t]), xx = x[0] + u * v[0],
                  yy = x[1] + u * v[1], zz = x[2] + u * v[2];
+    const F factor = F(.5 * width * qw[t]);
     long long i = (long long)floor(xx), j = (long long)floor(yy);
     if (i == (long long)g.nx) --i;
     if (j == (long long)g.ny) --j;
-    const double fx = xx - i, fy = yy - j;
-    Basis nodes, edge;
+    const F fx = F(xx - i), fy = F(yy - j);
+    Basis<F> nodes, edge;
     quintic_basis(zz, false, nodes);
     quintic_basis(zz, true, edge);
     for (int k = 0; k < nodes.count; ++k) {
-      const double w = factor * nodes.v[k];
-      if (w == 0.) continue;
-      for (int b = 0; b < 2; ++b) visit(0, i, j + b, nodes.first + k, w * (b ? fy : 1. - fy));
-      for (int a = 0; a < 2; ++a) visit(1, i + a, j, nodes.first + k, w * (a ? fx : 1. - fx));
+      const F w = factor * nodes.v[k];
+      if (w == F(0.)) continue;
+      for (int b = 0; b < 2; ++b) visit(0, i, j + b, nodes.first + k, w * (b ? fy : F(1.) - fy));
+      for (int a = 0; a < 2; ++a) visit(1, i + a, j, nodes.first + k, w * (a ? fx : F(1.) - fx));
     }
     for (int k = 0; k < edge.count; ++k) {
-      const double w = factor * edge.v[k];
-      if (w == 0.) continue;
+      const F w = factor * edge.v[k];
+      if (w == F(0.)) continue;
       for (int b = 0; b < 2; ++b)
         for (int a = 0; a < 2; ++a)
-          visit(2, i + a, j + b, edge.first + k, w * (a ? fx : 1. - fx) * (b ? fy : 1. - fy));
+          visit(2, i + a, j + b, edge.first + k,
+                w * (a ? fx : F(1.) - fx) * (b ? fy : F(1.) - fy));
     }
   }
 }
 
-template <class V>
-__device__ int shape_weights(const DGrid& g, int shape, const double begin[3],
+// longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
+// smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
+// when the chord exceeds the 64-cut crossing budget.
+template <class F, class V>
+__device__ int shape_weights(const GridT<F>& g, int shape, const double begin[3],
                              const double end[3], V& visit) {
   const double h[3] = {g.dx, g.dy, g.dz};
   // The cell-boundary cuts of the chord, ascending.  Along each axis the cuts
@@ -206,7 +218,8 @@ struct OpenOrbit {
 };
 
 // clipOpenOrbit at one rank (src/source_coupling_math.h:234-250).
-__device__ __forceinline__ bool clip_open_orbit(const DGrid& g, const double b[3],
+template <class F>
+__device__ __forceinline__ bool clip_open_orbit(const GridT<F>& g, const double b[3],
                                                 const double e[3], OpenOrbit& o) {
   const double ds[3] = {g.dx, g.dy, g.dz};
   const double size[3] = {(double)g.nx, (double)g.ny, (double)g.nz};
@@ -248,32 +261,32 @@ __device__ __forceinline__ bool clip_open_orbit(const DGrid& g, const double b[3
 // Orbit average of 1/2 (E_new + E^n) with the shape weights.  with_current
 // selects E_new = E* - dt/eps0 J (residual) or E* (first-trial guess, when
 // the grid still holds the zero-current preview).
+template <class F>
 struct ElectricVisitor {
   static constexpr bool kF3Segment = true;
-  const DGrid* g;
+  const GridT<F>* g;
   bool with_current;
-  double r[3];
-  __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k,
-                                             double w) {
-    const DGrid& G = *g;
+  F r[3];
+  __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k, F w) {
+    const GridT<F>& G = *g;
     if (i < 0 || j < 0 || i >= e_nx(G, d) || j >= e_ny(G, d)) return;
     if (k < 0 || k >= e_nz(G, d)) return;
     const int ii = (int)i, jj = (int)j, kk = (int)k;
     const size_t n = e_index(G, d, ii, jj, kk);
-    const double vn = with_current ? e_candidate(G, d, ii, jj, kk) : G.e_star[d][n];
-    r[d] += .5 * w * (vn + G.e_old[d][n]);
+    const F vn = with_current ? e_candidate(G, d, ii, jj, kk) : G.e_star[d][n];
+    r[d] += F(.5) * w * (vn + G.e_old[d][n]);
   }
 
   // One accumulation .5*w*(E_new + E^n) at ring/plain offsets (n, jn) of a
   // node whose applyCurrentSource mask is known to be true.
-  __device__ __forceinline__ double term(int d, size_t n, size_t jn, double w) const {
-    const DGrid& G = *g;
-    double vn = G.e_star[d][n];
+  __device__ __forceinline__ F term(int d, size_t n, size_t jn, F w) const {
+    const GridT<F>& G = *g;
+    F vn = G.e_star[d][n];
     if (with_current) {
-      const double jc = G.j[d][jn];
-      if (jc != 0.) vn += G.jcoef * jc;
+      const F jc = G.j[d][jn];
+      if (jc != F(0.)) vn += G.jcoef * jc;
     }
-    return .5 * w * (vn + G.e_old[d][n]);
+    return F(.5) * w * (vn + G.e_old[d][n]);
   }
 
   // binomialXZSegment specialised for the gather.  When the whole 4x2x4
@@ -282,9 +295,9 @@ struct ElectricVisitor {
   // row is addressed once and its nodes read back to back; otherwise the
   // generic visits run.  Per component the accumulation order is the
   // reference's (Ex: k, y, x; Ey: k, x; Ez: y, x, k).
-  __device__ __forceinline__ void f3_segment(const DGrid& G, const double s[3],
+  __device__ __forceinline__ void f3_segment(const GridT<F>& G, const double s[3],
                                              const double d[3], double first, double last) {
-    const double width = last - first;
+    const F width = F(last - first);
     const double mid = (first + last) * 0.5;
     const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
     long long i = (long long)floor(x), j = (long long)floor(y);
@@ -295,17 +308,17 @@ struct ElectricVisitor {
       binomial_xz_segment(G, s, d, first, last, *this);
       return;
     }
-    double wx[4], wz[4];
-    node_weights(x - i, wx);
-    node_weights(z - k, wz);
-    const double wy[2] = {1. - (y - j), y - j};
-    const double edge[3] = {0.25, 0.5, 0.25};
-    const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
-    const double sy[2] = {-1., 1.};
-    const double curvature = width * width / 12.;
-    const double xy = curvature * d[0] * d[1];
-    const double xz = curvature * d[0] * d[2];
-    const double yz = curvature * d[1] * d[2];
+    F wx[4], wz[4];
+    node_weights(F(x - i), wx);
+    node_weights(F(z - k), wz);
+    const F wy[2] = {F(1.) - F(y - j), F(y - j)};
+    const F edge[3] = {F(0.25), F(0.5), F(0.25)};
+    const F slope[4] = {F(-0.25), F(-0.25), F(0.25), F(0.25)};
+    const F sy[2] = {F(-1.), F(1.)};
+    const F curvature = width * width / F(12.);
+    const F xy = curvature * F(d[0]) * F(d[1]);
+    const F xz = curvature * F(d[0]) * F(d[2]);
+    const F yz = curvature * F(d[1]) * F(d[2]);
     const int I = (int)i, J = (int)j, K = (int)k;
     // Ex (nx, ny+1, nz+1): nodes x I-1..I+1, y J..J+1, z K-1..K+2
     {
@@ -316,7 +329,7 @@ struct ElectricVisitor {
         const size_t jplane = (size_t)(K - 1 + c) * nyc;
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-          const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+          const F weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
           const size_t n0 = (plane + J + b) * nxc + (I - 1);
           const size_t j0 = (jplane + J + b) * nxc + (I - 1);
 #pragma unroll
@@ -349,7 +362,7 @@ struct ElectricVisitor {
       for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          const double weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+          const F weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             r[2] += term(2, (plane[c] + J + b) * nxc + (I - 1 + a),
@@ -359,8 +372,9 @@ struct ElectricVisitor {
   }
 };
 
-__device__ __forceinline__ double open_b(const DGrid& g, int a, long long i, long long j,
-                                         long long k) {
+template <class F>
+__device__ __forceinline__ F open_b(const GridT<F>& g, int a, long long i, long long j,
+                                    long long k) {
   const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
   if (i < 0) i = 0;
   if (i > nxc - 1) i = nxc - 1;
@@ -374,7 +388,8 @@ __device__ __forceinline__ double open_b(const DGrid& g, int a, long long i, lon
 // binomialXZMagneticSample (src/source_coupling_math.h:142-167).  Rows of
 // the 4x2x4 stencil that lie inside the component are read without the
 // open-face clamps; the clamped form runs otherwise.  Same order either way.
-__device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const double p[3],
+template <class F>
+__device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const double p[3],
                                                      double value[3]) {
   const double h[3] = {g.dx, g.dy, g.dz};
 #pragma unroll
@@ -386,22 +401,22 @@ __device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const doubl
       cell[d] = (long long)floor(pos);
       fraction[d] = pos - cell[d];
     }
-    double wx[4], wz[4];
-    node_weights(fraction[0], wx);
-    node_weights(fraction[2], wz);
-    const double wy[2] = {1. - fraction[1], fraction[1]};
+    F wx[4], wz[4];
+    node_weights(F(fraction[0]), wx);
+    node_weights(F(fraction[2]), wz);
+    const F wy[2] = {F(1. - fraction[1]), F(fraction[1])};
     const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
-    double v = 0.;
+    F v = F(0.);
     if (cell[0] >= 1 && cell[0] + 2 <= nxc - 1 && cell[1] >= 0 && cell[1] + 1 <= nyc - 1 &&
         cell[2] >= 1 && cell[2] + 2 <= nzc - 1) {
-      const double* base = g.b[a];
+      const F* base = g.b[a];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const size_t plane = (size_t)ring((int)cell[2] - 1 + k, g.zb_b[a], (int)nzc) * nyc;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const double* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
-          double r = 0.;
+          const F* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
+          F r = F(0.);
 #pragma unroll
           for (int i = 0; i < 4; ++i) r += wx[i] * row[i];
           v += wz[k] * wy[j] * r;
@@ -410,18 +425,19 @@ __device__ __forceinline__ void binomial_xz_magnetic(const DGrid& g, const doubl
     } else {
       for (int k = 0; k < 4; ++k)
         for (int j = 0; j < 2; ++j) {
-          double row = 0.;
+          F row = F(0.);
           for (int i = 0; i < 4; ++i)
             row += wx[i] * open_b(g, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
           v += wz[k] * wy[j] * row;
         }
     }
-    value[a] = v;
+    value[a] = double(v);
   }
 }
 
 // magneticSample(bounds=false, halo, openFaces=true) (src/source_coupling_math.h:122-138).
-__device__ __forceinline__ void trilinear_magnetic(const DGrid& g, const double p[3],
+template <class F>
+__device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const double p[3],
                                                    double value[3]) {
   const double ds[3] = {g.dx, g.dy, g.dz};
   int cell[2][3];
@@ -434,36 +450,38 @@ __device__ __forceinline__ void trilinear_magnetic(const DGrid& g, const double 
     }
   for (int axis = 0; axis < 3; ++axis) {
     const int hx = axis == 0 ? 0 : 1, hy = axis == 1 ? 0 : 1, hz = axis == 2 ? 0 : 1;
-    double v = 0.;
+    F v = F(0.);
     for (int k = 0; k < 2; ++k)
       for (int j = 0; j < 2; ++j)
         for (int i = 0; i < 2; ++i) {
-          const double x = i ? fraction[hx][0] : 1 - fraction[hx][0],
-                       y = j ? fraction[hy][1] : 1 - fraction[hy][1],
-                       z = k ? fraction[hz][2] : 1 - fraction[hz][2];
+          const F x = F(i ? fraction[hx][0] : 1 - fraction[hx][0]),
+                  y = F(j ? fraction[hy][1] : 1 - fraction[hy][1]),
+                  z = F(k ? fraction[hz][2] : 1 - fraction[hz][2]);
           v += x * y * z *
                open_b(g, axis, cell[hx][0] + i, cell[hy][1] + j, cell[hz][2] + k);
         }
-    value[axis] = v;
+    value[axis] = double(v);
   }
 }
 
 // Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
-__device__ __forceinline__ unsigned gather_electric(const DGrid& g, int shape,
+template <class F>
+__device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
                                                     bool with_current, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
-  ElectricVisitor v{&g, with_current, {0., 0., 0.}};
+  ElectricVisitor<F> v{&g, with_current, {F(0.), F(0.), F(0.)}};
   if (shape_weights(g, shape, path.begin, path.end, v) < 0) return kErrCrossingBudget;
   const double fraction = path.last - path.first;
-  for (int d = 0; d < 3; ++d) out[d] = v.r[d] * fraction;
+  for (int d = 0; d < 3; ++d) out[d] = double(v.r[d]) * fraction;
   return kErrNone;
 }
 
 // Impl::magnetic (src/source_coupling.cpp:40-51).
-__device__ __forceinline__ unsigned gather_magnetic(const DGrid& g, int shape,
+template <class F>
+__device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
                                                     double out[3]) {
   OpenOrbit path;
@@ -480,16 +498,16 @@ __device__ __forceinline__ unsigned gather_magnetic(const DGrid& g, int shape,
 
 // ---------------------------------------------------------------------------
 // deposition: Current::deposit at one rank (src/longitudinal_shape.h:175-187)
+template <class F>
 struct DepositVisitor {
   static constexpr bool kF3Segment = false;
-  const DGrid* g;
-  double scale[3];
+  const GridT<F>* g;
+  F scale[3];
   bool smooth_x;
   unsigned error;
-  __device__ __forceinline__ void operator()(int a, long long i, long long j, long long k,
-                                             double w) {
-    if (scale[a] == 0.) return;
-    const DGrid& G = *g;
+  __device__ __forceinline__ void operator()(int a, long long i, long long j, long long k, F w) {
+    if (scale[a] == F(0.)) return;
+    const GridT<F>& G = *g;
     if (i < 0 || i >= e_nx(G, a)) {
       if (!smooth_x) error = kErrSupportX;
       return;
@@ -505,7 +523,8 @@ struct DepositVisitor {
 
 // ChargeConservingCurrentDepositor::depositSegment (src/eb_deposition.cpp:41-51,
 // validatePosition 228-246).
-__device__ unsigned deposit_segment(const DGrid& g, int shape, const double b[3],
+template <class F>
+__device__ unsigned deposit_segment(const GridT<F>& g, int shape, const double b[3],
                                     const double e[3], double charge) {
   const double extent[3] = {(double)g.nx * g.dx, (double)g.ny * g.dy, (double)g.nz * g.dz};
   for (int a = 0; a < 3; ++a) {
@@ -515,12 +534,12 @@ __device__ unsigned deposit_segment(const DGrid& g, int shape, const double b[3]
     if (!isfinite(e[a]) || re < -tol || re > extent[a] + tol) return kErrDepositOutside;
   }
   if (!isfinite(charge)) return kErrNonFinite;
-  DepositVisitor v;
+  DepositVisitor<F> v;
   v.g = &g;
   v.smooth_x = shape == 0;
   v.error = kErrNone;
   for (int a = 0; a < 3; ++a)
-    v.scale[a] = charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt);
+    v.scale[a] = F(charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt));
   if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
   return v.error;
 }
@@ -621,7 +640,8 @@ __device__ void magnet_lab(const DMagnet& m, const double pos[3], double b[3]) {
 
 // SIFieldSourceSet::addPrescribedBox (src/eb_sources.cpp:537-582) with lab
 // magnets only: box event -> lab event, sum of magnets, lab -> box fields.
-__device__ void add_prescribed_box(const PushArgs& a, const double pos[3], double t_box,
+template <class F>
+__device__ void add_prescribed_box(const PushArgs<F>& a, const double pos[3], double t_box,
                                    double e[3], double b[3]) {
   if (a.n_magnets == 0) return;
   const DFrame& f = a.frame;
@@ -780,7 +800,8 @@ struct CarrierState {
 
 // processCarrierSegment at one rank (src/simulation.cpp:4310-4407).
 // Returns an error code; *kept tells whether the carrier survives.
-__device__ unsigned carrier_segment(const DGrid& g, int shape, const DRegion& r,
+template <class F>
+__device__ unsigned carrier_segment(const GridT<F>& g, int shape, const DRegion& r,
                                     CarrierState& c, const double seg_start[3],
                                     double seg_start_fraction, TrialCounters* counters,
                                     bool& kept) {
@@ -824,7 +845,8 @@ __device__ unsigned carrier_segment(const DGrid& g, int shape, const DRegion& r,
 // Existing CPML carriers: ballistic step, damped deposit, outer exit
 // (src/simulation.cpp:4531-4537).  Carriers deposit with the run's shape,
 // like every ChargeConservingCurrentDepositor call.
-__global__ void carrier_kernel(CarrierArgs a) {
+template <class F>
+__global__ void carrier_kernel(CarrierArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   CarrierState c;
@@ -849,7 +871,8 @@ __global__ void carrier_kernel(CarrierArgs a) {
 // `substeps` Lapenta-Markidis substeps with the prescribed magnets, using the
 // slot's gathered fields (the ballistic-guess gather of the first trial, or
 // the previous residual's re-gather).
-__device__ unsigned coupling_push(const PushArgs& a, long long n, double pos[3], double u[3],
+template <class F>
+__device__ unsigned coupling_push(const PushArgs<F>& a, long long n, double pos[3], double u[3],
                                   double q, double m, double time, double dt, double used_e[3],
                                   double used_b[3], double& abs_work) {
   for (int d = 0; d < 3; ++d) {
@@ -889,14 +912,15 @@ __device__ unsigned coupling_push(const PushArgs& a, long long n, double pos[3],
 // validation (src/longitudinal_shape.h:175-187): the upstream part of an
 // admitted held particle and the frozen source support
 // (src/source_coupling.cpp:73-78) deposit this way.
-__device__ unsigned deposit_current(const DGrid& g, int shape, const double b[3],
+template <class F>
+__device__ unsigned deposit_current(const GridT<F>& g, int shape, const double b[3],
                                     const double e[3], double charge) {
-  DepositVisitor v;
+  DepositVisitor<F> v;
   v.g = &g;
   v.smooth_x = shape == 0;
   v.error = kErrNone;
   for (int a = 0; a < 3; ++a)
-    v.scale[a] = charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt);
+    v.scale[a] = F(charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt));
   if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
   return v.error;
 }
@@ -915,7 +939,8 @@ struct SlotPlan {
   unsigned err;
 };
 
-__device__ __forceinline__ SlotPlan plan_slot(const DGrid& g, const DFrame& f, double plane,
+template <class F>
+__device__ __forceinline__ SlotPlan plan_slot(const GridT<F>& g, const DFrame& f, double plane,
                                               double t, const double start[3], bool frozen,
                                               double beta) {
   SlotPlan s;
@@ -954,7 +979,8 @@ __device__ __forceinline__ SlotPlan plan_slot(const DGrid& g, const DFrame& f, d
 // (Impl::Slot::guess, src/source_coupling.cpp:92-95), gathered from E*
 // before any current of the trial is deposited; the push reads them as the
 // previous residual's fields.
-__global__ void guess_gather_kernel(PushArgs a) {
+template <class F>
+__global__ void guess_gather_kernel(PushArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   const double start[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
@@ -985,10 +1011,11 @@ __global__ void guess_gather_kernel(PushArgs a) {
 // up to an activation kink (4684-4756) and processActiveSegment (4760-4917)
 // with Simulation::firstMovingWindowEntry
 // (src/simulation_moving_window.cpp:380-395).
-__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs a) {
+template <class F>
+__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
-  const DGrid& g = a.g;
+  const GridT<F>& g = a.g;
   const double t = a.time, dt = g.dt;
   double start[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};
   double u[3] = {a.p.ux[n], a.p.uy[n], a.p.uz[n]};
@@ -1156,7 +1183,8 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs a) {
+template <class F>
+__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double force = 0.0, defect = 0.0, scale = 0.0;
   const unsigned char seen = n < a.count ? a.slot.seen[n] : 0;
@@ -1420,7 +1448,8 @@ __global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
 // (PendingParticleQueue::visitNear + depositFrozenSourceSupport,
 // src/simulation.cpp:4170-4172, src/source_coupling.cpp:73-78): each
 // deposits its held chord of this step without endpoint validation.
-__global__ void frozen_support_kernel(SupportArgs a) {
+template <class F>
+__global__ void frozen_support_kernel(SupportArgs<F> a) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.count) return;
   const long long k = a.begin + i;
@@ -1458,5 +1487,16 @@ __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen,
   if (i < n && z[i] < origin && !frozen[i])
     raise_error(status, kErrFellBehind, (unsigned long long)i);
 }
+
+// Both element types are built: FP64 drop-in and FP32-mixed.
+#define APRL_PARTICLE_KERNELS(F)                                              \
+  template __global__ void guess_gather_kernel<F>(PushArgs<F>);              \
+  template __global__ void push_deposit_kernel<F>(PushArgs<F>);              \
+  template __global__ void carrier_kernel<F>(CarrierArgs<F>);                \
+  template __global__ void residual_kernel<F>(ResidualArgs<F>);              \
+  template __global__ void frozen_support_kernel<F>(SupportArgs<F>);
+APRL_PARTICLE_KERNELS(double)
+APRL_PARTICLE_KERNELS(float)
+#undef APRL_PARTICLE_KERNELS
 
 }  // namespace aprl_gpu

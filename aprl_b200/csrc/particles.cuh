@@ -76,8 +76,12 @@ struct DSlots {
   unsigned char* seen;
 };
 
+// The argument blocks of the particle kernels are templated on the field
+// element type F (double: FP64 drop-in; float: FP32-mixed).  Particle
+// state, the push and the boundary logic are binary64 in both modes.
+template <class F>
 struct PushArgs {
-  DGrid g;
+  GridT<F> g;
   DFrame frame;
   DRegion region;
   DMagnet magnets[kMaxMagnets];
@@ -105,8 +109,9 @@ struct PushArgs {
   DeviceStatus* status;
 };
 
+template <class F>
 struct CarrierArgs {
-  DGrid g;
+  GridT<F> g;
   DRegion region;
   int shape;
   long long count;
@@ -117,8 +122,9 @@ struct CarrierArgs {
   DeviceStatus* status;
 };
 
+template <class F>
 struct ResidualArgs {
-  DGrid g;
+  GridT<F> g;
   int shape;
   long long count;
   DParticles p;
@@ -152,10 +158,10 @@ struct ResidualArgs {
 #define APRL_RESIDUAL_BOUNDS
 #endif
 
-__global__ void guess_gather_kernel(PushArgs a);
-__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs a);
-__global__ void carrier_kernel(CarrierArgs a);
-__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs a);
+template <class F> __global__ void guess_gather_kernel(PushArgs<F> a);
+template <class F> __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
+template <class F> __global__ void carrier_kernel(CarrierArgs<F> a);
+template <class F> __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
 
 // Stable compaction helpers (warp ballot + block scan + block-offset scan).
 constexpr int kScanBlock = 256;
@@ -195,8 +201,9 @@ struct DPending {
 __global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
                              long long begin, long long count, unsigned long long steps,
                              double held_distance_per_beta, unsigned long long first_order);
+template <class F>
 struct SupportArgs {
-  DGrid g;
+  GridT<F> g;
   int shape;
   DPending src;
   long long begin, count;
@@ -204,7 +211,7 @@ struct SupportArgs {
   double held_distance_per_beta; // c*dt
   DeviceStatus* status;
 };
-__global__ void frozen_support_kernel(SupportArgs a);
+template <class F> __global__ void frozen_support_kernel(SupportArgs<F> a);
 __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
                                   double lower, unsigned char* keep,
                                   TrialCounters* counters, DeviceStatus* status);

@@ -104,6 +104,17 @@ aprl_status device_error_status(unsigned code) {
   }
 }
 
+aprl_status device_alloc_bytes(void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 8;
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(APRL_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return APRL_OK;
+}
+
 template <class T>
 aprl_status device_alloc(T** p, size_t count) {
   *p = nullptr;
@@ -198,12 +209,15 @@ struct DeviceProfile {
 // One of the 8 active histories.  component: ABI index (0..5); derivative
 // axis 0/1; the history's k ring follows its component's ring.
 struct HistoryBuffer {
-  double* data = nullptr;
+  void* data = nullptr;  // field element type of the run
   int slots = 0, layers = 0, row = 0;
   int component = 0;
   int abi_index = 0;
   size_t length() const { return (size_t)slots * layers * row; }
-  CpmlHistory view() const { return CpmlHistory{data, slots, layers, row}; }
+  template <class F>
+  CpmlHistoryT<F> view() const {
+    return CpmlHistoryT<F>{static_cast<F*>(data), slots, layers, row};
+  }
 };
 
 struct Timing {
@@ -217,11 +231,15 @@ struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
   double coeff[12]{};
-  double* e[2][3]{};
+  // Field storage in the run's element type (double, or float in the
+  // FP32-mixed mode); `fes` is its size in bytes.
+  bool fp32 = false;
+  size_t fes = 8;
+  void* e[2][3]{};
   int cur = 0;  // e[cur] = E^n (committed), e[1-cur] = E*
-  double* b[3]{};
-  double* jc[3]{};
-  double* lower[3]{};
+  void* b[3]{};
+  void* jc[3]{};
+  void* lower[3]{};
   int zb_e[3]{}, zb_b[3]{};
   double* ref[6]{};
   bool ref_set[6]{};
@@ -365,8 +383,10 @@ aprl_status launch(aprl_run* r, unsigned id, K kernel, dim3 grid, dim3 block, Ar
     if (s_ != APRL_OK) return s_;    \
   } while (0)
 
-DGrid make_grid(const aprl_run* r) {
-  DGrid g{};
+// Device view of the grid in the run's field element type F.
+template <class F>
+GridT<F> make_grid(const aprl_run* r) {
+  GridT<F> g{};
   g.nx = (int)r->cfg.nx;
   g.ny = (int)r->cfg.ny;
   g.nz = (int)r->cfg.nz;
@@ -376,15 +396,45 @@ DGrid make_grid(const aprl_run* r) {
   g.dt = r->cfg.dt;
   for (int a = 0; a < 3; ++a) {
     g.origin[a] = r->origin[a];
-    g.e_old[a] = r->e[r->cur][a];
-    g.e_star[a] = r->e[1 - r->cur][a];
-    g.b[a] = r->b[a];
-    g.j[a] = r->jc[a];
+    g.e_old[a] = static_cast<F*>(r->e[r->cur][a]);
+    g.e_star[a] = static_cast<F*>(r->e[1 - r->cur][a]);
+    g.b[a] = static_cast<F*>(r->b[a]);
+    g.j[a] = static_cast<F*>(r->jc[a]);
     g.zb_e[a] = r->zb_e[a];
     g.zb_b[a] = r->zb_b[a];
   }
-  g.jcoef = -1. * r->cfg.dt / kEpsilon0;
+  g.jcoef = F(-1. * r->cfg.dt / kEpsilon0);
   return g;
+}
+
+// Geometry only (no field pointers), for the particle sort.
+DGrid make_geometry(const aprl_run* r) {
+  DGrid g{};
+  g.nx = (int)r->cfg.nx;
+  g.ny = (int)r->cfg.ny;
+  g.nz = (int)r->cfg.nz;
+  g.dx = r->cfg.dx;
+  g.dy = r->cfg.dy;
+  g.dz = r->cfg.dz;
+  g.dt = r->cfg.dt;
+  for (int a = 0; a < 3; ++a) g.origin[a] = r->origin[a];
+  return g;
+}
+
+// The detector arguments with the grid view of the run's field type.
+template <class F>
+DetectorArgs<F> retyped(const DetectorArgs<double>& d, const GridT<F>& g) {
+  DetectorArgs<F> a{};
+  a.g = g;
+  a.frame = d.frame;
+  a.origin_xy[0] = d.origin_xy[0];
+  a.origin_xy[1] = d.origin_xy[1];
+  a.vertex_lower = d.vertex_lower;
+  a.half_lower = d.half_lower;
+  a.vertex_fraction = d.vertex_fraction;
+  a.half_fraction = d.half_fraction;
+  a.out = d.out;
+  return a;
 }
 
 DFrame make_frame(const aprl_run_config& c) {
@@ -458,6 +508,8 @@ aprl_status validate(const aprl_run_config& g) {
       !(g.cpml_target_reflection > 0.0 && g.cpml_target_reflection < 1.0) ||
       !(g.cpml_kappa_max >= 1.0) || !(g.cpml_alpha_fraction >= 0.0))
     return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid CPML grading parameters");
+  if (g.precision != APRL_PRECISION_FP64 && g.precision != APRL_PRECISION_FP32_MIXED)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "precision must be APRL_PRECISION_FP64 or APRL_PRECISION_FP32_MIXED");
   if (g.shape != APRL_SHAPE_LINEAR_BINOMIAL3 && g.shape != APRL_SHAPE_QUINTIC_COMPENSATED)
     return fail(APRL_ERR_INVALID_ARGUMENT, "APRL 2.1 longitudinal_shape must be linear-binomial3 or quintic-compensated");
   if (g.substeps < 1 || g.max_trials < 1 || g.max_trials > 64)
@@ -604,23 +656,35 @@ aprl_status reserve_carriers(aprl_run* r, size_t n) {
   return ensure_scan(r, n);
 }
 
-// Rotate between logical (window) and physical (ring) plane order.
-aprl_status copy_ring(aprl_run* r, double* device, const double* host_in, double* host_out,
+// Rotate between logical (window) and physical (ring) plane order.  The
+// host side is always binary64; an FP32-mixed run converts through a float
+// staging copy.
+aprl_status copy_ring(aprl_run* r, void* device, const double* host_in, double* host_out,
                       size_t plane, size_t layers, int base, size_t slots = 1) {
+  const size_t es = r->fes, total = slots * layers * plane;
+  std::vector<float> stage;
+  if (es == 4) {
+    stage.resize(total);
+    if (host_in)
+      for (size_t i = 0; i < total; ++i) stage[i] = static_cast<float>(host_in[i]);
+  }
+  char* host = es == 4 ? reinterpret_cast<char*>(stage.data())
+                       : reinterpret_cast<char*>(host_in ? const_cast<double*>(host_in) : host_out);
   for (size_t s = 0; s < slots; ++s) {
     const size_t slot_offset = s * layers * plane;
     for (size_t k = 0; k < layers; ++k) {
       const size_t pk = (k + base) % layers;
-      double* d = device + slot_offset + pk * plane;
+      char* d = static_cast<char*>(device) + (slot_offset + pk * plane) * es;
+      char* h = host + (slot_offset + k * plane) * es;
       if (host_in)
-        CUDA_TRY(cudaMemcpyAsync(d, host_in + slot_offset + k * plane, plane * 8,
-                                 cudaMemcpyHostToDevice, r->stream));
+        CUDA_TRY(cudaMemcpyAsync(d, h, plane * es, cudaMemcpyHostToDevice, r->stream));
       else
-        CUDA_TRY(cudaMemcpyAsync(host_out + slot_offset + k * plane, d, plane * 8,
-                                 cudaMemcpyDeviceToHost, r->stream));
+        CUDA_TRY(cudaMemcpyAsync(h, d, plane * es, cudaMemcpyDeviceToHost, r->stream));
     }
   }
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (es == 4 && host_out)
+    for (size_t i = 0; i < total; ++i) host_out[i] = static_cast<double>(stage[i]);
   return APRL_OK;
 }
 
@@ -680,7 +744,7 @@ aprl_status compact_count(aprl_run* r, const unsigned char* flag, unsigned char 
 aprl_status sort_particles(aprl_run* r) {
   if (r->np == 0) return APRL_OK;
   const long long n = (long long)r->np;
-  const DGrid g = make_grid(r);
+  const DGrid g = make_geometry(r);
   CUDA_TRY(cudaMemsetAsync(r->tile_count, 0, r->ntiles * sizeof(unsigned), r->stream));
   TRY(launch(r, kTileCount, tile_count_kernel, dim3(blocks_for(r->np, 256)), dim3(256), r->p, n, g,
              r->tiles[0], r->tiles[1], r->tiles[2], r->tile_count, r->tile_of, r->tile_rank));
@@ -779,52 +843,58 @@ aprl_status admit_pending(aprl_run* r) {
   return APRL_OK;
 }
 
-aprl_status do_advance_magnetic(aprl_run* r) {
+template <class F>
+aprl_status advance_magnetic_t(aprl_run* r) {
   if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
   TRY(admit_pending(r));
   const aprl_run_config& c = r->cfg;
   for (int a = 0; a < 3; ++a)
-    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream));
-  InletPlaneArgs ia{};
+    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
+  InletPlaneArgs<F> ia{};
   ia.nx = (int)c.nx;
   ia.ny = (int)c.ny;
-  for (int a = 0; a < 3; ++a) ia.out[a] = r->lower[a];
+  for (int a = 0; a < 3; ++a) ia.out[a] = static_cast<F*>(r->lower[a]);
   TRY(inlet_table(r, r->offset - 1, r->step, ia.inlet));
-  TRY(launch(r, kInletLower, inlet_lower_kernel,
+  TRY(launch(r, kInletLower, inlet_lower_kernel<F>,
              dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), 3), dim3(32, 8), ia));
-  CowanArgs ca{};
-  ca.g = make_grid(r);
+  CowanArgs<F> ca{};
+  ca.g = make_grid<F>(r);
   for (int a = 0; a < 3; ++a) {
-    ca.e[a] = r->e[r->cur][a];
-    ca.lower[a] = r->lower[a];
-    ca.alpha[a] = r->coeff[a];
-    ca.beta[a] = r->coeff[3 + a];
+    ca.e[a] = static_cast<const F*>(r->e[r->cur][a]);
+    ca.lower[a] = static_cast<const F*>(r->lower[a]);
+    ca.alpha[a] = F(r->coeff[a]);
+    ca.beta[a] = F(r->coeff[3 + a]);
   }
-  ca.delta_xy = r->coeff[6];
-  ca.delta_yz = r->coeff[7];
-  ca.delta_zx = r->coeff[8];
+  ca.delta_xy = F(r->coeff[6]);
+  ca.delta_yz = F(r->coeff[7]);
+  ca.delta_zx = F(r->coeff[8]);
   ca.mx = r->mprof[0].view();
   ca.my = r->mprof[1].view();
-  for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
+  for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view<F>();
   // 32x8 column tiles, 16-plane z chunks (kTX, kTY, kKChunk in fields.cu).
   const dim3 cblock(32, 8);
   const dim3 cgrid(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), blocks_for(c.nz + 1, 16));
-  TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel, cgrid, cblock, ca));
+  TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel<F>, cgrid, cblock, ca));
   r->stage = 1;
   return APRL_OK;
 }
 
-aprl_status do_preview_electric(aprl_run* r) {
+aprl_status do_advance_magnetic(aprl_run* r) {
+  return r->fp32 ? advance_magnetic_t<float>(r) : advance_magnetic_t<double>(r);
+}
+
+template <class F>
+aprl_status preview_electric_t(aprl_run* r) {
   if (r->stage != 1) return fail(APRL_ERR_RUNTIME, "Moving-window electric phase mismatch");
   const aprl_run_config& c = r->cfg;
-  PreviewArgs pa{};
-  pa.g = make_grid(r);
+  PreviewArgs<F> pa{};
+  pa.g = make_grid<F>(r);
   pa.ex_prof = r->eprof[0].view();
   pa.ey_prof = r->eprof[1].view();
-  for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view();
+  for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view<F>();
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
-  TRY(launch(r, kElectricPreview, electric_preview_kernel, grid3(c, block), block, pa));
+  TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
   if (r->np)
     CUDA_TRY(cudaMemcpyAsync(r->slot_order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice,
                              r->stream));
@@ -834,15 +904,20 @@ aprl_status do_preview_electric(aprl_run* r) {
   return APRL_OK;
 }
 
-aprl_status do_trial(aprl_run* r, double residual[4]) {
+aprl_status do_preview_electric(aprl_run* r) {
+  return r->fp32 ? preview_electric_t<float>(r) : preview_electric_t<double>(r);
+}
+
+template <class F>
+aprl_status trial_t(aprl_run* r, double residual[4]) {
   if (r->stage != 2 && r->stage != 3)
     return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
   const aprl_run_config& c = r->cfg;
   for (int a = 0; a < 3; ++a)
-    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream));
+    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
   CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
   CUDA_TRY(cudaMemsetAsync(r->d_sums, 0, sizeof(ResidualSums), r->stream));
-  const DGrid g = make_grid(r);
+  const GridT<F> g = make_grid<F>(r);
   const DRegion region = make_region(r);
   if (r->queue.extracted) {
     // Frozen source support of the entries due within min(8, horizon) steps.
@@ -851,7 +926,7 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     const uint64_t until = r->step + std::min<uint64_t>(8, room);
     const size_t end = q.offsets[until - q.initial_step + 1];
     if (end > q.cursor) {
-      SupportArgs sa{};
+      SupportArgs<F> sa{};
       sa.g = g;
       sa.shape = c.shape;
       sa.src = q.d;
@@ -860,12 +935,12 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
       sa.steps = r->step - q.initial_step;
       sa.held_distance_per_beta = held_distance_per_beta(c);
       sa.status = r->d_status;
-      TRY(launch(r, kFrozenSupport, frozen_support_kernel, dim3(blocks_for(end - q.cursor, 128)),
+      TRY(launch(r, kFrozenSupport, frozen_support_kernel<F>, dim3(blocks_for(end - q.cursor, 128)),
                  dim3(128), sa));
     }
   }
   if (r->nc) {
-    CarrierArgs ca{};
+    CarrierArgs<F> ca{};
     ca.g = g;
     ca.region = region;
     ca.shape = c.shape;
@@ -875,10 +950,10 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     ca.keep = r->c_keep;
     ca.counters = r->d_counters;
     ca.status = r->d_status;
-    TRY(launch(r, kCarrier, carrier_kernel, dim3(blocks_for(r->nc, 128)), dim3(128), ca));
+    TRY(launch(r, kCarrier, carrier_kernel<F>, dim3(blocks_for(r->nc, 128)), dim3(128), ca));
   }
   if (r->np) {
-    PushArgs pa{};
+    PushArgs<F> pa{};
     pa.g = g;
     pa.frame = make_frame(c);
     pa.region = region;
@@ -921,10 +996,11 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     pa.counters = r->d_counters;
     pa.status = r->d_status;
     if (r->trials == 0)
-      TRY(launch(r, kGuessGather, guess_gather_kernel, dim3(blocks_for(r->np, 128)), dim3(128),
-                 pa));
-    TRY(launch(r, kPushDeposit, push_deposit_kernel, dim3(blocks_for(r->np, 128)), dim3(128), pa));
-    ResidualArgs ra{};
+      TRY(launch(r, kGuessGather, guess_gather_kernel<F>, dim3(blocks_for(r->np, 128)),
+                 dim3(128), pa));
+    TRY(launch(r, kPushDeposit, push_deposit_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128),
+               pa));
+    ResidualArgs<F> ra{};
     ra.g = g;
     ra.shape = c.shape;
     ra.count = (long long)r->np;
@@ -938,7 +1014,7 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
     ra.abs_grid_work = r->abs_work;
     ra.sums = r->d_sums;
     ra.status = r->d_status;
-    TRY(launch(r, kResidual, residual_kernel, dim3(blocks_for(r->np, 128)), dim3(128), ra));
+    TRY(launch(r, kResidual, residual_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
   CUDA_TRY(cudaMemcpyAsync(r->h_sums, r->d_sums, sizeof(ResidualSums), cudaMemcpyDeviceToHost,
                            r->stream));
@@ -955,12 +1031,20 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
   return APRL_OK;
 }
 
+aprl_status do_trial(aprl_run* r, double residual[4]) {
+  return r->fp32 ? trial_t<float>(r, residual) : trial_t<double>(r, residual);
+}
+
 aprl_status do_commit(aprl_run* r) {
   if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
   const aprl_run_config& c = r->cfg;
-  const DGrid g = make_grid(r);
   const dim3 block(32, 4);
-  TRY(launch(r, kElectricCommit, electric_commit_kernel, grid3(c, block), block, g));
+  if (r->fp32)
+    TRY(launch(r, kElectricCommit, electric_commit_kernel<float>, grid3(c, block), block,
+               make_grid<float>(r)));
+  else
+    TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
+               make_grid<double>(r)));
   r->cur = 1 - r->cur;
   // Counters of the converged trial become cumulative.
   CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
@@ -1007,6 +1091,25 @@ aprl_status do_commit(aprl_run* r) {
   return APRL_OK;
 }
 
+// MovingWindowFields::shift plane insertion on the ring (field type F).
+template <class F>
+aprl_status shift_insert_t(aprl_run* r) {
+  const aprl_run_config& c = r->cfg;
+  ShiftArgs<F> sa{};
+  sa.g = make_grid<F>(r);
+  TRY(inlet_table(r, r->offset, r->step, sa.inlet));
+  for (int h = 0; h < 8; ++h) {
+    sa.h[h] = r->hist[h].view<F>();
+    const int comp = r->hist[h].component;
+    sa.history_base[h] = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
+  }
+  int max_row = (int)std::max(c.nx, c.ny) + 1, max_slots = 1;
+  for (int h = 0; h < 8; ++h) max_slots = std::max(max_slots, r->hist[h].slots);
+  const int ydim = std::max(max_slots, (int)c.ny + 1);
+  return launch(r, kShiftInsert, shift_insert_kernel<F>,
+                dim3(blocks_for(max_row, 32), blocks_for(ydim, 8), 14), dim3(32, 8), sa);
+}
+
 aprl_status do_shift(aprl_run* r) {
   if (r->stage != 4)
     return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
@@ -1019,19 +1122,7 @@ aprl_status do_shift(aprl_run* r) {
     r->zb_e[a] = (r->zb_e[a] + nze - 1) % nze;
     r->zb_b[a] = (r->zb_b[a] + nzb - 1) % nzb;
   }
-  ShiftArgs sa{};
-  sa.g = make_grid(r);
-  TRY(inlet_table(r, r->offset, r->step, sa.inlet));
-  for (int h = 0; h < 8; ++h) {
-    sa.h[h] = r->hist[h].view();
-    const int comp = r->hist[h].component;
-    sa.history_base[h] = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
-  }
-  int max_row = (int)std::max(c.nx, c.ny) + 1, max_slots = 1;
-  for (int h = 0; h < 8; ++h) max_slots = std::max(max_slots, r->hist[h].slots);
-  const int ydim = std::max(max_slots, (int)c.ny + 1);
-  TRY(launch(r, kShiftInsert, shift_insert_kernel,
-             dim3(blocks_for(max_row, 32), blocks_for(ydim, 8), 14), dim3(32, 8), sa));
+  TRY(r->fp32 ? shift_insert_t<float>(r) : shift_insert_t<double>(r));
   r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
   if (r->np)
     TRY(launch(r, kInletCheck, inlet_check_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
@@ -1121,17 +1212,20 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
   };
   if (s != APRL_OK) return cleanup(s);
   const aprl_run_config& c = *config;
+  r->fp32 = c.precision == APRL_PRECISION_FP32_MIXED;
+  r->fes = r->fp32 ? sizeof(float) : sizeof(double);
+  const size_t fes = r->fes;
   for (int a = 0; a < 3; ++a) {
     for (int k = 0; k < 2; ++k) {
-      if ((s = device_alloc(&r->e[k][a], e_count(c, a))) != APRL_OK) return cleanup(s);
-      cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * 8, r->stream);
+      if ((s = device_alloc_bytes(&r->e[k][a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
+      cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * fes, r->stream);
     }
-    if ((s = device_alloc(&r->b[a], b_count(c, a))) != APRL_OK) return cleanup(s);
-    cudaMemsetAsync(r->b[a], 0, b_count(c, a) * 8, r->stream);
-    if ((s = device_alloc(&r->jc[a], e_count(c, a))) != APRL_OK) return cleanup(s);
-    cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * 8, r->stream);
+    if ((s = device_alloc_bytes(&r->b[a], b_count(c, a) * fes)) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(r->b[a], 0, b_count(c, a) * fes, r->stream);
+    if ((s = device_alloc_bytes(&r->jc[a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * fes, r->stream);
     const size_t plane = (size_t)(c.nx + (a != 0)) * (c.ny + (a != 1));
-    if ((s = device_alloc(&r->lower[a], plane)) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc_bytes(&r->lower[a], plane * fes)) != APRL_OK) return cleanup(s);
     r->max_rate[a] = maximum_rate(c, a);
   }
   // CPML profiles (x, y) for magnetic (half-integer) and electric nodes.
@@ -1165,8 +1259,8 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     hb.slots = prof.active;
     hb.layers = (int)sh[2];
     hb.row = (int)(der == 0 ? sh[1] : sh[0]);
-    if ((s = device_alloc(&hb.data, hb.length())) != APRL_OK) return cleanup(s);
-    cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * 8, r->stream);
+    if ((s = device_alloc_bytes(&hb.data, hb.length() * fes)) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * fes, r->stream);
   }
   for (int a = 0; a < 3; ++a) {
     const uint64_t cells = a == 0 ? c.nx : (a == 1 ? c.ny : c.nz);
@@ -1758,8 +1852,7 @@ aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double*
     else if (lattice >= static_cast<double>(size - 1)) { *lower = (int)size - 2; *fraction = 1.0; }
     else { *lower = (int)std::floor(lattice); *fraction = lattice - static_cast<double>(*lower); }
   };
-  DetectorArgs da{};
-  da.g = make_grid(r);
+  DetectorArgs<double> da{};
   da.frame = make_frame(c);
   da.origin_xy[0] = c.reference_origin[0];
   da.origin_xy[1] = c.reference_origin[1];
@@ -1771,8 +1864,13 @@ aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double*
     r->detector_cap = count;
   }
   da.out = r->d_detector;
-  TRY(launch(r, kDetectorPlane, detector_plane_kernel,
-             dim3(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), dim3(32, 8), da));
+  const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
+  if (r->fp32)
+    TRY(launch(r, kDetectorPlane, detector_plane_kernel<float>, grid, block,
+               retyped<float>(da, make_grid<float>(r))));
+  else
+    TRY(launch(r, kDetectorPlane, detector_plane_kernel<double>, grid, block,
+               retyped<double>(da, make_grid<double>(r))));
   CUDA_TRY(cudaMemcpyAsync(out, r->d_detector, count * 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;
@@ -1878,8 +1976,7 @@ aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* r, double plane_lab_z,
     else if (lattice >= static_cast<double>(size - 1)) { *lower = (int)size - 2; *fraction = 1.0; }
     else { *lower = (int)std::floor(lattice); *fraction = lattice - static_cast<double>(*lower); }
   };
-  DetectorArgs da{};
-  da.g = make_grid(r);
+  DetectorArgs<double> da{};
   da.frame = make_frame(c);
   da.origin_xy[0] = c.reference_origin[0];
   da.origin_xy[1] = c.reference_origin[1];
@@ -1888,7 +1985,12 @@ aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* r, double plane_lab_z,
   da.out = scratch;
   // A direct launch: no timing events are created on this path.
   const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
-  detector_plane_kernel<<<grid, block, 0, r->stream>>>(da);
+  if (r->fp32)
+    detector_plane_kernel<float><<<grid, block, 0, r->stream>>>(
+        retyped<float>(da, make_grid<float>(r)));
+  else
+    detector_plane_kernel<double><<<grid, block, 0, r->stream>>>(
+        retyped<double>(da, make_grid<double>(r)));
   CUDA_TRY(cudaGetLastError());
   ++r->kernel_launches[kDetectorPlane];
   ++r->launches;

@@ -45,6 +45,9 @@ def parse_args(argv=None):
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--particles", type=int, default=1_000_000)
     p.add_argument("--shape", default="linear-binomial3")
+    p.add_argument("--precision", choices=["fp64", "fp32-mixed"], default="fp64")
+    p.add_argument("--no-fp32-arm", action="store_true",
+                   help="skip the FP32-mixed comparison pass of an FP64 run")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     return p.parse_args(argv)
@@ -153,7 +156,7 @@ def run_ours(args):
     K, W = args.steps, args.warmup
     total_steps = W + 2 * K + 4
     w = workloads.dipole_c2(steps=total_steps, particles=args.particles, shape=args.shape,
-                            seed=17 + rank)
+                            seed=17 + rank, precision=args.precision)
     cfg = w.config
     lib = native.load()
     run = native.Run(lib, cfg, stream=stream.cuda_stream)
@@ -224,6 +227,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_stop)
     e2e_wall_ms = (time.perf_counter() - wall0) * 1e3
+    fp32_arm = None
+    if args.precision == "fp64" and not args.no_fp32_arm:
+        fp32_arm = time_fp32_arm(args, w, stream, run, detector_lab_z, world)
 
     # max over ranks, totals over ranks
     vals = torch.tensor([elapsed_ms, e2e_ms, float(particle_steps), float(e2e_particle_steps)],
@@ -265,11 +271,13 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "particle-steps/s",
         "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": elapsed_ms / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded Gaussian bunch, analytic inlet reference)",
         "config": {"workload": w.name, "cells": [cfg.nx, cfg.ny, cfg.nz],
                    "particles": args.particles, "shape": args.shape,
-                   "precision": "fp64-drop-in", "magnet": "uniform 1 T lab dipole",
+                   "precision": "fp64-drop-in" if args.precision == "fp64" else "fp32-mixed",
+                   "magnet": "uniform 1 T lab dipole",
                    "boost_gamma": cfg.boost_gamma, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (fields + particles > 126 MB)"},
         "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
@@ -285,9 +293,62 @@ def run_ours(args):
         "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
                    "reasons": clocks.get("reasons", [])},
     }
+    if fp32_arm:
+        line["fp32_mixed"] = fp32_arm
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
+
+
+def time_fp32_arm(args, w, stream, fp64_run, detector_lab_z, world):
+    """The same workload in the FP32-mixed mode: W warm-up and K timed steps
+    (CUDA events, inputs resident), then untimed steps up to the FP64 run's
+    step, where the lab detector planes of the two runs are compared."""
+    import torch
+    import torch.distributed as dist
+    K, W = args.steps, args.warmup
+    cfg = workloads.with_precision(w.config, "fp32-mixed")
+    run = native.Run(native.load(), cfg, stream=stream.cuda_stream)
+    run.set_reference(w.reference)
+    run.set_particles(w.particles)
+    for _ in range(W):
+        run.step(1)
+    run.synchronize()
+    run.b("run_reset_iteration_stats", run.handle)
+    particle_steps = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(K):
+        particle_steps += run.particle_count()
+        run.step(1)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    stats = run.stats()
+    vals = torch.tensor([ms, float(particle_steps)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = vals.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = vals.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, particle_steps = mx[0].item(), int(sm[1].item())
+    while run.stats()["step"] < fp64_run.stats()["step"]:
+        run.step(1)
+    mixed = run.sample_field_plane(detector_lab_z).reshape(-1, 6)
+    exact = fp64_run.sample_field_plane(detector_lab_z).reshape(-1, 6)
+    err = [float(np.linalg.norm(mixed[:, s] - exact[:, s]) / max(np.linalg.norm(exact[:, s]), 1e-300))
+           for s in (slice(0, 3), slice(3, 6))]
+    run.close()
+    return {"value": particle_steps / (ms * 1e-3), "unit": "particle-steps/s",
+            "ms_per_step": ms / K,
+            "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
+                                   "max": stats["max_iterations"]},
+            "tolerances": {"force": cfg.force_tolerance, "work": cfg.work_tolerance},
+            "detector_rel_l2_vs_fp64": {"E": err[0], "B": err[1],
+                                        "step": int(fp64_run.stats()["step"])}}
 
 
 # ---------------------------------------------------------------------------

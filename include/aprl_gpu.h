@@ -53,6 +53,18 @@ typedef enum {
   APRL_SHAPE_QUINTIC_COMPENSATED = 1
 } aprl_shape;
 
+/* Arithmetic of a run.  FP64 is the drop-in: every stage in binary64 with
+ * the reference's operation order.  FP32_MIXED stores and updates the fields,
+ * J, the CPML histories and the shape-weight walkers (gather and deposit) in
+ * binary32, evaluating the weights from binary64 cell-relative offsets;
+ * particle positions and momenta, the Lapenta-Markidis push, the boundary
+ * events, the window bookkeeping and the residual reductions stay binary64.
+ * The reference is binary64 only; this mode has no counterpart there. */
+typedef enum {
+  APRL_PRECISION_FP64 = 0,
+  APRL_PRECISION_FP32_MIXED = 1
+} aprl_precision;
+
 /* SIMagnetType (src/eb_sources.h:97-102). */
 typedef enum {
   APRL_MAGNET_PLANAR_UNDULATOR = 0,
@@ -100,7 +112,7 @@ typedef struct {
   int32_t shape;                  /* aprl_shape */
   uint32_t substeps;              /* particleSubsteps_ (src/simulation.cpp:2623-2685) */
   uint32_t max_trials;            /* 64 (src/simulation_source_coupling.cpp:40) */
-  uint32_t reserved0;
+  uint32_t precision;             /* aprl_precision */
   double force_tolerance;         /* 1e-13 (src/simulation_source_coupling.cpp:50) */
   double work_tolerance;          /* 1e-8 */
   /* BoostFrameTransform (src/boostframe.h:8-17) */

@@ -796,6 +796,8 @@ static aprl_status validate_config(const aprl_run_config* g) {
 aprl_status oracle_run_create(const aprl_run_config* config, oracle_run** out) {
   aprl_status s = validate_config(config);
   if (s != APRL_OK) return s;
+  if (config->precision != APRL_PRECISION_FP64)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "The oracle computes in binary64 only");
   oracle_run* r = (oracle_run*)calloc(1, sizeof(oracle_run));
   r->cfg = *config;
   double co[12];
