@@ -164,3 +164,47 @@ def history_shape(config, index):
     slots = 2 * cells
     row = shape[1] if der == 0 else shape[0]
     return (slots, shape[2], row)
+
+
+# Parameter-scan server (aprl_scan_*).
+SCAN_QUEUED, SCAN_RUNNING, SCAN_DONE = 0, 1, 2
+
+
+class ScanConfig(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_uint64),
+                ("max_slots", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+_PD = C.POINTER(C.c_double)
+
+
+class ScanRequest(C.Structure):
+    _fields_ = [("config", RunConfig),
+                ("steps", C.c_uint64),
+                ("particles", C.c_size_t),
+                ("x", _PD), ("y", _PD), ("z", _PD),
+                ("ux", _PD), ("uy", _PD), ("uz", _PD),
+                ("charge", _PD), ("mass", _PD),
+                ("id", C.POINTER(C.c_uint64)),
+                ("frozen", C.POINTER(C.c_uint8)),
+                ("frozen_beta_z", _PD),
+                ("reference", _PD * 6),
+                ("detector_lab_z", C.c_double),
+                ("detector", _PD)]
+
+
+class ScanResult(C.Structure):
+    _fields_ = [("state", C.c_int32),
+                ("status", C.c_int32),
+                ("detector_inside", C.c_int32),
+                ("slot", C.c_int32),
+                ("footprint_bytes", C.c_uint64),
+                ("queued_ms", C.c_double),
+                ("run_ms", C.c_double),
+                ("total_ms", C.c_double),
+                ("submit_s", C.c_double),
+                ("start_s", C.c_double),
+                ("finish_s", C.c_double),
+                ("stats", StepStats),
+                ("message", C.c_char * 256)]

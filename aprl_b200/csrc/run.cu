@@ -1159,6 +1159,15 @@ HistoryBuffer* find_history(aprl_run* r, unsigned index) {
 
 }  // namespace
 
+// The calling thread's error message, for the other host files of the
+// library (the scan server).
+namespace aprl_gpu {
+aprl_status report_error(aprl_status status, const char* message) {
+  g_error = message;
+  return status;
+}
+}  // namespace aprl_gpu
+
 // ===========================================================================
 extern "C" {
 

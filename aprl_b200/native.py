@@ -66,6 +66,12 @@ _PRODUCT_ONLY = {
     "run_reset_iteration_stats": (C.c_int, [_H]),
     "run_sample_field_plane_noalloc": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                                  C.POINTER(C.c_int)]),
+    "scan_footprint": (C.c_int, [C.POINTER(abi.RunConfig), C.c_size_t, _U64]),
+    "scan_create": (C.c_int, [C.POINTER(abi.ScanConfig), C.POINTER(C.c_void_p)]),
+    "scan_submit": (C.c_int, [C.c_void_p, C.POINTER(abi.ScanRequest), _U64]),
+    "scan_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double,
+                            C.POINTER(abi.ScanResult)]),
+    "scan_destroy": (C.c_int, [C.c_void_p]),
 }
 
 
@@ -353,3 +359,81 @@ class Run:
         n = C.c_uint64()
         self.b("run_launch_count", self.handle, C.byref(n))
         return n.value
+
+
+class Scan:
+    """A parameter-scan server (aprl_scan_*): independent runs admitted by
+    device footprint into `slots` concurrent streams of one GPU."""
+
+    def __init__(self, binding, budget_bytes=0, slots=4):
+        self.b = binding
+        cfg = abi.ScanConfig(int(budget_bytes), int(slots), 0)
+        handle = C.c_void_p()
+        binding("scan_create", C.byref(cfg), C.byref(handle))
+        self.handle = handle
+        self._inputs = {}
+
+    def footprint(self, config, particles):
+        out = C.c_uint64()
+        self.b("scan_footprint", C.byref(config), particles, C.byref(out))
+        return out.value
+
+    def submit(self, config, particles, steps, reference=None, held=None,
+               detector_lab_z=None):
+        """Queue one run; the arrays stay referenced until wait() returns it."""
+        keep = {}
+
+        def arr(a, dtype=np.float64):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            keep[len(keep)] = a
+            return a
+
+        q = abi.ScanRequest()
+        q.config = config
+        q.steps = int(steps)
+        n = int(np.asarray(particles["x"]).size)
+        q.particles = n
+        for name in ("x", "y", "z", "ux", "uy", "uz", "charge", "mass"):
+            setattr(q, name, _ptr(arr(particles[name])))
+        q.id = _ptr(arr(particles["id"], np.uint64), C.c_uint64)
+        if held is not None:
+            q.frozen = _ptr(arr(held[0], np.uint8), C.c_uint8)
+            q.frozen_beta_z = _ptr(arr(held[1]))
+        if reference is not None:
+            for a in range(6):
+                q.reference[a] = _ptr(arr(reference[a]))
+        detector = None
+        if detector_lab_z is not None:
+            detector = arr(np.full(6 * config.nx * config.ny, np.nan))
+            q.detector_lab_z = float(detector_lab_z)
+            q.detector = _ptr(detector)
+        ticket = C.c_uint64()
+        self.b("scan_submit", self.handle, C.byref(q), C.byref(ticket))
+        self._inputs[ticket.value] = (keep, detector)
+        return ticket.value
+
+    def wait(self, ticket, timeout=3600.0):
+        """The request's result as a dict (state, status, times, stats,
+        detector) once done, or its state when the timeout expired first."""
+        res = abi.ScanResult()
+        self.b("scan_wait", self.handle, ticket, float(timeout), C.byref(res))
+        out = {name: getattr(res, name) for name, _ in abi.ScanResult._fields_
+               if name not in ("stats", "message")}
+        out["message"] = res.message.decode(errors="replace")
+        if res.state == abi.SCAN_DONE:
+            out["stats"] = res.stats.as_dict()
+            _, detector = self._inputs.pop(ticket)
+            out["detector"] = detector if res.detector_inside else None
+        return out
+
+    def close(self):
+        if self.handle:
+            self.b("scan_destroy", self.handle)
+            self.handle = None
+            self._inputs.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

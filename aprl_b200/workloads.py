@@ -394,3 +394,43 @@ def small_case(nx=16, ny=16, nz=40, particles=400, steps=6,
                     synthetic_fields(cfg) if fields else [], steps=steps,
                     description={"cells": [nx, ny, nz], "particles": particles,
                                  "shape": shape})
+
+
+# ---------------------------------------------------------------------------
+# Batched ensemble and served scan: seeded draws of independent runs.
+def scan_draw(index, seed=2024, steps=500, precision="fp32-mixed",
+              shape="linear-binomial3", cells_min=(32, 32, 32), cells_max=(128, 128, 512),
+              particles_range=(1.0e4, 5.0e5)):
+    """Request `index` of a seeded parameter scan of drift/dipole runs: grid
+    extents uniform in [cells_min, cells_max], particle count log-uniform in
+    particles_range, lab dipole field uniform in [0, 1.5] T, bunch charge
+    uniform in [10, 200] pC, lab sigma_z uniform in [10, 50] um.  The inlet
+    is the vacuum (zero) reference.  Smallest useful extent: 2*(8+3)+2 cells
+    transversely (CPML plus particle margin)."""
+    rng = np.random.default_rng([seed, index])
+    nx = int(rng.integers(cells_min[0], cells_max[0] + 1))
+    ny = int(rng.integers(cells_min[1], cells_max[1] + 1))
+    nz = int(rng.integers(cells_min[2], cells_max[2] + 1))
+    lo, hi = math.log10(particles_range[0]), math.log10(particles_range[1])
+    particles = int(round(10.0 ** rng.uniform(lo, hi)))
+    bend = float(rng.uniform(0.0, 1.5))
+    charge = float(rng.uniform(10e-12, 200e-12))
+    sigma_z = float(rng.uniform(10e-6, 50e-6))
+    magnets = [dipole(bend)] if bend > 0.0 else []
+    cfg = with_precision(make_config(nx, ny, nz, 5e-6, 5e-6, 2e-6, 8, 10.0, shape, steps,
+                                     magnets=magnets), precision)
+    # sigma_xy is 50 um, narrowed on small grids to a quarter of the trusted
+    # transverse width so the bunch is not mostly truncated.
+    trusted = (min(nx, ny) - 2 * (8 + 3)) * 5e-6
+    sigma_xy = min(50e-6, 0.25 * trusted)
+    bunch = gaussian_bunch(cfg, particles, charge, 1e9, sigma_xy, sigma_z, 1e-6, 1e-4,
+                           seed=seed * 1000 + index)
+    return Workload(f"scan-{index}-{nx}x{ny}x{nz}", cfg, bunch, None, steps=steps,
+                    description={"cells": [nx, ny, nz], "particles": particles,
+                                 "dipole_T": bend, "charge_C": charge,
+                                 "sigma_z_m": sigma_z, "precision": precision})
+
+
+def detector_plane_lab_z(cfg, fraction=0.5):
+    """A fixed lab detector plane `fraction` of the way up the initial window."""
+    return cfg.lab_z_origin + cfg.boost_gamma * (fraction * cfg.nz * cfg.dz)

@@ -362,6 +362,73 @@ const char* aprl_kernel_name(unsigned kernel);
 /* Number of kernels this library launched on the run since creation. */
 aprl_status aprl_run_launch_count(const aprl_run* run, uint64_t* launches);
 
+/* ---------------------------------------------------------------------------
+ * Parameter-scan server.  The reference runs one simulation per MPI job; it
+ * has no counterpart of this.  A scan keeps independent runs (each an
+ * aprl_run) resident on one GPU and overlaps them: every request waits in a
+ * FIFO queue until a slot (a worker thread with its own CUDA stream) is free
+ * and its estimated device footprint fits the scan's memory budget next to
+ * the runs already on the device; requests that arrive while others run are
+ * admitted as slots and memory free up.  Each run's result is the result
+ * the same request gives alone, up to the order of the J atomics. */
+typedef struct aprl_scan aprl_scan;
+
+typedef struct {
+  uint64_t device_budget_bytes;   /* device memory the scan's runs may hold at
+                                     once; 0 = 90% of the free memory at create */
+  uint32_t max_slots;             /* runs in flight at once (1..256) */
+  uint32_t reserved;
+} aprl_scan_config;
+
+/* One run.  Every pointer is the caller's and must stay valid until the
+ * request has finished (aprl_scan_wait returned it done). */
+typedef struct {
+  aprl_run_config config;
+  uint64_t steps;                 /* coupled steps to run */
+  size_t particles;
+  const double *x, *y, *z, *ux, *uy, *uz, *charge, *mass;
+  const uint64_t* id;
+  const uint8_t* frozen;          /* optional held state (NULL: all active) */
+  const double* frozen_beta_z;
+  const double* reference[6];     /* inlet reference table per component;
+                                     NULL: the zero (vacuum) inlet */
+  double detector_lab_z;          /* lab plane sampled after the last step */
+  double* detector;               /* out: 6*nx*ny doubles, or NULL */
+} aprl_scan_request;
+
+enum { APRL_SCAN_QUEUED = 0, APRL_SCAN_RUNNING = 1, APRL_SCAN_DONE = 2 };
+
+typedef struct {
+  int32_t state;                  /* APRL_SCAN_* */
+  int32_t status;                 /* aprl_status of the finished run */
+  int32_t detector_inside;        /* the detector plane was inside the window */
+  int32_t slot;                   /* worker slot that ran it */
+  uint64_t footprint_bytes;       /* device memory reserved for it */
+  double queued_ms;               /* submit -> admission */
+  double run_ms;                  /* admission -> finish */
+  double total_ms;                /* submit -> finish (latency) */
+  double submit_s, start_s, finish_s;  /* steady-clock seconds since create */
+  aprl_step_stats stats;          /* of the finished run */
+  char message[256];              /* aprl_last_error of a failed run */
+} aprl_scan_result;
+
+/* Estimated device bytes of one run: fields, histories, the inlet table,
+ * particle and carrier storage. */
+aprl_status aprl_scan_footprint(const aprl_run_config* config, size_t particles,
+                                uint64_t* bytes);
+/* Creates the scan on the current device and starts its worker threads. */
+aprl_status aprl_scan_create(const aprl_scan_config* config, aprl_scan** out);
+/* Queues a request; a request larger than the whole budget is refused. */
+aprl_status aprl_scan_submit(aprl_scan* scan, const aprl_scan_request* request,
+                             uint64_t* ticket);
+/* Waits up to timeout_seconds (0: poll) for the request; *result holds its
+ * state and, once done, its outcome.  Returns APRL_OK whether or not it
+ * finished; a finished request is forgotten after it has been returned. */
+aprl_status aprl_scan_wait(aprl_scan* scan, uint64_t ticket, double timeout_seconds,
+                           aprl_scan_result* result);
+/* Finishes the queued and running requests, then stops the workers. */
+aprl_status aprl_scan_destroy(aprl_scan* scan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -885,8 +885,8 @@ aprl_status oracle_run_set_reference(oracle_run* r, unsigned a, const double* ho
   const size_t n = r->ref[a].nx * r->ref[a].ny * r->ref[a].nz;
   if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
   free(r->ref[a].v);
-  r->ref[a].v = (double*)malloc(n * sizeof(double));
-  memcpy(r->ref[a].v, host, n * sizeof(double));
+  r->ref[a].v = (double*)calloc(n ? n : 1, sizeof(double));
+  if (host) memcpy(r->ref[a].v, host, n * sizeof(double)); /* NULL: the zero inlet */
   r->ref_set[a] = 1;
   return APRL_OK;
 }

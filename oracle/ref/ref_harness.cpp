@@ -454,7 +454,8 @@ aprl_status ref_run_set_reference(ref_run* r, unsigned a, const double* host, si
   if (a >= 6) return failWith(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
   const auto& s = r->referenceShape[a];
   if (count != s[0] * s[1] * s[2]) return failWith(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
-  r->reference[a].assign(host, host + count);
+  if (host) r->reference[a].assign(host, host + count);
+  else r->reference[a].assign(count, 0.0);  // the zero inlet
   return APRL_OK;
 }
 
