@@ -49,6 +49,14 @@ def parse_args(argv=None):
     p.add_argument("--no-fp32-arm", action="store_true",
                    help="skip the FP32-mixed comparison pass of an FP64 run")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-scan", action="store_true",
+                   help="skip the batched-ensemble and served-scan measurements")
+    p.add_argument("--ensemble-runs", type=int, default=32)
+    p.add_argument("--ensemble-steps", type=int, default=100)
+    p.add_argument("--scan-requests", type=int, default=16)
+    p.add_argument("--scan-steps", type=int, default=500)
+    p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
+    p.add_argument("--scan-slots", type=int, default=12)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     return p.parse_args(argv)
 
@@ -295,6 +303,8 @@ def run_ours(args):
     }
     if fp32_arm:
         line["fp32_mixed"] = fp32_arm
+    if world == 1 and not args.no_scan:
+        line.update(scan_benchmarks(args))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
@@ -352,6 +362,103 @@ def time_fp32_arm(args, w, stream, fp64_run, detector_lab_z, world):
 
 
 # ---------------------------------------------------------------------------
+# Batched ensemble (64-run class) and served scan (Poisson arrivals): seeded
+# draws of independent drift/dipole runs (grid 32^3 .. 128x128x512, 1e4 ..
+# 5e5 particles log-uniform, 0 .. 1.5 T, 10 .. 200 pC, sigma_z 10 .. 50 um,
+# vacuum inlet).  The FP32-mixed form goes through the scan server; the
+# baseline is the plain FP64 drop-in path, one run at a time.  Times are host
+# wall clock around whole runs (each run ends with a device-to-host read of
+# its detector plane, so no device work is outstanding at the clock reads).
+def _rel_l2(a, b):
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _plain_fp64(lib, w, steps):
+    cfg = workloads.with_precision(w.config, "fp64")
+    run = native.Run(lib, cfg)
+    run.allocate_reference()
+    run.set_particles(w.particles)
+    run.step(steps)
+    det = run.sample_field_plane(workloads.detector_plane_lab_z(cfg))
+    run.close()
+    return det
+
+
+def _percentiles(values):
+    v = np.sort(np.asarray(values, dtype=np.float64))
+    return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))}
+
+
+def scan_benchmarks(args):
+    lib = native.load()
+    out = {}
+    # -- batched ensemble: every run submitted at once ---------------------
+    draws = [workloads.scan_draw(i, seed=4, steps=args.ensemble_steps, precision="fp32-mixed")
+             for i in range(args.ensemble_runs)]
+    t0 = time.perf_counter()
+    exact = [_plain_fp64(lib, w, args.ensemble_steps) for w in draws]
+    sequential_s = time.perf_counter() - t0
+    scan = native.Scan(lib, slots=args.scan_slots)
+    t0 = time.perf_counter()
+    tickets = [scan.submit(w.config, w.particles, args.ensemble_steps,
+                           detector_lab_z=workloads.detector_plane_lab_z(w.config))
+               for w in draws]
+    results = [scan.wait(t) for t in tickets]
+    batched_s = time.perf_counter() - t0
+    scan.close()
+    failed = [r["message"] for r in results if r["status"] != 0]
+    errors = [_rel_l2(r["detector"], e) for r, e in zip(results, exact)
+              if r["status"] == 0 and r["detector"] is not None and e is not None]
+    out["batched_ensemble"] = {
+        "runs": args.ensemble_runs, "steps": args.ensemble_steps, "slots": args.scan_slots,
+        "fp32_mixed_batched_solves_per_s": args.ensemble_runs / batched_s,
+        "fp64_sequential_solves_per_s": args.ensemble_runs / sequential_s,
+        "speedup": sequential_s / batched_s,
+        "detector_rel_l2_vs_fp64": {"max": max(errors) if errors else None,
+                                    "median": float(np.median(errors)) if errors else None},
+        "failed": failed[:3]}
+    # -- served scan: Poisson arrivals --------------------------------------
+    rng = np.random.default_rng(5)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.scan_rate, args.scan_requests))
+    reqs = [workloads.scan_draw(100 + i, seed=5, steps=args.scan_steps, precision="fp32-mixed")
+            for i in range(args.scan_requests)]
+
+    def serve(precision, slots):
+        scan = native.Scan(lib, slots=slots)
+        t_start = time.perf_counter()
+        tickets = []
+        for at, w in zip(arrivals, reqs):
+            delay = at - (time.perf_counter() - t_start)
+            if delay > 0:
+                time.sleep(delay)
+            cfg = workloads.with_precision(w.config, precision)
+            tickets.append(scan.submit(cfg, w.particles, args.scan_steps,
+                                       detector_lab_z=workloads.detector_plane_lab_z(cfg)))
+        res = [scan.wait(t) for t in tickets]
+        span = time.perf_counter() - t_start
+        scan.close()
+        return res, span
+
+    mixed, mixed_span = serve("fp32-mixed", args.scan_slots)
+    plain, plain_span = serve("fp64", 1)
+    errs = [_rel_l2(m["detector"], p["detector"]) for m, p in zip(mixed, plain)
+            if m["status"] == 0 and p["status"] == 0 and m["detector"] is not None]
+    out["served_scan"] = {
+        "requests": args.scan_requests, "steps": args.scan_steps,
+        "rate_req_per_s": args.scan_rate, "slots": args.scan_slots,
+        "fp32_mixed": {"solves_per_s": args.scan_requests / mixed_span,
+                       "latency_ms": _percentiles([r["total_ms"] for r in mixed]),
+                       "failed": sum(r["status"] != 0 for r in mixed)},
+        "fp64_sequential": {"solves_per_s": args.scan_requests / plain_span,
+                            "latency_ms": _percentiles([r["total_ms"] for r in plain]),
+                            "failed": sum(r["status"] != 0 for r in plain)},
+        "throughput_ratio": plain_span / mixed_span,
+        "detector_rel_l2_vs_fp64": {"max": max(errs) if errs else None},
+        "inlet": "vacuum (zero reference)"}
+    return out
+
+
 def reference_sample_workload(args, steps, seed=17):
     """A bounded slice of the benchmark workload for the CPU: the full
     transverse grid and 1/8 of the window length with 1/8 of the particles
