@@ -80,17 +80,18 @@ struct DFrame {  // BoostFrameTransform
   double lab_time_origin, lab_z_origin, box_z_origin;
 };
 
-// Everything the kernels need about the grid; passed by value.  F is the
-// field element type: double for the FP64 drop-in, float for the FP32-mixed
-// mode (geometry, origin and time stay binary64 in both).
+// Everything the kernels need about the grid; passed by value.  E and B are
+// binary64 in every mode.  F is the type of the current J and of the
+// particle-side weight arithmetic: double for the FP64 drop-in, float for
+// the FP32-mixed mode.
 template <class F>
 struct GridT {
   int nx, ny, nz;
   double dx, dy, dz, dt;
   double origin[3];      // localOriginBox_ of the current window
-  F* e_old[3];           // E^n  (ring)
-  F* e_star[3];          // E*   (ring)
-  F* b[3];               // B    (ring)
+  double* e_old[3];      // E^n  (ring)
+  double* e_star[3];     // E*   (ring)
+  double* b[3];          // B    (ring)
   F* j[3];               // J    (plain)
   int zb_e[3];           // ring bases of Ex Ey Ez
   int zb_b[3];           // ring bases of Bx By Bz
@@ -144,7 +145,7 @@ __device__ __forceinline__ bool current_mask(const GridT<F>& g, int c, int i, in
 // Trial candidate E* - dt/eps0 J at a native node (applyCurrentSource(-1)).
 template <class F>
 __device__ __forceinline__ F e_candidate(const GridT<F>& g, int c, int i, int j, int k) {
-  F v = g.e_star[c][e_index(g, c, i, j, k)];
+  F v = F(g.e_star[c][e_index(g, c, i, j, k)]);
   if (current_mask(g, c, i, j, k)) {
     const F jc = g.j[c][j_index(g, c, i, j, k)];
     if (jc != F(0.)) v += g.jcoef * jc;

@@ -3,11 +3,12 @@
 // electric correction, PEC termination and inlet overwrite, the commit
 // E^{n+1} = E* - dt/eps0 J, and the moving-window plane insertion.
 //
-// Every kernel is templated on the field element type F.  With F = double
-// (the FP64 drop-in) every expression keeps the reference's operation order
-// and the library is compiled without FMA contraction, so these kernels
-// reproduce the reference's translation units bit for bit; F = float is the
-// FP32-mixed mode (coefficients computed in binary64, then rounded once).
+// E, B and the CPML histories are binary64 in every mode, and every
+// expression keeps the reference's operation order; the library is compiled
+// without FMA contraction, so these kernels reproduce the reference's
+// translation units bit for bit.  The kernels are templated on the type F of
+// the current J (double, or float in the FP32-mixed mode), which only the
+// commit reads.
 #include "common.cuh"
 #include "fields.cuh"
 
@@ -17,9 +18,10 @@ namespace aprl_gpu {
 // PEC parity extension, z halo planes (lower = inlet reference plane,
 // upper = the last rank's zero plane).
 template <class F>
-__device__ __forceinline__ F electric_value(const CowanArgs<F>& a, int c, int i, int j, int k) {
+__device__ __forceinline__ double electric_value(const CowanArgs<F>& a, int c, int i, int j,
+                                                 int k) {
   const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1), nzc = a.g.nz + (c != 2);
-  F sign = F(1.0);
+  double sign = 1.0;
   if (i < 0) {
     if (c == 0) i = 0; else { i = -i; sign = -sign; }
   } else if (i >= nxc) {
@@ -31,22 +33,20 @@ __device__ __forceinline__ F electric_value(const CowanArgs<F>& a, int c, int i,
     if (c == 1) j = nyc - 1; else { j = 2 * (nyc - 1) - j; sign = -sign; }
   }
   if (k < 0) return sign * a.lower[c][(size_t)j * nxc + i];
-  if (k >= nzc) return sign * F(0.0);
+  if (k >= nzc) return sign * 0.0;
   return sign * a.e[c][((size_t)ring(k, a.g.zb_e[c], nzc) * nyc + j) * nxc + i];
 }
 
 // transformedCorrection (src/eb_cpml.cpp:131-138).
-template <class F>
-__device__ __forceinline__ F cpml_correction(const CpmlAxis& ax, int index, F difference,
-                                             F* history) {
-  const F psi = F(ax.decay[index]) * *history + F(ax.drive[index]) * difference;
+__device__ __forceinline__ double cpml_correction(const CpmlAxis& ax, int index,
+                                                  double difference, double* history) {
+  const double psi = ax.decay[index] * *history + ax.drive[index] * difference;
   *history = psi;
-  return F(ax.inverse_kappa_minus_one[index]) * difference + psi;
+  return ax.inverse_kappa_minus_one[index] * difference + psi;
 }
 
-template <class F>
-__device__ __forceinline__ F* history_at(const CpmlHistoryT<F>& h, int slot, int k, int zbase,
-                                         int row_index) {
+__device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, int k, int zbase,
+                                              int row_index) {
   return h.data + ((size_t)slot * h.layers + ring(k, zbase, h.layers)) * h.row + row_index;
 }
 
@@ -65,26 +65,24 @@ __device__ __forceinline__ F* history_at(const CpmlHistoryT<F>& h, int slot, int
 // (1,2,0), (2,1,0), (2,0,1), reusing the curl's smoothed difference.
 constexpr int kTX = 32, kTY = 8, kKChunk = 16;
 
-template <class F>
 struct ETile {
-  F v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
+  double v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
 };
 
 __device__ __forceinline__ int plane_slot(int k) { return ((k % 3) + 3) % 3; }
 
-template <class F>
-__device__ __forceinline__ F tile_at(const ETile<F>& t, int c, int i, int j, int k, int i0,
-                                     int j0) {
+__device__ __forceinline__ double tile_at(const ETile& t, int c, int i, int j, int k, int i0,
+                                          int j0) {
   return t.v[c][plane_slot(k)][j - j0 + 1][i - i0 + 1];
 }
 
 template <class F>
-__device__ __forceinline__ F tile_smoothed(const ETile<F>& t, const CowanArgs<F>& a, int c,
-                                           int d, int i, int j, int k, int i0, int j0) {
+__device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs<F>& a, int c,
+                                                int d, int i, int j, int k, int i0, int j0) {
   const int ta = (d + 1) % 3, tb = (d + 2) % 3;
-  const F delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
+  const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
   const int p[3] = {i, j, k};
-  F result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
+  double result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
 #pragma unroll
   for (int dir = -1; dir <= 1; dir += 2) {
     int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
@@ -110,7 +108,7 @@ __device__ __forceinline__ F tile_smoothed(const ETile<F>& t, const CowanArgs<F>
 // own reach); tile points farther out, which exist only where a small grid
 // ends inside a tile, are stored as zero and never used.
 template <class F>
-__device__ __forceinline__ void load_plane(ETile<F>& t, const CowanArgs<F>& a, int k, int i0,
+__device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int k, int i0,
                                            int j0) {
   const int slot = plane_slot(k);
   constexpr int W = kTX + 2, H = kTY + 2, N = W * H;
@@ -120,20 +118,20 @@ __device__ __forceinline__ void load_plane(ETile<F>& t, const CowanArgs<F>& a, i
       const int ii = n % W, jj = n / W;
       const int i = i0 - 1 + ii, j = j0 - 1 + jj;
       t.v[c][slot][jj][ii] = (i < -1 || i > nxc || j < -1 || j > nyc)
-                                 ? F(0.0) : electric_value(a, c, i, j, k);
+                                 ? 0.0 : electric_value(a, c, i, j, k);
     }
   }
 }
 
 template <class F>
 __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> a) {
-  __shared__ ETile<F> t;
+  __shared__ ETile t;
   const GridT<F>& g = a.g;
   const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
   const int k0 = blockIdx.z * kKChunk;
   const int k1 = min(k0 + kKChunk, g.nz + 1);
-  const F dtdx = F(g.dt / g.dx), dtdy = F(g.dt / g.dy), dtdz = F(g.dt / g.dz);
+  const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
   load_plane(t, a, k0 - 1, i0, j0);
   load_plane(t, a, k0, i0, j0);
   for (int k = k0; k < k1; ++k) {
@@ -141,45 +139,45 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
     __syncthreads();
     if (i <= g.nx && j <= g.ny) {
       if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
-        const F dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
+        const double dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
                              tile_smoothed(t, a, 2, 1, i, j, k, i0, j0);
-        const F dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
+        const double dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
                              tile_smoothed(t, a, 1, 2, i, j, k, i0, j0);
-        F* bx = &g.b[0][b_index(g, 0, i, j, k)];
-        F v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
+        double* bx = &g.b[0][b_index(g, 0, i, j, k)];
+        double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
         const int s = a.my.ordinal[j];
         if (s >= 0)
-          v += F(-1.0) * dtdy * cpml_correction(a.my, j, dEzDy,
+          v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
                                              history_at(a.h[0], s, k, g.zb_b[0], i));
         *bx = v;
       }
       if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
-        const F dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
+        const double dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
                              tile_smoothed(t, a, 0, 2, i, j, k, i0, j0);
-        const F dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
+        const double dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
                              tile_smoothed(t, a, 2, 0, i, j, k, i0, j0);
-        F* by = &g.b[1][b_index(g, 1, i, j, k)];
-        F v = *by - (dtdz * dExDz - dtdx * dEzDx);
+        double* by = &g.b[1][b_index(g, 1, i, j, k)];
+        double v = *by - (dtdz * dExDz - dtdx * dEzDx);
         const int s = a.mx.ordinal[i];
         if (s >= 0)
-          v += F(1.0) * dtdx * cpml_correction(a.mx, i, dEzDx,
+          v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
                                             history_at(a.h[1], s, k, g.zb_b[1], j));
         *by = v;
       }
       if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
-        const F dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
+        const double dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
                              tile_smoothed(t, a, 1, 0, i, j, k, i0, j0);
-        const F dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
+        const double dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
                              tile_smoothed(t, a, 0, 1, i, j, k, i0, j0);
-        F* bz = &g.b[2][b_index(g, 2, i, j, k)];
-        F v = *bz - (dtdx * dEyDx - dtdy * dExDy);
+        double* bz = &g.b[2][b_index(g, 2, i, j, k)];
+        double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
         const int sx = a.mx.ordinal[i];
         if (sx >= 0)
-          v += F(-1.0) * dtdx * cpml_correction(a.mx, i, dEyDx,
+          v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,
                                              history_at(a.h[2], sx, k, g.zb_b[2], j));
         const int sy = a.my.ordinal[j];
         if (sy >= 0)
-          v += F(1.0) * dtdy * cpml_correction(a.my, j, dExDy,
+          v += 1.0 * dtdy * cpml_correction(a.my, j, dExDy,
                                             history_at(a.h[3], sy, k, g.zb_b[2], i));
         *bz = v;
       }
@@ -189,7 +187,7 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
 }
 
 template <class F>
-__device__ __forceinline__ F bval(const GridT<F>& g, int c, int i, int j, int k) {
+__device__ __forceinline__ double bval(const GridT<F>& g, int c, int i, int j, int k) {
   return g.b[c][b_index(g, c, i, j, k)];
 }
 
@@ -207,46 +205,46 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
   const GridT<F>& g = a.g;
   if (i > g.nx || j > g.ny || k > g.nz) return;
   const double curl = g.dt / (kMu0 * kEpsilon0);
-  const F cx = F(curl / g.dx), cy = F(curl / g.dy), cz = F(curl / g.dz);
+  const double cx = curl / g.dx, cy = curl / g.dy, cz = curl / g.dz;
   if (i < g.nx) {  // Ex (nx, ny+1, nz+1)
     const size_t n = e_index(g, 0, i, j, k);
-    F v = g.e_old[0][n];
+    double v = g.e_old[0][n];
     if (k >= 1 && k < g.nz && j >= 1 && j < g.ny)
       v += cy * (bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k)) -
            cz * (bval(g, 1, i, j, k) - bval(g, 1, i, j, k - 1));
     if (j >= 1 && j < g.ny) {
       const int s = a.ey_prof.ordinal[j];
       if (s >= 0) {
-        const F diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
-        v += F(1.0) * cy * cpml_correction(a.ey_prof, j, diff,
+        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
+        v += 1.0 * cy * cpml_correction(a.ey_prof, j, diff,
                                         history_at(a.h[0], s, k, g.zb_e[0], i));
       }
     }
-    if (j == 0 || j == g.ny) v = F(0.0);
-    if (k == 0) v = F(inlet_value(a.inlet, 0, i, j));
+    if (j == 0 || j == g.ny) v = 0.0;
+    if (k == 0) v = inlet_value(a.inlet, 0, i, j);
     g.e_star[0][n] = v;
   }
   if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
     const size_t n = e_index(g, 1, i, j, k);
-    F v = g.e_old[1][n];
+    double v = g.e_old[1][n];
     if (k >= 1 && k < g.nz && i >= 1 && i < g.nx)
       v += cz * (bval(g, 0, i, j, k) - bval(g, 0, i, j, k - 1)) -
            cx * (bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k));
     if (i >= 1 && i < g.nx) {
       const int s = a.ex_prof.ordinal[i];
       if (s >= 0) {
-        const F diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
-        v += F(-1.0) * cx * cpml_correction(a.ex_prof, i, diff,
+        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
+        v += -1.0 * cx * cpml_correction(a.ex_prof, i, diff,
                                          history_at(a.h[1], s, k, g.zb_e[1], j));
       }
     }
-    if (i == 0 || i == g.nx) v = F(0.0);
-    if (k == 0) v = F(inlet_value(a.inlet, 1, i, j));
+    if (i == 0 || i == g.nx) v = 0.0;
+    if (k == 0) v = inlet_value(a.inlet, 1, i, j);
     g.e_star[1][n] = v;
   }
   if (k < g.nz) {  // Ez (nx+1, ny+1, nz)
     const size_t n = e_index(g, 2, i, j, k);
-    F v = g.e_old[2][n];
+    double v = g.e_old[2][n];
     const bool inner = i >= 1 && i < g.nx && j >= 1 && j < g.ny;
     if (inner)
       v += cx * (bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k)) -
@@ -254,18 +252,18 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
     if (inner) {
       const int sx = a.ex_prof.ordinal[i];
       if (sx >= 0) {
-        const F diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
-        v += F(1.0) * cx * cpml_correction(a.ex_prof, i, diff,
+        const double diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
+        v += 1.0 * cx * cpml_correction(a.ex_prof, i, diff,
                                         history_at(a.h[2], sx, k, g.zb_e[2], j));
       }
       const int sy = a.ey_prof.ordinal[j];
       if (sy >= 0) {
-        const F diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
-        v += F(-1.0) * cy * cpml_correction(a.ey_prof, j, diff,
+        const double diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
+        v += -1.0 * cy * cpml_correction(a.ey_prof, j, diff,
                                          history_at(a.h[3], sy, k, g.zb_e[2], i));
       }
     }
-    if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = F(0.0);
+    if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
     g.e_star[2][n] = v;
   }
 }
@@ -283,20 +281,25 @@ __global__ void electric_commit_kernel(GridT<F> g) {
     if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
     if (!current_mask(g, c, i, j, k)) continue;
     const F jc = g.j[c][j_index(g, c, i, j, k)];
-    if (jc != F(0.)) g.e_star[c][e_index(g, c, i, j, k)] += g.jcoef * jc;
+    if (jc != F(0.)) {
+      // binary64 J: g.jcoef is -dt/eps0 itself.  A binary32 J is widened and
+      // scaled by the binary64 coefficient.
+      const double jcoef =
+          sizeof(F) == sizeof(double) ? (double)g.jcoef : -1. * g.dt / kEpsilon0;
+      g.e_star[c][e_index(g, c, i, j, k)] += jcoef * (double)jc;
+    }
   }
 }
 
 // Boundary::begin lower halo planes (src/moving_window_fields.cpp:206-210):
 // reference(a, i, j, offset-1, step) for Ex, Ey, Ez.
-template <class F>
-__global__ void inlet_lower_kernel(InletPlaneArgs<F> a) {
+__global__ void inlet_lower_kernel(InletPlaneArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int c = blockIdx.z;
   const int nxc = a.nx + (c != 0), nyc = a.ny + (c != 1);
   if (i >= nxc || j >= nyc) return;
-  a.out[c][(size_t)j * nxc + i] = F(inlet_value(a.inlet, c, i, j));
+  a.out[c][(size_t)j * nxc + i] = inlet_value(a.inlet, c, i, j);
 }
 
 // MovingWindowFields::shift plane insertion (src/moving_window_fields.cpp:
@@ -312,18 +315,48 @@ __global__ void shift_insert_kernel(ShiftArgs<F> a) {
   if (c < 3) {
     const int nxc = e_nx(g, c), nyc = e_ny(g, c);
     if (i >= nxc || j >= nyc) return;
-    g.e_old[c][e_index(g, c, i, j, 0)] = F(inlet_value(a.inlet, c, i, j));
+    g.e_old[c][e_index(g, c, i, j, 0)] = inlet_value(a.inlet, c, i, j);
   } else if (c < 6) {
     const int b = c - 3;
     const int nxc = b_nx(g, b), nyc = b_ny(g, b);
     if (i >= nxc || j >= nyc) return;
-    g.b[b][b_index(g, b, i, j, 0)] = F(inlet_value(a.inlet, c, i, j));
+    g.b[b][b_index(g, b, i, j, 0)] = inlet_value(a.inlet, c, i, j);
   } else {
-    const CpmlHistoryT<F>& h = a.h[c - 6];
+    const CpmlHistory& h = a.h[c - 6];
     // i runs over the row, j over the slots.
     if (i >= h.row || j >= h.slots) return;
-    *history_at(h, j, 0, a.history_base[c - 6], i) = F(0.0);
+    *history_at(h, j, 0, a.history_base[c - 6], i) = 0.0;
   }
+}
+
+// The orbit sum the electric gathers read, one pass per trial:
+// S = E_new + E^n at every E node, with E_new = E* - dt/eps0 J on the
+// applyCurrentSource mask (with_current) or E* (the first-trial guess, before
+// any current).  In binary64 this is exactly the sum the orbit-averaged
+// gather forms node by node (Impl::electric, src/source_coupling.cpp:31-39),
+// so the gather is unchanged bit for bit; W = float rounds it once.
+template <class W>
+__global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_current) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  W* s[3] = {s0, s1, s2};
+  for (int c = 0; c < 3; ++c) {
+    if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
+    const size_t n = e_index(g, c, i, j, k);
+    double v = g.e_star[c][n];
+    if (with_current && current_mask(g, c, i, j, k)) {
+      const double jc = g.j[c][j_index(g, c, i, j, k)];
+      if (jc != 0.) v += g.jcoef * jc;
+    }
+    s[c][n] = W(v + g.e_old[c][n]);
+  }
+}
+
+// Binary32 copy of B (same ring layout) for the FP32-mixed gathers.
+__global__ void b_shadow_kernel(const double* b, float* out, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)b[i];
 }
 
 // Lab detector field plane (src/lab_detectors.cpp:39-99, 2836-2905).
@@ -360,8 +393,8 @@ __device__ double detector_component(const GridT<F>& g, int comp, double lx, dou
       for (int a = 0; a < 2; ++a) {
         const double wx = a ? xf : 1.0 - xf;
         const double wy = b ? yf : 1.0 - yf;
-        const double v = electric ? double(g.e_old[c][e_index(g, c, xl + a, yl + b, zl + cz)])
-                                  : double(g.b[c][b_index(g, c, xl + a, yl + b, zl + cz)]);
+        const double v = electric ? g.e_old[c][e_index(g, c, xl + a, yl + b, zl + cz)]
+                                  : g.b[c][b_index(g, c, xl + a, yl + b, zl + cz)];
         value += wx * wy * wz * v;
       }
   }
@@ -396,16 +429,16 @@ __global__ void detector_plane_kernel(DetectorArgs<F> a) {
   o[5] = bb[2];
 }
 
-// Both element types are built: FP64 drop-in and FP32-mixed.
+// Built for binary64 J (both modes of this library).
 #define APRL_FIELD_KERNELS(F)                                                  \
   template __global__ void cowan_magnetic_kernel<F>(CowanArgs<F>);            \
   template __global__ void electric_preview_kernel<F>(PreviewArgs<F>);        \
   template __global__ void electric_commit_kernel<F>(GridT<F>);               \
-  template __global__ void inlet_lower_kernel<F>(InletPlaneArgs<F>);          \
   template __global__ void shift_insert_kernel<F>(ShiftArgs<F>);              \
   template __global__ void detector_plane_kernel<F>(DetectorArgs<F>);
 APRL_FIELD_KERNELS(double)
-APRL_FIELD_KERNELS(float)
+template __global__ void orbit_sum_kernel<double>(GridT<double>, double*, double*, double*, int);
+template __global__ void orbit_sum_kernel<float>(GridT<double>, float*, float*, float*, int);
 #undef APRL_FIELD_KERNELS
 
 }  // namespace aprl_gpu

@@ -15,9 +15,8 @@ struct CpmlAxis {
 };
 
 // One active convolution history in [slot][k][row] order.
-template <class F>
-struct CpmlHistoryT {
-  F* data;
+struct CpmlHistory {
+  double* data;
   int slots, layers, row;
 };
 
@@ -40,29 +39,30 @@ __device__ __forceinline__ double inlet_value(const InletTable& t, int c, int i,
                                 t.fraction * t.table[c][(size_t)t.hi[c] * plane + cell];
 }
 
-// Argument blocks, templated on the field element type F (double or float).
+// Argument blocks.  E, B, the halo planes and the CPML histories are
+// binary64 in every mode; the template parameter F is the type of J (the
+// grid view GridT<F>), which only the commit reads.
 template <class F>
 struct CowanArgs {
   GridT<F> g;            // B (ring) is updated in place
-  const F* e[3];         // E^n (ring)
-  const F* lower[3];     // inlet lower halo planes
-  F alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
+  const double* e[3];    // E^n (ring)
+  const double* lower[3];  // inlet lower halo planes
+  double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
   CpmlAxis mx, my;       // magnetic profiles (half-integer positions)
-  CpmlHistoryT<F> h[4];  // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
+  CpmlHistory h[4];      // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
 };
 
 template <class F>
 struct PreviewArgs {
   GridT<F> g;            // e_old = E^n, e_star = E* (written)
   CpmlAxis ex_prof, ey_prof;  // electric profiles (integer positions)
-  CpmlHistoryT<F> h[4];  // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
+  CpmlHistory h[4];      // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
   InletTable inlet;      // reference(a, i, j, offset, step+1)
 };
 
-template <class F>
 struct InletPlaneArgs {
   int nx, ny;
-  F* out[3];
+  double* out[3];
   InletTable inlet;      // reference(a, i, j, offset-1, step)
 };
 
@@ -70,7 +70,7 @@ template <class F>
 struct ShiftArgs {
   GridT<F> g;            // e_old = the committed E (ring, bases already moved)
   InletTable inlet;      // reference(a, i, j, offset, step) after the shift
-  CpmlHistoryT<F> h[8];  // magnetic 0,3,4,5 then electric 6,9,10,11
+  CpmlHistory h[8];      // magnetic 0,3,4,5 then electric 6,9,10,11
   int history_base[8];
 };
 
@@ -87,8 +87,11 @@ struct DetectorArgs {
 template <class F> __global__ void cowan_magnetic_kernel(CowanArgs<F> a);
 template <class F> __global__ void electric_preview_kernel(PreviewArgs<F> a);
 template <class F> __global__ void electric_commit_kernel(GridT<F> g);
-template <class F> __global__ void inlet_lower_kernel(InletPlaneArgs<F> a);
+__global__ void inlet_lower_kernel(InletPlaneArgs a);
 template <class F> __global__ void shift_insert_kernel(ShiftArgs<F> a);
 template <class F> __global__ void detector_plane_kernel(DetectorArgs<F> a);
+template <class W>
+__global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_current);
+__global__ void b_shadow_kernel(const double* b, float* out, long long n);
 
 }  // namespace aprl_gpu

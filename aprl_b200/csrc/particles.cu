@@ -9,10 +9,12 @@
 // arithmetic matches the reference.  Deposition accumulates with atomics into
 // J; only the summation order of J differs from the reference.
 //
-// The walkers are templated on the field element type F.  Positions, chord
-// cuts and cell indices are always binary64; the weights are evaluated in F
-// from the cell-relative offsets, and the fields are read and accumulated in
-// F.  F = double is the FP64 drop-in, F = float the FP32-mixed mode.
+// The walkers are templated on the type F of J and of the weight
+// arithmetic.  Positions, chord cuts and cell indices are always binary64,
+// and so are the E and B arrays; the weights are evaluated in F from the
+// cell-relative offsets, the field values are rounded to F as they are read
+// and accumulated in F, and J is accumulated in F.  F = double is the FP64
+// drop-in, F = float the FP32-mixed mode.
 #include "common.cuh"
 #include "particles.cuh"
 
@@ -66,10 +68,11 @@ __device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) 
 }
 
 // binomialXZSegment (src/longitudinal_shape.h:61-94).
-template <class F, class V>
-__device__ __forceinline__ void binomial_xz_segment(const GridT<F>& g, const double s[3],
+template <class G, class V>
+__device__ __forceinline__ void binomial_xz_segment(const GridT<G>& g, const double s[3],
                                                     const double d[3], double first,
                                                     double last, V& visit) {
+  using F = typename V::Weight;
   const F width = F(last - first);
   const double mid = (first + last) * 0.5;
   const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
@@ -112,10 +115,11 @@ __device__ __forceinline__ void binomial_xz_segment(const GridT<F>& g, const dou
 
 // Four-point Gauss quadrature of the quintic-compensated shape over one cut
 // piece of the chord (the quintic branch of longitudinal_shape::weights).
-template <class F, class V>
-__device__ __forceinline__ void quintic_segment(const GridT<F>& g, const double x[3],
+template <class G, class V>
+__device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double x[3],
                                                 const double v[3], double lower,
                                                 double upper, double width, V& visit) {
+  using F = typename V::Weight;
   const double q[4] = {-.8611363115940525752, -.3399810435848562648,
                        .3399810435848562648, .8611363115940525752};
   const double qw[4] = {.3478548451374538574, .6521451548625461426,
@@ -258,35 +262,26 @@ __device__ __forceinline__ bool clip_open_orbit(const GridT<F>& g, const double 
   return true;
 }
 
-// Orbit average of 1/2 (E_new + E^n) with the shape weights.  with_current
-// selects E_new = E* - dt/eps0 J (residual) or E* (first-trial guess, when
-// the grid still holds the zero-current preview).
-template <class F>
+// Orbit average of 1/2 (E_new + E^n) with the shape weights, read from the
+// orbit sum S = E_new + E^n that orbit_sum_kernel forms once per trial
+// (E_new = E* - dt/eps0 J for the residual, E* for the first-trial guess).
+template <class W, class F>
 struct ElectricVisitor {
   static constexpr bool kF3Segment = true;
+  using Weight = W;
   const GridT<F>* g;
-  bool with_current;
-  F r[3];
-  __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k, F w) {
+  const W* const* s;     // orbit sum S = E_new + E^n per E node (ring layout)
+  W r[3];
+  __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k, W w) {
     const GridT<F>& G = *g;
     if (i < 0 || j < 0 || i >= e_nx(G, d) || j >= e_ny(G, d)) return;
     if (k < 0 || k >= e_nz(G, d)) return;
-    const int ii = (int)i, jj = (int)j, kk = (int)k;
-    const size_t n = e_index(G, d, ii, jj, kk);
-    const F vn = with_current ? e_candidate(G, d, ii, jj, kk) : G.e_star[d][n];
-    r[d] += F(.5) * w * (vn + G.e_old[d][n]);
+    r[d] += W(.5) * w * s[d][e_index(G, d, (int)i, (int)j, (int)k)];
   }
 
-  // One accumulation .5*w*(E_new + E^n) at ring/plain offsets (n, jn) of a
-  // node whose applyCurrentSource mask is known to be true.
-  __device__ __forceinline__ F term(int d, size_t n, size_t jn, F w) const {
-    const GridT<F>& G = *g;
-    F vn = G.e_star[d][n];
-    if (with_current) {
-      const F jc = G.j[d][jn];
-      if (jc != F(0.)) vn += G.jcoef * jc;
-    }
-    return F(.5) * w * (vn + G.e_old[d][n]);
+  // One accumulation .5*w*(E_new + E^n) at the ring offset n of a node.
+  __device__ __forceinline__ W term(int d, size_t n, size_t, W w) const {
+    return W(.5) * w * s[d][n];
   }
 
   // binomialXZSegment specialised for the gather.  When the whole 4x2x4
@@ -297,7 +292,7 @@ struct ElectricVisitor {
   // reference's (Ex: k, y, x; Ey: k, x; Ez: y, x, k).
   __device__ __forceinline__ void f3_segment(const GridT<F>& G, const double s[3],
                                              const double d[3], double first, double last) {
-    const F width = F(last - first);
+    const W width = W(last - first);
     const double mid = (first + last) * 0.5;
     const double x = s[0] + mid * d[0], y = s[1] + mid * d[1], z = s[2] + mid * d[2];
     long long i = (long long)floor(x), j = (long long)floor(y);
@@ -308,17 +303,17 @@ struct ElectricVisitor {
       binomial_xz_segment(G, s, d, first, last, *this);
       return;
     }
-    F wx[4], wz[4];
-    node_weights(F(x - i), wx);
-    node_weights(F(z - k), wz);
-    const F wy[2] = {F(1.) - F(y - j), F(y - j)};
-    const F edge[3] = {F(0.25), F(0.5), F(0.25)};
-    const F slope[4] = {F(-0.25), F(-0.25), F(0.25), F(0.25)};
-    const F sy[2] = {F(-1.), F(1.)};
-    const F curvature = width * width / F(12.);
-    const F xy = curvature * F(d[0]) * F(d[1]);
-    const F xz = curvature * F(d[0]) * F(d[2]);
-    const F yz = curvature * F(d[1]) * F(d[2]);
+    W wx[4], wz[4];
+    node_weights(W(x - i), wx);
+    node_weights(W(z - k), wz);
+    const W wy[2] = {W(1.) - W(y - j), W(y - j)};
+    const W edge[3] = {W(0.25), W(0.5), W(0.25)};
+    const W slope[4] = {W(-0.25), W(-0.25), W(0.25), W(0.25)};
+    const W sy[2] = {W(-1.), W(1.)};
+    const W curvature = width * width / W(12.);
+    const W xy = curvature * W(d[0]) * W(d[1]);
+    const W xz = curvature * W(d[0]) * W(d[2]);
+    const W yz = curvature * W(d[1]) * W(d[2]);
     const int I = (int)i, J = (int)j, K = (int)k;
     // Ex (nx, ny+1, nz+1): nodes x I-1..I+1, y J..J+1, z K-1..K+2
     {
@@ -329,7 +324,7 @@ struct ElectricVisitor {
         const size_t jplane = (size_t)(K - 1 + c) * nyc;
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-          const F weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+          const W weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
           const size_t n0 = (plane + J + b) * nxc + (I - 1);
           const size_t j0 = (jplane + J + b) * nxc + (I - 1);
 #pragma unroll
@@ -362,7 +357,7 @@ struct ElectricVisitor {
       for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          const F weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
+          const W weight = width * (wx[a] * wy[b] + xy * slope[a] * sy[b]);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             r[2] += term(2, (plane[c] + J + b) * nxc + (I - 1 + a),
@@ -372,9 +367,9 @@ struct ElectricVisitor {
   }
 };
 
-template <class F>
-__device__ __forceinline__ F open_b(const GridT<F>& g, int a, long long i, long long j,
-                                    long long k) {
+template <class W, class F>
+__device__ __forceinline__ W open_b(const GridT<F>& g, const W* const* bsrc, int a, long long i,
+                                    long long j, long long k) {
   const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
   if (i < 0) i = 0;
   if (i > nxc - 1) i = nxc - 1;
@@ -382,15 +377,15 @@ __device__ __forceinline__ F open_b(const GridT<F>& g, int a, long long i, long 
   if (j > nyc - 1) j = nyc - 1;
   if (k < 0) k = 0;
   if (k >= nzc) k = nzc - 1;
-  return g.b[a][b_index(g, a, (int)i, (int)j, (int)k)];
+  return bsrc[a][b_index(g, a, (int)i, (int)j, (int)k)];
 }
 
 // binomialXZMagneticSample (src/source_coupling_math.h:142-167).  Rows of
 // the 4x2x4 stencil that lie inside the component are read without the
 // open-face clamps; the clamped form runs otherwise.  Same order either way.
-template <class F>
-__device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const double p[3],
-                                                     double value[3]) {
+template <class W, class F>
+__device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const W* const* bsrc,
+                                                     const double p[3], double value[3]) {
   const double h[3] = {g.dx, g.dy, g.dz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -401,22 +396,22 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const do
       cell[d] = (long long)floor(pos);
       fraction[d] = pos - cell[d];
     }
-    F wx[4], wz[4];
-    node_weights(F(fraction[0]), wx);
-    node_weights(F(fraction[2]), wz);
-    const F wy[2] = {F(1. - fraction[1]), F(fraction[1])};
+    W wx[4], wz[4];
+    node_weights(W(fraction[0]), wx);
+    node_weights(W(fraction[2]), wz);
+    const W wy[2] = {W(1. - fraction[1]), W(fraction[1])};
     const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
-    F v = F(0.);
+    W v = W(0.);
     if (cell[0] >= 1 && cell[0] + 2 <= nxc - 1 && cell[1] >= 0 && cell[1] + 1 <= nyc - 1 &&
         cell[2] >= 1 && cell[2] + 2 <= nzc - 1) {
-      const F* base = g.b[a];
+      const W* base = bsrc[a];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const size_t plane = (size_t)ring((int)cell[2] - 1 + k, g.zb_b[a], (int)nzc) * nyc;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const F* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
-          F r = F(0.);
+          const W* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
+          W r = W(0.);
 #pragma unroll
           for (int i = 0; i < 4; ++i) r += wx[i] * row[i];
           v += wz[k] * wy[j] * r;
@@ -425,9 +420,9 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const do
     } else {
       for (int k = 0; k < 4; ++k)
         for (int j = 0; j < 2; ++j) {
-          F row = F(0.);
+          W row = W(0.);
           for (int i = 0; i < 4; ++i)
-            row += wx[i] * open_b(g, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
+            row += wx[i] * open_b(g, bsrc, a, cell[0] - 1 + i, cell[1] + j, cell[2] - 1 + k);
           v += wz[k] * wy[j] * row;
         }
     }
@@ -436,9 +431,9 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const do
 }
 
 // magneticSample(bounds=false, halo, openFaces=true) (src/source_coupling_math.h:122-138).
-template <class F>
-__device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const double p[3],
-                                                   double value[3]) {
+template <class W, class F>
+__device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const W* const* bsrc,
+                                                   const double p[3], double value[3]) {
   const double ds[3] = {g.dx, g.dy, g.dz};
   int cell[2][3];
   double fraction[2][3];
@@ -450,29 +445,29 @@ __device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const doub
     }
   for (int axis = 0; axis < 3; ++axis) {
     const int hx = axis == 0 ? 0 : 1, hy = axis == 1 ? 0 : 1, hz = axis == 2 ? 0 : 1;
-    F v = F(0.);
+    W v = W(0.);
     for (int k = 0; k < 2; ++k)
       for (int j = 0; j < 2; ++j)
         for (int i = 0; i < 2; ++i) {
-          const F x = F(i ? fraction[hx][0] : 1 - fraction[hx][0]),
-                  y = F(j ? fraction[hy][1] : 1 - fraction[hy][1]),
-                  z = F(k ? fraction[hz][2] : 1 - fraction[hz][2]);
+          const W x = W(i ? fraction[hx][0] : 1 - fraction[hx][0]),
+                  y = W(j ? fraction[hy][1] : 1 - fraction[hy][1]),
+                  z = W(k ? fraction[hz][2] : 1 - fraction[hz][2]);
           v += x * y * z *
-               open_b(g, axis, cell[hx][0] + i, cell[hy][1] + j, cell[hz][2] + k);
+               open_b(g, bsrc, axis, cell[hx][0] + i, cell[hy][1] + j, cell[hz][2] + k);
         }
     value[axis] = double(v);
   }
 }
 
 // Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
-template <class F>
+template <class W, class F>
 __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
-                                                    bool with_current, double out[3]) {
+                                                    const W* const* orbit, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
-  ElectricVisitor<F> v{&g, with_current, {F(0.), F(0.), F(0.)}};
+  ElectricVisitor<W, F> v{&g, orbit, {W(0.), W(0.), W(0.)}};
   if (shape_weights(g, shape, path.begin, path.end, v) < 0) return kErrCrossingBudget;
   const double fraction = path.last - path.first;
   for (int d = 0; d < 3; ++d) out[d] = double(v.r[d]) * fraction;
@@ -480,19 +475,19 @@ __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape
 }
 
 // Impl::magnetic (src/source_coupling.cpp:40-51).
-template <class F>
+template <class W, class F>
 __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
-                                                    double out[3]) {
+                                                    const W* const* bsrc, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
   double middle[3];
   for (int d = 0; d < 3; ++d) middle[d] = (path.begin[d] + path.end[d]) * .5;
   if (shape == 0)
-    binomial_xz_magnetic(g, middle, out);
+    binomial_xz_magnetic(g, bsrc, middle, out);
   else
-    trilinear_magnetic(g, middle, out);
+    trilinear_magnetic(g, bsrc, middle, out);
   return kErrNone;
 }
 
@@ -501,6 +496,7 @@ __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape
 template <class F>
 struct DepositVisitor {
   static constexpr bool kF3Segment = false;
+  using Weight = F;
   const GridT<F>* g;
   F scale[3];
   bool smooth_x;
@@ -979,7 +975,7 @@ __device__ __forceinline__ SlotPlan plan_slot(const GridT<F>& g, const DFrame& f
 // (Impl::Slot::guess, src/source_coupling.cpp:92-95), gathered from E*
 // before any current of the trial is deposited; the push reads them as the
 // previous residual's fields.
-template <class F>
+template <class W, class F>
 __global__ void guess_gather_kernel(PushArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
@@ -994,8 +990,12 @@ __global__ void guess_gather_kernel(PushArgs<F> a) {
   const double guess[3] = {s.start[0] + sc * u[0], s.start[1] + sc * u[1],
                            s.start[2] + sc * u[2]};
   double ne[3], nb[3];
-  unsigned err = gather_electric(a.g, a.shape, s.start, guess, false, ne);
-  if (!err) err = gather_magnetic(a.g, a.shape, s.start, guess, nb);
+  const W* orbit[3] = {static_cast<const W*>(a.orbit[0]), static_cast<const W*>(a.orbit[1]),
+                       static_cast<const W*>(a.orbit[2])};
+  const W* bsrc[3] = {static_cast<const W*>(a.bgather[0]), static_cast<const W*>(a.bgather[1]),
+                      static_cast<const W*>(a.bgather[2])};
+  unsigned err = gather_electric(a.g, a.shape, s.start, guess, orbit, ne);
+  if (!err) err = gather_magnetic(a.g, a.shape, s.start, guess, bsrc, nb);
   if (err) raise_error(a.status, err, (unsigned long long)n);
   double* next_e = const_cast<double*>(a.next_e);
   double* next_b = const_cast<double*>(a.next_b);
@@ -1183,7 +1183,7 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-template <class F>
+template <class W, class F>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double force = 0.0, defect = 0.0, scale = 0.0;
@@ -1200,8 +1200,13 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     }
     const double last[3] = {a.x1[n], a.y1[n], a.z1[n]};
     double ne[3], nb[3];
-    unsigned err = gather_electric(a.g, a.shape, first, last, true, ne);
-    if (!err) err = gather_magnetic(a.g, a.shape, first, last, nb);
+    const W* orbit[3] = {static_cast<const W*>(a.orbit[0]), static_cast<const W*>(a.orbit[1]),
+                         static_cast<const W*>(a.orbit[2])};
+    const W* bsrc[3] = {static_cast<const W*>(a.bgather[0]),
+                        static_cast<const W*>(a.bgather[1]),
+                        static_cast<const W*>(a.bgather[2])};
+    unsigned err = gather_electric(a.g, a.shape, first, last, orbit, ne);
+    if (!err) err = gather_magnetic(a.g, a.shape, first, last, bsrc, nb);
     if (err) {
       raise_error(a.status, err, (unsigned long long)n);
       for (int d = 0; d < 3; ++d) ne[d] = nb[d] = 0.0;
@@ -1488,15 +1493,14 @@ __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen,
     raise_error(status, kErrFellBehind, (unsigned long long)i);
 }
 
-// Both element types are built: FP64 drop-in and FP32-mixed.
-#define APRL_PARTICLE_KERNELS(F)                                              \
-  template __global__ void guess_gather_kernel<F>(PushArgs<F>);              \
-  template __global__ void push_deposit_kernel<F>(PushArgs<F>);              \
-  template __global__ void carrier_kernel<F>(CarrierArgs<F>);                \
-  template __global__ void residual_kernel<F>(ResidualArgs<F>);              \
-  template __global__ void frozen_support_kernel<F>(SupportArgs<F>);
-APRL_PARTICLE_KERNELS(double)
-APRL_PARTICLE_KERNELS(float)
-#undef APRL_PARTICLE_KERNELS
+// The grid and J are binary64 in every mode; the gathers are built with
+// binary64 (FP64 drop-in) and binary32 (FP32-mixed) arithmetic.
+template __global__ void push_deposit_kernel<double>(PushArgs<double>);
+template __global__ void carrier_kernel<double>(CarrierArgs<double>);
+template __global__ void frozen_support_kernel<double>(SupportArgs<double>);
+template __global__ void guess_gather_kernel<double, double>(PushArgs<double>);
+template __global__ void guess_gather_kernel<float, double>(PushArgs<double>);
+template __global__ void residual_kernel<double, double>(ResidualArgs<double>);
+template __global__ void residual_kernel<float, double>(ResidualArgs<double>);
 
 }  // namespace aprl_gpu

@@ -76,12 +76,16 @@ struct DSlots {
   unsigned char* seen;
 };
 
-// The argument blocks of the particle kernels are templated on the field
-// element type F (double: FP64 drop-in; float: FP32-mixed).  Particle
-// state, the push and the boundary logic are binary64 in both modes.
+// The argument blocks of the particle kernels are templated on the type F
+// of J in the grid view (binary64 in both modes of this library).  Particle
+// state, the push, the deposit and the boundary logic are binary64.
 template <class F>
 struct PushArgs {
   GridT<F> g;
+  // What the gathers read, in their arithmetic type: the orbit sum
+  // S = E_new + E^n per E node and B, both in the ring layout of E and B.
+  const void* orbit[3];
+  const void* bgather[3];
   DFrame frame;
   DRegion region;
   DMagnet magnets[kMaxMagnets];
@@ -125,6 +129,8 @@ struct CarrierArgs {
 template <class F>
 struct ResidualArgs {
   GridT<F> g;
+  const void* orbit[3];     // as in PushArgs
+  const void* bgather[3];
   int shape;
   long long count;
   DParticles p;
@@ -158,10 +164,12 @@ struct ResidualArgs {
 #define APRL_RESIDUAL_BOUNDS
 #endif
 
-template <class F> __global__ void guess_gather_kernel(PushArgs<F> a);
+// W: arithmetic of the gathers (double, or float in the FP32-mixed mode).
+template <class W, class F> __global__ void guess_gather_kernel(PushArgs<F> a);
 template <class F> __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
 template <class F> __global__ void carrier_kernel(CarrierArgs<F> a);
-template <class F> __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
+template <class W, class F>
+__global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
 
 // Stable compaction helpers (warp ballot + block scan + block-offset scan).
 constexpr int kScanBlock = 256;

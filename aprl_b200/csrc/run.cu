@@ -54,7 +54,7 @@ enum Kernel : unsigned {
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
-  kGuessGather, kKernelCount
+  kGuessGather, kOrbitSum, kBShadow, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -63,7 +63,7 @@ const char* kKernelNames[kKernelCount] = {
   "block_offset_scan", "gather_particles", "gather_carriers",
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
-  "frozen_support", "guess_gather"};
+  "frozen_support", "guess_gather", "orbit_sum", "b_shadow"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -209,15 +209,12 @@ struct DeviceProfile {
 // One of the 8 active histories.  component: ABI index (0..5); derivative
 // axis 0/1; the history's k ring follows its component's ring.
 struct HistoryBuffer {
-  void* data = nullptr;  // field element type of the run
+  double* data = nullptr;
   int slots = 0, layers = 0, row = 0;
   int component = 0;
   int abi_index = 0;
   size_t length() const { return (size_t)slots * layers * row; }
-  template <class F>
-  CpmlHistoryT<F> view() const {
-    return CpmlHistoryT<F>{static_cast<F*>(data), slots, layers, row};
-  }
+  CpmlHistory view() const { return CpmlHistory{data, slots, layers, row}; }
 };
 
 struct Timing {
@@ -231,15 +228,19 @@ struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
   double coeff[12]{};
-  // Field storage in the run's element type (double, or float in the
-  // FP32-mixed mode); `fes` is its size in bytes.
+  // E, B and J are binary64 in both modes (`fes`: J element size); the
+  // FP32-mixed mode runs the gathers in binary32.
   bool fp32 = false;
   size_t fes = 8;
-  void* e[2][3]{};
+  double* e[2][3]{};
   int cur = 0;  // e[cur] = E^n (committed), e[1-cur] = E*
-  void* b[3]{};
+  double* b[3]{};
   void* jc[3]{};
-  void* lower[3]{};
+  double* lower[3]{};
+  // What the gathers read: the orbit sum S = E_new + E^n per E node (binary64,
+  // or binary32 in the FP32-mixed mode) and, in that mode, a binary32 B.
+  void* orbit[3]{};
+  float* bshadow[3]{};
   int zb_e[3]{}, zb_b[3]{};
   double* ref[6]{};
   bool ref_set[6]{};
@@ -396,9 +397,9 @@ GridT<F> make_grid(const aprl_run* r) {
   g.dt = r->cfg.dt;
   for (int a = 0; a < 3; ++a) {
     g.origin[a] = r->origin[a];
-    g.e_old[a] = static_cast<F*>(r->e[r->cur][a]);
-    g.e_star[a] = static_cast<F*>(r->e[1 - r->cur][a]);
-    g.b[a] = static_cast<F*>(r->b[a]);
+    g.e_old[a] = r->e[r->cur][a];
+    g.e_star[a] = r->e[1 - r->cur][a];
+    g.b[a] = r->b[a];
     g.j[a] = static_cast<F*>(r->jc[a]);
     g.zb_e[a] = r->zb_e[a];
     g.zb_b[a] = r->zb_b[a];
@@ -656,35 +657,23 @@ aprl_status reserve_carriers(aprl_run* r, size_t n) {
   return ensure_scan(r, n);
 }
 
-// Rotate between logical (window) and physical (ring) plane order.  The
-// host side is always binary64; an FP32-mixed run converts through a float
-// staging copy.
-aprl_status copy_ring(aprl_run* r, void* device, const double* host_in, double* host_out,
+// Rotate between logical (window) and physical (ring) plane order.
+aprl_status copy_ring(aprl_run* r, double* device, const double* host_in, double* host_out,
                       size_t plane, size_t layers, int base, size_t slots = 1) {
-  const size_t es = r->fes, total = slots * layers * plane;
-  std::vector<float> stage;
-  if (es == 4) {
-    stage.resize(total);
-    if (host_in)
-      for (size_t i = 0; i < total; ++i) stage[i] = static_cast<float>(host_in[i]);
-  }
-  char* host = es == 4 ? reinterpret_cast<char*>(stage.data())
-                       : reinterpret_cast<char*>(host_in ? const_cast<double*>(host_in) : host_out);
   for (size_t s = 0; s < slots; ++s) {
     const size_t slot_offset = s * layers * plane;
     for (size_t k = 0; k < layers; ++k) {
       const size_t pk = (k + base) % layers;
-      char* d = static_cast<char*>(device) + (slot_offset + pk * plane) * es;
-      char* h = host + (slot_offset + k * plane) * es;
+      double* d = device + slot_offset + pk * plane;
       if (host_in)
-        CUDA_TRY(cudaMemcpyAsync(d, h, plane * es, cudaMemcpyHostToDevice, r->stream));
+        CUDA_TRY(cudaMemcpyAsync(d, host_in + slot_offset + k * plane, plane * 8,
+                                 cudaMemcpyHostToDevice, r->stream));
       else
-        CUDA_TRY(cudaMemcpyAsync(h, d, plane * es, cudaMemcpyDeviceToHost, r->stream));
+        CUDA_TRY(cudaMemcpyAsync(host_out + slot_offset + k * plane, d, plane * 8,
+                                 cudaMemcpyDeviceToHost, r->stream));
     }
   }
   CUDA_TRY(cudaStreamSynchronize(r->stream));
-  if (es == 4 && host_out)
-    for (size_t i = 0; i < total; ++i) host_out[i] = static_cast<double>(stage[i]);
   return APRL_OK;
 }
 
@@ -850,27 +839,27 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   const aprl_run_config& c = r->cfg;
   for (int a = 0; a < 3; ++a)
     CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
-  InletPlaneArgs<F> ia{};
+  InletPlaneArgs ia{};
   ia.nx = (int)c.nx;
   ia.ny = (int)c.ny;
-  for (int a = 0; a < 3; ++a) ia.out[a] = static_cast<F*>(r->lower[a]);
+  for (int a = 0; a < 3; ++a) ia.out[a] = r->lower[a];
   TRY(inlet_table(r, r->offset - 1, r->step, ia.inlet));
-  TRY(launch(r, kInletLower, inlet_lower_kernel<F>,
+  TRY(launch(r, kInletLower, inlet_lower_kernel,
              dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), 3), dim3(32, 8), ia));
   CowanArgs<F> ca{};
   ca.g = make_grid<F>(r);
   for (int a = 0; a < 3; ++a) {
-    ca.e[a] = static_cast<const F*>(r->e[r->cur][a]);
-    ca.lower[a] = static_cast<const F*>(r->lower[a]);
-    ca.alpha[a] = F(r->coeff[a]);
-    ca.beta[a] = F(r->coeff[3 + a]);
+    ca.e[a] = r->e[r->cur][a];
+    ca.lower[a] = r->lower[a];
+    ca.alpha[a] = r->coeff[a];
+    ca.beta[a] = r->coeff[3 + a];
   }
-  ca.delta_xy = F(r->coeff[6]);
-  ca.delta_yz = F(r->coeff[7]);
-  ca.delta_zx = F(r->coeff[8]);
+  ca.delta_xy = r->coeff[6];
+  ca.delta_yz = r->coeff[7];
+  ca.delta_zx = r->coeff[8];
   ca.mx = r->mprof[0].view();
   ca.my = r->mprof[1].view();
-  for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view<F>();
+  for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
   // 32x8 column tiles, 16-plane z chunks (kTX, kTY, kKChunk in fields.cu).
   const dim3 cblock(32, 8);
   const dim3 cgrid(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), blocks_for(c.nz + 1, 16));
@@ -880,7 +869,7 @@ aprl_status advance_magnetic_t(aprl_run* r) {
 }
 
 aprl_status do_advance_magnetic(aprl_run* r) {
-  return r->fp32 ? advance_magnetic_t<float>(r) : advance_magnetic_t<double>(r);
+  return advance_magnetic_t<double>(r);
 }
 
 template <class F>
@@ -891,10 +880,14 @@ aprl_status preview_electric_t(aprl_run* r) {
   pa.g = make_grid<F>(r);
   pa.ex_prof = r->eprof[0].view();
   pa.ey_prof = r->eprof[1].view();
-  for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view<F>();
+  for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view();
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
+  if (r->fp32)  // B is final for the step: its binary32 copy for the gathers
+    for (int a = 0; a < 3; ++a)
+      TRY(launch(r, kBShadow, b_shadow_kernel, dim3(blocks_for(b_count(c, a), 256)), dim3(256),
+                 (const double*)r->b[a], r->bshadow[a], (long long)b_count(c, a)));
   if (r->np)
     CUDA_TRY(cudaMemcpyAsync(r->slot_order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice,
                              r->stream));
@@ -905,11 +898,13 @@ aprl_status preview_electric_t(aprl_run* r) {
 }
 
 aprl_status do_preview_electric(aprl_run* r) {
-  return r->fp32 ? preview_electric_t<float>(r) : preview_electric_t<double>(r);
+  return preview_electric_t<double>(r);
 }
 
-template <class F>
+// One coupling trial; W is the arithmetic of the gathers.
+template <class W>
 aprl_status trial_t(aprl_run* r, double residual[4]) {
+  using F = double;
   if (r->stage != 2 && r->stage != 3)
     return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
   const aprl_run_config& c = r->cfg;
@@ -995,13 +990,30 @@ aprl_status trial_t(aprl_run* r, double residual[4]) {
     pa.key_base = (unsigned long long)(r->step + 1) << 32;
     pa.counters = r->d_counters;
     pa.status = r->d_status;
-    if (r->trials == 0)
-      TRY(launch(r, kGuessGather, guess_gather_kernel<F>, dim3(blocks_for(r->np, 128)),
+    W* orbit[3] = {static_cast<W*>(r->orbit[0]), static_cast<W*>(r->orbit[1]),
+                   static_cast<W*>(r->orbit[2])};
+    for (int a = 0; a < 3; ++a) {
+      pa.orbit[a] = orbit[a];
+      pa.bgather[a] = r->fp32 ? static_cast<const void*>(r->bshadow[a])
+                              : static_cast<const void*>(r->b[a]);
+    }
+    const dim3 oblock(32, 4);
+    if (r->trials == 0) {
+      TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
+                 orbit[1], orbit[2], 0));
+      TRY(launch(r, kGuessGather, guess_gather_kernel<W, F>, dim3(blocks_for(r->np, 128)),
                  dim3(128), pa));
+    }
     TRY(launch(r, kPushDeposit, push_deposit_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128),
                pa));
+    TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
+               orbit[1], orbit[2], 1));
     ResidualArgs<F> ra{};
     ra.g = g;
+    for (int a = 0; a < 3; ++a) {
+      ra.orbit[a] = pa.orbit[a];
+      ra.bgather[a] = pa.bgather[a];
+    }
     ra.shape = c.shape;
     ra.count = (long long)r->np;
     ra.p = r->p;
@@ -1014,7 +1026,7 @@ aprl_status trial_t(aprl_run* r, double residual[4]) {
     ra.abs_grid_work = r->abs_work;
     ra.sums = r->d_sums;
     ra.status = r->d_status;
-    TRY(launch(r, kResidual, residual_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
+    TRY(launch(r, kResidual, residual_kernel<W, F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
   CUDA_TRY(cudaMemcpyAsync(r->h_sums, r->d_sums, sizeof(ResidualSums), cudaMemcpyDeviceToHost,
                            r->stream));
@@ -1039,12 +1051,8 @@ aprl_status do_commit(aprl_run* r) {
   if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
   const aprl_run_config& c = r->cfg;
   const dim3 block(32, 4);
-  if (r->fp32)
-    TRY(launch(r, kElectricCommit, electric_commit_kernel<float>, grid3(c, block), block,
-               make_grid<float>(r)));
-  else
-    TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
-               make_grid<double>(r)));
+  TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
+             make_grid<double>(r)));
   r->cur = 1 - r->cur;
   // Counters of the converged trial become cumulative.
   CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
@@ -1099,7 +1107,7 @@ aprl_status shift_insert_t(aprl_run* r) {
   sa.g = make_grid<F>(r);
   TRY(inlet_table(r, r->offset, r->step, sa.inlet));
   for (int h = 0; h < 8; ++h) {
-    sa.h[h] = r->hist[h].view<F>();
+    sa.h[h] = r->hist[h].view();
     const int comp = r->hist[h].component;
     sa.history_base[h] = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
   }
@@ -1122,7 +1130,7 @@ aprl_status do_shift(aprl_run* r) {
     r->zb_e[a] = (r->zb_e[a] + nze - 1) % nze;
     r->zb_b[a] = (r->zb_b[a] + nzb - 1) % nzb;
   }
-  TRY(r->fp32 ? shift_insert_t<float>(r) : shift_insert_t<double>(r));
+  TRY(shift_insert_t<double>(r));
   r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
   if (r->np)
     TRY(launch(r, kInletCheck, inlet_check_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
@@ -1222,19 +1230,24 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
   if (s != APRL_OK) return cleanup(s);
   const aprl_run_config& c = *config;
   r->fp32 = c.precision == APRL_PRECISION_FP32_MIXED;
-  r->fes = r->fp32 ? sizeof(float) : sizeof(double);
+  r->fes = sizeof(double);
   const size_t fes = r->fes;
   for (int a = 0; a < 3; ++a) {
     for (int k = 0; k < 2; ++k) {
-      if ((s = device_alloc_bytes(&r->e[k][a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
-      cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * fes, r->stream);
+      if ((s = device_alloc(&r->e[k][a], e_count(c, a))) != APRL_OK) return cleanup(s);
+      cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * 8, r->stream);
     }
-    if ((s = device_alloc_bytes(&r->b[a], b_count(c, a) * fes)) != APRL_OK) return cleanup(s);
-    cudaMemsetAsync(r->b[a], 0, b_count(c, a) * fes, r->stream);
+    if ((s = device_alloc(&r->b[a], b_count(c, a))) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(r->b[a], 0, b_count(c, a) * 8, r->stream);
     if ((s = device_alloc_bytes(&r->jc[a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
     cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * fes, r->stream);
     const size_t plane = (size_t)(c.nx + (a != 0)) * (c.ny + (a != 1));
-    if ((s = device_alloc_bytes(&r->lower[a], plane * fes)) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc(&r->lower[a], plane)) != APRL_OK) return cleanup(s);
+    const size_t gather_bytes = r->fp32 ? sizeof(float) : sizeof(double);
+    if ((s = device_alloc_bytes(&r->orbit[a], e_count(c, a) * gather_bytes)) != APRL_OK)
+      return cleanup(s);
+    if (r->fp32 && (s = device_alloc(&r->bshadow[a], b_count(c, a))) != APRL_OK)
+      return cleanup(s);
     r->max_rate[a] = maximum_rate(c, a);
   }
   // CPML profiles (x, y) for magnetic (half-integer) and electric nodes.
@@ -1268,8 +1281,8 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     hb.slots = prof.active;
     hb.layers = (int)sh[2];
     hb.row = (int)(der == 0 ? sh[1] : sh[0]);
-    if ((s = device_alloc_bytes(&hb.data, hb.length() * fes)) != APRL_OK) return cleanup(s);
-    cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * fes, r->stream);
+    if ((s = device_alloc(&hb.data, hb.length())) != APRL_OK) return cleanup(s);
+    cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * 8, r->stream);
   }
   for (int a = 0; a < 3; ++a) {
     const uint64_t cells = a == 0 ? c.nx : (a == 1 ? c.ny : c.nz);
@@ -1311,6 +1324,8 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   for (int a = 0; a < 3; ++a) {
     cudaFree(r->e[0][a]); cudaFree(r->e[1][a]); cudaFree(r->b[a]); cudaFree(r->jc[a]);
     cudaFree(r->lower[a]);
+    cudaFree(r->orbit[a]);
+    cudaFree(r->bshadow[a]);
   }
   for (int a = 0; a < 6; ++a) cudaFree(r->ref[a]);
   for (int a = 0; a < 2; ++a) {
@@ -1413,7 +1428,7 @@ static aprl_status field_io(aprl_run* r, unsigned a, const double* in, double* o
     return fail(APRL_ERR_RUNTIME, "Fields can only be replaced between steps");
   const size_t plane = s[0] * s[1];
   if (a >= 6)
-    return copy_ring(r, r->jc[a - 6], in, out, plane, s[2], 0);
+    return copy_ring(r, static_cast<double*>(r->jc[a - 6]), in, out, plane, s[2], 0);
   if (a < 3) return copy_ring(r, r->e[r->cur][a], in, out, plane, s[2], r->zb_e[a]);
   return copy_ring(r, r->b[a - 3], in, out, plane, s[2], r->zb_b[a - 3]);
 }
@@ -1441,7 +1456,8 @@ static aprl_status history_io(aprl_run* r, unsigned index, const double* in, dou
   if (!length) return APRL_OK;
   const int comp = h->component;
   const int base = comp < 3 ? r->zb_e[comp] : r->zb_b[comp - 3];
-  return copy_ring(r, h->data, in, out, (size_t)h->row, (size_t)h->layers, base, (size_t)h->slots);
+  return copy_ring(r, h->data, in, out, (size_t)h->row, (size_t)h->layers, base,
+                   (size_t)h->slots);
 }
 
 aprl_status aprl_run_set_history(aprl_run* r, unsigned index, const double* host, size_t count) {
@@ -1874,12 +1890,8 @@ aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double*
   }
   da.out = r->d_detector;
   const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
-  if (r->fp32)
-    TRY(launch(r, kDetectorPlane, detector_plane_kernel<float>, grid, block,
-               retyped<float>(da, make_grid<float>(r))));
-  else
-    TRY(launch(r, kDetectorPlane, detector_plane_kernel<double>, grid, block,
-               retyped<double>(da, make_grid<double>(r))));
+  TRY(launch(r, kDetectorPlane, detector_plane_kernel<double>, grid, block,
+             retyped<double>(da, make_grid<double>(r))));
   CUDA_TRY(cudaMemcpyAsync(out, r->d_detector, count * 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;
@@ -1994,12 +2006,8 @@ aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* r, double plane_lab_z,
   da.out = scratch;
   // A direct launch: no timing events are created on this path.
   const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
-  if (r->fp32)
-    detector_plane_kernel<float><<<grid, block, 0, r->stream>>>(
-        retyped<float>(da, make_grid<float>(r)));
-  else
-    detector_plane_kernel<double><<<grid, block, 0, r->stream>>>(
-        retyped<double>(da, make_grid<double>(r)));
+  detector_plane_kernel<double><<<grid, block, 0, r->stream>>>(
+      retyped<double>(da, make_grid<double>(r)));
   CUDA_TRY(cudaGetLastError());
   ++r->kernel_launches[kDetectorPlane];
   ++r->launches;

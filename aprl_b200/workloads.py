@@ -94,10 +94,10 @@ class Workload:
     description: dict = field(default_factory=dict)
 
 
-# Fixed-point stopping rule of the FP32-mixed mode.  Its trial-to-trial
-# residual floor (binary32 fields and FP32 atomics) is force ~1e-10 and
-# relative work ~1e-9, so the binary64 tolerances 1e-13 / 1e-8 cannot be met;
-# 1e-9 / 1e-5 keep the detector field within 1e-6 of the FP64 oracle.
+# Fixed-point stopping rule of the FP32-mixed mode.  Its binary32 gathers
+# put a floor under the trial-to-trial residual (force ~1e-10, relative work
+# ~1e-9), so the binary64 tolerances 1e-13 / 1e-8 cannot be met; 1e-9 / 1e-5
+# stop at the minimum two trials.
 FP32_FORCE_TOLERANCE = 1.0e-9
 FP32_WORK_TOLERANCE = 1.0e-5
 

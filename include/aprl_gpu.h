@@ -54,12 +54,15 @@ typedef enum {
 } aprl_shape;
 
 /* Arithmetic of a run.  FP64 is the drop-in: every stage in binary64 with
- * the reference's operation order.  FP32_MIXED stores and updates the fields,
- * J, the CPML histories and the shape-weight walkers (gather and deposit) in
- * binary32, evaluating the weights from binary64 cell-relative offsets;
- * particle positions and momenta, the Lapenta-Markidis push, the boundary
- * events, the window bookkeeping and the residual reductions stay binary64.
- * The reference is binary64 only; this mode has no counterpart there. */
+ * the reference's operation order.  FP32_MIXED runs the field gathers in
+ * binary32: the shape weights (from binary64 cell-relative offsets), the
+ * orbit-averaged E and the B the gathers read (binary32 copies made once per
+ * trial / step) and their accumulation.  E, B, J, the CPML histories and
+ * every field update, the deposit, particle positions and momenta, the
+ * Lapenta-Markidis push, the boundary events, the window bookkeeping and the
+ * residual reductions stay binary64, so the rounding of the mode perturbs
+ * particle forces only, never the fields' own history.  The reference is
+ * binary64 only; this mode has no counterpart there. */
 typedef enum {
   APRL_PRECISION_FP64 = 0,
   APRL_PRECISION_FP32_MIXED = 1

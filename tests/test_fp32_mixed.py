@@ -1,11 +1,10 @@
 """FP32-mixed mode against the FP64 oracle.
 
-The mode keeps binary64 particle state, push, boundary events and window
-bookkeeping, and runs the fields, J, the CPML histories and the shape-weight
-walkers in binary32.  Its error is measured against the FP64 oracle on the
-same seeded input: the lab detector-plane field (relative L2 over the plane,
-target 1e-5), the particle states (same ids in the same order), and the grid
-fields.
+The mode runs the field gathers in binary32 (weights, the orbit-averaged E
+and B they read, and their accumulation) and everything else in binary64.
+Its error is measured against the FP64 oracle on the same seeded input: the
+lab detector-plane field (relative L2 over the plane, target 1e-5), the
+particle states (same ids in the same order), and the grid fields.
 """
 import numpy as np
 import pytest
