@@ -56,7 +56,7 @@ def parse_args(argv=None):
     p.add_argument("--scan-requests", type=int, default=16)
     p.add_argument("--scan-steps", type=int, default=500)
     p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
-    p.add_argument("--scan-slots", type=int, default=12)
+    p.add_argument("--scan-slots", type=int, default=4)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     return p.parse_args(argv)
 
