@@ -63,33 +63,41 @@ __device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, in
 // bit-identical to the reference.  Each B node is updated by the
 // curl, then by its CPML terms in the reference's term order (0,2,1),
 // (1,2,0), (2,1,0), (2,0,1), reusing the curl's smoothed difference.
-constexpr int kTX = 32, kTY = 8, kKChunk = 16;
+constexpr int kTX = kCowanTileX, kTY = kCowanTileY, kKChunk = kCowanChunk;
 
 struct ETile {
   double v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
 };
 
-__device__ __forceinline__ int plane_slot(int k) { return ((k % 3) + 3) % 3; }
+// Ring slots of the tile planes k-1, k, k+1 of the current z-march step,
+// rotated by one per step (no modular arithmetic in the stencil).
+struct PlaneSlots {
+  int s[3];
+};
 
-__device__ __forceinline__ double tile_at(const ETile& t, int c, int i, int j, int k, int i0,
-                                          int j0) {
-  return t.v[c][plane_slot(k)][j - j0 + 1][i - i0 + 1];
+__device__ __forceinline__ double tile_at(const ETile& t, int c, int li, int lj, int dk,
+                                          const PlaneSlots& ps) {
+  return t.v[c][ps.s[dk + 1]][lj][li];
 }
 
+// smoothedElectric from the tile: centre (li, lj) in tile coordinates, dk
+// the plane offset (-1..1) from the marching plane; every offset is a
+// compile-time constant after inlining, so the plane choice is a register.
 template <class F>
 __device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs<F>& a, int c,
-                                                int d, int i, int j, int k, int i0, int j0) {
+                                                int d, int li, int lj, int dk,
+                                                const PlaneSlots& ps) {
   const int ta = (d + 1) % 3, tb = (d + 2) % 3;
   const double delta = d == 0 ? a.delta_yz : (d == 1 ? a.delta_zx : a.delta_xy);
-  const int p[3] = {i, j, k};
-  double result = a.alpha[d] * tile_at(t, c, i, j, k, i0, j0);
+  const int p[3] = {li, lj, dk};
+  double result = a.alpha[d] * tile_at(t, c, li, lj, dk, ps);
 #pragma unroll
   for (int dir = -1; dir <= 1; dir += 2) {
     int qa[3] = {p[0], p[1], p[2]}, qb[3] = {p[0], p[1], p[2]};
     qa[ta] += dir;
     qb[tb] += dir;
-    result += a.beta[ta] * tile_at(t, c, qa[0], qa[1], qa[2], i0, j0);
-    result += a.beta[tb] * tile_at(t, c, qb[0], qb[1], qb[2], i0, j0);
+    result += a.beta[ta] * tile_at(t, c, qa[0], qa[1], qa[2], ps);
+    result += a.beta[tb] * tile_at(t, c, qb[0], qb[1], qb[2], ps);
   }
 #pragma unroll
   for (int da = -1; da <= 1; da += 2)
@@ -98,7 +106,7 @@ __device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs<
       int q[3] = {p[0], p[1], p[2]};
       q[ta] += da;
       q[tb] += db;
-      result += delta * tile_at(t, c, q[0], q[1], q[2], i0, j0);
+      result += delta * tile_at(t, c, q[0], q[1], q[2], ps);
     }
   return result;
 }
@@ -108,9 +116,8 @@ __device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs<
 // own reach); tile points farther out, which exist only where a small grid
 // ends inside a tile, are stored as zero and never used.
 template <class F>
-__device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int k, int i0,
-                                           int j0) {
-  const int slot = plane_slot(k);
+__device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int k, int slot,
+                                           int i0, int j0) {
   constexpr int W = kTX + 2, H = kTY + 2, N = W * H;
   for (int c = 0; c < 3; ++c) {
     const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1);
@@ -124,7 +131,8 @@ __device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int 
 }
 
 template <class F>
-__global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> a) {
+__global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
+    cowan_magnetic_kernel(CowanArgs<F> a) {
   __shared__ ETile t;
   const GridT<F>& g = a.g;
   const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
@@ -132,17 +140,19 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
   const int k0 = blockIdx.z * kKChunk;
   const int k1 = min(k0 + kKChunk, g.nz + 1);
   const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
-  load_plane(t, a, k0 - 1, i0, j0);
-  load_plane(t, a, k0, i0, j0);
+  const int li = threadIdx.x + 1, lj = threadIdx.y + 1;
+  PlaneSlots ps = {{0, 1, 2}};
+  load_plane(t, a, k0 - 1, ps.s[0], i0, j0);
+  load_plane(t, a, k0, ps.s[1], i0, j0);
   for (int k = k0; k < k1; ++k) {
-    load_plane(t, a, k + 1, i0, j0);
+    load_plane(t, a, k + 1, ps.s[2], i0, j0);
     __syncthreads();
     if (i <= g.nx && j <= g.ny) {
       if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
-        const double dEzDy = tile_smoothed(t, a, 2, 1, i, j + 1, k, i0, j0) -
-                             tile_smoothed(t, a, 2, 1, i, j, k, i0, j0);
-        const double dEyDz = tile_smoothed(t, a, 1, 2, i, j, k + 1, i0, j0) -
-                             tile_smoothed(t, a, 1, 2, i, j, k, i0, j0);
+        const double dEzDy = tile_smoothed(t, a, 2, 1, li, lj + 1, 0, ps) -
+                             tile_smoothed(t, a, 2, 1, li, lj, 0, ps);
+        const double dEyDz = tile_smoothed(t, a, 1, 2, li, lj, 1, ps) -
+                             tile_smoothed(t, a, 1, 2, li, lj, 0, ps);
         double* bx = &g.b[0][b_index(g, 0, i, j, k)];
         double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
         const int s = a.my.ordinal[j];
@@ -152,10 +162,10 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
         *bx = v;
       }
       if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
-        const double dExDz = tile_smoothed(t, a, 0, 2, i, j, k + 1, i0, j0) -
-                             tile_smoothed(t, a, 0, 2, i, j, k, i0, j0);
-        const double dEzDx = tile_smoothed(t, a, 2, 0, i + 1, j, k, i0, j0) -
-                             tile_smoothed(t, a, 2, 0, i, j, k, i0, j0);
+        const double dExDz = tile_smoothed(t, a, 0, 2, li, lj, 1, ps) -
+                             tile_smoothed(t, a, 0, 2, li, lj, 0, ps);
+        const double dEzDx = tile_smoothed(t, a, 2, 0, li + 1, lj, 0, ps) -
+                             tile_smoothed(t, a, 2, 0, li, lj, 0, ps);
         double* by = &g.b[1][b_index(g, 1, i, j, k)];
         double v = *by - (dtdz * dExDz - dtdx * dEzDx);
         const int s = a.mx.ordinal[i];
@@ -165,10 +175,10 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
         *by = v;
       }
       if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
-        const double dEyDx = tile_smoothed(t, a, 1, 0, i + 1, j, k, i0, j0) -
-                             tile_smoothed(t, a, 1, 0, i, j, k, i0, j0);
-        const double dExDy = tile_smoothed(t, a, 0, 1, i, j + 1, k, i0, j0) -
-                             tile_smoothed(t, a, 0, 1, i, j, k, i0, j0);
+        const double dEyDx = tile_smoothed(t, a, 1, 0, li + 1, lj, 0, ps) -
+                             tile_smoothed(t, a, 1, 0, li, lj, 0, ps);
+        const double dExDy = tile_smoothed(t, a, 0, 1, li, lj + 1, 0, ps) -
+                             tile_smoothed(t, a, 0, 1, li, lj, 0, ps);
         double* bz = &g.b[2][b_index(g, 2, i, j, k)];
         double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
         const int sx = a.mx.ordinal[i];
@@ -183,6 +193,7 @@ __global__ void __launch_bounds__(kTX * kTY) cowan_magnetic_kernel(CowanArgs<F> 
       }
     }
     __syncthreads();
+    ps = PlaneSlots{{ps.s[1], ps.s[2], ps.s[0]}};
   }
 }
 

@@ -84,6 +84,15 @@ struct DetectorArgs {
   double* out;
 };
 
+// Cowan kernel geometry: 32x8 column tiles marching kCowanChunk z planes;
+// APRL_COWAN_MIN_BLOCKS resident blocks per SM bound its registers.
+#ifndef APRL_COWAN_CHUNK
+#define APRL_COWAN_CHUNK 16
+#endif
+#ifndef APRL_COWAN_MIN_BLOCKS
+#define APRL_COWAN_MIN_BLOCKS 5
+#endif
+constexpr int kCowanTileX = 32, kCowanTileY = 8, kCowanChunk = APRL_COWAN_CHUNK;
 template <class F> __global__ void cowan_magnetic_kernel(CowanArgs<F> a);
 template <class F> __global__ void electric_preview_kernel(PreviewArgs<F> a);
 template <class F> __global__ void electric_commit_kernel(GridT<F> g);

@@ -860,9 +860,10 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   ca.mx = r->mprof[0].view();
   ca.my = r->mprof[1].view();
   for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
-  // 32x8 column tiles, 16-plane z chunks (kTX, kTY, kKChunk in fields.cu).
-  const dim3 cblock(32, 8);
-  const dim3 cgrid(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), blocks_for(c.nz + 1, 16));
+  // Column tiles marching z chunks (fields.cuh: kCowanTileX/Y, kCowanChunk).
+  const dim3 cblock(kCowanTileX, kCowanTileY);
+  const dim3 cgrid(blocks_for(c.nx + 1, kCowanTileX), blocks_for(c.ny + 1, kCowanTileY),
+                   blocks_for(c.nz + 1, kCowanChunk));
   TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel<F>, cgrid, cblock, ca));
   r->stage = 1;
   return APRL_OK;
