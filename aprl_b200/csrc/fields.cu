@@ -63,7 +63,7 @@ __device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, in
 // bit-identical to the reference.  Each B node is updated by the
 // curl, then by its CPML terms in the reference's term order (0,2,1),
 // (1,2,0), (2,1,0), (2,0,1), reusing the curl's smoothed difference.
-constexpr int kTX = kCowanTileX, kTY = kCowanTileY, kKChunk = kCowanChunk;
+constexpr int kTX = kCowanTileX, kTY = kCowanTileY;
 
 struct ETile {
   double v[3][3][kTY + 2][kTX + 2];  // [component][plane slot][y][x]
@@ -137,8 +137,8 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
   const GridT<F>& g = a.g;
   const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  const int k0 = blockIdx.z * kKChunk;
-  const int k1 = min(k0 + kKChunk, g.nz + 1);
+  const int k0 = blockIdx.z * a.chunk;
+  const int k1 = min(k0 + a.chunk, g.nz + 1);
   const double dtdx = g.dt / g.dx, dtdy = g.dt / g.dy, dtdz = g.dt / g.dz;
   const int li = threadIdx.x + 1, lj = threadIdx.y + 1;
   PlaneSlots ps = {{0, 1, 2}};
@@ -364,10 +364,12 @@ __global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_
   }
 }
 
-// Binary32 copy of B (same ring layout) for the FP32-mixed gathers.
-__global__ void b_shadow_kernel(const double* b, float* out, long long n) {
+// Binary32 copy of B (same ring layout) for the FP32-mixed gathers; one
+// launch for the three components (blockIdx.y).
+__global__ void b_shadow_kernel(BShadowArgs a) {
+  const int c = blockIdx.y;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (float)b[i];
+  if (i < a.n[c]) a.out[c][i] = (float)a.b[c][i];
 }
 
 // Lab detector field plane (src/lab_detectors.cpp:39-99, 2836-2905).

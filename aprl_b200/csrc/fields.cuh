@@ -50,6 +50,7 @@ struct CowanArgs {
   double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
   CpmlAxis mx, my;       // magnetic profiles (half-integer positions)
   CpmlHistory h[4];      // magnetic histories 0 (Bx,y) 3 (By,x) 4 (Bz,x) 5 (Bz,y)
+  int chunk;             // z planes marched by one block
 };
 
 template <class F>
@@ -84,8 +85,9 @@ struct DetectorArgs {
   double* out;
 };
 
-// Cowan kernel geometry: 32x8 column tiles marching kCowanChunk z planes;
-// APRL_COWAN_MIN_BLOCKS resident blocks per SM bound its registers.
+// Cowan kernel geometry: 32x8 column tiles, each block marching up to
+// kCowanChunk z planes (fewer on small grids, so that there are enough
+// blocks); APRL_COWAN_MIN_BLOCKS resident blocks per SM bound its registers.
 #ifndef APRL_COWAN_CHUNK
 #define APRL_COWAN_CHUNK 16
 #endif
@@ -101,6 +103,11 @@ template <class F> __global__ void shift_insert_kernel(ShiftArgs<F> a);
 template <class F> __global__ void detector_plane_kernel(DetectorArgs<F> a);
 template <class W>
 __global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_current);
-__global__ void b_shadow_kernel(const double* b, float* out, long long n);
+struct BShadowArgs {
+  const double* b[3];
+  float* out[3];
+  long long n[3];
+};
+__global__ void b_shadow_kernel(BShadowArgs a);
 
 }  // namespace aprl_gpu

@@ -662,6 +662,15 @@ __device__ void add_prescribed_box(const PushArgs<F>& a, const double pos[3], do
   }
 }
 
+// Adds the number of lanes with `flag` to *counter with one atomic per
+// converged group of the warp.
+__device__ __forceinline__ void count_lanes(unsigned long long* counter, bool flag) {
+  const unsigned group = __activemask();
+  const unsigned ballot = __ballot_sync(group, flag);
+  if (ballot && (threadIdx.x & 31) == __ffs(group) - 1)
+    atomicAdd(counter, (unsigned long long)__popc(ballot));
+}
+
 // ---------------------------------------------------------------------------
 // particle boundaries (src/particle_boundary.cpp)
 struct Hit {
@@ -855,6 +864,7 @@ __global__ void carrier_kernel(CarrierArgs<F> a) {
   bool kept = false;
   const unsigned err = carrier_segment(a.g, a.shape, a.region, c, start, 0.0, a.counters, kept);
   if (err) raise_error(a.status, err, (unsigned long long)n);
+  count_lanes(&a.counters->carriers_kept, kept);
   a.keep[n] = kept ? 1 : 0;
   a.out.px[n] = c.pos[0]; a.out.py[n] = c.pos[1]; a.out.pz[n] = c.pos[2];
   a.out.vx[n] = c.vel[0]; a.out.vy[n] = c.vel[1]; a.out.vz[n] = c.vel[2];
@@ -1138,12 +1148,10 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
     atomicAdd(&a.counters->direct_charge[selected.face], q);
   }
   if (err) raise_error(a.status, err, (unsigned long long)n);
-  // Held particles retained by this trial, one atomic per converged group.
-  const bool held = !err && action == 0 && frozen1;
-  const unsigned group = __activemask();
-  const unsigned held_ballot = __ballot_sync(group, held);
-  if (held_ballot && (threadIdx.x & 31) == __ffs(group) - 1)
-    atomicAdd(&a.counters->held, (unsigned long long)__popc(held_ballot));
+  // Retained, held and newborn-carrier counts (one atomic per warp group).
+  count_lanes(&a.counters->held, !err && action == 0 && frozen1);
+  count_lanes(&a.counters->retained, action == 0);
+  count_lanes(&a.counters->born_kept, born_kept);
   a.x1[n] = pos[0]; a.y1[n] = pos[1]; a.z1[n] = pos[2];
   a.ux1[n] = u[0]; a.uy1[n] = u[1]; a.uz1[n] = u[2];
   a.frozen1[n] = frozen1 ? 1 : 0;

@@ -57,6 +57,10 @@ struct TrialCounters {
   double cropped_charge;
   unsigned long long activations; // held particles crossing the activation plane
   unsigned long long held;        // held particles retained by the trial
+  // Compaction sizes, so the commit needs no further host round trip.
+  unsigned long long retained;    // particles with action 0
+  unsigned long long born_kept;   // newborn carriers kept
+  unsigned long long carriers_kept;  // existing carriers kept
 };
 
 struct ResidualSums {

@@ -710,22 +710,17 @@ void add_counters(TrialCounters& to, const TrialCounters& from) {
   to.activations += from.activations;
 }
 
-// Stable compaction of `n` flagged elements; returns the kept count.
-aprl_status compact_count(aprl_run* r, const unsigned char* flag, unsigned char want, size_t n,
-                          unsigned long long* kept) {
-  *kept = 0;
+// Block offsets of a stable compaction of `n` flagged elements (the kept
+// count is known to the caller).
+aprl_status compact_offsets(aprl_run* r, const unsigned char* flag, unsigned char want,
+                            size_t n) {
   if (n == 0) return APRL_OK;
   TRY(ensure_scan(r, n));
   const unsigned blocks = blocks_for(n, kScanBlock);
   TRY(launch(r, kFlagCount, flag_count_kernel, dim3(blocks), dim3(kScanBlock), flag, want,
              (long long)n, r->scan_count));
-  TRY(launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
-             (const unsigned*)r->scan_count, (int)blocks, r->scan_offset, r->scan_total));
-  CUDA_TRY(cudaMemcpyAsync(r->h_total, r->scan_total, sizeof(unsigned long long),
-                           cudaMemcpyDeviceToHost, r->stream));
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
-  *kept = *r->h_total;
-  return APRL_OK;
+  return launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
+                (const unsigned*)r->scan_count, (int)blocks, r->scan_offset, r->scan_total);
 }
 
 // Counting sort of the particle storage by 4x4x4 cell tiles
@@ -860,10 +855,17 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   ca.mx = r->mprof[0].view();
   ca.my = r->mprof[1].view();
   for (int h = 0; h < 4; ++h) ca.h[h] = r->hist[h].view();
-  // Column tiles marching z chunks (fields.cuh: kCowanTileX/Y, kCowanChunk).
+  // Column tiles marching z chunks (fields.cuh: kCowanTileX/Y, kCowanChunk):
+  // at most kCowanChunk planes per block, fewer when that leaves fewer than
+  // about four blocks per SM.
   const dim3 cblock(kCowanTileX, kCowanTileY);
+  const unsigned columns = blocks_for(c.nx + 1, kCowanTileX) * blocks_for(c.ny + 1, kCowanTileY);
+  const size_t planes = c.nz + 1;
+  const size_t target = 4 * 148;
+  ca.chunk = (int)std::min<size_t>(
+      kCowanChunk, std::max<size_t>(2, (planes * columns + target - 1) / target));
   const dim3 cgrid(blocks_for(c.nx + 1, kCowanTileX), blocks_for(c.ny + 1, kCowanTileY),
-                   blocks_for(c.nz + 1, kCowanChunk));
+                   blocks_for(planes, ca.chunk));
   TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel<F>, cgrid, cblock, ca));
   r->stage = 1;
   return APRL_OK;
@@ -885,10 +887,17 @@ aprl_status preview_electric_t(aprl_run* r) {
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
-  if (r->fp32)  // B is final for the step: its binary32 copy for the gathers
-    for (int a = 0; a < 3; ++a)
-      TRY(launch(r, kBShadow, b_shadow_kernel, dim3(blocks_for(b_count(c, a), 256)), dim3(256),
-                 (const double*)r->b[a], r->bshadow[a], (long long)b_count(c, a)));
+  if (r->fp32) {  // B is final for the step: its binary32 copy for the gathers
+    BShadowArgs sa{};
+    size_t most = 0;
+    for (int a = 0; a < 3; ++a) {
+      sa.b[a] = r->b[a];
+      sa.out[a] = r->bshadow[a];
+      sa.n[a] = (long long)b_count(c, a);
+      most = std::max(most, b_count(c, a));
+    }
+    TRY(launch(r, kBShadow, b_shadow_kernel, dim3(blocks_for(most, 256), 3), dim3(256), sa));
+  }
   if (r->np)
     CUDA_TRY(cudaMemcpyAsync(r->slot_order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice,
                              r->stream));
@@ -1031,6 +1040,8 @@ aprl_status trial_t(aprl_run* r, double residual[4]) {
   }
   CUDA_TRY(cudaMemcpyAsync(r->h_sums, r->d_sums, sizeof(ResidualSums), cudaMemcpyDeviceToHost,
                            r->stream));
+  CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
+                           cudaMemcpyDeviceToHost, r->stream));
   TRY(check_device(r));
   double force;
   const unsigned long long bits = r->h_sums->force_bits;
@@ -1055,23 +1066,22 @@ aprl_status do_commit(aprl_run* r) {
   TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
              make_grid<double>(r)));
   r->cur = 1 - r->cur;
-  // Counters of the converged trial become cumulative.
-  CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
-                           cudaMemcpyDeviceToHost, r->stream));
+  // The counters of the converged trial (read back with its residual) give
+  // every compaction size: no host round trip in the commit.
+  const TrialCounters& tc = *r->h_counters;
+  const unsigned long long kept_old = r->nc ? tc.carriers_kept : 0;
+  const unsigned long long kept_born = r->np ? tc.born_kept : 0;
   // Carriers: surviving old carriers, then carriers born this step, in
   // particle order (retainedCarriers, src/simulation.cpp:4401-4405).
-  unsigned long long kept_old = 0, kept_born = 0;
-  TRY(compact_count(r, r->c_keep, 1, r->nc, &kept_old));
-  TRY(compact_count(r, r->born_keep, 1, r->np, &kept_born));
   TRY(reserve_carriers(r, kept_old + kept_born));
   if (r->nc) {
-    TRY(compact_count(r, r->c_keep, 1, r->nc, &kept_old));
+    TRY(compact_offsets(r, r->c_keep, 1, r->nc));
     TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->nc, kScanBlock)),
                dim3(kScanBlock), r->c_alt, r->c_out, (const unsigned char*)r->c_keep,
                (unsigned char)1, (long long)r->nc, (const unsigned*)r->scan_offset, 0ull));
   }
-  if (r->np) {
-    TRY(compact_count(r, r->born_keep, 1, r->np, &kept_born));
+  if (r->np && kept_born) {
+    TRY(compact_offsets(r, r->born_keep, 1, r->np));
     TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->np, kScanBlock)),
                dim3(kScanBlock), r->c_alt, r->born, (const unsigned char*)r->born_keep,
                (unsigned char)1, (long long)r->np, (const unsigned*)r->scan_offset,
@@ -1081,8 +1091,8 @@ aprl_status do_commit(aprl_run* r) {
   r->nc = kept_old + kept_born;
   // Particles: the retained list in order (src/simulation.cpp:4916, 5581).
   if (r->np) {
-    unsigned long long kept = 0;
-    TRY(compact_count(r, r->action, 0, r->np, &kept));
+    const unsigned long long kept = tc.retained;
+    TRY(compact_offsets(r, r->action, 0, r->np));
     TRY(launch(r, kGatherParticles, gather_particles_kernel, dim3(blocks_for(r->np, kScanBlock)),
                dim3(kScanBlock), r->p_alt, r->p, (const double*)r->x1, (const double*)r->y1,
                (const double*)r->z1, (const double*)r->ux1, (const double*)r->uy1,
@@ -1093,9 +1103,8 @@ aprl_status do_commit(aprl_run* r) {
     r->np = kept;
     TRY(sort_particles(r));
   }
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
-  add_counters(r->cumulative, *r->h_counters);
-  r->held = r->h_counters->held;
+  add_counters(r->cumulative, tc);
+  r->held = tc.held;
   r->stage = 4;
   return APRL_OK;
 }
@@ -1119,7 +1128,9 @@ aprl_status shift_insert_t(aprl_run* r) {
                 dim3(blocks_for(max_row, 32), blocks_for(ydim, 8), 14), dim3(32, 8), sa);
 }
 
-aprl_status do_shift(aprl_run* r) {
+// `defer_check`: leave the device status to the next read (the stepping loop
+// reads it with the next trial's residual and once at its end).
+aprl_status do_shift(aprl_run* r, bool defer_check = false) {
   if (r->stage != 4)
     return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
   const aprl_run_config& c = r->cfg;
@@ -1138,24 +1149,26 @@ aprl_status do_shift(aprl_run* r) {
                (const double*)r->p.z, (const unsigned char*)r->p.frozen, (long long)r->np,
                r->origin[2], r->d_status));
   if (r->nc) {
+    // Crop flags and counts in one round trip (with the device status).
     const double upper = std::fma(static_cast<double>(c.nz), c.dz, r->origin[2]);
     CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
     TRY(launch(r, kCropFlags, crop_flags_kernel, dim3(blocks_for(r->nc, 256)), dim3(256), r->c,
                (long long)r->nc, upper, r->origin[2], r->c_keep, r->d_counters, r->d_status));
-    unsigned long long kept = 0;
-    TRY(compact_count(r, r->c_keep, 1, r->nc, &kept));
+    CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
+                             cudaMemcpyDeviceToHost, r->stream));
+    TRY(check_device(r));
+    const unsigned long long kept = r->nc - r->h_counters->cropped;
+    TRY(compact_offsets(r, r->c_keep, 1, r->nc));
     TRY(launch(r, kGatherCarriers, gather_carriers_kernel, dim3(blocks_for(r->nc, kScanBlock)),
                dim3(kScanBlock), r->c_alt, r->c, (const unsigned char*)r->c_keep,
                (unsigned char)1, (long long)r->nc, (const unsigned*)r->scan_offset, 0ull));
     std::swap(r->c, r->c_alt);
     r->nc = kept;
-    CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
-                             cudaMemcpyDeviceToHost, r->stream));
-    CUDA_TRY(cudaStreamSynchronize(r->stream));
     r->cumulative.cropped += r->h_counters->cropped;
     r->cumulative.cropped_charge += r->h_counters->cropped_charge;
+  } else if (!defer_check) {
+    TRY(check_device(r));
   }
-  TRY(check_device(r));
   r->stage = 0;
   return APRL_OK;
 }
@@ -1791,9 +1804,9 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
     r->last_force = force;
     r->last_work = work;
     TRY(do_commit(r));
-    TRY(do_shift(r));
+    TRY(do_shift(r, true));
   }
-  return APRL_OK;
+  return check_device(r);
 }
 
 aprl_status aprl_run_get_stats(const aprl_run* r, aprl_step_stats* st) {
