@@ -133,9 +133,27 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
         return particles * (48 + 16 + 48 + 8 + 48)
     if kernel == "guess_gather":        # read x,u,flags; write nextE/B
         return particles * (48 + 1 + 48)
+    if kernel == "orbit_sum":           # read E*, J, E^n; write S, per E node
+        return 4 * 8 * 3 * n_cells
     if kernel == "carrier":             # read + write 8 words
         return carriers * 128
     return None
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu capture of this workload's grid with 250k particles, cold L2: per
+# particle for the particle kernels, per launch for the grid passes.
+MEASURED_TRAFFIC = {"push_deposit": ("particle", 349.0),
+                    "residual": ("particle", 473.0),
+                    "cowan_magnetic": ("launch", 669.9e6),
+                    "orbit_sum": ("launch", 788.7e6)}
+
+
+def measured_traffic(kernel, particles):
+    kind, value = MEASURED_TRAFFIC.get(kernel, (None, None))
+    if kind == "particle":
+        return value * particles
+    return value
 
 
 # ---------------------------------------------------------------------------
@@ -269,7 +287,10 @@ def run_ours(args):
         roofline = {"bound": "hbm", "kernel": name,
                     "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": (achieved / peak) if achieved else None,
-                    "peak_source": peak_kind, "traffic": None,
+                    "peak_source": peak_kind,
+                    "traffic": measured_traffic(name, mean_particles),
+                    "traffic_source": "ncu DRAM bytes of the 250k-particle capture of this "
+                                      "grid, scaled per particle for particle kernels",
                     "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
                     "launches": count}
     kernels = {k: {"ms": v[0], "launches": v[1],
