@@ -368,8 +368,13 @@ __global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_
 // launch for the three components (blockIdx.y).
 __global__ void b_shadow_kernel(BShadowArgs a) {
   const int c = blockIdx.y;
+  // Select by branch: a run-time index into the parameter arrays would copy
+  // them to local memory in every thread.
+  const double* b = c == 0 ? a.b[0] : (c == 1 ? a.b[1] : a.b[2]);
+  float* out = c == 0 ? a.out[0] : (c == 1 ? a.out[1] : a.out[2]);
+  const long long n = c == 0 ? a.n[0] : (c == 1 ? a.n[1] : a.n[2]);
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < a.n[c]) a.out[c][i] = (float)a.b[c][i];
+  if (i < n) out[i] = (float)b[i];
 }
 
 // Lab detector field plane (src/lab_detectors.cpp:39-99, 2836-2905).

@@ -215,10 +215,12 @@ def held_beta_z(u_lab, boost_gamma):
 
 def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
                    emittance_n, energy_spread, seed=17, margin_cells=3,
-                   z_fraction=(0.05, 0.95), z_range=None):
+                   z_fraction=(0.05, 0.95), z_range=None, uniform_z=False):
     """Box-frame snapshot of a lab-frame Gaussian electron bunch, truncated
     to the moving window's trusted particle region (inside the transverse
-    CPML by `margin_cells`, above the inlet guard, below the exit plane)."""
+    CPML by `margin_cells`, above the inlet guard, below the exit plane).
+    uniform_z: the window holds a slice of a bunch much longer than it, so z
+    is drawn uniformly over the slice (seeded random longitudinal phases)."""
     gamma_lab = energy_ev / ELECTRON_REST_EV
     u0 = gamma_beta_from_gamma(gamma_lab)
     boost = cfg.boost_gamma
@@ -249,7 +251,10 @@ def gaussian_bunch(cfg, count, charge_c, energy_ev, sigma_xy, sigma_z_lab,
         index = np.uint64(int(index) + block)
         x = sigma_xy * gaussian(seed, ids, 0)
         y = sigma_xy * gaussian(seed, ids, 1)
-        z = z_center + sigma_z_box * gaussian(seed, ids, 2)
+        if uniform_z:
+            z = z_lo + (z_hi - z_lo) * _uniform_open(seed ^ 0x5DEECE66D, ids, 7)
+        else:
+            z = z_center + sigma_z_box * gaussian(seed, ids, 2)
         pseed = seed ^ 0xD6E8FEB86659FD93
         sigma_u = emittance_n / sigma_xy
         ux = sigma_u * gaussian(pseed, ids, 0)
@@ -323,9 +328,11 @@ def synthetic_fields(cfg, amplitude=1.0e4, seed=11):
 
 # --------------------------------------------------------------------------
 # named workloads (benchmark configurations and small parity cases)
-def drift_c1(steps=200, particles=100_000, shape="linear-binomial3", seed=17):
+def drift_c1(steps=200, particles=100_000, shape="linear-binomial3", seed=17,
+             precision="fp64"):
     """Plain FP64 drift: 64x64x256 cells, dx=dy=5 um, dz=2 um, 8-cell CPML."""
-    cfg = make_config(64, 64, 256, 5e-6, 5e-6, 2e-6, 8, 10.0, shape, steps)
+    cfg = with_precision(make_config(64, 64, 256, 5e-6, 5e-6, 2e-6, 8, 10.0, shape, steps),
+                         precision)
     bunch = gaussian_bunch(cfg, particles, 100e-12, 1e9, 50e-6, 20e-6, 1e-6,
                            1e-4, seed=seed)
     return Workload("drift-64x64x256", cfg, bunch, synthetic_reference(cfg),
@@ -347,6 +354,31 @@ def dipole_c2(steps=2000, particles=1_000_000, shape="linear-binomial3",
                     description={"cells": [128, 128, 512], "particles": particles,
                                  "shape": shape, "boost_gamma": 10.0,
                                  "dipole_T": 1.0, "precision": precision})
+
+
+def undulator_c3(steps=5000, particles=4_000_000, shape="linear-binomial3", seed=17,
+                 precision="fp32-mixed"):
+    """Planar-undulator beam: period 3 cm, K = 1, gamma_lab 3000 (energy
+    spread 1e-4, sigma_xy 30 um, sigma_z 50 um lab), boosted to the
+    undulator-resonant frame gamma_b = gamma / sqrt(1 + K^2/2)
+    (utilities/undulator_resonance.cpp:155-157); 128x128x2048 cells.  In that
+    frame the bunch is far longer than the window, so the window holds a
+    slice with uniformly random longitudinal phases (shot noise)."""
+    k_parameter, gamma_lab = 1.0, 3000.0
+    boost = gamma_lab / math.sqrt(1.0 + 0.5 * k_parameter ** 2)
+    cfg = with_precision(make_config(128, 128, 2048, 4e-6, 4e-6, 1e-6, 10, boost, shape, steps,
+                                     magnets=[planar_undulator(k_parameter, 0.03, -1.0, 1000)]),
+                         precision)
+    # weight ~355 per macro-particle
+    charge = 355.0 * particles * ELEMENTARY_CHARGE
+    bunch = gaussian_bunch(cfg, particles, charge, gamma_lab * ELECTRON_REST_EV, 30e-6, 50e-6,
+                           1e-6, 1e-4, seed=seed, uniform_z=True)
+    return Workload("undulator-128x128x2048", cfg, bunch, synthetic_reference(cfg),
+                    steps=steps,
+                    description={"cells": [128, 128, 2048], "particles": particles,
+                                 "shape": shape, "boost_gamma": boost,
+                                 "undulator": {"period_m": 0.03, "K": k_parameter},
+                                 "precision": precision})
 
 
 def split_held(cfg, bunch):

@@ -43,9 +43,12 @@ def parse_args(argv=None):
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--particles", type=int, default=1_000_000)
+    p.add_argument("--workload", choices=["dipole", "drift", "undulator"], default="dipole",
+                   help="dipole: 128x128x512, 1M particles (the headline); drift: "
+                        "64x64x256, 100k; undulator: 128x128x2048, 4M, FP32-mixed")
+    p.add_argument("--particles", type=int, default=None)
     p.add_argument("--shape", default="linear-binomial3")
-    p.add_argument("--precision", choices=["fp64", "fp32-mixed"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "fp32-mixed"], default=None)
     p.add_argument("--no-fp32-arm", action="store_true",
                    help="skip the FP32-mixed comparison pass of an FP64 run")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -58,7 +61,31 @@ def parse_args(argv=None):
     p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--scan-slots", type=int, default=4)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
-    return p.parse_args(argv)
+    args = p.parse_args(argv)
+    defaults = {"dipole": (1_000_000, "fp64"), "drift": (100_000, "fp64"),
+                "undulator": (4_000_000, "fp32-mixed")}[args.workload]
+    if args.particles is None:
+        args.particles = defaults[0]
+    if args.precision is None:
+        args.precision = defaults[1]
+    if args.workload != "dipole":
+        # the scan objects and the CPU slice belong to the dipole headline
+        args.no_scan = True
+        args.no_cpu_baseline = True
+    return args
+
+
+WORKLOADS = {
+    "dipole": (lambda steps, args, seed: workloads.dipole_c2(
+        steps=steps, particles=args.particles, shape=args.shape, seed=seed,
+        precision=args.precision), "uniform 1 T lab dipole"),
+    "drift": (lambda steps, args, seed: workloads.drift_c1(
+        steps=steps, particles=args.particles, shape=args.shape, seed=seed,
+        precision=args.precision), "none (free drift)"),
+    "undulator": (lambda steps, args, seed: workloads.undulator_c3(
+        steps=steps, particles=args.particles, shape=args.shape, seed=seed,
+        precision=args.precision), "planar undulator, period 3 cm, K = 1"),
+}
 
 
 def measured_peaks():
@@ -181,8 +208,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     K, W = args.steps, args.warmup
     total_steps = W + 2 * K + 4
-    w = workloads.dipole_c2(steps=total_steps, particles=args.particles, shape=args.shape,
-                            seed=17 + rank, precision=args.precision)
+    make, magnet = WORKLOADS[args.workload]
+    w = make(total_steps, args, 17 + rank)
     cfg = w.config
     lib = native.load()
     run = native.Run(lib, cfg, stream=stream.cuda_stream)
@@ -306,7 +333,7 @@ def run_ours(args):
         "config": {"workload": w.name, "cells": [cfg.nx, cfg.ny, cfg.nz],
                    "particles": args.particles, "shape": args.shape,
                    "precision": "fp64-drop-in" if args.precision == "fp64" else "fp32-mixed",
-                   "magnet": "uniform 1 T lab dipole",
+                   "magnet": magnet,
                    "boost_gamma": cfg.boost_gamma, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (fields + particles > 126 MB)"},
         "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
