@@ -265,23 +265,30 @@ __device__ __forceinline__ bool clip_open_orbit(const GridT<F>& g, const double 
 // Orbit average of 1/2 (E_new + E^n) with the shape weights, read from the
 // orbit sum S = E_new + E^n that orbit_sum_kernel forms once per trial
 // (E_new = E* - dt/eps0 J for the residual, E* for the first-trial guess).
+// Three component arrays passed by value, so that constant component
+// indices keep the pointers in registers.
+template <class W>
+struct Ptr3 {
+  const W* p[3];
+};
+
 template <class W, class F>
 struct ElectricVisitor {
   static constexpr bool kF3Segment = true;
   using Weight = W;
   const GridT<F>* g;
-  const W* const* s;     // orbit sum S = E_new + E^n per E node (ring layout)
+  Ptr3<W> s;             // orbit sum S = E_new + E^n per E node (ring layout)
   W r[3];
   __device__ __forceinline__ void operator()(int d, long long i, long long j, long long k, W w) {
     const GridT<F>& G = *g;
     if (i < 0 || j < 0 || i >= e_nx(G, d) || j >= e_ny(G, d)) return;
     if (k < 0 || k >= e_nz(G, d)) return;
-    r[d] += W(.5) * w * s[d][e_index(G, d, (int)i, (int)j, (int)k)];
+    r[d] += W(.5) * w * s.p[d][e_index(G, d, (int)i, (int)j, (int)k)];
   }
 
   // One accumulation .5*w*(E_new + E^n) at the ring offset n of a node.
   __device__ __forceinline__ W term(int d, size_t n, size_t, W w) const {
-    return W(.5) * w * s[d][n];
+    return W(.5) * w * s.p[d][n];
   }
 
   // binomialXZSegment specialised for the gather.  When the whole 4x2x4
@@ -368,7 +375,7 @@ struct ElectricVisitor {
 };
 
 template <class W, class F>
-__device__ __forceinline__ W open_b(const GridT<F>& g, const W* const* bsrc, int a, long long i,
+__device__ __forceinline__ W open_b(const GridT<F>& g, const Ptr3<W>& bsrc, int a, long long i,
                                     long long j, long long k) {
   const long long nxc = b_nx(g, a), nyc = b_ny(g, a), nzc = b_nz(g, a);
   if (i < 0) i = 0;
@@ -377,14 +384,14 @@ __device__ __forceinline__ W open_b(const GridT<F>& g, const W* const* bsrc, int
   if (j > nyc - 1) j = nyc - 1;
   if (k < 0) k = 0;
   if (k >= nzc) k = nzc - 1;
-  return bsrc[a][b_index(g, a, (int)i, (int)j, (int)k)];
+  return bsrc.p[a][b_index(g, a, (int)i, (int)j, (int)k)];
 }
 
 // binomialXZMagneticSample (src/source_coupling_math.h:142-167).  Rows of
 // the 4x2x4 stencil that lie inside the component are read without the
 // open-face clamps; the clamped form runs otherwise.  Same order either way.
 template <class W, class F>
-__device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const W* const* bsrc,
+__device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const Ptr3<W>& bsrc,
                                                      const double p[3], double value[3]) {
   const double h[3] = {g.dx, g.dy, g.dz};
 #pragma unroll
@@ -404,7 +411,7 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const W*
     W v = W(0.);
     if (cell[0] >= 1 && cell[0] + 2 <= nxc - 1 && cell[1] >= 0 && cell[1] + 1 <= nyc - 1 &&
         cell[2] >= 1 && cell[2] + 2 <= nzc - 1) {
-      const W* base = bsrc[a];
+      const W* base = bsrc.p[a];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const size_t plane = (size_t)ring((int)cell[2] - 1 + k, g.zb_b[a], (int)nzc) * nyc;
@@ -432,7 +439,7 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const W*
 
 // magneticSample(bounds=false, halo, openFaces=true) (src/source_coupling_math.h:122-138).
 template <class W, class F>
-__device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const W* const* bsrc,
+__device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const Ptr3<W>& bsrc,
                                                    const double p[3], double value[3]) {
   const double ds[3] = {g.dx, g.dy, g.dz};
   int cell[2][3];
@@ -463,7 +470,7 @@ __device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const W* c
 template <class W, class F>
 __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
-                                                    const W* const* orbit, double out[3]) {
+                                                    const Ptr3<W>& orbit, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
@@ -478,7 +485,7 @@ __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape
 template <class W, class F>
 __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape,
                                                     const double a[3], const double b[3],
-                                                    const W* const* bsrc, double out[3]) {
+                                                    const Ptr3<W>& bsrc, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
@@ -1000,10 +1007,10 @@ __global__ void guess_gather_kernel(PushArgs<F> a) {
   const double guess[3] = {s.start[0] + sc * u[0], s.start[1] + sc * u[1],
                            s.start[2] + sc * u[2]};
   double ne[3], nb[3];
-  const W* orbit[3] = {static_cast<const W*>(a.orbit[0]), static_cast<const W*>(a.orbit[1]),
-                       static_cast<const W*>(a.orbit[2])};
-  const W* bsrc[3] = {static_cast<const W*>(a.bgather[0]), static_cast<const W*>(a.bgather[1]),
-                      static_cast<const W*>(a.bgather[2])};
+  const Ptr3<W> orbit{{static_cast<const W*>(a.orbit[0]), static_cast<const W*>(a.orbit[1]),
+                       static_cast<const W*>(a.orbit[2])}};
+  const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]), static_cast<const W*>(a.bgather[1]),
+                      static_cast<const W*>(a.bgather[2])}};
   unsigned err = gather_electric(a.g, a.shape, s.start, guess, orbit, ne);
   if (!err) err = gather_magnetic(a.g, a.shape, s.start, guess, bsrc, nb);
   if (err) raise_error(a.status, err, (unsigned long long)n);
@@ -1208,11 +1215,12 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     }
     const double last[3] = {a.x1[n], a.y1[n], a.z1[n]};
     double ne[3], nb[3];
-    const W* orbit[3] = {static_cast<const W*>(a.orbit[0]), static_cast<const W*>(a.orbit[1]),
-                         static_cast<const W*>(a.orbit[2])};
-    const W* bsrc[3] = {static_cast<const W*>(a.bgather[0]),
+    const Ptr3<W> orbit{{static_cast<const W*>(a.orbit[0]),
+                         static_cast<const W*>(a.orbit[1]),
+                         static_cast<const W*>(a.orbit[2])}};
+    const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]),
                         static_cast<const W*>(a.bgather[1]),
-                        static_cast<const W*>(a.bgather[2])};
+                        static_cast<const W*>(a.bgather[2])}};
     unsigned err = gather_electric(a.g, a.shape, first, last, orbit, ne);
     if (!err) err = gather_magnetic(a.g, a.shape, first, last, bsrc, nb);
     if (err) {
