@@ -131,6 +131,29 @@ class StepStats(C.Structure):
         return out
 
 
+class EnergyLedger(C.Structure):
+    """aprl_energy_ledger: the moving-window energy ledger and the field and
+    particle energy sums of the current state (joules, watts)."""
+    _fields_ = [
+        ("inlet_overwrite_energy", C.c_double),
+        ("inserted_energy", C.c_double),
+        ("cropped_energy", C.c_double),
+        ("remap_energy", C.c_double),
+        ("outward_energy", C.c_double * 6),
+        ("overwrite_events", C.c_uint64),
+        ("flux_steps", C.c_uint64),
+        ("remap_steps", C.c_uint64),
+        ("field_energy_interior", C.c_double),
+        ("boundary_power", C.c_double * 6),
+        ("particle_kinetic", C.c_double),
+        ("particle_total", C.c_double),
+        ("represented_electrons", C.c_double),
+        ("particles", C.c_uint64),
+    ]
+
+    as_dict = StepStats.as_dict
+
+
 def field_shape(config, component):
     """Yee extents (nx_c, ny_c, nz_c) of an ABI component (x fastest)."""
     cells = (config.nx, config.ny, config.nz)

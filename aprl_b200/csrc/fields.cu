@@ -232,7 +232,10 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       }
     }
     if (j == 0 || j == g.ny) v = 0.0;
-    if (k == 0) v = inlet_value(a.inlet, 0, i, j);
+    if (k == 0) {
+      if (a.pre_inlet[0]) a.pre_inlet[0][(size_t)j * g.nx + i] = v;
+      v = inlet_value(a.inlet, 0, i, j);
+    }
     g.e_star[0][n] = v;
   }
   if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
@@ -250,7 +253,10 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       }
     }
     if (i == 0 || i == g.nx) v = 0.0;
-    if (k == 0) v = inlet_value(a.inlet, 1, i, j);
+    if (k == 0) {
+      if (a.pre_inlet[1]) a.pre_inlet[1][(size_t)j * (g.nx + 1) + i] = v;
+      v = inlet_value(a.inlet, 1, i, j);
+    }
     g.e_star[1][n] = v;
   }
   if (k < g.nz) {  // Ez (nx+1, ny+1, nz)

@@ -59,6 +59,7 @@ struct PreviewArgs {
   CpmlAxis ex_prof, ey_prof;  // electric profiles (integer positions)
   CpmlHistory h[4];      // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
   InletTable inlet;      // reference(a, i, j, offset, step+1)
+  double* pre_inlet[2];  // when set: Ex, Ey of plane 0 before the inlet overwrite
 };
 
 struct InletPlaneArgs {

@@ -1,0 +1,245 @@
+// ledger.cu -- double-double reductions of the moving-window energy ledger.
+#include "ledger.cuh"
+
+namespace aprl_gpu {
+
+constexpr double kElectronMass = 9.1093837139e-31;  // src/eb_field.cpp:18
+
+namespace {
+
+// Knuth's TwoSum: s + e == a + b exactly.
+__host__ __device__ __forceinline__ DD two_sum(double a, double b) {
+  const double s = a + b;
+  const double bb = s - a;
+  const double e = (a - (s - bb)) + (b - bb);
+  return DD{s, e};
+}
+
+// Requires |a| >= |b| (or a == 0).
+__host__ __device__ __forceinline__ DD quick_two_sum(double a, double b) {
+  const double s = a + b;
+  return DD{s, b - (s - a)};
+}
+
+// Dekker's exact product through a fused multiply-add.
+__host__ __device__ __forceinline__ DD two_prod(double a, double b) {
+  const double p = a * b;
+  return DD{p, fma(a, b, -p)};
+}
+
+__host__ __device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD s = two_sum(a.hi, b.hi);
+  const DD t = two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = quick_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+
+__host__ __device__ __forceinline__ DD dd_neg(DD a) { return DD{-a.hi, -a.lo}; }
+
+__host__ __device__ __forceinline__ DD dd_mul(DD a, double b) {
+  DD p = two_prod(a.hi, b);
+  p.lo += a.lo * b;
+  return quick_two_sum(p.hi, p.lo);
+}
+
+// Division of a double-double by a double (QD library, Hida-Li-Bailey).
+__host__ __device__ __forceinline__ DD dd_div(DD a, double b) {
+  const double q1 = a.hi / b;
+  const DD p = two_prod(q1, b);
+  const DD s = two_sum(a.hi, -p.hi);
+  double e = s.lo - p.lo;
+  e += a.lo;
+  const double q2 = (s.hi + e) / b;
+  return quick_two_sum(q1, q2);
+}
+
+__device__ __forceinline__ double ex_at(const LedgerArgs& a, int i, int j, int k, bool sub) {
+  if (sub && k == 0) return a.pre[0][(size_t)j * a.g.nx + i];
+  return a.g.e_old[0][e_index(a.g, 0, i, j, k)];
+}
+__device__ __forceinline__ double ey_at(const LedgerArgs& a, int i, int j, int k, bool sub) {
+  if (sub && k == 0) return a.pre[1][(size_t)j * (a.g.nx + 1) + i];
+  return a.g.e_old[1][e_index(a.g, 1, i, j, k)];
+}
+__device__ __forceinline__ double ez_at(const LedgerArgs& a, int i, int j, int k) {
+  return a.g.e_old[2][e_index(a.g, 2, i, j, k)];
+}
+__device__ __forceinline__ double b_at(const LedgerArgs& a, int c, int i, int j, int k) {
+  return a.g.b[c][b_index(a.g, c, i, j, k)];
+}
+
+struct CellFields {
+  double e[3], b[3];
+};
+
+// The cell's collocated E and B of fieldEnergyDensityCell and
+// poyntingComponentCell (src/eb_field.cpp:715-781), same operation order.
+__device__ __forceinline__ CellFields collocate(const LedgerArgs& a, int i, int j, int k,
+                                                bool sub) {
+  CellFields f;
+  f.e[0] = 0.25 * (((ex_at(a, i, j, k, sub) + ex_at(a, i, j + 1, k, sub)) +
+                    ex_at(a, i, j, k + 1, sub)) + ex_at(a, i, j + 1, k + 1, sub));
+  f.e[1] = 0.25 * (((ey_at(a, i, j, k, sub) + ey_at(a, i + 1, j, k, sub)) +
+                    ey_at(a, i, j, k + 1, sub)) + ey_at(a, i + 1, j, k + 1, sub));
+  f.e[2] = 0.25 * (((ez_at(a, i, j, k) + ez_at(a, i + 1, j, k)) + ez_at(a, i, j + 1, k)) +
+                   ez_at(a, i + 1, j + 1, k));
+  f.b[0] = 0.5 * (b_at(a, 0, i, j, k) + b_at(a, 0, i + 1, j, k));
+  f.b[1] = 0.5 * (b_at(a, 1, i, j, k) + b_at(a, 1, i, j + 1, k));
+  f.b[2] = 0.5 * (b_at(a, 2, i, j, k) + b_at(a, 2, i, j, k + 1));
+  return f;
+}
+
+__device__ __forceinline__ double energy_density(const CellFields& f) {
+  const double en = (f.e[0] * f.e[0] + f.e[1] * f.e[1]) + f.e[2] * f.e[2];
+  const double bn = (f.b[0] * f.b[0] + f.b[1] * f.b[1]) + f.b[2] * f.b[2];
+  return 0.5 * (kEpsilon0 * en + bn / kMu0);
+}
+
+__device__ __forceinline__ double poynting(const CellFields& f, int axis) {
+  const int p = axis == 0 ? 1 : axis == 1 ? 2 : 0;  // first transverse component
+  const int q = axis == 0 ? 2 : axis == 1 ? 0 : 1;  // second
+  return (f.e[p] * f.b[q] - f.e[q] * f.b[p]) / kMu0;
+}
+
+__device__ DD term_value(const LedgerArgs& a, const LedgerTerm& t, long long n) {
+  const int w = a.i1 - a.i0, h = a.j1 - a.j0;
+  const bool sub = t.substitute != 0;
+  switch (t.kind) {
+    case kLedgerPlane: {
+      const int j = a.j0 + (int)(n / w), i = a.i0 + (int)(n % w);
+      return dd_mul(a.volume, energy_density(collocate(a, i, j, t.index, sub)));
+    }
+    case kLedgerVolume: {
+      const long long per = (long long)w * h;
+      const int k = (int)(n / per);
+      const long long r = n % per;
+      const int j = a.j0 + (int)(r / w), i = a.i0 + (int)(r % w);
+      return dd_mul(a.volume, energy_density(collocate(a, i, j, k, false)));
+    }
+    case kLedgerFaceX: {
+      const int k = (int)(n / h), j = a.j0 + (int)(n % h);
+      return dd_mul(a.area_yz, t.sign * poynting(collocate(a, t.index, j, k, sub), 0));
+    }
+    case kLedgerFaceY: {
+      const int k = (int)(n / w), i = a.i0 + (int)(n % w);
+      return dd_mul(a.area_xz, t.sign * poynting(collocate(a, i, t.index, k, sub), 1));
+    }
+    case kLedgerFaceZ: {
+      const int j = a.j0 + (int)(n / w), i = a.i0 + (int)(n % w);
+      return dd_mul(a.area_xy, t.sign * poynting(collocate(a, i, j, t.index, sub), 2));
+    }
+    default: {
+      const double ux = a.ux[n], uy = a.uy[n], uz = a.uz[n], m = a.m[n];
+      if (t.kind == kLedgerRepresented) return dd_div(DD{m, 0.}, kElectronMass);
+      const DD rest = dd_mul(a.c2, m);
+      const double gamma = gamma_u(ux, uy, uz);
+      if (t.kind == kLedgerTotal) return dd_mul(rest, gamma);
+      const double u2 = (ux * ux + uy * uy) + uz * uz;
+      return dd_div(dd_mul(rest, u2), gamma + 1.0);
+    }
+  }
+}
+
+// Fixed-order tree over the block.
+__device__ DD block_sum(DD v, DD* shared) {
+  const int t = threadIdx.x;
+  shared[t] = v;
+  __syncthreads();
+  for (int s = kLedgerThreads / 2; s > 0; s >>= 1) {
+    if (t < s) shared[t] = dd_add(shared[t], shared[t + s]);
+    __syncthreads();
+  }
+  const DD out = shared[0];
+  __syncthreads();
+  return out;
+}
+
+// The term table with constant indices only (a dynamically indexed kernel
+// parameter would be copied to local memory).
+__device__ __forceinline__ LedgerTerm select_term(const LedgerArgs& a, int q) {
+  LedgerTerm t = a.q[0];
+#pragma unroll
+  for (int s = 1; s < kLedgerMaxTerms; ++s)
+    if (s == q) t = a.q[s];
+  return t;
+}
+
+}  // namespace
+
+DD ledger_product(double a, double b) { return two_prod(a, b); }
+DD ledger_product(DD a, double b) { return dd_mul(a, b); }
+
+__global__ void __launch_bounds__(kLedgerThreads) ledger_partial_kernel(LedgerArgs a) {
+  __shared__ DD shared[kLedgerThreads];
+  const int b = blockIdx.x;
+  int q = 0;
+#pragma unroll
+  for (int s = 1; s < kLedgerMaxTerms; ++s)
+    if (s < a.nq && b >= a.q[s].first_block) q = s;
+  const LedgerTerm t = select_term(a, q);
+  DD sum{0., 0.};
+  const long long stride = (long long)t.blocks * kLedgerThreads;
+  for (long long n = (long long)(b - t.first_block) * kLedgerThreads + threadIdx.x; n < t.count;
+       n += stride)
+    sum = dd_add(sum, term_value(a, t, n));
+  sum = block_sum(sum, shared);
+  if (threadIdx.x == 0) a.partial[b] = sum;
+}
+
+// One block, one warp per quantity: each quantity's partials in index order
+// (a fixed lane-strided sum and shuffle tree), then the ledger update of the
+// phase (src/moving_window_fields.cpp:214-218, 281-288, 431-436, 500-514).
+__global__ void __launch_bounds__(kLedgerFinishThreads) ledger_finish_kernel(LedgerArgs a) {
+  __shared__ DD result[kLedgerMaxTerms];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (int q = warp; q < a.nq; q += kLedgerFinishThreads / 32) {
+    const LedgerTerm t = select_term(a, q);
+    DD sum{0., 0.};
+    for (int n = lane; n < t.blocks; n += 32) sum = dd_add(sum, a.partial[t.first_block + n]);
+    for (int offset = 16; offset > 0; offset >>= 1) {
+      const DD other{__shfl_down_sync(0xffffffffu, sum.hi, offset),
+                     __shfl_down_sync(0xffffffffu, sum.lo, offset)};
+      sum = dd_add(sum, other);
+    }
+    if (lane == 0) result[q] = sum;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  DLedger& l = *a.ledger;
+  switch (a.phase) {
+    case kLedgerPhaseBegin:
+      for (int f = 0; f < 6; ++f) l.start[f] = result[f];
+      break;
+    case kLedgerPhaseFinish: {
+      // 0/1: plane 0 before/after the overwrite; 2-6/7-11: inlet-only face
+      // power before/after; 12-17: end power; 18: plane nz-1.
+      l.overwrite = dd_add(l.overwrite, dd_add(result[1], dd_neg(result[0])));
+      ++l.overwrite_events;
+      const DD half_dt{a.half_dt, 0.};
+      for (int f = 0; f < 6; ++f) {
+        const DD delta = f < 5 ? dd_add(result[7 + f], dd_neg(result[2 + f])) : DD{0., 0.};
+        const DD sum = dd_add(dd_add(l.start[f], result[12 + f]), dd_neg(delta));
+        l.outward[f] = dd_add(l.outward[f], dd_mul(sum, half_dt.hi));
+      }
+      ++l.flux_steps;
+      l.removed = result[18];
+      break;
+    }
+    case kLedgerPhaseShift:
+      // 0: the inserted plane; 1-6: the boundary power of the shifted state,
+      // which is the next step's start power.
+      l.remap = dd_add(l.remap, dd_add(result[0], dd_neg(l.removed)));
+      l.inserted = dd_add(l.inserted, result[0]);
+      l.cropped = dd_add(l.cropped, l.removed);
+      ++l.remap_steps;
+      for (int f = 0; f < 6; ++f) l.start[f] = result[1 + f];
+      break;
+    default:
+      for (int q = 0; q < a.nq && q < 10; ++q) l.snapshot[q] = result[q];
+      break;
+  }
+}
+
+}  // namespace aprl_gpu

@@ -24,6 +24,7 @@
 #include "../../include/aprl_gpu.h"
 #include "common.cuh"
 #include "fields.cuh"
+#include "ledger.cuh"
 #include "particles.cuh"
 
 using namespace aprl_gpu;
@@ -54,7 +55,7 @@ enum Kernel : unsigned {
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
-  kGuessGather, kOrbitSum, kBShadow, kKernelCount
+  kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -63,7 +64,8 @@ const char* kKernelNames[kKernelCount] = {
   "block_offset_scan", "gather_particles", "gather_carriers",
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
-  "frozen_support", "guess_gather", "orbit_sum", "b_shadow"};
+  "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
+  "ledger_finish"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -308,6 +310,13 @@ struct aprl_run {
   // detector scratch
   double* d_detector = nullptr;
   size_t detector_cap = 0;
+  // energy ledger (ledger.cuh): device state, block partials, and Ex/Ey of
+  // plane 0 before the inlet overwrite (written by the preview)
+  bool ledger_on = false;
+  bool ledger_start_ready = false;  // the last shift already took the start power
+  DLedger* d_ledger = nullptr;
+  DD* d_ledger_partial = nullptr;
+  double* ledger_pre[2]{};
   // profiling
   bool profile = false;
   std::vector<Timing> pending;
@@ -827,10 +836,138 @@ aprl_status admit_pending(aprl_run* r) {
   return APRL_OK;
 }
 
+// ---- energy ledger (ledger.cuh) -------------------------------------------
+constexpr int kLedgerMaxBlocks = 592;  // four blocks per SM
+
+aprl_status ensure_ledger(aprl_run* r) {
+  if (r->d_ledger) return APRL_OK;
+  const aprl_run_config& c = r->cfg;
+  TRY(device_alloc(&r->d_ledger, 1));
+  TRY(device_alloc(&r->d_ledger_partial, (size_t)kLedgerMaxTerms * kLedgerMaxBlocks));
+  TRY(device_alloc(&r->ledger_pre[0], (size_t)c.nx * (c.ny + 1)));
+  TRY(device_alloc(&r->ledger_pre[1], (size_t)(c.nx + 1) * c.ny));
+  CUDA_TRY(cudaMemsetAsync(r->d_ledger, 0, sizeof(DLedger), r->stream));
+  return APRL_OK;
+}
+
+LedgerArgs ledger_args(const aprl_run* r, int phase) {
+  const aprl_run_config& c = r->cfg;
+  LedgerArgs a{};
+  a.g = make_grid<double>(r);
+  a.pre[0] = r->ledger_pre[0];
+  a.pre[1] = r->ledger_pre[1];
+  a.ux = r->p.ux;
+  a.uy = r->p.uy;
+  a.uz = r->p.uz;
+  a.m = r->p.m;
+  a.i0 = (int)c.cpml_cells_x;
+  a.i1 = (int)(c.nx - c.cpml_cells_x);
+  a.j0 = (int)c.cpml_cells_y;
+  a.j1 = (int)(c.ny - c.cpml_cells_y);
+  a.volume = ledger_product(ledger_product(c.dx, c.dy), c.dz);
+  a.area_yz = ledger_product(c.dy, c.dz);
+  a.area_xz = ledger_product(c.dx, c.dz);
+  a.area_xy = ledger_product(c.dx, c.dy);
+  a.c2 = ledger_product(kC, kC);
+  a.half_dt = 0.5 * c.dt;
+  a.phase = phase;
+  a.partial = r->d_ledger_partial;
+  a.ledger = r->d_ledger;
+  return a;
+}
+
+void ledger_term(LedgerArgs& a, int kind, int index, int kmax, bool substitute, double sign,
+                 long long count) {
+  LedgerTerm& t = a.q[a.nq++];
+  t.kind = kind;
+  t.index = index;
+  t.kmax = kmax;
+  t.substitute = substitute ? 1 : 0;
+  t.sign = sign;
+  t.count = count;
+}
+
+void ledger_plane(LedgerArgs& a, int k, bool substitute) {
+  ledger_term(a, kLedgerPlane, k, 1, substitute, 1., (long long)(a.i1 - a.i0) * (a.j1 - a.j0));
+}
+
+// boundaryPower's faces x-, x+, y-, y+, z- and (unless inlet_only) z+.
+void ledger_faces(LedgerArgs& a, int nz, bool inlet_only, bool substitute) {
+  const long long w = a.i1 - a.i0, h = a.j1 - a.j0;
+  const int kmax = inlet_only ? 1 : nz;
+  ledger_term(a, kLedgerFaceX, a.i0, kmax, substitute, -1., h * kmax);
+  ledger_term(a, kLedgerFaceX, a.i1 - 1, kmax, substitute, 1., h * kmax);
+  ledger_term(a, kLedgerFaceY, a.j0, kmax, substitute, -1., w * kmax);
+  ledger_term(a, kLedgerFaceY, a.j1 - 1, kmax, substitute, 1., w * kmax);
+  ledger_term(a, kLedgerFaceZ, 0, 1, substitute, -1., w * h);
+  if (!inlet_only) ledger_term(a, kLedgerFaceZ, nz - 1, 1, substitute, 1., w * h);
+}
+
+aprl_status ledger_launch(aprl_run* r, LedgerArgs& a) {
+  int blocks = 0;
+  for (int q = 0; q < a.nq; ++q) {
+    LedgerTerm& t = a.q[q];
+    const long long per_block = (long long)kLedgerThreads * 4;
+    const long long want = (t.count + per_block - 1) / per_block;
+    t.blocks = (int)std::min<long long>(std::max<long long>(want, 1), kLedgerMaxBlocks);
+    t.first_block = blocks;
+    blocks += t.blocks;
+  }
+  TRY(launch(r, kLedgerPartial, ledger_partial_kernel, dim3(blocks), dim3(kLedgerThreads), a));
+  return launch(r, kLedgerFinish, ledger_finish_kernel, dim3(1), dim3(kLedgerFinishThreads), a);
+}
+
+// Boundary::begin (src/moving_window_fields.cpp:214-218): the step's start power.
+aprl_status ledger_begin(aprl_run* r) {
+  LedgerArgs a = ledger_args(r, kLedgerPhaseBegin);
+  ledger_faces(a, (int)r->cfg.nz, false, false);
+  return ledger_launch(r, a);
+}
+
+// After the commit: the measured inlet overwrite (src/moving_window_fields.cpp:265-290),
+// finishEnergyLedgerStep (:425-437) and the plane the shift drops (:446-450).
+aprl_status ledger_finish(aprl_run* r) {
+  LedgerArgs a = ledger_args(r, kLedgerPhaseFinish);
+  const int nz = (int)r->cfg.nz;
+  ledger_plane(a, 0, true);
+  ledger_plane(a, 0, false);
+  ledger_faces(a, nz, true, true);
+  ledger_faces(a, nz, true, false);
+  ledger_faces(a, nz, false, false);
+  ledger_plane(a, nz - 1, false);
+  return ledger_launch(r, a);
+}
+
+// After the shift: the inserted plane (src/moving_window_fields.cpp:500-515)
+// and the boundary power of the shifted fields, which the next begin would
+// measure on the same fields.
+aprl_status ledger_shift(aprl_run* r) {
+  LedgerArgs a = ledger_args(r, kLedgerPhaseShift);
+  ledger_plane(a, 0, false);
+  ledger_faces(a, (int)r->cfg.nz, false, false);
+  TRY(ledger_launch(r, a));
+  r->ledger_start_ready = true;
+  return APRL_OK;
+}
+
+aprl_status ledger_snapshot(aprl_run* r) {
+  LedgerArgs a = ledger_args(r, kLedgerPhaseSnapshot);
+  const int nz = (int)r->cfg.nz;
+  ledger_term(a, kLedgerVolume, 0, nz, false, 1.,
+              (long long)(a.i1 - a.i0) * (a.j1 - a.j0) * nz);
+  ledger_faces(a, nz, false, false);
+  ledger_term(a, kLedgerKinetic, 0, 0, false, 1., (long long)r->np);
+  ledger_term(a, kLedgerTotal, 0, 0, false, 1., (long long)r->np);
+  ledger_term(a, kLedgerRepresented, 0, 0, false, 1., (long long)r->np);
+  return ledger_launch(r, a);
+}
+
 template <class F>
 aprl_status advance_magnetic_t(aprl_run* r) {
   if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Moving-window beginStep phase/origin mismatch");
   TRY(admit_pending(r));
+  if (r->ledger_on && !r->ledger_start_ready) TRY(ledger_begin(r));
+  r->ledger_start_ready = false;
   const aprl_run_config& c = r->cfg;
   for (int a = 0; a < 3; ++a)
     CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
@@ -884,6 +1021,7 @@ aprl_status preview_electric_t(aprl_run* r) {
   pa.ex_prof = r->eprof[0].view();
   pa.ey_prof = r->eprof[1].view();
   for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view();
+  for (int a = 0; a < 2; ++a) pa.pre_inlet[a] = r->ledger_on ? r->ledger_pre[a] : nullptr;
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
@@ -1133,6 +1271,7 @@ aprl_status shift_insert_t(aprl_run* r) {
 aprl_status do_shift(aprl_run* r, bool defer_check = false) {
   if (r->stage != 4)
     return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
+  if (r->ledger_on) TRY(ledger_finish(r));
   const aprl_run_config& c = r->cfg;
   r->time += c.dt;
   r->step += 1;
@@ -1143,6 +1282,7 @@ aprl_status do_shift(aprl_run* r, bool defer_check = false) {
     r->zb_b[a] = (r->zb_b[a] + nzb - 1) % nzb;
   }
   TRY(shift_insert_t<double>(r));
+  if (r->ledger_on) TRY(ledger_shift(r));
   r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
   if (r->np)
     TRY(launch(r, kInletCheck, inlet_check_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
@@ -1372,6 +1512,10 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   free_carriers(r->c_alt);
   free_carriers(r->c_out);
   cudaFree(r->c_keep);
+  cudaFree(r->d_ledger);
+  cudaFree(r->d_ledger_partial);
+  cudaFree(r->ledger_pre[0]);
+  cudaFree(r->ledger_pre[1]);
   cudaFree(r->d_counters);
   cudaFree(r->d_sums);
   cudaFree(r->d_status);
@@ -1448,6 +1592,7 @@ static aprl_status field_io(aprl_run* r, unsigned a, const double* in, double* o
 }
 
 aprl_status aprl_run_set_field(aprl_run* r, unsigned a, const double* host, size_t count) {
+  if (r && a < 6) r->ledger_start_ready = false;  // the next begin measures the new fields
   return field_io(r, a, host, nullptr, count);
 }
 
@@ -1908,6 +2053,44 @@ aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double*
              retyped<double>(da, make_grid<double>(r))));
   CUDA_TRY(cudaMemcpyAsync(out, r->d_detector, count * 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_enable_energy_ledger(aprl_run* r, int enabled) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  if (r->step != 0 || r->stage != 0)
+    return fail(APRL_ERR_RUNTIME,
+                "Moving-window energy ledger must be configured before the first step");
+  if (enabled) TRY(ensure_ledger(r));
+  r->ledger_on = enabled != 0;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_energy_ledger(aprl_run* r, aprl_energy_ledger* out) {
+  if (!r || !out) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Energy ledger read inside a step");
+  TRY(ensure_ledger(r));
+  TRY(ledger_snapshot(r));
+  DLedger h{};
+  CUDA_TRY(cudaMemcpyAsync(&h, r->d_ledger, sizeof h, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  TRY(check_device(r));
+  const auto v = [](const DD& d) { return d.hi + d.lo; };
+  std::memset(out, 0, sizeof *out);
+  out->inlet_overwrite_energy = v(h.overwrite);
+  out->inserted_energy = v(h.inserted);
+  out->cropped_energy = v(h.cropped);
+  out->remap_energy = v(h.remap);
+  for (int f = 0; f < 6; ++f) out->outward_energy[f] = v(h.outward[f]);
+  out->overwrite_events = h.overwrite_events;
+  out->flux_steps = h.flux_steps;
+  out->remap_steps = h.remap_steps;
+  out->field_energy_interior = v(h.snapshot[0]);
+  for (int f = 0; f < 6; ++f) out->boundary_power[f] = v(h.snapshot[1 + f]);
+  out->particle_kinetic = v(h.snapshot[7]);
+  out->particle_total = v(h.snapshot[8]);
+  out->represented_electrons = v(h.snapshot[9]);
+  out->particles = r->np;
   return APRL_OK;
 }
 

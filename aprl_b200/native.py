@@ -52,6 +52,8 @@ _SIGNATURES = {
     "run_shift": (C.c_int, [_H]),
     "run_step": (C.c_int, [_H, C.c_uint32]),
     "run_get_stats": (C.c_int, [_H, C.POINTER(abi.StepStats)]),
+    "run_enable_energy_ledger": (C.c_int, [_H, C.c_int]),
+    "run_energy_ledger": (C.c_int, [_H, C.POINTER(abi.EnergyLedger)]),
     "run_get_slot_fields": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _SZ]),
     "run_sample_field_plane": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                          C.POINTER(C.c_int)]),
@@ -311,6 +313,14 @@ class Run:
         s = abi.StepStats()
         self.b("run_get_stats", self.handle, C.byref(s))
         return s.as_dict()
+
+    def enable_energy_ledger(self, enabled=True):
+        self.b("run_enable_energy_ledger", self.handle, int(enabled))
+
+    def energy_ledger(self):
+        out = abi.EnergyLedger()
+        self.b("run_energy_ledger", self.handle, C.byref(out))
+        return out.as_dict()
 
     def slot_fields(self):
         n = self.particle_count_slots()

@@ -61,7 +61,14 @@ def parse_args(argv=None):
     p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--scan-slots", type=int, default=4)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    p.add_argument("--energy-ledger", choices=["auto", "on", "off"], default="auto",
+                   help="keep the moving-window energy ledger during the timed steps "
+                        "(auto: on for the undulator workload)")
     args = p.parse_args(argv)
+    if args.energy_ledger == "auto":
+        args.energy_ledger = args.workload == "undulator"
+    else:
+        args.energy_ledger = args.energy_ledger == "on"
     defaults = {"dipole": (1_000_000, "fp64"), "drift": (100_000, "fp64"),
                 "undulator": (4_000_000, "fp32-mixed")}[args.workload]
     if args.particles is None:
@@ -215,6 +222,8 @@ def run_ours(args):
     run = native.Run(lib, cfg, stream=stream.cuda_stream)
     run.set_reference(w.reference)
     run.set_particles(w.particles)
+    if args.energy_ledger:
+        run.enable_energy_ledger()
 
     for _ in range(W):
         run.step(1)
@@ -280,6 +289,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_stop)
     e2e_wall_ms = (time.perf_counter() - wall0) * 1e3
+    ledger = run.energy_ledger() if args.energy_ledger else None
     fp32_arm = None
     if args.precision == "fp64" and not args.no_fp32_arm:
         fp32_arm = time_fp32_arm(args, w, stream, run, detector_lab_z, world)
@@ -335,6 +345,7 @@ def run_ours(args):
                    "precision": "fp64-drop-in" if args.precision == "fp64" else "fp32-mixed",
                    "magnet": magnet,
                    "boost_gamma": cfg.boost_gamma, "parallelism": f"replicas{world}",
+                   "energy_ledger": bool(args.energy_ledger),
                    "l2": "inputs larger than L2 (fields + particles > 126 MB)"},
         "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
                                "max": stats["max_iterations"]},
@@ -349,6 +360,14 @@ def run_ours(args):
         "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
                    "reasons": clocks.get("reasons", [])},
     }
+    if ledger:
+        line["energy_ledger"] = {
+            "steps": ledger["flux_steps"],
+            "field_energy_interior_J": ledger["field_energy_interior"],
+            "outward_energy_J": sum(ledger["outward_energy"]),
+            "remap_energy_J": ledger["remap_energy"],
+            "inlet_overwrite_energy_J": ledger["inlet_overwrite_energy"],
+            "particle_kinetic_J": ledger["particle_kinetic"]}
     if fp32_arm:
         line["fp32_mixed"] = fp32_arm
     if world == 1 and not args.no_scan:

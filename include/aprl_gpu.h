@@ -350,6 +350,43 @@ aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* run, double plane_lab_
                                                 double* out, size_t count,
                                                 int* inside);
 
+/* Energy ledger of the moving window (MovingWindowFieldEnergyLedger,
+ * src/moving_window_fields.h:37-57, with its measurements at
+ * src/moving_window_fields.cpp:206-218, 265-290, 387-437, 444-516) and the
+ * field and particle energy sums of the EnergyLedgerRecord
+ * (src/energy_ledger.h:17-57, src/simulation.cpp:3308-3340, 3591-3626).
+ * The reference sums in long double; every sum here is reduced on the GPU in
+ * double-double (compensated binary64) arithmetic, in a fixed order, and
+ * rounded to binary64 once.  Energies in joules and powers in watts, box
+ * frame; faces in the order x-, x+, y-, y+, z-, z+. */
+typedef struct {
+  /* Cumulative over the steps taken while the ledger was enabled. */
+  double inlet_overwrite_energy;  /* inletOverwriteEnergyJ */
+  double inserted_energy;         /* insertedEnergyJ */
+  double cropped_energy;          /* croppedEnergyJ */
+  double remap_energy;            /* remapEnergyJ */
+  double outward_energy[6];       /* outwardEnergyFace: trapezoid of the face powers */
+  uint64_t overwrite_events;
+  uint64_t flux_steps;
+  uint64_t remap_steps;
+  /* The current state (at the call). */
+  double field_energy_interior;   /* localInteriorFieldEnergy: cells outside the xy CPML */
+  double boundary_power[6];       /* boundaryPower: outward Poynting power per face */
+  double particle_kinetic;        /* sum m c^2 u^2 / (gamma + 1) over stored particles */
+  double particle_total;          /* sum m c^2 gamma */
+  double represented_electrons;   /* sum m / m_e */
+  uint64_t particles;             /* stored macroparticles (held ones included) */
+} aprl_energy_ledger;
+
+/* MovingWindowFields::enableEnergyLedger (src/moving_window_fields.cpp:541-545):
+ * configure before the first step.  Disabled by default; when enabled, every
+ * step adds a handful of plane and face reductions (no host round trip). */
+aprl_status aprl_run_enable_energy_ledger(aprl_run* run, int enabled);
+
+/* The ledger's cumulative terms and the reductions of the current state.
+ * Valid between steps (no stage in progress).  Waits for the run's stream. */
+aprl_status aprl_run_energy_ledger(aprl_run* run, aprl_energy_ledger* out);
+
 /* Synchronise the run's stream. */
 aprl_status aprl_run_synchronize(aprl_run* run);
 

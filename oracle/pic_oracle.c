@@ -173,6 +173,13 @@ struct oracle_run {
   double saved_exit_charge;
   uint64_t saved_counts[3][6];
   double saved_charges[3][6];
+  /* MovingWindowFieldEnergyLedger (src/moving_window_fields.h:37-57) and the
+   * Boundary's per-step flux state (src/moving_window_fields.cpp:158-161). */
+  int ledger;
+  long double start_power[6], overwrite_power_delta[6];
+  long double overwrite_energy, inserted_energy, cropped_energy, remap_energy;
+  long double outward_energy[6];
+  uint64_t overwrite_events, flux_steps, remap_steps;
 };
 
 static aprl_status pending_extract(oracle_run* r);
@@ -1354,6 +1361,144 @@ static aprl_status inlet_overwrite(oracle_run* r) {
   return APRL_OK;
 }
 
+/* ---- energy ledger ------------------------------------------------------ */
+/* EBFieldGrid::fieldEnergyDensityCell (src/eb_field.cpp:715-738): the cell's
+ * collocated E (four-node averages) and B (two-node averages), binary64. */
+static double energy_density_cell(const oracle_run* r, size_t i, size_t j, size_t k) {
+  const comp_t *ex = &r->f[0], *ey = &r->f[1], *ez = &r->f[2];
+  const comp_t *bx = &r->f[3], *by = &r->f[4], *bz = &r->f[5];
+  const double e0 = 0.25 * (AT(ex, i, j, k) + AT(ex, i, j + 1, k) + AT(ex, i, j, k + 1) +
+                            AT(ex, i, j + 1, k + 1));
+  const double e1 = 0.25 * (AT(ey, i, j, k) + AT(ey, i + 1, j, k) + AT(ey, i, j, k + 1) +
+                            AT(ey, i + 1, j, k + 1));
+  const double e2 = 0.25 * (AT(ez, i, j, k) + AT(ez, i + 1, j, k) + AT(ez, i, j + 1, k) +
+                            AT(ez, i + 1, j + 1, k));
+  const double b0 = 0.5 * (AT(bx, i, j, k) + AT(bx, i + 1, j, k));
+  const double b1 = 0.5 * (AT(by, i, j, k) + AT(by, i, j + 1, k));
+  const double b2 = 0.5 * (AT(bz, i, j, k) + AT(bz, i, j, k + 1));
+  const double en = e0 * e0 + e1 * e1 + e2 * e2;
+  const double bn = b0 * b0 + b1 * b1 + b2 * b2;
+  return 0.5 * (SI_EPSILON0 * en + bn / SI_MU0);
+}
+
+/* EBFieldGrid::poyntingComponentCell (src/eb_field.cpp:740-781). */
+static double poynting_cell(const oracle_run* r, size_t i, size_t j, size_t k, unsigned axis) {
+  const comp_t *ex = &r->f[0], *ey = &r->f[1], *ez = &r->f[2];
+  const comp_t *bx = &r->f[3], *by = &r->f[4], *bz = &r->f[5];
+  const double cx = 0.25 * (AT(ex, i, j, k) + AT(ex, i, j + 1, k) + AT(ex, i, j, k + 1) +
+                            AT(ex, i, j + 1, k + 1));
+  const double cy = 0.25 * (AT(ey, i, j, k) + AT(ey, i + 1, j, k) + AT(ey, i, j, k + 1) +
+                            AT(ey, i + 1, j, k + 1));
+  const double cz = 0.25 * (AT(ez, i, j, k) + AT(ez, i + 1, j, k) + AT(ez, i, j + 1, k) +
+                            AT(ez, i + 1, j + 1, k));
+  const double mx = 0.5 * (AT(bx, i, j, k) + AT(bx, i + 1, j, k));
+  const double my = 0.5 * (AT(by, i, j, k) + AT(by, i, j + 1, k));
+  const double mz = 0.5 * (AT(bz, i, j, k) + AT(bz, i, j, k + 1));
+  double ea, eb, ma, mb;
+  if (axis == 0) {
+    ea = cy; eb = cz; ma = my; mb = mz;
+  } else if (axis == 1) {
+    ea = cz; eb = cx; ma = mz; mb = mx;
+  } else {
+    ea = cx; eb = cy; ma = mx; mb = my;
+  }
+  double s = ea * mb - eb * ma;
+  s /= SI_MU0;
+  return s;
+}
+
+/* planeEnergy (src/moving_window_fields.cpp:387-397): cells of plane k
+ * outside the xy CPML, long double accumulation. */
+static long double plane_energy(const oracle_run* r, size_t k) {
+  const aprl_run_config* g = &r->cfg;
+  const long double volume = (long double)g->dx * (long double)g->dy * (long double)g->dz;
+  long double value = 0.;
+  for (size_t j = g->cpml_cells_y; j < g->ny - g->cpml_cells_y; ++j)
+    for (size_t i = g->cpml_cells_x; i < g->nx - g->cpml_cells_x; ++i)
+      value += (long double)energy_density_cell(r, i, j, k) * volume;
+  return value;
+}
+
+/* boundaryPower (src/moving_window_fields.cpp:399-423) at one rank (both z
+ * faces local); `inlet_only` restricts it to plane 0 and drops face z+. */
+static void boundary_power(const oracle_run* r, int inlet_only, long double power[6]) {
+  const aprl_run_config* g = &r->cfg;
+  const size_t i0 = g->cpml_cells_x, i1 = g->nx - i0;
+  const size_t j0 = g->cpml_cells_y, j1 = g->ny - j0;
+  const long double yz = (long double)g->dy * g->dz;
+  const long double xz = (long double)g->dx * g->dz;
+  const long double xy = (long double)g->dx * g->dy;
+  for (int f = 0; f < 6; ++f) power[f] = 0.;
+  for (size_t k = 0; k < (inlet_only ? 1 : g->nz); ++k) {
+    for (size_t j = j0; j < j1; ++j) {
+      power[0] -= (long double)poynting_cell(r, i0, j, k, 0) * yz;
+      power[1] += (long double)poynting_cell(r, i1 - 1, j, k, 0) * yz;
+    }
+    for (size_t i = i0; i < i1; ++i) {
+      power[2] -= (long double)poynting_cell(r, i, j0, k, 1) * xz;
+      power[3] += (long double)poynting_cell(r, i, j1 - 1, k, 1) * xz;
+    }
+  }
+  for (size_t j = j0; j < j1; ++j)
+    for (size_t i = i0; i < i1; ++i) {
+      power[4] -= (long double)poynting_cell(r, i, j, 0, 2) * xy;
+      if (!inlet_only) power[5] += (long double)poynting_cell(r, i, j, g->nz - 1, 2) * xy;
+    }
+}
+
+aprl_status oracle_run_enable_energy_ledger(oracle_run* r, int enabled) {
+  if (r->step != 0 || r->stage != 0)
+    return fail(APRL_ERR_RUNTIME,
+                "Moving-window energy ledger must be configured before the first step");
+  r->ledger = enabled != 0;
+  return APRL_OK;
+}
+
+/* The ledger terms plus Simulation::localInteriorFieldEnergy
+ * (src/simulation.cpp:3308-3340) and the particle energy sums of the ledger
+ * record (src/simulation.cpp:3591-3604) at the current state. */
+aprl_status oracle_run_energy_ledger(oracle_run* r, aprl_energy_ledger* out) {
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Energy ledger read inside a step");
+  const aprl_run_config* g = &r->cfg;
+  memset(out, 0, sizeof *out);
+  out->inlet_overwrite_energy = (double)r->overwrite_energy;
+  out->inserted_energy = (double)r->inserted_energy;
+  out->cropped_energy = (double)r->cropped_energy;
+  out->remap_energy = (double)r->remap_energy;
+  for (int f = 0; f < 6; ++f) out->outward_energy[f] = (double)r->outward_energy[f];
+  out->overwrite_events = r->overwrite_events;
+  out->flux_steps = r->flux_steps;
+  out->remap_steps = r->remap_steps;
+  const long double volume = (long double)g->dx * (long double)g->dy * (long double)g->dz;
+  long double energy = 0.;
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = g->cpml_cells_y; j < g->ny - g->cpml_cells_y; ++j)
+      for (size_t i = g->cpml_cells_x; i < g->nx - g->cpml_cells_x; ++i)
+        energy += (long double)energy_density_cell(r, i, j, k) * volume;
+  out->field_energy_interior = (double)energy;
+  long double power[6];
+  boundary_power(r, 0, power);
+  for (int f = 0; f < 6; ++f) out->boundary_power[f] = (double)power[f];
+  long double kinetic = 0., total = 0., represented = 0.;
+  for (size_t n = 0; n < r->np; ++n) {
+    const particle_t* p = &r->p[n];
+    const double gamma = gamma_u(p->u);
+    const long double mass = (long double)p->m;
+    const long double c = (long double)SI_C;
+    const long double rest = mass * c * c;
+    const long double u2 = (long double)(p->u[0] * p->u[0] + p->u[1] * p->u[1] +
+                                         p->u[2] * p->u[2]);
+    kinetic += rest * u2 / (long double)(gamma + 1.0);
+    total += rest * (long double)gamma;
+    represented += mass / (long double)SI_ME;
+  }
+  out->particle_kinetic = (double)kinetic;
+  out->particle_total = (double)total;
+  out->represented_electrons = (double)represented;
+  out->particles = r->np;
+  return APRL_OK;
+}
+
 /* ---- step stages -------------------------------------------------------- */
 /* clearCurrent (src/eb_field.cpp:271-295). */
 static void clear_current(oracle_run* r) {
@@ -1371,6 +1516,11 @@ aprl_status oracle_run_advance_magnetic(oracle_run* r) {
    * halo planes from the reference at (offset-1, step); the upper planes are
    * the zero vectors of the last rank. */
   clear_current(r);
+  /* Boundary::begin's flux start (src/moving_window_fields.cpp:214-218). */
+  if (r->ledger) {
+    boundary_power(r, 0, r->start_power);
+    for (int f = 0; f < 6; ++f) r->overwrite_power_delta[f] = 0.;
+  }
   for (unsigned a = 0; a < 3; ++a) {
     const comp_t* c = &r->f[a];
     for (size_t j = 0; j < c->ny; ++j)
@@ -2539,8 +2689,20 @@ aprl_status oracle_run_commit_electric(oracle_run* r) {
   r->preview_present = 0;
   apply_current_source(r, -1.);
   cpml_after_electric(r);
+  /* The measured inlet overwrite (src/moving_window_fields.cpp:265-290). */
+  long double energy_before = 0., power_before[6], power_after[6];
+  if (r->ledger) {
+    energy_before = plane_energy(r, 0);
+    boundary_power(r, 1, power_before);
+  }
   s = inlet_overwrite(r);
   if (s != APRL_OK) return s;
+  if (r->ledger) {
+    r->overwrite_energy += plane_energy(r, 0) - energy_before;
+    boundary_power(r, 1, power_after);
+    for (int f = 0; f < 6; ++f) r->overwrite_power_delta[f] = power_after[f] - power_before[f];
+    ++r->overwrite_events;
+  }
   r->stage = 4;
   return APRL_OK;
 }
@@ -2548,6 +2710,19 @@ aprl_status oracle_run_commit_electric(oracle_run* r) {
 aprl_status oracle_run_shift(oracle_run* r) {
   if (r->stage != 4) return fail(APRL_ERR_RUNTIME, "Moving-window requires one left shift after each complete step");
   const aprl_run_config* g = &r->cfg;
+  /* finishEnergyLedgerStep (src/moving_window_fields.cpp:425-437), then the
+   * energy of the plane the shift drops (src/moving_window_fields.cpp:446-450). */
+  long double removed = 0.;
+  if (r->ledger) {
+    long double end_power[6];
+    boundary_power(r, 0, end_power);
+    const long double half_dt = .5L * (long double)g->dt;
+    for (int f = 0; f < 6; ++f)
+      r->outward_energy[f] += half_dt * (r->start_power[f] + end_power[f] -
+                                         r->overwrite_power_delta[f]);
+    ++r->flux_steps;
+    removed = plane_energy(r, g->nz - 1);
+  }
   r->time += g->dt;
   r->step += 1;
   r->offset = g->initial_offset - (int64_t)r->step;
@@ -2580,6 +2755,14 @@ aprl_status oracle_run_shift(oracle_run* r) {
       memmove(base + row, base, (layers - 1) * row * sizeof(double));
       memset(base, 0, row * sizeof(double));
     }
+  }
+  /* Remap energy of the shift at one rank (src/moving_window_fields.cpp:500-515). */
+  if (r->ledger) {
+    const long double inserted = plane_energy(r, 0);
+    r->remap_energy += inserted - removed;
+    r->inserted_energy += inserted;
+    r->cropped_energy += removed;
+    ++r->remap_steps;
   }
   /* finishMovingWindowStep particle part (src/simulation_moving_window.cpp:352-371). */
   r->origin[2] = fma((double)r->offset, g->dz, g->reference_origin[2]);

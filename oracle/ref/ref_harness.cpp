@@ -101,6 +101,7 @@ struct ref_run {
   std::string directory;
   std::unique_ptr<PendingParticleQueue> pending;
   unsigned long long admitted = 0, activations = 0, savedActivations = 0;
+  bool ledger = false;
 };
 
 namespace {
@@ -672,6 +673,9 @@ aprl_status ref_run_commit_electric(ref_run* r) {
 aprl_status ref_run_shift(ref_run* r) {
   return guarded([&] {
     if (r->stage != 4) throw std::logic_error("Moving-window requires one left shift after each complete step");
+    // Simulation calls this after the electric step, before the shift
+    // (src/simulation.cpp:3490-3493).
+    if (r->ledger) r->window->finishEnergyLedgerStep(*r->fields);
     r->time += r->cfg.dt;
     ++r->step;
     r->offset = r->cfg.initial_offset - static_cast<std::ptrdiff_t>(r->step);
@@ -824,6 +828,79 @@ aprl_status ref_cowan_coefficients(double dx, double dy, double dz, double out[1
     const EBCowanCoefficients c = EBCowanCoefficients::forZDispersion(dx, dy, dz);
     for (int a = 0; a < 3; ++a) { out[a] = c.alpha[a]; out[3 + a] = c.beta[a]; out[9 + a] = c.ratio[a]; }
     out[6] = c.deltaXY; out[7] = c.deltaYZ; out[8] = c.deltaZX;
+  });
+}
+
+aprl_status ref_run_enable_energy_ledger(ref_run* r, int enabled) {
+  return guarded([&] {
+    r->window->enableEnergyLedger(enabled != 0);
+    r->ledger = enabled != 0;
+  });
+}
+
+// MovingWindowFields::energyLedger plus the field and particle sums of
+// Simulation's ledger record at one rank: localInteriorFieldEnergy
+// (src/simulation.cpp:3308-3340), boundaryPower's loops
+// (src/moving_window_fields.cpp:399-423) and the particle loop
+// (src/simulation.cpp:3591-3604), over the reference's own cell operators.
+aprl_status ref_run_energy_ledger(ref_run* r, aprl_energy_ledger* out) {
+  return guarded([&] {
+    std::memset(out, 0, sizeof *out);
+    const MovingWindowFieldEnergyLedger& l = r->window->energyLedger();
+    out->inlet_overwrite_energy = static_cast<double>(l.inletOverwriteEnergyJ);
+    out->inserted_energy = static_cast<double>(l.insertedEnergyJ);
+    out->cropped_energy = static_cast<double>(l.croppedEnergyJ);
+    out->remap_energy = static_cast<double>(l.remapEnergyJ);
+    for (int f = 0; f < 6; ++f) out->outward_energy[f] = static_cast<double>(l.outwardEnergyFace[f]);
+    out->overwrite_events = l.overwriteEvents;
+    out->flux_steps = l.fluxSteps;
+    out->remap_steps = l.remapSteps;
+    const EBGridGeometry& g = r->geometry;
+    const std::size_t i0 = r->cfg.cpml_cells_x, i1 = g.nx - i0;
+    const std::size_t j0 = r->cfg.cpml_cells_y, j1 = g.ny - j0;
+    const long double volume = static_cast<long double>(g.dx) *
+                               static_cast<long double>(g.dy) * static_cast<long double>(g.dz);
+    long double energy = 0.L;
+    for (std::size_t k = 0; k < g.nz; ++k)
+      for (std::size_t j = j0; j < j1; ++j)
+        for (std::size_t i = i0; i < i1; ++i)
+          energy += static_cast<long double>(r->fields->fieldEnergyDensityCell(i, j, k)) * volume;
+    out->field_energy_interior = static_cast<double>(energy);
+    long double power[6] = {};
+    const long double yz = static_cast<long double>(g.dy) * g.dz;
+    const long double xz = static_cast<long double>(g.dx) * g.dz;
+    const long double xy = static_cast<long double>(g.dx) * g.dy;
+    for (std::size_t k = 0; k < g.nz; ++k) {
+      for (std::size_t j = j0; j < j1; ++j) {
+        power[0] -= static_cast<long double>(r->fields->poyntingComponentCell(i0, j, k, 0)) * yz;
+        power[1] += static_cast<long double>(r->fields->poyntingComponentCell(i1 - 1, j, k, 0)) * yz;
+      }
+      for (std::size_t i = i0; i < i1; ++i) {
+        power[2] -= static_cast<long double>(r->fields->poyntingComponentCell(i, j0, k, 1)) * xz;
+        power[3] += static_cast<long double>(r->fields->poyntingComponentCell(i, j1 - 1, k, 1)) * xz;
+      }
+    }
+    for (std::size_t j = j0; j < j1; ++j)
+      for (std::size_t i = i0; i < i1; ++i) {
+        power[4] -= static_cast<long double>(r->fields->poyntingComponentCell(i, j, 0, 2)) * xy;
+        power[5] += static_cast<long double>(r->fields->poyntingComponentCell(i, j, g.nz - 1, 2)) * xy;
+      }
+    for (int f = 0; f < 6; ++f) out->boundary_power[f] = static_cast<double>(power[f]);
+    long double kinetic = 0.L, total = 0.L, represented = 0.L;
+    for (const auto& p : r->particles) {
+      const Double gammaBox = BoostFrameTransform::gammaFromProperVelocity(p.properVelocity);
+      const long double mass = static_cast<long double>(p.mass);
+      const long double c = static_cast<long double>(SI::c);
+      const long double rest = mass * c * c;
+      const long double u2 = static_cast<long double>(p.properVelocity.norm2());
+      kinetic += rest * u2 / static_cast<long double>(gammaBox + 1.0);
+      total += rest * static_cast<long double>(gammaBox);
+      represented += mass / static_cast<long double>(SI::electronMass);
+    }
+    out->particle_kinetic = static_cast<double>(kinetic);
+    out->particle_total = static_cast<double>(total);
+    out->represented_electrons = static_cast<double>(represented);
+    out->particles = r->particles.size();
   });
 }
 
