@@ -122,6 +122,17 @@ class PicRun {
     return s;
   }
 
+  // MovingWindowFields::enableEnergyLedger / energyLedger plus the ledger
+  // record's interior field energy and particle energy sums.
+  void enableEnergyLedger(bool enabled = true) {
+    check(aprl_run_enable_energy_ledger(run_, enabled ? 1 : 0));
+  }
+  aprl_energy_ledger energyLedger() {
+    aprl_energy_ledger l{};
+    check(aprl_run_energy_ledger(run_, &l));
+    return l;
+  }
+
   // LabDetectorManager::samplePlane on a fixed lab plane (lab-frame E, B).
   bool sampleFieldPlane(double labZ, std::vector<double>& out) {
     const auto ex = shape(Component::Bz);

@@ -41,10 +41,14 @@ int main() {
       p.id.push_back(n + 1);
     }
     run.setParticles(p);
+    run.enableEnergyLedger();
     run.solveStep(2);
     const aprl_step_stats s = run.stats();
-    std::printf("steps=%llu particles=%llu trials=%u\n", (unsigned long long)s.step,
-                (unsigned long long)s.particles, s.iterations);
+    const aprl_energy_ledger l = run.energyLedger();
+    std::printf("steps=%llu particles=%llu trials=%u ledger_steps=%llu kinetic=%g\n",
+                (unsigned long long)s.step, (unsigned long long)s.particles, s.iterations,
+                (unsigned long long)l.flux_steps, l.particle_kinetic);
+    if (l.flux_steps != 2 || !(l.particle_kinetic > 0.0)) return 3;
     // A bad argument must surface as the reference's exception type.
     try {
       run.setField(aprl::gpu::Component::Ex, std::vector<double>(3, 0.0));
