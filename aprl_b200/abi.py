@@ -154,6 +154,20 @@ class EnergyLedger(C.Structure):
     as_dict = StepStats.as_dict
 
 
+class GaussLaw(C.Structure):
+    """aprl_gauss_law: eps0 div E - rho over the nodes of the current state."""
+    _fields_ = [
+        ("max_residual", C.c_double),
+        ("rms_residual", C.c_double),
+        ("max_charge_density", C.c_double),
+        ("total_charge", C.c_double),
+        ("interior_nodes", C.c_uint64),
+        ("outside", C.c_uint64),
+    ]
+
+    as_dict = StepStats.as_dict
+
+
 def field_shape(config, component):
     """Yee extents (nx_c, ny_c, nz_c) of an ABI component (x fastest)."""
     cells = (config.nx, config.ny, config.nz)

@@ -242,4 +242,102 @@ __global__ void __launch_bounds__(kLedgerFinishThreads) ledger_finish_kernel(Led
   }
 }
 
+// ---- discrete Gauss law ----------------------------------------------------
+// Node charge density of one particle (verification/transverse_binomial_checks.cpp:12-66):
+// F3 weights in x over nodes i-1..i+2, linear in y over j, j+1, the
+// binomial3 smoothing of the linear z weights over k-1..k+2.
+__global__ void gauss_deposit_kernel(GaussArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.np) return;
+  const DGrid& g = a.g;
+  const double x = (a.x[n] - g.origin[0]) / g.dx;
+  const double y = (a.y[n] - g.origin[1]) / g.dy;
+  const double z = (a.z[n] - g.origin[2]) / g.dz;
+  const double fi = floor(x), fj = floor(y), fk = floor(z);
+  const int i = (int)fi, j = (int)fj, k = (int)fk;
+  const double fx = x - fi, fy = y - fj, fz = z - fk;
+  const double wx[4] = {0.25 * (1.0 - fx), 0.5 - 0.25 * fx, 0.25 + 0.25 * fx, 0.25 * fx};
+  const double wy[2] = {1.0 - fy, fy};
+  double wz[4] = {0., 0., 0., 0.};
+  const double bw[3] = {0.25, 0.5, 0.25};
+  for (int s = 0; s < 3; ++s) {
+    wz[s] += bw[s] * (1.0 - fz);
+    wz[s + 1] += bw[s] * fz;
+  }
+  const double q = a.q[n] / (g.dx * g.dy * g.dz);
+  const int nx = g.nx + 1, ny = g.ny + 1, nz = g.nz + 1;
+  unsigned long long missed = 0;
+  for (int t = 0; t < 4; ++t) {
+    const int kk = k - 1 + t;
+    for (int v = 0; v < 2; ++v) {
+      const int jj = j + v;
+      for (int u = 0; u < 4; ++u) {
+        const int ii = i - 1 + u;
+        if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) {
+          ++missed;
+          continue;
+        }
+        atomicAdd(&a.node[((size_t)kk * ny + jj) * nx + ii], q * wx[u] * wy[v] * wz[t]);
+      }
+    }
+  }
+  if (missed) atomicAdd(a.outside, missed);
+}
+
+__device__ __forceinline__ double e_or_zero(const DGrid& g, int c, int i, int j, int k) {
+  if (i < 0 || j < 0 || k < 0 || i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c))
+    return 0.;
+  return g.e_old[c][e_index(g, c, i, j, k)];
+}
+
+// G = eps0 div E - rho at each node (edges outside the grid count as zero),
+// written over rho; sum of G^2 and max |G| over the interior nodes, sum of
+// rho dV and max |rho| over all nodes.
+__global__ void __launch_bounds__(kLedgerThreads) gauss_residual_kernel(GaussArgs a) {
+  __shared__ DD shared[kLedgerThreads];
+  const DGrid& g = a.g;
+  const int nx = g.nx + 1, ny = g.ny + 1;
+  const long long count = (long long)nx * ny * (g.nz + 1);
+  DD g2{0., 0.}, charge{0., 0.};
+  double gmax = 0., rmax = 0.;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % nx);
+    const int j = (int)((n / nx) % ny);
+    const int k = (int)(n / ((long long)nx * ny));
+    const double rho = a.node[n];
+    const double div = (e_or_zero(g, 0, i, j, k) - e_or_zero(g, 0, i - 1, j, k)) / g.dx +
+                       (e_or_zero(g, 1, i, j, k) - e_or_zero(g, 1, i, j - 1, k)) / g.dy +
+                       (e_or_zero(g, 2, i, j, k) - e_or_zero(g, 2, i, j, k - 1)) / g.dz;
+    const double residual = kEpsilon0 * div - rho;
+    a.node[n] = residual;
+    charge = dd_add(charge, dd_mul(a.volume, rho));
+    rmax = fmax(rmax, fabs(rho));
+    if (i >= a.i0 && i < a.i1 && j >= a.j0 && j < a.j1 && k >= a.k0 && k < a.k1) {
+      g2 = dd_add(g2, two_prod(residual, residual));
+      gmax = fmax(gmax, fabs(residual));
+    }
+  }
+  g2 = block_sum(g2, shared);
+  charge = block_sum(charge, shared);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = g2;
+    a.partial[2 * blockIdx.x + 1] = charge;
+  }
+  // Non-negative doubles order like their bit patterns.
+  if (gmax > 0.) atomicMax(&a.max_bits[0], (unsigned long long)__double_as_longlong(gmax));
+  if (rmax > 0.) atomicMax(&a.max_bits[1], (unsigned long long)__double_as_longlong(rmax));
+}
+
+__global__ void __launch_bounds__(kLedgerThreads) gauss_finish_kernel(GaussArgs a, int blocks) {
+  __shared__ DD shared[kLedgerThreads];
+  for (int q = 0; q < 2; ++q) {
+    DD sum{0., 0.};
+    for (int n = threadIdx.x; n < blocks; n += kLedgerThreads)
+      sum = dd_add(sum, a.partial[2 * n + q]);
+    sum = block_sum(sum, shared);
+    if (threadIdx.x == 0) a.result[q] = sum;
+  }
+}
+
 }  // namespace aprl_gpu

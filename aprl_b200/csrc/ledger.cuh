@@ -79,6 +79,28 @@ struct LedgerArgs {
   DLedger* ledger;
 };
 
+// Discrete Gauss law: rho from the particles with the node density the
+// linear-binomial3 current conserves (F3 in x, linear in y, binomial3 in z),
+// then G = eps0 div E - rho at every node, reduced over the interior nodes.
+struct GaussArgs {
+  DGrid g;                         // e_old = the committed E
+  const double *x, *y, *z, *q;     // particle box positions and charges
+  long long np;
+  double* node;                    // (nx+1)(ny+1)(nz+1), [k][j][i]: rho, then G in place
+  int i0, i1, j0, j1, k0, k1;      // interior nodes [i0, i1) x [j0, j1) x [k0, k1)
+  DD volume;
+  DD* partial;                     // per residual block: sum G^2, sum rho dV
+  unsigned long long* max_bits;    // max |G| (interior), max |rho|, as ordered bits
+  unsigned long long* outside;     // node contributions that fell outside the grid
+  DD* result;                      // sum G^2, sum rho dV
+};
+
+constexpr int kGaussBlocks = 1184;  // eight 256-thread blocks per SM
+
+__global__ void gauss_deposit_kernel(GaussArgs a);
+__global__ void gauss_residual_kernel(GaussArgs a);
+__global__ void gauss_finish_kernel(GaussArgs a, int blocks);
+
 __global__ void ledger_partial_kernel(LedgerArgs a);
 __global__ void ledger_finish_kernel(LedgerArgs a);
 

@@ -55,7 +55,8 @@ enum Kernel : unsigned {
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
-  kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish, kKernelCount
+  kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
+  kGaussDeposit, kGaussResidual, kGaussFinish, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -65,7 +66,7 @@ const char* kKernelNames[kKernelCount] = {
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
   "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
-  "ledger_finish"};
+  "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -317,6 +318,9 @@ struct aprl_run {
   DLedger* d_ledger = nullptr;
   DD* d_ledger_partial = nullptr;
   double* ledger_pre[2]{};
+  // Gauss-law scratch: node array, then block partials, results and maxima
+  double* gauss_node = nullptr;
+  unsigned char* gauss_scratch = nullptr;
   // profiling
   bool profile = false;
   std::vector<Timing> pending;
@@ -1512,6 +1516,8 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   free_carriers(r->c_alt);
   free_carriers(r->c_out);
   cudaFree(r->c_keep);
+  cudaFree(r->gauss_node);
+  cudaFree(r->gauss_scratch);
   cudaFree(r->d_ledger);
   cudaFree(r->d_ledger_partial);
   cudaFree(r->ledger_pre[0]);
@@ -2091,6 +2097,76 @@ aprl_status aprl_run_energy_ledger(aprl_run* r, aprl_energy_ledger* out) {
   out->particle_total = v(h.snapshot[8]);
   out->represented_electrons = v(h.snapshot[9]);
   out->particles = r->np;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_gauss_law(aprl_run* r, aprl_gauss_law* out, double* residual,
+                               size_t count) {
+  if (!r || !out) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (r->stage != 0 && r->stage != 4)
+    return fail(APRL_ERR_RUNTIME, "Gauss-law reduction inside a step");
+  const aprl_run_config& c = r->cfg;
+  if (c.shape != APRL_SHAPE_LINEAR_BINOMIAL3)
+    return fail(APRL_ERR_UNSUPPORTED, "The node charge density is built for linear-binomial3");
+  const size_t nodes = (size_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
+  if (residual && count != nodes)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Gauss-law residual size mismatch");
+  const size_t partial_bytes = sizeof(DD) * 2 * kGaussBlocks;
+  const size_t result_bytes = sizeof(DD) * 2;
+  const size_t scratch_bytes = partial_bytes + result_bytes + 3 * sizeof(unsigned long long);
+  if (!r->gauss_node) {
+    TRY(device_alloc(&r->gauss_node, nodes));
+    TRY(device_alloc(&r->gauss_scratch, scratch_bytes));
+  }
+  GaussArgs a{};
+  a.g = make_grid<double>(r);
+  a.x = r->p.x;
+  a.y = r->p.y;
+  a.z = r->p.z;
+  a.q = r->p.q;
+  a.np = (long long)r->np;
+  a.node = r->gauss_node;
+  a.i0 = (int)c.cpml_cells_x + 1;
+  a.i1 = (int)(c.nx - c.cpml_cells_x);
+  a.j0 = (int)c.cpml_cells_y + 1;
+  a.j1 = (int)(c.ny - c.cpml_cells_y);
+  a.k0 = 1;
+  a.k1 = (int)c.nz;
+  a.volume = ledger_product(ledger_product(c.dx, c.dy), c.dz);
+  a.partial = reinterpret_cast<DD*>(r->gauss_scratch);
+  a.result = reinterpret_cast<DD*>(r->gauss_scratch + partial_bytes);
+  a.max_bits = reinterpret_cast<unsigned long long*>(r->gauss_scratch + partial_bytes + result_bytes);
+  a.outside = a.max_bits + 2;
+  CUDA_TRY(cudaMemsetAsync(r->gauss_node, 0, nodes * sizeof(double), r->stream));
+  CUDA_TRY(cudaMemsetAsync(a.max_bits, 0, 3 * sizeof(unsigned long long), r->stream));
+  if (r->np)
+    TRY(launch(r, kGaussDeposit, gauss_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), a));
+  const int blocks = (int)std::min<size_t>(kGaussBlocks, blocks_for(nodes, kLedgerThreads));
+  TRY(launch(r, kGaussResidual, gauss_residual_kernel, dim3(blocks), dim3(kLedgerThreads), a));
+  TRY(launch(r, kGaussFinish, gauss_finish_kernel, dim3(1), dim3(kLedgerThreads), a, blocks));
+  DD sums[2];
+  unsigned long long bits[3];
+  CUDA_TRY(cudaMemcpyAsync(sums, a.result, sizeof sums, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaMemcpyAsync(bits, a.max_bits, sizeof bits, cudaMemcpyDeviceToHost, r->stream));
+  if (residual)
+    CUDA_TRY(cudaMemcpyAsync(residual, r->gauss_node, nodes * sizeof(double),
+                             cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  TRY(check_device(r));
+  const auto as_double = [](unsigned long long b) {
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    return v;
+  };
+  const uint64_t interior = (uint64_t)std::max(0, a.i1 - a.i0) * std::max(0, a.j1 - a.j0) *
+                            std::max(0, a.k1 - a.k0);
+  std::memset(out, 0, sizeof *out);
+  out->max_residual = as_double(bits[0]);
+  out->rms_residual = interior ? std::sqrt((sums[0].hi + sums[0].lo) / (double)interior) : 0.;
+  out->max_charge_density = as_double(bits[1]);
+  out->total_charge = sums[1].hi + sums[1].lo;
+  out->interior_nodes = interior;
+  out->outside = bits[2];
   return APRL_OK;
 }
 

@@ -68,6 +68,7 @@ _PRODUCT_ONLY = {
     "run_reset_iteration_stats": (C.c_int, [_H]),
     "run_sample_field_plane_noalloc": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                                  C.POINTER(C.c_int)]),
+    "run_gauss_law": (C.c_int, [_H, C.POINTER(abi.GaussLaw), _D, C.c_size_t]),
     "scan_footprint": (C.c_int, [C.POINTER(abi.RunConfig), C.c_size_t, _U64]),
     "scan_create": (C.c_int, [C.POINTER(abi.ScanConfig), C.POINTER(C.c_void_p)]),
     "scan_submit": (C.c_int, [C.c_void_p, C.POINTER(abi.ScanRequest), _U64]),
@@ -320,6 +321,17 @@ class Run:
     def energy_ledger(self):
         out = abi.EnergyLedger()
         self.b("run_energy_ledger", self.handle, C.byref(out))
+        return out.as_dict()
+
+    def gauss_law(self, residual=False):
+        """Summary dict, and with residual=True also G per node [k][j][i]."""
+        cfg = self.config
+        out = abi.GaussLaw()
+        if residual:
+            nodes = np.empty((cfg.nz + 1, cfg.ny + 1, cfg.nx + 1))
+            self.b("run_gauss_law", self.handle, C.byref(out), _ptr(nodes), nodes.size)
+            return out.as_dict(), nodes
+        self.b("run_gauss_law", self.handle, C.byref(out), None, 0)
         return out.as_dict()
 
     def slot_fields(self):

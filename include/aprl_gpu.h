@@ -387,6 +387,36 @@ aprl_status aprl_run_enable_energy_ledger(aprl_run* run, int enabled);
  * Valid between steps (no stage in progress).  Waits for the run's stream. */
 aprl_status aprl_run_energy_ledger(aprl_run* run, aprl_energy_ledger* out);
 
+/* Discrete Gauss law of the current state, reduced on the GPU.  The node
+ * charge density is the one the linear-binomial3 current conserves: per
+ * particle, F3 node weights in x over nodes i-1..i+2, linear weights in y
+ * over j, j+1 and the binomial3-smoothed linear weights in z over
+ * k-1..k+2, times q/(dx dy dz) (the F3 density of
+ * verification/transverse_binomial_checks.cpp:12-66).  At every node
+ * G = eps0 div E - rho, div E from the Yee edges around the node (edges
+ * outside the grid count as zero).  The reference audits the same law
+ * through the charge continuity of its deposit
+ * (ChargeConservingCurrentDepositor::maxContinuityResidual,
+ * src/eb_deposition.cpp:195-226); with a charge-conserving current and the
+ * plain Yee curl of the Ampere update, G at interior nodes does not change
+ * in a step except by roundoff. */
+typedef struct {
+  double max_residual;        /* max |G| over the interior nodes (C/m^3) */
+  double rms_residual;        /* root mean square of G over the same nodes */
+  double max_charge_density;  /* max |rho| over all nodes */
+  double total_charge;        /* sum of rho dV over all nodes (C), double-double */
+  uint64_t interior_nodes;    /* nodes i in [cx+1, nx-cx-1], j in [cy+1, ny-cy-1], k in [1, nz-1] */
+  uint64_t outside;           /* particle node contributions that fell outside the grid */
+} aprl_gauss_law;
+
+/* Between steps, or after the commit and before the shift.  `residual` (may be NULL): (nx+1)*(ny+1)*(nz+1) doubles,
+ * G at node (i, j, k) at [(k*(ny+1) + j)*(nx+1) + i].  Only the
+ * linear-binomial3 shape has this node density (APRL_ERR_UNSUPPORTED
+ * otherwise).  The density is summed with FP64 atomics, so G varies in the
+ * last bits from call to call. */
+aprl_status aprl_run_gauss_law(aprl_run* run, aprl_gauss_law* out, double* residual,
+                               size_t count);
+
 /* Synchronise the run's stream. */
 aprl_status aprl_run_synchronize(aprl_run* run);
 

@@ -117,3 +117,58 @@ def max_relative(a, b):
     if scale == 0.0:
         return float(diff)
     return float(diff / scale)
+
+
+# ---------------------------------------------------------------------------
+# Node charge density and the discrete Gauss law (numpy restatements).
+def _f3_node(f):
+    return np.stack([0.25 * (1.0 - f), 0.5 - 0.25 * f, 0.25 + 0.25 * f, 0.25 * f])
+
+
+def charge_density(cfg, origin, p, pad=2):
+    """The node charge density the linear-binomial3 current conserves: F3
+    node weights in x, linear in y, binomial3 in z
+    (verification/transverse_binomial_checks.cpp:12-66), [k][j][i] with
+    `pad` extra nodes on every side (index pad is node 0)."""
+    rho = np.zeros((cfg.nz + 1 + 2 * pad, cfg.ny + 1 + 2 * pad, cfg.nx + 1 + 2 * pad))
+    x = (p["x"] - origin[0]) / cfg.dx
+    y = (p["y"] - origin[1]) / cfg.dy
+    z = (p["z"] - origin[2]) / cfg.dz
+    i = np.floor(x).astype(int)
+    j = np.floor(y).astype(int)
+    k = np.floor(z).astype(int)
+    wx = _f3_node(x - i)            # nodes i-1 .. i+2
+    fy = y - j
+    fz = z - k
+    wz = np.zeros((4, x.size))      # binomial3 over nodes k-1 .. k+2
+    for s, w in zip((-1, 0, 1), (0.25, 0.5, 0.25)):
+        wz[s + 1] += w * (1.0 - fz)
+        wz[s + 2] += w * fz
+    q = p["charge"] / (cfg.dx * cfg.dy * cfg.dz)
+    for u in range(4):
+        for v in range(2):
+            wy = fy if v else 1.0 - fy
+            for t in range(4):
+                np.add.at(rho, (k - 1 + t + pad, j + v + pad, i - 1 + u + pad),
+                          q * wx[u] * wy * wz[t])
+    return rho, pad
+
+
+def gauss_residual(cfg, origin, p, ex, ey, ez):
+    """eps0 div E - rho at every node [k][j][i]; edges outside the grid are
+    zero (ex, ey, ez in the [k][j][i] arrays of get_field)."""
+    eps0 = 8.8541878128e-12
+    rho, pad = charge_density(cfg, origin, p)
+    rho = rho[pad:-pad, pad:-pad, pad:-pad]
+    shape = rho.shape
+    dx = np.zeros(shape)
+    dx[:, :, :-1] += ex
+    dx[:, :, 1:] -= ex
+    dy = np.zeros(shape)
+    dy[:, :-1, :] += ey
+    dy[:, 1:, :] -= ey
+    dz = np.zeros(shape)
+    dz[:-1, :, :] += ez
+    dz[1:, :, :] -= ez
+    div = dx / cfg.dx + dy / cfg.dy + dz / cfg.dz
+    return eps0 * div - rho, rho

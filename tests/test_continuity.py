@@ -25,41 +25,9 @@ from aprl_b200 import native, workloads
 BOUND = 1e-12  # relative to max |rho| / dt
 
 
-def _f3_node(f):
-    return np.stack([0.25 * (1.0 - f), 0.5 - 0.25 * f, 0.25 + 0.25 * f, 0.25 * f])
-
-
-def charge_density(cfg, origin, p):
-    """F3/binomial3 charge density at the nodes, [k][j][i] with a one-node
-    pad on every side (index 0 is node -1)."""
-    pad = 2
-    rho = np.zeros((cfg.nz + 1 + 2 * pad, cfg.ny + 1 + 2 * pad, cfg.nx + 1 + 2 * pad))
-    x = (p["x"] - origin[0]) / cfg.dx
-    y = (p["y"] - origin[1]) / cfg.dy
-    z = (p["z"] - origin[2]) / cfg.dz
-    i = np.floor(x).astype(int)
-    j = np.floor(y).astype(int)
-    k = np.floor(z).astype(int)
-    wx = _f3_node(x - i)            # nodes i-1 .. i+2
-    fy = y - j
-    fz = z - k
-    wz = np.zeros((4, x.size))      # binomial3 over nodes k-1 .. k+2
-    for s, w in zip((-1, 0, 1), (0.25, 0.5, 0.25)):
-        wz[s + 1] += w * (1.0 - fz)
-        wz[s + 2] += w * fz
-    q = p["charge"] / (cfg.dx * cfg.dy * cfg.dz)
-    for u in range(4):
-        for v in range(2):
-            wy = fy if v else 1.0 - fy
-            for t in range(4):
-                np.add.at(rho, (k - 1 + t + pad, j + v + pad, i - 1 + u + pad),
-                          q * wx[u] * wy * wz[t])
-    return rho, pad
-
-
 def continuity(cfg, origin, before, after, jx, jy, jz):
-    r0, pad = charge_density(cfg, origin, before)
-    r1, _ = charge_density(cfg, origin, after)
+    r0, pad = checkers.charge_density(cfg, origin, before)
+    r1, _ = checkers.charge_density(cfg, origin, after)
     drho = (r1 - r0)[pad:-pad, pad:-pad, pad:-pad] / cfg.dt  # nodes 0..n
     div = np.zeros_like(drho)
     # Jx (nz+1, ny+1, nx): x-edges between nodes i and i+1
