@@ -293,7 +293,9 @@ struct aprl_run {
   unsigned long long* scan_total = nullptr;
   size_t scan_cap = 0;
   // pinned host mirrors
-  ResidualSums* h_sums = nullptr;
+  ResidualSums* h_sums = nullptr;        // the slot of the last trial read
+  ResidualSums* h_sums_pair = nullptr;   // two slots: a trial can be issued before
+  TrialCounters* h_counters_pair = nullptr;  // the previous one is read
   DeviceStatus* h_status = nullptr;
   TrialCounters* h_counters = nullptr;
   unsigned long long* h_total = nullptr;
@@ -1055,7 +1057,7 @@ aprl_status do_preview_electric(aprl_run* r) {
 
 // One coupling trial; W is the arithmetic of the gathers.
 template <class W>
-aprl_status trial_t(aprl_run* r, double residual[4]) {
+aprl_status trial_enqueue_t(aprl_run* r, int slot) {
   using F = double;
   if (r->stage != 2 && r->stage != 3)
     return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
@@ -1180,11 +1182,20 @@ aprl_status trial_t(aprl_run* r, double residual[4]) {
     ra.status = r->d_status;
     TRY(launch(r, kResidual, residual_kernel<W, F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
-  CUDA_TRY(cudaMemcpyAsync(r->h_sums, r->d_sums, sizeof(ResidualSums), cudaMemcpyDeviceToHost,
-                           r->stream));
-  CUDA_TRY(cudaMemcpyAsync(r->h_counters, r->d_counters, sizeof(TrialCounters),
+  CUDA_TRY(cudaMemcpyAsync(&r->h_sums_pair[slot], r->d_sums, sizeof(ResidualSums),
                            cudaMemcpyDeviceToHost, r->stream));
-  TRY(check_device(r));
+  CUDA_TRY(cudaMemcpyAsync(&r->h_counters_pair[slot], r->d_counters, sizeof(TrialCounters),
+                           cudaMemcpyDeviceToHost, r->stream));
+  ++r->trials;
+  r->stage = 3;
+  return APRL_OK;
+}
+
+// The residual of the trial copied to `slot` (after the stream has reached
+// it); the slot becomes the run's current trial counters.
+void trial_read(aprl_run* r, int slot, double residual[4]) {
+  r->h_sums = &r->h_sums_pair[slot];
+  r->h_counters = &r->h_counters_pair[slot];
   double force;
   const unsigned long long bits = r->h_sums->force_bits;
   std::memcpy(&force, &bits, sizeof force);
@@ -1192,13 +1203,26 @@ aprl_status trial_t(aprl_run* r, double residual[4]) {
   residual[1] = r->h_sums->defect;
   residual[2] = r->h_sums->scale;
   residual[3] = static_cast<double>(r->h_sums->calls);
-  ++r->trials;
-  r->stage = 3;
-  return APRL_OK;
+}
+
+aprl_status enqueue_trial(aprl_run* r, int slot) {
+  return r->fp32 ? trial_enqueue_t<float>(r, slot) : trial_enqueue_t<double>(r, slot);
+}
+
+// solveConservativeSourceStep's stopping rule (src/simulation_source_coupling.cpp:50).
+bool trial_converged(const aprl_run_config& c, unsigned iterations, const double res[4],
+                     double& force, double& work) {
+  force = res[0];
+  work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
+  return iterations >= (res[3] > 0. ? 2u : 1u) && force < c.force_tolerance &&
+         work < c.work_tolerance;
 }
 
 aprl_status do_trial(aprl_run* r, double residual[4]) {
-  return r->fp32 ? trial_t<float>(r, residual) : trial_t<double>(r, residual);
+  TRY(enqueue_trial(r, 0));
+  TRY(check_device(r));
+  trial_read(r, 0, residual);
+  return APRL_OK;
 }
 
 aprl_status do_commit(aprl_run* r) {
@@ -1456,11 +1480,13 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
   if ((s = device_alloc(&r->d_status, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(&r->scan_total, 1)) != APRL_OK) return cleanup(s);
   cudaMemsetAsync(r->d_status, 0, sizeof(DeviceStatus), r->stream);
-  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums), sizeof(ResidualSums)) != cudaSuccess ||
+  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums_pair), 2 * sizeof(ResidualSums)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_status), sizeof(DeviceStatus)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters), sizeof(TrialCounters)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters_pair), 2 * sizeof(TrialCounters)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_total), sizeof(unsigned long long)) != cudaSuccess)
     return cleanup(fail(APRL_ERR_CUDA, "cudaMallocHost failed"));
+  r->h_sums = r->h_sums_pair;
+  r->h_counters = r->h_counters_pair;
   r->offset = c.initial_offset;
   r->origin[0] = c.reference_origin[0];
   r->origin[1] = c.reference_origin[1];
@@ -1528,9 +1554,9 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   cudaFree(r->scan_count);
   cudaFree(r->scan_offset);
   cudaFree(r->scan_total);
-  cudaFreeHost(r->h_sums);
+  cudaFreeHost(r->h_sums_pair);
   cudaFreeHost(r->h_status);
-  cudaFreeHost(r->h_counters);
+  cudaFreeHost(r->h_counters_pair);
   cudaFreeHost(r->h_total);
   delete r;
   return APRL_OK;
@@ -1932,18 +1958,35 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
     bool converged = false;
     unsigned iterations = 0;
     double force = 0.0, work = 0.0;
-    for (unsigned t = 0; t < r->cfg.max_trials; ++t) {
+    unsigned t = 0;
+    if (r->cfg.max_trials >= 2) {
+      // The rule never stops after one trial that made residual calls, so
+      // the second trial is issued before the first one's residual is read.
+      // Without residual calls (no active particle) the second trial repeats
+      // the first (its J and particle states do not depend on the fields), and
+      // a first trial that converged is then reported as the only one.
+      TRY(enqueue_trial(r, 0));
+      TRY(enqueue_trial(r, 1));
+      TRY(check_device(r));
+      double res[4];
+      trial_read(r, 0, res);
+      iterations = 1;
+      converged = trial_converged(r->cfg, 1, res, force, work);
+      if (converged) {
+        double repeat[4];
+        trial_read(r, 1, repeat);
+      } else {
+        trial_read(r, 1, res);
+        iterations = 2;
+        converged = trial_converged(r->cfg, 2, res, force, work);
+      }
+      t = 2;
+    }
+    for (; !converged && t < r->cfg.max_trials; ++t) {
       double res[4];
       TRY(do_trial(r, res));
-      force = res[0];
-      work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
       iterations = t + 1;
-      // src/simulation_source_coupling.cpp:50
-      if (iterations >= (res[3] > 0. ? 2u : 1u) && force < r->cfg.force_tolerance &&
-          work < r->cfg.work_tolerance) {
-        converged = true;
-        break;
-      }
+      converged = trial_converged(r->cfg, iterations, res, force, work);
     }
     if (!converged)
       return fail(APRL_ERR_NOT_CONVERGED,
