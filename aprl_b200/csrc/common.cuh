@@ -96,7 +96,17 @@ struct GridT {
   int zb_e[3];           // ring bases of Ex Ey Ez
   int zb_b[3];           // ring bases of Bx By Bz
   F jcoef;               // (-1*dt)/eps0, applyCurrentSource(-1) scale
+  // Set for the kernels of a fixed-point trial issued ahead of the verdict
+  // on the previous one: nonzero once an earlier trial of the step has
+  // converged, and the trial's kernels then return at once.
+  const int* stop;
 };
+
+// True when the trial this grid view belongs to was made unnecessary.
+template <class F>
+__device__ __forceinline__ bool trial_skipped(const GridT<F>& g) {
+  return g.stop != nullptr && *g.stop != 0;
+}
 using DGrid = GridT<double>;
 
 template <class F>

@@ -354,6 +354,7 @@ __global__ void shift_insert_kernel(ShiftArgs<F> a) {
 // so the gather is unchanged bit for bit; W = float rounds it once.
 template <class W>
 __global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_current) {
+  if (trial_skipped(g)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;

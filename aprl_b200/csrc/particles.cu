@@ -859,6 +859,7 @@ __device__ unsigned carrier_segment(const GridT<F>& g, int shape, const DRegion&
 // like every ChargeConservingCurrentDepositor call.
 template <class F>
 __global__ void carrier_kernel(CarrierArgs<F> a) {
+  if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   CarrierState c;
@@ -1030,6 +1031,7 @@ __global__ void guess_gather_kernel(PushArgs<F> a) {
 // (src/simulation_moving_window.cpp:380-395).
 template <class F>
 __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
+  if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   const GridT<F>& g = a.g;
@@ -1200,6 +1202,7 @@ __device__ __forceinline__ double warp_max(double v) {
 
 template <class W, class F>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
+  if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double force = 0.0, defect = 0.0, scale = 0.0;
   const unsigned char seen = n < a.count ? a.slot.seen[n] : 0;
@@ -1471,6 +1474,7 @@ __global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
 // deposits its held chord of this step without endpoint validation.
 template <class F>
 __global__ void frozen_support_kernel(SupportArgs<F> a) {
+  if (trial_skipped(a.g)) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.count) return;
   const long long k = a.begin + i;
@@ -1507,6 +1511,31 @@ __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen,
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && z[i] < origin && !frozen[i])
     raise_error(status, kErrFellBehind, (unsigned long long)i);
+}
+
+__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums) {
+  if (trial_skipped(g)) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int c = 0; c < 3; ++c) {
+    const long long count = (long long)e_nx(g, c) * e_ny(g, c) * e_nz(g, c);
+    for (long long n = first; n < count; n += stride) g.j[c][n] = 0.;
+  }
+  if (first == 0) {
+    *counters = TrialCounters{};
+    *sums = ResidualSums{};
+  }
+}
+
+__global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iterations,
+                                     double force_tolerance, double work_tolerance, int* stop) {
+  if (*stop) return;
+  const double force = __longlong_as_double((long long)sums->force_bits);
+  const double calls = (double)sums->calls;
+  const double work =
+      calls == 0. ? 0. : (sums->scale > 0. ? sums->defect / sums->scale : sums->defect);
+  if (iterations >= (calls > 0. ? 2u : 1u) && force < force_tolerance && work < work_tolerance)
+    *stop = (int)iterations;
 }
 
 // The grid and J are binary64 in every mode; the gathers are built with

@@ -231,5 +231,12 @@ __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
 // an active particle may not fall behind the inlet; held ones may.
 __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen, long long n,
                                    double origin, DeviceStatus* status);
+// A trial's start: J, the trial counters and the residual sums cleared
+// (skipped with the trial).
+__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums);
+// solveConservativeSourceStep's stopping rule (src/simulation_source_coupling.cpp:50)
+// applied to trial `iterations`' residual sums: on convergence *stop = iterations.
+__global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iterations,
+                                     double force_tolerance, double work_tolerance, int* stop);
 
 }  // namespace aprl_gpu

@@ -56,7 +56,7 @@ enum Kernel : unsigned {
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
   kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
-  kGaussDeposit, kGaussResidual, kGaussFinish, kKernelCount
+  kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -66,7 +66,8 @@ const char* kKernelNames[kKernelCount] = {
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
   "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
-  "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish"};
+  "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish", "trial_clear",
+  "trial_verdict"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -227,6 +228,10 @@ struct Timing {
 
 }  // namespace
 
+// Fixed-point trials issued per step before the host reads any residual
+// (the usual count at FP64; FP32-mixed runs usually stop after two).
+constexpr unsigned kTrialSlots = 3;
+
 struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
@@ -294,8 +299,10 @@ struct aprl_run {
   size_t scan_cap = 0;
   // pinned host mirrors
   ResidualSums* h_sums = nullptr;        // the slot of the last trial read
-  ResidualSums* h_sums_pair = nullptr;   // two slots: a trial can be issued before
-  TrialCounters* h_counters_pair = nullptr;  // the previous one is read
+  ResidualSums* h_sums_slots = nullptr;  // one slot per trial issued ahead of a read
+  TrialCounters* h_counters_slots = nullptr;
+  int* d_stop = nullptr;                 // device verdict of the trials issued ahead
+  int* h_stop = nullptr;
   DeviceStatus* h_status = nullptr;
   TrialCounters* h_counters = nullptr;
   unsigned long long* h_total = nullptr;
@@ -1057,16 +1064,20 @@ aprl_status do_preview_electric(aprl_run* r) {
 
 // One coupling trial; W is the arithmetic of the gathers.
 template <class W>
-aprl_status trial_enqueue_t(aprl_run* r, int slot) {
+aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
   using F = double;
   if (r->stage != 2 && r->stage != 3)
     return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
   const aprl_run_config& c = r->cfg;
-  for (int a = 0; a < 3; ++a)
-    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
-  CUDA_TRY(cudaMemsetAsync(r->d_counters, 0, sizeof(TrialCounters), r->stream));
-  CUDA_TRY(cudaMemsetAsync(r->d_sums, 0, sizeof(ResidualSums), r->stream));
-  const GridT<F> g = make_grid<F>(r);
+  GridT<F> g = make_grid<F>(r);
+  if (ahead) g.stop = r->d_stop;
+  {
+    size_t most = 0;
+    for (int a = 0; a < 3; ++a) most = std::max(most, e_count(c, a));
+    const unsigned blocks = std::min<unsigned>(blocks_for(most, 256), 148 * 8);
+    TRY(launch(r, kTrialClear, trial_clear_kernel, dim3(blocks), dim3(256), g, r->d_counters,
+               r->d_sums));
+  }
   const DRegion region = make_region(r);
   if (r->queue.extracted) {
     // Frozen source support of the entries due within min(8, horizon) steps.
@@ -1182,9 +1193,13 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot) {
     ra.status = r->d_status;
     TRY(launch(r, kResidual, residual_kernel<W, F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
-  CUDA_TRY(cudaMemcpyAsync(&r->h_sums_pair[slot], r->d_sums, sizeof(ResidualSums),
+  if (ahead)
+    TRY(launch(r, kTrialVerdict, trial_verdict_kernel, dim3(1), dim3(1),
+               (const ResidualSums*)r->d_sums, r->trials + 1, c.force_tolerance,
+               c.work_tolerance, r->d_stop));
+  CUDA_TRY(cudaMemcpyAsync(&r->h_sums_slots[slot], r->d_sums, sizeof(ResidualSums),
                            cudaMemcpyDeviceToHost, r->stream));
-  CUDA_TRY(cudaMemcpyAsync(&r->h_counters_pair[slot], r->d_counters, sizeof(TrialCounters),
+  CUDA_TRY(cudaMemcpyAsync(&r->h_counters_slots[slot], r->d_counters, sizeof(TrialCounters),
                            cudaMemcpyDeviceToHost, r->stream));
   ++r->trials;
   r->stage = 3;
@@ -1194,8 +1209,8 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot) {
 // The residual of the trial copied to `slot` (after the stream has reached
 // it); the slot becomes the run's current trial counters.
 void trial_read(aprl_run* r, int slot, double residual[4]) {
-  r->h_sums = &r->h_sums_pair[slot];
-  r->h_counters = &r->h_counters_pair[slot];
+  r->h_sums = &r->h_sums_slots[slot];
+  r->h_counters = &r->h_counters_slots[slot];
   double force;
   const unsigned long long bits = r->h_sums->force_bits;
   std::memcpy(&force, &bits, sizeof force);
@@ -1205,8 +1220,8 @@ void trial_read(aprl_run* r, int slot, double residual[4]) {
   residual[3] = static_cast<double>(r->h_sums->calls);
 }
 
-aprl_status enqueue_trial(aprl_run* r, int slot) {
-  return r->fp32 ? trial_enqueue_t<float>(r, slot) : trial_enqueue_t<double>(r, slot);
+aprl_status enqueue_trial(aprl_run* r, int slot, bool ahead) {
+  return r->fp32 ? trial_enqueue_t<float>(r, slot, ahead) : trial_enqueue_t<double>(r, slot, ahead);
 }
 
 // solveConservativeSourceStep's stopping rule (src/simulation_source_coupling.cpp:50).
@@ -1219,7 +1234,7 @@ bool trial_converged(const aprl_run_config& c, unsigned iterations, const double
 }
 
 aprl_status do_trial(aprl_run* r, double residual[4]) {
-  TRY(enqueue_trial(r, 0));
+  TRY(enqueue_trial(r, 0, false));
   TRY(check_device(r));
   trial_read(r, 0, residual);
   return APRL_OK;
@@ -1480,13 +1495,17 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
   if ((s = device_alloc(&r->d_status, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(&r->scan_total, 1)) != APRL_OK) return cleanup(s);
   cudaMemsetAsync(r->d_status, 0, sizeof(DeviceStatus), r->stream);
-  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums_pair), 2 * sizeof(ResidualSums)) != cudaSuccess ||
+  if ((s = device_alloc(&r->d_stop, 1)) != APRL_OK) return cleanup(s);
+  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums_slots),
+                     kTrialSlots * sizeof(ResidualSums)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_status), sizeof(DeviceStatus)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters_pair), 2 * sizeof(TrialCounters)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters_slots),
+                     kTrialSlots * sizeof(TrialCounters)) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&r->h_stop), sizeof(int)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_total), sizeof(unsigned long long)) != cudaSuccess)
     return cleanup(fail(APRL_ERR_CUDA, "cudaMallocHost failed"));
-  r->h_sums = r->h_sums_pair;
-  r->h_counters = r->h_counters_pair;
+  r->h_sums = r->h_sums_slots;
+  r->h_counters = r->h_counters_slots;
   r->offset = c.initial_offset;
   r->origin[0] = c.reference_origin[0];
   r->origin[1] = c.reference_origin[1];
@@ -1554,9 +1573,11 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   cudaFree(r->scan_count);
   cudaFree(r->scan_offset);
   cudaFree(r->scan_total);
-  cudaFreeHost(r->h_sums_pair);
+  cudaFreeHost(r->h_sums_slots);
+  cudaFreeHost(r->h_stop);
+  cudaFree(r->d_stop);
   cudaFreeHost(r->h_status);
-  cudaFreeHost(r->h_counters_pair);
+  cudaFreeHost(r->h_counters_slots);
   cudaFreeHost(r->h_total);
   delete r;
   return APRL_OK;
@@ -1958,30 +1979,24 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
     bool converged = false;
     unsigned iterations = 0;
     double force = 0.0, work = 0.0;
+    // The first trials are issued without waiting: after each one a device
+    // verdict applies the stopping rule, and the kernels of the trials after
+    // a converged one return at once.  One round trip then reads them all.
+    const unsigned ahead = std::min<unsigned>(kTrialSlots, r->cfg.max_trials);
+    CUDA_TRY(cudaMemsetAsync(r->d_stop, 0, sizeof(int), r->stream));
+    for (unsigned t = 0; t < ahead; ++t) TRY(enqueue_trial(r, (int)t, true));
+    CUDA_TRY(cudaMemcpyAsync(r->h_stop, r->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
+                             r->stream));
+    TRY(check_device(r));
     unsigned t = 0;
-    if (r->cfg.max_trials >= 2) {
-      // The rule never stops after one trial that made residual calls, so
-      // the second trial is issued before the first one's residual is read.
-      // Without residual calls (no active particle) the second trial repeats
-      // the first (its J and particle states do not depend on the fields), and
-      // a first trial that converged is then reported as the only one.
-      TRY(enqueue_trial(r, 0));
-      TRY(enqueue_trial(r, 1));
-      TRY(check_device(r));
+    while (!converged && t < ahead) {
       double res[4];
-      trial_read(r, 0, res);
-      iterations = 1;
-      converged = trial_converged(r->cfg, 1, res, force, work);
-      if (converged) {
-        double repeat[4];
-        trial_read(r, 1, repeat);
-      } else {
-        trial_read(r, 1, res);
-        iterations = 2;
-        converged = trial_converged(r->cfg, 2, res, force, work);
-      }
-      t = 2;
+      trial_read(r, (int)t, res);
+      iterations = ++t;
+      converged = trial_converged(r->cfg, iterations, res, force, work);
     }
+    if ((converged ? (int)iterations : 0) != *r->h_stop)
+      return fail(APRL_ERR_RUNTIME, "Device and host verdicts on the coupling trials differ");
     for (; !converged && t < r->cfg.max_trials; ++t) {
       double res[4];
       TRY(do_trial(r, res));
