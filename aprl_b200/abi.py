@@ -168,6 +168,63 @@ class GaussLaw(C.Structure):
     as_dict = StepStats.as_dict
 
 
+SELF_FIELD_MODELS = {"relativistic-poisson": 0, "electrostatic-poisson": 1,
+                     "cowan-relativistic-poisson": 2}
+
+
+class SelfFieldConfig(C.Structure):
+    """aprl_self_field_config: EBGaussFieldInitializer::initialize's controls."""
+    _fields_ = [
+        ("model", C.c_int32),
+        ("include_transverse_cpml_particles", C.c_int32),
+        ("hold_transverse_until_activation", C.c_int32),
+        ("reserved", C.c_int32),
+        ("relative_tolerance", C.c_double),
+        ("maximum_mean_transverse_beta", C.c_double),
+        ("maximum_iterations", C.c_uint64),
+        ("guard_cells", C.c_uint64 * 3),
+    ]
+
+
+class SelfFieldReport(C.Structure):
+    """aprl_self_field_report: EBGaussInitializationReport."""
+    _fields_ = [
+        ("iterations", C.c_uint64),
+        ("relative_residual", C.c_double),
+        ("maximum_gauss_residual", C.c_double),
+        ("total_charge", C.c_double),
+        ("mean_beta_z", C.c_double),
+        ("mean_beta_transverse", C.c_double),
+        ("initial_electric_energy", C.c_double),
+        ("initial_magnetic_energy", C.c_double),
+        ("rms_position_cells", C.c_double * 3),
+        ("centre_padding_rms", C.c_double * 3),
+        ("static_field_guard_cells", C.c_uint64 * 3),
+        ("transverse_poisson_padding_cells", C.c_uint64),
+        ("temporary_bytes", C.c_uint64),
+    ]
+
+    as_dict = StepStats.as_dict
+
+
+def self_field_config(run_config, model="cowan-relativistic-poisson", tolerance=1e-10,
+                      maximum_iterations=20000, maximum_mean_transverse_beta=0.05,
+                      include_transverse_cpml_particles=False,
+                      hold_transverse_until_activation=False):
+    """The initializer controls with the CPML cells as the static guard."""
+    c = SelfFieldConfig()
+    c.model = SELF_FIELD_MODELS[model]
+    c.include_transverse_cpml_particles = int(include_transverse_cpml_particles)
+    c.hold_transverse_until_activation = int(hold_transverse_until_activation)
+    c.relative_tolerance = tolerance
+    c.maximum_mean_transverse_beta = maximum_mean_transverse_beta
+    c.maximum_iterations = maximum_iterations
+    c.guard_cells[0] = run_config.cpml_cells_x
+    c.guard_cells[1] = run_config.cpml_cells_y
+    c.guard_cells[2] = 0
+    return c
+
+
 def field_shape(config, component):
     """Yee extents (nx_c, ny_c, nz_c) of an ABI component (x fastest)."""
     cells = (config.nx, config.ny, config.nz)

@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUTPUT = os.path.join(HERE, "libaprl_b200.so")
-SOURCES = ["run.cu", "fields.cu", "particles.cu", "ledger.cu", "scan.cu"]
-HEADERS = ["common.cuh", "fields.cuh", "ledger.cuh", "particles.cuh"]
+SOURCES = ["run.cu", "fields.cu", "particles.cu", "ledger.cu", "selffield.cu", "scan.cu"]
+HEADERS = ["common.cuh", "dd.cuh", "fields.cuh", "ledger.cuh", "particles.cuh", "selffield.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

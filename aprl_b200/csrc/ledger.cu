@@ -7,54 +7,6 @@ constexpr double kElectronMass = 9.1093837139e-31;  // src/eb_field.cpp:18
 
 namespace {
 
-// Knuth's TwoSum: s + e == a + b exactly.
-__host__ __device__ __forceinline__ DD two_sum(double a, double b) {
-  const double s = a + b;
-  const double bb = s - a;
-  const double e = (a - (s - bb)) + (b - bb);
-  return DD{s, e};
-}
-
-// Requires |a| >= |b| (or a == 0).
-__host__ __device__ __forceinline__ DD quick_two_sum(double a, double b) {
-  const double s = a + b;
-  return DD{s, b - (s - a)};
-}
-
-// Dekker's exact product through a fused multiply-add.
-__host__ __device__ __forceinline__ DD two_prod(double a, double b) {
-  const double p = a * b;
-  return DD{p, fma(a, b, -p)};
-}
-
-__host__ __device__ __forceinline__ DD dd_add(DD a, DD b) {
-  DD s = two_sum(a.hi, b.hi);
-  const DD t = two_sum(a.lo, b.lo);
-  s.lo += t.hi;
-  s = quick_two_sum(s.hi, s.lo);
-  s.lo += t.lo;
-  return quick_two_sum(s.hi, s.lo);
-}
-
-__host__ __device__ __forceinline__ DD dd_neg(DD a) { return DD{-a.hi, -a.lo}; }
-
-__host__ __device__ __forceinline__ DD dd_mul(DD a, double b) {
-  DD p = two_prod(a.hi, b);
-  p.lo += a.lo * b;
-  return quick_two_sum(p.hi, p.lo);
-}
-
-// Division of a double-double by a double (QD library, Hida-Li-Bailey).
-__host__ __device__ __forceinline__ DD dd_div(DD a, double b) {
-  const double q1 = a.hi / b;
-  const DD p = two_prod(q1, b);
-  const DD s = two_sum(a.hi, -p.hi);
-  double e = s.lo - p.lo;
-  e += a.lo;
-  const double q2 = (s.hi + e) / b;
-  return quick_two_sum(q1, q2);
-}
-
 __device__ __forceinline__ double ex_at(const LedgerArgs& a, int i, int j, int k, bool sub) {
   if (sub && k == 0) return a.pre[0][(size_t)j * a.g.nx + i];
   return a.g.e_old[0][e_index(a.g, 0, i, j, k)];

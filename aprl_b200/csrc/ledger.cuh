@@ -16,12 +16,9 @@
 #pragma once
 
 #include "common.cuh"
+#include "dd.cuh"
 
 namespace aprl_gpu {
-
-struct DD {
-  double hi, lo;
-};
 
 enum LedgerKind : int {
   kLedgerPlane = 0,      // planeEnergy(k)

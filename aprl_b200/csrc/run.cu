@@ -26,6 +26,7 @@
 #include "fields.cuh"
 #include "ledger.cuh"
 #include "particles.cuh"
+#include "selffield.cuh"
 
 using namespace aprl_gpu;
 
@@ -56,7 +57,9 @@ enum Kernel : unsigned {
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
   kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
-  kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict, kKernelCount
+  kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict,
+  kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfAlpha, kSfUpdate, kSfBeta,
+  kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -67,7 +70,9 @@ const char* kKernelNames[kKernelCount] = {
   "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
   "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
   "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish", "trial_clear",
-  "trial_verdict"};
+  "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
+  "sf_alpha", "sf_update", "sf_beta", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
+  "sf_clear", "sf_gauss", "sf_energy"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -2225,6 +2230,344 @@ aprl_status aprl_run_gauss_law(aprl_run* r, aprl_gauss_law* out, double* residua
   out->total_charge = sums[1].hi + sums[1].lo;
   out->interior_nodes = interior;
   out->outside = bits[2];
+  return APRL_OK;
+}
+
+namespace {
+
+// Device buffers of one initial-field solve, released on every exit.
+struct SfBuffers {
+  double *slab[4] = {}, *rho = nullptr;
+  DD *partial = nullptr, *out = nullptr;
+  SfState* state = nullptr;
+  unsigned long long* max_bits = nullptr;
+  ~SfBuffers() {
+    for (double* p : slab) cudaFree(p);
+    cudaFree(rho);
+    cudaFree(partial);
+    cudaFree(out);
+    cudaFree(state);
+    cudaFree(max_bits);
+  }
+};
+
+aprl_status sf_read(aprl_run* r, const DD* device, DD* host, int count) {
+  CUDA_TRY(cudaMemcpyAsync(host, device, count * sizeof(DD), cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+}  // namespace
+
+aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_config* cfg,
+                                           aprl_self_field_report* rep) {
+  if (!r || !cfg || !rep) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "The initial self-field is set between steps");
+  std::memset(rep, 0, sizeof *rep);
+  const aprl_run_config& c = r->cfg;
+  if (!(cfg->relative_tolerance > 0.0) || !(cfg->relative_tolerance < 1.0) ||
+      !std::isfinite(cfg->relative_tolerance) || cfg->maximum_iterations == 0)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid initial Gauss-field convergence controls");
+  if (!(cfg->maximum_mean_transverse_beta >= 0.0) || !(cfg->maximum_mean_transverse_beta < 1.0) ||
+      !std::isfinite(cfg->maximum_mean_transverse_beta))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid initial self-field maximum mean transverse beta");
+  if (cfg->model < 0 || cfg->model > 2)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Unknown initial self-field model");
+  const bool include = cfg->include_transverse_cpml_particles != 0;
+  if (include && (cfg->guard_cells[0] < 2 || cfg->guard_cells[1] < 2))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Transverse CPML-source initialization requires at least two physical guard "
+                "cells in x and y");
+  const bool cowan = cfg->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON;
+  const bool relativistic = cfg->model == APRL_SELF_FIELD_RELATIVISTIC_POISSON || cowan;
+  const int pad = include ? 2 : 0;
+  const uint64_t cells[3] = {c.nx, c.ny, c.nz};
+  const uint64_t pcells[3] = {c.nx + 2 * pad, c.ny + 2 * pad, c.nz};
+  SfLattice L{};
+  int physical_lo[3], physical_hi[3];
+  for (int a = 0; a < 3; ++a) {
+    if (2 * cfg->guard_cells[a] + 2 >= cells[a])
+      return fail(APRL_ERR_INVALID_ARGUMENT,
+                  "Initial static-field guard leaves fewer than two physical cells");
+    physical_lo[a] = (int)cfg->guard_cells[a];
+    physical_hi[a] = (int)(cells[a] - cfg->guard_cells[a]);
+    L.lo[a] = include && a < 2 ? 0 : (int)cfg->guard_cells[a];
+    L.hi[a] = (int)(pcells[a] - L.lo[a]);
+  }
+  L.lx = (int)pcells[0] + 1;
+  L.ly = (int)pcells[1] + 1;
+  L.planes = (int)c.nz + 2;
+  L.pad = pad;
+  const size_t slab = (size_t)L.lx * L.ly * L.planes;
+  const size_t rho_count = (size_t)L.lx * L.ly * (c.nz + 1);
+
+  // clearFields (src/eb_field.cpp:265-269)
+  for (int a = 0; a < 3; ++a) {
+    CUDA_TRY(cudaMemsetAsync(r->e[r->cur][a], 0, e_count(c, a) * sizeof(double), r->stream));
+    CUDA_TRY(cudaMemsetAsync(r->b[a], 0, b_count(c, a) * sizeof(double), r->stream));
+  }
+  r->ledger_start_ready = false;
+
+  SfBuffers buf;
+  for (int q = 0; q < 4; ++q) TRY(device_alloc(&buf.slab[q], slab));
+  TRY(device_alloc(&buf.rho, rho_count));
+  TRY(device_alloc(&buf.partial, (size_t)kSelfFieldBlocks * kMoments));
+  TRY(device_alloc(&buf.out, 16));
+  TRY(device_alloc(&buf.state, 1));
+  TRY(device_alloc(&buf.max_bits, 1));
+  for (int q = 0; q < 4; ++q)
+    CUDA_TRY(cudaMemsetAsync(buf.slab[q], 0, slab * sizeof(double), r->stream));
+  CUDA_TRY(cudaMemsetAsync(buf.rho, 0, rho_count * sizeof(double), r->stream));
+
+  // meanVelocity and distributionResolution moments (src/eb_initial_field.cpp:629-741)
+  SfParticles P{r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m,
+                (long long)r->np, cfg->hold_transverse_until_activation != 0,
+                c.boost_gamma + c.boost_gamma_beta};
+  const int pblocks = (int)std::max<size_t>(1, std::min<size_t>(kSelfFieldBlocks,
+                                                                 blocks_for(r->np, kSelfFieldThreads)));
+  DD moments[kMoments] = {};
+  if (r->np) {
+    TRY(launch(r, kSfMoments, sf_moments_kernel, dim3(pblocks), dim3(kSelfFieldThreads), P,
+               buf.partial));
+    TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
+               (const DD*)buf.partial, pblocks, kMoments, buf.out));
+    TRY(sf_read(r, buf.out, moments, kMoments));
+  }
+  const long double m0 = sf_long(moments[0]);
+  if (!(m0 > 0.0L))
+    return fail(APRL_ERR_RUNTIME,
+                "Initial relativistic-Poisson field requires positive represented mass");
+  const double beta_x = (double)(sf_long(moments[1]) / m0);
+  const double beta_y = (double)(sf_long(moments[2]) / m0);
+  const double beta_z = (double)(sf_long(moments[3]) / m0);
+  const double beta_t = std::hypot(beta_x, beta_y);
+  if (!std::isfinite(beta_z) || !std::isfinite(beta_t) || beta_t >= 1.0 || std::fabs(beta_z) >= 1.0)
+    return fail(APRL_ERR_RUNTIME, "Initial particle mean velocity is not a finite subluminal vector");
+  if (relativistic && beta_t > cfg->maximum_mean_transverse_beta)
+    return fail(APRL_ERR_RUNTIME,
+                "%s mean beta_box_transverse=%.12g exceeds "
+                "initial_self_field.maximum_mean_transverse_beta=%.12g",
+                cowan ? "cowan-relativistic-poisson" : "relativistic-poisson", beta_t,
+                cfg->maximum_mean_transverse_beta);
+  const double applied = relativistic ? beta_z : 0.0;
+  const double longitudinal = std::fma(-applied, applied, 1.0);
+  if (!cowan && !(longitudinal > 64.0 * DBL_EPSILON))
+    return fail(APRL_ERR_RUNTIME,
+                "Initial relativistic-Poisson operator is ill-conditioned because the bunch "
+                "remains too relativistic in the simulation frame");
+
+  SfArgs A{};
+  A.g = make_grid<double>(r);
+  A.L = L;
+  A.potential = buf.slab[0];
+  A.residual = buf.slab[1];
+  A.direction = buf.slab[2];
+  A.image = buf.slab[3];
+  A.rho = buf.rho;
+  A.dx = c.dx;
+  A.dy = c.dy;
+  A.dz = c.dz;
+  A.cx = 1.0 / (c.dx * c.dx);
+  A.cy = 1.0 / (c.dy * c.dy);
+  A.cz = longitudinal / (c.dz * c.dz);
+  A.diagonal = 2.0 * (A.cx + A.cy + A.cz);
+  A.cowan = cowan ? 1 : 0;
+  A.tolerance = cfg->relative_tolerance;
+  A.partial = buf.partial;
+  A.state = buf.state;
+  for (int a = 0; a < 3; ++a) {
+    A.alpha[a] = r->coeff[a];
+    A.beta[a] = r->coeff[3 + a];
+  }
+  A.delta[0] = r->coeff[7];  // deltaYZ
+  A.delta[1] = r->coeff[8];  // deltaZX
+  A.delta[2] = r->coeff[6];  // deltaXY
+  if (cowan) {
+    // CowanPoissonOperator (src/eb_initial_field.cpp:246-316)
+    const double velocity = applied * kC;
+    A.translation = velocity * velocity * kEpsilon0 * kMu0;
+    const double spacing[3] = {c.dx, c.dy, c.dz};
+    double st[3][3][3] = {};
+    for (int axis = 0; axis < 3; ++axis) {
+      const int ta = (axis + 1) % 3, tb = (axis + 2) % 3;
+      const double delta = A.delta[axis];
+      double minimum = INFINITY;
+      for (int a = -1; a <= 1; a += 2)
+        for (int b = -1; b <= 1; b += 2)
+          minimum = std::min(minimum, A.alpha[axis] + 2.0 * A.beta[ta] * a +
+                                          2.0 * A.beta[tb] * b + 4.0 * delta * a * b);
+      if (axis == 2) minimum -= A.translation;
+      if (!(minimum > 64.0 * DBL_EPSILON))
+        return fail(APRL_ERR_RUNTIME,
+                    "Initial Cowan-Poisson operator fails the sufficient positive-definiteness "
+                    "bound on axis %d: minimum smoothing symbol=%.12g",
+                    axis, minimum);
+      const double inverse2 = 1.0 / (spacing[axis] * spacing[axis]);
+      for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b) {
+          const double weight =
+              a == 0 ? (b == 0 ? A.alpha[axis] : A.beta[tb]) : (b == 0 ? A.beta[ta] : delta);
+          int pt[3] = {1, 1, 1};
+          pt[ta] += a;
+          pt[tb] += b;
+          st[pt[2]][pt[1]][pt[0]] += 2.0 * weight * inverse2;
+          --pt[axis];
+          st[pt[2]][pt[1]][pt[0]] -= weight * inverse2;
+          pt[axis] += 2;
+          st[pt[2]][pt[1]][pt[0]] -= weight * inverse2;
+        }
+    }
+    const double tz = A.translation / (c.dz * c.dz);
+    st[1][1][1] -= 2.0 * tz;
+    st[0][1][1] += tz;
+    st[2][1][1] += tz;
+    std::memcpy(A.stencil, st, sizeof st);
+  }
+  rep->mean_beta_z = beta_z;
+  rep->mean_beta_transverse = beta_t;
+  rep->transverse_poisson_padding_cells = pad;
+  for (int a = 0; a < 3; ++a) rep->static_field_guard_cells[a] = L.lo[a];
+  {
+    // distributionResolution (src/eb_initial_field.cpp:693-741)
+    const double spacing[3] = {c.dx, c.dy, c.dz};
+    const double origin[3] = {r->origin[0] - (double)pad * c.dx, r->origin[1] - (double)pad * c.dy,
+                              r->origin[2]};
+    for (int a = 0; a < 3; ++a) {
+      const long double mean = sf_long(moments[4 + a]) / m0;
+      const long double variance = std::max(0.0L, sf_long(moments[7 + a]) / m0 - mean * mean);
+      const double rms = (double)std::sqrt(variance);
+      rep->rms_position_cells[a] = rms / spacing[a];
+      if (rms > 0.0) {
+        const double lower = origin[a] + (double)L.lo[a] * spacing[a];
+        const double upper = origin[a] + (double)L.hi[a] * spacing[a];
+        rep->centre_padding_rms[a] = std::min((double)mean - lower, upper - (double)mean) / rms;
+      }
+    }
+  }
+  rep->temporary_bytes = 4 * slab * sizeof(double) +
+                         (size_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1) * sizeof(double) +
+                         (pad ? rho_count * sizeof(double) : 0);
+
+  // The CIC charge and the Poisson source (src/eb_initial_field.cpp:979-1027)
+  const DGrid g = make_grid<double>(r);
+  TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
+             buf.rho, L.lx, L.ly, pad, r->d_status));
+  const int nblocks = (int)std::min<size_t>(kSelfFieldBlocks,
+                                            blocks_for(slab, kSelfFieldThreads));
+  const DD vertex_volume = ledger_product(ledger_product(c.dx, c.dy), c.dz);
+  TRY(launch(r, kSfSource, sf_source_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A,
+             vertex_volume));
+  TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
+             (const DD*)buf.partial, nblocks, 2, buf.out));
+  DD sums[2];
+  TRY(sf_read(r, buf.out, sums, 2));
+  TRY(check_device(r));
+  const long double total = sf_long(moments[10]);
+  rep->total_charge = (double)total;
+  const long double interior = sf_long(sums[0]);
+  if (std::fabs((interior - total) / total) > 1.0e-12L)
+    return fail(APRL_ERR_RUNTIME,
+                "Initial CIC charge cloud touches the static zero-potential boundary; move every "
+                "particle at least one complete cell inside the CPML entrance or enlarge the "
+                "physical mesh padding");
+  if (!(sums[1].hi > 0.0) || !std::isfinite(sums[1].hi))
+    return fail(APRL_ERR_RUNTIME, "Initial particle charge produced an invalid Poisson source norm");
+
+  // Conjugate gradients, in batches of iterations between host reads.
+  SfState state{};
+  state.rr = sums[1];
+  state.source = sums[1];
+  CUDA_TRY(cudaMemcpyAsync(buf.state, &state, sizeof state, cudaMemcpyHostToDevice, r->stream));
+  uint64_t issued = 0;
+  while (issued < cfg->maximum_iterations) {
+    const uint64_t batch = std::min<uint64_t>(32, cfg->maximum_iterations - issued);
+    for (uint64_t it = 0; it < batch; ++it) {
+      TRY(launch(r, kSfApply, sf_apply_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
+      TRY(launch(r, kSfAlpha, sf_alpha_kernel, dim3(1), dim3(kSelfFieldThreads), A, nblocks));
+      TRY(launch(r, kSfUpdate, sf_update_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
+      TRY(launch(r, kSfBeta, sf_beta_kernel, dim3(1), dim3(kSelfFieldThreads), A, nblocks));
+      TRY(launch(r, kSfDirection, sf_direction_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
+    }
+    issued += batch;
+    CUDA_TRY(cudaMemcpyAsync(&state, buf.state, sizeof state, cudaMemcpyDeviceToHost, r->stream));
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    if (state.done) break;
+  }
+  rep->iterations = state.iterations;
+  if (state.done == 2) return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG lost positive definiteness");
+  if (state.done == 3)
+    return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG produced a non-finite residual");
+  if (state.done != 1 || state.relative > cfg->relative_tolerance)
+    return fail(APRL_ERR_RUNTIME,
+                "Initial Gauss-field solve did not converge; increase "
+                "initial_self_field.maximum_iterations, relax its relative_tolerance, or reduce "
+                "the grid aspect ratio");
+
+  // E and B from the potential (src/eb_initial_field.cpp:427-553)
+  const int fblocks = (int)std::min<size_t>(kSelfFieldBlocks * 2, blocks_for(slab, 256));
+  if (cowan) {
+    for (int axis = 0; axis < 3; ++axis) {
+      CUDA_TRY(cudaMemsetAsync(A.image, 0, slab * sizeof(double), r->stream));
+      TRY(launch(r, kSfSmooth, sf_smooth_kernel, dim3(fblocks), dim3(256), A, axis));
+      TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, axis, 1.0, 1));
+    }
+  } else {
+    TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, 0, 1.0, 0));
+    TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, 1, 1.0, 0));
+    TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, 2, longitudinal,
+               0));
+  }
+  const double scale = cowan ? applied * kC * kEpsilon0 * kMu0 : applied / kC;
+  const double upper_w = 0.5 + 0.5 * applied * kC * c.dt / c.dz;
+  const double lower_w = 1.0 - upper_w;
+  if (upper_w < 0.0 || upper_w > 1.0)
+    return fail(APRL_ERR_RUNTIME, "Initial B half-step shift exceeds one longitudinal cell");
+  TRY(launch(r, kSfMagnetic, sf_magnetic_kernel, dim3(fblocks), dim3(256), A, scale, lower_w,
+             upper_w));
+  if (include)
+    for (int comp = 0; comp < 6; ++comp)
+      TRY(launch(r, kSfClear, sf_clear_outside_kernel, dim3(fblocks), dim3(256), A, comp,
+                 (int)cfg->guard_cells[0], (int)cfg->guard_cells[1], (int)cfg->guard_cells[2]));
+
+  // validateGauss on the unpadded CIC charge (src/eb_initial_field.cpp:1083-1091)
+  const int vx = (int)c.nx + 1, vy = (int)c.ny + 1;
+  CUDA_TRY(cudaMemsetAsync(buf.rho, 0, (size_t)vx * vy * (c.nz + 1) * sizeof(double), r->stream));
+  CUDA_TRY(cudaMemsetAsync(buf.max_bits, 0, sizeof(unsigned long long), r->stream));
+  TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
+             buf.rho, vx, vy, 0, r->d_status));
+  const int gblocks = (int)std::min<size_t>(kSelfFieldBlocks,
+                                            blocks_for((size_t)vx * vy * c.nz, kSelfFieldThreads));
+  TRY(launch(r, kSfGauss, sf_gauss_kernel, dim3(gblocks), dim3(kSelfFieldThreads), A,
+             (const double*)buf.rho, physical_lo[0], physical_hi[0], physical_lo[1],
+             physical_hi[1], physical_lo[2], physical_hi[2], buf.max_bits));
+  TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
+             (const DD*)buf.partial, gblocks, 2, buf.out));
+  TRY(sf_read(r, buf.out, sums, 2));
+  TRY(check_device(r));
+  unsigned long long worst_bits = 0;
+  CUDA_TRY(cudaMemcpy(&worst_bits, buf.max_bits, sizeof worst_bits, cudaMemcpyDeviceToHost));
+  double worst;
+  std::memcpy(&worst, &worst_bits, sizeof worst);
+  const long double res2 = sf_long(sums[0]), src2 = sf_long(sums[1]);
+  rep->relative_residual = src2 > 0.0L ? (double)std::sqrt(res2 / src2) : 0.0;
+  rep->maximum_gauss_residual = worst;
+  if (rep->relative_residual > 4.0 * cfg->relative_tolerance)
+    return fail(APRL_ERR_RUNTIME, "Initial E field failed the post-solve discrete Gauss check");
+
+  // initialFieldEnergy (src/eb_initial_field.cpp:665-691)
+  const DD electric_factor = ledger_product(vertex_volume, 0.5 * kEpsilon0);
+  const DD magnetic_factor = dd_div(ledger_product(vertex_volume, 0.5), kMu0);
+  A.stencil[0] = magnetic_factor.hi;
+  A.stencil[1] = magnetic_factor.lo;
+  const int eblocks = (int)std::min<size_t>(kSelfFieldBlocks,
+                                            blocks_for((size_t)c.nx * c.ny * c.nz, kSelfFieldThreads));
+  TRY(launch(r, kSfEnergy, sf_energy_kernel, dim3(eblocks), dim3(kSelfFieldThreads), A,
+             electric_factor));
+  TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
+             (const DD*)buf.partial, eblocks, 2, buf.out));
+  TRY(sf_read(r, buf.out, sums, 2));
+  rep->initial_electric_energy = (double)sf_long(sums[0]);
+  rep->initial_magnetic_energy = (double)sf_long(sums[1]);
   return APRL_OK;
 }
 

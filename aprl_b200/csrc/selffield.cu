@@ -1,0 +1,492 @@
+// selffield.cu -- kernels of the initial self-field solve (selffield.cuh).
+#include "selffield.cuh"
+
+namespace aprl_gpu {
+
+namespace {
+
+__device__ DD sf_block_sum(DD v, DD* shared) {
+  const int t = threadIdx.x;
+  shared[t] = v;
+  __syncthreads();
+  for (int s = kSelfFieldThreads / 2; s > 0; s >>= 1) {
+    if (t < s) shared[t] = dd_add(shared[t], shared[t + s]);
+    __syncthreads();
+  }
+  const DD out = shared[0];
+  __syncthreads();
+  return out;
+}
+
+// positiveLightFrontComponent, properVelocityFromPositiveLightFront and
+// heldLongitudinalBetaZ (src/boostframe.cpp:89-167).
+__device__ __forceinline__ double sf_positive(double u0, double u1, double u2) {
+  const double gamma = gamma_u(u0, u1, u2);
+  const double tms = fma(u0, u0, fma(u1, u1, 1.0));
+  if (u2 >= 0.0) return gamma + u2;
+  return tms / (gamma - u2);
+}
+__device__ __forceinline__ double sf_longitudinal(double u0, double u1, double positive) {
+  const double tms = fma(u0, u0, fma(u1, u1, 1.0));
+  const double negative = tms / positive;
+  return 0.5 * (positive - negative);
+}
+__device__ __forceinline__ double sf_held_beta_z(double u0, double u1, double u2,
+                                                 double rapidity) {
+  const double lab = sf_longitudinal(u0, u1, sf_positive(u0, u1, u2) * rapidity);
+  const double box = sf_longitudinal(0.0, 0.0, sf_positive(0.0, 0.0, lab) / rapidity);
+  return box / hypot(1.0, box);
+}
+
+__device__ __forceinline__ bool sf_interior(const SfLattice& L, int i, int j, int k) {
+  return i > L.lo[0] && i < L.hi[0] && j > L.lo[1] && j < L.hi[1] && k > L.lo[2] &&
+         k < L.hi[2];
+}
+
+__device__ __forceinline__ size_t sf_at(const SfLattice& L, int i, int j, int p) {
+  return ((size_t)p * L.ly + j) * L.lx + i;
+}
+
+// Node n of the planes 1..nz of the lattice: i, j and the plane p.
+__device__ __forceinline__ void sf_node(const SfLattice& L, long long n, int& i, int& j, int& p) {
+  i = (int)(n % L.lx);
+  const long long r = n / L.lx;
+  j = (int)(r % L.ly);
+  p = 1 + (int)(r / L.ly);
+}
+
+__device__ __forceinline__ long long sf_nodes(const SfLattice& L) {
+  return (long long)L.lx * L.ly * (L.planes - 2);
+}
+
+__device__ __forceinline__ bool sf_stopped(const SfArgs& a) { return a.state->done != 0; }
+
+}  // namespace
+
+// Host helpers.
+double sf_ratio(DD a, DD b) { return dd_value(dd_div_dd(a, b)); }
+long double sf_long(DD a) { return (long double)a.hi + (long double)a.lo; }
+
+// Per-block partial moments of the particles: mass, mass * beta (x, y, z;
+// or the held longitudinal beta_z), mass * position, mass * position^2,
+// charge (meanVelocity and distributionResolution,
+// src/eb_initial_field.cpp:629-741, and the total charge).
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_moments_kernel(SfParticles p, DD* partial) {
+  __shared__ DD shared[kSelfFieldThreads];
+  DD m[kMoments];
+  for (int q = 0; q < kMoments; ++q) m[q] = DD{0., 0.};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < p.n;
+       n += (long long)gridDim.x * blockDim.x) {
+    const double w = p.m[n];
+    const double u0 = p.ux[n], u1 = p.uy[n], u2 = p.uz[n];
+    m[0] = dd_add(m[0], DD{w, 0.});
+    if (p.hold) {
+      m[3] = dd_add(m[3], two_prod(w, sf_held_beta_z(u0, u1, u2, p.rapidity)));
+    } else {
+      const double gamma = gamma_u(u0, u1, u2);
+      m[1] = dd_add(m[1], two_prod(w, u0 / gamma));
+      m[2] = dd_add(m[2], two_prod(w, u1 / gamma));
+      m[3] = dd_add(m[3], two_prod(w, u2 / gamma));
+    }
+    const double x[3] = {p.x[n], p.y[n], p.z[n]};
+    for (int a = 0; a < 3; ++a) {
+      const DD wx = two_prod(w, x[a]);
+      m[4 + a] = dd_add(m[4 + a], wx);
+      m[7 + a] = dd_add(m[7 + a], dd_mul(wx, x[a]));
+    }
+    m[10] = dd_add(m[10], DD{p.q[n], 0.});
+  }
+  for (int q = 0; q < kMoments; ++q) {
+    const DD s = sf_block_sum(m[q], shared);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * kMoments + q] = s;
+  }
+}
+
+// One block: the partials of `quantities` sums, in block order.
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_finish_kernel(const DD* partial, int blocks,
+                                                                     int quantities, DD* out) {
+  __shared__ DD shared[kSelfFieldThreads];
+  for (int q = 0; q < quantities; ++q) {
+    DD s{0., 0.};
+    for (int b = threadIdx.x; b < blocks; b += kSelfFieldThreads)
+      s = dd_add(s, partial[(size_t)b * quantities + q]);
+    s = sf_block_sum(s, shared);
+    if (threadIdx.x == 0) out[q] = s;
+  }
+}
+
+// ChargeConservingCurrentDepositor::depositCharge (src/eb_deposition.cpp:168-193,
+// validatePosition 228-246, normalize 250-262, containingCell 264-279) into a
+// lattice lx nodes wide with the Maxwell grid's vertices at offset `pad`.
+__global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly, int pad,
+                                  DeviceStatus* status) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= p.n) return;
+  const double pos[3] = {p.x[n], p.y[n], p.z[n]};
+  const double h[3] = {g.dx, g.dy, g.dz};
+  const int cells[3] = {g.nx, g.ny, g.nz};
+  const double extent[3] = {(double)g.nx * g.dx, (double)g.ny * g.dy, (double)g.nz * g.dz};
+  int c[3];
+  double f[3];
+  for (int a = 0; a < 3; ++a) {
+    const double relative = pos[a] - g.origin[a];
+    const double tol = 64.0 * kEpsilon * fmax(1.0, fmax(fabs(g.origin[a]), extent[a]));
+    if (!isfinite(pos[a]) || relative < -tol || relative > extent[a] + tol) {
+      raise_error(status, kErrDepositOutside, (unsigned long long)n);
+      return;
+    }
+    const double x = fmax(0.0, fmin((double)cells[a], (pos[a] - g.origin[a]) / h[a]));
+    c[a] = x <= 0.0 ? 0 : (x >= (double)cells[a] ? cells[a] - 1 : (int)floor(x));
+    f[a] = fmax(0.0, fmin(1.0, x - (double)c[a]));
+  }
+  const double inverse_volume = 1.0 / (g.dx * g.dy * g.dz);
+  for (int cz = 0; cz < 2; ++cz)
+    for (int b = 0; b < 2; ++b)
+      for (int a = 0; a < 2; ++a) {
+        const double sa = a ? f[0] : 1.0 - f[0];
+        const double sb = b ? f[1] : 1.0 - f[1];
+        const double sc = cz ? f[2] : 1.0 - f[2];
+        atomicAdd(&rho[((size_t)(c[2] + cz) * ly + (c[1] + b + pad)) * lx + (c[0] + a + pad)],
+                  p.q[n] * inverse_volume * sa * sb * sc);
+      }
+}
+
+// The Poisson source rho/eps0 at the interior vertices (into the residual
+// and the first direction), with partial sums of the interior charge and of
+// the source norm (src/eb_initial_field.cpp:991-1027).
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_source_kernel(SfArgs a, DD volume) {
+  __shared__ DD shared[kSelfFieldThreads];
+  const SfLattice& L = a.L;
+  DD charge{0., 0.}, source{0., 0.};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, p;
+    sf_node(L, n, i, j, p);
+    if (!sf_interior(L, i, j, p - 1)) continue;
+    const double q = a.rho[((size_t)(p - 1) * L.ly + j) * L.lx + i];
+    const double v = q / kEpsilon0;
+    a.residual[sf_at(L, i, j, p)] = v;
+    a.direction[sf_at(L, i, j, p)] = v;
+    charge = dd_add(charge, dd_mul(volume, q));
+    source = dd_add(source, two_prod(v, v));
+  }
+  charge = sf_block_sum(charge, shared);
+  source = sf_block_sum(source, shared);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = charge;
+    a.partial[2 * blockIdx.x + 1] = source;
+  }
+}
+
+// image = A direction at the interior vertices: the 7-point relativistic
+// operator (applyNegativeLaplacian, src/eb_initial_field.cpp:210-236) or the
+// 27-point Cowan one (applyNegativeCowanLaplacian, :318-342); partial sums
+// of direction . image.
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_apply_kernel(SfArgs a) {
+  __shared__ DD shared[kSelfFieldThreads];
+  if (sf_stopped(a)) return;
+  const SfLattice& L = a.L;
+  DD dot{0., 0.};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, p;
+    sf_node(L, n, i, j, p);
+    if (!sf_interior(L, i, j, p - 1)) continue;
+    const double* d = a.direction;
+    double value;
+    if (a.cowan) {
+      value = 0.0;
+#pragma unroll
+      for (int z = 0; z < 3; ++z)
+#pragma unroll
+        for (int y = 0; y < 3; ++y)
+#pragma unroll
+          for (int x = 0; x < 3; ++x)
+            value += a.stencil[(z * 3 + y) * 3 + x] * d[sf_at(L, i - 1 + x, j - 1 + y, p - 1 + z)];
+    } else {
+      value = a.diagonal * d[sf_at(L, i, j, p)] -
+              a.cx * (d[sf_at(L, i - 1, j, p)] + d[sf_at(L, i + 1, j, p)]) -
+              a.cy * (d[sf_at(L, i, j - 1, p)] + d[sf_at(L, i, j + 1, p)]) -
+              a.cz * (d[sf_at(L, i, j, p - 1)] + d[sf_at(L, i, j, p + 1)]);
+    }
+    a.image[sf_at(L, i, j, p)] = value;
+    dot = dd_add(dot, two_prod(d[sf_at(L, i, j, p)], value));
+  }
+  dot = sf_block_sum(dot, shared);
+  if (threadIdx.x == 0) a.partial[blockIdx.x] = dot;
+}
+
+// alpha = |r|^2 / (d . A d), rounded once to binary64.
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_alpha_kernel(SfArgs a, int blocks) {
+  __shared__ DD shared[kSelfFieldThreads];
+  if (sf_stopped(a)) return;
+  DD s{0., 0.};
+  for (int b = threadIdx.x; b < blocks; b += kSelfFieldThreads) s = dd_add(s, a.partial[b]);
+  s = sf_block_sum(s, shared);
+  if (threadIdx.x != 0) return;
+  SfState& st = *a.state;
+  st.denominator = s;
+  if (!(s.hi > 0.) || !isfinite(s.hi)) {
+    st.done = 2;
+    return;
+  }
+  st.alpha = dd_value(dd_div_dd(st.rr, s));
+}
+
+// potential += alpha d, residual += (-alpha) A d at the interior vertices
+// (updateInterior, src/eb_initial_field.cpp:405-421); partial sums of |r|^2.
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_update_kernel(SfArgs a) {
+  __shared__ DD shared[kSelfFieldThreads];
+  if (sf_stopped(a)) return;
+  const SfLattice& L = a.L;
+  const double alpha = a.state->alpha;
+  DD dot{0., 0.};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, p;
+    sf_node(L, n, i, j, p);
+    if (!sf_interior(L, i, j, p - 1)) continue;
+    const size_t at = sf_at(L, i, j, p);
+    a.potential[at] += alpha * a.direction[at];
+    const double r = a.residual[at] + -alpha * a.image[at];
+    a.residual[at] = r;
+    dot = dd_add(dot, two_prod(r, r));
+  }
+  dot = sf_block_sum(dot, shared);
+  if (threadIdx.x == 0) a.partial[blockIdx.x] = dot;
+}
+
+// The relative residual, the stopping test and beta
+// (src/eb_initial_field.cpp:1046-1064).
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_beta_kernel(SfArgs a, int blocks) {
+  __shared__ DD shared[kSelfFieldThreads];
+  if (sf_stopped(a)) return;
+  DD s{0., 0.};
+  for (int b = threadIdx.x; b < blocks; b += kSelfFieldThreads) s = dd_add(s, a.partial[b]);
+  s = sf_block_sum(s, shared);
+  if (threadIdx.x != 0) return;
+  SfState& st = *a.state;
+  st.next = s;
+  st.iterations += 1;
+  st.relative = dd_value(dd_sqrt(dd_div_dd(s, st.source)));
+  if (st.relative <= a.tolerance) {
+    st.rr = s;
+    st.done = 1;
+    return;
+  }
+  if (!(s.hi >= 0.) || !isfinite(s.hi)) {
+    st.done = 3;
+    return;
+  }
+  st.beta = dd_value(dd_div_dd(s, st.rr));
+  st.rr = s;
+}
+
+// direction = r + beta direction at the interior vertices, zero elsewhere
+// (combineDirection, src/eb_initial_field.cpp:423-438).
+__global__ void sf_direction_kernel(SfArgs a) {
+  if (sf_stopped(a)) return;
+  const SfLattice& L = a.L;
+  const double beta = a.state->beta;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, p;
+    sf_node(L, n, i, j, p);
+    const size_t at = sf_at(L, i, j, p);
+    a.direction[at] = sf_interior(L, i, j, p - 1) ? a.residual[at] + beta * a.direction[at] : 0.0;
+  }
+}
+
+// The Cowan-smoothed potential of one axis minus the translation term, at
+// the interior vertices, into `image` (cowanSmoothedPotential and
+// fieldsFromCowanPotential, src/eb_initial_field.cpp:344-382, 503-517).
+__global__ void sf_smooth_kernel(SfArgs a, int axis) {
+  const SfLattice& L = a.L;
+  const int ta = (axis + 1) % 3, tb = (axis + 2) % 3;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, p;
+    sf_node(L, n, i, j, p);
+    if (!sf_interior(L, i, j, p - 1)) continue;
+    const double* phi = a.potential;
+    double value = a.alpha[axis] * phi[sf_at(L, i, j, p)];
+    for (int sign = -1; sign <= 1; sign += 2) {
+      int pa[3] = {i, j, p}, pb[3] = {i, j, p};
+      pa[ta] += sign;
+      pb[tb] += sign;
+      value += a.beta[ta] * phi[sf_at(L, pa[0], pa[1], pa[2])];
+      value += a.beta[tb] * phi[sf_at(L, pb[0], pb[1], pb[2])];
+    }
+    for (int s = -1; s <= 1; s += 2)
+      for (int t = -1; t <= 1; t += 2) {
+        int pt[3] = {i, j, p};
+        pt[ta] += s;
+        pt[tb] += t;
+        value += a.delta[axis] * phi[sf_at(L, pt[0], pt[1], pt[2])];
+      }
+    a.image[sf_at(L, i, j, p)] =
+        value - (axis == 2 ? a.translation * phi[sf_at(L, i, j, p)] : 0.0);
+  }
+}
+
+// One E component from the potential (or its smoothed form) by a forward
+// difference, E = -(coefficient * difference) / spacing
+// (fieldsFromPotential and fieldsFromCowanPotential,
+// src/eb_initial_field.cpp:427-449, 518-527), into the run's E.
+__global__ void sf_electric_kernel(SfArgs a, int axis, double coefficient, int from_smoothed) {
+  const DGrid& g = a.g;
+  const SfLattice& L = a.L;
+  const int nxc = e_nx(g, axis), nyc = e_ny(g, axis), nzc = e_nz(g, axis);
+  const long long count = (long long)nxc * nyc * nzc;
+  const double* s = from_smoothed ? a.image : a.potential;
+  const double h = axis == 0 ? g.dx : (axis == 1 ? g.dy : g.dz);
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % nxc);
+    const int j = (int)((n / nxc) % nyc);
+    const int k = (int)(n / ((long long)nxc * nyc));
+    const double upper = s[sf_at(L, i + L.pad + (axis == 0), j + L.pad + (axis == 1),
+                                 k + 1 + (axis == 2))];
+    const double lower = s[sf_at(L, i + L.pad, j + L.pad, k + 1)];
+    g.e_old[axis][e_index(g, axis, i, j, k)] = -coefficient * (upper - lower) / h;
+  }
+}
+
+// B at the half step from E of the rigidly translating charge
+// (src/eb_initial_field.cpp:451-484, 529-552).
+__global__ void sf_magnetic_kernel(SfArgs a, double scale, double lower_w, double upper_w) {
+  const DGrid& g = a.g;
+  const long long per = (long long)(g.nx + 1) * (g.ny + 1) * g.nz;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < per;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % (g.nx + 1));
+    const int j = (int)((n / (g.nx + 1)) % (g.ny + 1));
+    const int k = (int)(n / ((long long)(g.nx + 1) * (g.ny + 1)));
+    if (j < g.ny)  // Bx (nx+1, ny, nz)
+      g.b[0][b_index(g, 0, i, j, k)] =
+          -scale * (lower_w * g.e_old[1][e_index(g, 1, i, j, k)] +
+                    upper_w * g.e_old[1][e_index(g, 1, i, j, k + 1)]);
+    if (i < g.nx)  // By (nx, ny+1, nz)
+      g.b[1][b_index(g, 1, i, j, k)] =
+          scale * (lower_w * g.e_old[0][e_index(g, 0, i, j, k)] +
+                   upper_w * g.e_old[0][e_index(g, 0, i, j, k + 1)]);
+  }
+  const long long bz = (long long)g.nx * g.ny * (g.nz + 1);
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < bz;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % g.nx);
+    const int j = (int)((n / g.nx) % g.ny);
+    const int k = (int)(n / ((long long)g.nx * g.ny));
+    g.b[2][b_index(g, 2, i, j, k)] = 0.0;
+  }
+}
+
+// clearComponentOutsidePhysical (src/eb_initial_field.cpp:564-607) for
+// component 0..5 (Ex Ey Ez Bx By Bz).
+__global__ void sf_clear_outside_kernel(SfArgs a, int component, int gx, int gy, int gz) {
+  const DGrid& g = a.g;
+  const bool electric = component < 3;
+  const int axis = component % 3;
+  const int n3[3] = {electric ? e_nx(g, axis) : b_nx(g, axis),
+                     electric ? e_ny(g, axis) : b_ny(g, axis),
+                     electric ? e_nz(g, axis) : b_nz(g, axis)};
+  const int cells[3] = {g.nx, g.ny, g.nz};
+  const int guard[3] = {gx, gy, gz};
+  const long long count = (long long)n3[0] * n3[1] * n3[2];
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int c[3] = {(int)(n % n3[0]), (int)((n / n3[0]) % n3[1]),
+                      (int)(n / ((long long)n3[0] * n3[1]))};
+    bool inside = true;
+    for (int d = 0; d < 3; ++d) {
+      const bool vertex = electric ? d != axis : d == axis;
+      inside = inside && c[d] >= guard[d] &&
+               (vertex ? c[d] <= cells[d] - guard[d] : c[d] < cells[d] - guard[d]);
+    }
+    if (inside) continue;
+    if (electric)
+      g.e_old[axis][e_index(g, axis, c[0], c[1], c[2])] = 0.0;
+    else
+      g.b[axis][b_index(g, axis, c[0], c[1], c[2])] = 0.0;
+  }
+}
+
+// validateGauss (src/eb_initial_field.cpp:743-806): partial sums of the
+// squared Gauss error and source over the physical interior vertices, and
+// their largest error.
+__global__ void __launch_bounds__(kSelfFieldThreads)
+sf_gauss_kernel(SfArgs a, const double* rho, int plo0, int phi0, int plo1, int phi1, int plo2,
+                int phi2, unsigned long long* max_bits) {
+  __shared__ DD shared[kSelfFieldThreads];
+  const DGrid& g = a.g;
+  const int vx = g.nx + 1, vy = g.ny + 1;
+  const long long count = (long long)vx * vy * g.nz;
+  DD res{0., 0.}, src{0., 0.};
+  double worst = 0.0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % vx);
+    const int j = (int)((n / vx) % vy);
+    const int k = (int)(n / ((long long)vx * vy));
+    if (!(k > plo2 && k < phi2 && j > plo1 && j < phi1 && i > plo0 && i < phi0)) continue;
+    const double left_z = k > 0 ? g.e_old[2][e_index(g, 2, i, j, k - 1)] : 0.0;
+    const double divergence =
+        (g.e_old[0][e_index(g, 0, i, j, k)] - g.e_old[0][e_index(g, 0, i - 1, j, k)]) / g.dx +
+        (g.e_old[1][e_index(g, 1, i, j, k)] - g.e_old[1][e_index(g, 1, i, j - 1, k)]) / g.dy +
+        (g.e_old[2][e_index(g, 2, i, j, k)] - left_z) / g.dz;
+    const double source = rho[((size_t)k * vy + j) * vx + i] / kEpsilon0;
+    const double error = divergence - source;
+    res = dd_add(res, two_prod(error, error));
+    src = dd_add(src, two_prod(source, source));
+    worst = fmax(worst, fabs(error));
+  }
+  res = sf_block_sum(res, shared);
+  src = sf_block_sum(src, shared);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = res;
+    a.partial[2 * blockIdx.x + 1] = src;
+  }
+  if (worst > 0.) atomicMax(max_bits, (unsigned long long)__double_as_longlong(worst));
+}
+
+// initialFieldEnergy (src/eb_initial_field.cpp:665-691): partial sums of
+// the electric and magnetic energies over the cells; `volume` carries the
+// factors 0.5 eps0 dV (hi, lo) and the magnetic factor 0.5 dV / mu0 is
+// passed in a.stencil[0..1].
+__global__ void __launch_bounds__(kSelfFieldThreads) sf_energy_kernel(SfArgs a, DD volume) {
+  __shared__ DD shared[kSelfFieldThreads];
+  const DGrid& g = a.g;
+  const DD magnetic_factor{a.stencil[0], a.stencil[1]};
+  const long long count = (long long)g.nx * g.ny * g.nz;
+  DD we{0., 0.}, wm{0., 0.};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % g.nx);
+    const int j = (int)((n / g.nx) % g.ny);
+    const int k = (int)(n / ((long long)g.nx * g.ny));
+    const double* ex = g.e_old[0];
+    const double* ey = g.e_old[1];
+    const double* ez = g.e_old[2];
+    const double e0 = 0.25 * (((ex[e_index(g, 0, i, j, k)] + ex[e_index(g, 0, i, j + 1, k)]) +
+                               ex[e_index(g, 0, i, j, k + 1)]) + ex[e_index(g, 0, i, j + 1, k + 1)]);
+    const double e1 = 0.25 * (((ey[e_index(g, 1, i, j, k)] + ey[e_index(g, 1, i + 1, j, k)]) +
+                               ey[e_index(g, 1, i, j, k + 1)]) + ey[e_index(g, 1, i + 1, j, k + 1)]);
+    const double e2 = 0.25 * (((ez[e_index(g, 2, i, j, k)] + ez[e_index(g, 2, i + 1, j, k)]) +
+                               ez[e_index(g, 2, i, j + 1, k)]) + ez[e_index(g, 2, i + 1, j + 1, k)]);
+    const double m0 = 0.5 * (g.b[0][b_index(g, 0, i, j, k)] + g.b[0][b_index(g, 0, i + 1, j, k)]);
+    const double m1 = 0.5 * (g.b[1][b_index(g, 1, i, j, k)] + g.b[1][b_index(g, 1, i, j + 1, k)]);
+    const double m2 = 0.5 * (g.b[2][b_index(g, 2, i, j, k)] + g.b[2][b_index(g, 2, i, j, k + 1)]);
+    const double en = (e0 * e0 + e1 * e1) + e2 * e2;
+    const double bn = (m0 * m0 + m1 * m1) + m2 * m2;
+    we = dd_add(we, dd_mul(volume, en));
+    wm = dd_add(wm, dd_mul(magnetic_factor, bn));
+  }
+  we = sf_block_sum(we, shared);
+  wm = sf_block_sum(wm, shared);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = we;
+    a.partial[2 * blockIdx.x + 1] = wm;
+  }
+}
+
+}  // namespace aprl_gpu

@@ -1,0 +1,88 @@
+// selffield.cuh -- the initial self-field solve on the device
+// (EBGaussFieldInitializer, src/eb_initial_field.cpp:829-1095).
+//
+// Scalars (potential, residual, CG direction, operator image) live on the
+// node lattice of the Poisson geometry, lx = nx+1+2 pad by ly = ny+1+2 pad
+// nodes, with nz+2 planes: plane p holds node k = p-1 and planes 0 and nz+1
+// are the zero Dirichlet ghosts (the single-rank ScalarSlab).  Only the
+// interior vertices of the solve domain are ever written in the CG vectors.
+// Every reduction (dot products, charge and velocity moments, the Gauss
+// check, the field energies) is a double-double sum: per-block partials in
+// a fixed order, then one finishing block, so results do not depend on
+// scheduling and agree with the reference's long double sums to about an
+// ulp.  The CG scalars alpha, beta and the relative residual are formed on
+// the device from those sums, so iterations run back to back; the host
+// reads the iteration state once per batch.
+#pragma once
+
+#include "common.cuh"
+#include "ledger.cuh"
+
+namespace aprl_gpu {
+
+constexpr int kSelfFieldThreads = 128;
+constexpr int kSelfFieldBlocks = 1184;  // eight blocks per SM
+constexpr int kMoments = 11;            // mass, m beta[3], m x[3], m x^2[3], charge
+
+struct SfLattice {
+  int lx, ly, planes;           // Poisson node lattice, planes = nz + 2
+  int pad;                      // transverse padding (0 or 2)
+  int lo[3], hi[3];             // solve domain: interior i in (lo, hi), k = p-1 likewise
+};
+
+// CG state on the device.
+struct SfState {
+  DD rr, source, denominator, next;
+  double alpha, beta, relative;
+  unsigned long long iterations;
+  int done;                     // 1 converged, 2 lost positive definiteness, 3 non-finite
+};
+
+struct SfArgs {
+  DGrid g;                      // e_old = the run's E (written), b = the run's B
+  SfLattice L;
+  double *potential, *residual, *direction, *image;
+  double* rho;                  // lx x ly x (nz+1) charge (Poisson lattice)
+  double dx, dy, dz;
+  // 7-point operator
+  double cx, cy, cz, diagonal;
+  // 27-point Cowan operator and smoothing
+  int cowan;
+  double stencil[27];           // [z][y][x]
+  double alpha[3], beta[3], delta[3];  // delta per axis: yz, zx, xy
+  double translation;
+  double tolerance;
+  DD* partial;
+  SfState* state;
+};
+
+struct SfParticles {
+  const double *x, *y, *z, *ux, *uy, *uz, *q, *m;
+  long long n;
+  int hold;                     // mean beta_z from the held longitudinal velocity
+  double rapidity;              // gamma + gamma*beta of the boost
+};
+
+__global__ void sf_moments_kernel(SfParticles p, DD* partial);
+__global__ void sf_finish_kernel(const DD* partial, int blocks, int quantities, DD* out);
+__global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly, int pad,
+                                  DeviceStatus* status);
+__global__ void sf_source_kernel(SfArgs a, DD volume);
+__global__ void sf_apply_kernel(SfArgs a);
+__global__ void sf_alpha_kernel(SfArgs a, int blocks);
+__global__ void sf_update_kernel(SfArgs a);
+__global__ void sf_beta_kernel(SfArgs a, int blocks);
+__global__ void sf_direction_kernel(SfArgs a);
+__global__ void sf_smooth_kernel(SfArgs a, int axis);
+__global__ void sf_electric_kernel(SfArgs a, int axis, double coefficient, int from_smoothed);
+__global__ void sf_magnetic_kernel(SfArgs a, double scale, double lower_w, double upper_w);
+__global__ void sf_clear_outside_kernel(SfArgs a, int component, int gx, int gy, int gz);
+__global__ void sf_gauss_kernel(SfArgs a, const double* rho, int plo0, int phi0, int plo1,
+                                int phi1, int plo2, int phi2, unsigned long long* max_bits);
+__global__ void sf_energy_kernel(SfArgs a, DD volume);
+
+// Host helpers: the double-double quotient and square root rounded to binary64.
+double sf_ratio(DD a, DD b);
+long double sf_long(DD a);
+
+}  // namespace aprl_gpu

@@ -54,6 +54,8 @@ _SIGNATURES = {
     "run_get_stats": (C.c_int, [_H, C.POINTER(abi.StepStats)]),
     "run_enable_energy_ledger": (C.c_int, [_H, C.c_int]),
     "run_energy_ledger": (C.c_int, [_H, C.POINTER(abi.EnergyLedger)]),
+    "run_initialize_self_field": (C.c_int, [_H, C.POINTER(abi.SelfFieldConfig),
+                                            C.POINTER(abi.SelfFieldReport)]),
     "run_get_slot_fields": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _SZ]),
     "run_sample_field_plane": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                          C.POINTER(C.c_int)]),
@@ -317,6 +319,13 @@ class Run:
 
     def enable_energy_ledger(self, enabled=True):
         self.b("run_enable_energy_ledger", self.handle, int(enabled))
+
+    def initialize_self_field(self, config):
+        """EBGaussFieldInitializer::initialize on the run's particles; returns
+        the report as a dict (config: abi.SelfFieldConfig)."""
+        out = abi.SelfFieldReport()
+        self.b("run_initialize_self_field", self.handle, C.byref(config), C.byref(out))
+        return out.as_dict()
 
     def energy_ledger(self):
         out = abi.EnergyLedger()

@@ -428,6 +428,19 @@ def small_case(nx=16, ny=16, nz=40, particles=400, steps=6,
                                  "shape": shape})
 
 
+def self_field_case(energy_ev=8.84e6, nx=16, ny=16, nz=40, particles=400, seed=3,
+                    margin_cells=2, steps=6):
+    """A bunch whose box-frame mean velocity is moderate (lab energy near the
+    boost's: 5.11 MeV gives beta_z ~ 0, 8.84 MeV ~ 0.5), the regime the
+    initial self-field solve is meant for."""
+    cfg = make_config(nx, ny, nz, 5e-6, 5e-6, 2e-6, 4, 10.0, "linear-binomial3", steps,
+                      magnets=[])
+    bunch = gaussian_bunch(cfg, particles, 20e-12, energy_ev, 12e-6, 10e-6, 1e-6, 1e-4,
+                           seed=seed, margin_cells=margin_cells)
+    return Workload(f"self-field-{nx}x{ny}x{nz}", cfg, bunch, synthetic_reference(cfg), [],
+                    steps=steps, description={"energy_ev": energy_ev})
+
+
 # ---------------------------------------------------------------------------
 # Batched ensemble and served scan: seeded draws of independent runs.
 def scan_draw(index, seed=2024, steps=500, precision="fp32-mixed",

@@ -387,6 +387,58 @@ aprl_status aprl_run_enable_energy_ledger(aprl_run* run, int enabled);
  * Valid between steps (no stage in progress).  Waits for the run's stream. */
 aprl_status aprl_run_energy_ledger(aprl_run* run, aprl_energy_ledger* out);
 
+/* InitialSelfFieldModel (src/config.h:141-146). */
+typedef enum {
+  APRL_SELF_FIELD_RELATIVISTIC_POISSON = 0,
+  APRL_SELF_FIELD_ELECTROSTATIC_POISSON = 1,
+  APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON = 2
+} aprl_self_field_model;
+
+/* The arguments of EBGaussFieldInitializer::initialize
+ * (src/eb_initial_field.h:52-68) beyond the grid and the particles. */
+typedef struct {
+  int32_t model;                      /* aprl_self_field_model */
+  int32_t include_transverse_cpml_particles;
+  int32_t hold_transverse_until_activation;  /* mean beta_z from the held longitudinal velocity */
+  int32_t reserved;
+  double relative_tolerance;          /* CG stop: |r| <= tol |b| */
+  double maximum_mean_transverse_beta;
+  uint64_t maximum_iterations;
+  uint64_t guard_cells[3];            /* staticFieldGuardCells: the CPML cells per axis */
+} aprl_self_field_config;
+
+/* EBGaussInitializationReport (src/eb_initial_field.h:17-34). */
+typedef struct {
+  uint64_t iterations;
+  double relative_residual;           /* post-solve discrete Gauss check */
+  double maximum_gauss_residual;
+  double total_charge;
+  double mean_beta_z;
+  double mean_beta_transverse;
+  double initial_electric_energy;
+  double initial_magnetic_energy;
+  double rms_position_cells[3];
+  double centre_padding_rms[3];
+  uint64_t static_field_guard_cells[3];
+  uint64_t transverse_poisson_padding_cells;
+  uint64_t temporary_bytes;
+} aprl_self_field_report;
+
+/* EBGaussFieldInitializer::initialize (src/eb_initial_field.cpp:829-1095)
+ * at one rank, on the GPU, with the run's stored particles as the source:
+ * the CIC charge, a matrix-free conjugate-gradient solve of the
+ * relativistic (7-point) or Cowan (27-point) Poisson operator with zero
+ * potential on the guard surface, E from the potential, B = beta x E / c
+ * shifted to the half step, and the discrete Gauss check.  Replaces E and
+ * B of the run (J and the CPML histories are untouched); call it before
+ * the first step.  The CG dot products are double-double reductions on the
+ * device; the host reads the iteration state once per batch of iterations.
+ * The reference's own errors (charge touching the zero-potential surface,
+ * loss of positive definiteness, no convergence, ...) return
+ * APRL_ERR_RUNTIME / APRL_ERR_INVALID_ARGUMENT with its message. */
+aprl_status aprl_run_initialize_self_field(aprl_run* run, const aprl_self_field_config* config,
+                                           aprl_self_field_report* report);
+
 /* Discrete Gauss law of the current state, reduced on the GPU.  The node
  * charge density is the one the linear-binomial3 current conserves: per
  * particle, F3 node weights in x over nodes i-1..i+2, linear weights in y

@@ -2954,3 +2954,534 @@ aprl_status oracle_run_sample_field_plane(oracle_run* r, double plane_lab_z, dou
   }
   return APRL_OK;
 }
+
+/* ---- initial self-field ------------------------------------------------- */
+/* EBGaussFieldInitializer::initialize (src/eb_initial_field.cpp:829-1095)
+ * at one rank, restated with its long double reductions and loop orders.
+ * Scalars live on the node lattice of the Poisson geometry (nx+1+2 pad,
+ * ny+1+2 pad) with nz+2 planes: plane p holds node k = p-1, planes 0 and
+ * nz+1 are the zero ghosts of a single rank (ScalarSlab,
+ * src/eb_initial_field.cpp:30-82). */
+typedef struct {
+  size_t nx, ny, planes;
+  double* v;
+} slab_t;
+
+#define SAT(s, i, j, p) ((s)->v[((size_t)(p) * (s)->ny + (j)) * (s)->nx + (i)])
+
+typedef struct {
+  size_t lower[3], upper[3];
+} sdomain_t;
+
+static int sf_interior(size_t i, size_t j, size_t k, const sdomain_t* d) {
+  return i > d->lower[0] && i < d->upper[0] && j > d->lower[1] && j < d->upper[1] &&
+         k > d->lower[2] && k < d->upper[2];
+}
+
+/* positiveLightFrontComponent / properVelocityFromPositiveLightFront /
+ * heldLongitudinalBetaZ (src/boostframe.cpp:89-167). */
+static double sf_positive(const double u[3]) {
+  const double gamma = gamma_u(u);
+  const double tms = fma(u[0], u[0], fma(u[1], u[1], 1.0));
+  if (u[2] >= 0.0) return gamma + u[2];
+  return tms / (gamma - u[2]);
+}
+static void sf_from_positive(const double in[3], double positive, double out[3]) {
+  const double tms = fma(in[0], in[0], fma(in[1], in[1], 1.0));
+  const double negative = tms / positive;
+  out[0] = in[0];
+  out[1] = in[1];
+  out[2] = 0.5 * (positive - negative);
+}
+static double sf_held_beta_z(const aprl_run_config* g, const double u[3]) {
+  const double rapidity = g->boost_gamma + g->boost_gamma_beta;
+  double lab[3], lon[3] = {0.0, 0.0, 0.0}, box[3];
+  sf_from_positive(u, sf_positive(u) * rapidity, lab);
+  lon[2] = lab[2];
+  sf_from_positive(lon, sf_positive(lon) / rapidity, box);
+  return box[2] / hypot(1.0, box[2]);
+}
+
+/* ChargeConservingCurrentDepositor::depositCharge (src/eb_deposition.cpp:168-193)
+ * into an (nx+1, ny+1, nz+1) vertex array embedded at offset `pad` of a
+ * lattice `lx` x `ly` wide. */
+static aprl_status sf_deposit(const oracle_run* r, double* rho, size_t lx, size_t ly, size_t pad) {
+  const aprl_run_config* g = &r->cfg;
+  const double extent[3] = {(double)g->nx * g->dx, (double)g->ny * g->dy, (double)g->nz * g->dz};
+  const double h[3] = {g->dx, g->dy, g->dz};
+  const size_t cells[3] = {g->nx, g->ny, g->nz};
+  const double inverse_volume = 1.0 / (g->dx * g->dy * g->dz);
+  for (size_t n = 0; n < r->np; ++n) {
+    const particle_t* p = &r->p[n];
+    size_t c[3];
+    double f[3];
+    for (int a = 0; a < 3; ++a) {
+      const double relative = p->pos[a] - r->origin[a];
+      const double tol = 64.0 * DBL_EPSILON * fmax(1.0, fmax(fabs(r->origin[a]), extent[a]));
+      if (!isfinite(p->pos[a]) || relative < -tol || relative > extent[a] + tol)
+        return fail(APRL_ERR_OUT_OF_RANGE, "Particle trajectory endpoint is outside the E/B domain");
+      const double x = fmax(0.0, fmin((double)cells[a], (p->pos[a] - r->origin[a]) / h[a]));
+      if (x <= 0.0) c[a] = 0;
+      else if (x >= (double)cells[a]) c[a] = cells[a] - 1;
+      else c[a] = (size_t)floor(x);
+      f[a] = fmax(0.0, fmin(1.0, x - (double)c[a]));
+    }
+    for (unsigned cz = 0; cz < 2; ++cz)
+      for (unsigned b = 0; b < 2; ++b)
+        for (unsigned a = 0; a < 2; ++a) {
+          const double sa = a ? f[0] : 1.0 - f[0];
+          const double sb = b ? f[1] : 1.0 - f[1];
+          const double sc = cz ? f[2] : 1.0 - f[2];
+          rho[((c[2] + cz) * ly + (c[1] + b + pad)) * lx + (c[0] + a + pad)] +=
+              p->q * inverse_volume * sa * sb * sc;
+        }
+  }
+  return APRL_OK;
+}
+
+static long double sf_dot(const slab_t* a, const slab_t* b, const sdomain_t* d, size_t nz) {
+  long double local = 0.0L;
+  for (size_t p = 1; p <= nz; ++p) {
+    const size_t k = p - 1;
+    if (k <= d->lower[2] || k >= d->upper[2]) continue;
+    for (size_t j = d->lower[1] + 1; j < d->upper[1]; ++j)
+      for (size_t i = d->lower[0] + 1; i < d->upper[0]; ++i)
+        local += (long double)SAT(a, i, j, p) * (long double)SAT(b, i, j, p);
+  }
+  return local;
+}
+
+/* The CowanPoissonOperator stencil (src/eb_initial_field.cpp:246-316). */
+static aprl_status sf_cowan_stencil(const oracle_run* r, double beta_z, double* translation,
+                                    double stencil[3][3][3]) {
+  const aprl_run_config* g = &r->cfg;
+  const double velocity = beta_z * SI_C;
+  *translation = velocity * velocity * SI_EPSILON0 * SI_MU0;
+  const double spacing[3] = {g->dx, g->dy, g->dz};
+  const double deltas[3] = {r->delta_yz, r->delta_zx, r->delta_xy};
+  memset(stencil, 0, 27 * sizeof(double));
+  for (unsigned axis = 0; axis < 3; ++axis) {
+    const unsigned ta = (axis + 1) % 3, tb = (axis + 2) % 3;
+    const double delta = deltas[axis];
+    double minimum = INFINITY;
+    for (int a = -1; a <= 1; a += 2)
+      for (int b = -1; b <= 1; b += 2)
+        minimum = fmin(minimum, r->alpha[axis] + 2.0 * r->beta[ta] * a + 2.0 * r->beta[tb] * b +
+                                    4.0 * delta * a * b);
+    if (axis == 2) minimum -= *translation;
+    if (!(minimum > 64.0 * DBL_EPSILON))
+      return fail(APRL_ERR_RUNTIME,
+                  "Initial Cowan-Poisson operator fails the sufficient positive-definiteness "
+                  "bound on axis %u: minimum smoothing symbol=%.12g",
+                  axis, minimum);
+    const double inverse2 = 1.0 / (spacing[axis] * spacing[axis]);
+    for (int a = -1; a <= 1; ++a)
+      for (int b = -1; b <= 1; ++b) {
+        const double weight =
+            a == 0 ? (b == 0 ? r->alpha[axis] : r->beta[tb]) : (b == 0 ? r->beta[ta] : delta);
+        int pt[3] = {1, 1, 1};
+        pt[ta] += a;
+        pt[tb] += b;
+        stencil[pt[2]][pt[1]][pt[0]] += 2.0 * weight * inverse2;
+        --pt[axis];
+        stencil[pt[2]][pt[1]][pt[0]] -= weight * inverse2;
+        pt[axis] += 2;
+        stencil[pt[2]][pt[1]][pt[0]] -= weight * inverse2;
+      }
+  }
+  const double tz = *translation / (g->dz * g->dz);
+  stencil[1][1][1] -= 2.0 * tz;
+  stencil[0][1][1] += tz;
+  stencil[2][1][1] += tz;
+  return APRL_OK;
+}
+
+/* cowanSmoothedPotential (src/eb_initial_field.cpp:344-382). */
+static double sf_smoothed(const oracle_run* r, const slab_t* phi, unsigned axis, size_t i,
+                          size_t j, size_t p) {
+  const unsigned ta = (axis + 1) % 3, tb = (axis + 2) % 3;
+  const double deltas[3] = {r->delta_yz, r->delta_zx, r->delta_xy};
+  double value = r->alpha[axis] * SAT(phi, i, j, p);
+  for (int sign = -1; sign <= 1; sign += 2) {
+    size_t a[3] = {i, j, p}, b[3] = {i, j, p};
+    if (sign < 0) {
+      --a[ta];
+      --b[tb];
+    } else {
+      ++a[ta];
+      ++b[tb];
+    }
+    value += r->beta[ta] * SAT(phi, a[0], a[1], a[2]);
+    value += r->beta[tb] * SAT(phi, b[0], b[1], b[2]);
+  }
+  for (int a = -1; a <= 1; a += 2)
+    for (int b = -1; b <= 1; b += 2) {
+      size_t pt[3] = {i, j, p};
+      if (a < 0) --pt[ta]; else ++pt[ta];
+      if (b < 0) --pt[tb]; else ++pt[tb];
+      value += deltas[axis] * SAT(phi, pt[0], pt[1], pt[2]);
+    }
+  return value;
+}
+
+static void sf_free(slab_t* s, int n) {
+  for (int q = 0; q < n; ++q) free(s[q].v);
+}
+
+aprl_status oracle_run_initialize_self_field(oracle_run* r, const aprl_self_field_config* cfg,
+                                             aprl_self_field_report* rep) {
+  const aprl_run_config* g = &r->cfg;
+  memset(rep, 0, sizeof *rep);
+  if (!(cfg->relative_tolerance > 0.0) || !(cfg->relative_tolerance < 1.0) ||
+      !isfinite(cfg->relative_tolerance) || cfg->maximum_iterations == 0)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid initial Gauss-field convergence controls");
+  if (!(cfg->maximum_mean_transverse_beta >= 0.0) || !(cfg->maximum_mean_transverse_beta < 1.0) ||
+      !isfinite(cfg->maximum_mean_transverse_beta))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid initial self-field maximum mean transverse beta");
+  if (cfg->model < 0 || cfg->model > 2)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Unknown initial self-field model");
+  const int include = cfg->include_transverse_cpml_particles != 0;
+  if (include && (cfg->guard_cells[0] < 2 || cfg->guard_cells[1] < 2))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "Transverse CPML-source initialization requires at least two physical guard "
+                "cells in x and y");
+  const int cowan = cfg->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON;
+  const int relativistic = cfg->model == APRL_SELF_FIELD_RELATIVISTIC_POISSON || cowan;
+  const size_t pad = include ? 2 : 0;
+  const size_t pnx = g->nx + 2 * pad, pny = g->ny + 2 * pad;
+  const size_t cells[3] = {g->nx, g->ny, g->nz};
+  const size_t pcells[3] = {pnx, pny, g->nz};
+  sdomain_t domain, physical;
+  for (int a = 0; a < 3; ++a) {
+    if (2 * cfg->guard_cells[a] + 2 >= cells[a])
+      return fail(APRL_ERR_INVALID_ARGUMENT,
+                  "Initial static-field guard leaves fewer than two physical cells");
+    physical.lower[a] = cfg->guard_cells[a];
+    physical.upper[a] = cells[a] - cfg->guard_cells[a];
+    domain.lower[a] = include && a < 2 ? 0 : cfg->guard_cells[a];
+    domain.upper[a] = pcells[a] - domain.lower[a];
+  }
+  for (int a = 0; a < 6; ++a)
+    memset(r->f[a].v, 0, r->f[a].nx * r->f[a].ny * r->f[a].nz * sizeof(double));
+
+  /* meanVelocity (src/eb_initial_field.cpp:629-663) */
+  long double mv[4] = {0.L, 0.L, 0.L, 0.L};
+  for (size_t n = 0; n < r->np; ++n) {
+    const particle_t* p = &r->p[n];
+    const double gamma = gamma_u(p->u);
+    const long double w = (long double)p->m;
+    mv[0] += w;
+    if (cfg->hold_transverse_until_activation)
+      mv[3] += w * (long double)sf_held_beta_z(g, p->u);
+    else
+      for (int a = 0; a < 3; ++a) mv[a + 1] += w * (long double)(p->u[a] / gamma);
+  }
+  if (!(mv[0] > 0.0L))
+    return fail(APRL_ERR_RUNTIME, "Initial relativistic-Poisson field requires positive represented mass");
+  const double bx = (double)(mv[1] / mv[0]), by = (double)(mv[2] / mv[0]);
+  const double beta_z = (double)(mv[3] / mv[0]);
+  const double beta_t = hypot(bx, by);
+  if (!isfinite(beta_z) || !isfinite(beta_t) || beta_t >= 1.0 || fabs(beta_z) >= 1.0)
+    return fail(APRL_ERR_RUNTIME, "Initial particle mean velocity is not a finite subluminal vector");
+  if (relativistic && beta_t > cfg->maximum_mean_transverse_beta)
+    return fail(APRL_ERR_RUNTIME,
+                "%s mean beta_box_transverse=%.12g exceeds "
+                "initial_self_field.maximum_mean_transverse_beta=%.12g",
+                cowan ? "cowan-relativistic-poisson" : "relativistic-poisson", beta_t,
+                cfg->maximum_mean_transverse_beta);
+  const double applied = relativistic ? beta_z : 0.0;
+  const double longitudinal = fma(-applied, applied, 1.0);
+  if (!cowan && !(longitudinal > 64.0 * DBL_EPSILON))
+    return fail(APRL_ERR_RUNTIME,
+                "Initial relativistic-Poisson operator is ill-conditioned because the bunch "
+                "remains too relativistic in the simulation frame");
+  double translation = 0.0, stencil[3][3][3];
+  if (cowan) {
+    aprl_status s = sf_cowan_stencil(r, applied, &translation, stencil);
+    if (s != APRL_OK) return s;
+  }
+  rep->mean_beta_z = beta_z;
+  rep->mean_beta_transverse = beta_t;
+  rep->transverse_poisson_padding_cells = pad;
+  for (int a = 0; a < 3; ++a) rep->static_field_guard_cells[a] = domain.lower[a];
+
+  /* distributionResolution (src/eb_initial_field.cpp:693-741) */
+  {
+    long double m[7] = {0.L, 0.L, 0.L, 0.L, 0.L, 0.L, 0.L};
+    for (size_t n = 0; n < r->np; ++n) {
+      const long double w = (long double)r->p[n].m;
+      m[0] += w;
+      for (int a = 0; a < 3; ++a) {
+        const long double x = (long double)r->p[n].pos[a];
+        m[a + 1] += w * x;
+        m[a + 4] += w * x * x;
+      }
+    }
+    const double spacing[3] = {g->dx, g->dy, g->dz};
+    const double origin[3] = {r->origin[0] - (double)pad * g->dx,
+                              r->origin[1] - (double)pad * g->dy, r->origin[2]};
+    for (int a = 0; a < 3; ++a) {
+      const long double mean = m[a + 1] / m[0];
+      long double variance = m[a + 4] / m[0] - mean * mean;
+      if (variance < 0.0L) variance = 0.0L;
+      const double rms = (double)sqrtl(variance);
+      rep->rms_position_cells[a] = rms / spacing[a];
+      if (rms > 0.0) {
+        const double lower = origin[a] + (double)domain.lower[a] * spacing[a];
+        const double upper = origin[a] + (double)domain.upper[a] * spacing[a];
+        rep->centre_padding_rms[a] = fmin((double)mean - lower, upper - (double)mean) / rms;
+      }
+    }
+  }
+  slab_t s[4];
+  const size_t planes = g->nz + 2, lx = pnx + 1, ly = pny + 1;
+  for (int q = 0; q < 4; ++q) {
+    s[q].nx = lx;
+    s[q].ny = ly;
+    s[q].planes = planes;
+    s[q].v = (double*)calloc(lx * ly * planes, sizeof(double));
+  }
+  slab_t *potential = &s[0], *residual = &s[1], *direction = &s[2], *image = &s[3];
+  rep->temporary_bytes = 4 * lx * ly * planes * sizeof(double) +
+                         (g->nx + 1) * (g->ny + 1) * (g->nz + 1) * sizeof(double) +
+                         (pad ? lx * ly * (g->nz + 1) * sizeof(double) : 0);
+  double* rho = (double*)calloc(lx * ly * (g->nz + 1), sizeof(double));
+  aprl_status st = sf_deposit(r, rho, lx, ly, pad);
+  if (st != APRL_OK) {
+    free(rho);
+    sf_free(s, 4);
+    return st;
+  }
+  long double total = 0.L;
+  for (size_t n = 0; n < r->np; ++n) total += (long double)r->p[n].q;
+  rep->total_charge = (double)total;
+  long double interior = 0.L;
+  const long double vertex_volume = (long double)g->dx * (long double)g->dy * (long double)g->dz;
+  for (size_t p = 1; p <= g->nz; ++p)
+    for (size_t j = 0; j <= pny; ++j)
+      for (size_t i = 0; i <= pnx; ++i)
+        if (sf_interior(i, j, p - 1, &domain)) {
+          const double q = rho[((p - 1) * ly + j) * lx + i];
+          SAT(residual, i, j, p) = q / SI_EPSILON0;
+          interior += (long double)q * vertex_volume;
+        }
+  free(rho);
+  if (fabsl((interior - total) / total) > 1.0e-12L) {
+    sf_free(s, 4);
+    return fail(APRL_ERR_RUNTIME,
+                "Initial CIC charge cloud touches the static zero-potential boundary; move every "
+                "particle at least one complete cell inside the CPML entrance or enlarge the "
+                "physical mesh padding");
+  }
+  memcpy(direction->v, residual->v, lx * ly * planes * sizeof(double));
+  const long double source2 = sf_dot(residual, residual, &domain, g->nz);
+  if (!(source2 > 0.0L) || !isfinite((double)source2)) {
+    sf_free(s, 4);
+    return fail(APRL_ERR_RUNTIME, "Initial particle charge produced an invalid Poisson source norm");
+  }
+  long double r2 = source2;
+  const double cx = 1.0 / (g->dx * g->dx), cy = 1.0 / (g->dy * g->dy);
+  const double cz = longitudinal / (g->dz * g->dz);
+  const double diagonal = 2.0 * (cx + cy + cz);
+  double relative = 0.0;
+  for (uint64_t it = 0; it < cfg->maximum_iterations; ++it) {
+    memset(image->v, 0, lx * ly * planes * sizeof(double));
+    for (size_t p = 1; p <= g->nz; ++p) {
+      const size_t k = p - 1;
+      if (k <= domain.lower[2] || k >= domain.upper[2]) continue;
+      for (size_t j = domain.lower[1] + 1; j < domain.upper[1]; ++j)
+        for (size_t i = domain.lower[0] + 1; i < domain.upper[0]; ++i) {
+          if (cowan) {
+            double value = 0.0;
+            for (size_t z = 0; z < 3; ++z)
+              for (size_t y = 0; y < 3; ++y)
+                for (size_t x = 0; x < 3; ++x)
+                  value += stencil[z][y][x] * SAT(direction, i - 1 + x, j - 1 + y, p - 1 + z);
+            SAT(image, i, j, p) = value;
+          } else {
+            SAT(image, i, j, p) =
+                diagonal * SAT(direction, i, j, p) -
+                cx * (SAT(direction, i - 1, j, p) + SAT(direction, i + 1, j, p)) -
+                cy * (SAT(direction, i, j - 1, p) + SAT(direction, i, j + 1, p)) -
+                cz * (SAT(direction, i, j, p - 1) + SAT(direction, i, j, p + 1));
+          }
+        }
+    }
+    const long double denominator = sf_dot(direction, image, &domain, g->nz);
+    if (!(denominator > 0.0L) || !isfinite((double)denominator)) {
+      sf_free(s, 4);
+      return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG lost positive definiteness");
+    }
+    const double alpha = (double)(r2 / denominator);
+    for (size_t p = 1; p <= g->nz; ++p) {
+      const size_t k = p - 1;
+      if (k <= domain.lower[2] || k >= domain.upper[2]) continue;
+      for (size_t j = domain.lower[1] + 1; j < domain.upper[1]; ++j)
+        for (size_t i = domain.lower[0] + 1; i < domain.upper[0]; ++i) {
+          SAT(potential, i, j, p) += alpha * SAT(direction, i, j, p);
+          SAT(residual, i, j, p) += -alpha * SAT(image, i, j, p);
+        }
+    }
+    const long double next = sf_dot(residual, residual, &domain, g->nz);
+    rep->iterations = it + 1;
+    relative = (double)sqrtl(next / source2);
+    if (relative <= cfg->relative_tolerance) {
+      r2 = next;
+      break;
+    }
+    if (!(next >= 0.0L) || !isfinite((double)next)) {
+      sf_free(s, 4);
+      return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG produced a non-finite residual");
+    }
+    const double beta = (double)(next / r2);
+    for (size_t p = 1; p <= g->nz; ++p)
+      for (size_t j = 0; j <= pny; ++j)
+        for (size_t i = 0; i <= pnx; ++i)
+          SAT(direction, i, j, p) = sf_interior(i, j, p - 1, &domain)
+                                        ? SAT(residual, i, j, p) + beta * SAT(direction, i, j, p)
+                                        : 0.0;
+    r2 = next;
+  }
+  if (relative > cfg->relative_tolerance) {
+    sf_free(s, 4);
+    return fail(APRL_ERR_RUNTIME,
+                "Initial Gauss-field solve did not converge; increase "
+                "initial_self_field.maximum_iterations, relax its relative_tolerance, or reduce "
+                "the grid aspect ratio");
+  }
+  comp_t *ex = &r->f[0], *ey = &r->f[1], *ez = &r->f[2];
+  comp_t *bxc = &r->f[3], *byc = &r->f[4], *bzc = &r->f[5];
+  if (cowan) {
+    /* fieldsFromCowanPotential (src/eb_initial_field.cpp:487-553) */
+    const double spacing[3] = {g->dx, g->dy, g->dz};
+    for (unsigned axis = 0; axis < 3; ++axis) {
+      memset(image->v, 0, lx * ly * planes * sizeof(double));
+      for (size_t p = 1; p <= g->nz; ++p) {
+        const size_t k = p - 1;
+        if (k <= domain.lower[2] || k >= domain.upper[2]) continue;
+        for (size_t j = domain.lower[1] + 1; j < domain.upper[1]; ++j)
+          for (size_t i = domain.lower[0] + 1; i < domain.upper[0]; ++i)
+            SAT(image, i, j, p) = sf_smoothed(r, potential, axis, i, j, p) -
+                                  (axis == 2 ? translation * SAT(potential, i, j, p) : 0.0);
+      }
+      comp_t* c = &r->f[axis];
+      for (size_t k = 0; k < c->nz; ++k)
+        for (size_t j = 0; j < c->ny; ++j)
+          for (size_t i = 0; i < c->nx; ++i)
+            AT(c, i, j, k) = -(SAT(image, i + pad + (axis == 0), j + pad + (axis == 1),
+                                   k + 1 + (axis == 2)) -
+                               SAT(image, i + pad, j + pad, k + 1)) /
+                             spacing[axis];
+    }
+  } else {
+    /* fieldsFromPotential (src/eb_initial_field.cpp:427-485) */
+    for (size_t k = 0; k <= g->nz; ++k)
+      for (size_t j = 0; j <= g->ny; ++j)
+        for (size_t i = 0; i < g->nx; ++i)
+          AT(ex, i, j, k) = -(SAT(potential, i + pad + 1, j + pad, k + 1) -
+                              SAT(potential, i + pad, j + pad, k + 1)) / g->dx;
+    for (size_t k = 0; k <= g->nz; ++k)
+      for (size_t j = 0; j < g->ny; ++j)
+        for (size_t i = 0; i <= g->nx; ++i)
+          AT(ey, i, j, k) = -(SAT(potential, i + pad, j + pad + 1, k + 1) -
+                              SAT(potential, i + pad, j + pad, k + 1)) / g->dy;
+    for (size_t k = 0; k < g->nz; ++k)
+      for (size_t j = 0; j <= g->ny; ++j)
+        for (size_t i = 0; i <= g->nx; ++i)
+          AT(ez, i, j, k) = -longitudinal * (SAT(potential, i + pad, j + pad, k + 2) -
+                                             SAT(potential, i + pad, j + pad, k + 1)) / g->dz;
+  }
+  sf_free(s, 4);
+  const double scale = cowan ? applied * SI_C * SI_EPSILON0 * SI_MU0 : applied / SI_C;
+  const double upper_w = 0.5 + 0.5 * applied * SI_C * g->dt / g->dz;
+  const double lower_w = 1.0 - upper_w;
+  if (upper_w < 0.0 || upper_w > 1.0)
+    return fail(APRL_ERR_RUNTIME, "Initial B half-step shift exceeds one longitudinal cell");
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 0; j < g->ny; ++j)
+      for (size_t i = 0; i <= g->nx; ++i)
+        AT(bxc, i, j, k) = -scale * (lower_w * AT(ey, i, j, k) + upper_w * AT(ey, i, j, k + 1));
+  for (size_t k = 0; k < g->nz; ++k)
+    for (size_t j = 0; j <= g->ny; ++j)
+      for (size_t i = 0; i < g->nx; ++i)
+        AT(byc, i, j, k) = scale * (lower_w * AT(ex, i, j, k) + upper_w * AT(ex, i, j, k + 1));
+  memset(bzc->v, 0, bzc->nx * bzc->ny * bzc->nz * sizeof(double));
+  if (include) {
+    /* clearCpmlFields (src/eb_initial_field.cpp:564-626) */
+    for (unsigned a = 0; a < 6; ++a) {
+      comp_t* c = &r->f[a];
+      const int electric = a < 3;
+      const unsigned axis_c = a % 3;
+      for (size_t k = 0; k < c->nz; ++k)
+        for (size_t j = 0; j < c->ny; ++j)
+          for (size_t i = 0; i < c->nx; ++i) {
+            const size_t coord[3] = {i, j, k};
+            int inside = 1;
+            for (unsigned d = 0; d < 3; ++d) {
+              const int vertex = electric ? d != axis_c : d == axis_c;
+              const size_t gd = cfg->guard_cells[d];
+              inside = inside && coord[d] >= gd &&
+                       (vertex ? coord[d] <= cells[d] - gd : coord[d] < cells[d] - gd);
+            }
+            if (!inside) AT(c, i, j, k) = 0.0;
+          }
+    }
+  }
+  /* validateGauss (src/eb_initial_field.cpp:743-806) on the unpadded CIC charge */
+  {
+    const size_t vx = g->nx + 1, vy = g->ny + 1;
+    double* vrho = (double*)calloc(vx * vy * (g->nz + 1), sizeof(double));
+    st = sf_deposit(r, vrho, vx, vy, 0);
+    if (st != APRL_OK) {
+      free(vrho);
+      return st;
+    }
+    long double res2 = 0.L, src2 = 0.L;
+    double maximum = 0.0;
+    for (size_t k = 0; k < g->nz; ++k) {
+      if (k <= physical.lower[2] || k >= physical.upper[2]) continue;
+      for (size_t j = physical.lower[1] + 1; j < physical.upper[1]; ++j)
+        for (size_t i = physical.lower[0] + 1; i < physical.upper[0]; ++i) {
+          const double left_z = k > 0 ? AT(ez, i, j, k - 1) : 0.0;
+          const double divergence = (AT(ex, i, j, k) - AT(ex, i - 1, j, k)) / g->dx +
+                                    (AT(ey, i, j, k) - AT(ey, i, j - 1, k)) / g->dy +
+                                    (AT(ez, i, j, k) - left_z) / g->dz;
+          const double source = vrho[(k * vy + j) * vx + i] / SI_EPSILON0;
+          const double error = divergence - source;
+          res2 += (long double)error * error;
+          src2 += (long double)source * source;
+          maximum = fmax(maximum, fabs(error));
+        }
+    }
+    free(vrho);
+    rep->relative_residual = src2 > 0.0L ? (double)sqrtl(res2 / src2) : 0.0;
+    rep->maximum_gauss_residual = maximum;
+    if (rep->relative_residual > 4.0 * cfg->relative_tolerance)
+      return fail(APRL_ERR_RUNTIME, "Initial E field failed the post-solve discrete Gauss check");
+  }
+  /* initialFieldEnergy (src/eb_initial_field.cpp:665-691) */
+  {
+    long double we = 0.L, wm = 0.L;
+    const long double volume = (long double)g->dx * (long double)g->dy * (long double)g->dz;
+    for (size_t k = 0; k < g->nz; ++k)
+      for (size_t j = 0; j < g->ny; ++j)
+        for (size_t i = 0; i < g->nx; ++i) {
+          const double e0 = 0.25 * (AT(ex, i, j, k) + AT(ex, i, j + 1, k) + AT(ex, i, j, k + 1) +
+                                    AT(ex, i, j + 1, k + 1));
+          const double e1 = 0.25 * (AT(ey, i, j, k) + AT(ey, i + 1, j, k) + AT(ey, i, j, k + 1) +
+                                    AT(ey, i + 1, j, k + 1));
+          const double e2 = 0.25 * (AT(ez, i, j, k) + AT(ez, i + 1, j, k) + AT(ez, i, j + 1, k) +
+                                    AT(ez, i + 1, j + 1, k));
+          const double m0 = 0.5 * (AT(bxc, i, j, k) + AT(bxc, i + 1, j, k));
+          const double m1 = 0.5 * (AT(byc, i, j, k) + AT(byc, i, j + 1, k));
+          const double m2 = 0.5 * (AT(bzc, i, j, k) + AT(bzc, i, j, k + 1));
+          const double en = e0 * e0 + e1 * e1 + e2 * e2;
+          const double bn = m0 * m0 + m1 * m1 + m2 * m2;
+          we += 0.5L * (long double)SI_EPSILON0 * (long double)en * volume;
+          wm += 0.5L / (long double)SI_MU0 * (long double)bn * volume;
+        }
+    rep->initial_electric_energy = (double)we;
+    rep->initial_magnetic_energy = (double)wm;
+  }
+  return APRL_OK;
+}

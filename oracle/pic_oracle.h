@@ -76,6 +76,8 @@ aprl_status oracle_run_shift(oracle_run* run);
 aprl_status oracle_run_step(oracle_run* run, uint32_t steps);
 aprl_status oracle_run_enable_energy_ledger(oracle_run* run, int enabled);
 aprl_status oracle_run_energy_ledger(oracle_run* run, aprl_energy_ledger* out);
+aprl_status oracle_run_initialize_self_field(oracle_run* run, const aprl_self_field_config* config,
+                                             aprl_self_field_report* report);
 aprl_status oracle_run_get_stats(const oracle_run* run, aprl_step_stats* stats);
 aprl_status oracle_run_get_slot_fields(oracle_run* run, size_t capacity,
                                        double* used_e, double* used_b,

@@ -35,6 +35,7 @@
 #include "eb_cpml.h"
 #include "eb_deposition.h"
 #include "eb_field.h"
+#include "eb_initial_field.h"
 #include "eb_particles.h"
 #include "eb_sources.h"
 #include "longitudinal_shape.h"
@@ -901,6 +902,41 @@ aprl_status ref_run_energy_ledger(ref_run* r, aprl_energy_ledger* out) {
     out->particle_total = static_cast<double>(total);
     out->represented_electrons = static_cast<double>(represented);
     out->particles = r->particles.size();
+  });
+}
+
+// EBGaussFieldInitializer::initialize at one rank on the run's particles.
+aprl_status ref_run_initialize_self_field(ref_run* r, const aprl_self_field_config* c,
+                                          aprl_self_field_report* out) {
+  return guarded([&] {
+    std::memset(out, 0, sizeof *out);
+    const InitialSelfFieldModel model =
+        c->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON
+            ? InitialSelfFieldModel::CowanRelativisticPoisson
+            : (c->model == APRL_SELF_FIELD_ELECTROSTATIC_POISSON
+                   ? InitialSelfFieldModel::ElectrostaticPoisson
+                   : InitialSelfFieldModel::RelativisticPoisson);
+    const std::size_t guard[3] = {c->guard_cells[0], c->guard_cells[1], c->guard_cells[2]};
+    const EBGaussInitializationReport rep = EBGaussFieldInitializer::initialize(
+        *r->fields, r->geometry, 0, r->origin, r->particles, model,
+        c->maximum_mean_transverse_beta, guard, c->relative_tolerance, c->maximum_iterations,
+        MPI_COMM_WORLD, c->include_transverse_cpml_particles != 0,
+        c->hold_transverse_until_activation != 0, &r->frame);
+    out->iterations = rep.iterations;
+    out->relative_residual = rep.relativeResidual;
+    out->maximum_gauss_residual = rep.maximumGaussResidual;
+    out->total_charge = rep.totalCharge;
+    out->mean_beta_z = rep.meanBetaZ;
+    out->mean_beta_transverse = rep.meanBetaTransverse;
+    out->initial_electric_energy = rep.initialElectricEnergy;
+    out->initial_magnetic_energy = rep.initialMagneticEnergy;
+    for (int a = 0; a < 3; ++a) {
+      out->rms_position_cells[a] = rep.rmsPositionCells[a];
+      out->centre_padding_rms[a] = rep.centrePaddingRms[a];
+      out->static_field_guard_cells[a] = rep.staticFieldGuardCells[a];
+    }
+    out->transverse_poisson_padding_cells = rep.transversePoissonPaddingCells;
+    out->temporary_bytes = rep.temporaryBytes;
   });
 }
 
