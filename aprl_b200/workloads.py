@@ -441,6 +441,19 @@ def self_field_case(energy_ev=8.84e6, nx=16, ny=16, nz=40, particles=400, seed=3
                     steps=steps, description={"energy_ev": energy_ev})
 
 
+def self_field_c2(particles=1_000_000, seed=17, energy_ev=8.84e6):
+    """The dipole grid (128x128x512 cells, 10-cell CPML, boost gamma 10) with
+    a 100 pC bunch moving at beta_z ~ 0.5 in the box (8.84 MeV lab): the
+    initial self-field solve's regime."""
+    cfg = make_config(128, 128, 512, 5e-6, 5e-6, 2e-6, 10, 10.0, "linear-binomial3", 8,
+                      magnets=[])
+    bunch = gaussian_bunch(cfg, particles, 100e-12, energy_ev, 50e-6, 20e-6, 1e-6, 1e-4,
+                           seed=seed)
+    return Workload("self-field-128x128x512", cfg, bunch, synthetic_reference(cfg), [],
+                    steps=8, description={"cells": [128, 128, 512], "particles": particles,
+                                          "energy_ev": energy_ev})
+
+
 # ---------------------------------------------------------------------------
 # Batched ensemble and served scan: seeded draws of independent runs.
 def scan_draw(index, seed=2024, steps=500, precision="fp32-mixed",

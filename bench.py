@@ -61,6 +61,8 @@ def parse_args(argv=None):
     p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--scan-slots", type=int, default=4)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    p.add_argument("--no-self-field", action="store_true",
+                   help="skip the timing of the initial self-field solve")
     p.add_argument("--energy-ledger", choices=["auto", "on", "off"], default="auto",
                    help="keep the moving-window energy ledger during the timed steps "
                         "(auto: on for the undulator workload)")
@@ -372,6 +374,8 @@ def run_ours(args):
         line["fp32_mixed"] = fp32_arm
     if world == 1 and not args.no_scan:
         line.update(scan_benchmarks(args))
+    if world == 1 and args.workload == "dipole" and not args.no_self_field:
+        line.update(self_field_benchmark(args, stream))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
@@ -455,6 +459,39 @@ def _plain_fp64(lib, w, steps):
 def _percentiles(values):
     v = np.sort(np.asarray(values, dtype=np.float64))
     return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))}
+
+
+def self_field_benchmark(args, stream):
+    """The initial self-field solve (Cowan relativistic Poisson, tolerance
+    1e-10) on the dipole grid with 1M particles at beta_z ~ 0.5, timed with
+    CUDA events on the run's stream; the conjugate-gradient iterations move
+    88 algorithmic bytes per lattice node (apply: read d, write Ad;
+    update: read x, d, r, Ad, write x, r; direction: read r, d, write d)."""
+    import torch
+    w = workloads.self_field_c2(particles=args.particles)
+    run = native.Run(native.load(), w.config, stream=stream.cuda_stream)
+    run.set_particles(w.particles)
+    config = abi.self_field_config(w.config)
+    run.initialize_self_field(config)          # warm-up (allocation paths, module load)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    report = run.initialize_self_field(config)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    run.close()
+    cfg = w.config
+    nodes = (cfg.nx + 1) * (cfg.ny + 1) * cfg.nz
+    iterations = report["iterations"]
+    return {"initial_self_field": {
+        "workload": w.name, "model": "cowan-relativistic-poisson", "tolerance": 1e-10,
+        "particles": args.particles, "ms": ms, "iterations": iterations,
+        "ms_per_iteration": ms / max(iterations, 1),
+        "cg_bytes_per_iteration": 88 * nodes,
+        "cg_gbs_upper_bound": 88 * nodes * iterations / (ms * 1e-3) / 1e9,
+        "gauss_relative_residual": report["relative_residual"],
+        "mean_beta_z": report["mean_beta_z"]}}
 
 
 def scan_benchmarks(args):
