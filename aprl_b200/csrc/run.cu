@@ -2308,10 +2308,18 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   }
   r->ledger_start_ready = false;
 
+  // Tiled CG grid: (i, j) column tiles, z split into chunks for about two
+  // blocks per SM's worth of blocks.
+  const unsigned gx = blocks_for((size_t)L.lx, kSfTileX), gy = blocks_for((size_t)L.ly, kSfTileY);
+  const unsigned gz = (unsigned)std::max<size_t>(
+      1, std::min<size_t>(c.nz, (2 * kSelfFieldBlocks + gx * gy - 1) / (gx * gy)));
+  const dim3 tile_grid(gx, gy, gz), tile_block(kSfTileX, kSfTileY);
+  const int tblocks = (int)(gx * gy * gz);
   SfBuffers buf;
   for (int q = 0; q < 4; ++q) TRY(device_alloc(&buf.slab[q], slab));
   TRY(device_alloc(&buf.rho, rho_count));
-  TRY(device_alloc(&buf.partial, (size_t)kSelfFieldBlocks * kMoments));
+  TRY(device_alloc(&buf.partial,
+                   std::max<size_t>((size_t)kSelfFieldBlocks * kMoments, 2 * (size_t)tblocks)));
   TRY(device_alloc(&buf.out, 16));
   TRY(device_alloc(&buf.state, 1));
   TRY(device_alloc(&buf.max_bits, 1));
@@ -2373,6 +2381,7 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   A.diagonal = 2.0 * (A.cx + A.cy + A.cz);
   A.cowan = cowan ? 1 : 0;
   A.tolerance = cfg->relative_tolerance;
+  A.chunk = (int)((c.nz + gz - 1) / gz);
   A.partial = buf.partial;
   A.state = buf.state;
   for (int a = 0; a < 3; ++a) {
@@ -2452,13 +2461,10 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   const DGrid g = make_grid<double>(r);
   TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
              buf.rho, L.lx, L.ly, pad, r->d_status));
-  const int nblocks = (int)std::min<size_t>(kSelfFieldBlocks,
-                                            blocks_for(slab, kSelfFieldThreads));
   const DD vertex_volume = ledger_product(ledger_product(c.dx, c.dy), c.dz);
-  TRY(launch(r, kSfSource, sf_source_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A,
-             vertex_volume));
+  TRY(launch(r, kSfSource, sf_source_kernel, tile_grid, tile_block, A, vertex_volume));
   TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
-             (const DD*)buf.partial, nblocks, 2, buf.out));
+             (const DD*)buf.partial, tblocks, 2, buf.out));
   DD sums[2];
   TRY(sf_read(r, buf.out, sums, 2));
   TRY(check_device(r));
@@ -2482,11 +2488,11 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   while (issued < cfg->maximum_iterations) {
     const uint64_t batch = std::min<uint64_t>(32, cfg->maximum_iterations - issued);
     for (uint64_t it = 0; it < batch; ++it) {
-      TRY(launch(r, kSfApply, sf_apply_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
-      TRY(launch(r, kSfAlpha, sf_alpha_kernel, dim3(1), dim3(kSelfFieldThreads), A, nblocks));
-      TRY(launch(r, kSfUpdate, sf_update_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
-      TRY(launch(r, kSfBeta, sf_beta_kernel, dim3(1), dim3(kSelfFieldThreads), A, nblocks));
-      TRY(launch(r, kSfDirection, sf_direction_kernel, dim3(nblocks), dim3(kSelfFieldThreads), A));
+      TRY(launch(r, kSfApply, sf_apply_kernel, tile_grid, tile_block, A));
+      TRY(launch(r, kSfAlpha, sf_alpha_kernel, dim3(1), dim3(kSelfFieldThreads), A, tblocks));
+      TRY(launch(r, kSfUpdate, sf_update_kernel, tile_grid, tile_block, A));
+      TRY(launch(r, kSfBeta, sf_beta_kernel, dim3(1), dim3(kSelfFieldThreads), A, tblocks));
+      TRY(launch(r, kSfDirection, sf_direction_kernel, tile_grid, tile_block, A));
     }
     issued += batch;
     CUDA_TRY(cudaMemcpyAsync(&state, buf.state, sizeof state, cudaMemcpyDeviceToHost, r->stream));
@@ -2508,7 +2514,7 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   if (cowan) {
     for (int axis = 0; axis < 3; ++axis) {
       CUDA_TRY(cudaMemsetAsync(A.image, 0, slab * sizeof(double), r->stream));
-      TRY(launch(r, kSfSmooth, sf_smooth_kernel, dim3(fblocks), dim3(256), A, axis));
+      TRY(launch(r, kSfSmooth, sf_smooth_kernel, tile_grid, tile_block, A, axis));
       TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, axis, 1.0, 1));
     }
   } else {

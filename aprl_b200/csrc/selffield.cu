@@ -6,7 +6,7 @@ namespace aprl_gpu {
 namespace {
 
 __device__ DD sf_block_sum(DD v, DD* shared) {
-  const int t = threadIdx.x;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
   shared[t] = v;
   __syncthreads();
   for (int s = kSelfFieldThreads / 2; s > 0; s >>= 1) {
@@ -38,28 +38,32 @@ __device__ __forceinline__ double sf_held_beta_z(double u0, double u1, double u2
   return box / hypot(1.0, box);
 }
 
-__device__ __forceinline__ bool sf_interior(const SfLattice& L, int i, int j, int k) {
-  return i > L.lo[0] && i < L.hi[0] && j > L.lo[1] && j < L.hi[1] && k > L.lo[2] &&
-         k < L.hi[2];
-}
-
 __device__ __forceinline__ size_t sf_at(const SfLattice& L, int i, int j, int p) {
   return ((size_t)p * L.ly + j) * L.lx + i;
 }
 
-// Node n of the planes 1..nz of the lattice: i, j and the plane p.
-__device__ __forceinline__ void sf_node(const SfLattice& L, long long n, int& i, int& j, int& p) {
-  i = (int)(n % L.lx);
-  const long long r = n / L.lx;
-  j = (int)(r % L.ly);
-  p = 1 + (int)(r / L.ly);
-}
-
-__device__ __forceinline__ long long sf_nodes(const SfLattice& L) {
-  return (long long)L.lx * L.ly * (L.planes - 2);
-}
-
 __device__ __forceinline__ bool sf_stopped(const SfArgs& a) { return a.state->done != 0; }
+
+// The interior vertices of this block's tile: (i, j) and planes [p0, p1].
+struct SfTile {
+  int i, j, p0, p1;
+  bool column;  // (i, j) is an interior column
+};
+__device__ __forceinline__ SfTile sf_tile(const SfArgs& a) {
+  const SfLattice& L = a.L;
+  SfTile t;
+  t.i = blockIdx.x * kSfTileX + threadIdx.x;
+  t.j = blockIdx.y * kSfTileY + threadIdx.y;
+  t.column = t.i > L.lo[0] && t.i < L.hi[0] && t.j > L.lo[1] && t.j < L.hi[1];
+  // planes p = k + 1 with k in (lo2, hi2)
+  t.p0 = max(L.lo[2] + 2, 1 + (int)blockIdx.z * a.chunk);
+  t.p1 = min(L.hi[2], (int)(blockIdx.z + 1) * a.chunk);
+  return t;
+}
+__device__ __forceinline__ int sf_block_index() {
+  return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+}
+__device__ __forceinline__ bool sf_first_thread() { return threadIdx.x == 0 && threadIdx.y == 0; }
 
 }  // namespace
 
@@ -157,24 +161,22 @@ __global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, i
 __global__ void __launch_bounds__(kSelfFieldThreads) sf_source_kernel(SfArgs a, DD volume) {
   __shared__ DD shared[kSelfFieldThreads];
   const SfLattice& L = a.L;
+  const SfTile t = sf_tile(a);
   DD charge{0., 0.}, source{0., 0.};
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
-       n += (long long)gridDim.x * blockDim.x) {
-    int i, j, p;
-    sf_node(L, n, i, j, p);
-    if (!sf_interior(L, i, j, p - 1)) continue;
-    const double q = a.rho[((size_t)(p - 1) * L.ly + j) * L.lx + i];
-    const double v = q / kEpsilon0;
-    a.residual[sf_at(L, i, j, p)] = v;
-    a.direction[sf_at(L, i, j, p)] = v;
-    charge = dd_add(charge, dd_mul(volume, q));
-    source = dd_add(source, two_prod(v, v));
-  }
+  if (t.column)
+    for (int p = t.p0; p <= t.p1; ++p) {
+      const double q = a.rho[((size_t)(p - 1) * L.ly + t.j) * L.lx + t.i];
+      const double v = q / kEpsilon0;
+      a.residual[sf_at(L, t.i, t.j, p)] = v;
+      a.direction[sf_at(L, t.i, t.j, p)] = v;
+      charge = dd_add(charge, dd_mul(volume, q));
+      source = dd_add(source, two_prod(v, v));
+    }
   charge = sf_block_sum(charge, shared);
   source = sf_block_sum(source, shared);
-  if (threadIdx.x == 0) {
-    a.partial[2 * blockIdx.x] = charge;
-    a.partial[2 * blockIdx.x + 1] = source;
+  if (sf_first_thread()) {
+    a.partial[2 * sf_block_index()] = charge;
+    a.partial[2 * sf_block_index() + 1] = source;
   }
 }
 
@@ -186,34 +188,34 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_apply_kernel(SfArgs a) {
   __shared__ DD shared[kSelfFieldThreads];
   if (sf_stopped(a)) return;
   const SfLattice& L = a.L;
+  const SfTile t = sf_tile(a);
+  const int i = t.i, j = t.j;
   DD dot{0., 0.};
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
-       n += (long long)gridDim.x * blockDim.x) {
-    int i, j, p;
-    sf_node(L, n, i, j, p);
-    if (!sf_interior(L, i, j, p - 1)) continue;
-    const double* d = a.direction;
-    double value;
-    if (a.cowan) {
-      value = 0.0;
+  if (t.column)
+    for (int p = t.p0; p <= t.p1; ++p) {
+      const double* d = a.direction;
+      double value;
+      if (a.cowan) {
+        value = 0.0;
 #pragma unroll
-      for (int z = 0; z < 3; ++z)
+        for (int z = 0; z < 3; ++z)
 #pragma unroll
-        for (int y = 0; y < 3; ++y)
+          for (int y = 0; y < 3; ++y)
 #pragma unroll
-          for (int x = 0; x < 3; ++x)
-            value += a.stencil[(z * 3 + y) * 3 + x] * d[sf_at(L, i - 1 + x, j - 1 + y, p - 1 + z)];
-    } else {
-      value = a.diagonal * d[sf_at(L, i, j, p)] -
-              a.cx * (d[sf_at(L, i - 1, j, p)] + d[sf_at(L, i + 1, j, p)]) -
-              a.cy * (d[sf_at(L, i, j - 1, p)] + d[sf_at(L, i, j + 1, p)]) -
-              a.cz * (d[sf_at(L, i, j, p - 1)] + d[sf_at(L, i, j, p + 1)]);
+            for (int x = 0; x < 3; ++x)
+              value +=
+                  a.stencil[(z * 3 + y) * 3 + x] * d[sf_at(L, i - 1 + x, j - 1 + y, p - 1 + z)];
+      } else {
+        value = a.diagonal * d[sf_at(L, i, j, p)] -
+                a.cx * (d[sf_at(L, i - 1, j, p)] + d[sf_at(L, i + 1, j, p)]) -
+                a.cy * (d[sf_at(L, i, j - 1, p)] + d[sf_at(L, i, j + 1, p)]) -
+                a.cz * (d[sf_at(L, i, j, p - 1)] + d[sf_at(L, i, j, p + 1)]);
+      }
+      a.image[sf_at(L, i, j, p)] = value;
+      dot = dd_add(dot, two_prod(d[sf_at(L, i, j, p)], value));
     }
-    a.image[sf_at(L, i, j, p)] = value;
-    dot = dd_add(dot, two_prod(d[sf_at(L, i, j, p)], value));
-  }
   dot = sf_block_sum(dot, shared);
-  if (threadIdx.x == 0) a.partial[blockIdx.x] = dot;
+  if (sf_first_thread()) a.partial[sf_block_index()] = dot;
 }
 
 // alpha = |r|^2 / (d . A d), rounded once to binary64.
@@ -239,21 +241,19 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_update_kernel(SfArgs a) 
   __shared__ DD shared[kSelfFieldThreads];
   if (sf_stopped(a)) return;
   const SfLattice& L = a.L;
+  const SfTile t = sf_tile(a);
   const double alpha = a.state->alpha;
   DD dot{0., 0.};
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
-       n += (long long)gridDim.x * blockDim.x) {
-    int i, j, p;
-    sf_node(L, n, i, j, p);
-    if (!sf_interior(L, i, j, p - 1)) continue;
-    const size_t at = sf_at(L, i, j, p);
-    a.potential[at] += alpha * a.direction[at];
-    const double r = a.residual[at] + -alpha * a.image[at];
-    a.residual[at] = r;
-    dot = dd_add(dot, two_prod(r, r));
-  }
+  if (t.column)
+    for (int p = t.p0; p <= t.p1; ++p) {
+      const size_t at = sf_at(L, t.i, t.j, p);
+      a.potential[at] += alpha * a.direction[at];
+      const double r = a.residual[at] + -alpha * a.image[at];
+      a.residual[at] = r;
+      dot = dd_add(dot, two_prod(r, r));
+    }
   dot = sf_block_sum(dot, shared);
-  if (threadIdx.x == 0) a.partial[blockIdx.x] = dot;
+  if (sf_first_thread()) a.partial[sf_block_index()] = dot;
 }
 
 // The relative residual, the stopping test and beta
@@ -282,19 +282,19 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_beta_kernel(SfArgs a, in
   st.rr = s;
 }
 
-// direction = r + beta direction at the interior vertices, zero elsewhere
-// (combineDirection, src/eb_initial_field.cpp:423-438).
+// direction = r + beta direction at the interior vertices
+// (combineDirection, src/eb_initial_field.cpp:423-438); the other vertices
+// of the direction are zero from the start and stay zero.
 __global__ void sf_direction_kernel(SfArgs a) {
   if (sf_stopped(a)) return;
   const SfLattice& L = a.L;
+  const SfTile t = sf_tile(a);
   const double beta = a.state->beta;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
-       n += (long long)gridDim.x * blockDim.x) {
-    int i, j, p;
-    sf_node(L, n, i, j, p);
-    const size_t at = sf_at(L, i, j, p);
-    a.direction[at] = sf_interior(L, i, j, p - 1) ? a.residual[at] + beta * a.direction[at] : 0.0;
-  }
+  if (t.column)
+    for (int p = t.p0; p <= t.p1; ++p) {
+      const size_t at = sf_at(L, t.i, t.j, p);
+      a.direction[at] = a.residual[at] + beta * a.direction[at];
+    }
 }
 
 // The Cowan-smoothed potential of one axis minus the translation term, at
@@ -303,11 +303,10 @@ __global__ void sf_direction_kernel(SfArgs a) {
 __global__ void sf_smooth_kernel(SfArgs a, int axis) {
   const SfLattice& L = a.L;
   const int ta = (axis + 1) % 3, tb = (axis + 2) % 3;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < sf_nodes(L);
-       n += (long long)gridDim.x * blockDim.x) {
-    int i, j, p;
-    sf_node(L, n, i, j, p);
-    if (!sf_interior(L, i, j, p - 1)) continue;
+  const SfTile t = sf_tile(a);
+  if (!t.column) return;
+  for (int p = t.p0; p <= t.p1; ++p) {
+    const int i = t.i, j = t.j;
     const double* phi = a.potential;
     double value = a.alpha[axis] * phi[sf_at(L, i, j, p)];
     for (int sign = -1; sign <= 1; sign += 2) {
@@ -318,10 +317,10 @@ __global__ void sf_smooth_kernel(SfArgs a, int axis) {
       value += a.beta[tb] * phi[sf_at(L, pb[0], pb[1], pb[2])];
     }
     for (int s = -1; s <= 1; s += 2)
-      for (int t = -1; t <= 1; t += 2) {
+      for (int u = -1; u <= 1; u += 2) {
         int pt[3] = {i, j, p};
         pt[ta] += s;
-        pt[tb] += t;
+        pt[tb] += u;
         value += a.delta[axis] * phi[sf_at(L, pt[0], pt[1], pt[2])];
       }
     a.image[sf_at(L, i, j, p)] =

@@ -52,9 +52,14 @@ struct SfArgs {
   double alpha[3], beta[3], delta[3];  // delta per axis: yz, zx, xy
   double translation;
   double tolerance;
+  int chunk;                    // planes per block of the tiled CG kernels
   DD* partial;
   SfState* state;
 };
+
+// Tiled CG kernels: blocks of kSfTileX x kSfTileY threads over the lattice's
+// (i, j) columns, each marching `chunk` planes; one partial per block.
+constexpr int kSfTileX = 32, kSfTileY = 4;
 
 struct SfParticles {
   const double *x, *y, *z, *ux, *uy, *uz, *q, *m;
