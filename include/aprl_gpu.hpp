@@ -122,6 +122,14 @@ class PicRun {
     return s;
   }
 
+  // EBGaussFieldInitializer::initialize on the run's particles (before the
+  // first step).
+  aprl_self_field_report initializeSelfField(const aprl_self_field_config& config) {
+    aprl_self_field_report report{};
+    check(aprl_run_initialize_self_field(run_, &config, &report));
+    return report;
+  }
+
   // MovingWindowFields::enableEnergyLedger / energyLedger plus the ledger
   // record's interior field energy and particle energy sums.
   void enableEnergyLedger(bool enabled = true) {
