@@ -185,6 +185,25 @@ MEASURED_TRAFFIC = {"push_deposit": ("particle", 349.0),
                     "orbit_sum": ("launch", 788.7e6)}
 
 
+# L2 reduction sectors per particle of one push_deposit launch (ncu
+# lts__t_sectors_op_red of the 250k-particle dipole capture: 22.6 M).
+RED_SECTORS_PER_PARTICLE = 90.4
+
+
+def atomic_peak():
+    """Measured L2 FP64 reduction rate of this GPU (aprl_b200/csrc/probe.cu):
+    every lane adds to its own 32-byte sector of a 16 MB window, neighbouring
+    lanes on neighbouring sectors, as the cell-sorted deposit's reductions
+    land; best of 5 launches, in G reductions/s."""
+    import ctypes
+    from aprl_b200 import build as product_build
+    lib = ctypes.CDLL(product_build.build_probe(verbose=False))
+    rate = ctypes.c_double()
+    if lib.aprl_probe_reduction_rate(16, 5, ctypes.byref(rate)) != 0:
+        return None
+    return rate.value / 1e9
+
+
 def measured_traffic(kernel, particles):
     kind, value = MEASURED_TRAFFIC.get(kernel, (None, None))
     if kind == "particle":
@@ -332,6 +351,21 @@ def run_ours(args):
                                       "grid, scaled per particle for particle kernels",
                     "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
                     "launches": count}
+    atomic_roofline = None
+    if "push_deposit" in profile and world == 1:
+        ms, count = profile["push_deposit"]
+        per_launch_ms = ms / max(count, 1)
+        sectors = RED_SECTORS_PER_PARTICLE * particle_steps / max(K, 1)
+        achieved_atomic = sectors / (per_launch_ms * 1e-3) / 1e9
+        peak_atomic = atomic_peak()
+        atomic_roofline = {
+            "kernel": "push_deposit", "bound": "l2-fp64-atomics",
+            "achieved": achieved_atomic, "peak": peak_atomic, "unit": "G reductions/s",
+            "frac": achieved_atomic / peak_atomic if peak_atomic else None,
+            "peak_source": "measured here: one FP64 reduction per lane per 32-byte sector, "
+                           "neighbouring sectors, 16 MB window (aprl_b200/csrc/probe.cu)",
+            "reductions_per_particle": RED_SECTORS_PER_PARTICLE,
+            "note": "whole push_deposit launch time, push arithmetic included"}
     kernels = {k: {"ms": v[0], "launches": v[1],
                    "share": v[0] / max(sum(x[0] for x in profile.values()), 1e-12)}
                for k, v in profile.items()}
@@ -358,6 +392,7 @@ def run_ours(args):
                 "wall_ms_per_step": e2e_wall_ms / K},
         "gpu_launches": launches,
         "roofline": roofline,
+        "atomic_roofline": atomic_roofline,
         "kernels": kernels,
         "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
                    "reasons": clocks.get("reasons", [])},
