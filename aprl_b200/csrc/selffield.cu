@@ -182,8 +182,10 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_source_kernel(SfArgs a, 
 
 // image = A direction at the interior vertices: the 7-point relativistic
 // operator (applyNegativeLaplacian, src/eb_initial_field.cpp:210-236) or the
-// 27-point Cowan one (applyNegativeCowanLaplacian, :318-342); partial sums
-// of direction . image.
+// 27-point Cowan one (applyNegativeCowanLaplacian, :318-342; its 27-term sum
+// in the reference's order, each term a fused multiply-add, which halves the
+// kernel's FP64 instructions and moves each sum by at most a rounding per
+// term); partial sums of direction . image.
 __global__ void __launch_bounds__(kSelfFieldThreads) sf_apply_kernel(SfArgs a) {
   __shared__ DD shared[kSelfFieldThreads];
   if (sf_stopped(a)) return;
@@ -203,8 +205,8 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_apply_kernel(SfArgs a) {
           for (int y = 0; y < 3; ++y)
 #pragma unroll
             for (int x = 0; x < 3; ++x)
-              value +=
-                  a.stencil[(z * 3 + y) * 3 + x] * d[sf_at(L, i - 1 + x, j - 1 + y, p - 1 + z)];
+              value = fma(a.stencil[(z * 3 + y) * 3 + x],
+                          d[sf_at(L, i - 1 + x, j - 1 + y, p - 1 + z)], value);
       } else {
         value = a.diagonal * d[sf_at(L, i, j, p)] -
                 a.cx * (d[sf_at(L, i - 1, j, p)] + d[sf_at(L, i + 1, j, p)]) -
