@@ -496,6 +496,9 @@ def _percentiles(values):
     return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))}
 
 
+SELF_FIELD_SMALL = {"cells": (48, 48, 128), "particles": 50_000, "energy_ev": 8.84e6}
+
+
 def self_field_benchmark(args, stream):
     """The initial self-field solve (Cowan relativistic Poisson, tolerance
     1e-10) on the dipole grid with 1M particles at beta_z ~ 0.5, timed with
@@ -516,6 +519,17 @@ def self_field_benchmark(args, stream):
     torch.cuda.synchronize()
     ms = start.elapsed_time(stop)
     run.close()
+    # The small case the CPU baseline also solves.
+    sw = workloads.self_field_case(SELF_FIELD_SMALL["energy_ev"], nx=SELF_FIELD_SMALL["cells"][0],
+                                   ny=SELF_FIELD_SMALL["cells"][1], nz=SELF_FIELD_SMALL["cells"][2],
+                                   particles=SELF_FIELD_SMALL["particles"])
+    small = native.Run(native.load(), sw.config, stream=stream.cuda_stream)
+    small.load_workload(sw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    small_report = small.initialize_self_field(abi.self_field_config(sw.config))
+    small_ms = (time.perf_counter() - t0) * 1e3
+    small.close()
     cfg = w.config
     nodes = (cfg.nx + 1) * (cfg.ny + 1) * cfg.nz
     iterations = report["iterations"]
@@ -526,7 +540,9 @@ def self_field_benchmark(args, stream):
         "cg_bytes_per_iteration": 88 * nodes,
         "cg_gbs_upper_bound": 88 * nodes * iterations / (ms * 1e-3) / 1e9,
         "gauss_relative_residual": report["relative_residual"],
-        "mean_beta_z": report["mean_beta_z"]}}
+        "mean_beta_z": report["mean_beta_z"],
+        "small": {"workload": sw.name, "particles": SELF_FIELD_SMALL["particles"],
+                  "ms_wall": small_ms, "iterations": small_report["iterations"]}}}
 
 
 def scan_benchmarks(args):
@@ -635,9 +651,22 @@ def cpu_baseline(args):
             break
     elapsed = time.perf_counter() - t0
     run.close()
-    return {"value": ps / elapsed, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-            "sample": f"{done} steps of a 128x128x64-cell slice with "
-                      f"{w.particles['x'].size} particles (1/8 of the window and bunch)"}
+    out = {"value": ps / elapsed, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+           "sample": f"{done} steps of a 128x128x64-cell slice with "
+                     f"{w.particles['x'].size} particles (1/8 of the window and bunch)"}
+    # The initial self-field solve of the same checker on the small solve
+    # case that the GPU leg also times (initial_self_field.small).
+    sw = workloads.self_field_case(SELF_FIELD_SMALL["energy_ev"], nx=SELF_FIELD_SMALL["cells"][0],
+                                   ny=SELF_FIELD_SMALL["cells"][1], nz=SELF_FIELD_SMALL["cells"][2],
+                                   particles=SELF_FIELD_SMALL["particles"])
+    srun = native.Run(binding, sw.config).load_workload(sw)
+    t0 = time.perf_counter()
+    report = srun.initialize_self_field(abi.self_field_config(sw.config))
+    out["initial_self_field_small"] = {"ms": (time.perf_counter() - t0) * 1e3,
+                                       "iterations": report["iterations"], "cores": 1,
+                                       "kind": kind, "sample": sw.name}
+    srun.close()
+    return out
 
 
 def run_reference(args):
