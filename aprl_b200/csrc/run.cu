@@ -2577,6 +2577,63 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   return APRL_OK;
 }
 
+aprl_status aprl_run_get_reference(aprl_run* r, unsigned a, double* host, size_t count) {
+  if (!r || a >= 6 || !host) return fail(APRL_ERR_OUT_OF_RANGE, "Moving-window component");
+  size_t s[3];
+  comp_shape(r->cfg, a, s);
+  const size_t n = s[0] * s[1] * (r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0));
+  if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
+  if (!r->ref_set[a]) return fail(APRL_ERR_RUNTIME, "Moving-window reference component is not set");
+  CUDA_TRY(cudaMemcpyAsync(host, r->ref[a], n * 8, cudaMemcpyDeviceToHost, r->stream));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+aprl_status aprl_run_prepare_reference(aprl_run* r, size_t n, const double* x, const double* y,
+                                       const double* z, const double* ux, const double* uy,
+                                       const double* uz, const double* q, const double* m,
+                                       const aprl_self_field_config* config,
+                                       aprl_self_field_report* report) {
+  if (!r || !config || !report) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  if (r->stage != 0 || r->step != 0)
+    return fail(APRL_ERR_RUNTIME, "The inlet reference is prepared before the first step");
+  // The reference grid as a run of its own: reference_nz cells from the
+  // reference origin.
+  aprl_run_config tc = r->cfg;
+  tc.nz = r->cfg.reference_nz;
+  tc.initial_offset = 0;
+  aprl_run* t = nullptr;
+  TRY(aprl_run_create(&tc, r->stream, &t));
+  std::vector<uint64_t> ids(n);
+  for (size_t i = 0; i < n; ++i) ids[i] = i;
+  aprl_status s = aprl_run_set_particles(t, n, x, y, z, ux, uy, uz, q, m, ids.data(), 1);
+  if (s == APRL_OK) s = aprl_run_initialize_self_field(t, config, report);
+  for (int a = 0; s == APRL_OK && a < 6; ++a) {
+    const size_t count = a < 3 ? e_count(tc, a) : b_count(tc, a - 3);
+    const double* from = a < 3 ? t->e[t->cur][a] : t->b[a - 3];
+    if (cudaStreamSynchronize(r->stream) != cudaSuccess) {
+      s = fail(APRL_ERR_CUDA, "cudaStreamSynchronize failed");
+      break;
+    }
+    cudaFree(r->ref[a]);
+    r->ref[a] = nullptr;
+    s = device_alloc(&r->ref[a], count);
+    if (s != APRL_OK) break;
+    // A fresh run's rings start at base 0: its fields are in native order.
+    const cudaError_t e =
+        cudaMemcpyAsync(r->ref[a], from, count * 8, cudaMemcpyDeviceToDevice, r->stream);
+    if (e != cudaSuccess) {
+      s = fail(APRL_ERR_CUDA, "cudaMemcpyAsync: %s", cudaGetErrorString(e));
+      break;
+    }
+    r->ref_set[a] = true;
+  }
+  if (s == APRL_OK && cudaStreamSynchronize(r->stream) != cudaSuccess)
+    s = fail(APRL_ERR_CUDA, "cudaStreamSynchronize failed");
+  aprl_run_destroy(t);
+  return s;
+}
+
 aprl_status aprl_run_synchronize(aprl_run* r) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
   CUDA_TRY(cudaStreamSynchronize(r->stream));

@@ -71,6 +71,10 @@ _PRODUCT_ONLY = {
     "run_sample_field_plane_noalloc": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                                  C.POINTER(C.c_int)]),
     "run_gauss_law": (C.c_int, [_H, C.POINTER(abi.GaussLaw), _D, C.c_size_t]),
+    "run_prepare_reference": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D, _D, _D,
+                                        C.POINTER(abi.SelfFieldConfig),
+                                        C.POINTER(abi.SelfFieldReport)]),
+    "run_get_reference": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
     "scan_footprint": (C.c_int, [C.POINTER(abi.RunConfig), C.c_size_t, _U64]),
     "scan_create": (C.c_int, [C.POINTER(abi.ScanConfig), C.POINTER(C.c_void_p)]),
     "scan_submit": (C.c_int, [C.c_void_p, C.POINTER(abi.ScanRequest), _U64]),
@@ -331,6 +335,23 @@ class Run:
         out = abi.EnergyLedger()
         self.b("run_energy_ledger", self.handle, C.byref(out))
         return out.as_dict()
+
+    def prepare_reference(self, particles, config):
+        """The inlet reference tables from the Cowan self-field of `particles`
+        on the reference grid (aprl_run_prepare_reference)."""
+        p = {k: np.ascontiguousarray(particles[k], dtype=np.float64)
+             for k in ("x", "y", "z", "ux", "uy", "uz", "charge", "mass")}
+        out = abi.SelfFieldReport()
+        self.b("run_prepare_reference", self.handle, p["x"].size, _ptr(p["x"]), _ptr(p["y"]),
+               _ptr(p["z"]), _ptr(p["ux"]), _ptr(p["uy"]), _ptr(p["uz"]), _ptr(p["charge"]),
+               _ptr(p["mass"]), C.byref(config), C.byref(out))
+        return out.as_dict()
+
+    def get_reference(self, component):
+        nx_c, ny_c, nz_c = abi.reference_shape(self.config, component)
+        out = np.empty((nz_c, ny_c, nx_c))
+        self.b("run_get_reference", self.handle, component, _ptr(out), out.size)
+        return out
 
     def gauss_law(self, residual=False):
         """Summary dict, and with residual=True also G per node [k][j][i]."""

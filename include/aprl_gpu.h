@@ -439,6 +439,28 @@ typedef struct {
 aprl_status aprl_run_initialize_self_field(aprl_run* run, const aprl_self_field_config* config,
                                            aprl_self_field_report* report);
 
+/* The inlet reference of a moving window prepared on the GPU from a bunch
+ * (the role of BlockedCowanReference, src/blocked_cowan_reference.h:59-130,
+ * and its fill of MovingWindowReference): the Cowan initial self-field
+ * (aprl_run_initialize_self_field with `config`) of the given particles on
+ * the reference grid (nx, ny, reference_nz cells from reference_origin),
+ * whose E and B become the run's six reference tables.  The reference
+ * checks that the blocked modal solve reproduces this initializer on the
+ * same grid to its CG tolerance (verification/blocked_cowan_reference_checks.cpp:61-130);
+ * here the initializer itself is the solve.  Particles in box coordinates
+ * at box time 0; ids are not needed.  Allocates a temporary run of the
+ * reference grid's size for the solve.  Before the first step. */
+aprl_status aprl_run_prepare_reference(aprl_run* run, size_t count, const double* x,
+                                       const double* y, const double* z, const double* ux,
+                                       const double* uy, const double* uz,
+                                       const double* charge, const double* mass,
+                                       const aprl_self_field_config* config,
+                                       aprl_self_field_report* report);
+
+/* Read back one reference table (the layout of aprl_run_set_reference). */
+aprl_status aprl_run_get_reference(aprl_run* run, unsigned component, double* host,
+                                   size_t count);
+
 /* Discrete Gauss law of the current state, reduced on the GPU.  The node
  * charge density is the one the linear-binomial3 current conserves: per
  * particle, F3 node weights in x over nodes i-1..i+2, linear weights in y

@@ -130,6 +130,17 @@ class PicRun {
     return report;
   }
 
+  // The inlet reference from the Cowan self-field of a bunch on the
+  // reference grid (before the first step).
+  aprl_self_field_report prepareReference(const ParticleArrays& p,
+                                          const aprl_self_field_config& config) {
+    aprl_self_field_report report{};
+    check(aprl_run_prepare_reference(run_, p.x.size(), p.x.data(), p.y.data(), p.z.data(),
+                                     p.ux.data(), p.uy.data(), p.uz.data(), p.charge.data(),
+                                     p.mass.data(), &config, &report));
+    return report;
+  }
+
   // MovingWindowFields::enableEnergyLedger / energyLedger plus the ledger
   // record's interior field energy and particle energy sums.
   void enableEnergyLedger(bool enabled = true) {
