@@ -97,6 +97,26 @@ WORKLOADS = {
 }
 
 
+def over_ranks(times, counts, world, device="cuda"):
+    """The job's figures from every rank's: the maximum of `times` (a run
+    ends when its slowest replica does) and the sums of `counts` (the units
+    all replicas processed).  One rank: the inputs unchanged.  The same
+    collective steps on every rank, in the same order."""
+    import torch
+    import torch.distributed as dist
+    vals = torch.tensor([float(t) for t in times] + [float(c) for c in counts],
+                        dtype=torch.float64, device=device)
+    if world <= 1:
+        return [float(t) for t in times], [int(c) for c in counts]
+    mx = vals.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = vals.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    n = len(times)
+    return ([mx[i].item() for i in range(n)],
+            [int(round(sm[n + i].item())) for i in range(len(counts))])
+
+
 def measured_peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -316,15 +336,8 @@ def run_ours(args):
         fp32_arm = time_fp32_arm(args, w, stream, run, detector_lab_z, world)
 
     # max over ranks, totals over ranks
-    vals = torch.tensor([elapsed_ms, e2e_ms, float(particle_steps), float(e2e_particle_steps)],
-                        dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = vals.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = vals.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        elapsed_ms, e2e_ms = mx[0].item(), mx[1].item()
-        particle_steps, e2e_particle_steps = int(sm[2].item()), int(sm[3].item())
+    (elapsed_ms, e2e_ms), (particle_steps, e2e_particle_steps) = over_ranks(
+        [elapsed_ms, e2e_ms], [particle_steps, e2e_particle_steps], world)
     run.close()
     if world > 1:
         dist.destroy_process_group()
@@ -444,13 +457,7 @@ def time_fp32_arm(args, w, stream, fp64_run, detector_lab_z, world):
     torch.cuda.synchronize()
     ms = start.elapsed_time(stop)
     stats = run.stats()
-    vals = torch.tensor([ms, float(particle_steps)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = vals.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = vals.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms, particle_steps = mx[0].item(), int(sm[1].item())
+    (ms,), (particle_steps,) = over_ranks([ms], [particle_steps], world)
     while run.stats()["step"] < fp64_run.stats()["step"]:
         run.step(1)
     mixed = run.sample_field_plane(detector_lab_z).reshape(-1, 6)
