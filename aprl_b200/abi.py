@@ -87,7 +87,7 @@ class RunConfig(C.Structure):
         ("activation_plane_lab_z", C.c_double),
         ("maximum_step", C.c_uint64),
         ("n_magnets", C.c_uint32),
-        ("reserved1", C.c_uint32),
+        ("inlet_charge_match", C.c_uint32),
         ("magnets", Magnet * MAX_MAGNETS),
     ]
 

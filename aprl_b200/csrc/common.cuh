@@ -52,6 +52,8 @@ enum DeviceError : unsigned {
   kErrEarlyRelease = 17,      // held particle released before entering the window
   kErrAdmission = 18,         // invalid upstream admission of a held particle
   kErrHeldBoundary = 19,      // held segment crossed a particle boundary
+  kErrInletSource = 20,       // non-finite charge-matched inlet source
+  kErrInletField = 21,        // non-finite charge-matched inlet field
   kErrCount
 };
 

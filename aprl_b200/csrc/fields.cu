@@ -10,6 +10,7 @@
 // the current J (double, or float in the FP32-mixed mode), which only the
 // commit reads.
 #include "common.cuh"
+#include "dd.cuh"
 #include "fields.cuh"
 
 namespace aprl_gpu {
@@ -317,6 +318,34 @@ __global__ void inlet_lower_kernel(InletPlaneArgs a) {
   const int nxc = a.nx + (c != 0), nyc = a.ny + (c != 1);
   if (i >= nxc || j >= nyc) return;
   a.out[c][(size_t)j * nxc + i] = inlet_value(a.inlet, c, i, j);
+}
+
+__global__ void inlet_complete_kernel(InletCompleteArgs a) {
+  const DGrid& g = a.g;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i <= a.cx || i >= g.nx - a.cx || j <= a.cy || j >= g.ny - a.cy) return;
+  // The reference evaluates this in long double; double-double here.
+  const DD dex = two_sum(g.e_old[0][e_index(g, 0, i, j, 1)], -g.e_old[0][e_index(g, 0, i - 1, j, 1)]);
+  const DD dey = two_sum(g.e_old[1][e_index(g, 1, i, j, 1)], -g.e_old[1][e_index(g, 1, i, j - 1, 1)]);
+  const DD divxy = dd_add(dd_div(dex, g.dx), dd_div(dey, g.dy));
+  const DD source = dd_div(DD{a.rho[(size_t)j * (g.nx + 1) + i], 0.}, kEpsilon0);
+  const DD change = dd_mul(dd_add(divxy, dd_neg(source)), g.dz);
+  const double value = dd_value(dd_add(DD{g.e_old[2][e_index(g, 2, i, j, 1)], 0.}, change));
+  if (!isfinite(value)) {
+    raise_error(a.status, kErrInletField, (unsigned long long)((size_t)j * (g.nx + 1) + i));
+    return;
+  }
+  g.e_old[2][e_index(g, 2, i, j, 0)] = value;
+}
+
+__global__ void inlet_halo_kernel(InletHaloArgs a) {
+  const DGrid& g = a.g;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i <= a.cx || i >= g.nx - a.cx || j <= a.cy || j >= g.ny - a.cy) return;
+  a.lower_ez[(size_t)j * (g.nx + 1) + i] -=
+      g.e_old[2][e_index(g, 2, i, j, 0)] - inlet_value(a.inlet, 2, i, j);
 }
 
 // MovingWindowFields::shift plane insertion (src/moving_window_fields.cpp:

@@ -62,6 +62,26 @@ struct PreviewArgs {
   double* pre_inlet[2];  // when set: Ex, Ey of plane 0 before the inlet overwrite
 };
 
+// ChargeMatchedInlet::complete (src/charge_matched_inlet.h:55-71): Ez of the
+// inserted layer at the interior nodes from the discrete Gauss law.
+struct InletCompleteArgs {
+  DGrid g;                  // e_old = E after the shift
+  const double* rho;        // (nx+1) x (ny+1) inlet-layer charge
+  int cx, cy;
+  DeviceStatus* status;
+};
+__global__ void inlet_complete_kernel(InletCompleteArgs a);
+
+// Boundary::begin with centred normal matching (src/moving_window_fields.cpp:225-236):
+// the lower Ez halo takes minus Ez's departure from the reference at k = 0.
+struct InletHaloArgs {
+  DGrid g;
+  double* lower_ez;         // (nx+1) x (ny+1)
+  InletTable inlet;         // reference(a, i, j, offset, step)
+  int cx, cy;
+};
+__global__ void inlet_halo_kernel(InletHaloArgs a);
+
 struct InletPlaneArgs {
   int nx, ny;
   double* out[3];

@@ -1513,6 +1513,68 @@ __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen,
     raise_error(status, kErrFellBehind, (unsigned long long)i);
 }
 
+__global__ void inlet_charge_kernel(InletMatchArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.np + a.pcount) return;
+  double pos[3], q;
+  long long where;
+  if (n < a.np) {
+    pos[0] = a.p.x[n];
+    pos[1] = a.p.y[n];
+    pos[2] = a.p.z[n];
+    q = a.p.q[n];
+    where = n;
+  } else {
+    const long long k = a.pbegin + (n - a.np);
+    pos[0] = a.src.x[k];
+    pos[1] = a.src.y[k];
+    pos[2] = repeat_held_addition(a.src.z[k], a.held_distance_per_beta * a.src.beta[k], a.steps);
+    q = a.src.q[k];
+    where = k;
+  }
+  // longitudinal_shape::nodeWeight(z, 1, shape) (src/longitudinal_shape.h:25-56)
+  const double z = (pos[2] - a.origin[2]) / a.dz;
+  double wz = 0.;
+  if (a.shape == 0) {
+    const double cell = floor(z), f = z - cell;
+    double v[4] = {0., 0., 0., 0.};
+    const double c[3] = {.25, .5, .25};
+    for (int k = -1; k <= 1; ++k) {
+      v[k + 1] += c[k + 1] * (1. - f);
+      v[k + 2] += c[k + 1] * f;
+    }
+    const long long first = (long long)cell - 1;
+    if (1 >= first && 1 < first + 4) wz = v[1 - first];
+  } else {
+    Basis<double> b;
+    quintic_basis<double>(z, false, b);
+    if (1 >= b.first && 1 < b.first + b.count) wz = b.v[1 - b.first];
+  }
+  if (wz == 0.) return;
+  const double x = (pos[0] - a.origin[0]) / a.dx, y = (pos[1] - a.origin[1]) / a.dy;
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z) || !isfinite(q)) {
+    raise_error(a.status, kErrInletSource, (unsigned long long)where);
+    return;
+  }
+  const bool binomial3 = a.shape == 0;
+  if (y < 0. || y > (double)a.ny) return;
+  if (binomial3 ? (x <= -2. || x >= (double)a.nx + 2.) : (x < 0. || x > (double)a.nx)) return;
+  const long long ix = (long long)floor(x);
+  const long long j = (long long)floor(y);
+  const double fx = x - ix, fy = y - j, scale = q * (1. / (a.dx * a.dy * a.dz));
+  double wx[4] = {1. - fx, fx, 0., 0.};
+  if (binomial3) node_weights(fx, wx);
+  const int n_x = binomial3 ? 4 : 2;
+  const long long first = ix - (binomial3 ? 1 : 0);
+  for (int b = 0; b < 2; ++b)
+    for (int c = 0; c < n_x; ++c) {
+      const long long i = first + c;
+      if (i >= 0 && i <= a.nx && j + b <= a.ny)
+        atomicAdd(&a.rho[(size_t)(j + b) * (a.nx + 1) + (size_t)i],
+                  scale * wx[c] * (b ? fy : 1. - fy) * wz);
+    }
+}
+
 __global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums) {
   if (trial_skipped(g)) return;
   const long long stride = (long long)gridDim.x * blockDim.x;

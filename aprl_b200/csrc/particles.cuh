@@ -231,6 +231,25 @@ __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
 // an active particle may not fall behind the inlet; held ones may.
 __global__ void inlet_check_kernel(const double* z, const unsigned char* frozen, long long n,
                                    double origin, DeviceStatus* status);
+// The inlet-layer charge of the charge-matched inlet (ChargeMatchedInlet::particle,
+// src/charge_matched_inlet.h:31-53) from the stored particles and the
+// pending entries [pbegin, pbegin + pcount) at their held positions of step
+// `steps` after the queue's first.
+struct InletMatchArgs {
+  DParticles p;
+  long long np;
+  DPending src;
+  long long pbegin, pcount;
+  unsigned long long steps;
+  double held_distance_per_beta;
+  double origin[3];
+  double dx, dy, dz;
+  int nx, ny, shape;
+  double* rho;                 // (nx+1) x (ny+1) node plane
+  DeviceStatus* status;
+};
+__global__ void inlet_charge_kernel(InletMatchArgs a);
+
 // A trial's start: J, the trial counters and the residual sums cleared
 // (skipped with the trial).
 __global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums);

@@ -59,7 +59,8 @@ enum Kernel : unsigned {
   kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
   kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict,
   kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfAlpha, kSfUpdate, kSfBeta,
-  kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy, kKernelCount
+  kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
+  kInletHalo, kInletCharge, kInletComplete, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -72,7 +73,7 @@ const char* kKernelNames[kKernelCount] = {
   "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish", "trial_clear",
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
   "sf_alpha", "sf_update", "sf_beta", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
-  "sf_clear", "sf_gauss", "sf_energy"};
+  "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -98,6 +99,8 @@ const char* device_error_text(unsigned code) {
       return "Moving-window upstream admission requires an unreleased held particle on rank zero";
     case kErrHeldBoundary:
       return "Held-transverse activation crossed a particle boundary during the frozen part of a field step";
+    case kErrInletSource: return "Nonfinite charge-matched inlet source";
+    case kErrInletField: return "Nonfinite charge-matched inlet field";
   }
   return "unknown device error";
 }
@@ -257,6 +260,7 @@ struct aprl_run {
   int zb_e[3]{}, zb_b[3]{};
   double* ref[6]{};
   bool ref_set[6]{};
+  double* inlet_rho = nullptr;  // charge-matched inlet: the inlet-layer charge plane
   DeviceProfile mprof[2], eprof[2];
   HistoryBuffer hist[8];  // ABI indices 0,3,4,5,6,9,10,11
   double max_rate[3]{};
@@ -546,6 +550,10 @@ aprl_status validate(const aprl_run_config& g) {
     return fail(APRL_ERR_INVALID_ARGUMENT, "Lorentz gamma must be finite and >= 1");
   if (g.n_magnets > APRL_MAX_MAGNETS)
     return fail(APRL_ERR_INVALID_ARGUMENT, "Too many prescribed magnets");
+  // ChargeMatchedInlet's constructor (src/charge_matched_inlet.h:21-27).
+  if (g.inlet_charge_match &&
+      (g.cpml_cells_x + 1 >= g.nx - g.cpml_cells_x || g.cpml_cells_y + 1 >= g.ny - g.cpml_cells_y))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Charge-matched inlet needs an interior physical aperture");
   return APRL_OK;
 }
 
@@ -996,6 +1004,16 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   TRY(inlet_table(r, r->offset - 1, r->step, ia.inlet));
   TRY(launch(r, kInletLower, inlet_lower_kernel,
              dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8), 3), dim3(32, 8), ia));
+  if (c.inlet_charge_match) {
+    InletHaloArgs ha{};
+    ha.g = make_grid<double>(r);
+    ha.lower_ez = r->lower[2];
+    ha.cx = (int)c.cpml_cells_x;
+    ha.cy = (int)c.cpml_cells_y;
+    TRY(inlet_table(r, r->offset, r->step, ha.inlet));
+    TRY(launch(r, kInletHalo, inlet_halo_kernel,
+               dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8)), dim3(32, 8), ha));
+  }
   CowanArgs<F> ca{};
   ca.g = make_grid<F>(r);
   for (int a = 0; a < 3; ++a) {
@@ -1314,6 +1332,54 @@ aprl_status shift_insert_t(aprl_run* r) {
                 dim3(blocks_for(max_row, 32), blocks_for(ydim, 8), 14), dim3(32, 8), sa);
 }
 
+// Simulation::completeMovingInletLayer (src/simulation_moving_window.cpp:312-318):
+// the inlet-layer charge of the stored particles and of the pending entries
+// due within 8 steps (visitNear), then Ez of the inserted layer.
+aprl_status inlet_charge_match(aprl_run* r) {
+  const aprl_run_config& c = r->cfg;
+  InletMatchArgs m{};
+  m.p = r->p;
+  m.np = (long long)r->np;
+  m.src = r->queue.d;
+  const auto& q = r->queue;
+  if (q.extracted) {
+    if (r->step < q.initial_step || r->step > q.maximum_step)
+      return fail(APRL_ERR_RUNTIME, "Invalid pending support view");
+    const uint64_t room = q.maximum_step - r->step;
+    const uint64_t until = r->step + std::min<uint64_t>(8, room);
+    const size_t end = q.offsets[until - q.initial_step + 1];
+    if (end > q.cursor) {
+      m.pbegin = (long long)q.cursor;
+      m.pcount = (long long)(end - q.cursor);
+    }
+    m.steps = r->step - q.initial_step;
+  }
+  m.held_distance_per_beta = held_distance_per_beta(c);
+  m.origin[0] = c.reference_origin[0];
+  m.origin[1] = c.reference_origin[1];
+  m.origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
+  m.dx = c.dx;
+  m.dy = c.dy;
+  m.dz = c.dz;
+  m.nx = (int)c.nx;
+  m.ny = (int)c.ny;
+  m.shape = c.shape;
+  m.rho = r->inlet_rho;
+  m.status = r->d_status;
+  CUDA_TRY(cudaMemsetAsync(r->inlet_rho, 0, (size_t)(c.nx + 1) * (c.ny + 1) * sizeof(double),
+                           r->stream));
+  TRY(launch(r, kInletCharge, inlet_charge_kernel, dim3(blocks_for(m.np + m.pcount, 128)),
+             dim3(128), m));
+  InletCompleteArgs ca{};
+  ca.g = make_grid<double>(r);
+  ca.rho = r->inlet_rho;
+  ca.cx = (int)c.cpml_cells_x;
+  ca.cy = (int)c.cpml_cells_y;
+  ca.status = r->d_status;
+  return launch(r, kInletComplete, inlet_complete_kernel,
+                dim3(blocks_for(c.nx + 1, 32), blocks_for(c.ny + 1, 8)), dim3(32, 8), ca);
+}
+
 // `defer_check`: leave the device status to the next read (the stepping loop
 // reads it with the next trial's residual and once at its end).
 aprl_status do_shift(aprl_run* r, bool defer_check = false) {
@@ -1330,6 +1396,7 @@ aprl_status do_shift(aprl_run* r, bool defer_check = false) {
     r->zb_b[a] = (r->zb_b[a] + nzb - 1) % nzb;
   }
   TRY(shift_insert_t<double>(r));
+  if (c.inlet_charge_match) TRY(inlet_charge_match(r));
   if (r->ledger_on) TRY(ledger_shift(r));
   r->origin[2] = std::fma(static_cast<double>(r->offset), c.dz, c.reference_origin[2]);
   if (r->np)
@@ -1501,6 +1568,9 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
   if ((s = device_alloc(&r->scan_total, 1)) != APRL_OK) return cleanup(s);
   cudaMemsetAsync(r->d_status, 0, sizeof(DeviceStatus), r->stream);
   if ((s = device_alloc(&r->d_stop, 1)) != APRL_OK) return cleanup(s);
+  if (c.inlet_charge_match &&
+      (s = device_alloc(&r->inlet_rho, (size_t)(c.nx + 1) * (c.ny + 1))) != APRL_OK)
+    return cleanup(s);
   if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums_slots),
                      kTrialSlots * sizeof(ResidualSums)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_status), sizeof(DeviceStatus)) != cudaSuccess ||
@@ -1581,6 +1651,7 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   cudaFreeHost(r->h_sums_slots);
   cudaFreeHost(r->h_stop);
   cudaFree(r->d_stop);
+  cudaFree(r->inlet_rho);
   cudaFreeHost(r->h_status);
   cudaFreeHost(r->h_counters_slots);
   cudaFreeHost(r->h_total);

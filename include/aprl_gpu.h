@@ -133,7 +133,13 @@ typedef struct {
   uint64_t maximum_step;          /* pending-queue horizon (PendingWindowGeometry) */
   /* prescribed lab magnets (SIFieldSourceSet::addPrescribedLabMagnet) */
   uint32_t n_magnets;
-  uint32_t reserved1;
+  /* mesh.moving_window.inlet_charge_match (src/config.cpp:711, 1152-1153;
+   * off by default): complete Ez of each inserted inlet layer from the
+   * discrete Gauss law of the incoming charge (ChargeMatchedInlet,
+   * src/charge_matched_inlet.h:17-72) and extend its departure from the
+   * reference oddly across the inlet for the Cowan magnetic update
+   * (src/moving_window_fields.cpp:225-236). */
+  uint32_t inlet_charge_match;
   aprl_magnet magnets[APRL_MAX_MAGNETS];
 } aprl_run_config;
 

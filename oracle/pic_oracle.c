@@ -791,6 +791,10 @@ static aprl_status validate_config(const aprl_run_config* g) {
   if (g->shape != APRL_SHAPE_LINEAR_BINOMIAL3 && g->shape != APRL_SHAPE_QUINTIC_COMPENSATED)
     return fail(APRL_ERR_INVALID_ARGUMENT,
                 "APRL 2.1 longitudinal_shape must be linear-binomial3 or quintic-compensated");
+  /* ChargeMatchedInlet's constructor (src/charge_matched_inlet.h:21-27). */
+  if (g->inlet_charge_match &&
+      (g->cpml_cells_x + 1 >= g->nx - g->cpml_cells_x || g->cpml_cells_y + 1 >= g->ny - g->cpml_cells_y))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Charge-matched inlet needs an interior physical aperture");
   if (g->substeps < 1 || g->max_trials < 1 || g->max_trials > 64)
     return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid substep or trial count");
   if (!(g->boost_gamma >= 1.0) || !isfinite(g->boost_gamma))
@@ -1529,6 +1533,18 @@ aprl_status oracle_run_advance_magnetic(oracle_run* r) {
         aprl_status s = reference_value(r, a, i, j, r->offset - 1, r->step, &v);
         if (s != APRL_OK) return s;
         r->lower[a][j * c->nx + i] = v;
+      }
+  }
+  /* With the charge-matched inlet, Ez's departure from the reference at the
+   * inlet is extended oddly across it (src/moving_window_fields.cpp:225-236). */
+  if (r->cfg.inlet_charge_match) {
+    const comp_t* ez = &r->f[2];
+    for (size_t j = r->cfg.cpml_cells_y + 1; j < r->cfg.ny - r->cfg.cpml_cells_y; ++j)
+      for (size_t i = r->cfg.cpml_cells_x + 1; i < r->cfg.nx - r->cfg.cpml_cells_x; ++i) {
+        double v;
+        aprl_status s = reference_value(r, 2, i, j, r->offset, r->step, &v);
+        if (s != APRL_OK) return s;
+        r->lower[2][j * ez->nx + i] -= AT(ez, i, j, 0) - v;
       }
   }
   advance_magnetic_cowan(r);
@@ -2396,6 +2412,84 @@ static aprl_status pending_admit(oracle_run* r) {
   return APRL_OK;
 }
 
+/* ChargeMatchedInlet::particle (src/charge_matched_inlet.h:31-53): one
+ * particle's share of the inlet-layer charge at node plane 1, with the wide
+ * longitudinal node weight of the run's shape and, for linear-binomial3, the
+ * transverse three-point x weights. */
+static aprl_status charge_match_particle(const oracle_run* r, const double origin[3],
+                                         const particle_t* p, double* rho) {
+  const aprl_run_config* g = &r->cfg;
+  const int binomial3 = g->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+  const double z = (p->pos[2] - origin[2]) / g->dz;
+  const basis_t bz = shape_basis(z, 0, g->shape);
+  const double wz = 1 < bz.first || 1 >= bz.first + (long long)bz.count ? 0. : bz.v[1 - bz.first];
+  if (wz == 0.) return APRL_OK;
+  const double x = (p->pos[0] - origin[0]) / g->dx, y = (p->pos[1] - origin[1]) / g->dy;
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z) || !isfinite(p->q))
+    return fail(APRL_ERR_RUNTIME, "Nonfinite charge-matched inlet source");
+  if (y < 0. || y > (double)g->ny) return APRL_OK;
+  if (binomial3 ? (x <= -2. || x >= (double)g->nx + 2.) : (x < 0. || x > (double)g->nx))
+    return APRL_OK;
+  const long long ix = (long long)floor(x);
+  const size_t j = (size_t)floor(y);
+  const double fx = x - ix, fy = y - j, scale = p->q * (1. / (g->dx * g->dy * g->dz));
+  double wx[4] = {1. - fx, fx, 0., 0.};
+  if (binomial3) node_weights(fx, wx);
+  const unsigned n_x = binomial3 ? 4 : 2;
+  const long long first = ix - (binomial3 ? 1 : 0);
+  for (unsigned b = 0; b < 2; ++b)
+    for (unsigned a = 0; a < n_x; ++a) {
+      const long long i = first + a;
+      if (i >= 0 && i <= (long long)g->nx && j + b <= g->ny)
+        rho[(j + b) * (g->nx + 1) + (size_t)i] += scale * wx[a] * (b ? fy : 1. - fy) * wz;
+    }
+  return APRL_OK;
+}
+
+/* Simulation::completeMovingInletLayer (src/simulation_moving_window.cpp:312-318)
+ * with ChargeMatchedInlet::complete (src/charge_matched_inlet.h:55-71): the
+ * stored particles and the pending ones due within 8 steps (visitNear), then
+ * Ez of the inserted layer from the discrete Gauss law, in long double. */
+static aprl_status inlet_charge_match(oracle_run* r) {
+  const aprl_run_config* g = &r->cfg;
+  const double origin[3] = {g->reference_origin[0], g->reference_origin[1],
+                            fma((double)r->offset, g->dz, g->reference_origin[2])};
+  double* rho = (double*)calloc((g->nx + 1) * (g->ny + 1), sizeof(double));
+  aprl_status s = APRL_OK;
+  for (size_t n = 0; n < r->np && s == APRL_OK; ++n)
+    s = charge_match_particle(r, origin, &r->p[n], rho);
+  const pending_t* q = &r->pending;
+  if (s == APRL_OK && q->extracted) {
+    const uint64_t step = r->step, room = q->maximum_step - step;
+    const uint64_t until = step + (8 < room ? 8 : room);
+    const size_t end = q->offsets[until - q->initial_step + 1];
+    for (size_t n = q->cursor; n < end && s == APRL_OK; ++n) {
+      particle_t p = q->p[q->order[n]];
+      p.pos[2] = repeat_held_addition(p.pos[2], held_increment(r, &p), step - q->initial_step);
+      s = charge_match_particle(r, origin, &p, rho);
+    }
+  }
+  if (s != APRL_OK) {
+    free(rho);
+    return s;
+  }
+  comp_t *ex = &r->f[0], *ey = &r->f[1], *ez = &r->f[2];
+  for (size_t j = g->cpml_cells_y + 1; j < g->ny - g->cpml_cells_y; ++j)
+    for (size_t i = g->cpml_cells_x + 1; i < g->nx - g->cpml_cells_x; ++i) {
+      const long double divxy = ((long double)AT(ex, i, j, 1) - AT(ex, i - 1, j, 1)) / g->dx +
+                                ((long double)AT(ey, i, j, 1) - AT(ey, i, j - 1, 1)) / g->dy;
+      const long double q_node = rho[j * (g->nx + 1) + i], retained = AT(ez, i, j, 1);
+      const double value = (double)(retained + g->dz * (divxy - q_node / SI_EPSILON0));
+      if (!isfinite(value)) {
+        free(rho);
+        return fail(APRL_ERR_RUNTIME, "Nonfinite charge-matched inlet field");
+      }
+      AT(ez, i, j, 0) = value;
+    }
+  free(rho);
+  return APRL_OK;
+}
+
 /* Frozen source support of the pending particles due within 8 steps
  * (visitNear + depositFrozenSourceSupport, src/simulation.cpp:4170-4172). */
 static aprl_status pending_support(oracle_run* r) {
@@ -2755,6 +2849,10 @@ aprl_status oracle_run_shift(oracle_run* r) {
       memmove(base + row, base, (layers - 1) * row * sizeof(double));
       memset(base, 0, row * sizeof(double));
     }
+  }
+  if (g->inlet_charge_match) {
+    aprl_status s = inlet_charge_match(r);
+    if (s != APRL_OK) return s;
   }
   /* Remap energy of the shift at one rank (src/moving_window_fields.cpp:500-515). */
   if (r->ledger) {

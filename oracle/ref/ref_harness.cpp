@@ -31,6 +31,7 @@
 
 #include "aprl_gpu.h"
 #include "boostframe.h"
+#include "charge_matched_inlet.h"
 #include "compute_threads.h"
 #include "eb_cpml.h"
 #include "eb_deposition.h"
@@ -103,6 +104,7 @@ struct ref_run {
   std::unique_ptr<PendingParticleQueue> pending;
   unsigned long long admitted = 0, activations = 0, savedActivations = 0;
   bool ledger = false;
+  std::unique_ptr<ChargeMatchedInlet> inlet;
 };
 
 namespace {
@@ -119,6 +121,23 @@ Double referenceValue(void* context, unsigned a, std::size_t i, std::size_t j,
   const auto& s = r.referenceShape[a];
   const double f = z - lo, lower = r.reference[a].at((lo * s[1] + j) * s[0] + i);
   return f == 0. ? lower : (1. - f) * lower + f * r.reference[a].at((hi * s[1] + j) * s[0] + i);
+}
+
+// Simulation::completeMovingInletLayer (src/simulation_moving_window.cpp:312-323)
+// without its ledger file: the charge-matched Ez of the inserted inlet layer.
+void completeInletLayer(void* context, EBFieldGrid& f, std::size_t step, std::ptrdiff_t offset) {
+  ref_run& r = *static_cast<ref_run*>(context);
+  Vec origin(0.);
+  origin[0] = r.cfg.reference_origin[0];
+  origin[1] = r.cfg.reference_origin[1];
+  origin[2] = std::fma(static_cast<double>(offset), f.geometry().dz, r.cfg.reference_origin[2]);
+  r.inlet->begin(origin);
+  for (const auto& p : r.particles) r.inlet->particle(p);
+  if (r.pending) {
+    const auto visit = [&](const RelativisticParticleSI& p) { r.inlet->particle(p); };
+    r.pending->visitNear(step, 8, visit);
+  }
+  r.inlet->complete(f, false);
 }
 
 YeeComponent& component(EBFieldGrid& f, unsigned a) {
@@ -401,6 +420,13 @@ aprl_status ref_run_create(const aprl_run_config* config, ref_run** out) {
     reference.value = &referenceValue;
     r.window.reset(new MovingWindowFields(r.geometry, config->nz, 0, MPI_COMM_WORLD, r.cpml, reference));
     r.window->installBoundary(*r.fields);
+    if (config->inlet_charge_match) {
+      // Simulation::initializeMovingWindow (src/simulation_moving_window.cpp:300-303)
+      const bool binomial3 = config->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+      r.inlet.reset(new ChargeMatchedInlet(r.geometry, config->cpml_cells_x, config->cpml_cells_y,
+                                           !binomial3, false, binomial3, binomial3));
+      r.window->setNewLayerCompletion(&completeInletLayer, &r, true);
+    }
     char pattern[] = "/tmp/aprl_ref_XXXXXX";
     const char* dir = mkdtemp(pattern);
     if (!dir) throw std::runtime_error("Cannot create coupling log directory");

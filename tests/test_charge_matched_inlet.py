@@ -1,0 +1,113 @@
+"""The charge-matched inlet (mesh.moving_window.inlet_charge_match; off by
+default in the reference, src/config.cpp:711).
+
+After each shift, Ez of the inserted inlet layer is completed from the
+discrete Gauss law of the incoming charge and the retained fields
+(ChargeMatchedInlet, src/charge_matched_inlet.h:17-72, driven by
+Simulation::completeMovingInletLayer, src/simulation_moving_window.cpp:312-318),
+and at each step's begin the lower Ez halo carries Ez's departure from the
+reference oddly across the inlet (src/moving_window_fields.cpp:225-236).
+The oracle restates both and is pinned bit for bit to the reference's own
+ChargeMatchedInlet and MovingWindowFields (the harness registers the same
+completion hook as Simulation).  The GPU sums the inlet-layer charge with
+FP64 atomics and the Gauss completion in double-double (the reference: long
+double), so it must follow the oracle to the parity bound of the step.
+"""
+import numpy as np
+import pytest
+
+import checkers
+from aprl_b200 import abi, native, workloads
+
+RTOL = 1e-12
+SHAPES = ["linear-binomial3", "quintic-compensated"]
+
+
+def matched(w):
+    w.config.inlet_charge_match = 1
+    return w
+
+
+def fields(run):
+    return [run.get_field(a) for a in range(6)]
+
+
+@pytest.mark.skipif(not checkers.reference_available(),
+                    reason="reference translation units not built")
+@pytest.mark.parametrize("shape", SHAPES)
+def test_oracle_matches_reference_bitwise(shape):
+    w = matched(workloads.small_case(steps=4, shape=shape))
+    o = checkers.run(checkers.oracle(), w)
+    r = checkers.run(checkers.reference(), w)
+    for _ in range(4):
+        o.step(1)
+        r.step(1)
+        for x, y in zip(fields(o), fields(r)):
+            np.testing.assert_array_equal(x, y)
+        po, pr = o.get_particles(), r.get_particles()
+        for k in po:
+            np.testing.assert_array_equal(po[k], pr[k])
+
+
+@pytest.mark.skipif(not checkers.reference_available(),
+                    reason="reference translation units not built")
+def test_oracle_matches_reference_with_held_injection():
+    w = matched(workloads.streaming_case(shape="linear-binomial3", steps=12))
+    o = checkers.run(checkers.oracle(), w)
+    r = checkers.run(checkers.reference(), w)
+    for _ in range(w.steps):
+        o.step(1)
+        r.step(1)
+        for x, y in zip(fields(o), fields(r)):
+            np.testing.assert_array_equal(x, y)
+    assert o.stats()["admitted"] > 0
+
+
+def test_completion_changes_the_inlet_layer_only_through_ez():
+    w = workloads.small_case(steps=2)
+    plain = checkers.run(checkers.oracle(), w)
+    m = checkers.run(checkers.oracle(), matched(workloads.small_case(steps=2)))
+    plain.step(1)
+    m.step(1)
+    ez_plain, ez_matched = plain.get_field(2), m.get_field(2)
+    assert np.abs(ez_plain[0] - ez_matched[0]).max() > 0.0
+
+
+def test_aperture_without_interior_is_rejected():
+    cfg = workloads.make_config(9, 16, 20, 5e-6, 5e-6, 2e-6, 4, 10.0, "linear-binomial3", 2)
+    cfg.inlet_charge_match = 1
+    with pytest.raises(native.AprlError, match="interior physical aperture"):
+        native.Run(checkers.oracle(), cfg)
+
+
+def compare(g, o):
+    for a, (x, y) in enumerate(zip(fields(g), fields(o))):
+        assert checkers.max_relative(x, y) <= RTOL, f"field {a}"
+    pg, po = g.get_particles(), o.get_particles()
+    np.testing.assert_array_equal(pg["id"], po["id"])
+    for k in ("x", "y", "z", "ux", "uy", "uz"):
+        assert checkers.max_relative(pg[k], po[k]) <= RTOL, k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", SHAPES)
+def test_gpu_matches_oracle(shape):
+    w = matched(workloads.small_case(steps=4, shape=shape))
+    g = native.Run(native.load(), w.config).load_workload(w)
+    o = checkers.run(checkers.oracle(), w)
+    for _ in range(4):
+        g.step(1)
+        o.step(1)
+        compare(g, o)
+
+
+@pytest.mark.gpu
+def test_gpu_matches_oracle_with_held_injection():
+    w = matched(workloads.streaming_case(shape="linear-binomial3", steps=12))
+    g = native.Run(native.load(), w.config).load_workload(w)
+    o = checkers.run(checkers.oracle(), w)
+    for _ in range(w.steps):
+        g.step(1)
+        o.step(1)
+    compare(g, o)
+    assert g.stats()["admitted"] == o.stats()["admitted"] > 0
