@@ -2058,7 +2058,9 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
     // The first trials are issued without waiting: after each one a device
     // verdict applies the stopping rule, and the kernels of the trials after
     // a converged one return at once.  One round trip then reads them all.
-    const unsigned ahead = std::min<unsigned>(kTrialSlots, r->cfg.max_trials);
+    // (three at FP64, where steps take three; two in the FP32-mixed mode,
+    // whose looser tolerances stop at the minimum two)
+    const unsigned ahead = std::min<unsigned>(r->fp32 ? 2u : kTrialSlots, r->cfg.max_trials);
     CUDA_TRY(cudaMemsetAsync(r->d_stop, 0, sizeof(int), r->stream));
     for (unsigned t = 0; t < ahead; ++t) TRY(enqueue_trial(r, (int)t, true));
     CUDA_TRY(cudaMemcpyAsync(r->h_stop, r->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
