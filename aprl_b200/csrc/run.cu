@@ -2482,8 +2482,10 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
       if (!(minimum > 64.0 * DBL_EPSILON))
         return fail(APRL_ERR_RUNTIME,
                     "Initial Cowan-Poisson operator fails the sufficient positive-definiteness "
-                    "bound on axis %d: minimum smoothing symbol=%.12g",
-                    axis, minimum);
+                    "bound on axis %d: minimum smoothing symbol%s=%.12g; choose boost_gamma "
+                    "closer to the bunch mean gamma or a grid aspect ratio with positive Cowan "
+                    "symbols",
+                    axis, axis == 2 ? " minus v^2*epsilon0*mu0" : "", minimum);
       const double inverse2 = 1.0 / (spacing[axis] * spacing[axis]);
       for (int a = -1; a <= 1; ++a)
         for (int b = -1; b <= 1; ++b) {

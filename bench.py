@@ -61,12 +61,20 @@ def parse_args(argv=None):
     p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--scan-slots", type=int, default=4)
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    p.add_argument("--initial-self-field", choices=["auto", "on", "off"], default="auto",
+                   help="start from the Cowan initial self-field (auto: on for the undulator "
+                        "workload; the dipole and drift bunches, beta_z ~ 1 in the box, are "
+                        "rejected by the reference's own initializer)")
     p.add_argument("--no-self-field", action="store_true",
                    help="skip the timing of the initial self-field solve")
     p.add_argument("--energy-ledger", choices=["auto", "on", "off"], default="auto",
                    help="keep the moving-window energy ledger during the timed steps "
                         "(auto: on for the undulator workload)")
     args = p.parse_args(argv)
+    if args.initial_self_field == "auto":
+        args.initial_self_field = args.workload == "undulator"
+    else:
+        args.initial_self_field = args.initial_self_field == "on"
     if args.energy_ledger == "auto":
         args.energy_ledger = args.workload == "undulator"
     else:
@@ -263,6 +271,12 @@ def run_ours(args):
     run = native.Run(lib, cfg, stream=stream.cuda_stream)
     run.set_reference(w.reference)
     run.set_particles(w.particles)
+    initial_fields = "zero"
+    if args.initial_self_field:
+        report = run.initialize_self_field(abi.self_field_config(
+            cfg, hold_transverse_until_activation=True))
+        initial_fields = (f"cowan-relativistic-poisson self-field ({report['iterations']} CG "
+                          f"iterations, beta_z {report['mean_beta_z']:.3f})")
     if args.energy_ledger:
         run.enable_energy_ledger()
 
@@ -395,6 +409,7 @@ def run_ours(args):
                    "magnet": magnet,
                    "boost_gamma": cfg.boost_gamma, "parallelism": f"replicas{world}",
                    "energy_ledger": bool(args.energy_ledger),
+                   "initial_fields": initial_fields,
                    "l2": "inputs larger than L2 (fields + particles > 126 MB)"},
         "fixed_point_trials": {"mean": stats["total_iterations"] / max(K, 1),
                                "max": stats["max_iterations"]},

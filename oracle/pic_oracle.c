@@ -3170,8 +3170,10 @@ static aprl_status sf_cowan_stencil(const oracle_run* r, double beta_z, double* 
     if (!(minimum > 64.0 * DBL_EPSILON))
       return fail(APRL_ERR_RUNTIME,
                   "Initial Cowan-Poisson operator fails the sufficient positive-definiteness "
-                  "bound on axis %u: minimum smoothing symbol=%.12g",
-                  axis, minimum);
+                  "bound on axis %u: minimum smoothing symbol%s=%.12g; choose boost_gamma "
+                  "closer to the bunch mean gamma or a grid aspect ratio with positive Cowan "
+                  "symbols",
+                  axis, axis == 2 ? " minus v^2*epsilon0*mu0" : "", minimum);
     const double inverse2 = 1.0 / (spacing[axis] * spacing[axis]);
     for (int a = -1; a <= 1; ++a)
       for (int b = -1; b <= 1; ++b) {

@@ -110,3 +110,23 @@ def test_gpu_reports_charge_touching_the_boundary():
     run = checkers.run(native.load(), w)
     with pytest.raises(native.AprlError, match="touches the static zero-potential"):
         run.initialize_self_field(abi.self_field_config(w.config))
+
+
+def test_oracle_rejects_the_relativistic_bunch_like_the_reference():
+    """A 1 GeV bunch boosted to gamma 10 moves at beta_z ~ 1 in the box: the
+    Cowan operator fails its positive-definiteness bound on z, in the
+    reference and the oracle alike, with the reference's message."""
+    cfg = workloads.make_config(32, 32, 64, 5e-6, 5e-6, 2e-6, 10, 10.0, "linear-binomial3", 4,
+                                magnets=[])
+    bunch = workloads.gaussian_bunch(cfg, 500, 100e-12, 1e9, 50e-6, 20e-6, 1e-6, 1e-4, seed=17,
+                                     margin_cells=2)
+    w = workloads.Workload("relativistic", cfg, bunch, workloads.synthetic_reference(cfg), [],
+                           steps=4)
+    messages = []
+    bindings = [checkers.oracle()] + ([checkers.reference()] if checkers.reference_available()
+                                      else [])
+    for binding in bindings:
+        with pytest.raises(native.AprlError, match="positive-definiteness bound on axis 2") as e:
+            solve(binding, w)
+        messages.append(str(e.value).split(": ", 1)[1])
+    assert len(set(messages)) == 1
