@@ -152,6 +152,99 @@ __device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double 
   }
 }
 
+// quintic_segment for a deposit: every Gauss point of a cut piece lies in
+// the same cell, so the 4 x 92 node visits fall on 92 nodes; each node's four
+// weights are summed first and visited once (a quarter of the atomics).  The
+// weights are quintic_segment's; only their summation order changes.  Per
+// component and transverse corner the Gauss points' bases are recomputed,
+// which keeps the accumulators to one z column (12 values).  A piece whose
+// Gauss points straddle a cell (only possible through rounding at a cut) is
+// visited point by point.
+template <class G, class V>
+__device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const double x[3],
+                                                       const double v[3], double lower,
+                                                       double upper, double width, V& visit) {
+  using F = typename V::Weight;
+  const double q[4] = {-.8611363115940525752, -.3399810435848562648,
+                       .3399810435848562648, .8611363115940525752};
+  const double qw[4] = {.3478548451374538574, .6521451548625461426,
+                        .6521451548625461426, .3478548451374538574};
+  double zz[4];
+  F factor[4], fx[4], fy[4];
+  long long i = 0, j = 0, kz = 0;
+  bool same = true;
+  for (int t = 0; t < 4; ++t) {
+    const double u = .5 * (upper + lower + width * q[t]), xx = x[0] + u * v[0],
+                 yy = x[1] + u * v[1];
+    zz[t] = x[2] + u * v[2];
+    factor[t] = F(.5 * width * qw[t]);
+    long long it = (long long)floor(xx), jt = (long long)floor(yy);
+    if (it == (long long)g.nx) --it;
+    if (jt == (long long)g.ny) --jt;
+    const long long kt = (long long)floor(zz[t]);
+    fx[t] = F(xx - it);
+    fy[t] = F(yy - jt);
+    if (t == 0) {
+      i = it;
+      j = jt;
+      kz = kt;
+    } else if (it != i || jt != j || kt != kz) {
+      same = false;
+    }
+  }
+  if (!same) {
+    quintic_segment(g, x, v, lower, upper, width, visit);
+    return;
+  }
+  Basis<F> b;
+  // Jx at (i, j + c) and Jy at (i + c, j): node basis, 12 nodes.
+  for (int axis = 0; axis < 2; ++axis)
+    for (int c = 0; c < 2; ++c) {
+      F acc[12];
+      unsigned hit = 0;
+      long long first = 0;
+      for (int k = 0; k < 12; ++k) acc[k] = F(0.);
+      for (int t = 0; t < 4; ++t) {
+        quintic_basis(zz[t], false, b);
+        first = b.first;
+        const F side = axis == 0 ? (c ? fy[t] : F(1.) - fy[t]) : (c ? fx[t] : F(1.) - fx[t]);
+        for (int k = 0; k < b.count; ++k) {
+          const F w = factor[t] * b.v[k];
+          if (w == F(0.)) continue;
+          acc[k] += w * side;
+          hit |= 1u << k;
+        }
+      }
+      for (int k = 0; k < 12; ++k)
+        if (hit & (1u << k)) {
+          if (axis == 0)
+            visit(0, i, j + c, first + k, acc[k]);
+          else
+            visit(1, i + c, j, first + k, acc[k]);
+        }
+    }
+  // Jz at (i + a, j + c): edge basis, 11 nodes.
+  for (int c = 0; c < 2; ++c)
+    for (int a = 0; a < 2; ++a) {
+      F acc[12];
+      unsigned hit = 0;
+      long long first = 0;
+      for (int k = 0; k < 12; ++k) acc[k] = F(0.);
+      for (int t = 0; t < 4; ++t) {
+        quintic_basis(zz[t], true, b);
+        first = b.first;
+        for (int k = 0; k < b.count; ++k) {
+          const F w = factor[t] * b.v[k];
+          if (w == F(0.)) continue;
+          acc[k] += w * (a ? fx[t] : F(1.) - fx[t]) * (c ? fy[t] : F(1.) - fy[t]);
+          hit |= 1u << k;
+        }
+      }
+      for (int k = 0; k < 12; ++k)
+        if (hit & (1u << k)) visit(2, i + a, j + c, first + k, acc[k]);
+    }
+}
+
 // longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
 // smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
 // when the chord exceeds the 64-cut crossing budget.
@@ -205,7 +298,10 @@ __device__ int shape_weights(const GridT<F>& g, int shape, const double begin[3]
         else
           binomial_xz_segment(g, x, v, piece_lower, upper, visit);
       } else {
-        quintic_segment(g, x, v, piece_lower, upper, width, visit);
+        if constexpr (V::kQuinticSummed)
+          quintic_segment_summed(g, x, v, piece_lower, upper, width, visit);
+        else
+          quintic_segment(g, x, v, piece_lower, upper, width, visit);
       }
     }
     if (axis < 0) break;
@@ -275,6 +371,7 @@ struct Ptr3 {
 template <class W, class F>
 struct ElectricVisitor {
   static constexpr bool kF3Segment = true;
+  static constexpr bool kQuinticSummed = false;  // gathers keep the reference's visit order
   using Weight = W;
   const GridT<F>* g;
   Ptr3<W> s;             // orbit sum S = E_new + E^n per E node (ring layout)
@@ -503,6 +600,7 @@ __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape
 template <class F>
 struct DepositVisitor {
   static constexpr bool kF3Segment = false;
+  static constexpr bool kQuinticSummed = true;
   using Weight = F;
   const GridT<F>* g;
   F scale[3];
