@@ -6,8 +6,10 @@
 //
 // One thread owns one particle; its gathers and weights run in the
 // reference's visit order, so in FP64 (no FMA contraction) the per-particle
-// arithmetic matches the reference.  Deposition accumulates with atomics into
-// J; only the summation order of J differs from the reference.
+// arithmetic matches the reference, except that the quintic shape's four
+// Gauss points of a cut piece are summed per node before the gather's read
+// and the deposit's atomic.  Deposition accumulates with atomics into J; the
+// summation order of J differs from the reference.
 //
 // The walkers are templated on the type F of J and of the weight
 // arithmetic.  Positions, chord cuts and cell indices are always binary64,
@@ -371,7 +373,12 @@ struct Ptr3 {
 template <class W, class F>
 struct ElectricVisitor {
   static constexpr bool kF3Segment = true;
-  static constexpr bool kQuinticSummed = false;  // gathers keep the reference's visit order
+  // Quintic pieces arrive with each node's four Gauss-point weights summed:
+  // the gather is linear in the weights, so this reads each S node once
+  // instead of four times; the per-particle sum then differs from the
+  // reference's point-by-point order in the last bits (binomial3 pieces keep
+  // the reference's order exactly).
+  static constexpr bool kQuinticSummed = true;
   using Weight = W;
   const GridT<F>* g;
   Ptr3<W> s;             // orbit sum S = E_new + E^n per E node (ring layout)
