@@ -1099,7 +1099,7 @@ __device__ __forceinline__ SlotPlan plan_slot(const GridT<F>& g, const DFrame& f
 // before any current of the trial is deposited; the push reads them as the
 // previous residual's fields.
 template <class W, class F>
-__global__ void guess_gather_kernel(PushArgs<F> a) {
+__global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
   const double start[3] = {a.p.x[n], a.p.y[n], a.p.z[n]};

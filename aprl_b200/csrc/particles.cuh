@@ -149,13 +149,27 @@ struct ResidualArgs {
   DeviceStatus* status;
 };
 
-// Occupancy knobs of the two hot particle kernels (blocks of 128 threads
+// Occupancy knobs of the hot particle kernels (blocks of 128 threads
 // that must fit one SM; 0 leaves the register count to the compiler).
+// Measured on the 128x128x512 dipole grid with 1M particles: push_deposit at
+// 8 blocks (64 registers, with spills) beats 4, 10, 12 and 16 blocks on the
+// binomial3, quintic, FP32-mixed and drift workloads -- its FP64 reductions
+// want many warps in flight; guess_gather at 4 blocks (128 registers) takes
+// 0.28 ms against 0.33 ms unbounded (240 registers); the residual stays at 4
+// (6 and 8 spill more and are no faster).
 #ifndef APRL_PUSH_MIN_BLOCKS
-#define APRL_PUSH_MIN_BLOCKS 4
+#define APRL_PUSH_MIN_BLOCKS 8
 #endif
 #ifndef APRL_RESIDUAL_MIN_BLOCKS
 #define APRL_RESIDUAL_MIN_BLOCKS 4
+#endif
+#ifndef APRL_GATHER_MIN_BLOCKS
+#define APRL_GATHER_MIN_BLOCKS 4
+#endif
+#if APRL_GATHER_MIN_BLOCKS > 0
+#define APRL_GATHER_BOUNDS __launch_bounds__(128, APRL_GATHER_MIN_BLOCKS)
+#else
+#define APRL_GATHER_BOUNDS
 #endif
 #if APRL_PUSH_MIN_BLOCKS > 0
 #define APRL_PUSH_BOUNDS __launch_bounds__(128, APRL_PUSH_MIN_BLOCKS)

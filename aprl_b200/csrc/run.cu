@@ -243,6 +243,11 @@ constexpr unsigned kTrialSlots = 3;
 struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
+  // The CPML carriers of a trial run on `side`, forked from `stream` after
+  // the trial's clear and joined before the orbit sum that reads J, so their
+  // short, latency-bound launch overlaps the particles' push.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   double coeff[12]{};
   // E, B and J are binary64 in both modes (`fes`: J element size); the
   // FP32-mixed mode runs the gathers in binary32.
@@ -363,6 +368,26 @@ void comp_shape(const aprl_run_config& g, unsigned a, size_t s[3]) {
   for (unsigned d = 0; d < 3; ++d) s[d] = cells[d] + (electric ? (d != axis) : (d == axis));
 }
 
+// True when every value is finite.  A binary64 is non-finite exactly when its
+// 11 exponent bits are all ones; adding one to that field then carries into
+// bit 11.  The branch-free OR over a chunk vectorises with plain SSE2
+// integer ops, so a host inlet plane is checked at memory speed rather than
+// one compare-and-branch per value.
+bool all_finite(const double* v, size_t n) {
+  constexpr size_t kChunk = 4096;
+  for (size_t lo = 0; lo < n; lo += kChunk) {
+    const size_t hi = std::min(n, lo + kChunk);
+    uint64_t bad = 0;
+    for (size_t i = lo; i < hi; ++i) {
+      uint64_t bits;
+      std::memcpy(&bits, v + i, 8);
+      bad |= (((bits >> 52) & 0x7ffu) + 1u) >> 11;
+    }
+    if (bad) return false;
+  }
+  return true;
+}
+
 cudaEvent_t take_event(aprl_run* r) {
   if (!r->event_pool.empty()) {
     cudaEvent_t e = r->event_pool.back();
@@ -387,26 +412,33 @@ aprl_status drain_timings(aprl_run* r) {
   return APRL_OK;
 }
 
-// Launch with optional stage timing on the run's stream.
+// Launch on `stream` with optional stage timing.
 template <class K, class... Args>
-aprl_status launch(aprl_run* r, unsigned id, K kernel, dim3 grid, dim3 block, Args... args) {
+aprl_status launch_on(aprl_run* r, cudaStream_t stream, unsigned id, K kernel, dim3 grid,
+                      dim3 block, Args... args) {
   if (grid.x == 0 || grid.y == 0 || grid.z == 0) return APRL_OK;
   Timing t{};
   if (r->profile) {
     t.start = take_event(r);
     t.stop = take_event(r);
     t.kernel = id;
-    CUDA_TRY(cudaEventRecord(t.start, r->stream));
+    CUDA_TRY(cudaEventRecord(t.start, stream));
   }
-  kernel<<<grid, block, 0, r->stream>>>(args...);
+  kernel<<<grid, block, 0, stream>>>(args...);
   CUDA_TRY(cudaGetLastError());
   if (r->profile) {
-    CUDA_TRY(cudaEventRecord(t.stop, r->stream));
+    CUDA_TRY(cudaEventRecord(t.stop, stream));
     r->pending.push_back(t);
   }
   ++r->kernel_launches[id];
   ++r->launches;
   return APRL_OK;
+}
+
+// Launch on the run's stream.
+template <class K, class... Args>
+aprl_status launch(aprl_run* r, unsigned id, K kernel, dim3 grid, dim3 block, Args... args) {
+  return launch_on(r, r->stream, id, kernel, grid, block, args...);
 }
 
 #define TRY(expr)                    \
@@ -668,9 +700,13 @@ aprl_status copy_carriers(DCarriers& dst, const DCarriers& src, size_t n) {
 
 // Carrier capacity.  The current list and the per-step outputs (c_out,
 // c_keep) of the `nc` existing carriers survive a reallocation.
+// The first reservation takes at least a sixteenth of the particle capacity
+// (and 4096), so that the carriers a bunch sheds into the CPML over its
+// first steps do not regrow the lists -- each regrowth is a stream sync plus
+// 27 cudaMalloc/cudaFree calls inside a step.
 aprl_status reserve_carriers(aprl_run* r, size_t n) {
   if (n <= r->ccap) return APRL_OK;
-  n = std::max(n, 2 * r->ccap);
+  n = std::max({n, 2 * r->ccap, std::max<size_t>(4096, r->pcap / 16)});
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   DCarriers nc{}, nout{};
   unsigned char* nkeep = nullptr;
@@ -1122,6 +1158,9 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
                  dim3(128), sa));
     }
   }
+  // Carriers share only J, the counters and the status word with the
+  // particle kernels, all through atomics, so they run beside them.
+  bool joined = true;
   if (r->nc) {
     CarrierArgs<F> ca{};
     ca.g = g;
@@ -1133,8 +1172,18 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ca.keep = r->c_keep;
     ca.counters = r->d_counters;
     ca.status = r->d_status;
-    TRY(launch(r, kCarrier, carrier_kernel<F>, dim3(blocks_for(r->nc, 128)), dim3(128), ca));
+    CUDA_TRY(cudaEventRecord(r->fork, r->stream));
+    CUDA_TRY(cudaStreamWaitEvent(r->side, r->fork, 0));
+    TRY(launch_on(r, r->side, kCarrier, carrier_kernel<F>, dim3(blocks_for(r->nc, 128)),
+                  dim3(128), ca));
+    CUDA_TRY(cudaEventRecord(r->join, r->side));
+    joined = false;
   }
+  auto join_carriers = [&]() -> aprl_status {
+    if (!joined) CUDA_TRY(cudaStreamWaitEvent(r->stream, r->join, 0));
+    joined = true;
+    return APRL_OK;
+  };
   if (r->np) {
     PushArgs<F> pa{};
     pa.g = g;
@@ -1194,6 +1243,7 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     }
     TRY(launch(r, kPushDeposit, push_deposit_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128),
                pa));
+    TRY(join_carriers());
     TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
                orbit[1], orbit[2], 1));
     ResidualArgs<F> ra{};
@@ -1216,6 +1266,7 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ra.status = r->d_status;
     TRY(launch(r, kResidual, residual_kernel<W, F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
+  TRY(join_carriers());
   if (ahead)
     TRY(launch(r, kTrialVerdict, trial_verdict_kernel, dim3(1), dim3(1),
                (const ResidualSums*)r->d_sums, r->trials + 1, c.force_tolerance,
@@ -1579,6 +1630,10 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
       cudaMallocHost(reinterpret_cast<void**>(&r->h_stop), sizeof(int)) != cudaSuccess ||
       cudaMallocHost(reinterpret_cast<void**>(&r->h_total), sizeof(unsigned long long)) != cudaSuccess)
     return cleanup(fail(APRL_ERR_CUDA, "cudaMallocHost failed"));
+  if (cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r->join, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup(fail(APRL_ERR_CUDA, "side stream creation failed"));
   r->h_sums = r->h_sums_slots;
   r->h_counters = r->h_counters_slots;
   r->offset = c.initial_offset;
@@ -1594,6 +1649,12 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
 aprl_status aprl_run_destroy(aprl_run* r) {
   if (!r) return APRL_OK;
   if (r->stream) cudaStreamSynchronize(r->stream); else cudaDeviceSynchronize();
+  if (r->side) {
+    cudaStreamSynchronize(r->side);
+    cudaStreamDestroy(r->side);
+  }
+  if (r->fork) cudaEventDestroy(r->fork);
+  if (r->join) cudaEventDestroy(r->join);
   for (auto& t : r->pending) {
     cudaEventDestroy(t.start);
     cudaEventDestroy(t.stop);
@@ -1665,9 +1726,7 @@ aprl_status aprl_run_set_reference(aprl_run* r, unsigned a, const double* host, 
   comp_shape(r->cfg, a, s);
   const size_t n = s[0] * s[1] * (r->cfg.reference_nz + ((a == 0 || a == 1 || a == 5) ? 1 : 0));
   if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
-  if (host)
-    for (size_t i = 0; i < n; ++i)
-      if (!std::isfinite(host[i])) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
+  if (host && !all_finite(host, n)) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   cudaFree(r->ref[a]);
   r->ref[a] = nullptr;
@@ -1690,8 +1749,8 @@ aprl_status aprl_run_set_reference_planes(aprl_run* r, unsigned a, uint64_t firs
   if (!host || first > layers || planes > layers - first)
     return fail(APRL_ERR_OUT_OF_RANGE, "Reference planes outside the prepared native field");
   const size_t plane = s[0] * s[1];
-  for (size_t i = 0; i < planes * plane; ++i)
-    if (!std::isfinite(host[i])) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
+  if (!all_finite(host, planes * plane))
+    return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
   CUDA_TRY(cudaMemcpyAsync(r->ref[a] + first * plane, host, planes * plane * 8,
                            cudaMemcpyHostToDevice, r->stream));
   return APRL_OK;
@@ -1770,6 +1829,7 @@ aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const
         !std::isfinite(q[i]) || !(m[i] > 0.0))
       return fail(APRL_ERR_INVALID_ARGUMENT, "Particle %zu has a non-finite state or nonpositive mass", i);
   TRY(reserve_particles(r, n));
+  TRY(reserve_carriers(r, 1));
   r->np = 0;
   const double* src[] = {x, y, z, ux, uy, uz, q, m};
   double* dst[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
@@ -2157,8 +2217,10 @@ aprl_status aprl_run_get_slot_fields(aprl_run* r, size_t capacity, double* used_
   return APRL_OK;
 }
 
-aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double* out, size_t count,
-                                        int* inside) {
+// The detector plane's kernel and its copy to `out`, in stream order; `wait`
+// returns only once the copy has landed.
+static aprl_status sample_plane(aprl_run* r, double plane_lab_z, double* out, size_t count,
+                                int* inside, bool wait) {
   if (!r || !out || !inside) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
   const aprl_run_config& c = r->cfg;
   if (count != 6 * c.nx * c.ny) return fail(APRL_ERR_INVALID_ARGUMENT, "Detector buffer size mismatch");
@@ -2194,8 +2256,18 @@ aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double*
   TRY(launch(r, kDetectorPlane, detector_plane_kernel<double>, grid, block,
              retyped<double>(da, make_grid<double>(r))));
   CUDA_TRY(cudaMemcpyAsync(out, r->d_detector, count * 8, cudaMemcpyDeviceToHost, r->stream));
-  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  if (wait) CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;
+}
+
+aprl_status aprl_run_sample_field_plane(aprl_run* r, double plane_lab_z, double* out, size_t count,
+                                        int* inside) {
+  return sample_plane(r, plane_lab_z, out, count, inside, true);
+}
+
+aprl_status aprl_run_sample_field_plane_async(aprl_run* r, double plane_lab_z, double* out,
+                                              size_t count, int* inside) {
+  return sample_plane(r, plane_lab_z, out, count, inside, false);
 }
 
 aprl_status aprl_run_enable_energy_ledger(aprl_run* r, int enabled) {

@@ -77,8 +77,10 @@ uint64_t footprint(const aprl_run_config& c, size_t particles) {
     bytes += plane * (c.reference_nz + 1) * 8;
   }
   // Particles (two state copies, trial outputs, slots, newborn carriers,
-  // sort scratch) and a carrier allowance of a quarter of the particles.
-  bytes += (uint64_t)particles * 480 + (uint64_t)(particles / 4 + 1024) * 3 * 80;
+  // sort scratch) and a carrier allowance of a quarter of the particles (at
+  // least the 4096 carriers a run reserves up front).
+  bytes += (uint64_t)particles * 480 +
+           (std::max<uint64_t>(particles / 4, 4096) + 1024) * 3 * 80;
   // Cell sort and scan scratch, reductions.
   bytes += (uint64_t)c.nx * c.ny * c.nz * 8 + (32ull << 20);
   return bytes;

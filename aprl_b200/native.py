@@ -70,6 +70,8 @@ _PRODUCT_ONLY = {
     "run_reset_iteration_stats": (C.c_int, [_H]),
     "run_sample_field_plane_noalloc": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
                                                  C.POINTER(C.c_int)]),
+    "run_sample_field_plane_async": (C.c_int, [_H, C.c_double, _D, C.c_size_t,
+                                               C.POINTER(C.c_int)]),
     "run_gauss_law": (C.c_int, [_H, C.POINTER(abi.GaussLaw), _D, C.c_size_t]),
     "run_prepare_reference": (C.c_int, [_H, C.c_size_t, _D, _D, _D, _D, _D, _D, _D, _D,
                                         C.POINTER(abi.SelfFieldConfig),
@@ -391,6 +393,20 @@ class Run:
         return out if inside.value else None
 
     # -- product-only ---------------------------------------------------
+    def sample_field_plane_async(self, lab_z, out):
+        """Queue the detector plane's copy into `out` (a C-contiguous
+        (ny, nx, 6) float64 array, best page-locked) and return whether the
+        plane is inside the window; `out` holds the values once the run's
+        stream has passed the copy (synchronize(), or the next step)."""
+        cfg = self.config
+        if out.shape != (cfg.ny, cfg.nx, 6) or out.dtype != np.float64 or \
+                not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("detector buffer must be a C-contiguous (ny, nx, 6) float64 array")
+        inside = C.c_int()
+        self.b("run_sample_field_plane_async", self.handle, lab_z, _ptr(out),
+               out.size, C.byref(inside))
+        return bool(inside.value)
+
     def synchronize(self):
         self.b("run_synchronize", self.handle)
 

@@ -268,22 +268,27 @@ def run_ours(args):
     w = make(total_steps, args, 17 + rank)
     cfg = w.config
     lib = native.load()
-    run = native.Run(lib, cfg, stream=stream.cuda_stream)
-    run.set_reference(w.reference)
-    run.set_particles(w.particles)
-    initial_fields = "zero"
-    if args.initial_self_field:
-        report = run.initialize_self_field(abi.self_field_config(
-            cfg, hold_transverse_until_activation=True))
-        initial_fields = (f"cowan-relativistic-poisson self-field ({report['iterations']} CG "
-                          f"iterations, beta_z {report['mean_beta_z']:.3f})")
-    if args.energy_ledger:
-        run.enable_energy_ledger()
 
-    for _ in range(W):
-        run.step(1)
-    run.synchronize()
-    run.b("run_reset_iteration_stats", run.handle)
+    def start_run():
+        """A run of the workload after its W warm-up steps."""
+        run = native.Run(lib, cfg, stream=stream.cuda_stream)
+        run.set_reference(w.reference)
+        run.set_particles(w.particles)
+        initial_fields = "zero"
+        if args.initial_self_field:
+            report = run.initialize_self_field(abi.self_field_config(
+                cfg, hold_transverse_until_activation=True))
+            initial_fields = (f"cowan-relativistic-poisson self-field ({report['iterations']} "
+                              f"CG iterations, beta_z {report['mean_beta_z']:.3f})")
+        if args.energy_ledger:
+            run.enable_energy_ledger()
+        for _ in range(W):
+            run.step(1)
+        run.synchronize()
+        run.b("run_reset_iteration_stats", run.handle)
+        return run, initial_fields
+
+    run, initial_fields = start_run()
 
     # ---- device-resident timed region ------------------------------------
     launches0 = run.launch_count()
@@ -309,37 +314,65 @@ def run_ours(args):
     stats = run.stats()
 
     # ---- end to end through the C ABI with host buffers -------------------
-    pinned = {}
-    for a in range(6):
-        nx_c, ny_c, _ = abi.reference_shape(cfg, a)
-        pinned[a] = torch.empty((4, ny_c, nx_c), dtype=torch.float64, pin_memory=True).numpy()
-    detector = torch.empty((cfg.ny, cfg.nx, 6), dtype=torch.float64, pin_memory=True).numpy()
+    # A second run of the same workload, from the same start and warm-up, so
+    # that both legs time the same K steps (the cost of a step changes as the
+    # run goes on, so steps W+K.. are not a like-for-like comparison).
+    run.close()
+    run, _ = start_run()
+    # The inlet reference table lives in pinned host memory (48 MB on the
+    # dipole grid); each step uploads the native planes that step's inlet
+    # queries touch.  Step k+1's planes are issued right after step k is
+    # enqueued, so their host-side finiteness check overlaps step k's tail;
+    # the copy is stream-ordered behind step k.  K steps, K uploads, all
+    # inside the timed region (the first one before the loop).
+    pinned_ref = []
+    for table in w.reference:
+        host = torch.empty(table.shape, dtype=torch.float64, pin_memory=True).numpy()
+        np.copyto(host, table)
+        pinned_ref.append(host)
+
+    def upload(step):
+        lo, hi = reference_planes_for_step(cfg, step)
+        sent = 0
+        for a in range(6):
+            planes = pinned_ref[a][lo:hi + 1]
+            run.set_reference_planes(a, lo, planes)
+            sent += planes.nbytes
+        return sent
+
+    # The detector plane of step k is queued without a wait into one of two
+    # page-locked buffers; step k+1's own trial read-back waits for the
+    # stream, so the plane is read on the host while step k+1's tail runs.
+    # The last plane is completed by the synchronize before the stop event.
+    detectors = [torch.empty((cfg.ny, cfg.nx, 6), dtype=torch.float64,
+                             pin_memory=True).numpy() for _ in range(2)]
     detector_lab_z = cfg.boost_gamma * (0.5 * cfg.nz * cfg.dz)
     e2e_particle_steps, h2d, d2h = 0, 0, 0
+    planes_read, planes_finite = 0, True
+    step0 = run.stats()["step"]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     wall0 = time.perf_counter()
     e_start.record(stream)
-    for _ in range(K):
-        step = run.stats()["step"]
-        lo, hi = reference_planes_for_step(cfg, step)
-        for a in range(6):
-            planes = w.reference[a][lo:hi + 1]
-            buf = pinned[a][:planes.shape[0]]
-            np.copyto(buf, planes)
-            run.set_reference_planes(a, lo, buf)
-            h2d += buf.nbytes
+    h2d += upload(step0)
+    inside = [False, False]
+    for i in range(K):
         e2e_particle_steps += run.particle_count()
         run.step(1)
-        out = np.empty(cfg.nx * cfg.ny * 6)
-        inside = __import__("ctypes").c_int()
-        run.b("run_sample_field_plane", run.handle, detector_lab_z,
-              detector.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)),
-              detector.size, __import__("ctypes").byref(inside))
-        d2h += detector.nbytes + 8 * 24  # plane + stats block
+        if i > 0 and inside[(i - 1) % 2]:
+            planes_finite &= bool(np.isfinite(detectors[(i - 1) % 2]).all())
+            planes_read += 1
+        inside[i % 2] = run.sample_field_plane_async(detector_lab_z, detectors[i % 2])
+        d2h += detectors[0].nbytes + 8 * 24  # plane + stats block
+        if i + 1 < K:
+            h2d += upload(step0 + i + 1)
         run.stats()
+    run.synchronize()
+    if inside[(K - 1) % 2]:
+        planes_finite &= bool(np.isfinite(detectors[(K - 1) % 2]).all())
+        planes_read += 1
     e_stop.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_stop)
@@ -417,7 +450,11 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": h2d // max(K, 1),
                 "d2h_bytes_per_step": d2h // max(K, 1),
-                "wall_ms_per_step": e2e_wall_ms / K},
+                "wall_ms_per_step": e2e_wall_ms / K,
+                "detector_planes_read": planes_read,
+                "detector_planes_finite": planes_finite,
+                "path": "aprl_run_set_reference_planes (pinned table), aprl_run_step, "
+                        "aprl_run_sample_field_plane_async (pinned, double-buffered)"},
         "gpu_launches": launches,
         "roofline": roofline,
         "atomic_roofline": atomic_roofline,

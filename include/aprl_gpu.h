@@ -327,6 +327,20 @@ aprl_status aprl_run_sample_field_plane(aprl_run* run, double plane_lab_z,
                                         double* out, size_t count,
                                         int* inside);
 
+/* aprl_run_sample_field_plane without the wait: the plane's kernel and its
+ * copy into `out` are queued on the run's stream and the call returns at
+ * once (*inside is set before it returns).  The values are in `out` once the
+ * stream has passed the copy: after aprl_run_synchronize, or after any later
+ * call on the run that waits for its stream -- aprl_run_step does, at each
+ * step's coupling-trial read-back.  So a stepping loop can read step n's plane
+ * while step n+1 runs.  `out` must stay valid, and unread, until then; it
+ * should be page-locked host memory (cudaHostAlloc), or the copy is staged
+ * and the call waits for it.  The reference writes each plane synchronously
+ * (src/lab_detectors.cpp:2426-2490); this call has no counterpart there. */
+aprl_status aprl_run_sample_field_plane_async(aprl_run* run, double plane_lab_z,
+                                              double* out, size_t count,
+                                              int* inside);
+
 /* Largest plane (count = 6*nx*ny values) that
  * aprl_run_sample_field_plane_noalloc accepts: 6*256*256 doubles, i.e. a
  * fixed 3 MiB device array that every GPU which loads this library keeps

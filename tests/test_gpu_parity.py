@@ -109,6 +109,30 @@ def test_detector_plane_matches_oracle():
     assert checkers.max_relative(dg, do) <= RTOL
 
 
+def test_async_detector_planes_complete_at_the_next_step():
+    """aprl_run_sample_field_plane_async into two page-locked buffers: step
+    n's plane, read after step n+1 returned (whose trial read-back waits for
+    the stream), equals the oracle's plane sampled right after step n."""
+    import torch
+    w = workloads.small_case(steps=5)
+    cfg = w.config
+    g, o = gpu_run(w), checkers.run(checkers.oracle(), w)
+    lab_z = cfg.boost_gamma * (0.5 * cfg.nz * cfg.dz)
+    buffers = [torch.empty((cfg.ny, cfg.nx, 6), dtype=torch.float64,
+                           pin_memory=True).numpy() for _ in range(2)]
+    expected = []
+    for n in range(4):
+        g.step(1)
+        o.step(1)
+        if n > 0:
+            assert checkers.max_relative(buffers[(n - 1) % 2], expected[n - 1]) <= RTOL, n
+        buffers[n % 2].fill(np.nan)
+        assert g.sample_field_plane_async(lab_z, buffers[n % 2])
+        expected.append(o.sample_field_plane(lab_z))
+    g.synchronize()
+    assert checkers.max_relative(buffers[1], expected[3]) <= RTOL
+
+
 @pytest.mark.parametrize("shape", ["linear-binomial3", "quintic-compensated"])
 def test_held_injection_matches_oracle(shape):
     """Held lab-plane injection: queue extraction, admission, frozen source
