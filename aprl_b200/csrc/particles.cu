@@ -250,9 +250,9 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
 // longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
 // smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
 // when the chord exceeds the 64-cut crossing budget.
-template <class F, class V>
-__device__ int shape_weights(const GridT<F>& g, int shape, const double begin[3],
-                             const double end[3], V& visit) {
+template <int S, class F, class V>
+__device__ int shape_weights(const GridT<F>& g, const double begin[3], const double end[3],
+                             V& visit) {
   const double h[3] = {g.dx, g.dy, g.dz};
   // The cell-boundary cuts of the chord, ascending.  Along each axis the cuts
   // (j - x)/v of the crossed lattice planes j are already monotone, so a
@@ -294,7 +294,7 @@ __device__ int shape_weights(const GridT<F>& g, int shape, const double begin[3]
     lower = upper;
     if (width > 0.) {
       ++segments;
-      if (shape == 0) {
+      if constexpr (S == 0) {
         if constexpr (V::kF3Segment)
           visit.f3_segment(g, x, v, piece_lower, upper);
         else
@@ -571,23 +571,23 @@ __device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const Ptr3
 }
 
 // Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
-template <class W, class F>
-__device__ __forceinline__ unsigned gather_electric(const GridT<F>& g, int shape,
+template <int S, class W, class F>
+__device__ __forceinline__ unsigned gather_electric(const GridT<F>& g,
                                                     const double a[3], const double b[3],
                                                     const Ptr3<W>& orbit, double out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
   ElectricVisitor<W, F> v{&g, orbit, {W(0.), W(0.), W(0.)}};
-  if (shape_weights(g, shape, path.begin, path.end, v) < 0) return kErrCrossingBudget;
+  if (shape_weights<S>(g, path.begin, path.end, v) < 0) return kErrCrossingBudget;
   const double fraction = path.last - path.first;
   for (int d = 0; d < 3; ++d) out[d] = double(v.r[d]) * fraction;
   return kErrNone;
 }
 
 // Impl::magnetic (src/source_coupling.cpp:40-51).
-template <class W, class F>
-__device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape,
+template <int S, class W, class F>
+__device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g,
                                                     const double a[3], const double b[3],
                                                     const Ptr3<W>& bsrc, double out[3]) {
   OpenOrbit path;
@@ -595,7 +595,7 @@ __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g, int shape
   if (!path.valid) return kErrOrbitOutside;
   double middle[3];
   for (int d = 0; d < 3; ++d) middle[d] = (path.begin[d] + path.end[d]) * .5;
-  if (shape == 0)
+  if constexpr (S == 0)
     binomial_xz_magnetic(g, bsrc, middle, out);
   else
     trilinear_magnetic(g, bsrc, middle, out);
@@ -631,8 +631,8 @@ struct DepositVisitor {
 
 // ChargeConservingCurrentDepositor::depositSegment (src/eb_deposition.cpp:41-51,
 // validatePosition 228-246).
-template <class F>
-__device__ unsigned deposit_segment(const GridT<F>& g, int shape, const double b[3],
+template <int S, class F>
+__device__ unsigned deposit_segment(const GridT<F>& g, const double b[3],
                                     const double e[3], double charge) {
   const double extent[3] = {(double)g.nx * g.dx, (double)g.ny * g.dy, (double)g.nz * g.dz};
   for (int a = 0; a < 3; ++a) {
@@ -644,11 +644,11 @@ __device__ unsigned deposit_segment(const GridT<F>& g, int shape, const double b
   if (!isfinite(charge)) return kErrNonFinite;
   DepositVisitor<F> v;
   v.g = &g;
-  v.smooth_x = shape == 0;
+  v.smooth_x = S == 0;
   v.error = kErrNone;
   for (int a = 0; a < 3; ++a)
     v.scale[a] = F(charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt));
-  if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
+  if (shape_weights<S>(g, b, e, v) < 0) return kErrCrossingBudget;
   return v.error;
 }
 
@@ -917,8 +917,8 @@ struct CarrierState {
 
 // processCarrierSegment at one rank (src/simulation.cpp:4310-4407).
 // Returns an error code; *kept tells whether the carrier survives.
-template <class F>
-__device__ unsigned carrier_segment(const GridT<F>& g, int shape, const DRegion& r,
+template <int S, class F>
+__device__ unsigned carrier_segment(const GridT<F>& g, const DRegion& r,
                                     CarrierState& c, const double seg_start[3],
                                     double seg_start_fraction, TrialCounters* counters,
                                     bool& kept) {
@@ -944,7 +944,7 @@ __device__ unsigned carrier_segment(const GridT<F>& g, int shape, const DRegion&
   const double end_damping = damping_factor(r, seg_start, seg_end, duration);
   const double deposited = c.w * mid_damping;
   const double end_weight = c.w * end_damping;
-  err = deposit_segment(g, shape, seg_start, seg_end, c.q * deposited);
+  err = deposit_segment<S>(g, seg_start, seg_end, c.q * deposited);
   if (err) return err;
   if (exits) {
     atomicAdd(&counters->carrier_outer[outer.face], 1ull);
@@ -962,7 +962,7 @@ __device__ unsigned carrier_segment(const GridT<F>& g, int shape, const DRegion&
 // Existing CPML carriers: ballistic step, damped deposit, outer exit
 // (src/simulation.cpp:4531-4537).  Carriers deposit with the run's shape,
 // like every ChargeConservingCurrentDepositor call.
-template <class F>
+template <class F, int S>
 __global__ void carrier_kernel(CarrierArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -975,7 +975,7 @@ __global__ void carrier_kernel(CarrierArgs<F> a) {
   const double start[3] = {c.pos[0], c.pos[1], c.pos[2]};
   for (int d = 0; d < 3; ++d) c.pos[d] += a.g.dt * c.vel[d];
   bool kept = false;
-  const unsigned err = carrier_segment(a.g, a.shape, a.region, c, start, 0.0, a.counters, kept);
+  const unsigned err = carrier_segment<S>(a.g, a.region, c, start, 0.0, a.counters, kept);
   if (err) raise_error(a.status, err, (unsigned long long)n);
   count_lanes(&a.counters->carriers_kept, kept);
   a.keep[n] = kept ? 1 : 0;
@@ -1031,16 +1031,16 @@ __device__ unsigned coupling_push(const PushArgs<F>& a, long long n, double pos[
 // validation (src/longitudinal_shape.h:175-187): the upstream part of an
 // admitted held particle and the frozen source support
 // (src/source_coupling.cpp:73-78) deposit this way.
-template <class F>
-__device__ unsigned deposit_current(const GridT<F>& g, int shape, const double b[3],
+template <int S, class F>
+__device__ unsigned deposit_current(const GridT<F>& g, const double b[3],
                                     const double e[3], double charge) {
   DepositVisitor<F> v;
   v.g = &g;
-  v.smooth_x = shape == 0;
+  v.smooth_x = S == 0;
   v.error = kErrNone;
   for (int a = 0; a < 3; ++a)
     v.scale[a] = F(charge * (e[a] - b[a]) / (g.dx * g.dy * g.dz * g.dt));
-  if (shape_weights(g, shape, b, e, v) < 0) return kErrCrossingBudget;
+  if (shape_weights<S>(g, b, e, v) < 0) return kErrCrossingBudget;
   return v.error;
 }
 
@@ -1098,7 +1098,7 @@ __device__ __forceinline__ SlotPlan plan_slot(const GridT<F>& g, const DFrame& f
 // (Impl::Slot::guess, src/source_coupling.cpp:92-95), gathered from E*
 // before any current of the trial is deposited; the push reads them as the
 // previous residual's fields.
-template <class W, class F>
+template <class W, class F, int S>
 __global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.count) return;
@@ -1117,8 +1117,8 @@ __global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
                        static_cast<const W*>(a.orbit[2])}};
   const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]), static_cast<const W*>(a.bgather[1]),
                       static_cast<const W*>(a.bgather[2])}};
-  unsigned err = gather_electric(a.g, a.shape, s.start, guess, orbit, ne);
-  if (!err) err = gather_magnetic(a.g, a.shape, s.start, guess, bsrc, nb);
+  unsigned err = gather_electric<S>(a.g, s.start, guess, orbit, ne);
+  if (!err) err = gather_magnetic<S>(a.g, s.start, guess, bsrc, nb);
   if (err) raise_error(a.status, err, (unsigned long long)n);
   double* next_e = const_cast<double*>(a.next_e);
   double* next_b = const_cast<double*>(a.next_b);
@@ -1134,7 +1134,7 @@ __global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
 // up to an activation kink (4684-4756) and processActiveSegment (4760-4917)
 // with Simulation::firstMovingWindowEntry
 // (src/simulation_moving_window.cpp:380-395).
-template <class F>
+template <class F, int S>
 __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1236,7 +1236,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
         e[d] = action ? selected.position[d] : pos[d];
       }
     }
-    err = validate ? deposit_segment(g, a.shape, b, e, q) : deposit_current(g, a.shape, b, e, q);
+    err = validate ? deposit_segment<S>(g, b, e, q) : deposit_current<S>(g, b, e, q);
   }
   bool born_kept = false;
   CarrierState born;
@@ -1255,7 +1255,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
     born.q = q;
     born.w = 1.0;
     const double global_end = seg_frac + selected.fraction * (1.0 - seg_frac);
-    err = carrier_segment(g, a.shape, a.region, born, selected.position, global_end, a.counters,
+    err = carrier_segment<S>(g, a.region, born, selected.position, global_end, a.counters,
                           born_kept);
   } else if (!err && has_main && action == 2) {
     atomicAdd(&a.counters->direct[selected.face], 1ull);
@@ -1305,7 +1305,7 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-template <class W, class F>
+template <class W, class F, int S>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1329,8 +1329,8 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]),
                         static_cast<const W*>(a.bgather[1]),
                         static_cast<const W*>(a.bgather[2])}};
-    unsigned err = gather_electric(a.g, a.shape, first, last, orbit, ne);
-    if (!err) err = gather_magnetic(a.g, a.shape, first, last, bsrc, nb);
+    unsigned err = gather_electric<S>(a.g, first, last, orbit, ne);
+    if (!err) err = gather_magnetic<S>(a.g, first, last, bsrc, nb);
     if (err) {
       raise_error(a.status, err, (unsigned long long)n);
       for (int d = 0; d < 3; ++d) ne[d] = nb[d] = 0.0;
@@ -1577,7 +1577,7 @@ __global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
 // (PendingParticleQueue::visitNear + depositFrozenSourceSupport,
 // src/simulation.cpp:4170-4172, src/source_coupling.cpp:73-78): each
 // deposits its held chord of this step without endpoint validation.
-template <class F>
+template <class F, int S>
 __global__ void frozen_support_kernel(SupportArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1588,7 +1588,7 @@ __global__ void frozen_support_kernel(SupportArgs<F> a) {
   const double start[3] = {a.src.x[k], a.src.y[k],
                            repeat_held_addition(a.src.z[k], increment, a.steps)};
   const double stop[3] = {start[0], start[1], start[2] + increment};
-  const unsigned err = deposit_current(a.g, a.shape, start, stop, a.src.q[k]);
+  const unsigned err = deposit_current<S>(a.g, start, stop, a.src.q[k]);
   if (err) raise_error(a.status, err, (unsigned long long)k);
 }
 
@@ -1707,12 +1707,19 @@ __global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iteratio
 
 // The grid and J are binary64 in every mode; the gathers are built with
 // binary64 (FP64 drop-in) and binary32 (FP32-mixed) arithmetic.
-template __global__ void push_deposit_kernel<double>(PushArgs<double>);
-template __global__ void carrier_kernel<double>(CarrierArgs<double>);
-template __global__ void frozen_support_kernel<double>(SupportArgs<double>);
-template __global__ void guess_gather_kernel<double, double>(PushArgs<double>);
-template __global__ void guess_gather_kernel<float, double>(PushArgs<double>);
-template __global__ void residual_kernel<double, double>(ResidualArgs<double>);
-template __global__ void residual_kernel<float, double>(ResidualArgs<double>);
+// Each particle kernel is built once per shape (S = 0 linear-binomial3,
+// 1 quintic-compensated), so a kernel carries the registers and local
+// memory of its own shape's weights only.
+#define APRL_SHAPE_KERNELS(S)                                                        \
+  template __global__ void push_deposit_kernel<double, S>(PushArgs<double>);         \
+  template __global__ void carrier_kernel<double, S>(CarrierArgs<double>);           \
+  template __global__ void frozen_support_kernel<double, S>(SupportArgs<double>);    \
+  template __global__ void guess_gather_kernel<double, double, S>(PushArgs<double>); \
+  template __global__ void guess_gather_kernel<float, double, S>(PushArgs<double>);  \
+  template __global__ void residual_kernel<double, double, S>(ResidualArgs<double>); \
+  template __global__ void residual_kernel<float, double, S>(ResidualArgs<double>);
+APRL_SHAPE_KERNELS(0)
+APRL_SHAPE_KERNELS(1)
+#undef APRL_SHAPE_KERNELS
 
 }  // namespace aprl_gpu

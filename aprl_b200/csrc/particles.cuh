@@ -151,20 +151,21 @@ struct ResidualArgs {
 
 // Occupancy knobs of the hot particle kernels (blocks of 128 threads
 // that must fit one SM; 0 leaves the register count to the compiler).
-// Measured on the 128x128x512 dipole grid with 1M particles: push_deposit at
-// 8 blocks (64 registers, with spills) beats 4, 10, 12 and 16 blocks on the
-// binomial3, quintic, FP32-mixed and drift workloads -- its FP64 reductions
-// want many warps in flight; guess_gather at 4 blocks (128 registers) takes
-// 0.28 ms against 0.33 ms unbounded (240 registers); the residual stays at 4
-// (6 and 8 spill more and are no faster).
+// Measured on the 128x128x512 dipole grid with 1M particles, with the
+// kernels built per shape: push_deposit at 8 blocks (64 registers, with
+// spills) beats 4, 10, 12 and 16 blocks on the binomial3, quintic,
+// FP32-mixed and drift workloads -- its FP64 reductions want many warps in
+// flight; the residual and the guess gather at 6 blocks (80 registers) beat
+// 4, 5 and 8 (dipole step 4.47 -> 4.44 ms, FP32-mixed 3.44 -> 3.35 ms,
+// quintic 15.99 -> 15.62 ms).
 #ifndef APRL_PUSH_MIN_BLOCKS
 #define APRL_PUSH_MIN_BLOCKS 8
 #endif
 #ifndef APRL_RESIDUAL_MIN_BLOCKS
-#define APRL_RESIDUAL_MIN_BLOCKS 4
+#define APRL_RESIDUAL_MIN_BLOCKS 6
 #endif
 #ifndef APRL_GATHER_MIN_BLOCKS
-#define APRL_GATHER_MIN_BLOCKS 4
+#define APRL_GATHER_MIN_BLOCKS 6
 #endif
 #if APRL_GATHER_MIN_BLOCKS > 0
 #define APRL_GATHER_BOUNDS __launch_bounds__(128, APRL_GATHER_MIN_BLOCKS)
@@ -183,10 +184,11 @@ struct ResidualArgs {
 #endif
 
 // W: arithmetic of the gathers (double, or float in the FP32-mixed mode).
-template <class W, class F> __global__ void guess_gather_kernel(PushArgs<F> a);
-template <class F> __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
-template <class F> __global__ void carrier_kernel(CarrierArgs<F> a);
-template <class W, class F>
+// S: the particle shape, 0 linear-binomial3, 1 quintic-compensated.
+template <class W, class F, int S> __global__ void guess_gather_kernel(PushArgs<F> a);
+template <class F, int S> __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
+template <class F, int S> __global__ void carrier_kernel(CarrierArgs<F> a);
+template <class W, class F, int S>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
 
 // Stable compaction helpers (warp ballot + block scan + block-offset scan).
@@ -237,7 +239,7 @@ struct SupportArgs {
   double held_distance_per_beta; // c*dt
   DeviceStatus* status;
 };
-template <class F> __global__ void frozen_support_kernel(SupportArgs<F> a);
+template <class F, int S> __global__ void frozen_support_kernel(SupportArgs<F> a);
 __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
                                   double lower, unsigned char* keep,
                                   TrialCounters* counters, DeviceStatus* status);

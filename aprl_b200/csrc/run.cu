@@ -1138,6 +1138,8 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
                r->d_sums));
   }
   const DRegion region = make_region(r);
+  // Each particle kernel is built per shape: 0 linear-binomial3, else quintic.
+  const bool binomial = c.shape == 0;
   if (r->queue.extracted) {
     // Frozen source support of the entries due within min(8, horizon) steps.
     const auto& q = r->queue;
@@ -1154,7 +1156,9 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
       sa.steps = r->step - q.initial_step;
       sa.held_distance_per_beta = held_distance_per_beta(c);
       sa.status = r->d_status;
-      TRY(launch(r, kFrozenSupport, frozen_support_kernel<F>, dim3(blocks_for(end - q.cursor, 128)),
+      TRY(launch(r, kFrozenSupport,
+                 binomial ? frozen_support_kernel<F, 0> : frozen_support_kernel<F, 1>,
+                 dim3(blocks_for(end - q.cursor, 128)),
                  dim3(128), sa));
     }
   }
@@ -1174,7 +1178,8 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ca.status = r->d_status;
     CUDA_TRY(cudaEventRecord(r->fork, r->stream));
     CUDA_TRY(cudaStreamWaitEvent(r->side, r->fork, 0));
-    TRY(launch_on(r, r->side, kCarrier, carrier_kernel<F>, dim3(blocks_for(r->nc, 128)),
+    TRY(launch_on(r, r->side, kCarrier, binomial ? carrier_kernel<F, 0> : carrier_kernel<F, 1>,
+                  dim3(blocks_for(r->nc, 128)),
                   dim3(128), ca));
     CUDA_TRY(cudaEventRecord(r->join, r->side));
     joined = false;
@@ -1238,10 +1243,13 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     if (r->trials == 0) {
       TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
                  orbit[1], orbit[2], 0));
-      TRY(launch(r, kGuessGather, guess_gather_kernel<W, F>, dim3(blocks_for(r->np, 128)),
+      TRY(launch(r, kGuessGather,
+                 binomial ? guess_gather_kernel<W, F, 0> : guess_gather_kernel<W, F, 1>,
+                 dim3(blocks_for(r->np, 128)),
                  dim3(128), pa));
     }
-    TRY(launch(r, kPushDeposit, push_deposit_kernel<F>, dim3(blocks_for(r->np, 128)), dim3(128),
+    TRY(launch(r, kPushDeposit, binomial ? push_deposit_kernel<F, 0> : push_deposit_kernel<F, 1>,
+               dim3(blocks_for(r->np, 128)), dim3(128),
                pa));
     TRY(join_carriers());
     TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
@@ -1264,7 +1272,8 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ra.abs_grid_work = r->abs_work;
     ra.sums = r->d_sums;
     ra.status = r->d_status;
-    TRY(launch(r, kResidual, residual_kernel<W, F>, dim3(blocks_for(r->np, 128)), dim3(128), ra));
+    TRY(launch(r, kResidual, binomial ? residual_kernel<W, F, 0> : residual_kernel<W, F, 1>,
+               dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
   TRY(join_carriers());
   if (ahead)
