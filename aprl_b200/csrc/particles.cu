@@ -1680,11 +1680,12 @@ __global__ void inlet_charge_kernel(InletMatchArgs a) {
     }
 }
 
-__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums) {
+__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums,
+                                   int clear_current) {
   if (trial_skipped(g)) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < 3 && clear_current; ++c) {
     const long long count = (long long)e_nx(g, c) * e_ny(g, c) * e_nz(g, c);
     for (long long n = first; n < count; n += stride) g.j[c][n] = 0.;
   }

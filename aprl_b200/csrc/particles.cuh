@@ -268,7 +268,8 @@ __global__ void inlet_charge_kernel(InletMatchArgs a);
 
 // A trial's start: J, the trial counters and the residual sums cleared
 // (skipped with the trial).
-__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums);
+__global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums,
+                                   int clear_current);
 // solveConservativeSourceStep's stopping rule (src/simulation_source_coupling.cpp:50)
 // applied to trial `iterations`' residual sums: on convergence *stop = iterations.
 __global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iterations,

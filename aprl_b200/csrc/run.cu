@@ -257,6 +257,11 @@ struct aprl_run {
   int cur = 0;  // e[cur] = E^n (committed), e[1-cur] = E*
   double* b[3]{};
   void* jc[3]{};
+  // J is known to be zero everywhere (set by a clear, kept by a trial that
+  // deposits nothing): the next clear and the commit's pass over J are
+  // skipped, which is most of a field-only step's work besides the field
+  // updates.
+  bool j_zero = true;
   double* lower[3]{};
   // What the gathers read: the orbit sum S = E_new + E^n per E node (binary64,
   // or binary32 in the FP32-mixed mode) and, in that mode, a binary32 B.
@@ -1031,8 +1036,10 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   if (r->ledger_on && !r->ledger_start_ready) TRY(ledger_begin(r));
   r->ledger_start_ready = false;
   const aprl_run_config& c = r->cfg;
-  for (int a = 0; a < 3; ++a)
-    CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
+  if (!r->j_zero)
+    for (int a = 0; a < 3; ++a)
+      CUDA_TRY(cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * sizeof(F), r->stream));
+  r->j_zero = true;
   InletPlaneArgs ia{};
   ia.nx = (int)c.nx;
   ia.ny = (int)c.ny;
@@ -1130,22 +1137,32 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
   const aprl_run_config& c = r->cfg;
   GridT<F> g = make_grid<F>(r);
   if (ahead) g.stop = r->d_stop;
+  // Frozen source support of the entries due within min(8, horizon) steps.
+  size_t frozen_end = 0;
+  if (r->queue.extracted) {
+    const auto& q = r->queue;
+    const uint64_t room = q.maximum_step - r->step;
+    const uint64_t until = r->step + std::min<uint64_t>(8, room);
+    frozen_end = q.offsets[until - q.initial_step + 1];
+  }
+  const bool deposits = r->np || r->nc || (r->queue.extracted && frozen_end > r->queue.cursor);
   {
+    // The counters and sums always; J unless it is known to be zero.
     size_t most = 0;
     for (int a = 0; a < 3; ++a) most = std::max(most, e_count(c, a));
-    const unsigned blocks = std::min<unsigned>(blocks_for(most, 256), 148 * 8);
+    const int clear_current = r->j_zero ? 0 : 1;
+    const unsigned blocks =
+        clear_current ? std::min<unsigned>(blocks_for(most, 256), 148 * 8) : 1u;
     TRY(launch(r, kTrialClear, trial_clear_kernel, dim3(blocks), dim3(256), g, r->d_counters,
-               r->d_sums));
+               r->d_sums, clear_current));
   }
+  r->j_zero = !deposits;
   const DRegion region = make_region(r);
   // Each particle kernel is built per shape: 0 linear-binomial3, else quintic.
   const bool binomial = c.shape == 0;
   if (r->queue.extracted) {
-    // Frozen source support of the entries due within min(8, horizon) steps.
     const auto& q = r->queue;
-    const uint64_t room = q.maximum_step - r->step;
-    const uint64_t until = r->step + std::min<uint64_t>(8, room);
-    const size_t end = q.offsets[until - q.initial_step + 1];
+    const size_t end = frozen_end;
     if (end > q.cursor) {
       SupportArgs<F> sa{};
       sa.g = g;
@@ -1327,8 +1344,11 @@ aprl_status do_commit(aprl_run* r) {
   if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
   const aprl_run_config& c = r->cfg;
   const dim3 block(32, 4);
-  TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
-             make_grid<double>(r)));
+  // E^{n+1} = E* - dt/eps0 J, in place where J is nonzero: nothing to do
+  // when J is known to be zero.
+  if (!r->j_zero)
+    TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
+               make_grid<double>(r)));
   r->cur = 1 - r->cur;
   // The counters of the converged trial (read back with its residual) give
   // every compaction size: no host round trip in the commit.
@@ -1782,8 +1802,10 @@ static aprl_status field_io(aprl_run* r, unsigned a, const double* in, double* o
   if (r->stage != 0 && r->stage != 4 && in)
     return fail(APRL_ERR_RUNTIME, "Fields can only be replaced between steps");
   const size_t plane = s[0] * s[1];
-  if (a >= 6)
+  if (a >= 6) {
+    if (in) r->j_zero = false;
     return copy_ring(r, static_cast<double*>(r->jc[a - 6]), in, out, plane, s[2], 0);
+  }
   if (a < 3) return copy_ring(r, r->e[r->cur][a], in, out, plane, s[2], r->zb_e[a]);
   return copy_ring(r, r->b[a - 3], in, out, plane, s[2], r->zb_b[a - 3]);
 }
