@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -114,25 +115,6 @@ aprl_status device_error_status(unsigned code) {
     default:
       return APRL_ERR_RUNTIME;
   }
-}
-
-aprl_status device_alloc_bytes(void** p, size_t bytes) {
-  *p = nullptr;
-  if (bytes == 0) bytes = 8;
-  const cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(APRL_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
-  }
-  return APRL_OK;
-}
-
-template <class T>
-aprl_status device_alloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
-  return APRL_OK;
 }
 
 // EBCowanCoefficients::forZDispersion (src/eb_field.cpp:33-73).
@@ -243,6 +225,8 @@ constexpr unsigned kTrialSlots = 3;
 struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;   // device memory (device_pool of the run's device)
+  void* pinned = nullptr;         // the page-locked block the h_* read-backs live in
   // The CPML carriers of a trial run on `side`, forked from `stream` after
   // the trial's clear and joined before the orbit sum that reads J, so their
   // short, latency-bound launch overlaps the particles' push.
@@ -359,6 +343,113 @@ struct aprl_run {
 };
 
 namespace {
+
+// Device memory of every run comes from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the run's stream).  Memory a
+// run frees goes back to the pool and the next run reuses it, so creating
+// and destroying runs -- once per request in the scan server -- maps and
+// unmaps no device memory: with cudaMalloc/cudaFree that took 0.4-1.5 s for
+// some large runs and varied several-fold from call to call.  A block is
+// reused only once its free has completed on the GPU or the allocating stream
+// is already ordered after it (no opportunistic reuse).  Up to kPoolKeepBytes
+// of freed memory stay in the pool; the driver releases the rest at the next
+// synchronisation.
+constexpr uint64_t kPoolKeepBytes = 16ull << 30;
+
+cudaMemPool_t device_pool(int device) {
+  static std::mutex lock;
+  static std::vector<cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> hold(lock);
+  if (device < 0) return nullptr;
+  if ((size_t)device >= pools.size()) pools.resize(device + 1, nullptr);
+  if (!pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = kPoolKeepBytes;
+    int no = 0;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &no) != cudaSuccess ||
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no) !=
+            cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return nullptr;
+    }
+    pools[device] = pool;
+  }
+  return pools[device];
+}
+
+// The allocation is waited for on the run's stream, so the block is valid for
+// every stream and for the synchronous copies that fill it (allocations are
+// made outside the step loop, or on a stream that is idle anyway).
+aprl_status device_alloc_bytes(aprl_run* r, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 8;
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes, r->pool, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(APRL_ERR_CUDA, "device allocation of %zu bytes failed: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  return APRL_OK;
+}
+
+template <class T>
+aprl_status device_alloc(aprl_run* r, T** p, size_t count) {
+  void* v = nullptr;
+  const aprl_status s = device_alloc_bytes(r, &v, (count ? count : 1) * sizeof(T));
+  *p = static_cast<T*>(v);
+  return s;
+}
+
+// Back to the pool in stream order (after the work queued on the run's stream).
+void device_free(aprl_run* r, void* p) {
+  if (p) cudaFreeAsync(p, r->stream);
+}
+
+// Page-locked 4 KiB blocks for the runs' small read-back areas, kept for
+// reuse (cudaMallocHost/cudaFreeHost per run cost milliseconds each).
+constexpr size_t kPinnedBlock = 4096;
+
+static_assert(kTrialSlots * sizeof(ResidualSums) + sizeof(DeviceStatus) +
+                      kTrialSlots * sizeof(TrialCounters) + sizeof(int) +
+                      sizeof(unsigned long long) + 5 * 64 <= kPinnedBlock,
+              "read-back areas exceed the pinned block");
+
+std::mutex& pinned_lock() {
+  static std::mutex lock;
+  return lock;
+}
+std::vector<void*>& pinned_free() {
+  static std::vector<void*> blocks;
+  return blocks;
+}
+
+void* pinned_take() {
+  {
+    std::lock_guard<std::mutex> hold(pinned_lock());
+    if (!pinned_free().empty()) {
+      void* b = pinned_free().back();
+      pinned_free().pop_back();
+      return b;
+    }
+  }
+  void* b = nullptr;
+  if (cudaMallocHost(&b, kPinnedBlock) != cudaSuccess) return nullptr;
+  return b;
+}
+
+void pinned_give(void* b) {
+  if (!b) return;
+  std::lock_guard<std::mutex> hold(pinned_lock());
+  pinned_free().push_back(b);
+}
 
 size_t e_count(const aprl_run_config& g, int c) {
   return (size_t)(g.nx + (c != 0)) * (g.ny + (c != 1)) * (g.nz + (c != 2));
@@ -597,42 +688,42 @@ aprl_status validate(const aprl_run_config& g) {
 aprl_status ensure_scan(aprl_run* r, size_t n) {
   const size_t blocks = (n + kScanBlock - 1) / kScanBlock + 1;
   if (blocks <= r->scan_cap) return APRL_OK;
-  cudaFree(r->scan_count);
-  cudaFree(r->scan_offset);
-  TRY(device_alloc(&r->scan_count, blocks));
-  TRY(device_alloc(&r->scan_offset, blocks));
+  device_free(r, r->scan_count);
+  device_free(r, r->scan_offset);
+  TRY(device_alloc(r, &r->scan_count, blocks));
+  TRY(device_alloc(r, &r->scan_offset, blocks));
   r->scan_cap = blocks;
   return APRL_OK;
 }
 
-aprl_status alloc_particles(DParticles& p, size_t n) {
-  TRY(device_alloc(&p.x, n)); TRY(device_alloc(&p.y, n)); TRY(device_alloc(&p.z, n));
-  TRY(device_alloc(&p.ux, n)); TRY(device_alloc(&p.uy, n)); TRY(device_alloc(&p.uz, n));
-  TRY(device_alloc(&p.q, n)); TRY(device_alloc(&p.m, n)); TRY(device_alloc(&p.id, n));
-  TRY(device_alloc(&p.order, n));
-  TRY(device_alloc(&p.frozen, n)); TRY(device_alloc(&p.beta, n));
+aprl_status alloc_particles(aprl_run* r, DParticles& p, size_t n) {
+  TRY(device_alloc(r, &p.x, n)); TRY(device_alloc(r, &p.y, n)); TRY(device_alloc(r, &p.z, n));
+  TRY(device_alloc(r, &p.ux, n)); TRY(device_alloc(r, &p.uy, n)); TRY(device_alloc(r, &p.uz, n));
+  TRY(device_alloc(r, &p.q, n)); TRY(device_alloc(r, &p.m, n)); TRY(device_alloc(r, &p.id, n));
+  TRY(device_alloc(r, &p.order, n));
+  TRY(device_alloc(r, &p.frozen, n)); TRY(device_alloc(r, &p.beta, n));
   return APRL_OK;
 }
-void free_particles(DParticles& p) {
-  cudaFree(p.x); cudaFree(p.y); cudaFree(p.z); cudaFree(p.ux); cudaFree(p.uy);
-  cudaFree(p.uz); cudaFree(p.q); cudaFree(p.m); cudaFree(p.id); cudaFree(p.order);
-  cudaFree(p.frozen); cudaFree(p.beta);
+void free_particles(aprl_run* r, DParticles& p) {
+  device_free(r, p.x); device_free(r, p.y); device_free(r, p.z); device_free(r, p.ux); device_free(r, p.uy);
+  device_free(r, p.uz); device_free(r, p.q); device_free(r, p.m); device_free(r, p.id); device_free(r, p.order);
+  device_free(r, p.frozen); device_free(r, p.beta);
   p = DParticles{};
 }
-void free_pending(DPending& d) {
-  cudaFree(d.x); cudaFree(d.y); cudaFree(d.z); cudaFree(d.ux); cudaFree(d.uy);
-  cudaFree(d.uz); cudaFree(d.q); cudaFree(d.m); cudaFree(d.beta); cudaFree(d.id);
+void free_pending(aprl_run* r, DPending& d) {
+  device_free(r, d.x); device_free(r, d.y); device_free(r, d.z); device_free(r, d.ux); device_free(r, d.uy);
+  device_free(r, d.uz); device_free(r, d.q); device_free(r, d.m); device_free(r, d.beta); device_free(r, d.id);
   d = DPending{};
 }
-aprl_status alloc_carriers(DCarriers& c, size_t n) {
-  TRY(device_alloc(&c.px, n)); TRY(device_alloc(&c.py, n)); TRY(device_alloc(&c.pz, n));
-  TRY(device_alloc(&c.vx, n)); TRY(device_alloc(&c.vy, n)); TRY(device_alloc(&c.vz, n));
-  TRY(device_alloc(&c.q, n)); TRY(device_alloc(&c.w, n)); TRY(device_alloc(&c.key, n));
+aprl_status alloc_carriers(aprl_run* r, DCarriers& c, size_t n) {
+  TRY(device_alloc(r, &c.px, n)); TRY(device_alloc(r, &c.py, n)); TRY(device_alloc(r, &c.pz, n));
+  TRY(device_alloc(r, &c.vx, n)); TRY(device_alloc(r, &c.vy, n)); TRY(device_alloc(r, &c.vz, n));
+  TRY(device_alloc(r, &c.q, n)); TRY(device_alloc(r, &c.w, n)); TRY(device_alloc(r, &c.key, n));
   return APRL_OK;
 }
-void free_carriers(DCarriers& c) {
-  cudaFree(c.px); cudaFree(c.py); cudaFree(c.pz); cudaFree(c.vx); cudaFree(c.vy);
-  cudaFree(c.vz); cudaFree(c.q); cudaFree(c.w); cudaFree(c.key);
+void free_carriers(aprl_run* r, DCarriers& c) {
+  device_free(r, c.px); device_free(r, c.py); device_free(r, c.pz); device_free(r, c.vx); device_free(r, c.vy);
+  device_free(r, c.vz); device_free(r, c.q); device_free(r, c.w); device_free(r, c.key);
   c = DCarriers{};
 }
 
@@ -642,7 +733,7 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   if (n <= r->pcap) return APRL_OK;
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   DParticles np{};
-  TRY(alloc_particles(np, n));
+  TRY(alloc_particles(r, np, n));
   if (r->np) {
     CUDA_TRY(cudaMemcpy(np.x, r->p.x, r->np * 8, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.y, r->p.y, r->np * 8, cudaMemcpyDeviceToDevice));
@@ -657,38 +748,38 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
     CUDA_TRY(cudaMemcpy(np.frozen, r->p.frozen, r->np, cudaMemcpyDeviceToDevice));
     CUDA_TRY(cudaMemcpy(np.beta, r->p.beta, r->np * 8, cudaMemcpyDeviceToDevice));
   }
-  free_particles(r->p);
-  free_particles(r->p_alt);
+  free_particles(r, r->p);
+  free_particles(r, r->p_alt);
   r->p = np;
-  TRY(alloc_particles(r->p_alt, n));
+  TRY(alloc_particles(r, r->p_alt, n));
   double** trial[] = {&r->x1,       &r->y1,       &r->z1,       &r->ux1,     &r->uy1,
                       &r->uz1,      &r->abs_work, &r->slots.x0, &r->slots.y0, &r->slots.z0,
                       &r->slots.dt};
   for (double** t : trial) {
-    cudaFree(*t);
-    TRY(device_alloc(t, n));
+    device_free(r, *t);
+    TRY(device_alloc(r, t, n));
   }
   double** slot[] = {&r->used_e, &r->used_b, &r->next_e, &r->next_b};
   for (double** t : slot) {
-    cudaFree(*t);
-    TRY(device_alloc(t, 3 * n));
+    device_free(r, *t);
+    TRY(device_alloc(r, t, 3 * n));
   }
-  cudaFree(r->action);
-  cudaFree(r->born_keep);
-  cudaFree(r->slot_order);
-  cudaFree(r->tile_of);
-  cudaFree(r->tile_rank);
-  cudaFree(r->frozen1);
-  cudaFree(r->slots.seen);
-  TRY(device_alloc(&r->frozen1, n));
-  TRY(device_alloc(&r->slots.seen, n));
-  TRY(device_alloc(&r->action, n));
-  TRY(device_alloc(&r->born_keep, n));
-  TRY(device_alloc(&r->slot_order, n));
-  TRY(device_alloc(&r->tile_of, n));
-  TRY(device_alloc(&r->tile_rank, n));
-  free_carriers(r->born);
-  TRY(alloc_carriers(r->born, n));
+  device_free(r, r->action);
+  device_free(r, r->born_keep);
+  device_free(r, r->slot_order);
+  device_free(r, r->tile_of);
+  device_free(r, r->tile_rank);
+  device_free(r, r->frozen1);
+  device_free(r, r->slots.seen);
+  TRY(device_alloc(r, &r->frozen1, n));
+  TRY(device_alloc(r, &r->slots.seen, n));
+  TRY(device_alloc(r, &r->action, n));
+  TRY(device_alloc(r, &r->born_keep, n));
+  TRY(device_alloc(r, &r->slot_order, n));
+  TRY(device_alloc(r, &r->tile_of, n));
+  TRY(device_alloc(r, &r->tile_rank, n));
+  free_carriers(r, r->born);
+  TRY(alloc_carriers(r, r->born, n));
   r->pcap = n;
   return ensure_scan(r, n);
 }
@@ -715,20 +806,20 @@ aprl_status reserve_carriers(aprl_run* r, size_t n) {
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   DCarriers nc{}, nout{};
   unsigned char* nkeep = nullptr;
-  TRY(alloc_carriers(nc, n));
-  TRY(alloc_carriers(nout, n));
-  TRY(device_alloc(&nkeep, n));
+  TRY(alloc_carriers(r, nc, n));
+  TRY(alloc_carriers(r, nout, n));
+  TRY(device_alloc(r, &nkeep, n));
   TRY(copy_carriers(nc, r->c, r->nc));
   TRY(copy_carriers(nout, r->c_out, r->nc));
   if (r->nc) CUDA_TRY(cudaMemcpy(nkeep, r->c_keep, r->nc, cudaMemcpyDeviceToDevice));
-  free_carriers(r->c);
-  free_carriers(r->c_alt);
-  free_carriers(r->c_out);
-  cudaFree(r->c_keep);
+  free_carriers(r, r->c);
+  free_carriers(r, r->c_alt);
+  free_carriers(r, r->c_out);
+  device_free(r, r->c_keep);
   r->c = nc;
   r->c_out = nout;
   r->c_keep = nkeep;
-  TRY(alloc_carriers(r->c_alt, n));
+  TRY(alloc_carriers(r, r->c_alt, n));
   r->ccap = n;
   return ensure_scan(r, n);
 }
@@ -909,10 +1000,10 @@ constexpr int kLedgerMaxBlocks = 592;  // four blocks per SM
 aprl_status ensure_ledger(aprl_run* r) {
   if (r->d_ledger) return APRL_OK;
   const aprl_run_config& c = r->cfg;
-  TRY(device_alloc(&r->d_ledger, 1));
-  TRY(device_alloc(&r->d_ledger_partial, (size_t)kLedgerMaxTerms * kLedgerMaxBlocks));
-  TRY(device_alloc(&r->ledger_pre[0], (size_t)c.nx * (c.ny + 1)));
-  TRY(device_alloc(&r->ledger_pre[1], (size_t)(c.nx + 1) * c.ny));
+  TRY(device_alloc(r, &r->d_ledger, 1));
+  TRY(device_alloc(r, &r->d_ledger_partial, (size_t)kLedgerMaxTerms * kLedgerMaxBlocks));
+  TRY(device_alloc(r, &r->ledger_pre[0], (size_t)c.nx * (c.ny + 1)));
+  TRY(device_alloc(r, &r->ledger_pre[1], (size_t)(c.nx + 1) * c.ny));
   CUDA_TRY(cudaMemsetAsync(r->d_ledger, 0, sizeof(DLedger), r->stream));
   return APRL_OK;
 }
@@ -1577,25 +1668,30 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     return st;
   };
   if (s != APRL_OK) return cleanup(s);
+  {
+    int device = -1;
+    if (cudaGetDevice(&device) != cudaSuccess || !(r->pool = device_pool(device)))
+      return cleanup(fail(APRL_ERR_CUDA, "no stream-ordered memory pool on this device"));
+  }
   const aprl_run_config& c = *config;
   r->fp32 = c.precision == APRL_PRECISION_FP32_MIXED;
   r->fes = sizeof(double);
   const size_t fes = r->fes;
   for (int a = 0; a < 3; ++a) {
     for (int k = 0; k < 2; ++k) {
-      if ((s = device_alloc(&r->e[k][a], e_count(c, a))) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(r, &r->e[k][a], e_count(c, a))) != APRL_OK) return cleanup(s);
       cudaMemsetAsync(r->e[k][a], 0, e_count(c, a) * 8, r->stream);
     }
-    if ((s = device_alloc(&r->b[a], b_count(c, a))) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc(r, &r->b[a], b_count(c, a))) != APRL_OK) return cleanup(s);
     cudaMemsetAsync(r->b[a], 0, b_count(c, a) * 8, r->stream);
-    if ((s = device_alloc_bytes(&r->jc[a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc_bytes(r, &r->jc[a], e_count(c, a) * fes)) != APRL_OK) return cleanup(s);
     cudaMemsetAsync(r->jc[a], 0, e_count(c, a) * fes, r->stream);
     const size_t plane = (size_t)(c.nx + (a != 0)) * (c.ny + (a != 1));
-    if ((s = device_alloc(&r->lower[a], plane)) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc(r, &r->lower[a], plane)) != APRL_OK) return cleanup(s);
     const size_t gather_bytes = r->fp32 ? sizeof(float) : sizeof(double);
-    if ((s = device_alloc_bytes(&r->orbit[a], e_count(c, a) * gather_bytes)) != APRL_OK)
+    if ((s = device_alloc_bytes(r, &r->orbit[a], e_count(c, a) * gather_bytes)) != APRL_OK)
       return cleanup(s);
-    if (r->fp32 && (s = device_alloc(&r->bshadow[a], b_count(c, a))) != APRL_OK)
+    if (r->fp32 && (s = device_alloc(r, &r->bshadow[a], b_count(c, a))) != APRL_OK)
       return cleanup(s);
     r->max_rate[a] = maximum_rate(c, a);
   }
@@ -1605,10 +1701,10 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
       const HostProfile hp = make_profile(c, axis, electric != 0);
       DeviceProfile& dp = electric ? r->eprof[axis] : r->mprof[axis];
       const size_t n = hp.ikm1.size();
-      if ((s = device_alloc(&dp.ikm1, n)) != APRL_OK) return cleanup(s);
-      if ((s = device_alloc(&dp.decay, n)) != APRL_OK) return cleanup(s);
-      if ((s = device_alloc(&dp.drive, n)) != APRL_OK) return cleanup(s);
-      if ((s = device_alloc(&dp.ordinal, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(r, &dp.ikm1, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(r, &dp.decay, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(r, &dp.drive, n)) != APRL_OK) return cleanup(s);
+      if ((s = device_alloc(r, &dp.ordinal, n)) != APRL_OK) return cleanup(s);
       cudaMemcpy(dp.ikm1, hp.ikm1.data(), n * 8, cudaMemcpyHostToDevice);
       cudaMemcpy(dp.decay, hp.decay.data(), n * 8, cudaMemcpyHostToDevice);
       cudaMemcpy(dp.drive, hp.drive.data(), n * 8, cudaMemcpyHostToDevice);
@@ -1630,7 +1726,7 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     hb.slots = prof.active;
     hb.layers = (int)sh[2];
     hb.row = (int)(der == 0 ? sh[1] : sh[0]);
-    if ((s = device_alloc(&hb.data, hb.length())) != APRL_OK) return cleanup(s);
+    if ((s = device_alloc(r, &hb.data, hb.length())) != APRL_OK) return cleanup(s);
     cudaMemsetAsync(hb.data, 0, std::max<size_t>(1, hb.length()) * 8, r->stream);
   }
   for (int a = 0; a < 3; ++a) {
@@ -1638,27 +1734,36 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     r->tiles[a] = (int)((cells + (1u << kTileShift) - 1) >> kTileShift);
   }
   r->ntiles = (size_t)r->tiles[0] * r->tiles[1] * r->tiles[2];
-  if ((s = device_alloc(&r->tile_count, r->ntiles)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->tile_offset, r->ntiles)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->chunk_sum, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->chunk_offset, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->d_counters, 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->d_sums, 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->d_status, 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(&r->scan_total, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->tile_count, r->ntiles)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->tile_offset, r->ntiles)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->chunk_sum, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->chunk_offset, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->d_counters, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->d_sums, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->d_status, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->scan_total, 1)) != APRL_OK) return cleanup(s);
   cudaMemsetAsync(r->d_status, 0, sizeof(DeviceStatus), r->stream);
-  if ((s = device_alloc(&r->d_stop, 1)) != APRL_OK) return cleanup(s);
+  if ((s = device_alloc(r, &r->d_stop, 1)) != APRL_OK) return cleanup(s);
   if (c.inlet_charge_match &&
-      (s = device_alloc(&r->inlet_rho, (size_t)(c.nx + 1) * (c.ny + 1))) != APRL_OK)
+      (s = device_alloc(r, &r->inlet_rho, (size_t)(c.nx + 1) * (c.ny + 1))) != APRL_OK)
     return cleanup(s);
-  if (cudaMallocHost(reinterpret_cast<void**>(&r->h_sums_slots),
-                     kTrialSlots * sizeof(ResidualSums)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_status), sizeof(DeviceStatus)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_counters_slots),
-                     kTrialSlots * sizeof(TrialCounters)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_stop), sizeof(int)) != cudaSuccess ||
-      cudaMallocHost(reinterpret_cast<void**>(&r->h_total), sizeof(unsigned long long)) != cudaSuccess)
+  // The read-back areas, 64-byte aligned inside one reused page-locked block.
+  if (!(r->pinned = pinned_take()))
     return cleanup(fail(APRL_ERR_CUDA, "cudaMallocHost failed"));
+  {
+    char* at = static_cast<char*>(r->pinned);
+    auto carve = [&](size_t bytes) {
+      char* p = at;
+      at += (bytes + 63) / 64 * 64;
+      return static_cast<void*>(p);
+    };
+    r->h_sums_slots = static_cast<ResidualSums*>(carve(kTrialSlots * sizeof(ResidualSums)));
+    r->h_status = static_cast<DeviceStatus*>(carve(sizeof(DeviceStatus)));
+    r->h_counters_slots = static_cast<TrialCounters*>(carve(kTrialSlots * sizeof(TrialCounters)));
+    r->h_stop = static_cast<int*>(carve(sizeof(int)));
+    r->h_total = static_cast<unsigned long long*>(carve(sizeof(unsigned long long)));
+    std::memset(r->pinned, 0, kPinnedBlock);
+  }
   if (cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->join, cudaEventDisableTiming) != cudaSuccess)
@@ -1690,61 +1795,62 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   }
   for (auto e : r->event_pool) cudaEventDestroy(e);
   for (int a = 0; a < 3; ++a) {
-    cudaFree(r->e[0][a]); cudaFree(r->e[1][a]); cudaFree(r->b[a]); cudaFree(r->jc[a]);
-    cudaFree(r->lower[a]);
-    cudaFree(r->orbit[a]);
-    cudaFree(r->bshadow[a]);
+    device_free(r, r->e[0][a]); device_free(r, r->e[1][a]); device_free(r, r->b[a]); device_free(r, r->jc[a]);
+    device_free(r, r->lower[a]);
+    device_free(r, r->orbit[a]);
+    device_free(r, r->bshadow[a]);
   }
-  for (int a = 0; a < 6; ++a) cudaFree(r->ref[a]);
+  for (int a = 0; a < 6; ++a) device_free(r, r->ref[a]);
   for (int a = 0; a < 2; ++a) {
     for (DeviceProfile* dp : {&r->mprof[a], &r->eprof[a]}) {
-      cudaFree(dp->ikm1); cudaFree(dp->decay); cudaFree(dp->drive); cudaFree(dp->ordinal);
+      device_free(r, dp->ikm1); device_free(r, dp->decay); device_free(r, dp->drive); device_free(r, dp->ordinal);
     }
   }
-  for (auto& h : r->hist) cudaFree(h.data);
-  free_particles(r->p);
-  free_particles(r->p_alt);
+  for (auto& h : r->hist) device_free(r, h.data);
+  free_particles(r, r->p);
+  free_particles(r, r->p_alt);
   double* singles[] = {r->x1,       r->y1,       r->z1,       r->ux1,        r->uy1,
                        r->uz1,      r->used_e,   r->used_b,   r->next_e,     r->next_b,
                        r->abs_work, r->slots.x0, r->slots.y0, r->slots.z0,   r->slots.dt,
                        r->d_detector};
-  for (double* d : singles) cudaFree(d);
-  cudaFree(r->slots.seen);
-  cudaFree(r->frozen1);
-  free_pending(r->queue.d);
-  cudaFree(r->action);
-  cudaFree(r->born_keep);
-  cudaFree(r->slot_order);
-  cudaFree(r->tile_of);
-  cudaFree(r->tile_rank);
-  cudaFree(r->tile_count);
-  cudaFree(r->tile_offset);
-  cudaFree(r->chunk_sum);
-  cudaFree(r->chunk_offset);
-  free_carriers(r->born);
-  free_carriers(r->c);
-  free_carriers(r->c_alt);
-  free_carriers(r->c_out);
-  cudaFree(r->c_keep);
-  cudaFree(r->gauss_node);
-  cudaFree(r->gauss_scratch);
-  cudaFree(r->d_ledger);
-  cudaFree(r->d_ledger_partial);
-  cudaFree(r->ledger_pre[0]);
-  cudaFree(r->ledger_pre[1]);
-  cudaFree(r->d_counters);
-  cudaFree(r->d_sums);
-  cudaFree(r->d_status);
-  cudaFree(r->scan_count);
-  cudaFree(r->scan_offset);
-  cudaFree(r->scan_total);
-  cudaFreeHost(r->h_sums_slots);
-  cudaFreeHost(r->h_stop);
-  cudaFree(r->d_stop);
-  cudaFree(r->inlet_rho);
-  cudaFreeHost(r->h_status);
-  cudaFreeHost(r->h_counters_slots);
-  cudaFreeHost(r->h_total);
+  for (double* d : singles) device_free(r, d);
+  device_free(r, r->slots.seen);
+  device_free(r, r->frozen1);
+  free_pending(r, r->queue.d);
+  device_free(r, r->action);
+  device_free(r, r->born_keep);
+  device_free(r, r->slot_order);
+  device_free(r, r->tile_of);
+  device_free(r, r->tile_rank);
+  device_free(r, r->tile_count);
+  device_free(r, r->tile_offset);
+  device_free(r, r->chunk_sum);
+  device_free(r, r->chunk_offset);
+  free_carriers(r, r->born);
+  free_carriers(r, r->c);
+  free_carriers(r, r->c_alt);
+  free_carriers(r, r->c_out);
+  device_free(r, r->c_keep);
+  device_free(r, r->gauss_node);
+  device_free(r, r->gauss_scratch);
+  device_free(r, r->d_ledger);
+  device_free(r, r->d_ledger_partial);
+  device_free(r, r->ledger_pre[0]);
+  device_free(r, r->ledger_pre[1]);
+  device_free(r, r->d_counters);
+  device_free(r, r->d_sums);
+  device_free(r, r->d_status);
+  device_free(r, r->scan_count);
+  device_free(r, r->scan_offset);
+  device_free(r, r->scan_total);
+  r->h_sums_slots = nullptr;
+  r->h_stop = nullptr;
+  device_free(r, r->d_stop);
+  device_free(r, r->inlet_rho);
+  r->h_status = nullptr;
+  r->h_counters_slots = nullptr;
+  r->h_total = nullptr;
+  pinned_give(r->pinned);
   delete r;
   return APRL_OK;
 }
@@ -1757,9 +1863,9 @@ aprl_status aprl_run_set_reference(aprl_run* r, unsigned a, const double* host, 
   if (count != n) return fail(APRL_ERR_INVALID_ARGUMENT, "Reference component size mismatch");
   if (host && !all_finite(host, n)) return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
   CUDA_TRY(cudaStreamSynchronize(r->stream));
-  cudaFree(r->ref[a]);
+  device_free(r, r->ref[a]);
   r->ref[a] = nullptr;
-  TRY(device_alloc(&r->ref[a], n));
+  TRY(device_alloc(r, &r->ref[a], n));
   if (host)
     CUDA_TRY(cudaMemcpy(r->ref[a], host, n * 8, cudaMemcpyHostToDevice));
   else
@@ -1978,7 +2084,7 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
     for (size_t j = 0; j < queued.size(); ++j) slot[insertion[due[j]]++] = j;
   }
   // Queue entries on the device, in due order.
-  free_pending(q.d);
+  free_pending(r, q.d);
   const size_t nq = queued.size();
   q.n = nq;
   q.cursor = 0;
@@ -1986,16 +2092,16 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
     double** qd[] = {&q.d.x, &q.d.y, &q.d.z, &q.d.ux, &q.d.uy, &q.d.uz, &q.d.q, &q.d.m};
     std::vector<double> t(nq);
     for (int k = 0; k < 8; ++k) {
-      TRY(device_alloc(qd[k], nq));
+      TRY(device_alloc(r, qd[k], nq));
       for (size_t s = 0; s < nq; ++s) t[s] = v[k][queued[slot[s]]];
       CUDA_TRY(cudaMemcpy(*qd[k], t.data(), nq * 8, cudaMemcpyHostToDevice));
     }
-    TRY(device_alloc(&q.d.beta, nq));
+    TRY(device_alloc(r, &q.d.beta, nq));
     for (size_t s = 0; s < nq; ++s) t[s] = beta[queued[slot[s]]];
     CUDA_TRY(cudaMemcpy(q.d.beta, t.data(), nq * 8, cudaMemcpyHostToDevice));
     std::vector<unsigned long long> qi(nq);
     for (size_t s = 0; s < nq; ++s) qi[s] = id[queued[slot[s]]];
-    TRY(device_alloc(&q.d.id, nq));
+    TRY(device_alloc(r, &q.d.id, nq));
     CUDA_TRY(cudaMemcpy(q.d.id, qi.data(), nq * 8, cudaMemcpyHostToDevice));
   }
   // The retained list, in order, with its held state.
@@ -2278,8 +2384,8 @@ static aprl_status sample_plane(aprl_run* r, double plane_lab_z, double* out, si
   axis(coordinate, c.nz + 1, &da.vertex_lower, &da.vertex_fraction);
   axis(coordinate - 0.5, c.nz, &da.half_lower, &da.half_fraction);
   if (r->detector_cap < count) {
-    cudaFree(r->d_detector);
-    TRY(device_alloc(&r->d_detector, count));
+    device_free(r, r->d_detector);
+    TRY(device_alloc(r, &r->d_detector, count));
     r->detector_cap = count;
   }
   da.out = r->d_detector;
@@ -2354,8 +2460,8 @@ aprl_status aprl_run_gauss_law(aprl_run* r, aprl_gauss_law* out, double* residua
   const size_t result_bytes = sizeof(DD) * 2;
   const size_t scratch_bytes = partial_bytes + result_bytes + 3 * sizeof(unsigned long long);
   if (!r->gauss_node) {
-    TRY(device_alloc(&r->gauss_node, nodes));
-    TRY(device_alloc(&r->gauss_scratch, scratch_bytes));
+    TRY(device_alloc(r, &r->gauss_node, nodes));
+    TRY(device_alloc(r, &r->gauss_scratch, scratch_bytes));
   }
   GaussArgs a{};
   a.g = make_grid<double>(r);
@@ -2413,17 +2519,18 @@ namespace {
 
 // Device buffers of one initial-field solve, released on every exit.
 struct SfBuffers {
+  aprl_run* r;
   double *slab[4] = {}, *rho = nullptr;
   DD *partial = nullptr, *out = nullptr;
   SfState* state = nullptr;
   unsigned long long* max_bits = nullptr;
   ~SfBuffers() {
-    for (double* p : slab) cudaFree(p);
-    cudaFree(rho);
-    cudaFree(partial);
-    cudaFree(out);
-    cudaFree(state);
-    cudaFree(max_bits);
+    for (double* p : slab) device_free(r, p);
+    device_free(r, rho);
+    device_free(r, partial);
+    device_free(r, out);
+    device_free(r, state);
+    device_free(r, max_bits);
   }
 };
 
@@ -2491,14 +2598,14 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
       1, std::min<size_t>(c.nz, (2 * kSelfFieldBlocks + gx * gy - 1) / (gx * gy)));
   const dim3 tile_grid(gx, gy, gz), tile_block(kSfTileX, kSfTileY);
   const int tblocks = (int)(gx * gy * gz);
-  SfBuffers buf;
-  for (int q = 0; q < 4; ++q) TRY(device_alloc(&buf.slab[q], slab));
-  TRY(device_alloc(&buf.rho, rho_count));
-  TRY(device_alloc(&buf.partial,
+  SfBuffers buf{r};
+  for (int q = 0; q < 4; ++q) TRY(device_alloc(r, &buf.slab[q], slab));
+  TRY(device_alloc(r, &buf.rho, rho_count));
+  TRY(device_alloc(r, &buf.partial,
                    std::max<size_t>((size_t)kSelfFieldBlocks * kMoments, 2 * (size_t)tblocks)));
-  TRY(device_alloc(&buf.out, 16));
-  TRY(device_alloc(&buf.state, 1));
-  TRY(device_alloc(&buf.max_bits, 1));
+  TRY(device_alloc(r, &buf.out, 16));
+  TRY(device_alloc(r, &buf.state, 1));
+  TRY(device_alloc(r, &buf.max_bits, 1));
   for (int q = 0; q < 4; ++q)
     CUDA_TRY(cudaMemsetAsync(buf.slab[q], 0, slab * sizeof(double), r->stream));
   CUDA_TRY(cudaMemsetAsync(buf.rho, 0, rho_count * sizeof(double), r->stream));
@@ -2793,9 +2900,9 @@ aprl_status aprl_run_prepare_reference(aprl_run* r, size_t n, const double* x, c
       s = fail(APRL_ERR_CUDA, "cudaStreamSynchronize failed");
       break;
     }
-    cudaFree(r->ref[a]);
+    device_free(r, r->ref[a]);
     r->ref[a] = nullptr;
-    s = device_alloc(&r->ref[a], count);
+    s = device_alloc(r, &r->ref[a], count);
     if (s != APRL_OK) break;
     // A fresh run's rings start at base 0: its fields are in native order.
     const cudaError_t e =

@@ -193,7 +193,15 @@ aprl_status aprl_cowan_coefficients(double dx, double dy, double dz,
  * ConservativeSourceCoupling construction (src/eb_field.cpp:211-229,
  * src/eb_cpml.cpp:296-372, src/moving_window_fields.cpp:327-360,
  * src/source_coupling.cpp:62-68).  `stream` is a cudaStream_t (NULL = the
- * legacy default stream).  Allocates all device state of the run. */
+ * legacy default stream).  Allocates all device state of the run.
+ *
+ * Device memory: every run draws from one stream-ordered memory pool per
+ * device owned by the library (cudaMallocFromPoolAsync on the run's stream).
+ * aprl_run_destroy returns the run's memory to that pool, and later runs
+ * reuse it without mapping new memory; up to 16 GiB of freed memory stays
+ * in the pool for the life of the process (the rest is released to the
+ * driver), so that memory is not available to other allocators in the
+ * process, such as a framework's caching allocator, while it is held. */
 aprl_status aprl_run_create(const aprl_run_config* config, void* stream,
                             aprl_run** out);
 aprl_status aprl_run_destroy(aprl_run* run);
