@@ -119,16 +119,43 @@ __device__ __forceinline__ double tile_smoothed(const ETile& t, const CowanArgs<
 template <class F>
 __device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int k, int slot,
                                            int i0, int j0) {
-  constexpr int W = kTX + 2, H = kTY + 2, N = W * H;
+  constexpr int W = kTX + 2, H = kTY + 2, N = W * H, T = kTX * kTY, R = (N + T - 1) / T;
+  const int tid = threadIdx.y * kTX + threadIdx.x;
+  // A tile whose rim lies inside every component's index range, on a plane
+  // inside every component's z range, needs none of electricValue's parity
+  // and halo rules: its values are read straight from E.
+  const bool interior = i0 >= 1 && i0 + kTX <= a.g.nx - 1 && j0 >= 1 &&
+                        j0 + kTY <= a.g.ny - 1 && k >= 0 && k < a.g.nz;
+  // All of a thread's loads are issued before any shared-memory store, so
+  // their latencies overlap instead of adding up.
+  double v[3][R];
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1);
-    for (int n = threadIdx.y * kTX + threadIdx.x; n < N; n += kTX * kTY) {
-      const int ii = n % W, jj = n / W;
-      const int i = i0 - 1 + ii, j = j0 - 1 + jj;
-      t.v[c][slot][jj][ii] = (i < -1 || i > nxc || j < -1 || j > nyc)
-                                 ? 0.0 : electric_value(a, c, i, j, k);
+    const int nxc = a.g.nx + (c != 0), nyc = a.g.ny + (c != 1), nzc = a.g.nz + (c != 2);
+    const double* plane =
+        interior ? a.e[c] + (size_t)ring(k, a.g.zb_e[c], nzc) * nyc * nxc : nullptr;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = tid + r * T;
+      double x = 0.0;
+      if (n < N) {
+        const int ii = n % W, jj = n / W;
+        const int i = i0 - 1 + ii, j = j0 - 1 + jj;
+        if (interior)
+          x = plane[(size_t)j * nxc + i];
+        else if (!(i < -1 || i > nxc || j < -1 || j > nyc))
+          x = electric_value(a, c, i, j, k);
+      }
+      v[c][r] = x;
     }
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = tid + r * T;
+      if (n < N) t.v[c][slot][n / W][n % W] = v[c][r];
+    }
 }
 
 template <class F>

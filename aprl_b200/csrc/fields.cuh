@@ -109,11 +109,15 @@ struct DetectorArgs {
 // Cowan kernel geometry: 32x8 column tiles, each block marching up to
 // kCowanChunk z planes (fewer on small grids, so that there are enough
 // blocks); APRL_COWAN_MIN_BLOCKS resident blocks per SM bound its registers.
+// Measured on the 128x128x512 dipole grid: 8 planes at 6 blocks per SM,
+// 0.47 ms, against 0.50 (16 at 5), 0.49 (16 at 6), 0.56-0.58 (32) and 0.47
+// (4 at 6): more, shorter marches hide the plane loads better than the two
+// halo planes per chunk cost.
 #ifndef APRL_COWAN_CHUNK
-#define APRL_COWAN_CHUNK 16
+#define APRL_COWAN_CHUNK 8
 #endif
 #ifndef APRL_COWAN_MIN_BLOCKS
-#define APRL_COWAN_MIN_BLOCKS 5
+#define APRL_COWAN_MIN_BLOCKS 6
 #endif
 constexpr int kCowanTileX = 32, kCowanTileY = 8, kCowanChunk = APRL_COWAN_CHUNK;
 template <class F> __global__ void cowan_magnetic_kernel(CowanArgs<F> a);

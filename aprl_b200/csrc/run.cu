@@ -1195,7 +1195,7 @@ aprl_status preview_electric_t(aprl_run* r) {
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
-  if (r->fp32) {  // B is final for the step: its binary32 copy for the gathers
+  if (r->fp32 && r->np) {  // B is final for the step: its binary32 copy for the gathers
     BShadowArgs sa{};
     size_t most = 0;
     for (int a = 0; a < 3; ++a) {
