@@ -237,6 +237,16 @@ __device__ __forceinline__ double bval(const GridT<F>& g, int c, int i, int j, i
 // the same B), PEC on the x/y faces, and the inlet Ex/Ey overwrite at k=0.
 // Reads E^n from e_old, writes E* to e_star.
 template <class F>
+__device__ __forceinline__ void preview_orbit(const PreviewArgs<F>& a, int c, size_t n,
+                                              double e_star, double e_old) {
+  // orbit_sum_kernel without current: S = W(E* + E^n), the same expression.
+  if (a.orbit_float)
+    static_cast<float*>(a.orbit[c])[n] = float(e_star + e_old);
+  else
+    static_cast<double*>(a.orbit[c])[n] = e_star + e_old;
+}
+
+template <class F>
 __global__ void electric_preview_kernel(PreviewArgs<F> a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -247,7 +257,8 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
   const double cx = curl / g.dx, cy = curl / g.dy, cz = curl / g.dz;
   if (i < g.nx) {  // Ex (nx, ny+1, nz+1)
     const size_t n = e_index(g, 0, i, j, k);
-    double v = g.e_old[0][n];
+    const double old = g.e_old[0][n];
+    double v = old;
     if (k >= 1 && k < g.nz && j >= 1 && j < g.ny)
       v += cy * (bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k)) -
            cz * (bval(g, 1, i, j, k) - bval(g, 1, i, j, k - 1));
@@ -265,10 +276,12 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       v = inlet_value(a.inlet, 0, i, j);
     }
     g.e_star[0][n] = v;
+    if (a.orbit[0]) preview_orbit(a, 0, n, v, old);
   }
   if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
     const size_t n = e_index(g, 1, i, j, k);
-    double v = g.e_old[1][n];
+    const double old = g.e_old[1][n];
+    double v = old;
     if (k >= 1 && k < g.nz && i >= 1 && i < g.nx)
       v += cz * (bval(g, 0, i, j, k) - bval(g, 0, i, j, k - 1)) -
            cx * (bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k));
@@ -286,10 +299,12 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       v = inlet_value(a.inlet, 1, i, j);
     }
     g.e_star[1][n] = v;
+    if (a.orbit[0]) preview_orbit(a, 1, n, v, old);
   }
   if (k < g.nz) {  // Ez (nx+1, ny+1, nz)
     const size_t n = e_index(g, 2, i, j, k);
-    double v = g.e_old[2][n];
+    const double old = g.e_old[2][n];
+    double v = old;
     const bool inner = i >= 1 && i < g.nx && j >= 1 && j < g.ny;
     if (inner)
       v += cx * (bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k)) -
@@ -310,6 +325,7 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
     }
     if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
     g.e_star[2][n] = v;
+    if (a.orbit[0]) preview_orbit(a, 2, n, v, old);
   }
 }
 

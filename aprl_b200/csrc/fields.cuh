@@ -60,6 +60,11 @@ struct PreviewArgs {
   CpmlHistory h[4];      // electric histories 6 (Ex,y) 9 (Ey,x) 10 (Ez,x) 11 (Ez,y)
   InletTable inlet;      // reference(a, i, j, offset, step+1)
   double* pre_inlet[2];  // when set: Ex, Ey of plane 0 before the inlet overwrite
+  // When set: the first trial's orbit sum S = E* + E^n (the current-free pass
+  // of orbit_sum_kernel), written here from the values already in hand;
+  // binary32 when orbit_float, else binary64.
+  void* orbit[3];
+  int orbit_float;
 };
 
 // ChargeMatchedInlet::complete (src/charge_matched_inlet.h:55-71): Ez of the

@@ -246,6 +246,8 @@ struct aprl_run {
   // skipped, which is most of a field-only step's work besides the field
   // updates.
   bool j_zero = true;
+  // The preview of this step wrote the current-free orbit sum.
+  bool orbit_from_preview = false;
   double* lower[3]{};
   // What the gathers read: the orbit sum S = E_new + E^n per E node (binary64,
   // or binary32 in the FP32-mixed mode) and, in that mode, a binary32 B.
@@ -1192,6 +1194,11 @@ aprl_status preview_electric_t(aprl_run* r) {
   pa.ey_prof = r->eprof[1].view();
   for (int h = 0; h < 4; ++h) pa.h[h] = r->hist[4 + h].view();
   for (int a = 0; a < 2; ++a) pa.pre_inlet[a] = r->ledger_on ? r->ledger_pre[a] : nullptr;
+  // With particles to gather, the first trial's current-free orbit sum is
+  // written by the preview itself (E* and E^n are in its registers there).
+  r->orbit_from_preview = r->np != 0;
+  for (int a = 0; a < 3; ++a) pa.orbit[a] = r->orbit_from_preview ? r->orbit[a] : nullptr;
+  pa.orbit_float = r->fp32 ? 1 : 0;
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
   const dim3 block(32, 4);
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
@@ -1349,8 +1356,9 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     }
     const dim3 oblock(32, 4);
     if (r->trials == 0) {
-      TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
-                 orbit[1], orbit[2], 0));
+      if (!r->orbit_from_preview)
+        TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
+                   orbit[1], orbit[2], 0));
       TRY(launch(r, kGuessGather,
                  binomial ? guess_gather_kernel<W, F, 0> : guess_gather_kernel<W, F, 1>,
                  dim3(blocks_for(r->np, 128)),
