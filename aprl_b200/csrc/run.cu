@@ -415,6 +415,22 @@ void device_free(aprl_run* r, void* p) {
   if (p) cudaFreeAsync(p, r->stream);
 }
 
+// Every copy and fill of a run goes through the run's stream.  A plain
+// cudaMemcpy or cudaMemset runs on the legacy default stream, which the
+// run's (possibly non-blocking) stream does not wait for, and returns before
+// a device-to-device copy or a fill is done; a stream-ordered free of the
+// source right after it could then hand the block to another run while the
+// copy still reads it.  A copy returns once it has completed, as its callers
+// expect (host buffers are reused or read right after).
+cudaError_t run_copy(aprl_run* r, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  return e;
+}
+cudaError_t run_fill(aprl_run* r, void* dst, int value, size_t bytes) {
+  return cudaMemsetAsync(dst, value, bytes, r->stream);
+}
+
 // Page-locked 4 KiB blocks for the runs' small read-back areas, kept for
 // reuse (cudaMallocHost/cudaFreeHost per run cost milliseconds each).
 constexpr size_t kPinnedBlock = 4096;
@@ -737,18 +753,18 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   DParticles np{};
   TRY(alloc_particles(r, np, n));
   if (r->np) {
-    CUDA_TRY(cudaMemcpy(np.x, r->p.x, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.y, r->p.y, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.z, r->p.z, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.ux, r->p.ux, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.uy, r->p.uy, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.uz, r->p.uz, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.q, r->p.q, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.m, r->p.m, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.id, r->p.id, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.frozen, r->p.frozen, r->np, cudaMemcpyDeviceToDevice));
-    CUDA_TRY(cudaMemcpy(np.beta, r->p.beta, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.x, r->p.x, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.y, r->p.y, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.z, r->p.z, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.ux, r->p.ux, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.uy, r->p.uy, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.uz, r->p.uz, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.q, r->p.q, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.m, r->p.m, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.id, r->p.id, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.order, r->p.order, r->np * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.frozen, r->p.frozen, r->np, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, np.beta, r->p.beta, r->np * 8, cudaMemcpyDeviceToDevice));
   }
   free_particles(r, r->p);
   free_particles(r, r->p_alt);
@@ -786,13 +802,13 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   return ensure_scan(r, n);
 }
 
-aprl_status copy_carriers(DCarriers& dst, const DCarriers& src, size_t n) {
+aprl_status copy_carriers(aprl_run* r, DCarriers& dst, const DCarriers& src, size_t n) {
   if (!n) return APRL_OK;
   const double* s[] = {src.px, src.py, src.pz, src.vx, src.vy, src.vz, src.q, src.w};
   double* d[] = {dst.px, dst.py, dst.pz, dst.vx, dst.vy, dst.vz, dst.q, dst.w};
   for (int k = 0; k < 8; ++k)
-    CUDA_TRY(cudaMemcpy(d[k], s[k], n * 8, cudaMemcpyDeviceToDevice));
-  CUDA_TRY(cudaMemcpy(dst.key, src.key, n * 8, cudaMemcpyDeviceToDevice));
+    CUDA_TRY(run_copy(r, d[k], s[k], n * 8, cudaMemcpyDeviceToDevice));
+  CUDA_TRY(run_copy(r, dst.key, src.key, n * 8, cudaMemcpyDeviceToDevice));
   return APRL_OK;
 }
 
@@ -811,9 +827,9 @@ aprl_status reserve_carriers(aprl_run* r, size_t n) {
   TRY(alloc_carriers(r, nc, n));
   TRY(alloc_carriers(r, nout, n));
   TRY(device_alloc(r, &nkeep, n));
-  TRY(copy_carriers(nc, r->c, r->nc));
-  TRY(copy_carriers(nout, r->c_out, r->nc));
-  if (r->nc) CUDA_TRY(cudaMemcpy(nkeep, r->c_keep, r->nc, cudaMemcpyDeviceToDevice));
+  TRY(copy_carriers(r, nc, r->c, r->nc));
+  TRY(copy_carriers(r, nout, r->c_out, r->nc));
+  if (r->nc) CUDA_TRY(run_copy(r, nkeep, r->c_keep, r->nc, cudaMemcpyDeviceToDevice));
   free_carriers(r, r->c);
   free_carriers(r, r->c_alt);
   free_carriers(r, r->c_out);
@@ -1713,10 +1729,10 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
       if ((s = device_alloc(r, &dp.decay, n)) != APRL_OK) return cleanup(s);
       if ((s = device_alloc(r, &dp.drive, n)) != APRL_OK) return cleanup(s);
       if ((s = device_alloc(r, &dp.ordinal, n)) != APRL_OK) return cleanup(s);
-      cudaMemcpy(dp.ikm1, hp.ikm1.data(), n * 8, cudaMemcpyHostToDevice);
-      cudaMemcpy(dp.decay, hp.decay.data(), n * 8, cudaMemcpyHostToDevice);
-      cudaMemcpy(dp.drive, hp.drive.data(), n * 8, cudaMemcpyHostToDevice);
-      cudaMemcpy(dp.ordinal, hp.ordinal.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+      run_copy(r, dp.ikm1, hp.ikm1.data(), n * 8, cudaMemcpyHostToDevice);
+      run_copy(r, dp.decay, hp.decay.data(), n * 8, cudaMemcpyHostToDevice);
+      run_copy(r, dp.drive, hp.drive.data(), n * 8, cudaMemcpyHostToDevice);
+      run_copy(r, dp.ordinal, hp.ordinal.data(), n * sizeof(int), cudaMemcpyHostToDevice);
       dp.active = hp.active;
     }
   }
@@ -1875,9 +1891,9 @@ aprl_status aprl_run_set_reference(aprl_run* r, unsigned a, const double* host, 
   r->ref[a] = nullptr;
   TRY(device_alloc(r, &r->ref[a], n));
   if (host)
-    CUDA_TRY(cudaMemcpy(r->ref[a], host, n * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, r->ref[a], host, n * 8, cudaMemcpyHostToDevice));
   else
-    CUDA_TRY(cudaMemset(r->ref[a], 0, n * 8));
+    CUDA_TRY(run_fill(r, r->ref[a], 0, n * 8));
   r->ref_set[a] = true;
   return APRL_OK;
 }
@@ -1979,14 +1995,14 @@ aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const
   const double* src[] = {x, y, z, ux, uy, uz, q, m};
   double* dst[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
   for (int k = 0; k < 8; ++k)
-    CUDA_TRY(cudaMemcpy(dst[k], src[k], n * 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(r->p.id, id, n * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, dst[k], src[k], n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(run_copy(r, r->p.id, id, n * 8, cudaMemcpyHostToDevice));
   std::vector<unsigned long long> order(n);
   for (size_t i = 0; i < n; ++i) order[i] = i;
-  if (n) CUDA_TRY(cudaMemcpy(r->p.order, order.data(), n * 8, cudaMemcpyHostToDevice));
+  if (n) CUDA_TRY(run_copy(r, r->p.order, order.data(), n * 8, cudaMemcpyHostToDevice));
   if (n) {
-    CUDA_TRY(cudaMemset(r->p.frozen, 0, n));
-    CUDA_TRY(cudaMemset(r->p.beta, 0, n * 8));
+    CUDA_TRY(run_fill(r, r->p.frozen, 0, n));
+    CUDA_TRY(run_fill(r, r->p.beta, 0, n * 8));
   }
   r->next_order = n;
   r->np = n;
@@ -2007,7 +2023,7 @@ aprl_status aprl_run_particle_count(const aprl_run* r, size_t* count) {
 static aprl_status storage_permutation(aprl_run* r, const unsigned long long* device_order,
                                        size_t n, std::vector<size_t>& perm) {
   std::vector<unsigned long long> order(n);
-  if (n) CUDA_TRY(cudaMemcpy(order.data(), device_order, n * 8, cudaMemcpyDeviceToHost));
+  if (n) CUDA_TRY(run_copy(r, order.data(), device_order, n * 8, cudaMemcpyDeviceToHost));
   perm.resize(n);
   for (size_t i = 0; i < n; ++i) perm[i] = i;
   std::sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return order[a] < order[b]; });
@@ -2028,12 +2044,12 @@ aprl_status aprl_run_get_particles(aprl_run* r, size_t capacity, double* x, doub
   const double* src[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
   for (int k = 0; k < 8; ++k) {
     if (!dst[k] || !n) continue;
-    CUDA_TRY(cudaMemcpy(t.data(), src[k], n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, t.data(), src[k], n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) dst[k][i] = t[perm[i]];
   }
   if (id && n) {
     std::vector<uint64_t> ids(n);
-    CUDA_TRY(cudaMemcpy(ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) id[i] = ids[perm[i]];
   }
   *count = n;
@@ -2062,12 +2078,12 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
   const double* dsrc[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
   for (int k = 0; k < 8; ++k) {
     std::vector<double> t(n);
-    if (n) CUDA_TRY(cudaMemcpy(t.data(), dsrc[k], n * 8, cudaMemcpyDeviceToHost));
+    if (n) CUDA_TRY(run_copy(r, t.data(), dsrc[k], n * 8, cudaMemcpyDeviceToHost));
     v[k].resize(n);
     for (size_t i = 0; i < n; ++i) v[k][i] = t[perm[i]];
   }
   std::vector<unsigned long long> ids(n), id(n);
-  if (n) CUDA_TRY(cudaMemcpy(ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
+  if (n) CUDA_TRY(run_copy(r, ids.data(), r->p.id, n * 8, cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < n; ++i) id[i] = ids[perm[i]];
   // PendingParticleQueue::extract (src/pending_particle_queue.cpp:128-154).
   const size_t buckets = static_cast<size_t>(q.maximum_step - q.initial_step + 2);
@@ -2102,15 +2118,15 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
     for (int k = 0; k < 8; ++k) {
       TRY(device_alloc(r, qd[k], nq));
       for (size_t s = 0; s < nq; ++s) t[s] = v[k][queued[slot[s]]];
-      CUDA_TRY(cudaMemcpy(*qd[k], t.data(), nq * 8, cudaMemcpyHostToDevice));
+      CUDA_TRY(run_copy(r, *qd[k], t.data(), nq * 8, cudaMemcpyHostToDevice));
     }
     TRY(device_alloc(r, &q.d.beta, nq));
     for (size_t s = 0; s < nq; ++s) t[s] = beta[queued[slot[s]]];
-    CUDA_TRY(cudaMemcpy(q.d.beta, t.data(), nq * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, q.d.beta, t.data(), nq * 8, cudaMemcpyHostToDevice));
     std::vector<unsigned long long> qi(nq);
     for (size_t s = 0; s < nq; ++s) qi[s] = id[queued[slot[s]]];
     TRY(device_alloc(r, &q.d.id, nq));
-    CUDA_TRY(cudaMemcpy(q.d.id, qi.data(), nq * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, q.d.id, qi.data(), nq * 8, cudaMemcpyHostToDevice));
   }
   // The retained list, in order, with its held state.
   const size_t nk = kept.size();
@@ -2119,10 +2135,10 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
     std::vector<double> t(nk);
     for (int k = 0; k < 8; ++k) {
       for (size_t s = 0; s < nk; ++s) t[s] = v[k][kept[s]];
-      CUDA_TRY(cudaMemcpy(pd[k], t.data(), nk * 8, cudaMemcpyHostToDevice));
+      CUDA_TRY(run_copy(r, pd[k], t.data(), nk * 8, cudaMemcpyHostToDevice));
     }
     for (size_t s = 0; s < nk; ++s) t[s] = beta[kept[s]];
-    CUDA_TRY(cudaMemcpy(r->p.beta, t.data(), nk * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, r->p.beta, t.data(), nk * 8, cudaMemcpyHostToDevice));
     std::vector<unsigned long long> ki(nk), ko(nk);
     std::vector<unsigned char> kf(nk);
     uint64_t held = 0;
@@ -2132,9 +2148,9 @@ aprl_status aprl_run_set_held(aprl_run* r, size_t n, const uint8_t* frozen, cons
       kf[s] = frozen[kept[s]] ? 1 : 0;
       held += kf[s];
     }
-    CUDA_TRY(cudaMemcpy(r->p.id, ki.data(), nk * 8, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(r->p.order, ko.data(), nk * 8, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(r->p.frozen, kf.data(), nk, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, r->p.id, ki.data(), nk * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, r->p.order, ko.data(), nk * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, r->p.frozen, kf.data(), nk, cudaMemcpyHostToDevice));
     r->held = held;
   } else {
     r->held = 0;
@@ -2158,12 +2174,12 @@ aprl_status aprl_run_get_held(aprl_run* r, size_t capacity, uint8_t* frozen, dou
   TRY(storage_permutation(r, r->p.order, n, perm));
   if (frozen && n) {
     std::vector<unsigned char> f(n);
-    CUDA_TRY(cudaMemcpy(f.data(), r->p.frozen, n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, f.data(), r->p.frozen, n, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) frozen[i] = f[perm[i]];
   }
   if (beta && n) {
     std::vector<double> b(n);
-    CUDA_TRY(cudaMemcpy(b.data(), r->p.beta, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, b.data(), r->p.beta, n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) beta[i] = b[perm[i]];
   }
   *count = n;
@@ -2189,14 +2205,14 @@ aprl_status aprl_run_get_carriers(aprl_run* r, size_t capacity, double* pos, dou
   for (int k = 0; k < 6; ++k) {
     double* dst = k < 3 ? pos : vel;
     if (!dst || !n) continue;
-    CUDA_TRY(cudaMemcpy(t.data(), comps[k], n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, t.data(), comps[k], n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) dst[3 * i + (k % 3)] = t[perm[i]];
   }
   double* scalars[] = {q, w};
   const double* ssrc[] = {r->c.q, r->c.w};
   for (int k = 0; k < 2; ++k) {
     if (!scalars[k] || !n) continue;
-    CUDA_TRY(cudaMemcpy(t.data(), ssrc[k], n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, t.data(), ssrc[k], n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) scalars[k][i] = t[perm[i]];
   }
   *count = n;
@@ -2213,13 +2229,13 @@ aprl_status aprl_run_set_carriers(aprl_run* r, size_t n, const double* pos, cons
   for (int k = 0; k < 6; ++k) {
     const double* src = k < 3 ? pos : vel;
     for (size_t i = 0; i < n; ++i) t[i] = src[3 * i + (k % 3)];
-    if (n) CUDA_TRY(cudaMemcpy(comps[k], t.data(), n * 8, cudaMemcpyHostToDevice));
+    if (n) CUDA_TRY(run_copy(r, comps[k], t.data(), n * 8, cudaMemcpyHostToDevice));
   }
-  if (n) CUDA_TRY(cudaMemcpy(r->c.q, q, n * 8, cudaMemcpyHostToDevice));
-  if (n) CUDA_TRY(cudaMemcpy(r->c.w, w, n * 8, cudaMemcpyHostToDevice));
+  if (n) CUDA_TRY(run_copy(r, r->c.q, q, n * 8, cudaMemcpyHostToDevice));
+  if (n) CUDA_TRY(run_copy(r, r->c.w, w, n * 8, cudaMemcpyHostToDevice));
   std::vector<unsigned long long> keys(n);
   for (size_t i = 0; i < n; ++i) keys[i] = i;
-  if (n) CUDA_TRY(cudaMemcpy(r->c.key, keys.data(), n * 8, cudaMemcpyHostToDevice));
+  if (n) CUDA_TRY(run_copy(r, r->c.key, keys.data(), n * 8, cudaMemcpyHostToDevice));
   r->nc = n;
   return APRL_OK;
 }
@@ -2355,7 +2371,7 @@ aprl_status aprl_run_get_slot_fields(aprl_run* r, size_t capacity, double* used_
   const double* src[] = {r->used_e, r->used_b, r->next_e, r->next_b};
   for (int k = 0; k < 4; ++k) {
     if (!dst[k] || !n) continue;
-    CUDA_TRY(cudaMemcpy(t.data(), src[k], 3 * n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(run_copy(r, t.data(), src[k], 3 * n * 8, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i)
       for (int d = 0; d < 3; ++d) dst[k][3 * i + d] = t[3 * perm[i] + d];
   }
@@ -2844,7 +2860,7 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   TRY(sf_read(r, buf.out, sums, 2));
   TRY(check_device(r));
   unsigned long long worst_bits = 0;
-  CUDA_TRY(cudaMemcpy(&worst_bits, buf.max_bits, sizeof worst_bits, cudaMemcpyDeviceToHost));
+  CUDA_TRY(run_copy(r, &worst_bits, buf.max_bits, sizeof worst_bits, cudaMemcpyDeviceToHost));
   double worst;
   std::memcpy(&worst, &worst_bits, sizeof worst);
   const long double res2 = sf_long(sums[0]), src2 = sf_long(sums[1]);

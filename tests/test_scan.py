@@ -127,3 +127,37 @@ def test_request_larger_than_budget_is_refused():
         scan.submit(w.config, w.particles, STEPS)
     scan.close()
     assert err.value.status == abi.APRL_ERR_OUT_OF_RANGE
+
+
+@pytest.mark.gpu
+def test_runs_growing_their_lists_beside_each_other_stay_intact():
+    """Sixteen requests, four at a time, three times over, whose carrier
+    lists outgrow their first reservation mid-run (up to ~12k carriers)
+    while other runs are created and destroyed beside them.  A run's memory
+    comes from a pool shared by all runs, and a list that grows is copied
+    and its old storage freed in the run's stream order; a copy issued
+    outside that order (on the legacy default stream) once let another run
+    take the old storage while it was still being read, which corrupted
+    particles and carriers ("Active particle fell behind moving inlet",
+    "Invalid CPML carrier current weight").  Every request must finish, and
+    every repetition must give the same detector plane."""
+    steps = 40
+    ws = [workloads.scan_draw(i, seed=11, steps=steps, precision="fp32-mixed",
+                              cells_min=(40, 40, 48), cells_max=(72, 72, 128),
+                              particles_range=(2.0e4, 1.5e5)) for i in range(16)]
+    planes = []
+    for _ in range(3):
+        scan = native.Scan(native.load(), slots=4)
+        tickets = [scan.submit(w.config, w.particles, steps,
+                               detector_lab_z=workloads.detector_plane_lab_z(w.config))
+                   for w in ws]
+        results = [scan.wait(t) for t in tickets]
+        scan.close()
+        for r in results:
+            assert r["status"] == abi.APRL_OK, r["message"]
+        planes.append([r["detector"] for r in results])
+    assert max(r["stats"]["carriers"] for r in results) > 4096   # the lists did grow
+    for later in planes[1:]:
+        for a, b in zip(later, planes[0]):
+            if b is not None:
+                assert rel_l2(a, b) <= 1e-6
