@@ -109,6 +109,45 @@ def test_detector_plane_matches_oracle():
     assert checkers.max_relative(dg, do) <= RTOL
 
 
+def test_field_only_steps_match_oracle():
+    """Steps without particles or carriers deposit no current: the run keeps
+    J known to be zero and skips its clears and the commit's pass over J.
+    The fields must still follow the oracle to the step-level FP64 bound the
+    other step tests use (after five steps about one plane of Ex differs in
+    the last bits, up to 1e-13 relative), and J stays zero."""
+    w = workloads.small_case(steps=5)
+    w.particles = {k: v[:0] for k, v in w.particles.items()}
+    g, o = gpu_run(w), checkers.run(checkers.oracle(), w)
+    g.step(5)
+    o.step(5)
+    for a in range(6):
+        assert checkers.max_relative(g.get_field(a), o.get_field(a)) <= RTOL, a
+    for a in range(6, 9):
+        assert not np.any(g.get_field(a))
+    assert g.stats()["particles"] == o.stats()["particles"] == 0
+
+
+def test_steps_after_the_particles_are_removed_match_oracle():
+    """A bunch deposits current for three steps, then the particle list is
+    emptied (carriers too): the next step clears the leftover J once at its
+    start and the steps after it skip the clears and the commit."""
+    w = workloads.small_case(nx=32, ny=24, nz=80, particles=4000, steps=8,
+                             z_fraction=(0.02, 0.99), margin_cells=1)
+    g, o = gpu_run(w), checkers.run(checkers.oracle(), w)
+    g.step(3)
+    o.step(3)
+    empty = {k: v[:0] for k, v in w.particles.items()}
+    g.set_particles(empty)
+    o.set_particles(empty)
+    g.step(4)
+    o.step(4)
+    for a in range(6):
+        assert checkers.max_relative(g.get_field(a), o.get_field(a)) <= RTOL, a
+    for a in range(6, 9):   # J of the last step: zero everywhere
+        assert not np.any(g.get_field(a))
+        assert not np.any(o.get_field(a))
+
+
 def test_async_detector_planes_complete_at_the_next_step():
     """aprl_run_sample_field_plane_async into two page-locked buffers: step
     n's plane, read after step n+1 returned (whose trial read-back waits for
