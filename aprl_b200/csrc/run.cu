@@ -59,7 +59,7 @@ enum Kernel : unsigned {
   kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
   kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
   kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict,
-  kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfAlpha, kSfUpdate, kSfBeta,
+  kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfUpdate,
   kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
   kInletHalo, kInletCharge, kInletComplete, kKernelCount
 };
@@ -73,7 +73,7 @@ const char* kKernelNames[kKernelCount] = {
   "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
   "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish", "trial_clear",
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
-  "sf_alpha", "sf_update", "sf_beta", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
+  "sf_update", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
   "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete"};
 
 const char* device_error_text(unsigned code) {
@@ -2805,10 +2805,9 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   while (issued < cfg->maximum_iterations) {
     const uint64_t batch = std::min<uint64_t>(32, cfg->maximum_iterations - issued);
     for (uint64_t it = 0; it < batch; ++it) {
+      // alpha and beta are formed by the last block of apply and of update.
       TRY(launch(r, kSfApply, sf_apply_kernel, tile_grid, tile_block, A));
-      TRY(launch(r, kSfAlpha, sf_alpha_kernel, dim3(1), dim3(kSelfFieldThreads), A, tblocks));
       TRY(launch(r, kSfUpdate, sf_update_kernel, tile_grid, tile_block, A));
-      TRY(launch(r, kSfBeta, sf_beta_kernel, dim3(1), dim3(kSelfFieldThreads), A, tblocks));
       TRY(launch(r, kSfDirection, sf_direction_kernel, tile_grid, tile_block, A));
     }
     issued += batch;

@@ -65,6 +65,37 @@ __device__ __forceinline__ int sf_block_index() {
 }
 __device__ __forceinline__ bool sf_first_thread() { return threadIdx.x == 0 && threadIdx.y == 0; }
 
+// Called by every thread of a block after its first thread has stored the
+// block's partial: true in the one block of the launch that arrives last,
+// when every block's partial is in memory (each first thread fences its
+// store before it counts itself).  That block resets the count for the next
+// launch.  No block waits on another.
+__device__ __forceinline__ bool sf_last_block(const SfArgs& a) {
+  __shared__ int last;
+  if (sf_first_thread()) {
+    __threadfence();
+    const unsigned blocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned before = atomicAdd(&a.state->arrivals, 1u);
+    last = before == blocks - 1;
+    if (last) a.state->arrivals = 0;
+  }
+  __syncthreads();
+  return last != 0;
+}
+
+// The sum of the launch's per-block partials in a fixed order (thread t adds
+// partials t, t + 128, ..., then the block tree), read through L2 since other
+// blocks of this launch wrote them.
+__device__ DD sf_partials_sum(const SfArgs& a, DD* shared) {
+  const int blocks = (int)(gridDim.x * gridDim.y * gridDim.z);
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  const double* words = reinterpret_cast<const double*>(a.partial);
+  DD s{0., 0.};
+  for (int b = t; b < blocks; b += kSelfFieldThreads)
+    s = dd_add(s, DD{__ldcg(words + 2 * b), __ldcg(words + 2 * b + 1)});
+  return sf_block_sum(s, shared);
+}
+
 }  // namespace
 
 // Host helpers.
@@ -218,16 +249,10 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_apply_kernel(SfArgs a) {
     }
   dot = sf_block_sum(dot, shared);
   if (sf_first_thread()) a.partial[sf_block_index()] = dot;
-}
-
-// alpha = |r|^2 / (d . A d), rounded once to binary64.
-__global__ void __launch_bounds__(kSelfFieldThreads) sf_alpha_kernel(SfArgs a, int blocks) {
-  __shared__ DD shared[kSelfFieldThreads];
-  if (sf_stopped(a)) return;
-  DD s{0., 0.};
-  for (int b = threadIdx.x; b < blocks; b += kSelfFieldThreads) s = dd_add(s, a.partial[b]);
-  s = sf_block_sum(s, shared);
-  if (threadIdx.x != 0) return;
+  if (!sf_last_block(a)) return;
+  // The last block: alpha = |r|^2 / (d . A d), rounded once to binary64.
+  const DD s = sf_partials_sum(a, shared);
+  if (!sf_first_thread()) return;
   SfState& st = *a.state;
   st.denominator = s;
   if (!(s.hi > 0.) || !isfinite(s.hi)) {
@@ -256,17 +281,11 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_update_kernel(SfArgs a) 
     }
   dot = sf_block_sum(dot, shared);
   if (sf_first_thread()) a.partial[sf_block_index()] = dot;
-}
-
-// The relative residual, the stopping test and beta
-// (src/eb_initial_field.cpp:1046-1064).
-__global__ void __launch_bounds__(kSelfFieldThreads) sf_beta_kernel(SfArgs a, int blocks) {
-  __shared__ DD shared[kSelfFieldThreads];
-  if (sf_stopped(a)) return;
-  DD s{0., 0.};
-  for (int b = threadIdx.x; b < blocks; b += kSelfFieldThreads) s = dd_add(s, a.partial[b]);
-  s = sf_block_sum(s, shared);
-  if (threadIdx.x != 0) return;
+  if (!sf_last_block(a)) return;
+  // The last block: the relative residual, the stopping test and beta
+  // (src/eb_initial_field.cpp:1046-1064).
+  const DD s = sf_partials_sum(a, shared);
+  if (!sf_first_thread()) return;
   SfState& st = *a.state;
   st.next = s;
   st.iterations += 1;

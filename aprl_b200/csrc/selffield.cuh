@@ -36,6 +36,9 @@ struct SfState {
   double alpha, beta, relative;
   unsigned long long iterations;
   int done;                     // 1 converged, 2 lost positive definiteness, 3 non-finite
+  // Blocks of the running apply or update launch that have written their
+  // partial; the last one to arrive forms alpha or beta and resets it to 0.
+  unsigned int arrivals;
 };
 
 struct SfArgs {
@@ -73,10 +76,11 @@ __global__ void sf_finish_kernel(const DD* partial, int blocks, int quantities, 
 __global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly, int pad,
                                   DeviceStatus* status);
 __global__ void sf_source_kernel(SfArgs a, DD volume);
+// One CG iteration is three launches: apply (its last block forms alpha),
+// update (its last block forms the relative residual, the stopping test and
+// beta) and direction.
 __global__ void sf_apply_kernel(SfArgs a);
-__global__ void sf_alpha_kernel(SfArgs a, int blocks);
 __global__ void sf_update_kernel(SfArgs a);
-__global__ void sf_beta_kernel(SfArgs a, int blocks);
 __global__ void sf_direction_kernel(SfArgs a);
 __global__ void sf_smooth_kernel(SfArgs a, int axis);
 __global__ void sf_electric_kernel(SfArgs a, int axis, double coefficient, int from_smoothed);
