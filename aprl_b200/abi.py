@@ -89,7 +89,18 @@ class RunConfig(C.Structure):
         ("n_magnets", C.c_uint32),
         ("inlet_charge_match", C.c_uint32),
         ("magnets", Magnet * MAX_MAGNETS),
+        ("deterministic", C.c_uint32),
+        ("reserved_flags", C.c_uint32),
     ]
+
+    @classmethod
+    def from_bytes(cls, raw):
+        """A config from its raw bytes; fields appended after an older layout
+        was written (the deterministic flag) read as zero."""
+        raw = bytes(raw)
+        if len(raw) < C.sizeof(cls):
+            raw = raw + bytes(C.sizeof(cls) - len(raw))
+        return cls.from_buffer_copy(raw)
 
 
 class StepStats(C.Structure):

@@ -58,29 +58,11 @@ def build(force=False, verbose=True):
     return OUTPUT
 
 
-PROBE_SOURCE = os.path.join(CSRC, "probe.cu")
-PROBE_OUTPUT = os.path.join(HERE, "libaprl_probe.so")
-
-
-def build_probe(force=False, verbose=True):
-    """The benchmark's measurement probe (libaprl_probe.so)."""
-    if (not force and os.path.exists(PROBE_OUTPUT) and
-            os.path.getmtime(PROBE_SOURCE) <= os.path.getmtime(PROBE_OUTPUT)):
-        return PROBE_OUTPUT
-    cmd = [nvcc(), "-shared", "-o", PROBE_OUTPUT, PROBE_SOURCE, "-std=c++17", "-O3",
-           "-Xcompiler", "-fPIC"] + ARCH
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.check_call(cmd)
-    return PROBE_OUTPUT
-
-
 def main(argv=None):
     parser = argparse.ArgumentParser()
     parser.add_argument("--force", action="store_true")
     args = parser.parse_args(argv)
     build(force=args.force)
-    build_probe(force=args.force)
 
 
 if __name__ == "__main__":

@@ -54,6 +54,7 @@ enum DeviceError : unsigned {
   kErrHeldBoundary = 19,      // held segment crossed a particle boundary
   kErrInletSource = 20,       // non-finite charge-matched inlet source
   kErrInletField = 21,        // non-finite charge-matched inlet field
+  kErrFixedRange = 22,        // deterministic deposit: contribution beyond the fixed-point range
   kErrCount
 };
 
@@ -98,6 +99,11 @@ struct GridT {
   int zb_e[3];           // ring bases of Ex Ey Ez
   int zb_b[3];           // ring bases of Bx By Bz
   F jcoef;               // (-1*dt)/eps0, applyCurrentSource(-1) scale
+  // Deterministic mode: the deposit adds into these (lo, hi) word pairs
+  // (fixed_add, scale jq_scale) instead of J, and a conversion pass writes J
+  // from them once per trial.  Null in the default mode.
+  unsigned long long* jq[3];
+  double jq_scale;
   // Set for the kernels of a fixed-point trial issued ahead of the verdict
   // on the previous one: nonzero once an earlier trial of the step has
   // converged, and the trial's kernels then return at once.
@@ -163,6 +169,62 @@ __device__ __forceinline__ F e_candidate(const GridT<F>& g, int c, int i, int j,
     if (jc != F(0.)) v += g.jcoef * jc;
   }
   return v;
+}
+
+// ---------------------------------------------------------------------------
+// Order-free summation of binary64 contributions (the deterministic mode).
+// A contribution v becomes the integer n = round(v * scale), |n| < 2^62,
+// split into lo = n mod 2^32 (0 <= lo < 2^32) and hi = floor(n / 2^32), and
+// both parts are added with 64-bit integer reductions into a (lo, hi) word
+// pair.  Integer addition is associative, so after any interleaving of the
+// adds the pair holds the exact sum of the rounded contributions,
+// hi * 2^32 + lo (hi two's complement), and so does every other run: the
+// pair's value does not depend on the order of the adds.  lo stays below
+// 2^64 for fewer than 2^32 adds and hi below 2^63 in magnitude for fewer
+// than 2^33.  `scale` is a power of two chosen by the host so that the
+// largest contribution a run can make maps below 2^62.
+constexpr double kFixedLimit = 4611686018427387904.0;  // 2^62
+
+// Returns false (and adds nothing) for a value outside the range.
+__device__ __forceinline__ bool fixed_add(unsigned long long* pair, double v, double scale) {
+  const double s = v * scale;
+  if (!(fabs(s) < kFixedLimit)) return false;
+  const long long n = __double2ll_rn(s);
+  const unsigned long long lo = (unsigned long long)n & 0xffffffffull;
+  const long long hi = n >> 32;
+  if (lo) atomicAdd(&pair[0], lo);
+  if (hi) atomicAdd(&pair[1], (unsigned long long)hi);
+  return true;
+}
+
+// The pair's value hi * 2^32 + lo, rounded once to binary64 and multiplied
+// by `unscale` (1/scale, a power of two, so that product is exact).
+__device__ __forceinline__ double fixed_value(unsigned long long lo, unsigned long long hi_word,
+                                              double unscale) {
+  const long long hi = (long long)hi_word;
+  // 128-bit two's complement (vh:vl) = hi * 2^32 + lo.
+  const unsigned long long shifted = (unsigned long long)hi << 32;
+  unsigned long long vl = shifted + lo;
+  long long vh = (hi >> 32) + (vl < shifted ? 1 : 0);
+  const bool negative = vh < 0;
+  unsigned long long mh = (unsigned long long)vh, ml = vl;
+  if (negative) {  // magnitude: two's complement negation of the 128-bit value
+    ml = ~ml + 1ull;
+    mh = ~mh + (ml == 0ull ? 1ull : 0ull);
+  }
+  double m;
+  if (mh == 0ull) {
+    m = __ull2double_rn(ml);
+  } else {
+    // The leading 64 bits, with every bit below them folded into bit 0 (a
+    // sticky bit under the 11 bits the conversion drops), round once.
+    const int lz = __clzll((long long)mh);
+    unsigned long long top = lz ? (mh << lz) | (ml >> (64 - lz)) : mh;
+    const unsigned long long rest = lz ? ml << lz : ml;
+    top |= rest != 0ull ? 1ull : 0ull;
+    m = ldexp(__ull2double_rn(top), 64 - lz);
+  }
+  return (negative ? -m : m) * unscale;
 }
 
 // BoostFrameTransform::gammaFromProperVelocity (src/boostframe.cpp:74-87).

@@ -604,7 +604,9 @@ __device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g,
 
 // ---------------------------------------------------------------------------
 // deposition: Current::deposit at one rank (src/longitudinal_shape.h:175-187)
-template <class F>
+// Q: the deterministic mode's fixed-point sum (fixed_add into G.jq) instead
+// of binary64 atomics into J.
+template <class F, bool Q>
 struct DepositVisitor {
   static constexpr bool kF3Segment = false;
   static constexpr bool kQuinticSummed = true;
@@ -625,15 +627,21 @@ struct DepositVisitor {
       return;
     }
     if (k < 0 || k >= e_nz(G, a)) return;
-    atomicAdd(&G.j[a][j_index(G, a, (int)i, (int)j, (int)k)], scale[a] * w);
+    const size_t at = j_index(G, a, (int)i, (int)j, (int)k);
+    if constexpr (Q) {
+      // Order-free integer sum, converted to J once per trial.
+      if (!fixed_add(G.jq[a] + 2 * at, double(scale[a] * w), G.jq_scale)) error = kErrFixedRange;
+    } else {
+      atomicAdd(&G.j[a][at], scale[a] * w);
+    }
   }
 };
 
 // ChargeConservingCurrentDepositor::depositSegment (src/eb_deposition.cpp:41-51,
 // validatePosition 228-246).
-template <int S, class F>
-__device__ unsigned deposit_segment(const GridT<F>& g, const double b[3],
-                                    const double e[3], double charge) {
+template <class F>
+__device__ __forceinline__ unsigned validate_segment(const GridT<F>& g, const double b[3],
+                                                     const double e[3], double charge) {
   const double extent[3] = {(double)g.nx * g.dx, (double)g.ny * g.dy, (double)g.nz * g.dz};
   for (int a = 0; a < 3; ++a) {
     const double tol = 64.0 * kEpsilon * fmax(1.0, fmax(fabs(g.origin[a]), extent[a]));
@@ -642,7 +650,15 @@ __device__ unsigned deposit_segment(const GridT<F>& g, const double b[3],
     if (!isfinite(e[a]) || re < -tol || re > extent[a] + tol) return kErrDepositOutside;
   }
   if (!isfinite(charge)) return kErrNonFinite;
-  DepositVisitor<F> v;
+  return kErrNone;
+}
+
+template <int S, bool Q, class F>
+__device__ unsigned deposit_segment(const GridT<F>& g, const double b[3],
+                                    const double e[3], double charge) {
+  const unsigned invalid = validate_segment(g, b, e, charge);
+  if (invalid) return invalid;
+  DepositVisitor<F, Q> v;
   v.g = &g;
   v.smooth_x = S == 0;
   v.error = kErrNone;
@@ -917,7 +933,7 @@ struct CarrierState {
 
 // processCarrierSegment at one rank (src/simulation.cpp:4310-4407).
 // Returns an error code; *kept tells whether the carrier survives.
-template <int S, class F>
+template <int S, bool Q, class F>
 __device__ unsigned carrier_segment(const GridT<F>& g, const DRegion& r,
                                     CarrierState& c, const double seg_start[3],
                                     double seg_start_fraction, TrialCounters* counters,
@@ -944,7 +960,7 @@ __device__ unsigned carrier_segment(const GridT<F>& g, const DRegion& r,
   const double end_damping = damping_factor(r, seg_start, seg_end, duration);
   const double deposited = c.w * mid_damping;
   const double end_weight = c.w * end_damping;
-  err = deposit_segment<S>(g, seg_start, seg_end, c.q * deposited);
+  err = deposit_segment<S, Q>(g, seg_start, seg_end, c.q * deposited);
   if (err) return err;
   if (exits) {
     atomicAdd(&counters->carrier_outer[outer.face], 1ull);
@@ -962,7 +978,7 @@ __device__ unsigned carrier_segment(const GridT<F>& g, const DRegion& r,
 // Existing CPML carriers: ballistic step, damped deposit, outer exit
 // (src/simulation.cpp:4531-4537).  Carriers deposit with the run's shape,
 // like every ChargeConservingCurrentDepositor call.
-template <class F, int S>
+template <class F, int S, bool Q>
 __global__ void carrier_kernel(CarrierArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -975,7 +991,7 @@ __global__ void carrier_kernel(CarrierArgs<F> a) {
   const double start[3] = {c.pos[0], c.pos[1], c.pos[2]};
   for (int d = 0; d < 3; ++d) c.pos[d] += a.g.dt * c.vel[d];
   bool kept = false;
-  const unsigned err = carrier_segment<S>(a.g, a.region, c, start, 0.0, a.counters, kept);
+  const unsigned err = carrier_segment<S, Q>(a.g, a.region, c, start, 0.0, a.counters, kept);
   if (err) raise_error(a.status, err, (unsigned long long)n);
   count_lanes(&a.counters->carriers_kept, kept);
   a.keep[n] = kept ? 1 : 0;
@@ -1031,10 +1047,10 @@ __device__ unsigned coupling_push(const PushArgs<F>& a, long long n, double pos[
 // validation (src/longitudinal_shape.h:175-187): the upstream part of an
 // admitted held particle and the frozen source support
 // (src/source_coupling.cpp:73-78) deposit this way.
-template <int S, class F>
+template <int S, bool Q, class F>
 __device__ unsigned deposit_current(const GridT<F>& g, const double b[3],
                                     const double e[3], double charge) {
-  DepositVisitor<F> v;
+  DepositVisitor<F, Q> v;
   v.g = &g;
   v.smooth_x = S == 0;
   v.error = kErrNone;
@@ -1134,7 +1150,7 @@ __global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
 // up to an activation kink (4684-4756) and processActiveSegment (4760-4917)
 // with Simulation::firstMovingWindowEntry
 // (src/simulation_moving_window.cpp:380-395).
-template <class F, int S>
+template <class F, int S, bool Q>
 __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1193,6 +1209,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
     seg_frac = (s.time - t) / dt;
   }
   unsigned char action = 0;
+  bool deferred = false;
   Hit selected;
   for (int piece = has_pre ? 0 : 1; piece < (has_main ? 2 : 1) && !err; ++piece) {
     double b[3], e[3];
@@ -1236,7 +1253,23 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
         e[d] = action ? selected.position[d] : pos[d];
       }
     }
-    err = validate ? deposit_segment<S>(g, b, e, q) : deposit_current<S>(g, b, e, q);
+    if constexpr (S == 0 && kDeferChords<Q>) {
+      // The main chord of a linear-binomial3 particle is validated here and
+      // deposited by chord_deposit_kernel, whose converged warps merge the
+      // stencils of particles in the same cell before the reductions.
+      if (piece == 1) {
+        err = validate_segment(g, b, e, q);
+        if (!err) {
+          for (int d = 0; d < 3; ++d) {
+            a.dep_b[d][n] = b[d];
+            a.dep_e[d][n] = e[d];
+          }
+          deferred = true;
+        }
+        continue;
+      }
+    }
+    err = validate ? deposit_segment<S, Q>(g, b, e, q) : deposit_current<S, Q>(g, b, e, q);
   }
   bool born_kept = false;
   CarrierState born;
@@ -1255,7 +1288,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
     born.q = q;
     born.w = 1.0;
     const double global_end = seg_frac + selected.fraction * (1.0 - seg_frac);
-    err = carrier_segment<S>(g, a.region, born, selected.position, global_end, a.counters,
+    err = carrier_segment<S, Q>(g, a.region, born, selected.position, global_end, a.counters,
                           born_kept);
   } else if (!err && has_main && action == 2) {
     atomicAdd(&a.counters->direct[selected.face], 1ull);
@@ -1282,6 +1315,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
   }
   a.abs_grid_work[n] = abs_work;
   a.action[n] = action;
+  if constexpr (S == 0 && kDeferChords<Q>) a.dep_mode[n] = deferred ? 1 : 0;
   a.born_keep[n] = born_kept ? 1 : 0;
   if (born_kept) {
     a.born.px[n] = born.pos[0]; a.born.py[n] = born.pos[1]; a.born.pz[n] = born.pos[2];
@@ -1290,6 +1324,204 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
     a.born.w[n] = born.w;
     a.born.key[n] = a.key_base | (a.p.order[n] & 0xffffffffull);
   }
+}
+
+// ---------------------------------------------------------------------------
+// The deposit of the main chords of linear-binomial3 particles
+// (Current::deposit, src/longitudinal_shape.h:175-187, with the cut pieces of
+// weights() and binomialXZSegment, :61-117), one thread per particle with the
+// warp converged.  The warp walks the cut pieces of its lanes' chords in
+// step: at each step every lane holds at most one piece, whose 4x2x4 node
+// block is fixed by the piece's cell (i, j, k).  Particles are stored in cell
+// order, so lanes holding pieces of the same cell sit side by side; such a
+// run of lanes adds its 32 stencil weights (8 Jx, 16 Jy, 8 Jz products of
+// the x, y and z factors; the edge smoothing [1/4, 1/2, 1/4] of Jx along x
+// and of Jz along z is applied after the sum) with a segmented shuffle scan,
+// and the run's last lane issues the 64 reductions for all of them.  A lone
+// lane adds its own weights.  The weights are binomialXZSegment's; only the
+// order of the floating-point additions into J differs from one reduction
+// per particle and node.
+struct CutWalker {
+  double x[3], v[3], next[3], lower;
+  long long plane[3], left[3];
+  int dir[3];
+  bool done;
+  // The chord's lattice coordinates; false beyond the 64-cut budget.
+  __device__ bool init(const double begin[3], const double end[3], const double origin[3],
+                       const double h[3]) {
+    long long total = 0;
+    for (int a = 0; a < 3; ++a) {
+      x[a] = (begin[a] - origin[a]) / h[a];
+      v[a] = (end[a] - begin[a]) / h[a];
+      left[a] = 0;
+      dir[a] = 1;
+      plane[a] = 0;
+      next[a] = 0.;
+      if (v[a] != 0.) {
+        const double lo = fmin(x[a], x[a] + v[a]), hi = fmax(x[a], x[a] + v[a]);
+        const long long first = (long long)floor(lo) + 1, last = (long long)ceil(hi) - 1;
+        left[a] = last >= first ? last - first + 1 : 0;
+        dir[a] = v[a] > 0. ? 1 : -1;
+        plane[a] = v[a] > 0. ? first : last;
+        if (left[a]) next[a] = (plane[a] - x[a]) / v[a];
+      }
+      total += left[a];
+    }
+    lower = 0.;
+    done = false;
+    return total <= 62;
+  }
+  // The next piece of nonzero width, as shape_weights cuts the chord.
+  __device__ bool advance(double& first, double& last) {
+    while (!done) {
+      int axis = -1;
+      for (int a = 0; a < 3; ++a)
+        if (left[a] && (axis < 0 || next[a] < next[axis])) axis = a;
+      double upper = 1.;
+      if (axis >= 0) {
+        upper = next[axis];
+        plane[axis] += dir[axis];
+        if (--left[axis]) next[axis] = (plane[axis] - x[axis]) / v[axis];
+      } else {
+        done = true;
+      }
+      const double width = upper - lower;
+      first = lower;
+      last = upper;
+      lower = upper;
+      if (width > 0.) return true;
+    }
+    return false;
+  }
+};
+
+// Inclusive sum of v over the lanes from `head` (the first lane of this
+// lane's run) to this lane; `span` = the longest run in the warp.
+__device__ __forceinline__ double run_sum(double v, int lane, int head, unsigned span) {
+  for (unsigned d = 1; d < span; d <<= 1) {
+    const double u = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane - (int)d >= head) v += u;
+  }
+  return v;
+}
+
+template <bool Q>
+__device__ __forceinline__ void chord_add(const DGrid& g, int a, size_t at, double v,
+                                          unsigned& err) {
+  if constexpr (Q) {
+    if (!fixed_add(g.jq[a] + 2 * at, v, g.jq_scale)) err = kErrFixedRange;
+  } else {
+    atomicAdd(&g.j[a][at], v);
+  }
+}
+
+template <bool Q>
+__global__ void __launch_bounds__(128) chord_deposit_kernel(ChordArgs a) {
+  if (trial_skipped(a.g)) return;
+  const DGrid& g = a.g;
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool alive = n < a.count && a.mode[n] != 0;
+  unsigned err = kErrNone;
+  double scale[3] = {0., 0., 0.};
+  CutWalker w;
+  w.done = true;
+  if (alive) {
+    double b[3], e[3];
+    for (int d = 0; d < 3; ++d) {
+      b[d] = a.b[d][n];
+      e[d] = a.e[d][n];
+    }
+    const double q = a.q[n];
+    for (int d = 0; d < 3; ++d) scale[d] = q * (e[d] - b[d]) / (g.dx * g.dy * g.dz * g.dt);
+    const double h[3] = {g.dx, g.dy, g.dz};
+    if (!w.init(b, e, g.origin, h)) {
+      err = kErrCrossingBudget;
+      alive = false;
+    }
+  }
+  const double edge[3] = {0.25, 0.5, 0.25};
+  const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
+  const double sy[2] = {-1., 1.};
+  const unsigned at_or_below = 0xffffffffu >> (31 - lane);
+  while (__any_sync(0xffffffffu, alive)) {
+    double first = 0., last = 0.;
+    const bool have = alive && w.advance(first, last);
+    if (!have) alive = false;
+    // The piece's cell and factors, as binomialXZSegment forms them.  A lane
+    // without a piece takes a key no other lane has and adds nothing.
+    long long i = 0, j = 0, k = 0;
+    double wx[4] = {0., 0., 0., 0.}, wz[4] = {0., 0., 0., 0.}, wy[2] = {0., 0.};
+    double width = 0., xy = 0., xz = 0., yz = 0.;
+    unsigned long long key = ~0ull - (unsigned long long)lane;
+    if (have) {
+      width = last - first;
+      const double mid = (first + last) * 0.5;
+      const double px = w.x[0] + mid * w.v[0], py = w.x[1] + mid * w.v[1],
+                   pz = w.x[2] + mid * w.v[2];
+      i = (long long)floor(px);
+      j = (long long)floor(py);
+      k = (long long)floor(pz);
+      if (i == (long long)g.nx) --i;
+      if (j == (long long)g.ny) --j;
+      node_weights(px - i, wx);
+      node_weights(pz - k, wz);
+      wy[0] = 1. - (py - j);
+      wy[1] = py - j;
+      const double curvature = width * width / 12.;
+      xy = curvature * w.v[0] * w.v[1];
+      xz = curvature * w.v[0] * w.v[2];
+      yz = curvature * w.v[1] * w.v[2];
+      key = ((unsigned long long)(k + 2) << 42) | ((unsigned long long)(j + 2) << 21) |
+            (unsigned long long)(i + 2);
+    }
+    // Runs of neighbouring lanes on the same cell.
+    const unsigned long long previous = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || previous != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int run_head = 31 - __clz(heads & at_or_below);
+    const bool adds = have && (lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u);
+    const unsigned span = __reduce_max_sync(0xffffffffu, (unsigned)(lane - run_head + 1));
+    // One node of the piece: the visitor's support rules for this lane
+    // (x outside: skipped, the F3 x-support may leave the grid; y outside:
+    // an error when this lane carries current on the axis; z outside:
+    // skipped), and the run's sum added by its last lane.
+    auto node = [&](int ax, long long ii, long long jj, long long kk, double total) {
+      if (ii < 0 || ii >= e_nx(g, ax)) return;
+      if (jj < 0 || jj >= e_ny(g, ax)) {
+        if (have && scale[ax] != 0.) err = kErrSupportY;
+        return;
+      }
+      if (kk < 0 || kk >= e_nz(g, ax)) return;
+      if (adds && total != 0.) chord_add<Q>(g, ax, j_index(g, ax, (int)ii, (int)jj, (int)kk),
+                                            total, err);
+    };
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
+        const double total = run_sum(scale[0] * weight, lane, run_head, span);
+#pragma unroll
+        for (int x = 0; x < 3; ++x) node(0, i - 1 + x, j + b, k - 1 + c, total * edge[x]);
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const double weight = width * (wx[x] * wz[c] + xz * slope[x] * slope[c]);
+        node(1, i - 1 + x, j, k - 1 + c, run_sum(scale[1] * weight, lane, run_head, span));
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const double weight = width * (wx[x] * wy[b] + xy * slope[x] * sy[b]);
+        const double total = run_sum(scale[2] * weight, lane, run_head, span);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) node(2, i - 1 + x, j + b, k - 1 + c, total * edge[c]);
+      }
+  }
+  if (err) raise_error(a.status, err, (unsigned long long)n);
 }
 
 // ---------------------------------------------------------------------------
@@ -1380,10 +1612,46 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     for (int o = 16; o > 0; o >>= 1) block_calls += __shfl_xor_sync(0xffffffffu, block_calls, o);
     if (lane == 0) {
       atomicMax(&a.sums->force_bits, (unsigned long long)__double_as_longlong(force));
-      atomicAdd(&a.sums->defect, defect);
-      atomicAdd(&a.sums->scale, scale);
       if (block_calls) atomicAdd(&a.sums->calls, (unsigned long long)block_calls);
+      a.partial[2 * blockIdx.x] = defect;
+      a.partial[2 * blockIdx.x + 1] = scale;
     }
+  }
+  // The defect and scale sums in a fixed order: the last block to finish
+  // adds the block partials (thread t takes blocks t, t + 128, ... in turn,
+  // then a fixed shuffle tree), so the sums do not depend on which blocks
+  // finished first.
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  defect = 0.0;
+  scale = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    defect += __ldcg(&a.partial[2 * b]);
+    scale += __ldcg(&a.partial[2 * b + 1]);
+  }
+  defect = warp_sum(defect);
+  scale = warp_sum(scale);
+  __syncthreads();
+  if (lane == 0) {
+    s_defect[warp] = defect;
+    s_scale[warp] = scale;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double d = 0.0, c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      d += s_defect[w];
+      c += s_scale[w];
+    }
+    a.sums->defect = d;
+    a.sums->scale = c;
+    *a.ticket = 0u;
   }
 }
 
@@ -1491,23 +1759,102 @@ __global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsig
 }
 
 // ---------------------------------------------------------------------------
-// Tile sort: particles of one 4x4x4 cell tile become contiguous, so the
-// 4x4x3 F3 stencils of a warp overlap in L1 instead of scattering over HBM.
-__global__ void tile_count_kernel(DParticles p, long long n, DGrid g, int tiles_x,
-                                  int tiles_y, int tiles_z, unsigned* tile_count,
-                                  unsigned* tile_of, unsigned* rank_in_tile) {
+// Cell sort: particles of one cell become contiguous, in cell order (x
+// fastest), so the 4x2x4 F3 stencils of a warp overlap in L1 instead of
+// scattering over HBM.  A stable least-significant-digit radix sort of the
+// cell index (8-bit digits): the order of particles within a cell is their
+// previous storage order, so the permutation -- and every block reduction
+// over the particle list -- is the same from run to run.
+__global__ void sort_key_kernel(DParticles p, long long n, DGrid g, int tiles_x, int tiles_y,
+                                unsigned* key, unsigned* index) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double lx = (p.x[i] - g.origin[0]) / g.dx;
   const double ly = (p.y[i] - g.origin[1]) / g.dy;
   const double lz = (p.z[i] - g.origin[2]) / g.dz;
-  int cx = (int)fmin(fmax(floor(lx), 0.0), (double)(g.nx - 1));
-  int cy = (int)fmin(fmax(floor(ly), 0.0), (double)(g.ny - 1));
-  int cz = (int)fmin(fmax(floor(lz), 0.0), (double)(g.nz - 1));
-  const unsigned t = (unsigned)((((cz >> kTileShift) * tiles_y) + (cy >> kTileShift)) * tiles_x +
-                                (cx >> kTileShift));
-  tile_of[i] = t;
-  rank_in_tile[i] = atomicAdd(&tile_count[t], 1u);
+  const int cx = (int)fmin(fmax(floor(lx), 0.0), (double)(g.nx - 1));
+  const int cy = (int)fmin(fmax(floor(ly), 0.0), (double)(g.ny - 1));
+  const int cz = (int)fmin(fmax(floor(lz), 0.0), (double)(g.nz - 1));
+  key[i] = (unsigned)((((cz >> kTileShift) * tiles_y) + (cy >> kTileShift)) * tiles_x +
+                      (cx >> kTileShift));
+  index[i] = (unsigned)i;
+}
+
+// Digit counts of each block's kRadixTile keys: count[digit * blocks + block].
+__global__ void __launch_bounds__(kRadixThreads) radix_count_kernel(const unsigned* key,
+                                                                    long long n, int shift,
+                                                                    unsigned* count) {
+  __shared__ unsigned c[kRadixBins];
+  c[threadIdx.x] = 0u;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kRadixTile;
+  for (int r = 0; r < kRadixItems; ++r) {
+    const long long i = base + r * kRadixThreads + threadIdx.x;
+    if (i < n) atomicAdd(&c[(key[i] >> shift) & (kRadixBins - 1)], 1u);
+  }
+  __syncthreads();
+  count[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = c[threadIdx.x];
+}
+
+// Stable scatter of one digit pass.  offset[digit * blocks + block] is the
+// exclusive scan of radix_count_kernel's counts in that digit-major order.
+// A block walks its keys in index order, 256 at a time; within a round a
+// key's rank among equal digits is its warp's lanes below it (match_any)
+// plus the equal digits of the warps before it and of the earlier rounds.
+__global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(
+    const unsigned* key_in, const unsigned* index_in, unsigned* key_out, unsigned* index_out,
+    long long n, int shift, const unsigned* offset) {
+  constexpr int kWarps = kRadixThreads / 32;
+  __shared__ unsigned running[kRadixBins];
+  __shared__ unsigned warp_count[kWarps][kRadixBins];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  running[threadIdx.x] = offset[(size_t)threadIdx.x * gridDim.x + blockIdx.x];
+  const long long base = (long long)blockIdx.x * kRadixTile;
+  for (int r = 0; r < kRadixItems; ++r) {
+    const long long i = base + r * kRadixThreads + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned k = valid ? key_in[i] : 0u;
+    const unsigned digit = valid ? (k >> shift) & (kRadixBins - 1) : kRadixBins;
+    for (int w = 0; w < kWarps; ++w) warp_count[w][threadIdx.x] = 0u;
+    __syncthreads();
+    const unsigned peers = __match_any_sync(0xffffffffu, digit);
+    const unsigned rank = __popc(peers & below);
+    if (valid && rank == 0) warp_count[warp][digit] = __popc(peers);
+    __syncthreads();
+    {  // per digit: exclusive prefix over the warps, then advance the running base
+      unsigned at = running[threadIdx.x];
+      for (int w = 0; w < kWarps; ++w) {
+        const unsigned c = warp_count[w][threadIdx.x];
+        warp_count[w][threadIdx.x] = at;
+        at += c;
+      }
+      running[threadIdx.x] = at;
+    }
+    __syncthreads();
+    if (valid) {
+      const unsigned d = warp_count[warp][digit] + rank;
+      key_out[d] = k;
+      index_out[d] = index_in[i];
+    }
+    __syncthreads();
+  }
+}
+
+// The storage permutation: out[d] = src[index[d]].
+__global__ void permute_particles_kernel(DParticles out, DParticles src, long long n,
+                                         const unsigned* index) {
+  const long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  const long long i = index[d];
+  out.x[d] = src.x[i]; out.y[d] = src.y[i]; out.z[d] = src.z[i];
+  out.ux[d] = src.ux[i]; out.uy[d] = src.uy[i]; out.uz[d] = src.uz[i];
+  out.q[d] = src.q[i];
+  out.m[d] = src.m[i];
+  out.id[d] = src.id[i];
+  out.order[d] = src.order[i];
+  out.frozen[d] = src.frozen[i];
+  out.beta[d] = src.beta[i];
 }
 
 // Exclusive scan of 1024-element chunks; chunk totals go to chunk_sum.
@@ -1531,23 +1878,6 @@ __global__ void chunk_scan_kernel(const unsigned* in, long long n, unsigned* out
 __global__ void chunk_add_kernel(unsigned* data, long long n, const unsigned* chunk_offset) {
   const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
   if (i < n) data[i] += chunk_offset[blockIdx.x];
-}
-
-__global__ void scatter_particles_kernel(DParticles out, DParticles src, long long n,
-                                         const unsigned* tile_of,
-                                         const unsigned* rank_in_tile,
-                                         const unsigned* tile_offset) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const long long d = (long long)tile_offset[tile_of[i]] + rank_in_tile[i];
-  out.x[d] = src.x[i]; out.y[d] = src.y[i]; out.z[d] = src.z[i];
-  out.ux[d] = src.ux[i]; out.uy[d] = src.uy[i]; out.uz[d] = src.uz[i];
-  out.q[d] = src.q[i];
-  out.m[d] = src.m[i];
-  out.id[d] = src.id[i];
-  out.order[d] = src.order[i];
-  out.frozen[d] = src.frozen[i];
-  out.beta[d] = src.beta[i];
 }
 
 // PendingParticleQueue::admit (src/pending_particle_queue.cpp:163-186): the
@@ -1577,7 +1907,7 @@ __global__ void admit_kernel(DParticles out, long long first_slot, DPending src,
 // (PendingParticleQueue::visitNear + depositFrozenSourceSupport,
 // src/simulation.cpp:4170-4172, src/source_coupling.cpp:73-78): each
 // deposits its held chord of this step without endpoint validation.
-template <class F, int S>
+template <class F, int S, bool Q>
 __global__ void frozen_support_kernel(SupportArgs<F> a) {
   if (trial_skipped(a.g)) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1588,7 +1918,7 @@ __global__ void frozen_support_kernel(SupportArgs<F> a) {
   const double start[3] = {a.src.x[k], a.src.y[k],
                            repeat_held_addition(a.src.z[k], increment, a.steps)};
   const double stop[3] = {start[0], start[1], start[2] + increment};
-  const unsigned err = deposit_current<S>(a.g, start, stop, a.src.q[k]);
+  const unsigned err = deposit_current<S, Q>(a.g, start, stop, a.src.q[k]);
   if (err) raise_error(a.status, err, (unsigned long long)k);
 }
 
@@ -1674,9 +2004,14 @@ __global__ void inlet_charge_kernel(InletMatchArgs a) {
   for (int b = 0; b < 2; ++b)
     for (int c = 0; c < n_x; ++c) {
       const long long i = first + c;
-      if (i >= 0 && i <= a.nx && j + b <= a.ny)
-        atomicAdd(&a.rho[(size_t)(j + b) * (a.nx + 1) + (size_t)i],
-                  scale * wx[c] * (b ? fy : 1. - fy) * wz);
+      if (i >= 0 && i <= a.nx && j + b <= a.ny) {
+        const size_t at = (size_t)(j + b) * (a.nx + 1) + (size_t)i;
+        const double v = scale * wx[c] * (b ? fy : 1. - fy) * wz;
+        if (a.rho_pairs == nullptr)
+          atomicAdd(&a.rho[at], v);
+        else if (!fixed_add(a.rho_pairs + 2 * at, v, a.rho_scale))
+          raise_error(a.status, kErrFixedRange, (unsigned long long)where);
+      }
     }
 }
 
@@ -1687,12 +2022,39 @@ __global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, Res
   const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   for (int c = 0; c < 3 && clear_current; ++c) {
     const long long count = (long long)e_nx(g, c) * e_ny(g, c) * e_nz(g, c);
-    for (long long n = first; n < count; n += stride) g.j[c][n] = 0.;
+    if (clear_current == 2) {
+      ulonglong2* pairs = reinterpret_cast<ulonglong2*>(g.jq[c]);
+      for (long long n = first; n < count; n += stride) pairs[n] = make_ulonglong2(0ull, 0ull);
+    } else {
+      for (long long n = first; n < count; n += stride) g.j[c][n] = 0.;
+    }
   }
   if (first == 0) {
     *counters = TrialCounters{};
     *sums = ResidualSums{};
   }
+}
+
+__global__ void current_convert_kernel(GridT<double> g, double unscale) {
+  if (trial_skipped(g)) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int c = 0; c < 3; ++c) {
+    const long long count = (long long)e_nx(g, c) * e_ny(g, c) * e_nz(g, c);
+    const ulonglong2* pairs = reinterpret_cast<const ulonglong2*>(g.jq[c]);
+    for (long long n = first; n < count; n += stride) {
+      const ulonglong2 v = pairs[n];
+      g.j[c][n] = (v.x | v.y) ? fixed_value(v.x, v.y, unscale) : 0.;
+    }
+  }
+}
+
+__global__ void fixed_convert_kernel(const unsigned long long* pairs, double* out, long long n,
+                                     double unscale) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long lo = pairs[2 * i], hi = pairs[2 * i + 1];
+  out[i] = (lo | hi) ? fixed_value(lo, hi, unscale) : 0.;
 }
 
 __global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iterations,
@@ -1712,15 +2074,20 @@ __global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iteratio
 // 1 quintic-compensated), so a kernel carries the registers and local
 // memory of its own shape's weights only.
 #define APRL_SHAPE_KERNELS(S)                                                        \
-  template __global__ void push_deposit_kernel<double, S>(PushArgs<double>);         \
-  template __global__ void carrier_kernel<double, S>(CarrierArgs<double>);           \
-  template __global__ void frozen_support_kernel<double, S>(SupportArgs<double>);    \
+  template __global__ void push_deposit_kernel<double, S, false>(PushArgs<double>);  \
+  template __global__ void push_deposit_kernel<double, S, true>(PushArgs<double>);   \
+  template __global__ void carrier_kernel<double, S, false>(CarrierArgs<double>);    \
+  template __global__ void carrier_kernel<double, S, true>(CarrierArgs<double>);     \
+  template __global__ void frozen_support_kernel<double, S, false>(SupportArgs<double>); \
+  template __global__ void frozen_support_kernel<double, S, true>(SupportArgs<double>); \
   template __global__ void guess_gather_kernel<double, double, S>(PushArgs<double>); \
   template __global__ void guess_gather_kernel<float, double, S>(PushArgs<double>);  \
   template __global__ void residual_kernel<double, double, S>(ResidualArgs<double>); \
   template __global__ void residual_kernel<float, double, S>(ResidualArgs<double>);
 APRL_SHAPE_KERNELS(0)
 APRL_SHAPE_KERNELS(1)
+template __global__ void chord_deposit_kernel<false>(ChordArgs);
+template __global__ void chord_deposit_kernel<true>(ChordArgs);
 #undef APRL_SHAPE_KERNELS
 
 }  // namespace aprl_gpu

@@ -111,6 +111,11 @@ struct PushArgs {
   double* abs_grid_work; // sum over substeps of |grid work|
   unsigned char* action; // 0 retain, 1 CPML/exit carrier, 2 outer exit
   DCarriers born;        // carrier created by a CPML entry (when kept)
+  // linear-binomial3: the main chord, validated, for chord_deposit_kernel
+  // (dep_mode 1; 0 when the particle deposits no main chord this trial)
+  double* dep_b[3];
+  double* dep_e[3];
+  unsigned char* dep_mode;
   unsigned long long key_base;  // (step + 1) << 32 for newborn carrier keys
   unsigned char* born_keep;
   TrialCounters* counters;
@@ -146,6 +151,28 @@ struct ResidualArgs {
   double* next_b;
   const double* abs_grid_work;
   ResidualSums* sums;
+  // defect and scale per block; the last block to finish sums them in block
+  // order (ticket counts the finished blocks and is left at zero).
+  double* partial;
+  unsigned* ticket;
+  DeviceStatus* status;
+};
+
+// Whether push_deposit_kernel leaves the main chords of linear-binomial3
+// particles to chord_deposit_kernel (per current-summation mode Q): the
+// merged deposit halves the fixed-point mode's reductions, which bound it;
+// with binary64 atomics the fused deposit measured faster (0.50 ms per
+// dipole-workload trial against 0.13 + 0.47 ms).
+template <bool Q> constexpr bool kDeferChords = Q;
+
+// The deferred main chords of a linear-binomial3 trial.
+struct ChordArgs {
+  GridT<double> g;
+  long long count;
+  const unsigned char* mode;
+  const double* b[3];
+  const double* e[3];
+  const double* q;
   DeviceStatus* status;
 };
 
@@ -186,8 +213,11 @@ struct ResidualArgs {
 // W: arithmetic of the gathers (double, or float in the FP32-mixed mode).
 // S: the particle shape, 0 linear-binomial3, 1 quintic-compensated.
 template <class W, class F, int S> __global__ void guess_gather_kernel(PushArgs<F> a);
-template <class F, int S> __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
-template <class F, int S> __global__ void carrier_kernel(CarrierArgs<F> a);
+// Q: the deterministic mode's fixed-point current sum.
+template <class F, int S, bool Q>
+__global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
+template <class F, int S, bool Q> __global__ void carrier_kernel(CarrierArgs<F> a);
+template <bool Q> __global__ void chord_deposit_kernel(ChordArgs a);
 template <class W, class F, int S>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
 
@@ -209,17 +239,23 @@ __global__ void gather_carriers_kernel(DCarriers out, DCarriers src,
                                        const unsigned char* flag, unsigned char want,
                                        long long n, const unsigned* block_offset,
                                        unsigned long long base);
-// Counting sort of the particle storage by cell tile.
-__global__ void tile_count_kernel(DParticles p, long long n, DGrid g, int tiles_x,
-                                  int tiles_y, int tiles_z, unsigned* tile_count,
-                                  unsigned* tile_of, unsigned* rank_in_tile);
+// Stable radix sort of the particle storage by cell (8-bit digits).
+constexpr int kRadixBins = 256;
+constexpr int kRadixThreads = 256;  // one thread per digit in the scatter's prefix
+constexpr int kRadixItems = 8;
+constexpr int kRadixTile = kRadixThreads * kRadixItems;
+static_assert(kRadixThreads == kRadixBins, "radix_scatter_kernel: one thread per digit");
+__global__ void sort_key_kernel(DParticles p, long long n, DGrid g, int tiles_x, int tiles_y,
+                                unsigned* key, unsigned* index);
+__global__ void radix_count_kernel(const unsigned* key, long long n, int shift, unsigned* count);
+__global__ void radix_scatter_kernel(const unsigned* key_in, const unsigned* index_in,
+                                     unsigned* key_out, unsigned* index_out, long long n,
+                                     int shift, const unsigned* offset);
+__global__ void permute_particles_kernel(DParticles out, DParticles src, long long n,
+                                         const unsigned* index);
 __global__ void chunk_scan_kernel(const unsigned* in, long long n, unsigned* out,
                                   unsigned* chunk_sum);
 __global__ void chunk_add_kernel(unsigned* data, long long n, const unsigned* chunk_offset);
-__global__ void scatter_particles_kernel(DParticles out, DParticles src, long long n,
-                                         const unsigned* tile_of,
-                                         const unsigned* rank_in_tile,
-                                         const unsigned* tile_offset);
 // Pending queue (PendingParticleQueue) on the device: particles sorted by
 // their due step, initial state.
 struct DPending {
@@ -239,7 +275,7 @@ struct SupportArgs {
   double held_distance_per_beta; // c*dt
   DeviceStatus* status;
 };
-template <class F, int S> __global__ void frozen_support_kernel(SupportArgs<F> a);
+template <class F, int S, bool Q> __global__ void frozen_support_kernel(SupportArgs<F> a);
 __global__ void crop_flags_kernel(DCarriers c, long long n, double upper,
                                   double lower, unsigned char* keep,
                                   TrialCounters* counters, DeviceStatus* status);
@@ -262,14 +298,25 @@ struct InletMatchArgs {
   double dx, dy, dz;
   int nx, ny, shape;
   double* rho;                 // (nx+1) x (ny+1) node plane
+  // Deterministic mode: the charge goes into these (lo, hi) word pairs
+  // instead (fixed_add with rho_scale), converted by fixed_convert_kernel.
+  unsigned long long* rho_pairs;
+  double rho_scale;
   DeviceStatus* status;
 };
 __global__ void inlet_charge_kernel(InletMatchArgs a);
 
 // A trial's start: J, the trial counters and the residual sums cleared
 // (skipped with the trial).
+// clear_current: 1 clears J; in the deterministic mode 2 clears the
+// fixed-point pairs of J instead (J is then written by current_convert).
 __global__ void trial_clear_kernel(GridT<double> g, TrialCounters* counters, ResidualSums* sums,
                                    int clear_current);
+// Deterministic mode: J from its fixed-point pairs, every node.
+__global__ void current_convert_kernel(GridT<double> g, double unscale);
+// out[i] = value of pair i (fixed_value), for i < n.
+__global__ void fixed_convert_kernel(const unsigned long long* pairs, double* out, long long n,
+                                     double unscale);
 // solveConservativeSourceStep's stopping rule (src/simulation_source_coupling.cpp:50)
 // applied to trial `iterations`' residual sums: on convergence *stop = iterations.
 __global__ void trial_verdict_kernel(const ResidualSums* sums, unsigned iterations,

@@ -56,12 +56,13 @@ enum Kernel : unsigned {
   kInletLower, kCowanMagnetic, kElectricPreview, kCarrier, kPushDeposit,
   kResidual, kElectricCommit, kFlagCount, kBlockScan, kGatherParticles,
   kGatherCarriers, kShiftInsert, kCropFlags, kInletCheck, kDetectorPlane,
-  kTileCount, kChunkScan, kChunkAdd, kScatterParticles, kAdmit, kFrozenSupport,
+  kSortKey, kChunkScan, kChunkAdd, kRadixScatter, kAdmit, kFrozenSupport,
   kGuessGather, kOrbitSum, kBShadow, kLedgerPartial, kLedgerFinish,
   kGaussDeposit, kGaussResidual, kGaussFinish, kTrialClear, kTrialVerdict,
   kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfUpdate,
   kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
-  kInletHalo, kInletCharge, kInletComplete, kKernelCount
+  kInletHalo, kInletCharge, kInletComplete, kRadixCount, kPermuteParticles,
+  kCurrentConvert, kFixedConvert, kChordDeposit, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -69,12 +70,13 @@ const char* kKernelNames[kKernelCount] = {
   "push_deposit", "residual", "electric_commit", "flag_count",
   "block_offset_scan", "gather_particles", "gather_carriers",
   "shift_insert", "crop_flags", "inlet_check", "detector_plane",
-  "tile_count", "chunk_scan", "chunk_add", "scatter_particles", "admit",
+  "sort_key", "chunk_scan", "chunk_add", "radix_scatter", "admit",
   "frozen_support", "guess_gather", "orbit_sum", "b_shadow", "ledger_partial",
   "ledger_finish", "gauss_deposit", "gauss_residual", "gauss_finish", "trial_clear",
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
   "sf_update", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
-  "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete"};
+  "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete",
+  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -102,6 +104,8 @@ const char* device_error_text(unsigned code) {
       return "Held-transverse activation crossed a particle boundary during the frozen part of a field step";
     case kErrInletSource: return "Nonfinite charge-matched inlet source";
     case kErrInletField: return "Nonfinite charge-matched inlet field";
+    case kErrFixedRange:
+      return "Deposit contribution beyond the deterministic fixed-point range";
   }
   return "unknown device error";
 }
@@ -270,6 +274,11 @@ struct aprl_run {
          *uz1 = nullptr;
   double *used_e = nullptr, *used_b = nullptr, *next_e = nullptr, *next_b = nullptr;
   double* abs_work = nullptr;
+  // linear-binomial3: each particle's validated main chord of the trial,
+  // deposited by chord_deposit_kernel after the push
+  double* dep_b[3]{};
+  double* dep_e[3]{};
+  unsigned char* dep_mode = nullptr;
   unsigned char* action = nullptr;
   DCarriers born{};
   unsigned char* born_keep = nullptr;
@@ -288,11 +297,25 @@ struct aprl_run {
   } queue;
   uint64_t admitted = 0;
   uint64_t held = 0;              // frozen particles in the list
-  // tile sort scratch
-  unsigned *tile_count = nullptr, *tile_offset = nullptr, *tile_of = nullptr,
-           *tile_rank = nullptr, *chunk_sum = nullptr, *chunk_offset = nullptr;
+  // cell sort scratch: keys and storage indices (two of each for the radix
+  // passes), per-block digit counts and their chunk sums
+  unsigned *sort_key[2]{}, *sort_index[2]{};
+  unsigned *radix_count = nullptr, *chunk_sum = nullptr, *chunk_offset = nullptr;
   size_t ntiles = 0;
   int tiles[3]{};
+  int sort_bits = 0;
+  // Deterministic mode (aprl_run_config.deterministic): J's fixed-point
+  // (lo, hi) pairs, the scale that maps the largest possible contribution
+  // below 2^61 (a power of two), and the largest |charge| uploaded so far.
+  bool deterministic = false;
+  unsigned long long* jq[3]{};
+  double jq_scale = 1.0;
+  double max_abs_charge = 0.0;
+  unsigned long long* inlet_rho_pairs = nullptr;
+  // residual block partials (defect, scale) and the finished-block ticket
+  double* res_partial = nullptr;
+  unsigned* res_ticket = nullptr;
+  size_t res_blocks = 0;
   // carriers
   size_t nc = 0, ccap = 0;
   DCarriers c{}, c_alt{}, c_out{};
@@ -585,7 +608,31 @@ GridT<F> make_grid(const aprl_run* r) {
     g.zb_b[a] = r->zb_b[a];
   }
   g.jcoef = F(-1. * r->cfg.dt / kEpsilon0);
+  if (r->deterministic) {
+    for (int a = 0; a < 3; ++a) g.jq[a] = r->jq[a];
+    g.jq_scale = r->jq_scale;
+  }
   return g;
+}
+
+// The fixed-point scale of the deterministic mode: a power of two 2^e with
+// bound * 2^e < 2^61, where `bound` exceeds any single contribution the run
+// can make.  A deposit visit adds q * (dx_a / dt) / (dx dy dz) * w with
+// |dx_a / dt| <= c and |w| <= 2 (the quintic compensation's largest node
+// weight is about 1.6), so bound = 4 max|q| c / (dx dy dz); the layer
+// charge of the charge-matched inlet is at most max|q| / (dx dy dz).
+double fixed_scale(double bound) {
+  if (!(bound > 0.0) || !std::isfinite(bound)) return 1.0;
+  int exponent = 0;
+  std::frexp(bound, &exponent);  // bound < 2^exponent
+  return std::ldexp(1.0, std::max(-1000, std::min(1000, 61 - exponent)));
+}
+
+void note_charges(aprl_run* r, const double* charge, size_t n) {
+  double m = r->max_abs_charge;
+  for (size_t i = 0; i < n; ++i) m = std::max(m, std::fabs(charge[i]));
+  r->max_abs_charge = m;
+  r->jq_scale = fixed_scale(4.0 * m * kC / (r->cfg.dx * r->cfg.dy * r->cfg.dz));
 }
 
 // Geometry only (no field pointers), for the particle sort.
@@ -773,9 +820,10 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   free_particles(r, r->p_alt);
   r->p = np;
   TRY(alloc_particles(r, r->p_alt, n));
-  double** trial[] = {&r->x1,       &r->y1,       &r->z1,       &r->ux1,     &r->uy1,
+  double** trial[] = {&r->x1,       &r->y1,       &r->z1,       &r->ux1,      &r->uy1,
                       &r->uz1,      &r->abs_work, &r->slots.x0, &r->slots.y0, &r->slots.z0,
-                      &r->slots.dt};
+                      &r->slots.dt, &r->dep_b[0], &r->dep_b[1], &r->dep_b[2], &r->dep_e[0],
+                      &r->dep_e[1], &r->dep_e[2]};
   for (double** t : trial) {
     device_free(r, *t);
     TRY(device_alloc(r, t, n));
@@ -788,17 +836,35 @@ aprl_status reserve_particles(aprl_run* r, size_t n) {
   device_free(r, r->action);
   device_free(r, r->born_keep);
   device_free(r, r->slot_order);
-  device_free(r, r->tile_of);
-  device_free(r, r->tile_rank);
+  for (int k = 0; k < 2; ++k) {
+    device_free(r, r->sort_key[k]);
+    device_free(r, r->sort_index[k]);
+  }
+  device_free(r, r->radix_count);
+  device_free(r, r->chunk_sum);
+  device_free(r, r->chunk_offset);
+  device_free(r, r->res_partial);
   device_free(r, r->frozen1);
   device_free(r, r->slots.seen);
   TRY(device_alloc(r, &r->frozen1, n));
   TRY(device_alloc(r, &r->slots.seen, n));
+  device_free(r, r->dep_mode);
   TRY(device_alloc(r, &r->action, n));
+  TRY(device_alloc(r, &r->dep_mode, n));
   TRY(device_alloc(r, &r->born_keep, n));
   TRY(device_alloc(r, &r->slot_order, n));
-  TRY(device_alloc(r, &r->tile_of, n));
-  TRY(device_alloc(r, &r->tile_rank, n));
+  for (int k = 0; k < 2; ++k) {
+    TRY(device_alloc(r, &r->sort_key[k], n));
+    TRY(device_alloc(r, &r->sort_index[k], n));
+  }
+  {
+    const size_t counts = (size_t)kRadixBins * ((n + kRadixTile - 1) / kRadixTile);
+    TRY(device_alloc(r, &r->radix_count, counts));
+    TRY(device_alloc(r, &r->chunk_sum, counts / 1024 + 1));
+    TRY(device_alloc(r, &r->chunk_offset, counts / 1024 + 1));
+  }
+  r->res_blocks = (n + 127) / 128;
+  TRY(device_alloc(r, &r->res_partial, 2 * r->res_blocks));
   free_carriers(r, r->born);
   TRY(alloc_carriers(r, r->born, n));
   r->pcap = n;
@@ -911,25 +977,39 @@ aprl_status compact_offsets(aprl_run* r, const unsigned char* flag, unsigned cha
                 (const unsigned*)r->scan_count, (int)blocks, r->scan_offset, r->scan_total);
 }
 
-// Counting sort of the particle storage by 4x4x4 cell tiles
-// (tile_count -> chunked exclusive scan -> scatter).
+// Stable radix sort of the particle storage by cell index: the key pass,
+// then per 8-bit digit the block digit counts, their exclusive scan in
+// digit-major order (chunk scan, chunk-sum scan, chunk add) and the stable
+// scatter of keys and storage indices; finally the particle arrays are
+// permuted.  No atomic ticket decides an order, so the storage order after
+// a sort is a function of the storage order before it.
 aprl_status sort_particles(aprl_run* r) {
-  if (r->np == 0) return APRL_OK;
+  if (r->np < 2 || r->sort_bits == 0) return APRL_OK;
   const long long n = (long long)r->np;
   const DGrid g = make_geometry(r);
-  CUDA_TRY(cudaMemsetAsync(r->tile_count, 0, r->ntiles * sizeof(unsigned), r->stream));
-  TRY(launch(r, kTileCount, tile_count_kernel, dim3(blocks_for(r->np, 256)), dim3(256), r->p, n, g,
-             r->tiles[0], r->tiles[1], r->tiles[2], r->tile_count, r->tile_of, r->tile_rank));
-  const unsigned chunks = blocks_for(r->ntiles, 1024);
-  TRY(launch(r, kChunkScan, chunk_scan_kernel, dim3(chunks), dim3(1024),
-             (const unsigned*)r->tile_count, (long long)r->ntiles, r->tile_offset, r->chunk_sum));
-  TRY(launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
-             (const unsigned*)r->chunk_sum, (int)chunks, r->chunk_offset, r->scan_total));
-  TRY(launch(r, kChunkAdd, chunk_add_kernel, dim3(chunks), dim3(1024), r->tile_offset,
-             (long long)r->ntiles, (const unsigned*)r->chunk_offset));
-  TRY(launch(r, kScatterParticles, scatter_particles_kernel, dim3(blocks_for(r->np, 256)),
-             dim3(256), r->p_alt, r->p, n, (const unsigned*)r->tile_of,
-             (const unsigned*)r->tile_rank, (const unsigned*)r->tile_offset));
+  TRY(launch(r, kSortKey, sort_key_kernel, dim3(blocks_for(r->np, 256)), dim3(256), r->p, n, g,
+             r->tiles[0], r->tiles[1], r->sort_key[0], r->sort_index[0]));
+  const unsigned blocks = blocks_for(r->np, kRadixTile);
+  const long long counts = (long long)kRadixBins * blocks;
+  const unsigned chunks = blocks_for((size_t)counts, 1024);
+  int from = 0;
+  for (int shift = 0; shift < r->sort_bits; shift += 8) {
+    TRY(launch(r, kRadixCount, radix_count_kernel, dim3(blocks), dim3(kRadixThreads),
+               (const unsigned*)r->sort_key[from], n, shift, r->radix_count));
+    TRY(launch(r, kChunkScan, chunk_scan_kernel, dim3(chunks), dim3(1024),
+               (const unsigned*)r->radix_count, counts, r->radix_count, r->chunk_sum));
+    TRY(launch(r, kBlockScan, block_offset_scan_kernel, dim3(1), dim3(1024),
+               (const unsigned*)r->chunk_sum, (int)chunks, r->chunk_offset, r->scan_total));
+    TRY(launch(r, kChunkAdd, chunk_add_kernel, dim3(chunks), dim3(1024), r->radix_count,
+               counts, (const unsigned*)r->chunk_offset));
+    TRY(launch(r, kRadixScatter, radix_scatter_kernel, dim3(blocks), dim3(kRadixThreads),
+               (const unsigned*)r->sort_key[from], (const unsigned*)r->sort_index[from],
+               r->sort_key[1 - from], r->sort_index[1 - from], n, shift,
+               (const unsigned*)r->radix_count));
+    from = 1 - from;
+  }
+  TRY(launch(r, kPermuteParticles, permute_particles_kernel, dim3(blocks_for(r->np, 256)),
+             dim3(256), r->p_alt, r->p, n, (const unsigned*)r->sort_index[from]));
   std::swap(r->p, r->p_alt);
   return APRL_OK;
 }
@@ -1263,17 +1343,28 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     frozen_end = q.offsets[until - q.initial_step + 1];
   }
   const bool deposits = r->np || r->nc || (r->queue.extracted && frozen_end > r->queue.cursor);
+  size_t most = 0;
+  for (int a = 0; a < 3; ++a) most = std::max(most, e_count(c, a));
+  const unsigned grid_blocks = std::min<unsigned>(blocks_for(most, 256), 148 * 8);
+  // Deterministic mode: the deposits of the trial go into J's fixed-point
+  // pairs, and J is written from them once they are all done.
+  const bool convert = r->deterministic && deposits;
   {
-    // The counters and sums always; J unless it is known to be zero.
-    size_t most = 0;
-    for (int a = 0; a < 3; ++a) most = std::max(most, e_count(c, a));
-    const int clear_current = r->j_zero ? 0 : 1;
-    const unsigned blocks =
-        clear_current ? std::min<unsigned>(blocks_for(most, 256), 148 * 8) : 1u;
+    // The counters and sums always; J unless it is known to be zero (its
+    // pairs instead when the conversion will write J).
+    const int clear_current = convert ? 2 : (r->j_zero ? 0 : 1);
+    const unsigned blocks = clear_current ? grid_blocks : 1u;
     TRY(launch(r, kTrialClear, trial_clear_kernel, dim3(blocks), dim3(256), g, r->d_counters,
                r->d_sums, clear_current));
   }
   r->j_zero = !deposits;
+  bool converted = !convert;
+  auto convert_current = [&]() -> aprl_status {
+    if (converted) return APRL_OK;
+    converted = true;
+    return launch(r, kCurrentConvert, current_convert_kernel, dim3(grid_blocks), dim3(256), g,
+                  1.0 / r->jq_scale);
+  };
   const DRegion region = make_region(r);
   // Each particle kernel is built per shape: 0 linear-binomial3, else quintic.
   const bool binomial = c.shape == 0;
@@ -1291,7 +1382,9 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
       sa.held_distance_per_beta = held_distance_per_beta(c);
       sa.status = r->d_status;
       TRY(launch(r, kFrozenSupport,
-                 binomial ? frozen_support_kernel<F, 0> : frozen_support_kernel<F, 1>,
+                 r->deterministic
+                     ? (binomial ? frozen_support_kernel<F, 0, true> : frozen_support_kernel<F, 1, true>)
+                     : (binomial ? frozen_support_kernel<F, 0, false> : frozen_support_kernel<F, 1, false>),
                  dim3(blocks_for(end - q.cursor, 128)),
                  dim3(128), sa));
     }
@@ -1312,7 +1405,10 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ca.status = r->d_status;
     CUDA_TRY(cudaEventRecord(r->fork, r->stream));
     CUDA_TRY(cudaStreamWaitEvent(r->side, r->fork, 0));
-    TRY(launch_on(r, r->side, kCarrier, binomial ? carrier_kernel<F, 0> : carrier_kernel<F, 1>,
+    TRY(launch_on(r, r->side, kCarrier,
+                  r->deterministic
+                      ? (binomial ? carrier_kernel<F, 0, true> : carrier_kernel<F, 1, true>)
+                      : (binomial ? carrier_kernel<F, 0, false> : carrier_kernel<F, 1, false>),
                   dim3(blocks_for(r->nc, 128)),
                   dim3(128), ca));
     CUDA_TRY(cudaEventRecord(r->join, r->side));
@@ -1363,6 +1459,11 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     pa.action = r->action;
     pa.born = r->born;
     pa.born_keep = r->born_keep;
+    for (int d = 0; d < 3; ++d) {
+      pa.dep_b[d] = r->dep_b[d];
+      pa.dep_e[d] = r->dep_e[d];
+    }
+    pa.dep_mode = r->dep_mode;
     pa.key_base = (unsigned long long)(r->step + 1) << 32;
     pa.counters = r->d_counters;
     pa.status = r->d_status;
@@ -1383,10 +1484,29 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
                  dim3(blocks_for(r->np, 128)),
                  dim3(128), pa));
     }
-    TRY(launch(r, kPushDeposit, binomial ? push_deposit_kernel<F, 0> : push_deposit_kernel<F, 1>,
+    TRY(launch(r, kPushDeposit,
+               r->deterministic
+                   ? (binomial ? push_deposit_kernel<F, 0, true> : push_deposit_kernel<F, 1, true>)
+                   : (binomial ? push_deposit_kernel<F, 0, false> : push_deposit_kernel<F, 1, false>),
                dim3(blocks_for(r->np, 128)), dim3(128),
                pa));
+    if (binomial && (r->deterministic ? kDeferChords<true> : kDeferChords<false>)) {
+      ChordArgs da{};
+      da.g = g;
+      da.count = (long long)r->np;
+      da.mode = r->dep_mode;
+      for (int d = 0; d < 3; ++d) {
+        da.b[d] = r->dep_b[d];
+        da.e[d] = r->dep_e[d];
+      }
+      da.q = r->p.q;
+      da.status = r->d_status;
+      TRY(launch(r, kChordDeposit,
+                 r->deterministic ? chord_deposit_kernel<true> : chord_deposit_kernel<false>,
+                 dim3(blocks_for(r->np, 128)), dim3(128), da));
+    }
     TRY(join_carriers());
+    TRY(convert_current());
     TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
                orbit[1], orbit[2], 1));
     ResidualArgs<F> ra{};
@@ -1406,11 +1526,14 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     ra.next_b = r->next_b;
     ra.abs_grid_work = r->abs_work;
     ra.sums = r->d_sums;
+    ra.partial = r->res_partial;
+    ra.ticket = r->res_ticket;
     ra.status = r->d_status;
     TRY(launch(r, kResidual, binomial ? residual_kernel<W, F, 0> : residual_kernel<W, F, 1>,
                dim3(blocks_for(r->np, 128)), dim3(128), ra));
   }
   TRY(join_carriers());
+  TRY(convert_current());
   if (ahead)
     TRY(launch(r, kTrialVerdict, trial_verdict_kernel, dim3(1), dim3(1),
                (const ResidualSums*)r->d_sums, r->trials + 1, c.force_tolerance,
@@ -1507,7 +1630,9 @@ aprl_status do_commit(aprl_run* r) {
     // few steps: re-sorting every kSortInterval steps kept push_deposit and
     // the residual at their sorted speed on the dipole and drift workloads
     // (1M particles: step 4.24 -> 4.14 ms against sorting every step; never
-    // sorting, 8.4 ms).  Storage order does not change any result.
+    // sorting, 8.4 ms).  Storage order changes no integer result; it changes
+    // J only to roundoff through the order of the FP64 atomics, and not at
+    // all in the deterministic mode, whose fixed-point sum is order-free.
     if (r->step % kSortInterval == 0) TRY(sort_particles(r));
   }
   add_counters(r->cumulative, tc);
@@ -1569,10 +1694,21 @@ aprl_status inlet_charge_match(aprl_run* r) {
   m.shape = c.shape;
   m.rho = r->inlet_rho;
   m.status = r->d_status;
-  CUDA_TRY(cudaMemsetAsync(r->inlet_rho, 0, (size_t)(c.nx + 1) * (c.ny + 1) * sizeof(double),
-                           r->stream));
+  const size_t nodes = (size_t)(c.nx + 1) * (c.ny + 1);
+  if (r->deterministic) {
+    m.rho_pairs = r->inlet_rho_pairs;
+    m.rho_scale = fixed_scale(4.0 * r->max_abs_charge / (c.dx * c.dy * c.dz));
+    CUDA_TRY(cudaMemsetAsync(r->inlet_rho_pairs, 0, 2 * nodes * sizeof(unsigned long long),
+                             r->stream));
+  } else {
+    CUDA_TRY(cudaMemsetAsync(r->inlet_rho, 0, nodes * sizeof(double), r->stream));
+  }
   TRY(launch(r, kInletCharge, inlet_charge_kernel, dim3(blocks_for(m.np + m.pcount, 128)),
              dim3(128), m));
+  if (r->deterministic)
+    TRY(launch(r, kFixedConvert, fixed_convert_kernel, dim3(blocks_for(nodes, 256)), dim3(256),
+               (const unsigned long long*)r->inlet_rho_pairs, r->inlet_rho, (long long)nodes,
+               1.0 / m.rho_scale));
   InletCompleteArgs ca{};
   ca.g = make_grid<double>(r);
   ca.rho = r->inlet_rho;
@@ -1766,10 +1902,19 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     r->tiles[a] = (int)((cells + (1u << kTileShift) - 1) >> kTileShift);
   }
   r->ntiles = (size_t)r->tiles[0] * r->tiles[1] * r->tiles[2];
-  if ((s = device_alloc(r, &r->tile_count, r->ntiles)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(r, &r->tile_offset, r->ntiles)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(r, &r->chunk_sum, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
-  if ((s = device_alloc(r, &r->chunk_offset, r->ntiles / 1024 + 1)) != APRL_OK) return cleanup(s);
+  while (r->sort_bits < 32 && ((size_t)1 << r->sort_bits) < r->ntiles) ++r->sort_bits;
+  if ((s = device_alloc(r, &r->res_ticket, 1)) != APRL_OK) return cleanup(s);
+  cudaMemsetAsync(r->res_ticket, 0, sizeof(unsigned), r->stream);
+  r->deterministic = c.deterministic != 0;
+  if (r->deterministic) {
+    for (int a = 0; a < 3; ++a) {
+      if ((s = device_alloc(r, &r->jq[a], 2 * e_count(c, a))) != APRL_OK) return cleanup(s);
+      cudaMemsetAsync(r->jq[a], 0, 2 * e_count(c, a) * sizeof(unsigned long long), r->stream);
+    }
+    if (c.inlet_charge_match &&
+        (s = device_alloc(r, &r->inlet_rho_pairs, 2 * (size_t)(c.nx + 1) * (c.ny + 1))) != APRL_OK)
+      return cleanup(s);
+  }
   if ((s = device_alloc(r, &r->d_counters, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(r, &r->d_sums, 1)) != APRL_OK) return cleanup(s);
   if ((s = device_alloc(r, &r->d_status, 1)) != APRL_OK) return cleanup(s);
@@ -1844,20 +1989,27 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   double* singles[] = {r->x1,       r->y1,       r->z1,       r->ux1,        r->uy1,
                        r->uz1,      r->used_e,   r->used_b,   r->next_e,     r->next_b,
                        r->abs_work, r->slots.x0, r->slots.y0, r->slots.z0,   r->slots.dt,
-                       r->d_detector};
+                       r->d_detector, r->dep_b[0], r->dep_b[1], r->dep_b[2], r->dep_e[0],
+                       r->dep_e[1], r->dep_e[2]};
   for (double* d : singles) device_free(r, d);
   device_free(r, r->slots.seen);
   device_free(r, r->frozen1);
   free_pending(r, r->queue.d);
   device_free(r, r->action);
+  device_free(r, r->dep_mode);
   device_free(r, r->born_keep);
   device_free(r, r->slot_order);
-  device_free(r, r->tile_of);
-  device_free(r, r->tile_rank);
-  device_free(r, r->tile_count);
-  device_free(r, r->tile_offset);
+  for (int k = 0; k < 2; ++k) {
+    device_free(r, r->sort_key[k]);
+    device_free(r, r->sort_index[k]);
+  }
+  device_free(r, r->radix_count);
   device_free(r, r->chunk_sum);
   device_free(r, r->chunk_offset);
+  device_free(r, r->res_partial);
+  device_free(r, r->res_ticket);
+  for (int a = 0; a < 3; ++a) device_free(r, r->jq[a]);
+  device_free(r, r->inlet_rho_pairs);
   free_carriers(r, r->born);
   free_carriers(r, r->c);
   free_carriers(r, r->c_alt);
@@ -1999,6 +2151,7 @@ aprl_status aprl_run_set_particles(aprl_run* r, size_t n, const double* x, const
       return fail(APRL_ERR_INVALID_ARGUMENT, "Particle %zu has a non-finite state or nonpositive mass", i);
   TRY(reserve_particles(r, n));
   TRY(reserve_carriers(r, 1));
+  note_charges(r, q, n);
   r->np = 0;
   const double* src[] = {x, y, z, ux, uy, uz, q, m};
   double* dst[] = {r->p.x, r->p.y, r->p.z, r->p.ux, r->p.uy, r->p.uz, r->p.q, r->p.m};
@@ -2231,7 +2384,9 @@ aprl_status aprl_run_set_carriers(aprl_run* r, size_t n, const double* pos, cons
                                   const double* q, const double* w) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
   if (r->stage != 0) return fail(APRL_ERR_RUNTIME, "Carriers can only be replaced between steps");
+  if (n && (!pos || !vel || !q || !w)) return fail(APRL_ERR_INVALID_ARGUMENT, "null carrier array");
   TRY(reserve_carriers(r, n));
+  note_charges(r, q, n);
   std::vector<double> t(n);
   double* comps[] = {r->c.px, r->c.py, r->c.pz, r->c.vx, r->c.vy, r->c.vz};
   for (int k = 0; k < 6; ++k) {
@@ -2296,11 +2451,15 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
                              r->stream));
     TRY(check_device(r));
     unsigned t = 0;
+    // forceHistory / workHistory of the reference's failure message.
+    std::vector<double> history;
     while (!converged && t < ahead) {
       double res[4];
       trial_read(r, (int)t, res);
       iterations = ++t;
       converged = trial_converged(r->cfg, iterations, res, force, work);
+      history.push_back(force);
+      history.push_back(work);
     }
     if ((converged ? (int)iterations : 0) != *r->h_stop)
       return fail(APRL_ERR_RUNTIME, "Device and host verdicts on the coupling trials differ");
@@ -2309,11 +2468,27 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
       TRY(do_trial(r, res));
       iterations = t + 1;
       converged = trial_converged(r->cfg, iterations, res, force, work);
+      history.push_back(force);
+      history.push_back(work);
     }
-    if (!converged)
-      return fail(APRL_ERR_NOT_CONVERGED,
-                  "Conservative source coupling failed at step %llu: force=%g work=%g iterations=%u",
-                  (unsigned long long)(r->step + 1), force, work, iterations);
+    if (!converged) {
+      // The reference's message (src/simulation_source_coupling.cpp:54):
+      // the last residual, the trial count and every trial's force/work.
+      std::string text;
+      char item[64];
+      std::snprintf(item, sizeof item, "%g", force);
+      text = "Conservative source coupling failed at step " + std::to_string(r->step + 1) +
+             ": force=" + item;
+      std::snprintf(item, sizeof item, "%g", work);
+      text += std::string(" work=") + item + " iterations=" + std::to_string(iterations) +
+              " history(force/work)=";
+      for (size_t h = 0; h + 1 < history.size(); h += 2) {
+        std::snprintf(item, sizeof item, " %g/%g", history[h], history[h + 1]);
+        text += item;
+      }
+      g_error = text;
+      return APRL_ERR_NOT_CONVERGED;
+    }
     r->last_iterations = iterations;
     r->max_iterations = std::max(r->max_iterations, iterations);
     r->total_iterations += iterations;
@@ -3057,13 +3232,11 @@ aprl_status aprl_run_sample_field_plane_noalloc(aprl_run* r, double plane_lab_z,
   axis(coordinate, c.nz + 1, &da.vertex_lower, &da.vertex_fraction);
   axis(coordinate - 0.5, c.nz, &da.half_lower, &da.half_fraction);
   da.out = scratch;
-  // A direct launch: no timing events are created on this path.
+  // The run's launch helper: with profiling on it times the kernel with CUDA
+  // events (host-side objects, not device memory), like every other launch.
   const dim3 grid(blocks_for(c.nx, 32), blocks_for(c.ny, 8)), block(32, 8);
-  detector_plane_kernel<double><<<grid, block, 0, r->stream>>>(
-      retyped<double>(da, make_grid<double>(r)));
-  CUDA_TRY(cudaGetLastError());
-  ++r->kernel_launches[kDetectorPlane];
-  ++r->launches;
+  TRY(launch(r, kDetectorPlane, detector_plane_kernel<double>, grid, block,
+             retyped<double>(da, make_grid<double>(r))));
   CUDA_TRY(cudaMemcpyAsync(out, scratch, count * 8, cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
   return APRL_OK;

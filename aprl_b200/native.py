@@ -90,6 +90,7 @@ class AprlError(RuntimeError):
     def __init__(self, status, message):
         super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
         self.status = status
+        self.message = message
 
 
 class Binding:

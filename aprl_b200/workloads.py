@@ -116,6 +116,13 @@ def with_precision(cfg, precision):
     return out
 
 
+def with_determinism(cfg, deterministic=True):
+    """A copy of `cfg` with the bit-reproducible current summation on or off."""
+    out = abi.RunConfig.from_buffer_copy(bytes(cfg))
+    out.deterministic = 1 if deterministic else 0
+    return out
+
+
 def make_config(nx, ny, nz, dx, dy, dz, cpml_cells, boost_gamma, shape,
                 steps, substeps=1, magnets=(), right_margin=None,
                 translation_beta=1.0, release_cells=6):

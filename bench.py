@@ -49,9 +49,13 @@ def parse_args(argv=None):
     p.add_argument("--particles", type=int, default=None)
     p.add_argument("--shape", default="linear-binomial3")
     p.add_argument("--precision", choices=["fp64", "fp32-mixed"], default=None)
+    p.add_argument("--deterministic", action="store_true",
+                   help="sum the current in the bit-reproducible fixed-point mode")
     p.add_argument("--no-fp32-arm", action="store_true",
                    help="skip the FP32-mixed comparison pass of an FP64 run")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-other-configs", action="store_true",
+                   help="skip the drift, quintic and bit-reproducible step rates")
     p.add_argument("--no-scan", action="store_true",
                    help="skip the batched-ensemble and served-scan measurements")
     p.add_argument("--ensemble-runs", type=int, default=32)
@@ -218,16 +222,35 @@ MEASURED_TRAFFIC = {"push_deposit": ("particle", 349.0),
 RED_SECTORS_PER_PARTICLE = 90.4
 
 
-def atomic_peak():
-    """Measured L2 FP64 reduction rate of this GPU (aprl_b200/csrc/probe.cu):
-    every lane adds to its own 32-byte sector of a 16 MB window, neighbouring
-    lanes on neighbouring sectors, as the cell-sorted deposit's reductions
-    land; best of 5 launches, in G reductions/s."""
-    import ctypes
+PROBE_SOURCE = os.path.join(REPO, "bench_probe.cu")
+PROBE_OUTPUT = os.path.join(REPO, "bench_probe.so")
+
+
+def build_probe(force=False, verbose=True):
+    """The benchmark's measurement probe (bench_probe.so, sm_100a)."""
+    if (not force and os.path.exists(PROBE_OUTPUT) and
+            os.path.getmtime(PROBE_SOURCE) <= os.path.getmtime(PROBE_OUTPUT)):
+        return PROBE_OUTPUT
     from aprl_b200 import build as product_build
-    lib = ctypes.CDLL(product_build.build_probe(verbose=False))
+    cmd = [product_build.nvcc(), "-shared", "-o", PROBE_OUTPUT, PROBE_SOURCE, "-std=c++17",
+           "-O3", "-Xcompiler", "-fPIC"] + product_build.ARCH
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return PROBE_OUTPUT
+
+
+def atomic_peak(integer=False):
+    """Measured L2 reduction rate of this GPU (bench_probe.cu): every lane
+    adds to its own 32-byte sector of a 16 MB window, neighbouring lanes on
+    neighbouring sectors, as the cell-sorted deposit's reductions land; best
+    of 5 launches, in G reductions/s.  Binary64 adds (the default deposit),
+    or 64-bit integer adds (the deterministic deposit)."""
+    import ctypes
+    lib = ctypes.CDLL(build_probe(verbose=False))
     rate = ctypes.c_double()
-    if lib.aprl_probe_reduction_rate(16, 5, ctypes.byref(rate)) != 0:
+    probe = lib.aprl_probe_integer_reduction_rate if integer else lib.aprl_probe_reduction_rate
+    if probe(16, 5, ctypes.byref(rate)) != 0:
         return None
     return rate.value / 1e9
 
@@ -266,6 +289,8 @@ def run_ours(args):
     total_steps = W + 2 * K + 4
     make, magnet = WORKLOADS[args.workload]
     w = make(total_steps, args, 17 + rank)
+    if args.deterministic:
+        w.config = workloads.with_determinism(w.config)
     cfg = w.config
     lib = native.load()
 
@@ -423,7 +448,7 @@ def run_ours(args):
             "achieved": achieved_atomic, "peak": peak_atomic, "unit": "G reductions/s",
             "frac": achieved_atomic / peak_atomic if peak_atomic else None,
             "peak_source": "measured here: one FP64 reduction per lane per 32-byte sector, "
-                           "neighbouring sectors, 16 MB window (aprl_b200/csrc/probe.cu)",
+                           "neighbouring sectors, 16 MB window (bench_probe.cu)",
             "reductions_per_particle": RED_SECTORS_PER_PARTICLE,
             "note": "whole push_deposit launch time, push arithmetic included"}
     kernels = {k: {"ms": v[0], "launches": v[1],
@@ -476,9 +501,61 @@ def run_ours(args):
         line.update(scan_benchmarks(args))
     if world == 1 and args.workload == "dipole" and not args.no_self_field:
         line.update(self_field_benchmark(args, stream))
+    if world == 1 and args.workload == "dipole" and not args.no_other_configs:
+        line["other_configs"] = other_configs(args, stream)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
+
+
+def other_configs(args, stream):
+    """Device-resident step rates of the other single-GPU configurations,
+    W warm-up and K timed steps each (CUDA events on the run's stream): the
+    plain FP64 drift (64x64x256, 100k), the dipole workload with the
+    quintic-compensated shape, and the dipole workload in the bit-reproducible
+    current mode."""
+    import torch
+    K, W = args.steps, args.warmup
+    cases = {
+        "drift_64x64x256_100k_binomial3_fp64": lambda: workloads.drift_c1(
+            steps=W + K + 4, particles=100_000, seed=17),
+        "dipole_128x128x512_1M_quintic_fp64": lambda: workloads.dipole_c2(
+            steps=W + K + 4, particles=args.particles, shape="quintic-compensated", seed=17),
+        "dipole_128x128x512_1M_binomial3_fp64_deterministic": lambda: workloads.dipole_c2(
+            steps=W + K + 4, particles=args.particles, seed=17),
+    }
+    out = {}
+    lib = native.load()
+    for name, make in cases.items():
+        w = make()
+        cfg = w.config
+        if name.endswith("deterministic"):
+            cfg = workloads.with_determinism(cfg)
+        run = native.Run(lib, cfg, stream=stream.cuda_stream)
+        run.set_reference(w.reference)
+        run.set_particles(w.particles)
+        for _ in range(W):
+            run.step(1)
+        run.synchronize()
+        run.b("run_reset_iteration_stats", run.handle)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ps = 0
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(K):
+            ps += run.particle_count()
+            run.step(1)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+        stats = run.stats()
+        run.close()
+        out[name] = {"value": ps / (ms * 1e-3), "unit": "particle-steps/s",
+                     "ms_per_step": ms / K, "steps": K, "warmup": W,
+                     "cells": list(w.description["cells"]),
+                     "particles": int(w.particles["x"].size),
+                     "fixed_point_trials_mean": stats["total_iterations"] / max(K, 1)}
+    return out
 
 
 def time_fp32_arm(args, w, stream, fp64_run, detector_lab_z, world):
@@ -678,17 +755,11 @@ def scan_benchmarks(args):
     return out
 
 
-def reference_sample_workload(args, steps, seed=17):
-    """A bounded slice of the benchmark workload for the CPU: the full
-    transverse grid and 1/8 of the window length with 1/8 of the particles
-    (same particles per cell)."""
-    cfg = workloads.make_config(128, 128, 64, 5e-6, 5e-6, 2e-6, 10, 10.0, args.shape,
-                                steps, magnets=[workloads.dipole(1.0)], right_margin=8)
-    bunch = workloads.gaussian_bunch(cfg, max(args.particles // 8, 1), 100e-12 / 8, 1e9,
-                                     50e-6, 20e-6, 1e-6, 1e-4, seed=seed,
-                                     z_fraction=(0.05, 0.95))
-    return workloads.Workload("dipole-slice-128x128x64", cfg, bunch,
-                              workloads.synthetic_reference(cfg), steps=steps)
+def reference_workload(args, steps, seed=17):
+    """The benchmark workload itself (same grid, bunch, seed and inlet as the
+    GPU arm's rank 0), for the reference's CPU translation units."""
+    make, _ = WORKLOADS[args.workload]
+    return make(steps, args, seed)
 
 
 def _cpu_checker():
@@ -704,8 +775,9 @@ def _cpu_checker():
 def cpu_baseline(args):
     binding, kind, cores = _cpu_checker()
     steps = 3
-    w = reference_sample_workload(args, steps + 1)
+    w = reference_workload(args, steps + 2)
     run = native.Run(binding, w.config).load_workload(w)
+    run.step(1)  # warm-up
     done, ps, t0 = 0, 0, time.perf_counter()
     while done < steps:
         ps += run.particle_count()
@@ -716,8 +788,8 @@ def cpu_baseline(args):
     elapsed = time.perf_counter() - t0
     run.close()
     out = {"value": ps / elapsed, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-           "sample": f"{done} steps of a 128x128x64-cell slice with "
-                     f"{w.particles['x'].size} particles (1/8 of the window and bunch)"}
+           "sample": f"{done} steps (after one warm-up step) of the full workload, "
+                     f"{w.description['cells']} cells with {w.particles['x'].size} particles"}
     # The initial self-field solve of the same checker on the small solve
     # case that the GPU leg also times (initial_self_field.small).
     sw = workloads.self_field_case(SELF_FIELD_SMALL["energy_ev"], nx=SELF_FIELD_SMALL["cells"][0],
@@ -739,7 +811,7 @@ def run_reference(args):
         return
     binding, kind, cores = _cpu_checker()
     K, W = args.steps, args.warmup
-    w = reference_sample_workload(args, K + W + 2)
+    w = reference_workload(args, K + W + 2)
     run = native.Run(binding, w.config).load_workload(w)
     for _ in range(W):
         run.step(1)
@@ -752,15 +824,18 @@ def run_reference(args):
     stats = run.stats()
     run.close()
     value = ps / elapsed
-    sample = (f"each step: one reference step of a 128x128x64-cell slice with "
-              f"{w.particles['x'].size} particles (1/8 of the window and bunch)")
+    sample = (f"each step: one reference step of the full workload, "
+              f"{w.description['cells']} cells with {w.particles['x'].size} particles")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K, "warmup": W,
         "ms_per_step": elapsed * 1e3 / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "dipole-128x128x512", "sample": w.name,
-                   "shape": args.shape, "precision": "fp64"},
+        "config": {"workload": w.name, "cells": list(w.description["cells"]),
+                   "particles": args.particles, "shape": args.shape,
+                   "precision": "fp64-drop-in" if args.precision == "fp64" else "fp32-mixed",
+                   "magnet": WORKLOADS[args.workload][1], "boost_gamma": w.config.boost_gamma,
+                   "parallelism": "replicas1", "same_config": True},
         "fixed_point_trials": {"mean": stats["total_iterations"] / max(K + W, 1),
                                "max": stats["max_iterations"]},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
@@ -770,8 +845,24 @@ def run_reference(args):
     }), flush=True)
 
 
+def launch_replicas(args, argv):
+    """`--gpus N` without a launcher: start N ranks (one per GPU) through
+    torch.distributed.run on this node and pass rank 0's line through."""
+    import socket
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+    return subprocess.call(cmd)
+
+
 def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
     args = parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_replicas(args, argv))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define APRL_GPU_ABI_VERSION 1
+#define APRL_GPU_ABI_VERSION 2
 
 typedef enum {
   APRL_OK = 0,
@@ -141,6 +141,21 @@ typedef struct {
    * (src/moving_window_fields.cpp:225-236). */
   uint32_t inlet_charge_match;
   aprl_magnet magnets[APRL_MAX_MAGNETS];
+  /* Bit-reproducible mode (no counterpart in the reference, whose deposit is
+   * serial and therefore repeatable).  0: the current J is summed with FP64
+   * atomics, whose order -- and so the last bits of J -- varies from run to
+   * run.  1: every deposit contribution is rounded once to a 128-bit fixed
+   * point (2^-62 of the run's largest possible single contribution,
+   * 4*max|q|*c/(dx*dy*dz)) and summed as integers, which is exact and
+   * order-free, then converted to binary64 once per trial; the charge-matched
+   * inlet's layer charge is summed the same way.  Two runs of the same
+   * requests then give identical bits on the same GPU, and J is closer to
+   * the exact sum than either the FP64 atomics or the reference's serial
+   * binary64 sum.  The particle sort, the compactions and the residual sums
+   * are deterministic in both modes.  Costs a second L2 reduction per
+   * contribution and one grid pass per trial. */
+  uint32_t deterministic;
+  uint32_t reserved_flags;        /* 0 */
 } aprl_run_config;
 
 /* Per-step results of the coupled step (SourceCoupling log row,

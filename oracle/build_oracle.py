@@ -8,6 +8,10 @@
   Built only where the APRL source tree is present; the built library then
   travels with the repository copy.
 
+The APRL source tree (its src/ folder) is taken from --reference-src, else
+from the environment variable APRL_REFERENCE_SRC, else from a checkout named
+`reference` beside this repository (../reference/src).
+
 Usage: python oracle/build_oracle.py [--reference-src DIR]
 """
 import argparse
@@ -17,7 +21,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-DEFAULT_REFERENCE_SRC = "/root/reference/src"
+
+
+def default_reference_src():
+    return os.environ.get("APRL_REFERENCE_SRC") or os.path.join(
+        os.path.dirname(REPO), "reference", "src")
 
 # The hot-path translation units of APRL 2.1 that compile against the MPI
 # stand-in (the remaining ones need HDF5, yaml-cpp or FFTW).
@@ -88,10 +96,10 @@ def build_reference(reference_src):
 
 def main(argv=None):
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference-src", default=DEFAULT_REFERENCE_SRC)
+    parser.add_argument("--reference-src", default=None)
     args = parser.parse_args(argv)
     build_oracle()
-    build_reference(args.reference_src)
+    build_reference(args.reference_src or default_reference_src())
 
 
 if __name__ == "__main__":

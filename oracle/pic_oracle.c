@@ -29,7 +29,7 @@
 #define K_PI 3.14159265358979323846
 #define K_TWO_PI (2.0 * K_PI)
 
-static __thread char g_error[512];
+static __thread char g_error[4096];
 
 static aprl_status fail(aprl_status status, const char* format, ...) {
   va_list args;
@@ -2896,6 +2896,7 @@ aprl_status oracle_run_step(oracle_run* r, uint32_t steps) {
     int converged = 0;
     unsigned iterations = 0;
     double force = 0., work = 0.;
+    double history[2 * 64];
     for (unsigned t = 0; t < r->cfg.max_trials; ++t) {
       double res[4];
       s = oracle_run_coupling_trial(r, res);
@@ -2903,16 +2904,28 @@ aprl_status oracle_run_step(oracle_run* r, uint32_t steps) {
       force = res[0];
       work = res[3] == 0. ? 0. : (res[2] > 0. ? res[1] / res[2] : res[1]);
       iterations = t + 1;
+      if (t < 64) {
+        history[2 * t] = force;
+        history[2 * t + 1] = work;
+      }
       if (iterations >= (res[3] > 0. ? 2u : 1u) && force < r->cfg.force_tolerance &&
           work < r->cfg.work_tolerance) {
         converged = 1;
         break;
       }
     }
-    if (!converged)
-      return fail(APRL_ERR_NOT_CONVERGED,
-                  "Conservative source coupling failed at step %llu: force=%g work=%g iterations=%u",
-                  (unsigned long long)(r->step + 1), force, work, iterations);
+    if (!converged) {
+      /* The message of src/simulation_source_coupling.cpp:54, with the
+       * per-trial force/work history. */
+      int at = snprintf(g_error, sizeof g_error,
+                        "Conservative source coupling failed at step %llu: force=%g work=%g "
+                        "iterations=%u history(force/work)=",
+                        (unsigned long long)(r->step + 1), force, work, iterations);
+      for (unsigned t = 0; t < iterations && t < 64 && at > 0 && at < (int)sizeof g_error; ++t)
+        at += snprintf(g_error + at, sizeof g_error - (size_t)at, " %g/%g", history[2 * t],
+                       history[2 * t + 1]);
+      return APRL_ERR_NOT_CONVERGED;
+    }
     r->last_iterations = iterations;
     if (iterations > r->max_iterations) r->max_iterations = iterations;
     r->total_iterations += iterations;

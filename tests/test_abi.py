@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function():
 
 def test_abi_version_and_struct_layout():
     b = native.load()
-    assert b.fn["abi_version"]() == 1
+    assert b.fn["abi_version"]() == 2
     # Layout of the plain-data structs as the C compiler sees them.
     assert C.sizeof(abi.Magnet) == 8 + 3 * 8 + 10 * 8
     assert abi.RunConfig.magnets.offset % 8 == 0

@@ -17,7 +17,7 @@ STATS = ("iterations", "total_iterations", "exits", "carriers", "particles",
 
 def load_case(name):
     d = np.load(os.path.join(HERE, name + ".npz"))
-    cfg = abi.RunConfig.from_buffer_copy(d["config"].tobytes())
+    cfg = abi.RunConfig.from_bytes(d["config"].tobytes())
     return cfg, d
 
 
