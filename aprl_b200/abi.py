@@ -278,7 +278,7 @@ SCAN_QUEUED, SCAN_RUNNING, SCAN_DONE = 0, 1, 2
 class ScanConfig(C.Structure):
     _fields_ = [("device_budget_bytes", C.c_uint64),
                 ("max_slots", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("runs_per_slot", C.c_uint32)]
 
 
 _PD = C.POINTER(C.c_double)

@@ -35,27 +35,42 @@ def flags():
             "-I", os.path.join(REPO, "include")] + ARCH
 
 
-def build(force=False, verbose=True):
+# The bounds-checked variant: every field, current, orbit-sum, CPML-history
+# and inlet-plane index of the step's kernels is tested before the access; an
+# index outside its array raises the run's device error instead of touching
+# memory (never a trap).  Slower; for testing.
+CHECKED_OUTPUT = os.path.join(HERE, "libaprl_b200_checked.so")
+
+
+def _build_library(output, objdir, extra, force, verbose):
     deps = ([os.path.join(CSRC, s) for s in SOURCES + HEADERS] +
-            [os.path.join(REPO, "include", "aprl_gpu.h")])
-    if (not force and os.path.exists(OUTPUT) and
-            all(os.path.getmtime(d) <= os.path.getmtime(OUTPUT) for d in deps)):
-        return OUTPUT
-    objdir = os.path.join(HERE, "_build")
+            [os.path.join(REPO, "include", "aprl_gpu.h"), os.path.abspath(__file__)])
+    if (not force and os.path.exists(output) and
+            all(os.path.getmtime(d) <= os.path.getmtime(output) for d in deps)):
+        return output
     os.makedirs(objdir, exist_ok=True)
     objects = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), "-rdc=false", "-c", os.path.join(CSRC, src), "-o", obj] + flags()
+        cmd = [nvcc(), "-rdc=false", "-c", os.path.join(CSRC, src), "-o", obj] + flags() + extra
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
         objects.append(obj)
-    cmd = [nvcc(), "-shared", "-o", OUTPUT] + objects + ARCH + ["-lcudart"]
+    cmd = [nvcc(), "-shared", "-o", output] + objects + ARCH + ["-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
-    return OUTPUT
+    return output
+
+
+def build(force=False, verbose=True):
+    return _build_library(OUTPUT, os.path.join(HERE, "_build"), [], force, verbose)
+
+
+def build_checked(force=False, verbose=True):
+    return _build_library(CHECKED_OUTPUT, os.path.join(HERE, "_build_checked"),
+                          ["-DAPRL_GPU_BOUNDS_CHECK"], force, verbose)
 
 
 def main(argv=None):
@@ -63,6 +78,7 @@ def main(argv=None):
     parser.add_argument("--force", action="store_true")
     args = parser.parse_args(argv)
     build(force=args.force)
+    build_checked(force=args.force)
 
 
 if __name__ == "__main__":

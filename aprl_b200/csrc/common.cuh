@@ -55,6 +55,7 @@ enum DeviceError : unsigned {
   kErrInletSource = 20,       // non-finite charge-matched inlet source
   kErrInletField = 21,        // non-finite charge-matched inlet field
   kErrFixedRange = 22,        // deterministic deposit: contribution beyond the fixed-point range
+  kErrBounds = 23,            // bounds-checked build: an index outside its array
   kErrCount
 };
 
@@ -67,6 +68,27 @@ __device__ __forceinline__ void raise_error(DeviceStatus* s, unsigned code,
                                             unsigned long long where) {
   if (atomicCAS(&s->code, 0u, code) == 0u) s->where = where;
 }
+
+// The bounds-checked build (-DAPRL_GPU_BOUNDS_CHECK, libaprl_b200_checked.so):
+// every field, current, orbit-sum, CPML-history and inlet-plane index of the
+// step's kernels is tested against its array before the access.  An index
+// outside raises kErrBounds in the run's status word with `site` (which
+// access) in the top 16 bits of the recorded element and the index below,
+// and the access goes to element 0 instead: the kernel never touches memory
+// outside its arrays and never traps.  In the normal build the checks
+// compile to nothing.
+#ifdef APRL_GPU_BOUNDS_CHECK
+__device__ __forceinline__ size_t bounded(DeviceStatus* s, size_t index, size_t extent,
+                                          unsigned site) {
+  if (index < extent) return index;
+  if (s) raise_error(s, kErrBounds, ((unsigned long long)site << 48) | (index & 0xffffffffffffull));
+  return 0;
+}
+#define APRL_BOUNDED(status, index, extent, site) \
+  ::aprl_gpu::bounded((status), (size_t)(index), (size_t)(extent), (site))
+#else
+#define APRL_BOUNDED(status, index, extent, site) ((size_t)(index))
+#endif
 
 // One magnet of SIFieldSourceSet (src/eb_sources.h:103-140).
 struct DMagnet {
@@ -108,6 +130,7 @@ struct GridT {
   // on the previous one: nonzero once an earlier trial of the step has
   // converged, and the trial's kernels then return at once.
   const int* stop;
+  DeviceStatus* status;  // the run's status word (the bounds-checked build reports here)
 };
 
 // True when the trial this grid view belongs to was made unnecessary.
@@ -135,21 +158,51 @@ __device__ __forceinline__ int ring(int k, int base, int n) {
   return p >= n ? p - n : p;
 }
 
+#ifdef APRL_GPU_BOUNDS_CHECK
+// (i, j, k) inside an nx x ny x nz component, else kErrBounds and node 0.
+__device__ __forceinline__ bool node_inside(DeviceStatus* s, int i, int j, int k, int nx, int ny,
+                                            int nz, unsigned site) {
+  if (i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz) return true;
+  if (s) raise_error(s, kErrBounds, ((unsigned long long)site << 48) |
+                                        ((unsigned long long)(unsigned)k << 24) |
+                                        (((unsigned long long)(unsigned)j & 0xfffull) << 12) |
+                                        ((unsigned long long)(unsigned)i & 0xfffull));
+  return false;
+}
+#define APRL_NODE_CHECK(g, i, j, k, nx, ny, nz, site) \
+  if (!node_inside((g).status, (i), (j), (k), (nx), (ny), (nz), (site))) return 0
+#else
+#define APRL_NODE_CHECK(g, i, j, k, nx, ny, nz, site)
+#endif
+
 template <class F>
 __device__ __forceinline__ size_t e_index(const GridT<F>& g, int c, int i, int j, int k) {
   const int nzc = e_nz(g, c);
+  APRL_NODE_CHECK(g, i, j, k, e_nx(g, c), e_ny(g, c), nzc, 1 + c);
   return ((size_t)ring(k, g.zb_e[c], nzc) * e_ny(g, c) + j) * e_nx(g, c) + i;
 }
 
 template <class F>
 __device__ __forceinline__ size_t b_index(const GridT<F>& g, int c, int i, int j, int k) {
   const int nzc = b_nz(g, c);
+  APRL_NODE_CHECK(g, i, j, k, b_nx(g, c), b_ny(g, c), nzc, 4 + c);
   return ((size_t)ring(k, g.zb_b[c], nzc) * b_ny(g, c) + j) * b_nx(g, c) + i;
 }
 
 template <class F>
 __device__ __forceinline__ size_t j_index(const GridT<F>& g, int c, int i, int j, int k) {
+  APRL_NODE_CHECK(g, i, j, k, e_nx(g, c), e_ny(g, c), e_nz(g, c), 7 + c);
   return ((size_t)k * e_ny(g, c) + j) * e_nx(g, c) + i;
+}
+
+// Elements of E component c (also of J and of the orbit sum) and of B component c.
+template <class F>
+__device__ __forceinline__ size_t e_count(const GridT<F>& g, int c) {
+  return (size_t)e_nx(g, c) * e_ny(g, c) * e_nz(g, c);
+}
+template <class F>
+__device__ __forceinline__ size_t b_count(const GridT<F>& g, int c) {
+  return (size_t)b_nx(g, c) * b_ny(g, c) * b_nz(g, c);
 }
 
 // applyCurrentSource's interior mask (src/source_coupling.cpp:87) at one rank.
@@ -225,6 +278,46 @@ __device__ __forceinline__ double fixed_value(unsigned long long lo, unsigned lo
     m = ldexp(__ull2double_rn(top), 64 - lz);
   }
   return (negative ? -m : m) * unscale;
+}
+
+// ---------------------------------------------------------------------------
+// The quintic-compensated node and edge bases, shared by the deposit, the
+// gathers, the charge-matched inlet and the Gauss-law node density.
+template <class F>
+struct Basis {
+  long long first;
+  int count;
+  F v[12];
+};
+
+// basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54): the
+// cell in binary64, the B-spline and compensation arithmetic in F on the
+// cell-relative offset.
+template <class F>
+__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) {
+  const unsigned degree = edge ? 4 : 5;
+  const double cell = floor(z);
+  const F f = F(z - cell);
+  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
+  for (unsigned j = 1; j <= degree; ++j) {
+    F saved = F(0.);
+    for (unsigned k = 0; k < j; ++k) {
+      const F t = n[k] / F(j);
+      n[k] = saved + (F(k + 1) - f) * t;
+      saved = (f + F(j) - F(k) - F(1)) * t;
+    }
+    n[j] = saved;
+  }
+  const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
+               d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
+  const F c[7] = {F(-d / 64.), F(b / 16. + 3 * d / 32.), F(-a / 4. - b / 4. - 15 * d / 64.),
+                  F(1 + a / 2. + 3 * b / 8. + 5 * d / 16.),
+                  F(-a / 4. - b / 4. - 15 * d / 64.), F(b / 16. + 3 * d / 32.), F(-d / 64.)};
+  r.first = (long long)cell - 5;
+  r.count = degree + 7;
+  for (int q = 0; q < 12; ++q) r.v[q] = F(0.);
+  for (unsigned j = 0; j <= degree; ++j)
+    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
 }
 
 // BoostFrameTransform::gammaFromProperVelocity (src/boostframe.cpp:74-87).

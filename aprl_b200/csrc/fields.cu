@@ -33,9 +33,12 @@ __device__ __forceinline__ double electric_value(const CowanArgs<F>& a, int c, i
   } else if (j >= nyc) {
     if (c == 1) j = nyc - 1; else { j = 2 * (nyc - 1) - j; sign = -sign; }
   }
-  if (k < 0) return sign * a.lower[c][(size_t)j * nxc + i];
+  if (k < 0)
+    return sign * a.lower[c][APRL_BOUNDED(a.g.status, (size_t)j * nxc + i, (size_t)nxc * nyc, 10 + c)];
   if (k >= nzc) return sign * 0.0;
-  return sign * a.e[c][((size_t)ring(k, a.g.zb_e[c], nzc) * nyc + j) * nxc + i];
+  return sign * a.e[c][APRL_BOUNDED(a.g.status,
+                                    ((size_t)ring(k, a.g.zb_e[c], nzc) * nyc + j) * nxc + i,
+                                    (size_t)nxc * nyc * nzc, 13 + c)];
 }
 
 // transformedCorrection (src/eb_cpml.cpp:131-138).
@@ -47,8 +50,12 @@ __device__ __forceinline__ double cpml_correction(const CpmlAxis& ax, int index,
 }
 
 __device__ __forceinline__ double* history_at(const CpmlHistory& h, int slot, int k, int zbase,
-                                              int row_index) {
-  return h.data + ((size_t)slot * h.layers + ring(k, zbase, h.layers)) * h.row + row_index;
+                                              int row_index, DeviceStatus* status) {
+  (void)status;
+  return h.data + APRL_BOUNDED(status,
+                               ((size_t)slot * h.layers + ring(k, zbase, h.layers)) * h.row +
+                                   row_index,
+                               (size_t)h.slots * h.layers * h.row, 16);
 }
 
 // advanceMagneticCowan (src/eb_field.cpp:488-558) fused with
@@ -142,7 +149,7 @@ __device__ __forceinline__ void load_plane(ETile& t, const CowanArgs<F>& a, int 
         const int ii = n % W, jj = n / W;
         const int i = i0 - 1 + ii, j = j0 - 1 + jj;
         if (interior)
-          x = plane[(size_t)j * nxc + i];
+          x = plane[APRL_BOUNDED(a.g.status, (size_t)j * nxc + i, (size_t)nxc * nyc, 19 + c)];
         else if (!(i < -1 || i > nxc || j < -1 || j > nyc))
           x = electric_value(a, c, i, j, k);
       }
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         const int s = a.my.ordinal[j];
         if (s >= 0)
           v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
-                                             history_at(a.h[0], s, k, g.zb_b[0], i));
+                                             history_at(a.h[0], s, k, g.zb_b[0], i, g.status));
         *bx = v;
       }
       if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         const int s = a.mx.ordinal[i];
         if (s >= 0)
           v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
-                                            history_at(a.h[1], s, k, g.zb_b[1], j));
+                                            history_at(a.h[1], s, k, g.zb_b[1], j, g.status));
         *by = v;
       }
       if (i < g.nx && j < g.ny) {  // Bz (nx, ny, nz+1)
@@ -212,11 +219,11 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         const int sx = a.mx.ordinal[i];
         if (sx >= 0)
           v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,
-                                             history_at(a.h[2], sx, k, g.zb_b[2], j));
+                                             history_at(a.h[2], sx, k, g.zb_b[2], j, g.status));
         const int sy = a.my.ordinal[j];
         if (sy >= 0)
           v += 1.0 * dtdy * cpml_correction(a.my, j, dExDy,
-                                            history_at(a.h[3], sy, k, g.zb_b[2], i));
+                                            history_at(a.h[3], sy, k, g.zb_b[2], i, g.status));
         *bz = v;
       }
     }
@@ -267,12 +274,13 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       if (s >= 0) {
         const double diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
         v += 1.0 * cy * cpml_correction(a.ey_prof, j, diff,
-                                        history_at(a.h[0], s, k, g.zb_e[0], i));
+                                        history_at(a.h[0], s, k, g.zb_e[0], i, g.status));
       }
     }
     if (j == 0 || j == g.ny) v = 0.0;
     if (k == 0) {
-      if (a.pre_inlet[0]) a.pre_inlet[0][(size_t)j * g.nx + i] = v;
+      if (a.pre_inlet[0])
+        a.pre_inlet[0][APRL_BOUNDED(g.status, (size_t)j * g.nx + i, (size_t)g.nx * (g.ny + 1), 22)] = v;
       v = inlet_value(a.inlet, 0, i, j);
     }
     g.e_star[0][n] = v;
@@ -290,12 +298,14 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       if (s >= 0) {
         const double diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
         v += -1.0 * cx * cpml_correction(a.ex_prof, i, diff,
-                                         history_at(a.h[1], s, k, g.zb_e[1], j));
+                                         history_at(a.h[1], s, k, g.zb_e[1], j, g.status));
       }
     }
     if (i == 0 || i == g.nx) v = 0.0;
     if (k == 0) {
-      if (a.pre_inlet[1]) a.pre_inlet[1][(size_t)j * (g.nx + 1) + i] = v;
+      if (a.pre_inlet[1])
+        a.pre_inlet[1][APRL_BOUNDED(g.status, (size_t)j * (g.nx + 1) + i,
+                                    (size_t)(g.nx + 1) * g.ny, 23)] = v;
       v = inlet_value(a.inlet, 1, i, j);
     }
     g.e_star[1][n] = v;
@@ -314,13 +324,13 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
       if (sx >= 0) {
         const double diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
         v += 1.0 * cx * cpml_correction(a.ex_prof, i, diff,
-                                        history_at(a.h[2], sx, k, g.zb_e[2], j));
+                                        history_at(a.h[2], sx, k, g.zb_e[2], j, g.status));
       }
       const int sy = a.ey_prof.ordinal[j];
       if (sy >= 0) {
         const double diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
         v += -1.0 * cy * cpml_correction(a.ey_prof, j, diff,
-                                         history_at(a.h[3], sy, k, g.zb_e[2], i));
+                                         history_at(a.h[3], sy, k, g.zb_e[2], i, g.status));
       }
     }
     if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
@@ -414,7 +424,7 @@ __global__ void shift_insert_kernel(ShiftArgs<F> a) {
     const CpmlHistory& h = a.h[c - 6];
     // i runs over the row, j over the slots.
     if (i >= h.row || j >= h.slots) return;
-    *history_at(h, j, 0, a.history_base[c - 6], i) = 0.0;
+    *history_at(h, j, 0, a.history_base[c - 6], i, g.status) = 0.0;
   }
 }
 

@@ -195,9 +195,15 @@ __global__ void __launch_bounds__(kLedgerFinishThreads) ledger_finish_kernel(Led
 }
 
 // ---- discrete Gauss law ----------------------------------------------------
-// Node charge density of one particle (verification/transverse_binomial_checks.cpp:12-66):
-// F3 weights in x over nodes i-1..i+2, linear in y over j, j+1, the
-// binomial3 smoothing of the linear z weights over k-1..k+2.
+// Node charge density of one particle: the density whose change the
+// run's current balances.  linear-binomial3 (the F3 density of
+// verification/transverse_binomial_checks.cpp:12-66): F3 weights in x over
+// nodes i-1..i+2, linear in y over j, j+1, the binomial3 smoothing of the
+// linear z weights over k-1..k+2.  quintic-compensated: linear in x and y
+// (nodes i, i+1 and j, j+1) and the quintic node basis in z
+// (longitudinal_shape::nodeWeight, src/longitudinal_shape.h:48-56, nodes
+// floor(z)-5 .. floor(z)+6), the density of quintic_segment's current (x and
+// y edge currents with linear transverse weights, the edge basis along z).
 __global__ void gauss_deposit_kernel(GaussArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.np) return;
@@ -208,23 +214,44 @@ __global__ void gauss_deposit_kernel(GaussArgs a) {
   const double fi = floor(x), fj = floor(y), fk = floor(z);
   const int i = (int)fi, j = (int)fj, k = (int)fk;
   const double fx = x - fi, fy = y - fj, fz = z - fk;
-  const double wx[4] = {0.25 * (1.0 - fx), 0.5 - 0.25 * fx, 0.25 + 0.25 * fx, 0.25 * fx};
-  const double wy[2] = {1.0 - fy, fy};
-  double wz[4] = {0., 0., 0., 0.};
-  const double bw[3] = {0.25, 0.5, 0.25};
-  for (int s = 0; s < 3; ++s) {
-    wz[s] += bw[s] * (1.0 - fz);
-    wz[s + 1] += bw[s] * fz;
+  double wx[4], wz[12];
+  int xfirst, xcount, zfirst, zcount;
+  if (a.shape == 0) {
+    wx[0] = 0.25 * (1.0 - fx);
+    wx[1] = 0.5 - 0.25 * fx;
+    wx[2] = 0.25 + 0.25 * fx;
+    wx[3] = 0.25 * fx;
+    xfirst = i - 1;
+    xcount = 4;
+    for (int t = 0; t < 4; ++t) wz[t] = 0.;
+    const double bw[3] = {0.25, 0.5, 0.25};
+    for (int s = 0; s < 3; ++s) {
+      wz[s] += bw[s] * (1.0 - fz);
+      wz[s + 1] += bw[s] * fz;
+    }
+    zfirst = k - 1;
+    zcount = 4;
+  } else {
+    wx[0] = 1.0 - fx;
+    wx[1] = fx;
+    xfirst = i;
+    xcount = 2;
+    Basis<double> b;
+    quintic_basis<double>(z, false, b);
+    for (int t = 0; t < 12; ++t) wz[t] = b.v[t];
+    zfirst = (int)b.first;
+    zcount = b.count;
   }
+  const double wy[2] = {1.0 - fy, fy};
   const double q = a.q[n] / (g.dx * g.dy * g.dz);
   const int nx = g.nx + 1, ny = g.ny + 1, nz = g.nz + 1;
   unsigned long long missed = 0;
-  for (int t = 0; t < 4; ++t) {
-    const int kk = k - 1 + t;
+  for (int t = 0; t < zcount; ++t) {
+    const int kk = zfirst + t;
     for (int v = 0; v < 2; ++v) {
       const int jj = j + v;
-      for (int u = 0; u < 4; ++u) {
-        const int ii = i - 1 + u;
+      for (int u = 0; u < xcount; ++u) {
+        const int ii = xfirst + u;
         if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) {
           ++missed;
           continue;

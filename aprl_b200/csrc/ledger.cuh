@@ -83,6 +83,7 @@ struct GaussArgs {
   DGrid g;                         // e_old = the committed E
   const double *x, *y, *z, *q;     // particle box positions and charges
   long long np;
+  int shape;                       // 0 linear-binomial3, 1 quintic-compensated
   double* node;                    // (nx+1)(ny+1)(nz+1), [k][j][i]: rho, then G in place
   int i0, i1, j0, j1, k0, k1;      // interior nodes [i0, i1) x [j0, j1) x [k0, k1)
   DD volume;

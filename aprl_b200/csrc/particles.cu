@@ -32,43 +32,6 @@ __device__ __forceinline__ void node_weights(F f, F w[4]) {
   w[3] = F(0.25) * f;
 }
 
-template <class F>
-struct Basis {
-  long long first;
-  int count;
-  F v[12];
-};
-
-// basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54): the
-// cell in binary64, the B-spline and compensation arithmetic in F on the
-// cell-relative offset.
-template <class F>
-__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) {
-  const unsigned degree = edge ? 4 : 5;
-  const double cell = floor(z);
-  const F f = F(z - cell);
-  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
-  for (unsigned j = 1; j <= degree; ++j) {
-    F saved = F(0.);
-    for (unsigned k = 0; k < j; ++k) {
-      const F t = n[k] / F(j);
-      n[k] = saved + (F(k + 1) - f) * t;
-      saved = (f + F(j) - F(k) - F(1)) * t;
-    }
-    n[j] = saved;
-  }
-  const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
-               d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
-  const F c[7] = {F(-d / 64.), F(b / 16. + 3 * d / 32.), F(-a / 4. - b / 4. - 15 * d / 64.),
-                  F(1 + a / 2. + 3 * b / 8. + 5 * d / 16.),
-                  F(-a / 4. - b / 4. - 15 * d / 64.), F(b / 16. + 3 * d / 32.), F(-d / 64.)};
-  r.first = (long long)cell - 5;
-  r.count = degree + 7;
-  for (int q = 0; q < 12; ++q) r.v[q] = F(0.);
-  for (unsigned j = 0; j <= degree; ++j)
-    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
-}
-
 // binomialXZSegment (src/longitudinal_shape.h:61-94).
 template <class G, class V>
 __device__ __forceinline__ void binomial_xz_segment(const GridT<G>& g, const double s[3],
@@ -392,7 +355,7 @@ struct ElectricVisitor {
 
   // One accumulation .5*w*(E_new + E^n) at the ring offset n of a node.
   __device__ __forceinline__ W term(int d, size_t n, size_t, W w) const {
-    return W(.5) * w * s.p[d][n];
+    return W(.5) * w * s.p[d][APRL_BOUNDED(g->status, n, e_count(*g, d), 24 + d)];
   }
 
   // binomialXZSegment specialised for the gather.  When the whole 4x2x4
@@ -521,10 +484,11 @@ __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const Pt
         const size_t plane = (size_t)ring((int)cell[2] - 1 + k, g.zb_b[a], (int)nzc) * nyc;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const W* row = base + (plane + cell[1] + j) * nxc + (cell[0] - 1);
+          const size_t row = (plane + cell[1] + j) * nxc + (cell[0] - 1);
           W r = W(0.);
 #pragma unroll
-          for (int i = 0; i < 4; ++i) r += wx[i] * row[i];
+          for (int i = 0; i < 4; ++i)
+            r += wx[i] * base[APRL_BOUNDED(g.status, row + i, b_count(g, a), 27 + a)];
           v += wz[k] * wy[j] * r;
         }
       }
@@ -1253,7 +1217,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
         e[d] = action ? selected.position[d] : pos[d];
       }
     }
-    if constexpr (S == 0 && kDeferChords<Q>) {
+    if constexpr (S == 0) {
       // The main chord of a linear-binomial3 particle is validated here and
       // deposited by chord_deposit_kernel, whose converged warps merge the
       // stencils of particles in the same cell before the reductions.
@@ -1315,7 +1279,7 @@ __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a) {
   }
   a.abs_grid_work[n] = abs_work;
   a.action[n] = action;
-  if constexpr (S == 0 && kDeferChords<Q>) a.dep_mode[n] = deferred ? 1 : 0;
+  if constexpr (S == 0) a.dep_mode[n] = deferred ? 1 : 0;
   a.born_keep[n] = born_kept ? 1 : 0;
   if (born_kept) {
     a.born.px[n] = born.pos[0]; a.born.py[n] = born.pos[1]; a.born.pz[n] = born.pos[2];
@@ -1405,6 +1369,40 @@ __device__ __forceinline__ double run_sum(double v, int lane, int head, unsigned
   return v;
 }
 
+// The 4x2x4 node block of component `ax` around a piece in cell (i, j, k):
+// nodes (i-1+x, j+b, k-1+c), with in-range masks per x, b and c.
+struct ChordBlock {
+  long long base, row, plane;
+  unsigned xok, yok, zok;
+  __device__ __forceinline__ bool in(int c, int b) const {
+    return ((zok >> c) & 1u) && ((yok >> b) & 1u);
+  }
+  __device__ __forceinline__ size_t at(int c, int b, int x) const {
+    return (size_t)(base + c * plane + b * row + x);
+  }
+};
+
+// `levels`: z levels k-1 .. k-2+levels.
+__device__ __forceinline__ ChordBlock chord_block(const DGrid& g, int ax, long long i,
+                                                  long long j, long long k, int levels) {
+  const long long nxc = e_nx(g, ax), nyc = e_ny(g, ax), nzc = e_nz(g, ax);
+  ChordBlock s;
+  s.row = nxc;
+  s.plane = nxc * nyc;
+  s.base = ((k - 1) * nyc + j) * nxc + (i - 1);
+  s.xok = s.yok = s.zok = 0u;
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+    if (i - 1 + x >= 0 && i - 1 + x < nxc) s.xok |= 1u << x;
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+    if (j + b >= 0 && j + b < nyc) s.yok |= 1u << b;
+#pragma unroll
+  for (int c = 0; c < 5; ++c)
+    if (c < levels && k - 1 + c >= 0 && k - 1 + c < nzc) s.zok |= 1u << c;
+  return s;
+}
+
 template <bool Q>
 __device__ __forceinline__ void chord_add(const DGrid& g, int a, size_t at, double v,
                                           unsigned& err) {
@@ -1415,8 +1413,60 @@ __device__ __forceinline__ void chord_add(const DGrid& g, int a, size_t at, doub
   }
 }
 
+// One cut piece's cell and binomialXZSegment factors.
+struct PieceGeometry {
+  long long i, j, k;
+  double wx[4], wz[4], wy[2];
+  double width, xy, xz, yz;
+};
+
+__device__ __forceinline__ void piece_geometry(const DGrid& g, const CutWalker& w, double first,
+                                               double last, PieceGeometry& p) {
+  p.width = last - first;
+  const double mid = (first + last) * 0.5;
+  const double px = w.x[0] + mid * w.v[0], py = w.x[1] + mid * w.v[1], pz = w.x[2] + mid * w.v[2];
+  p.i = (long long)floor(px);
+  p.j = (long long)floor(py);
+  p.k = (long long)floor(pz);
+  if (p.i == (long long)g.nx) --p.i;
+  if (p.j == (long long)g.ny) --p.j;
+  node_weights(px - p.i, p.wx);
+  node_weights(pz - p.k, p.wz);
+  p.wy[0] = 1. - (py - p.j);
+  p.wy[1] = py - p.j;
+  const double curvature = p.width * p.width / 12.;
+  p.xy = curvature * w.v[0] * w.v[1];
+  p.xz = curvature * w.v[0] * w.v[2];
+  p.yz = curvature * w.v[1] * w.v[2];
+}
+
+__device__ __forceinline__ unsigned long long piece_key(long long i, long long j, long long k,
+                                                        unsigned long long kind) {
+  return (kind << 63) | ((unsigned long long)(k + 2) << 42) |
+         ((unsigned long long)(j + 2) << 21) | (unsigned long long)(i + 2);
+}
+
+// Runs of neighbouring lanes holding the same key: this lane's run head,
+// whether it is the run's last lane, and the longest run of the warp.
+struct Runs {
+  int head;
+  bool last;
+  unsigned span;
+};
+
+__device__ __forceinline__ Runs lane_runs(unsigned long long key, int lane) {
+  const unsigned long long previous = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = lane == 0 || previous != key;
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
+  Runs r;
+  r.head = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+  r.last = lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u;
+  r.span = __reduce_max_sync(0xffffffffu, (unsigned)(lane - r.head + 1));
+  return r;
+}
+
 template <bool Q>
-__global__ void __launch_bounds__(128) chord_deposit_kernel(ChordArgs a) {
+__global__ void APRL_CHORD_BOUNDS chord_deposit_kernel(ChordArgs a) {
   if (trial_skipped(a.g)) return;
   const DGrid& g = a.g;
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1443,85 +1493,204 @@ __global__ void __launch_bounds__(128) chord_deposit_kernel(ChordArgs a) {
   const double edge[3] = {0.25, 0.5, 0.25};
   const double slope[4] = {-0.25, -0.25, 0.25, 0.25};
   const double sy[2] = {-1., 1.};
-  const unsigned at_or_below = 0xffffffffu >> (31 - lane);
+  // ---- chords of exactly two pieces in z-neighbouring cells of one (i, j)
+  // column (a chord crossing one z plane: nearly every chord of a beam that
+  // moves about a cell per step along z).  Their stencils overlap, so the two
+  // pieces are added per node of the union before the reductions: 82 nodes
+  // instead of 2 x 64.
+  double f0 = 0., l0 = 0., f1 = 0., l1 = 0.;
+  bool pair = false;
+  if (alive) {
+    const bool two = w.advance(f0, l0) && w.advance(f1, l1);
+    double fx, lx;
+    if (two && !w.advance(fx, lx)) {
+      PieceGeometry p0, p1;
+      piece_geometry(g, w, f0, l0, p0);
+      piece_geometry(g, w, f1, l1, p1);
+      pair = p0.i == p1.i && p0.j == p1.j && (p1.k - p0.k == 1 || p0.k - p1.k == 1);
+      if (pair && p1.k < p0.k) {  // lower piece first
+        double t = f0; f0 = f1; f1 = t;
+        t = l0; l0 = l1; l1 = t;
+      }
+    }
+    if (!pair) {  // the general walk below starts over
+      double b[3], e[3];
+      for (int d = 0; d < 3; ++d) {
+        b[d] = a.b[d][n];
+        e[d] = a.e[d][n];
+      }
+      const double h[3] = {g.dx, g.dy, g.dz};
+      w.init(b, e, g.origin, h);
+    }
+  }
+  if (__any_sync(0xffffffffu, pair)) {
+    PieceGeometry lo, up;
+    unsigned long long key = ~0ull - (unsigned long long)lane;
+    if (pair) {
+      piece_geometry(g, w, f0, l0, lo);
+      piece_geometry(g, w, f1, l1, up);
+      key = piece_key(lo.i, lo.j, lo.k, 1);
+    } else {
+      lo = PieceGeometry{};
+      up = PieceGeometry{};
+    }
+    const Runs runs = lane_runs(key, lane);
+    const bool adds = pair && runs.last;
+    const long long i = lo.i, j = lo.j, k = lo.k;
+    // Node blocks of the union: z levels k-1 .. k+3 (Jx, Jy) and k-1 .. k+2 (Jz).
+    const ChordBlock bx = chord_block(g, 0, i, j, k, 5), by = chord_block(g, 1, i, j, k, 5),
+                     bz = chord_block(g, 2, i, j, k, 4);
+    if (pair) {
+      if (scale[0] != 0. && (bx.xok & 7u) && (bx.yok & 3u) != 3u) err = kErrSupportY;
+      if (scale[1] != 0. && (by.xok & 15u) && !(by.yok & 1u)) err = kErrSupportY;
+      if (scale[2] != 0. && (bz.xok & 15u) && (bz.yok & 3u) != 3u) err = kErrSupportY;
+    }
+    // Jx: level zz takes the lower piece's c = zz and the upper's c = zz - 1.
+#pragma unroll
+    for (int zz = 0; zz < 5; ++zz) {
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        double v = 0.;
+        if (zz < 4) v += lo.width * (lo.wy[b] * lo.wz[zz] + lo.yz * sy[b] * slope[zz]);
+        if (zz >= 1)
+          v += up.width * (up.wy[b] * up.wz[zz - 1] + up.yz * sy[b] * slope[zz - 1]);
+        const double total = run_sum(scale[0] * v, lane, runs.head, runs.span);
+        if (adds && total != 0. && bx.in(zz, b))
+#pragma unroll
+          for (int x = 0; x < 3; ++x)
+            if ((bx.xok >> x) & 1u) chord_add<Q>(g, 0, bx.at(zz, b, x), total * edge[x], err);
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        double v = 0.;
+        if (zz < 4) v += lo.width * (lo.wx[x] * lo.wz[zz] + lo.xz * slope[x] * slope[zz]);
+        if (zz >= 1)
+          v += up.width * (up.wx[x] * up.wz[zz - 1] + up.xz * slope[x] * slope[zz - 1]);
+        const double total = run_sum(scale[1] * v, lane, runs.head, runs.span);
+        if (adds && total != 0. && by.in(zz, 0) && ((by.xok >> x) & 1u))
+          chord_add<Q>(g, 1, by.at(zz, 0, x), total, err);
+      }
+    }
+    // Jz: each piece's weight is smoothed over three z nodes (its k-1, k,
+    // k+1), so the lower piece covers levels 0..2 and the upper 1..3.
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const double vl = lo.width * (lo.wx[x] * lo.wy[b] + lo.xy * slope[x] * sy[b]);
+        const double vu = up.width * (up.wx[x] * up.wy[b] + up.xy * slope[x] * sy[b]);
+        const double tl = run_sum(scale[2] * vl, lane, runs.head, runs.span);
+        const double tu = run_sum(scale[2] * vu, lane, runs.head, runs.span);
+        if (adds && ((bz.xok >> x) & 1u) && ((bz.yok >> b) & 1u)) {
+          const double level[4] = {tl * edge[0], tl * edge[1] + tu * edge[0],
+                                   tl * edge[2] + tu * edge[1], tu * edge[2]};
+#pragma unroll
+          for (int zz = 0; zz < 4; ++zz)
+            if (((bz.zok >> zz) & 1u) && level[zz] != 0.)
+              chord_add<Q>(g, 2, bz.at(zz, b, x), level[zz], err);
+        }
+      }
+  }
+  if (pair) alive = false;
+  // ---- every other chord, one piece per lane per round
   while (__any_sync(0xffffffffu, alive)) {
     double first = 0., last = 0.;
     const bool have = alive && w.advance(first, last);
     if (!have) alive = false;
-    // The piece's cell and factors, as binomialXZSegment forms them.  A lane
-    // without a piece takes a key no other lane has and adds nothing.
-    long long i = 0, j = 0, k = 0;
-    double wx[4] = {0., 0., 0., 0.}, wz[4] = {0., 0., 0., 0.}, wy[2] = {0., 0.};
-    double width = 0., xy = 0., xz = 0., yz = 0.;
+    // A lane without a piece takes a key no other lane has and adds nothing.
+    PieceGeometry p;
     unsigned long long key = ~0ull - (unsigned long long)lane;
     if (have) {
-      width = last - first;
-      const double mid = (first + last) * 0.5;
-      const double px = w.x[0] + mid * w.v[0], py = w.x[1] + mid * w.v[1],
-                   pz = w.x[2] + mid * w.v[2];
-      i = (long long)floor(px);
-      j = (long long)floor(py);
-      k = (long long)floor(pz);
-      if (i == (long long)g.nx) --i;
-      if (j == (long long)g.ny) --j;
-      node_weights(px - i, wx);
-      node_weights(pz - k, wz);
-      wy[0] = 1. - (py - j);
-      wy[1] = py - j;
-      const double curvature = width * width / 12.;
-      xy = curvature * w.v[0] * w.v[1];
-      xz = curvature * w.v[0] * w.v[2];
-      yz = curvature * w.v[1] * w.v[2];
-      key = ((unsigned long long)(k + 2) << 42) | ((unsigned long long)(j + 2) << 21) |
-            (unsigned long long)(i + 2);
+      piece_geometry(g, w, first, last, p);
+      key = piece_key(p.i, p.j, p.k, 0);
+    } else {
+      p = PieceGeometry{};
     }
-    // Runs of neighbouring lanes on the same cell.
-    const unsigned long long previous = __shfl_up_sync(0xffffffffu, key, 1);
-    const bool head = lane == 0 || previous != key;
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const int run_head = 31 - __clz(heads & at_or_below);
-    const bool adds = have && (lane == 31 || ((heads >> (lane + 1)) & 1u) != 0u);
-    const unsigned span = __reduce_max_sync(0xffffffffu, (unsigned)(lane - run_head + 1));
-    // One node of the piece: the visitor's support rules for this lane
-    // (x outside: skipped, the F3 x-support may leave the grid; y outside:
-    // an error when this lane carries current on the axis; z outside:
-    // skipped), and the run's sum added by its last lane.
-    auto node = [&](int ax, long long ii, long long jj, long long kk, double total) {
-      if (ii < 0 || ii >= e_nx(g, ax)) return;
-      if (jj < 0 || jj >= e_ny(g, ax)) {
-        if (have && scale[ax] != 0.) err = kErrSupportY;
-        return;
-      }
-      if (kk < 0 || kk >= e_nz(g, ax)) return;
-      if (adds && total != 0.) chord_add<Q>(g, ax, j_index(g, ax, (int)ii, (int)jj, (int)kk),
-                                            total, err);
-    };
+    const Runs runs = lane_runs(key, lane);
+    const bool adds = have && runs.last;
+    const long long i = p.i, j = p.j, k = p.k;
+    // The three node blocks of the piece, with the visitor's support rules
+    // for this lane: x outside is skipped (the F3 x-support may leave the
+    // grid), y outside is an error when the lane carries current on that
+    // axis, z outside is skipped.  The run's sums are added by its last lane.
+    const ChordBlock bx = chord_block(g, 0, i, j, k, 4), by = chord_block(g, 1, i, j, k, 4),
+                     bz = chord_block(g, 2, i, j, k, 4);
+    if (have) {
+      if (scale[0] != 0. && (bx.xok & 7u) && (bx.yok & 3u) != 3u) err = kErrSupportY;
+      if (scale[1] != 0. && (by.xok & 15u) && !(by.yok & 1u)) err = kErrSupportY;
+      if (scale[2] != 0. && (bz.xok & 15u) && (bz.yok & 3u) != 3u) err = kErrSupportY;
+    }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const double weight = width * (wy[b] * wz[c] + yz * sy[b] * slope[c]);
-        const double total = run_sum(scale[0] * weight, lane, run_head, span);
+        const double weight = p.width * (p.wy[b] * p.wz[c] + p.yz * sy[b] * slope[c]);
+        const double total = run_sum(scale[0] * weight, lane, runs.head, runs.span);
+        if (adds && total != 0. && bx.in(c, b))
 #pragma unroll
-        for (int x = 0; x < 3; ++x) node(0, i - 1 + x, j + b, k - 1 + c, total * edge[x]);
+          for (int x = 0; x < 3; ++x)
+            if ((bx.xok >> x) & 1u) chord_add<Q>(g, 0, bx.at(c, b, x), total * edge[x], err);
       }
 #pragma unroll
       for (int x = 0; x < 4; ++x) {
-        const double weight = width * (wx[x] * wz[c] + xz * slope[x] * slope[c]);
-        node(1, i - 1 + x, j, k - 1 + c, run_sum(scale[1] * weight, lane, run_head, span));
+        const double weight = p.width * (p.wx[x] * p.wz[c] + p.xz * slope[x] * slope[c]);
+        const double total = run_sum(scale[1] * weight, lane, runs.head, runs.span);
+        if (adds && total != 0. && by.in(c, 0) && ((by.xok >> x) & 1u))
+          chord_add<Q>(g, 1, by.at(c, 0, x), total, err);
       }
     }
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
       for (int x = 0; x < 4; ++x) {
-        const double weight = width * (wx[x] * wy[b] + xy * slope[x] * sy[b]);
-        const double total = run_sum(scale[2] * weight, lane, run_head, span);
+        const double weight = p.width * (p.wx[x] * p.wy[b] + p.xy * slope[x] * sy[b]);
+        const double total = run_sum(scale[2] * weight, lane, runs.head, runs.span);
+        if (adds && total != 0. && ((bz.xok >> x) & 1u) && ((bz.yok >> b) & 1u))
 #pragma unroll
-        for (int c = 0; c < 3; ++c) node(2, i - 1 + x, j + b, k - 1 + c, total * edge[c]);
+          for (int c = 0; c < 3; ++c)
+            if ((bz.zok >> c) & 1u) chord_add<Q>(g, 2, bz.at(c, b, x), total * edge[c], err);
       }
   }
   if (err) raise_error(a.status, err, (unsigned long long)n);
+}
+
+// ---------------------------------------------------------------------------
+// RelativisticBorisPusher::push (src/eb_particles.cpp:207-216): the Boris
+// momentum update with the half electric kicks and the magnetic rotation
+// (pushMomentum, :99-127), then the drift at the new proper velocity
+// (pushPosition, :129-136), in the reference's operation order.
+__device__ __forceinline__ void boris_push(double x[3], double u[3], const double e[3],
+                                           const double b[3], double q, double m, double dt) {
+  const double kick = q * dt / (2.0 * m * kC);
+  double minus[3];
+  for (int d = 0; d < 3; ++d) minus[d] = u[d] + kick * e[d];
+  const double gamma_minus = gamma_u(minus[0], minus[1], minus[2]);
+  const double rs = q * dt / (2.0 * m * gamma_minus);
+  const double t[3] = {rs * b[0], rs * b[1], rs * b[2]};
+  double prime[3] = {minus[1] * t[2] - minus[2] * t[1], minus[2] * t[0] - minus[0] * t[2],
+                     minus[0] * t[1] - minus[1] * t[0]};
+  for (int d = 0; d < 3; ++d) prime[d] += minus[d];
+  const double norm2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+  const double f = 2.0 / (1.0 + norm2);
+  const double sv[3] = {t[0] * f, t[1] * f, t[2] * f};
+  double plus[3] = {prime[1] * sv[2] - prime[2] * sv[1], prime[2] * sv[0] - prime[0] * sv[2],
+                    prime[0] * sv[1] - prime[1] * sv[0]};
+  for (int d = 0; d < 3; ++d) plus[d] += minus[d];
+  for (int d = 0; d < 3; ++d) u[d] = plus[d] + kick * e[d];
+  const double gamma = gamma_u(u[0], u[1], u[2]);
+  const double drift = kC * dt / gamma;
+  for (int d = 0; d < 3; ++d) x[d] += drift * u[d];
+}
+
+__global__ void boris_push_kernel(BorisArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.count) return;
+  double x[3] = {a.x[n], a.y[n], a.z[n]}, u[3] = {a.ux[n], a.uy[n], a.uz[n]};
+  const double e[3] = {a.e[3 * n], a.e[3 * n + 1], a.e[3 * n + 2]};
+  const double b[3] = {a.b[3 * n], a.b[3 * n + 1], a.b[3 * n + 2]};
+  boris_push(x, u, e, b, a.q[n], a.m[n], a.dt);
+  a.x[n] = x[0]; a.y[n] = x[1]; a.z[n] = x[2];
+  a.ux[n] = u[0]; a.uy[n] = u[1]; a.uz[n] = u[2];
 }
 
 // ---------------------------------------------------------------------------

@@ -158,12 +158,12 @@ struct ResidualArgs {
   DeviceStatus* status;
 };
 
-// Whether push_deposit_kernel leaves the main chords of linear-binomial3
-// particles to chord_deposit_kernel (per current-summation mode Q): the
-// merged deposit halves the fixed-point mode's reductions, which bound it;
-// with binary64 atomics the fused deposit measured faster (0.50 ms per
-// dipole-workload trial against 0.13 + 0.47 ms).
-template <bool Q> constexpr bool kDeferChords = Q;
+// push_deposit_kernel leaves the main chords of linear-binomial3 particles
+// to chord_deposit_kernel, in both current-summation modes.  On the dipole
+// workload (1M particles, 128x128x512 cells) per trial: fused push and
+// deposit 0.49 ms; push 0.13 ms + merged deposit 0.30 ms with binary64
+// atomics; with the fixed-point sum, whose two integer reductions per
+// contribution bound it, 1.13 ms fused against 0.14 + 0.65 ms.
 
 // The deferred main chords of a linear-binomial3 trial.
 struct ChordArgs {
@@ -194,6 +194,14 @@ struct ChordArgs {
 #ifndef APRL_GATHER_MIN_BLOCKS
 #define APRL_GATHER_MIN_BLOCKS 6
 #endif
+#ifndef APRL_CHORD_MIN_BLOCKS
+#define APRL_CHORD_MIN_BLOCKS 0
+#endif
+#if APRL_CHORD_MIN_BLOCKS > 0
+#define APRL_CHORD_BOUNDS __launch_bounds__(128, APRL_CHORD_MIN_BLOCKS)
+#else
+#define APRL_CHORD_BOUNDS __launch_bounds__(128)
+#endif
 #if APRL_GATHER_MIN_BLOCKS > 0
 #define APRL_GATHER_BOUNDS __launch_bounds__(128, APRL_GATHER_MIN_BLOCKS)
 #else
@@ -217,9 +225,19 @@ template <class W, class F, int S> __global__ void guess_gather_kernel(PushArgs<
 template <class F, int S, bool Q>
 __global__ void APRL_PUSH_BOUNDS push_deposit_kernel(PushArgs<F> a);
 template <class F, int S, bool Q> __global__ void carrier_kernel(CarrierArgs<F> a);
-template <bool Q> __global__ void chord_deposit_kernel(ChordArgs a);
+template <bool Q> __global__ void APRL_CHORD_BOUNDS chord_deposit_kernel(ChordArgs a);
 template <class W, class F, int S>
 __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a);
+
+// RelativisticBorisPusher::push of `count` particles (SoA, in place) with
+// per-particle E and B (3 values each).
+struct BorisArgs {
+  long long count;
+  double *x, *y, *z, *ux, *uy, *uz;
+  const double *q, *m, *e, *b;
+  double dt;
+};
+__global__ void boris_push_kernel(BorisArgs a);
 
 // Stable compaction helpers (warp ballot + block scan + block-offset scan).
 constexpr int kScanBlock = 256;

@@ -106,6 +106,8 @@ const char* device_error_text(unsigned code) {
     case kErrInletField: return "Nonfinite charge-matched inlet field";
     case kErrFixedRange:
       return "Deposit contribution beyond the deterministic fixed-point range";
+    case kErrBounds:
+      return "Array index outside its array (bounds-checked build)";
   }
   return "unknown device error";
 }
@@ -231,6 +233,7 @@ constexpr uint64_t kSortInterval = 4;
 
 struct aprl_run {
   aprl_run_config cfg{};
+  std::string error;  // the message of this run's failure in aprl_runs_step
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;   // device memory (device_pool of the run's device)
   void* pinned = nullptr;         // the page-locked block the h_* read-backs live in
@@ -608,6 +611,7 @@ GridT<F> make_grid(const aprl_run* r) {
     g.zb_b[a] = r->zb_b[a];
   }
   g.jcoef = F(-1. * r->cfg.dt / kEpsilon0);
+  g.status = r->d_status;
   if (r->deterministic) {
     for (int a = 0; a < 3; ++a) g.jq[a] = r->jq[a];
     g.jq_scale = r->jq_scale;
@@ -1490,7 +1494,7 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
                    : (binomial ? push_deposit_kernel<F, 0, false> : push_deposit_kernel<F, 1, false>),
                dim3(blocks_for(r->np, 128)), dim3(128),
                pa));
-    if (binomial && (r->deterministic ? kDeferChords<true> : kDeferChords<false>)) {
+    if (binomial) {
       ChordArgs da{};
       da.g = g;
       da.count = (long long)r->np;
@@ -1778,6 +1782,9 @@ HistoryBuffer* find_history(aprl_run* r, unsigned index) {
 // The calling thread's error message, for the other host files of the
 // library (the scan server).
 namespace aprl_gpu {
+// The message of a run's failure in aprl_runs_step (the scan server).
+const char* run_error(const aprl_run* r) { return r->error.c_str(); }
+
 aprl_status report_error(aprl_status status, const char* message) {
   g_error = message;
   return status;
@@ -1819,6 +1826,54 @@ aprl_status aprl_magnet_prepare(aprl_magnet* m) {
                          : 0.0;
   m->cos_angle = std::cos(m->polarization_angle);
   m->sin_angle = std::sin(m->polarization_angle);
+  return APRL_OK;
+}
+
+aprl_status aprl_boris_push(size_t count, double* x, double* y, double* z, double* ux, double* uy,
+                            double* uz, const double* charge, const double* mass,
+                            const double* electric, const double* magnetic, double dt) {
+  if (count && (!x || !y || !z || !ux || !uy || !uz || !charge || !mass || !electric || !magnetic))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  // pushMomentum's parameter check (src/eb_particles.cpp:104-107).
+  if (!(dt > 0.0) || !std::isfinite(dt))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI particle pusher parameters");
+  for (size_t i = 0; i < count; ++i)
+    if (!(mass[i] > 0.0) || !std::isfinite(mass[i]) || !std::isfinite(charge[i]))
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI particle pusher parameters");
+  if (!count) return APRL_OK;
+  cudaStream_t stream = nullptr;
+  CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  double* d = nullptr;
+  const size_t words = 14 * count;  // x y z ux uy uz q m, E and B (3 each)
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&d), words * sizeof(double), stream);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(stream);
+    return fail(APRL_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e));
+  }
+  double* in[8] = {x, y, z, ux, uy, uz, const_cast<double*>(charge), const_cast<double*>(mass)};
+  for (int k = 0; k < 8 && e == cudaSuccess; ++k)
+    e = cudaMemcpyAsync(d + k * count, in[k], count * 8, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d + 8 * count, electric, 3 * count * 8, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d + 11 * count, magnetic, 3 * count * 8, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) {
+    BorisArgs a{};
+    a.count = (long long)count;
+    a.x = d; a.y = d + count; a.z = d + 2 * count;
+    a.ux = d + 3 * count; a.uy = d + 4 * count; a.uz = d + 5 * count;
+    a.q = d + 6 * count; a.m = d + 7 * count; a.e = d + 8 * count; a.b = d + 11 * count;
+    a.dt = dt;
+    boris_push_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(a);
+    e = cudaGetLastError();
+  }
+  for (int k = 0; k < 6 && e == cudaSuccess; ++k)
+    e = cudaMemcpyAsync(in[k], d + k * count, count * 8, cudaMemcpyDeviceToHost, stream);
+  cudaFreeAsync(d, stream);
+  const cudaError_t s2 = cudaStreamSynchronize(stream);
+  cudaStreamDestroy(stream);
+  if (e == cudaSuccess) e = s2;
+  if (e != cudaSuccess) return fail(APRL_ERR_CUDA, "Boris push: %s", cudaGetErrorString(e));
   return APRL_OK;
 }
 
@@ -2431,73 +2486,136 @@ aprl_status aprl_run_shift(aprl_run* r) {
   return do_shift(r);
 }
 
+}  // extern "C"
+
+namespace {
+
+// A coupled step in two halves, so that several runs can be stepped in lock
+// step with one host wait per run and step: step_enqueue queues the begin,
+// the magnetic update, the preview and the fixed-point trials issued ahead
+// (each followed by a device verdict) and the read-back of their residuals,
+// and returns without waiting; step_finish waits for that read-back, applies
+// the stopping rule (running further trials one at a time if none of those
+// converged), then queues the commit and the shift.
+unsigned trials_ahead(const aprl_run* r) {
+  // three at FP64, where steps take three; two in the FP32-mixed mode,
+  // whose looser tolerances stop at the minimum two
+  return std::min<unsigned>(r->fp32 ? 2u : kTrialSlots, r->cfg.max_trials);
+}
+
+aprl_status step_enqueue(aprl_run* r) {
+  TRY(do_advance_magnetic(r));
+  TRY(do_preview_electric(r));
+  // The first trials are issued without waiting: after each one a device
+  // verdict applies the stopping rule, and the kernels of the trials after
+  // a converged one return at once.  One round trip then reads them all.
+  const unsigned ahead = trials_ahead(r);
+  CUDA_TRY(cudaMemsetAsync(r->d_stop, 0, sizeof(int), r->stream));
+  for (unsigned t = 0; t < ahead; ++t) TRY(enqueue_trial(r, (int)t, true));
+  CUDA_TRY(cudaMemcpyAsync(r->h_stop, r->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
+                           r->stream));
+  return APRL_OK;
+}
+
+aprl_status step_finish(aprl_run* r) {
+  bool converged = false;
+  unsigned iterations = 0;
+  double force = 0.0, work = 0.0;
+  const unsigned ahead = trials_ahead(r);
+  TRY(check_device(r));
+  unsigned t = 0;
+  // forceHistory / workHistory of the reference's failure message.
+  std::vector<double> history;
+  while (!converged && t < ahead) {
+    double res[4];
+    trial_read(r, (int)t, res);
+    iterations = ++t;
+    converged = trial_converged(r->cfg, iterations, res, force, work);
+    history.push_back(force);
+    history.push_back(work);
+  }
+  if ((converged ? (int)iterations : 0) != *r->h_stop)
+    return fail(APRL_ERR_RUNTIME, "Device and host verdicts on the coupling trials differ");
+  for (; !converged && t < r->cfg.max_trials; ++t) {
+    double res[4];
+    TRY(do_trial(r, res));
+    iterations = t + 1;
+    converged = trial_converged(r->cfg, iterations, res, force, work);
+    history.push_back(force);
+    history.push_back(work);
+  }
+  if (!converged) {
+    // The reference's message (src/simulation_source_coupling.cpp:54):
+    // the last residual, the trial count and every trial's force/work.
+    std::string text;
+    char item[64];
+    std::snprintf(item, sizeof item, "%g", force);
+    text = "Conservative source coupling failed at step " + std::to_string(r->step + 1) +
+           ": force=" + item;
+    std::snprintf(item, sizeof item, "%g", work);
+    text += std::string(" work=") + item + " iterations=" + std::to_string(iterations) +
+            " history(force/work)=";
+    for (size_t h = 0; h + 1 < history.size(); h += 2) {
+      std::snprintf(item, sizeof item, " %g/%g", history[h], history[h + 1]);
+      text += item;
+    }
+    g_error = text;
+    return APRL_ERR_NOT_CONVERGED;
+  }
+  r->last_iterations = iterations;
+  r->max_iterations = std::max(r->max_iterations, iterations);
+  r->total_iterations += iterations;
+  r->last_force = force;
+  r->last_work = work;
+  TRY(do_commit(r));
+  return do_shift(r, true);
+}
+
+}  // namespace
+
+extern "C" {
+
 aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
   for (uint32_t n = 0; n < steps; ++n) {
-    TRY(do_advance_magnetic(r));
-    TRY(do_preview_electric(r));
-    bool converged = false;
-    unsigned iterations = 0;
-    double force = 0.0, work = 0.0;
-    // The first trials are issued without waiting: after each one a device
-    // verdict applies the stopping rule, and the kernels of the trials after
-    // a converged one return at once.  One round trip then reads them all.
-    // (three at FP64, where steps take three; two in the FP32-mixed mode,
-    // whose looser tolerances stop at the minimum two)
-    const unsigned ahead = std::min<unsigned>(r->fp32 ? 2u : kTrialSlots, r->cfg.max_trials);
-    CUDA_TRY(cudaMemsetAsync(r->d_stop, 0, sizeof(int), r->stream));
-    for (unsigned t = 0; t < ahead; ++t) TRY(enqueue_trial(r, (int)t, true));
-    CUDA_TRY(cudaMemcpyAsync(r->h_stop, r->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
-                             r->stream));
-    TRY(check_device(r));
-    unsigned t = 0;
-    // forceHistory / workHistory of the reference's failure message.
-    std::vector<double> history;
-    while (!converged && t < ahead) {
-      double res[4];
-      trial_read(r, (int)t, res);
-      iterations = ++t;
-      converged = trial_converged(r->cfg, iterations, res, force, work);
-      history.push_back(force);
-      history.push_back(work);
-    }
-    if ((converged ? (int)iterations : 0) != *r->h_stop)
-      return fail(APRL_ERR_RUNTIME, "Device and host verdicts on the coupling trials differ");
-    for (; !converged && t < r->cfg.max_trials; ++t) {
-      double res[4];
-      TRY(do_trial(r, res));
-      iterations = t + 1;
-      converged = trial_converged(r->cfg, iterations, res, force, work);
-      history.push_back(force);
-      history.push_back(work);
-    }
-    if (!converged) {
-      // The reference's message (src/simulation_source_coupling.cpp:54):
-      // the last residual, the trial count and every trial's force/work.
-      std::string text;
-      char item[64];
-      std::snprintf(item, sizeof item, "%g", force);
-      text = "Conservative source coupling failed at step " + std::to_string(r->step + 1) +
-             ": force=" + item;
-      std::snprintf(item, sizeof item, "%g", work);
-      text += std::string(" work=") + item + " iterations=" + std::to_string(iterations) +
-              " history(force/work)=";
-      for (size_t h = 0; h + 1 < history.size(); h += 2) {
-        std::snprintf(item, sizeof item, " %g/%g", history[h], history[h + 1]);
-        text += item;
-      }
-      g_error = text;
-      return APRL_ERR_NOT_CONVERGED;
-    }
-    r->last_iterations = iterations;
-    r->max_iterations = std::max(r->max_iterations, iterations);
-    r->total_iterations += iterations;
-    r->last_force = force;
-    r->last_work = work;
-    TRY(do_commit(r));
-    TRY(do_shift(r, true));
+    TRY(step_enqueue(r));
+    TRY(step_finish(r));
   }
   return check_device(r);
+}
+
+aprl_status aprl_runs_step(aprl_run* const* runs, size_t count, uint32_t steps,
+                           aprl_status* statuses) {
+  if (count && !runs) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  for (size_t i = 0; i < count; ++i)
+    if (!runs[i]) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  std::vector<aprl_status> status(count, APRL_OK);
+  std::string first_error;
+  auto note = [&](size_t i, aprl_status st) {
+    if (st != APRL_OK && status[i] == APRL_OK) {
+      status[i] = st;
+      runs[i]->error = g_error;
+      if (first_error.empty()) first_error = g_error;
+    }
+  };
+  for (uint32_t n = 0; n < steps; ++n) {
+    // Every run's step is queued before the first wait, so the GPU works
+    // through the runs' kernels (on their own streams) while the host waits
+    // for the first read-back.
+    for (size_t i = 0; i < count; ++i)
+      if (status[i] == APRL_OK) note(i, step_enqueue(runs[i]));
+    for (size_t i = 0; i < count; ++i)
+      if (status[i] == APRL_OK) note(i, step_finish(runs[i]));
+  }
+  for (size_t i = 0; i < count; ++i)
+    if (status[i] == APRL_OK) note(i, check_device(runs[i]));
+  aprl_status worst = APRL_OK;
+  for (size_t i = 0; i < count; ++i) {
+    if (statuses) statuses[i] = status[i];
+    if (worst == APRL_OK) worst = status[i];
+  }
+  if (worst != APRL_OK) g_error = first_error;
+  return worst;
 }
 
 aprl_status aprl_run_get_stats(const aprl_run* r, aprl_step_stats* st) {
@@ -2658,8 +2776,6 @@ aprl_status aprl_run_gauss_law(aprl_run* r, aprl_gauss_law* out, double* residua
   if (r->stage != 0 && r->stage != 4)
     return fail(APRL_ERR_RUNTIME, "Gauss-law reduction inside a step");
   const aprl_run_config& c = r->cfg;
-  if (c.shape != APRL_SHAPE_LINEAR_BINOMIAL3)
-    return fail(APRL_ERR_UNSUPPORTED, "The node charge density is built for linear-binomial3");
   const size_t nodes = (size_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   if (residual && count != nodes)
     return fail(APRL_ERR_INVALID_ARGUMENT, "Gauss-law residual size mismatch");
@@ -2678,6 +2794,7 @@ aprl_status aprl_run_gauss_law(aprl_run* r, aprl_gauss_law* out, double* residua
   a.q = r->p.q;
   a.np = (long long)r->np;
   a.node = r->gauss_node;
+  a.shape = c.shape == APRL_SHAPE_LINEAR_BINOMIAL3 ? 0 : 1;
   a.i0 = (int)c.cpml_cells_x + 1;
   a.i1 = (int)(c.nx - c.cpml_cells_x);
   a.j0 = (int)c.cpml_cells_y + 1;

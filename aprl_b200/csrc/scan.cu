@@ -29,6 +29,7 @@
 
 namespace aprl_gpu {
 aprl_status report_error(aprl_status status, const char* message);
+const char* run_error(const aprl_run* r);
 }
 
 namespace {
@@ -105,14 +106,18 @@ struct aprl_scan {
   std::map<uint64_t, std::shared_ptr<Job>> jobs;
   std::vector<std::thread> workers;
 
+  uint32_t runs_per_slot = 1;
+
   void work(int slot);
-  void run_job(Job& job, int slot, cudaStream_t stream);
+  aprl_run* start_job(Job& job, int slot, cudaStream_t stream);
+  void end_job(Job& job, aprl_run* run, aprl_status s);
 };
 
-void aprl_scan::run_job(Job& job, int slot, cudaStream_t stream) {
+// A request's run: created on `stream`, inlet tables and particles set.
+// Returns nullptr (with the failure in the job's result) when that fails.
+aprl_run* aprl_scan::start_job(Job& job, int slot, cudaStream_t stream) {
   const aprl_scan_request& q = job.request;
-  aprl_scan_result& res = job.result;
-  res.slot = slot;
+  job.result.slot = slot;
   aprl_run* run = nullptr;
   aprl_status s = aprl_run_create(&q.config, stream, &run);
   for (unsigned a = 0; a < 6 && s == APRL_OK; ++a) {
@@ -128,52 +133,122 @@ void aprl_scan::run_job(Job& job, int slot, cudaStream_t stream) {
                                q.mass, q.id, 1);
   if (s == APRL_OK && q.frozen)
     s = aprl_run_set_held(run, q.particles, q.frozen, q.frozen_beta_z);
-  if (s == APRL_OK) s = aprl_run_step(run, (uint32_t)q.steps);
+  if (s != APRL_OK) {
+    end_job(job, run, s);
+    return nullptr;
+  }
+  return run;
+}
+
+// The detector plane and statistics of a finished run (or its failure),
+// then the run is destroyed.
+void aprl_scan::end_job(Job& job, aprl_run* run, aprl_status s) {
+  const aprl_scan_request& q = job.request;
+  aprl_scan_result& res = job.result;
   int inside = 0;
   if (s == APRL_OK && q.detector)
     s = aprl_run_sample_field_plane(run, q.detector_lab_z, q.detector,
                                     (size_t)(6 * q.config.nx * q.config.ny), &inside);
-  if (run) {
-    aprl_run_get_stats(run, &res.stats);
-  }
+  if (run) aprl_run_get_stats(run, &res.stats);
   res.status = s;
   res.detector_inside = inside;
-  if (s != APRL_OK) {
-    std::snprintf(res.message, sizeof res.message, "%s", aprl_last_error());
-  }
+  if (s != APRL_OK) std::snprintf(res.message, sizeof res.message, "%s", aprl_last_error());
   if (run) aprl_run_destroy(run);
 }
 
+// A worker steps a group of up to runs_per_slot runs in lock step.  At every
+// step boundary it admits queue heads that fit the budget into free places
+// of the group (FIFO, the head never overtaken) and retires the runs that
+// have taken their steps, so requests join and leave a running group.
 void aprl_scan::work(int slot) {
   cudaSetDevice(device);
-  cudaStream_t stream = nullptr;
-  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-  for (;;) {
+  const size_t capacity = std::max<uint32_t>(1u, runs_per_slot);
+  std::vector<cudaStream_t> streams(capacity, nullptr);
+  for (auto& st : streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  struct Active {
     std::shared_ptr<Job> job;
-    {
-      std::unique_lock<std::mutex> lock(mutex);
-      changed.wait(lock, [&] {
-        return (!queue.empty() && in_use + queue.front()->footprint <= budget) ||
-               (stopping && queue.empty());
-      });
-      if (queue.empty()) break;
-      job = queue.front();
-      queue.pop_front();
-      in_use += job->footprint;
-      job->state = APRL_SCAN_RUNNING;
-      job->started = Clock::now();
-    }
-    changed.notify_all();
-    run_job(*job, slot, stream);
+    aprl_run* run;
+    size_t place;
+    uint64_t done;
+  };
+  std::vector<Active> group;
+  std::vector<bool> busy(capacity, false);
+  auto retire = [&](Active& a, aprl_status s) {
+    end_job(*a.job, a.run, s);
+    busy[a.place] = false;
     {
       std::lock_guard<std::mutex> lock(mutex);
-      job->finished = Clock::now();
-      job->state = APRL_SCAN_DONE;
-      in_use -= job->footprint;
+      a.job->finished = Clock::now();
+      a.job->state = APRL_SCAN_DONE;
+      in_use -= a.job->footprint;
     }
     changed.notify_all();
+  };
+  for (;;) {
+    std::vector<std::shared_ptr<Job>> admitted;
+    {
+      std::unique_lock<std::mutex> lock(mutex);
+      if (group.empty())
+        changed.wait(lock, [&] {
+          return (!queue.empty() && in_use + queue.front()->footprint <= budget) ||
+                 (stopping && queue.empty());
+        });
+      if (group.empty() && queue.empty()) break;
+      while (group.size() + admitted.size() < capacity && !queue.empty() &&
+             in_use + queue.front()->footprint <= budget) {
+        auto job = queue.front();
+        queue.pop_front();
+        in_use += job->footprint;
+        job->state = APRL_SCAN_RUNNING;
+        job->started = Clock::now();
+        admitted.push_back(job);
+      }
+    }
+    if (!admitted.empty()) changed.notify_all();
+    for (auto& job : admitted) {
+      size_t place = 0;
+      while (busy[place]) ++place;
+      busy[place] = true;
+      Active a{job, nullptr, place, 0};
+      a.run = start_job(*job, slot, streams[place]);
+      if (!a.run) {
+        busy[place] = false;
+        std::lock_guard<std::mutex> lock(mutex);
+        job->finished = Clock::now();
+        job->state = APRL_SCAN_DONE;
+        in_use -= job->footprint;
+        continue;
+      }
+      if (job->request.steps == 0) {
+        retire(a, APRL_OK);
+        continue;
+      }
+      group.push_back(a);
+    }
+    if (group.empty()) {
+      changed.notify_all();
+      continue;
+    }
+    std::vector<aprl_run*> runs(group.size());
+    std::vector<aprl_status> status(group.size(), APRL_OK);
+    for (size_t i = 0; i < group.size(); ++i) runs[i] = group[i].run;
+    aprl_runs_step(runs.data(), runs.size(), 1, status.data());
+    std::vector<Active> next;
+    for (size_t i = 0; i < group.size(); ++i) {
+      Active& a = group[i];
+      if (status[i] != APRL_OK) {
+        aprl_gpu::report_error(status[i], aprl_gpu::run_error(a.run));
+        retire(a, status[i]);
+      } else if (++a.done >= a.job->request.steps) {
+        retire(a, APRL_OK);
+      } else {
+        next.push_back(a);
+      }
+    }
+    group.swap(next);
   }
-  if (stream) cudaStreamDestroy(stream);
+  for (auto& st : streams)
+    if (st) cudaStreamDestroy(st);
 }
 
 extern "C" {
@@ -197,6 +272,7 @@ aprl_status aprl_scan_create(const aprl_scan_config* config, aprl_scan** out) {
     return scan_fail(APRL_ERR_CUDA, "No current CUDA device for the scan");
   }
   scan->budget = config->device_budget_bytes;
+  scan->runs_per_slot = std::max<uint32_t>(1u, config->runs_per_slot);
   if (scan->budget == 0) {
     size_t free_bytes = 0, total = 0;
     if (cudaMemGetInfo(&free_bytes, &total) != cudaSuccess) {

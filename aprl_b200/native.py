@@ -27,6 +27,8 @@ _SIGNATURES = {
     "last_error": (C.c_char_p, []),
     "magnet_prepare": (C.c_int, [C.POINTER(abi.Magnet)]),
     "cowan_coefficients": (C.c_int, [C.c_double, C.c_double, C.c_double, _D]),
+    "runs_step": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, C.c_uint32, C.POINTER(C.c_int)]),
+    "boris_push": (C.c_int, [C.c_size_t, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, C.c_double]),
     "run_destroy": (C.c_int, [_H]),
     "run_set_reference": (C.c_int, [_H, C.c_uint, _D, C.c_size_t]),
     "run_set_reference_planes": (C.c_int, [_H, C.c_uint, C.c_uint64, C.c_uint64, _D]),
@@ -149,6 +151,23 @@ def load():
                 "(run `python -m aprl_b200.build`); there is no CPU fallback")
         _PRODUCT = bind(C.CDLL(LIBRARY_PATH), "aprl_", product=True)
     return _PRODUCT
+
+
+CHECKED_LIBRARY_PATH = os.path.join(_HERE, "libaprl_b200_checked.so")
+_CHECKED = None
+
+
+def load_checked():
+    """The bounds-checked build of the library (every field, current and
+    history index tested on the device; an index outside its array is a
+    device error, never an access).  For tests; raises when not built."""
+    global _CHECKED
+    if _CHECKED is None:
+        if not os.path.exists(CHECKED_LIBRARY_PATH):
+            raise ImportError(f"bounds-checked library not built: {CHECKED_LIBRARY_PATH} "
+                              "(run `python -m aprl_b200.build`)")
+        _CHECKED = bind(C.CDLL(CHECKED_LIBRARY_PATH), "aprl_", product=True)
+    return _CHECKED
 
 
 def _ptr(array, ctype=C.c_double):
@@ -434,9 +453,9 @@ class Scan:
     """A parameter-scan server (aprl_scan_*): independent runs admitted by
     device footprint into `slots` concurrent streams of one GPU."""
 
-    def __init__(self, binding, budget_bytes=0, slots=4):
+    def __init__(self, binding, budget_bytes=0, slots=4, runs_per_slot=1):
         self.b = binding
-        cfg = abi.ScanConfig(int(budget_bytes), int(slots), 0)
+        cfg = abi.ScanConfig(int(budget_bytes), int(slots), int(runs_per_slot))
         handle = C.c_void_p()
         binding("scan_create", C.byref(cfg), C.byref(handle))
         self.handle = handle

@@ -145,8 +145,8 @@ typedef struct {
    * serial and therefore repeatable).  0: the current J is summed with FP64
    * atomics, whose order -- and so the last bits of J -- varies from run to
    * run.  1: every deposit contribution is rounded once to a 128-bit fixed
-   * point (2^-62 of the run's largest possible single contribution,
-   * 4*max|q|*c/(dx*dy*dz)) and summed as integers, which is exact and
+   * point (a power-of-two quantum below 2^-61 of the run's largest possible
+   * single contribution, 4*max|q|*c/(dx*dy*dz)) and summed as integers, which is exact and
    * order-free, then converted to binary64 once per trial; the charge-matched
    * inlet's layer charge is summed the same way.  Two runs of the same
    * requests then give identical bits on the same GPU, and J is closer to
@@ -203,6 +203,22 @@ aprl_status aprl_magnet_prepare(aprl_magnet* magnet);
  * deltaZX, ratio[3] (12 doubles). */
 aprl_status aprl_cowan_coefficients(double dx, double dy, double dz,
                                     double out[12]);
+
+/* RelativisticBorisPusher::push (src/eb_particles.cpp:207-216): for each of
+ * `count` particles, pushMomentum (:99-127: half electric kick, magnetic
+ * rotation at the kicked gamma, half kick) with its own E and B
+ * (electric/magnetic: 3*count values, box frame, SI), then pushPosition
+ * (:129-136: drift over dt at the new proper velocity).  Positions and
+ * proper velocities are updated in place (host arrays; the work runs on the
+ * current device).  The reference checks the parameters the same way
+ * ("Invalid SI particle pusher parameters", std::invalid_argument).  The
+ * moving-window coupled step does not use it: held particles drift at
+ * c*frozenBetaZ and active ones take the Lapenta-Markidis push. */
+aprl_status aprl_boris_push(size_t count, double* x, double* y, double* z,
+                            double* ux, double* uy, double* uz,
+                            const double* charge, const double* mass,
+                            const double* electric, const double* magnetic,
+                            double dt);
 
 /* EBFieldGrid(EBGridGeometry) + EBConvolutionalPML + MovingWindowFields +
  * ConservativeSourceCoupling construction (src/eb_field.cpp:211-229,
@@ -325,6 +341,20 @@ aprl_status aprl_run_shift(aprl_run* run);
 /* Whole steps: Simulation::solve's loop body for one rank with the moving
  * window and conservative-source coupling (src/simulation.cpp:493-613). */
 aprl_status aprl_run_step(aprl_run* run, uint32_t steps);
+
+/* `steps` coupled steps of `count` independent runs in lock step (no
+ * counterpart in the reference, which steps one Simulation per job): each
+ * step of every run is queued -- begin, magnetic update, preview and the
+ * fixed-point trials issued ahead -- before the host waits for any of them,
+ * then each run's residuals are read, its stopping rule applied and its
+ * commit and shift queued.  The runs' kernels overlap on their own streams
+ * (give each run its own stream at aprl_run_create) and the host waits once
+ * per run and step instead of stalling the GPU between runs.  Each run's
+ * result is exactly what aprl_run_step gives it.  A run that fails stops
+ * there (its status in statuses[i], which may be NULL) while the others go
+ * on; the return value is the first failure's status, with its message. */
+aprl_status aprl_runs_step(aprl_run* const* runs, size_t count, uint32_t steps,
+                           aprl_status* statuses);
 
 aprl_status aprl_run_get_stats(const aprl_run* run, aprl_step_stats* stats);
 aprl_status aprl_run_reset_iteration_stats(aprl_run* run);
@@ -505,11 +535,14 @@ aprl_status aprl_run_get_reference(aprl_run* run, unsigned component, double* ho
                                    size_t count);
 
 /* Discrete Gauss law of the current state, reduced on the GPU.  The node
- * charge density is the one the linear-binomial3 current conserves: per
- * particle, F3 node weights in x over nodes i-1..i+2, linear weights in y
- * over j, j+1 and the binomial3-smoothed linear weights in z over
- * k-1..k+2, times q/(dx dy dz) (the F3 density of
- * verification/transverse_binomial_checks.cpp:12-66).  At every node
+ * charge density is the one the run's current conserves, times q/(dx dy dz)
+ * per particle: for linear-binomial3, F3 node weights in x over nodes
+ * i-1..i+2, linear weights in y over j, j+1 and the binomial3-smoothed
+ * linear weights in z over k-1..k+2 (the F3 density of
+ * verification/transverse_binomial_checks.cpp:12-66); for
+ * quintic-compensated, linear weights in x and y and the quintic node basis
+ * in z over floor(z)-5..floor(z)+6 (longitudinal_shape::nodeWeight,
+ * src/longitudinal_shape.h:48-56).  At every node
  * G = eps0 div E - rho, div E from the Yee edges around the node (edges
  * outside the grid count as zero).  The reference audits the same law
  * through the charge continuity of its deposit
@@ -527,10 +560,8 @@ typedef struct {
 } aprl_gauss_law;
 
 /* Between steps, or after the commit and before the shift.  `residual` (may be NULL): (nx+1)*(ny+1)*(nz+1) doubles,
- * G at node (i, j, k) at [(k*(ny+1) + j)*(nx+1) + i].  Only the
- * linear-binomial3 shape has this node density (APRL_ERR_UNSUPPORTED
- * otherwise).  The density is summed with FP64 atomics, so G varies in the
- * last bits from call to call. */
+ * G at node (i, j, k) at [(k*(ny+1) + j)*(nx+1) + i].  The density is
+ * summed with FP64 atomics, so G varies in the last bits from call to call. */
 aprl_status aprl_run_gauss_law(aprl_run* run, aprl_gauss_law* out, double* residual,
                                size_t count);
 
@@ -563,8 +594,13 @@ typedef struct aprl_scan aprl_scan;
 typedef struct {
   uint64_t device_budget_bytes;   /* device memory the scan's runs may hold at
                                      once; 0 = 90% of the free memory at create */
-  uint32_t max_slots;             /* runs in flight at once (1..256) */
-  uint32_t reserved;
+  uint32_t max_slots;             /* worker threads (1..256) */
+  /* Runs each worker steps in lock step with aprl_runs_step (0 or 1: one run
+   * per worker, stepped alone).  A worker admits queued requests into its
+   * group at every step boundary while the group has room and the budget
+   * allows, and a finished run leaves the group at once, so a request that
+   * arrives while others run joins them at the next step. */
+  uint32_t runs_per_slot;
 } aprl_scan_config;
 
 /* One run.  Every pointer is the caller's and must stay valid until the

@@ -415,6 +415,43 @@ static inline void cross3(const double l[3], const double r[3], double o[3]) {
   o[2] = l[0] * r[1] - l[1] * r[0];
 }
 
+/* RelativisticBorisPusher::push (src/eb_particles.cpp:99-139, 207-216):
+ * pushMomentum then pushPosition, per particle, in place. */
+aprl_status oracle_boris_push(size_t count, double* x, double* y, double* z, double* ux,
+                              double* uy, double* uz, const double* charge, const double* mass,
+                              const double* electric, const double* magnetic, double dt) {
+  if (!(dt > 0.0) || !isfinite(dt))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI particle pusher parameters");
+  for (size_t n = 0; n < count; ++n) {
+    const double q = charge[n], m = mass[n];
+    if (!(m > 0.0) || !isfinite(m) || !isfinite(q))
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid SI particle pusher parameters");
+    const double* e = electric + 3 * n;
+    const double* b = magnetic + 3 * n;
+    double u[3] = {ux[n], uy[n], uz[n]};
+    const double kick = q * dt / (2.0 * m * SI_C);
+    double minus[3], t[3], prime[3], sv[3], plus[3];
+    for (int d = 0; d < 3; ++d) minus[d] = u[d] + kick * e[d];
+    const double rs = q * dt / (2.0 * m * gamma_u(minus));
+    for (int d = 0; d < 3; ++d) t[d] = rs * b[d];
+    cross3(minus, t, prime);
+    for (int d = 0; d < 3; ++d) prime[d] += minus[d];
+    const double f = 2.0 / (1.0 + (t[0] * t[0] + t[1] * t[1] + t[2] * t[2]));
+    for (int d = 0; d < 3; ++d) sv[d] = t[d] * f;
+    cross3(prime, sv, plus);
+    for (int d = 0; d < 3; ++d) plus[d] += minus[d];
+    for (int d = 0; d < 3; ++d) u[d] = plus[d] + kick * e[d];
+    const double drift = SI_C * dt / gamma_u(u);
+    x[n] += drift * u[0];
+    y[n] += drift * u[1];
+    z[n] += drift * u[2];
+    ux[n] = u[0];
+    uy[n] = u[1];
+    uz[n] = u[2];
+  }
+  return APRL_OK;
+}
+
 /* source_coupling_math::momentum: Lapenta-Markidis mean-gamma Newton solve
  * (src/source_coupling_math.h:272-293).  Returns iterations+1, or -1 for a
  * nonphysical root, -2 for no convergence. */

@@ -99,6 +99,10 @@ int oracle_momentum(double u[3], const double e[3], const double b[3],
                     double q, double m, double h, double known_gamma);
 /* BoostFrameTransform::gammaFromProperVelocity. */
 double oracle_gamma(const double u[3]);
+/* RelativisticBorisPusher::push per particle (src/eb_particles.cpp:207-216). */
+aprl_status oracle_boris_push(size_t count, double* x, double* y, double* z, double* ux,
+                              double* uy, double* uz, const double* charge, const double* mass,
+                              const double* electric, const double* magnetic, double dt);
 /* Prescribed lab magnets seen in the box frame at (position, time). */
 aprl_status oracle_prescribed_box(const aprl_run_config* config,
                                   const double position[3], double time,

@@ -834,6 +834,36 @@ int ref_momentum(double u[3], const double e[3], const double b[3], double q, do
   }
 }
 
+// The reference's own RelativisticBorisPusher::push, particle by particle.
+aprl_status ref_boris_push(size_t count, double* x, double* y, double* z, double* ux, double* uy,
+                           double* uz, const double* charge, const double* mass,
+                           const double* electric, const double* magnetic, double dt) {
+  try {
+    for (size_t n = 0; n < count; ++n) {
+      aprl::RelativisticParticleSI p;
+      p.position[0] = x[n]; p.position[1] = y[n]; p.position[2] = z[n];
+      p.properVelocity[0] = ux[n]; p.properVelocity[1] = uy[n]; p.properVelocity[2] = uz[n];
+      p.charge = charge[n];
+      p.mass = mass[n];
+      Vec e, b;
+      for (unsigned a = 0; a < 3; ++a) {
+        e[a] = electric[3 * n + a];
+        b[a] = magnetic[3 * n + a];
+      }
+      aprl::RelativisticBorisPusher::push(p, e, b, dt);
+      x[n] = p.position[0]; y[n] = p.position[1]; z[n] = p.position[2];
+      ux[n] = p.properVelocity[0]; uy[n] = p.properVelocity[1]; uz[n] = p.properVelocity[2];
+    }
+    return APRL_OK;
+  } catch (const std::invalid_argument& ex) {
+    g_error = ex.what();
+    return APRL_ERR_INVALID_ARGUMENT;
+  } catch (const std::exception& ex) {
+    g_error = ex.what();
+    return APRL_ERR_RUNTIME;
+  }
+}
+
 double ref_gamma(const double u[3]) {
   Vec uu;
   for (unsigned a = 0; a < 3; ++a) uu[a] = u[a];

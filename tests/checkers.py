@@ -125,11 +125,61 @@ def _f3_node(f):
     return np.stack([0.25 * (1.0 - f), 0.5 - 0.25 * f, 0.25 + 0.25 * f, 0.25 * f])
 
 
-def charge_density(cfg, origin, p, pad=2):
-    """The node charge density the linear-binomial3 current conserves: F3
-    node weights in x, linear in y, binomial3 in z
-    (verification/transverse_binomial_checks.cpp:12-66), [k][j][i] with
-    `pad` extra nodes on every side (index pad is node 0)."""
+def _quintic_node(f):
+    """The quintic-compensated node basis (longitudinal_shape.h:48-54) for
+    cell-relative offsets f: 12 weights per particle, nodes cell-5 .. cell+6."""
+    n = np.zeros((6, f.size))
+    n[0] = 1.0
+    for j in range(1, 6):
+        saved = np.zeros(f.size)
+        for k in range(j):
+            t = n[k] / j
+            n[k] = saved + (k + 1 - f) * t
+            saved = (f + j - k - 1) * t
+        n[j] = saved
+    p = 5.0
+    a = p / 6.0
+    b = 3 * p / 40.0 + p * (p - 1) / 72.0
+    d = 5 * p / 112.0 + p * (p - 1) / 80.0 + p * (p - 1) * (p - 2) / 1296.0
+    c = [-d / 64.0, b / 16.0 + 3 * d / 32.0, -a / 4.0 - b / 4.0 - 15 * d / 64.0,
+         1 + a / 2.0 + 3 * b / 8.0 + 5 * d / 16.0, -a / 4.0 - b / 4.0 - 15 * d / 64.0,
+         b / 16.0 + 3 * d / 32.0, -d / 64.0]
+    v = np.zeros((12, f.size))
+    for j in range(6):
+        for k in range(7):
+            v[j + k] += n[j] * c[k]
+    return v
+
+
+def charge_density(cfg, origin, p, pad=6):
+    """The node charge density the run's current conserves, [k][j][i] with
+    `pad` extra nodes on every side (index pad is node 0): for
+    linear-binomial3 F3 in x, linear in y, binomial3 in z
+    (verification/transverse_binomial_checks.cpp:12-66); for
+    quintic-compensated linear in x and y and the quintic node basis in z."""
+    if cfg.shape == 0:
+        return _binomial3_density(cfg, origin, p, pad)
+    rho = np.zeros((cfg.nz + 1 + 2 * pad, cfg.ny + 1 + 2 * pad, cfg.nx + 1 + 2 * pad))
+    x = (p["x"] - origin[0]) / cfg.dx
+    y = (p["y"] - origin[1]) / cfg.dy
+    z = (p["z"] - origin[2]) / cfg.dz
+    i = np.floor(x).astype(int)
+    j = np.floor(y).astype(int)
+    k = np.floor(z).astype(int)
+    fx, fy = x - i, y - j
+    wz = _quintic_node(z - k)
+    q = p["charge"] / (cfg.dx * cfg.dy * cfg.dz)
+    for u in range(2):
+        wx = fx if u else 1.0 - fx
+        for v in range(2):
+            wy = fy if v else 1.0 - fy
+            for t in range(12):
+                np.add.at(rho, (k - 5 + t + pad, j + v + pad, i + u + pad),
+                          q * wx * wy * wz[t])
+    return rho, pad
+
+
+def _binomial3_density(cfg, origin, p, pad):
     rho = np.zeros((cfg.nz + 1 + 2 * pad, cfg.ny + 1 + 2 * pad, cfg.nx + 1 + 2 * pad))
     x = (p["x"] - origin[0]) / cfg.dx
     y = (p["y"] - origin[1]) / cfg.dy

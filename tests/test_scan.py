@@ -66,11 +66,13 @@ def test_footprint_grows_with_grid_particles_and_precision():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("group", [1, 4])
 @pytest.mark.parametrize("precision,bound", [("fp64", 1e-12), ("fp32-mixed", 1e-6)])
-def test_each_result_is_the_same_alone_and_in_the_mix(precision, bound):
+def test_each_result_is_the_same_alone_and_in_the_mix(precision, bound, group):
+    """group: runs each worker steps in lock step (aprl_runs_step)."""
     ws = draws(6, precision)
     alone = [plain_detector(w) for w in ws]
-    scan = native.Scan(native.load(), slots=4)
+    scan = native.Scan(native.load(), slots=4 if group == 1 else 2, runs_per_slot=group)
     tickets = submit_all(scan, ws)
     results = [scan.wait(t) for t in tickets]
     scan.close()
@@ -83,7 +85,40 @@ def test_each_result_is_the_same_alone_and_in_the_mix(precision, bound):
     # Requests submitted together ran at the same time on different slots.
     spans = sorted((r["start_s"], r["finish_s"]) for r in results)
     assert any(b0 < a1 for (a0, a1), (b0, b1) in zip(spans, spans[1:]))
-    assert len({r["slot"] for r in results}) > 1
+    if group == 1:
+        assert len({r["slot"] for r in results}) > 1
+
+
+@pytest.mark.gpu
+def test_lock_step_gives_each_run_its_own_bits():
+    """aprl_runs_step: three different runs (bit-reproducible current sum)
+    stepped in lock step end with the bits each gets stepped alone."""
+    import ctypes
+    ws = draws(3, "fp64", seed=5)
+    for w in ws:
+        w.config = workloads.with_determinism(w.config)
+    def start(w):
+        run = native.Run(native.load(), w.config)
+        run.allocate_reference()
+        run.set_particles(w.particles)
+        return run
+    alone = []
+    for w in ws:
+        r = start(w)
+        r.step(STEPS)
+        alone.append(checkers.state(r))
+    runs = [start(w) for w in ws]
+    handles = (ctypes.c_void_p * len(runs))(*[r.handle for r in runs])
+    statuses = (ctypes.c_int * len(runs))()
+    native.load()("runs_step", handles, len(runs), STEPS, statuses)
+    assert list(statuses) == [0] * len(runs)
+    for r, a in zip(runs, alone):
+        b = checkers.state(r)
+        for x, y in zip(a["fields"] + a["histories"], b["fields"] + b["histories"]):
+            np.testing.assert_array_equal(x, y)
+        for k in a["particles"]:
+            np.testing.assert_array_equal(a["particles"][k], b["particles"][k])
+        assert a["stats"] == b["stats"]
 
 
 @pytest.mark.gpu
