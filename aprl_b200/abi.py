@@ -189,7 +189,7 @@ class SelfFieldConfig(C.Structure):
         ("model", C.c_int32),
         ("include_transverse_cpml_particles", C.c_int32),
         ("hold_transverse_until_activation", C.c_int32),
-        ("reserved", C.c_int32),
+        ("solver", C.c_int32),
         ("relative_tolerance", C.c_double),
         ("maximum_mean_transverse_beta", C.c_double),
         ("maximum_iterations", C.c_uint64),
@@ -221,9 +221,12 @@ class SelfFieldReport(C.Structure):
 def self_field_config(run_config, model="cowan-relativistic-poisson", tolerance=1e-10,
                       maximum_iterations=20000, maximum_mean_transverse_beta=0.05,
                       include_transverse_cpml_particles=False,
-                      hold_transverse_until_activation=False):
-    """The initializer controls with the CPML cells as the static guard."""
+                      hold_transverse_until_activation=False, solver="cg"):
+    """The initializer controls with the CPML cells as the static guard;
+    solver "cg" (the reference's initializer) or "modal" (transverse sine
+    modes and a tridiagonal solve along z per mode)."""
     c = SelfFieldConfig()
+    c.solver = {"cg": 0, "modal": 1}[solver]
     c.model = SELF_FIELD_MODELS[model]
     c.include_transverse_cpml_particles = int(include_transverse_cpml_particles)
     c.hold_transverse_until_activation = int(hold_transverse_until_activation)

@@ -62,7 +62,7 @@ enum Kernel : unsigned {
   kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfUpdate,
   kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
   kInletHalo, kInletCharge, kInletComplete, kRadixCount, kPermuteParticles,
-  kCurrentConvert, kFixedConvert, kChordDeposit, kKernelCount
+  kCurrentConvert, kFixedConvert, kChordDeposit, kSfModal, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -76,7 +76,7 @@ const char* kKernelNames[kKernelCount] = {
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
   "sf_update", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
   "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete",
-  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit"};
+  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit", "sf_modal"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -116,7 +116,7 @@ aprl_status device_error_status(unsigned code) {
   switch (code) {
     case kErrOrbitOutside: case kErrDepositOutside: case kErrSupportX:
     case kErrSupportY: case kErrStartInCpml: case kErrStartOutside:
-    case kErrReferenceRange:
+    case kErrReferenceRange: case kErrBounds:
       return APRL_ERR_OUT_OF_RANGE;
     default:
       return APRL_ERR_RUNTIME;
@@ -3088,8 +3088,60 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   if (!(sums[1].hi > 0.0) || !std::isfinite(sums[1].hi))
     return fail(APRL_ERR_RUNTIME, "Initial particle charge produced an invalid Poisson source norm");
 
-  // Conjugate gradients, in batches of iterations between host reads.
   SfState state{};
+  if (cfg->solver == APRL_SELF_FIELD_SOLVER_MODAL) {
+    // The transverse-mode direct solve on the same box (sf_modal_*): the
+    // source b = rho/eps0 (in the residual slab) into a compact interior
+    // array, sine transforms along x and y, one tridiagonal solve along z per
+    // mode, the inverse transforms, and the potential back into the lattice.
+    const int ix = L.hi[0] - L.lo[0] - 1, iy = L.hi[1] - L.lo[1] - 1, iz = L.hi[2] - L.lo[2] - 1;
+    if (ix < 1 || iy < 1 || iz < 1)
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Initial field solve domain has no interior");
+    const size_t count = (size_t)ix * iy * iz;
+    std::vector<double> table_x((size_t)ix * ix), table_y((size_t)iy * iy), cos_x(ix), cos_y(iy);
+    for (int m = 0; m < ix; ++m) {
+      cos_x[m] = std::cos(kPi * (m + 1) / (ix + 1));
+      for (int t = 0; t < ix; ++t)
+        table_x[(size_t)m * ix + t] = std::sin(kPi * (double)((long long)(m + 1) * (t + 1) % (2 * (ix + 1))) / (ix + 1));
+    }
+    for (int m = 0; m < iy; ++m) {
+      cos_y[m] = std::cos(kPi * (m + 1) / (iy + 1));
+      for (int t = 0; t < iy; ++t)
+        table_y[(size_t)m * iy + t] = std::sin(kPi * (double)((long long)(m + 1) * (t + 1) % (2 * (iy + 1))) / (iy + 1));
+    }
+    double* tables = nullptr;
+    const size_t table_words = table_x.size() + table_y.size() + ix + iy;
+    TRY(device_alloc(r, &tables, table_words));
+    double* tx = tables;
+    double* ty = tx + table_x.size();
+    double* cx = ty + table_y.size();
+    double* cy = cx + ix;
+    CUDA_TRY(run_copy(r, tx, table_x.data(), table_x.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, ty, table_y.data(), table_y.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, cx, cos_x.data(), ix * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(run_copy(r, cy, cos_y.data(), iy * 8, cudaMemcpyHostToDevice));
+    double* w0 = A.direction;  // compact arrays: the two free CG slabs and
+    double* w1 = A.image;      // the residual slab (after the gather)
+    double* work = A.residual;
+    const unsigned blocks = blocks_for(count, 256);
+    TRY(launch(r, kSfModal, sf_modal_gather_kernel, dim3(blocks), dim3(256), A, w0, ix, iy, iz));
+    TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
+               (const double*)w0, w1, (const double*)tx, 0, ix, iy, iz, 1.0));
+    TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
+               (const double*)w1, w0, (const double*)ty, 1, ix, iy, iz, 1.0));
+    TRY(launch(r, kSfModal, sf_modal_z_kernel, dim3(blocks_for(ix, 32), blocks_for(iy, 4)),
+               dim3(32, 4), A, w0, work, (const double*)cx, (const double*)cy, ix, iy, iz));
+    TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
+               (const double*)w0, w1, (const double*)ty, 1, ix, iy, iz, 2.0 / (iy + 1)));
+    TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
+               (const double*)w1, w0, (const double*)tx, 0, ix, iy, iz, 2.0 / (ix + 1)));
+    TRY(launch(r, kSfModal, sf_modal_scatter_kernel, dim3(blocks), dim3(256), A,
+               (const double*)w0, ix, iy, iz));
+    device_free(r, tables);
+    state.done = 1;
+    rep->iterations = 0;
+  } else {
+  // Conjugate gradients, in batches of iterations between host reads.
   state.rr = sums[1];
   state.source = sums[1];
   CUDA_TRY(cudaMemcpyAsync(buf.state, &state, sizeof state, cudaMemcpyHostToDevice, r->stream));
@@ -3108,10 +3160,12 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
     if (state.done) break;
   }
   rep->iterations = state.iterations;
+  }
   if (state.done == 2) return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG lost positive definiteness");
   if (state.done == 3)
     return fail(APRL_ERR_RUNTIME, "Initial Gauss-field CG produced a non-finite residual");
-  if (state.done != 1 || state.relative > cfg->relative_tolerance)
+  if (state.done != 1 || (cfg->solver != APRL_SELF_FIELD_SOLVER_MODAL &&
+                          state.relative > cfg->relative_tolerance))
     return fail(APRL_ERR_RUNTIME,
                 "Initial Gauss-field solve did not converge; increase "
                 "initial_self_field.maximum_iterations, relax its relative_tolerance, or reduce "

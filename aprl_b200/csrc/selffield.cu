@@ -510,3 +510,104 @@ __global__ void __launch_bounds__(kSelfFieldThreads) sf_energy_kernel(SfArgs a, 
 }
 
 }  // namespace aprl_gpu
+
+namespace aprl_gpu {
+
+// ---------------------------------------------------------------------------
+// The transverse-mode (modal) direct solve of the same discrete operator on
+// the same Dirichlet box: the method of the reference's blocked Cowan
+// reference (src/blocked_cowan_reference.h:59-130), which expands the
+// potential in the sine modes of the transverse Dirichlet problem and solves
+// one tridiagonal system along z per mode.  The 7-point and 27-point
+// operators have constant coefficients and are even in x and in y, so the
+// type-I sine transform along x and along y diagonalises them: mode (m, n)
+// sees the z stencil lambda_c = sum over (dy, dx) of st[c][dy][dx] *
+// C_x(dx) * C_y(dy), C(0) = 1, C(+-1) = cos(pi (m+1) / (N+1)).  Transforms
+// are dense sums against a sine table (the interior is at most a few
+// hundred nodes across), in binary64 with fused multiply-adds.
+//
+// Compact interior layout: index (k * Iy + j) * Ix + i.
+
+__global__ void sf_modal_gather_kernel(SfArgs a, double* out, int ix, int iy, int iz) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (long long)ix * iy * iz) return;
+  const int i = (int)(n % ix), j = (int)((n / ix) % iy), k = (int)(n / ((long long)ix * iy));
+  const SfLattice& L = a.L;
+  out[n] = a.residual[sf_at(L, L.lo[0] + 1 + i, L.lo[1] + 1 + j, L.lo[2] + 2 + k)];
+}
+
+__global__ void sf_modal_scatter_kernel(SfArgs a, const double* in, int ix, int iy, int iz) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (long long)ix * iy * iz) return;
+  const int i = (int)(n % ix), j = (int)((n / ix) % iy), k = (int)(n / ((long long)ix * iy));
+  const SfLattice& L = a.L;
+  a.potential[sf_at(L, L.lo[0] + 1 + i, L.lo[1] + 1 + j, L.lo[2] + 2 + k)] = in[n];
+}
+
+// out = scale * S in along x (axis 0) or y (axis 1), S[m][t] = table[m * len + t].
+__global__ void sf_modal_transform_kernel(const double* in, double* out, const double* table,
+                                          int axis, int ix, int iy, int iz, double scale) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (long long)ix * iy * iz) return;
+  const int i = (int)(n % ix), j = (int)((n / ix) % iy);
+  const long long plane = n / ((long long)ix * iy) * ((long long)ix * iy);
+  double v = 0.0;
+  if (axis == 0) {
+    const double* line = in + plane + (long long)j * ix;
+    const double* row = table + (long long)i * ix;
+    for (int t = 0; t < ix; ++t) v = fma(row[t], line[t], v);
+  } else {
+    const double* column = in + plane + i;
+    const double* row = table + (long long)j * iy;
+    for (int t = 0; t < iy; ++t) v = fma(row[t], column[(long long)t * ix], v);
+  }
+  out[n] = scale * v;
+}
+
+// One tridiagonal solve along z per transverse mode (Thomas elimination; the
+// per-mode operator is symmetric positive definite).  `work` holds the
+// eliminated super-diagonal.
+__global__ void sf_modal_z_kernel(SfArgs a, double* data, double* work, const double* cos_x,
+                                  const double* cos_y, int ix, int iy, int iz) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = blockIdx.y * blockDim.y + threadIdx.y;
+  if (m >= ix || n >= iy) return;
+  double st[27];
+  if (a.cowan) {
+    for (int q = 0; q < 27; ++q) st[q] = a.stencil[q];
+  } else {
+    for (int q = 0; q < 27; ++q) st[q] = 0.0;
+    st[13] = a.diagonal;
+    st[12] = st[14] = -a.cx;
+    st[10] = st[16] = -a.cy;
+    st[4] = st[22] = -a.cz;
+  }
+  const double cx = cos_x[m], cy = cos_y[n];
+  const double fx[3] = {cx, 1.0, cx}, fy[3] = {cy, 1.0, cy};
+  double lambda[3];
+  for (int c = 0; c < 3; ++c) {
+    double v = 0.0;
+    for (int y = 0; y < 3; ++y)
+      for (int x = 0; x < 3; ++x) v = fma(st[(c * 3 + y) * 3 + x], fx[x] * fy[y], v);
+    lambda[c] = v;
+  }
+  const long long step = (long long)ix * iy, base = (long long)n * ix + m;
+  const double sub = lambda[0], diag = lambda[1], sup = lambda[2];
+  double previous_c = 0.0, previous_d = 0.0;
+  for (int k = 0; k < iz; ++k) {
+    const double den = diag - sub * previous_c;
+    const double ck = sup / den;
+    const double dk = (data[base + k * step] - sub * previous_d) / den;
+    work[base + k * step] = ck;
+    data[base + k * step] = dk;
+    previous_c = ck;
+    previous_d = dk;
+  }
+  double next = 0.0;
+  for (int k = iz - 1; k >= 0; --k) {
+    next = data[base + k * step] - work[base + k * step] * next;
+    data[base + k * step] = next;
+  }
+}
+
+}  // namespace aprl_gpu

@@ -89,6 +89,13 @@ __global__ void sf_clear_outside_kernel(SfArgs a, int component, int gx, int gy,
 __global__ void sf_gauss_kernel(SfArgs a, const double* rho, int plo0, int phi0, int plo1,
                                 int phi1, int plo2, int phi2, unsigned long long* max_bits);
 __global__ void sf_energy_kernel(SfArgs a, DD volume);
+// The transverse-mode direct solve (interior box in a compact layout).
+__global__ void sf_modal_gather_kernel(SfArgs a, double* out, int ix, int iy, int iz);
+__global__ void sf_modal_scatter_kernel(SfArgs a, const double* in, int ix, int iy, int iz);
+__global__ void sf_modal_transform_kernel(const double* in, double* out, const double* table,
+                                          int axis, int ix, int iy, int iz, double scale);
+__global__ void sf_modal_z_kernel(SfArgs a, double* data, double* work, const double* cos_x,
+                                  const double* cos_y, int ix, int iy, int iz);
 
 // Host helpers: the double-double quotient and square root rounded to binary64.
 double sf_ratio(DD a, DD b);

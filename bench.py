@@ -58,12 +58,15 @@ def parse_args(argv=None):
                    help="skip the drift, quintic and bit-reproducible step rates")
     p.add_argument("--no-scan", action="store_true",
                    help="skip the batched-ensemble and served-scan measurements")
-    p.add_argument("--ensemble-runs", type=int, default=32)
+    p.add_argument("--ensemble-runs", type=int, default=64)
     p.add_argument("--ensemble-steps", type=int, default=100)
-    p.add_argument("--scan-requests", type=int, default=16)
+    p.add_argument("--scan-requests", type=int, default=64, help="requests per arrival rate")
     p.add_argument("--scan-steps", type=int, default=500)
-    p.add_argument("--scan-rate", type=float, default=10.0, help="Poisson arrivals per second")
-    p.add_argument("--scan-slots", type=int, default=4)
+    p.add_argument("--scan-rates", default="5,10,20,50",
+                   help="Poisson arrival rates (requests per second), comma-separated")
+    p.add_argument("--scan-slots", type=int, default=4, help="scan worker threads")
+    p.add_argument("--scan-group", type=int, default=8,
+                   help="runs each worker steps in lock step")
     p.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     p.add_argument("--initial-self-field", choices=["auto", "on", "off"], default="auto",
                    help="start from the Cowan initial self-field (auto: on for the undulator "
@@ -659,6 +662,25 @@ def self_field_benchmark(args, stream):
         torch.cuda.synchronize()
         solves.append(start.elapsed_time(stop))
     ms = statistics.median(solves)
+    # The same solve by transverse modes (sine transforms in x and y, one
+    # tridiagonal system along z per mode): the direct method of the
+    # reference's blocked Cowan reference, on the same operator and box.
+    modal_config = abi.self_field_config(w.config, solver="modal")
+    run.initialize_self_field(modal_config)
+    modal = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        modal_report = run.initialize_self_field(modal_config)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        modal.append(start.elapsed_time(stop))
+    modal_fields = [run.get_field(a) for a in range(6)]
+    run.initialize_self_field(config)
+    cg_fields = [run.get_field(a) for a in range(6)]
+    modal_vs_cg = max(float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 1e-300)
+                      for a, b in zip(modal_fields, cg_fields))
     run.close()
     # The small case the CPU baseline also solves.
     sw = workloads.self_field_case(SELF_FIELD_SMALL["energy_ev"], nx=SELF_FIELD_SMALL["cells"][0],
@@ -682,11 +704,18 @@ def self_field_benchmark(args, stream):
         "cg_gbs_upper_bound": 88 * nodes * iterations / (ms * 1e-3) / 1e9,
         "gauss_relative_residual": report["relative_residual"],
         "mean_beta_z": report["mean_beta_z"],
+        "modal": {"ms": statistics.median(modal), "ms_solves": modal,
+                  "gauss_relative_residual": modal_report["relative_residual"],
+                  "fields_vs_cg_max_relative": modal_vs_cg},
         "small": {"workload": sw.name, "particles": SELF_FIELD_SMALL["particles"],
                   "ms_wall": small_ms, "iterations": small_report["iterations"]}}}
 
 
 def scan_benchmarks(args):
+    """The batched ensemble (64 seeded drift/dipole runs submitted at once)
+    and the served scan (Poisson arrivals at each rate), FP32-mixed through
+    the scan server (worker threads each stepping a group of runs in lock
+    step) against the plain FP64 path one run at a time."""
     lib = native.load()
     out = {}
     # -- batched ensemble: every run submitted at once ---------------------
@@ -695,7 +724,7 @@ def scan_benchmarks(args):
     t0 = time.perf_counter()
     exact = [_plain_fp64(lib, w, args.ensemble_steps) for w in draws]
     sequential_s = time.perf_counter() - t0
-    scan = native.Scan(lib, slots=args.scan_slots)
+    scan = native.Scan(lib, slots=args.scan_slots, runs_per_slot=args.scan_group)
     t0 = time.perf_counter()
     tickets = [scan.submit(w.config, w.particles, args.ensemble_steps,
                            detector_lab_z=workloads.detector_plane_lab_z(w.config))
@@ -708,20 +737,19 @@ def scan_benchmarks(args):
               if r["status"] == 0 and r["detector"] is not None and e is not None]
     out["batched_ensemble"] = {
         "runs": args.ensemble_runs, "steps": args.ensemble_steps, "slots": args.scan_slots,
+        "runs_per_slot": args.scan_group,
         "fp32_mixed_batched_solves_per_s": args.ensemble_runs / batched_s,
         "fp64_sequential_solves_per_s": args.ensemble_runs / sequential_s,
         "speedup": sequential_s / batched_s,
         "detector_rel_l2_vs_fp64": {"max": max(errors) if errors else None,
                                     "median": float(np.median(errors)) if errors else None},
         "failed": failed[:3]}
-    # -- served scan: Poisson arrivals --------------------------------------
-    rng = np.random.default_rng(5)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.scan_rate, args.scan_requests))
+    # -- served scan: Poisson arrivals at each rate ---------------------------
     reqs = [workloads.scan_draw(100 + i, seed=5, steps=args.scan_steps, precision="fp32-mixed")
             for i in range(args.scan_requests)]
 
-    def serve(precision, slots):
-        scan = native.Scan(lib, slots=slots)
+    def serve(arrivals, precision, slots, group):
+        scan = native.Scan(lib, slots=slots, runs_per_slot=group)
         t_start = time.perf_counter()
         tickets = []
         for at, w in zip(arrivals, reqs):
@@ -736,22 +764,28 @@ def scan_benchmarks(args):
         scan.close()
         return res, span
 
-    mixed, mixed_span = serve("fp32-mixed", args.scan_slots)
-    plain, plain_span = serve("fp64", 1)
-    errs = [_rel_l2(m["detector"], p["detector"]) for m, p in zip(mixed, plain)
-            if m["status"] == 0 and p["status"] == 0 and m["detector"] is not None]
-    out["served_scan"] = {
-        "requests": args.scan_requests, "steps": args.scan_steps,
-        "rate_req_per_s": args.scan_rate, "slots": args.scan_slots,
-        "fp32_mixed": {"solves_per_s": args.scan_requests / mixed_span,
-                       "latency_ms": _percentiles([r["total_ms"] for r in mixed]),
-                       "failed": sum(r["status"] != 0 for r in mixed)},
-        "fp64_sequential": {"solves_per_s": args.scan_requests / plain_span,
-                            "latency_ms": _percentiles([r["total_ms"] for r in plain]),
-                            "failed": sum(r["status"] != 0 for r in plain)},
-        "throughput_ratio": plain_span / mixed_span,
-        "detector_rel_l2_vs_fp64": {"max": max(errs) if errs else None},
-        "inlet": "vacuum (zero reference)"}
+    served = []
+    for rate in [float(x) for x in args.scan_rates.split(",") if x]:
+        rng = np.random.default_rng(5)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, args.scan_requests))
+        mixed, mixed_span = serve(arrivals, "fp32-mixed", args.scan_slots, args.scan_group)
+        plain, plain_span = serve(arrivals, "fp64", 1, 1)
+        errs = [_rel_l2(m["detector"], p["detector"]) for m, p in zip(mixed, plain)
+                if m["status"] == 0 and p["status"] == 0 and m["detector"] is not None]
+        served.append({
+            "rate_req_per_s": rate, "requests": args.scan_requests,
+            "arrival_span_s": float(arrivals[-1]),
+            "fp32_mixed": {"solves_per_s": args.scan_requests / mixed_span,
+                           "latency_ms": _percentiles([r["total_ms"] for r in mixed]),
+                           "failed": sum(r["status"] != 0 for r in mixed)},
+            "fp64_sequential": {"solves_per_s": args.scan_requests / plain_span,
+                                "latency_ms": _percentiles([r["total_ms"] for r in plain]),
+                                "failed": sum(r["status"] != 0 for r in plain)},
+            "throughput_ratio": plain_span / mixed_span,
+            "detector_rel_l2_vs_fp64": {"max": max(errs) if errs else None}})
+    out["served_scan"] = {"steps": args.scan_steps, "slots": args.scan_slots,
+                          "runs_per_slot": args.scan_group, "inlet": "vacuum (zero reference)",
+                          "rates": served}
     return out
 
 

@@ -469,11 +469,24 @@ typedef enum {
 
 /* The arguments of EBGaussFieldInitializer::initialize
  * (src/eb_initial_field.h:52-68) beyond the grid and the particles. */
+/* How the potential is solved.  CG: conjugate gradients, as
+ * EBGaussFieldInitializer (src/eb_initial_field.cpp:829-1095).  MODAL: a
+ * direct solve of the same discrete operator on the same Dirichlet box by
+ * transverse sine modes and one tridiagonal system along z per mode, the
+ * method of the blocked Cowan reference (src/blocked_cowan_reference.h:59-130,
+ * whose own check holds it to the CG initializer, verification/
+ * blocked_cowan_reference_checks.cpp:61-130); relative_tolerance and
+ * maximum_iterations are then unused and iterations is reported as 0. */
+typedef enum {
+  APRL_SELF_FIELD_SOLVER_CG = 0,
+  APRL_SELF_FIELD_SOLVER_MODAL = 1
+} aprl_self_field_solver;
+
 typedef struct {
   int32_t model;                      /* aprl_self_field_model */
   int32_t include_transverse_cpml_particles;
   int32_t hold_transverse_until_activation;  /* mean beta_z from the held longitudinal velocity */
-  int32_t reserved;
+  int32_t solver;                     /* aprl_self_field_solver */
   double relative_tolerance;          /* CG stop: |r| <= tol |b| */
   double maximum_mean_transverse_beta;
   uint64_t maximum_iterations;

@@ -130,3 +130,32 @@ def test_oracle_rejects_the_relativistic_bunch_like_the_reference():
             solve(binding, w)
         messages.append(str(e.value).split(": ", 1)[1])
     assert len(set(messages)) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("energy", [5.11e6, 8.84e6])
+@pytest.mark.parametrize("model", MODELS)
+def test_gpu_modal_solve_matches_the_oracle_initializer(model, energy):
+    """The transverse-mode direct solve (solver="modal", the blocked Cowan
+    reference's method) on the same box gives the CG initializer's fields to
+    the CG's own tolerance (the reference holds its modal reference to the
+    initializer the same way, verification/blocked_cowan_reference_checks.cpp:61-130)."""
+    w = workloads.self_field_case(energy)
+    _, rg, fg = solve(native.load(), w, model=model, solver="modal")
+    _, ro, fo = solve(checkers.oracle(), w, model=model)
+    assert rg["iterations"] == 0
+    assert rg["relative_residual"] <= 1e-12
+    for a, b in zip(fg, fo):
+        assert checkers.max_relative(a, b) <= FIELD_BOUND
+    assert rg["total_charge"] == pytest.approx(ro["total_charge"], rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_modal_solve_with_cpml_sources_and_held_velocity():
+    w = workloads.self_field_case(8.84e6, margin_cells=-1)
+    opts = dict(include_transverse_cpml_particles=True, hold_transverse_until_activation=True)
+    _, rg, fg = solve(native.load(), w, solver="modal", **opts)
+    _, ro, fo = solve(checkers.oracle(), w, **opts)
+    assert rg["transverse_poisson_padding_cells"] == 2
+    for a, b in zip(fg, fo):
+        assert checkers.max_relative(a, b) <= FIELD_BOUND
