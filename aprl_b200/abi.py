@@ -316,3 +316,21 @@ class ScanResult(C.Structure):
                 ("finish_s", C.c_double),
                 ("stats", StepStats),
                 ("message", C.c_char * 256)]
+
+
+class Tuning(C.Structure):
+    """aprl_tuning: the autotuner's launch shapes for one grid extent."""
+    _fields_ = [("decided", C.c_int32),
+                ("cowan_planes_per_block", C.c_uint32),
+                ("preview_block", C.c_uint32 * 2),
+                ("orbit_block", C.c_uint32 * 2),
+                ("commit_block", C.c_uint32 * 2),
+                ("candidate_ms", (C.c_float * 4) * 4)]
+
+    def as_dict(self):
+        return {"decided": [bool(self.decided >> k & 1) for k in range(4)],
+                "cowan_planes_per_block": self.cowan_planes_per_block,
+                "preview_block": list(self.preview_block),
+                "orbit_block": list(self.orbit_block),
+                "commit_block": list(self.commit_block),
+                "candidate_ms": [list(row) for row in self.candidate_ms]}

@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -231,9 +232,19 @@ constexpr unsigned kTrialSlots = 3;
 // Steps between the cell sorts of the particle list (see do_commit).
 constexpr uint64_t kSortInterval = 4;
 
+// A launch of the autotuner's measurements, harvested after the next wait.
+struct TunePending {
+  int kernel;
+  int candidate;
+  cudaEvent_t start, stop;
+};
+
 struct aprl_run {
   aprl_run_config cfg{};
   std::string error;  // the message of this run's failure in aprl_runs_step
+  int device = 0;
+  int tune_choice[4] = {-1, -1, -1, -1};  // autotuner choices seen by this run
+  std::vector<TunePending> tune_pending;
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;   // device memory (device_pool of the run's device)
   void* pinned = nullptr;         // the page-locked block the h_* read-backs live in
@@ -589,6 +600,135 @@ aprl_status launch(aprl_run* r, unsigned id, K kernel, dim3 grid, dim3 block, Ar
     aprl_status s_ = (expr);         \
     if (s_ != APRL_OK) return s_;    \
   } while (0)
+
+// ---- autotuner -------------------------------------------------------------
+// The launch shapes of the grid kernels are chosen by measurement, per device
+// and grid extent: the Cowan magnetic kernel's z planes per block and the
+// thread-block shape of the preview, orbit-sum and commit kernels.  Every
+// candidate computes each node exactly as the others do (one thread per node,
+// or the same plane ring over a different split of z), so a choice changes
+// timing only, never a bit of a result.  While a grid extent has no choice
+// yet, the runs on it launch the candidates in turn -- each a real launch of
+// the step, timed with CUDA events and read after the step's own wait -- and
+// once every candidate has two samples the one with the smallest sample
+// becomes the choice for every later launch of every run of that extent in
+// the process.
+enum TunedKernel { kTuneCowan = 0, kTunePreview, kTuneOrbit, kTuneCommit, kTuneCount };
+constexpr int kTuneCandidates = 4;
+constexpr int kTuneSamples = 2;
+constexpr int kCowanChunks[kTuneCandidates] = {2, 4, 8, 16};
+const dim3 kGridBlocks[kTuneCandidates] = {dim3(32, 4), dim3(32, 8), dim3(64, 2), dim3(64, 4)};
+
+struct TuneKey {
+  int device, kernel;
+  uint64_t nx, ny, nz;
+  bool operator<(const TuneKey& o) const {
+    if (device != o.device) return device < o.device;
+    if (kernel != o.kernel) return kernel < o.kernel;
+    if (nx != o.nx) return nx < o.nx;
+    if (ny != o.ny) return ny < o.ny;
+    return nz < o.nz;
+  }
+};
+
+struct TuneEntry {
+  float best[kTuneCandidates] = {0.f, 0.f, 0.f, 0.f};
+  int samples[kTuneCandidates] = {0, 0, 0, 0};
+  int choice = -1;
+};
+
+std::mutex& tune_lock() {
+  static std::mutex m;
+  return m;
+}
+std::map<TuneKey, TuneEntry>& tune_table() {
+  static std::map<TuneKey, TuneEntry> t;
+  return t;
+}
+
+TuneKey tune_key(const aprl_run* r, int kernel) {
+  return TuneKey{r->device, kernel, r->cfg.nx, r->cfg.ny, r->cfg.nz};
+}
+
+// The candidate for this launch of `kernel`; *timed is set when the launch
+// is a measurement.
+int tune_pick(aprl_run* r, int kernel, bool* timed) {
+  *timed = false;
+  if (r->tune_choice[kernel] >= 0) return r->tune_choice[kernel];
+  std::lock_guard<std::mutex> lock(tune_lock());
+  TuneEntry& e = tune_table()[tune_key(r, kernel)];
+  if (e.choice >= 0) {
+    r->tune_choice[kernel] = e.choice;
+    return e.choice;
+  }
+  int pending[kTuneCandidates] = {0, 0, 0, 0};
+  for (const auto& p : r->tune_pending)
+    if (p.kernel == kernel) ++pending[p.candidate];
+  int pick = 0;
+  for (int c = 1; c < kTuneCandidates; ++c)
+    if (e.samples[c] + pending[c] < e.samples[pick] + pending[pick]) pick = c;
+  *timed = true;
+  return pick;
+}
+
+// Reads the measurements whose launches have completed.
+void tune_harvest(aprl_run* r) {
+  if (r->tune_pending.empty()) return;
+  std::vector<TunePending> still;
+  std::lock_guard<std::mutex> lock(tune_lock());
+  for (auto& p : r->tune_pending) {
+    if (cudaEventQuery(p.stop) != cudaSuccess) {
+      still.push_back(p);
+      continue;
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+      TuneEntry& e = tune_table()[tune_key(r, p.kernel)];
+      if (e.samples[p.candidate] == 0 || ms < e.best[p.candidate]) e.best[p.candidate] = ms;
+      ++e.samples[p.candidate];
+      if (e.choice < 0) {
+        bool complete = true;
+        int best = 0;
+        for (int c = 0; c < kTuneCandidates; ++c) {
+          complete = complete && e.samples[c] >= kTuneSamples;
+          if (e.best[c] < e.best[best]) best = c;
+        }
+        if (complete) e.choice = best;
+      }
+    }
+    r->event_pool.push_back(p.start);
+    r->event_pool.push_back(p.stop);
+  }
+  (void)cudaGetLastError();  // a not-ready query leaves no error behind
+  r->tune_pending.swap(still);
+}
+
+// A tuned launch: tune_begin picks the candidate (and starts a measurement
+// when the choice is still open); the caller launches with that candidate's
+// shape; tune_end closes the measurement.
+struct TuneLaunch {
+  int kernel = 0, candidate = 0;
+  bool timed = false;
+  cudaEvent_t start = nullptr, stop = nullptr;
+};
+
+aprl_status tune_begin(aprl_run* r, int kernel, TuneLaunch& t) {
+  t.kernel = kernel;
+  t.candidate = tune_pick(r, kernel, &t.timed);
+  if (t.timed) {
+    t.start = take_event(r);
+    t.stop = take_event(r);
+    CUDA_TRY(cudaEventRecord(t.start, r->stream));
+  }
+  return APRL_OK;
+}
+
+aprl_status tune_end(aprl_run* r, const TuneLaunch& t) {
+  if (!t.timed) return APRL_OK;
+  CUDA_TRY(cudaEventRecord(t.stop, r->stream));
+  r->tune_pending.push_back(TunePending{t.kernel, t.candidate, t.start, t.stop});
+  return APRL_OK;
+}
 
 // Device view of the grid in the run's field element type F.
 template <class F>
@@ -1272,13 +1412,15 @@ aprl_status advance_magnetic_t(aprl_run* r) {
   // about four blocks per SM.
   const dim3 cblock(kCowanTileX, kCowanTileY);
   const unsigned columns = blocks_for(c.nx + 1, kCowanTileX) * blocks_for(c.ny + 1, kCowanTileY);
+  (void)columns;
   const size_t planes = c.nz + 1;
-  const size_t target = 4 * 148;
-  ca.chunk = (int)std::min<size_t>(
-      kCowanChunk, std::max<size_t>(2, (planes * columns + target - 1) / target));
+  TuneLaunch tl;
+  TRY(tune_begin(r, kTuneCowan, tl));
+  ca.chunk = (int)std::min<size_t>(kCowanChunks[tl.candidate], planes);
   const dim3 cgrid(blocks_for(c.nx + 1, kCowanTileX), blocks_for(c.ny + 1, kCowanTileY),
                    blocks_for(planes, ca.chunk));
   TRY(launch(r, kCowanMagnetic, cowan_magnetic_kernel<F>, cgrid, cblock, ca));
+  TRY(tune_end(r, tl));
   r->stage = 1;
   return APRL_OK;
 }
@@ -1303,8 +1445,11 @@ aprl_status preview_electric_t(aprl_run* r) {
   for (int a = 0; a < 3; ++a) pa.orbit[a] = r->orbit_from_preview ? r->orbit[a] : nullptr;
   pa.orbit_float = r->fp32 ? 1 : 0;
   TRY(inlet_table(r, r->offset, r->step + 1, pa.inlet));
-  const dim3 block(32, 4);
+  TuneLaunch tl;
+  TRY(tune_begin(r, kTunePreview, tl));
+  const dim3 block = kGridBlocks[tl.candidate];
   TRY(launch(r, kElectricPreview, electric_preview_kernel<F>, grid3(c, block), block, pa));
+  TRY(tune_end(r, tl));
   if (r->fp32 && r->np) {  // B is final for the step: its binary32 copy for the gathers
     BShadowArgs sa{};
     size_t most = 0;
@@ -1511,8 +1656,20 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     }
     TRY(join_carriers());
     TRY(convert_current());
-    TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, oblock), oblock, g, orbit[0],
-               orbit[1], orbit[2], 1));
+    {
+      // Measured only in a step's first trial: a trial issued ahead may be
+      // skipped (its kernels return at once), which would time nothing.
+      TuneLaunch tl;
+      if (r->trials == 0) {
+        TRY(tune_begin(r, kTuneOrbit, tl));
+      } else {
+        tl.candidate = std::max(0, r->tune_choice[kTuneOrbit]);
+      }
+      const dim3 sblock = kGridBlocks[tl.candidate];
+      TRY(launch(r, kOrbitSum, orbit_sum_kernel<W>, grid3(c, sblock), sblock, g, orbit[0],
+                 orbit[1], orbit[2], 1));
+      TRY(tune_end(r, tl));
+    }
     ResidualArgs<F> ra{};
     ra.g = g;
     for (int a = 0; a < 3; ++a) {
@@ -1588,12 +1745,16 @@ aprl_status do_trial(aprl_run* r, double residual[4]) {
 aprl_status do_commit(aprl_run* r) {
   if (r->stage != 3) return fail(APRL_ERR_RUNTIME, "Commit requires a completed coupling trial");
   const aprl_run_config& c = r->cfg;
-  const dim3 block(32, 4);
   // E^{n+1} = E* - dt/eps0 J, in place where J is nonzero: nothing to do
   // when J is known to be zero.
-  if (!r->j_zero)
+  if (!r->j_zero) {
+    TuneLaunch tl;
+    TRY(tune_begin(r, kTuneCommit, tl));
+    const dim3 block = kGridBlocks[tl.candidate];
     TRY(launch(r, kElectricCommit, electric_commit_kernel<double>, grid3(c, block), block,
                make_grid<double>(r)));
+    TRY(tune_end(r, tl));
+  }
   r->cur = 1 - r->cur;
   // The counters of the converged trial (read back with its residual) give
   // every compaction size: no host round trip in the commit.
@@ -1895,6 +2056,7 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
     int device = -1;
     if (cudaGetDevice(&device) != cudaSuccess || !(r->pool = device_pool(device)))
       return cleanup(fail(APRL_ERR_CUDA, "no stream-ordered memory pool on this device"));
+    r->device = device;
   }
   const aprl_run_config& c = *config;
   r->fp32 = c.precision == APRL_PRECISION_FP32_MIXED;
@@ -2024,6 +2186,10 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   for (auto& t : r->pending) {
     cudaEventDestroy(t.start);
     cudaEventDestroy(t.stop);
+  }
+  for (auto& p : r->tune_pending) {
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
   }
   for (auto e : r->event_pool) cudaEventDestroy(e);
   for (int a = 0; a < 3; ++a) {
@@ -2523,6 +2689,7 @@ aprl_status step_finish(aprl_run* r) {
   double force = 0.0, work = 0.0;
   const unsigned ahead = trials_ahead(r);
   TRY(check_device(r));
+  tune_harvest(r);
   unsigned t = 0;
   // forceHistory / workHistory of the reference's failure message.
   std::vector<double> history;
@@ -2616,6 +2783,33 @@ aprl_status aprl_runs_step(aprl_run* const* runs, size_t count, uint32_t steps,
   }
   if (worst != APRL_OK) g_error = first_error;
   return worst;
+}
+
+aprl_status aprl_run_tuning(const aprl_run* r, aprl_tuning* out) {
+  if (!r || !out) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  std::memset(out, 0, sizeof *out);
+  std::lock_guard<std::mutex> lock(tune_lock());
+  for (int k = 0; k < kTuneCount; ++k) {
+    const auto it = tune_table().find(tune_key(r, k));
+    int choice = 0;
+    if (it != tune_table().end()) {
+      const TuneEntry& e = it->second;
+      for (int c = 0; c < kTuneCandidates; ++c) out->candidate_ms[k][c] = e.best[c];
+      if (e.choice >= 0) {
+        out->decided |= 1 << k;
+        choice = e.choice;
+      }
+    }
+    if (k == kTuneCowan) {
+      out->cowan_planes_per_block = (uint32_t)kCowanChunks[choice];
+    } else {
+      uint32_t* b = k == kTunePreview ? out->preview_block
+                                      : (k == kTuneOrbit ? out->orbit_block : out->commit_block);
+      b[0] = kGridBlocks[choice].x;
+      b[1] = kGridBlocks[choice].y;
+    }
+  }
+  return APRL_OK;
 }
 
 aprl_status aprl_run_get_stats(const aprl_run* r, aprl_step_stats* st) {

@@ -54,6 +54,7 @@ _SIGNATURES = {
     "run_shift": (C.c_int, [_H]),
     "run_step": (C.c_int, [_H, C.c_uint32]),
     "run_get_stats": (C.c_int, [_H, C.POINTER(abi.StepStats)]),
+    "run_tuning": (C.c_int, [_H, C.POINTER(abi.Tuning)]),
     "run_enable_energy_ledger": (C.c_int, [_H, C.c_int]),
     "run_energy_ledger": (C.c_int, [_H, C.POINTER(abi.EnergyLedger)]),
     "run_initialize_self_field": (C.c_int, [_H, C.POINTER(abi.SelfFieldConfig),
@@ -337,6 +338,11 @@ class Run:
 
     def step(self, steps=1):
         self.b("run_step", self.handle, steps)
+
+    def tuning(self):
+        t = abi.Tuning()
+        self.b("run_tuning", self.handle, C.byref(t))
+        return t.as_dict()
 
     def stats(self):
         s = abi.StepStats()

@@ -357,6 +357,23 @@ aprl_status aprl_runs_step(aprl_run* const* runs, size_t count, uint32_t steps,
                            aprl_status* statuses);
 
 aprl_status aprl_run_get_stats(const aprl_run* run, aprl_step_stats* stats);
+
+/* The autotuner's launch shapes for the run's grid extent (no counterpart in
+ * the reference).  The grid kernels' launch shapes -- the Cowan magnetic
+ * kernel's z planes per block (2, 4, 8, 16) and the thread blocks of the
+ * preview, orbit-sum and commit kernels (32x4, 32x8, 64x2, 64x4) -- are
+ * chosen per device and grid extent by timing each candidate twice on the
+ * first steps of the runs of that extent (real launches of those steps, with
+ * CUDA events); every candidate gives the same bits, so tuning changes no
+ * result.  Kernels in order: Cowan magnetic, preview, orbit sum, commit. */
+typedef struct {
+  int32_t decided;                    /* bit k: kernel k's shape is chosen */
+  uint32_t cowan_planes_per_block;    /* the choice, or the first candidate */
+  uint32_t preview_block[2], orbit_block[2], commit_block[2];
+  float candidate_ms[4][4];           /* smallest sample per kernel and candidate (0: none) */
+} aprl_tuning;
+
+aprl_status aprl_run_tuning(const aprl_run* run, aprl_tuning* out);
 aprl_status aprl_run_reset_iteration_stats(aprl_run* run);
 
 /* Gathered fields of the particles after the last trial: usedE/usedB of the

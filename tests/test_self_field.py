@@ -144,7 +144,7 @@ def test_gpu_modal_solve_matches_the_oracle_initializer(model, energy):
     _, rg, fg = solve(native.load(), w, model=model, solver="modal")
     _, ro, fo = solve(checkers.oracle(), w, model=model)
     assert rg["iterations"] == 0
-    assert rg["relative_residual"] <= 1e-12
+    assert rg["relative_residual"] <= 1e-11
     for a, b in zip(fg, fo):
         assert checkers.max_relative(a, b) <= FIELD_BOUND
     assert rg["total_charge"] == pytest.approx(ro["total_charge"], rel=1e-12)
