@@ -90,7 +90,7 @@ class RunConfig(C.Structure):
         ("inlet_charge_match", C.c_uint32),
         ("magnets", Magnet * MAX_MAGNETS),
         ("deterministic", C.c_uint32),
-        ("reserved_flags", C.c_uint32),
+        ("reference_surface_current", C.c_uint32),
     ]
 
     @classmethod

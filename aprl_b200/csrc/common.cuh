@@ -56,6 +56,7 @@ enum DeviceError : unsigned {
   kErrInletField = 21,        // non-finite charge-matched inlet field
   kErrFixedRange = 22,        // deterministic deposit: contribution beyond the fixed-point range
   kErrBounds = 23,            // bounds-checked build: an index outside its array
+  kErrSurfaceCurrent = 24,    // non-finite equivalent boundary current of the reference
   kErrCount
 };
 

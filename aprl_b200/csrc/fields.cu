@@ -548,4 +548,39 @@ template __global__ void orbit_sum_kernel<double>(GridT<double>, double*, double
 template __global__ void orbit_sum_kernel<float>(GridT<double>, float*, float*, float*, int);
 #undef APRL_FIELD_KERNELS
 
+// TransverseReferenceCurrent::prepare's values (src/transverse_reference_current.cpp:
+// 52-58): curl_z of the reference B at every target point and reference plane,
+// ((By(i,j,k) - By(i-1,j,k))/dx - (Bx(i,j,k) - Bx(i,j-1,k))/dy)/mu0.
+__global__ void surface_prepare_kernel(SurfaceArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.count * a.planes) return;
+  const long long k = n / a.count, p = n % a.count;
+  const size_t i = a.points[2 * p], j = a.points[2 * p + 1];
+  // native reference layouts: Bx (nx+1, ny, planes), By (nx, ny+1, planes)
+  const size_t bx0 = ((size_t)k * a.ny + j) * (a.nx + 1) + i;
+  const size_t bx1 = ((size_t)k * a.ny + j - 1) * (a.nx + 1) + i;
+  const size_t by0 = ((size_t)k * (a.ny + 1) + j) * a.nx + i;
+  const double v = ((a.by[by0] - a.by[by0 - 1]) / a.dx - (a.bx[bx0] - a.bx[bx1]) / a.dy) / kMu0;
+  if (!isfinite(v)) raise_error(a.status, kErrSurfaceCurrent, (unsigned long long)n);
+  a.table[n] = v;
+}
+
+// TransverseReferenceCurrent::apply (src/transverse_reference_current.cpp:104-118):
+// Jz(i, j, k) += the lerp of the prepared planes at offset + k - beta*step.
+__global__ void surface_add_kernel(SurfaceArgs a) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const DGrid& g = a.g;
+  if (trial_skipped(g) || n >= a.count * g.nz) return;
+  const int k = (int)(n / a.count);
+  const long long p = n % a.count;
+  const double z = static_cast<double>(a.offset + k) - a.beta * static_cast<double>(a.step);
+  const long long lo = (long long)floor(z);
+  const long long hi = lo + 1 < a.planes ? lo + 1 : a.planes - 1;
+  const double fraction = z - (double)lo;
+  const double low = a.table[lo * a.count + p], high = a.table[hi * a.count + p];
+  const double value = fraction == 0. ? low : (1. - fraction) * low + fraction * high;
+  const int i = (int)a.points[2 * p], j = (int)a.points[2 * p + 1];
+  g.j[2][j_index(g, 2, i, j, k)] += value;
+}
+
 }  // namespace aprl_gpu

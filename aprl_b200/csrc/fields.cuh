@@ -140,4 +140,21 @@ struct BShadowArgs {
 };
 __global__ void b_shadow_kernel(BShadowArgs a);
 
+// The reference's equivalent surface current (TransverseReferenceCurrent).
+struct SurfaceArgs {
+  const unsigned* points;   // (i, j) per target point
+  double* table;            // [reference plane][point]
+  long long count, planes;
+  const double *bx, *by;    // reference B tables (native layout), for the preparation
+  int nx, ny;
+  double dx, dy;
+  DeviceStatus* status;
+  GridT<double> g;          // J of the trial, for the addition
+  long long offset;
+  unsigned long long step;  // step + 1 of the trial
+  double beta;
+};
+__global__ void surface_prepare_kernel(SurfaceArgs a);
+__global__ void surface_add_kernel(SurfaceArgs a);
+
 }  // namespace aprl_gpu

@@ -63,7 +63,7 @@ enum Kernel : unsigned {
   kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfUpdate,
   kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
   kInletHalo, kInletCharge, kInletComplete, kRadixCount, kPermuteParticles,
-  kCurrentConvert, kFixedConvert, kChordDeposit, kSfModal, kKernelCount
+  kCurrentConvert, kFixedConvert, kChordDeposit, kSfModal, kSurfaceCurrent, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -77,7 +77,7 @@ const char* kKernelNames[kKernelCount] = {
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
   "sf_update", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
   "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete",
-  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit", "sf_modal"};
+  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit", "sf_modal", "surface_current"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -107,6 +107,7 @@ const char* device_error_text(unsigned code) {
     case kErrInletField: return "Nonfinite charge-matched inlet field";
     case kErrFixedRange:
       return "Deposit contribution beyond the deterministic fixed-point range";
+    case kErrSurfaceCurrent: return "Nonfinite equivalent boundary current";
     case kErrBounds:
       return "Array index outside its array (bounds-checked build)";
   }
@@ -326,6 +327,12 @@ struct aprl_run {
   double jq_scale = 1.0;
   double max_abs_charge = 0.0;
   unsigned long long* inlet_rho_pairs = nullptr;
+  // the reference's equivalent surface current: target points (i, j) and
+  // curl_z(B_ref)/mu0 per reference plane and point
+  unsigned* surface_points = nullptr;
+  double* surface_table = nullptr;
+  size_t surface_count = 0;
+  bool surface_ready = false;
   // residual block partials (defect, scale) and the finished-block ticket
   double* res_partial = nullptr;
   unsigned* res_ticket = nullptr;
@@ -1474,6 +1481,82 @@ aprl_status do_preview_electric(aprl_run* r) {
   return preview_electric_t<double>(r);
 }
 
+// TransverseReferenceCurrent (src/transverse_reference_current.cpp:19-28,
+// 46-63, 104-118): the target points of the physical region's transverse
+// faces in the reference's order, curl_z(B_ref)/mu0 at each for every
+// reference plane (prepared on the device from the reference tables when
+// first needed), and each trial Jz += the plane lerp at
+// offset + k - beta (step + 1) for every window plane k.
+aprl_status surface_current_prepare(aprl_run* r) {
+  if (r->surface_ready) return APRL_OK;
+  const aprl_run_config& c = r->cfg;
+  if (!c.cpml_cells_x || !c.cpml_cells_y)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Reference surface current requires transverse-only CPML");
+  if (!r->ref_set[3] || !r->ref_set[4])
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Missing moving-window inlet reference component");
+  const size_t x0 = c.cpml_cells_x, x1 = c.nx - c.cpml_cells_x;
+  const size_t y0 = c.cpml_cells_y, y1 = c.ny - c.cpml_cells_y;
+  std::vector<unsigned> points;
+  for (size_t i = x0; i <= x1; ++i) {
+    points.push_back((unsigned)i); points.push_back((unsigned)y0);
+    points.push_back((unsigned)i); points.push_back((unsigned)y1);
+  }
+  for (size_t j = y0 + 1; j < y1; ++j) {
+    points.push_back((unsigned)x0); points.push_back((unsigned)j);
+    points.push_back((unsigned)x1); points.push_back((unsigned)j);
+  }
+  const size_t count = points.size() / 2;
+  device_free(r, r->surface_points);
+  device_free(r, r->surface_table);
+  r->surface_points = nullptr;
+  r->surface_table = nullptr;
+  TRY(device_alloc(r, &r->surface_points, points.size()));
+  TRY(device_alloc(r, &r->surface_table, count * std::max<uint64_t>(1, c.reference_nz)));
+  CUDA_TRY(run_copy(r, r->surface_points, points.data(), points.size() * sizeof(unsigned),
+                    cudaMemcpyHostToDevice));
+  SurfaceArgs a{};
+  a.points = r->surface_points;
+  a.table = r->surface_table;
+  a.count = (long long)count;
+  a.planes = (long long)c.reference_nz;
+  a.bx = r->ref[3];
+  a.by = r->ref[4];
+  a.nx = (int)c.nx;
+  a.ny = (int)c.ny;
+  a.dx = c.dx;
+  a.dy = c.dy;
+  a.status = r->d_status;
+  TRY(launch(r, kSurfaceCurrent, surface_prepare_kernel,
+             dim3(blocks_for(count * c.reference_nz, 256)), dim3(256), a));
+  TRY(check_device(r));
+  r->surface_count = count;
+  r->surface_ready = true;
+  return APRL_OK;
+}
+
+aprl_status surface_current_add(aprl_run* r, const GridT<double>& g) {
+  TRY(surface_current_prepare(r));
+  const aprl_run_config& c = r->cfg;
+  // The reference's range check (src/transverse_reference_current.cpp:109-110),
+  // for the first and last window planes (z grows with k).
+  const double step = static_cast<double>(r->step + 1);
+  const double z0 = static_cast<double>(r->offset) - c.translation_beta * step;
+  const double z1 = static_cast<double>(r->offset + (int64_t)c.nz - 1) - c.translation_beta * step;
+  if (!std::isfinite(z0) || z0 < 0. || z1 > static_cast<double>(c.reference_nz) - 1.)
+    return fail(APRL_ERR_OUT_OF_RANGE, "Reference surface-current query outside domain");
+  SurfaceArgs a{};
+  a.points = r->surface_points;
+  a.table = r->surface_table;
+  a.count = (long long)r->surface_count;
+  a.planes = (long long)c.reference_nz;
+  a.offset = r->offset;
+  a.step = r->step + 1;
+  a.beta = c.translation_beta;
+  a.g = g;
+  return launch(r, kSurfaceCurrent, surface_add_kernel,
+                dim3(blocks_for(r->surface_count * c.nz, 256)), dim3(256), a);
+}
+
 // One coupling trial; W is the arithmetic of the gathers.
 template <class W>
 aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
@@ -1506,13 +1589,19 @@ aprl_status trial_enqueue_t(aprl_run* r, int slot, bool ahead) {
     TRY(launch(r, kTrialClear, trial_clear_kernel, dim3(blocks), dim3(256), g, r->d_counters,
                r->d_sums, clear_current));
   }
-  r->j_zero = !deposits;
-  bool converted = !convert;
+  const bool surface = c.reference_surface_current != 0;
+  r->j_zero = !deposits && !surface;
+  // J complete for the trial: the fixed-point pairs converted (deterministic
+  // mode), then the reference's equivalent surface current added.
+  bool converted = false;
   auto convert_current = [&]() -> aprl_status {
     if (converted) return APRL_OK;
     converted = true;
-    return launch(r, kCurrentConvert, current_convert_kernel, dim3(grid_blocks), dim3(256), g,
-                  1.0 / r->jq_scale);
+    if (convert)
+      TRY(launch(r, kCurrentConvert, current_convert_kernel, dim3(grid_blocks), dim3(256), g,
+                 1.0 / r->jq_scale));
+    if (surface) TRY(surface_current_add(r, g));
+    return APRL_OK;
   };
   const DRegion region = make_region(r);
   // Each particle kernel is built per shape: 0 linear-binomial3, else quintic.
@@ -2229,6 +2318,8 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   device_free(r, r->chunk_offset);
   device_free(r, r->res_partial);
   device_free(r, r->res_ticket);
+  device_free(r, r->surface_points);
+  device_free(r, r->surface_table);
   for (int a = 0; a < 3; ++a) device_free(r, r->jq[a]);
   device_free(r, r->inlet_rho_pairs);
   free_carriers(r, r->born);
@@ -2276,6 +2367,7 @@ aprl_status aprl_run_set_reference(aprl_run* r, unsigned a, const double* host, 
   else
     CUDA_TRY(run_fill(r, r->ref[a], 0, n * 8));
   r->ref_set[a] = true;
+  if (a == 3 || a == 4) r->surface_ready = false;  // prepared again from the new table
   return APRL_OK;
 }
 
@@ -2293,6 +2385,7 @@ aprl_status aprl_run_set_reference_planes(aprl_run* r, unsigned a, uint64_t firs
     return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
   CUDA_TRY(cudaMemcpyAsync(r->ref[a] + first * plane, host, planes * plane * 8,
                            cudaMemcpyHostToDevice, r->stream));
+  if (a == 3 || a == 4) r->surface_ready = false;
   return APRL_OK;
 }
 
@@ -3484,6 +3577,7 @@ aprl_status aprl_run_prepare_reference(aprl_run* r, size_t n, const double* x, c
     }
     r->ref_set[a] = true;
   }
+  r->surface_ready = false;
   if (s == APRL_OK && cudaStreamSynchronize(r->stream) != cudaSuccess)
     s = fail(APRL_ERR_CUDA, "cudaStreamSynchronize failed");
   aprl_run_destroy(t);

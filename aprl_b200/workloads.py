@@ -123,6 +123,18 @@ def with_determinism(cfg, deterministic=True):
     return out
 
 
+def with_reference_surface_current(w):
+    """`w` with the reference's equivalent surface current on: the prepared
+    reference then has to cover the whole window over the run (the current
+    is sampled at every window plane), so its table is extended to
+    initial_offset + nz + 2 planes and drawn again."""
+    cfg = abi.RunConfig.from_buffer_copy(bytes(w.config))
+    cfg.reference_surface_current = 1
+    cfg.reference_nz = max(cfg.reference_nz, cfg.initial_offset + cfg.nz + 2)
+    return Workload(w.name + "-surface-current", cfg, w.particles, synthetic_reference(cfg),
+                    w.fields, steps=w.steps, description=dict(w.description))
+
+
 def make_config(nx, ny, nz, dx, dy, dz, cpml_cells, boost_gamma, shape,
                 steps, substeps=1, magnets=(), right_margin=None,
                 translation_beta=1.0, release_cells=6):

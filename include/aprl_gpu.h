@@ -155,7 +155,17 @@ typedef struct {
    * are deterministic in both modes.  Costs a second L2 reduction per
    * contribution and one grid pass per trial. */
   uint32_t deterministic;
-  uint32_t reserved_flags;        /* 0 */
+  /* mesh.moving_window.reference_surface_current (src/config.cpp:1150; off
+   * by default; transverse-only CPML): the prescribed equivalent surface
+   * current of the inlet reference (TransverseReferenceCurrent,
+   * src/transverse_reference_current.h:12-28).  At the points of the
+   * physical region's four transverse faces, Jz += curl_z(B_ref)/mu0 of the
+   * reference planes lerped to the step (weights as the inlet lerp), after
+   * every fixed-point trial's deposit, so it is in every trial's candidate
+   * field and in the commit (src/simulation_source_coupling.cpp:44,
+   * src/simulation.cpp:548-561).  Outgoing perturbations keep the plain
+   * Maxwell/CPML update. */
+  uint32_t reference_surface_current;
 } aprl_run_config;
 
 /* Per-step results of the coupled step (SourceCoupling log row,

@@ -33,7 +33,7 @@ REFERENCE_UNITS = [
     "eb_field", "eb_cpml", "eb_deposition", "eb_particles", "boostframe",
     "eb_sources", "compute_threads", "source_coupling",
     "moving_window_fields", "particle_boundary", "pending_particle_queue",
-    "eb_initial_field",
+    "eb_initial_field", "transverse_reference_current",
 ]
 
 

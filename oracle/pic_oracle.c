@@ -112,8 +112,19 @@ typedef struct {
   double value;
 } preview_delta_t;
 
+/* The equivalent surface current of the reference (TransverseReferenceCurrent):
+ * target points and their prepared values per reference plane. */
+typedef struct {
+  size_t count;
+  size_t* i;
+  size_t* j;
+  double* table; /* [reference plane][point] */
+  int ready;
+} surface_current_t;
+
 struct oracle_run {
   aprl_run_config cfg;
+  surface_current_t surface;
   double alpha[3], beta[3], delta_xy, delta_yz, delta_zx;
   comp_t f[9];    /* Ex Ey Ez Bx By Bz Jx Jy Jz */
   comp_t old[3];  /* ConservativeSourceCoupling::Impl::old */
@@ -905,6 +916,9 @@ aprl_status oracle_run_create(const aprl_run_config* config, oracle_run** out) {
 
 aprl_status oracle_run_destroy(oracle_run* r) {
   if (!r) return APRL_OK;
+  free(r->surface.i);
+  free(r->surface.j);
+  free(r->surface.table);
   for (int a = 0; a < 9; ++a) free(r->f[a].v);
   for (int a = 0; a < 3; ++a) {
     free(r->old[a].v);
@@ -936,6 +950,12 @@ aprl_status oracle_run_set_reference(oracle_run* r, unsigned a, const double* ho
   r->ref[a].v = (double*)calloc(n ? n : 1, sizeof(double));
   if (host) memcpy(r->ref[a].v, host, n * sizeof(double)); /* NULL: the zero inlet */
   r->ref_set[a] = 1;
+  if (a == 3 || a == 4) { /* the surface current is prepared from Bx, By again */
+    free(r->surface.i);
+    free(r->surface.j);
+    free(r->surface.table);
+    memset(&r->surface, 0, sizeof r->surface);
+  }
   return APRL_OK;
 }
 
@@ -2774,6 +2794,74 @@ static aprl_status local_residual(oracle_run* r, double out[4]) {
   return APRL_OK;
 }
 
+/* TransverseReferenceCurrent at one rank: the target points of points()
+ * (src/transverse_reference_current.cpp:19-28) in the same order, the
+ * prepared value curl_z(B_ref)/mu0 per reference plane (prepare, :46-63)
+ * and, each trial, Jz += the plane lerp at offset + k - beta*(step+1)
+ * (apply, :104-118). */
+static aprl_status surface_prepare(oracle_run* r) {
+  surface_current_t* s = &r->surface;
+  if (s->ready) return APRL_OK;
+  const aprl_run_config* g = &r->cfg;
+  if (!g->cpml_cells_x || !g->cpml_cells_y)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Reference surface current requires transverse-only CPML");
+  if (!r->ref_set[3] || !r->ref_set[4])
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Missing moving-window inlet reference component");
+  const size_t x0 = g->cpml_cells_x, x1 = g->nx - g->cpml_cells_x;
+  const size_t y0 = g->cpml_cells_y, y1 = g->ny - g->cpml_cells_y;
+  const size_t count = 2 * (x1 - x0 + 1) + 2 * (y1 - y0 - 1);
+  s->i = (size_t*)malloc(count * sizeof(size_t));
+  s->j = (size_t*)malloc(count * sizeof(size_t));
+  const size_t planes = g->reference_nz;
+  s->table = (double*)malloc((planes ? planes : 1) * count * sizeof(double));
+  size_t p = 0;
+  for (size_t i = x0; i <= x1; ++i) {
+    s->i[p] = i; s->j[p] = y0; ++p;
+    s->i[p] = i; s->j[p] = y1; ++p;
+  }
+  for (size_t j = y0 + 1; j < y1; ++j) {
+    s->i[p] = x0; s->j[p] = j; ++p;
+    s->i[p] = x1; s->j[p] = j; ++p;
+  }
+  s->count = count;
+  const comp_t* bx = &r->ref[3];
+  const comp_t* by = &r->ref[4];
+  for (size_t k = 0; k < planes; ++k)
+    for (size_t q = 0; q < count; ++q) {
+      const size_t i = s->i[q], j = s->j[q];
+      const double v = ((AT(by, i, j, k) - AT(by, i - 1, j, k)) / g->dx -
+                        (AT(bx, i, j, k) - AT(bx, i, j - 1, k)) / g->dy) / SI_MU0;
+      if (!isfinite(v)) return fail(APRL_ERR_RUNTIME, "Nonfinite equivalent boundary current");
+      s->table[k * count + q] = v;
+    }
+  s->ready = 1;
+  return APRL_OK;
+}
+
+static aprl_status surface_apply(oracle_run* r) {
+  if (!r->cfg.reference_surface_current) return APRL_OK;
+  aprl_status st = surface_prepare(r);
+  if (st != APRL_OK) return st;
+  surface_current_t* s = &r->surface;
+  const size_t planes = r->cfg.reference_nz;
+  comp_t* jz = &r->f[8];
+  for (size_t k = 0; k < r->cfg.nz; ++k) {
+    const double z = (double)r->offset + (double)k - r->cfg.translation_beta * (double)(r->step + 1);
+    if (!isfinite(z) || z < 0. || z > (double)planes - 1.)
+      return fail(APRL_ERR_OUT_OF_RANGE, "Reference surface-current query outside domain");
+    const size_t lo = (size_t)floor(z);
+    const size_t hi = lo + 1 < planes ? lo + 1 : planes - 1;
+    const double fraction = z - (double)lo;
+    const double* a = s->table + lo * s->count;
+    const double* b = s->table + hi * s->count;
+    for (size_t q = 0; q < s->count; ++q) {
+      const double value = fraction == 0. ? a[q] : (1. - fraction) * a[q] + fraction * b[q];
+      AT(jz, s->i[q], s->j[q], k) += value;
+    }
+  }
+  return APRL_OK;
+}
+
 aprl_status oracle_run_coupling_trial(oracle_run* r, double residual[4]) {
   if (r->stage != 2 && r->stage != 3)
     return fail(APRL_ERR_RUNTIME, "Coupling trial requires a previewed electric field");
@@ -2784,6 +2872,8 @@ aprl_status oracle_run_coupling_trial(oracle_run* r, double residual[4]) {
   for (size_t n = 0; n < r->nslot; ++n) r->slot[n].seen = 0; /* beginTrial */
   r->replay = 0;
   aprl_status s = push_deposit(r);
+  if (s != APRL_OK) return s;
+  s = surface_apply(r);
   if (s != APRL_OK) return s;
   apply_current_source(r, -1.);
   s = local_residual(r, residual);
@@ -2808,6 +2898,9 @@ aprl_status oracle_run_commit_electric(oracle_run* r) {
   r->replay = 1;
   aprl_status s = push_deposit(r);
   r->replay = 0;
+  if (s != APRL_OK) return s;
+  /* applyMovingTransverseReferenceCurrent before the commit (src/simulation.cpp:548-549). */
+  s = surface_apply(r);
   if (s != APRL_OK) return s;
   for (int a = 0; a < 3; ++a) {
     double* t = r->f[a].v;

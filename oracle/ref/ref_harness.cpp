@@ -45,6 +45,8 @@
 #include "pending_particle_queue.h"
 #include "source_coupling.h"
 #include "source_coupling_math.h"
+#include "blocked_cowan_reference.h"
+#include "transverse_reference_current.h"
 
 using namespace aprl;
 typedef FieldVector<Double> Vec;
@@ -72,8 +74,21 @@ aprl_status guarded(F f) {
 }
 }  // namespace
 
+// The blocked modal reference needs FFTW, which this image lacks; the
+// harness writes the surface-current file itself (below), so the only caller
+// of this member, TransverseReferenceCurrent::prepare, is never reached.
+namespace aprl { namespace verification {
+Double BlockedCowanReference::field(unsigned, std::size_t, std::size_t, std::size_t) {
+  throw std::runtime_error("BlockedCowanReference is not built here");
+}
+}}  // namespace aprl::verification
+
 struct ref_run {
   aprl_run_config cfg;
+  // The reference's own TransverseReferenceCurrent over a file the harness
+  // prepared from the supplied reference tables.
+  std::unique_ptr<aprl::TransverseReferenceCurrent> surface;
+  std::string surfaceFile;
   EBGridGeometry geometry;
   EBCPMLParameters cpml;
   std::unique_ptr<EBFieldGrid> fields;
@@ -464,6 +479,7 @@ aprl_status ref_run_create(const aprl_run_config* config, ref_run** out) {
 
 aprl_status ref_run_destroy(ref_run* r) {
   if (r) {
+    if (!r->surfaceFile.empty()) ::unlink(r->surfaceFile.c_str());
     const std::string dir = r->directory;
     delete r;
     if (!dir.empty()) {
@@ -658,6 +674,79 @@ aprl_status ref_run_preview_electric(ref_run* r) {
   });
 }
 
+// TransverseReferenceCurrent::prepare's file (src/transverse_reference_current.cpp:
+// 17-18, 29-33, 46-63) written from the in-memory reference tables: the
+// header, curl_z(B_ref)/mu0 at the points() targets for every reference
+// plane, and the completion marker; then the reference's class opens it.
+void prepare_surface(ref_run& r) {
+  if (r.surface) return;
+  const aprl_run_config& c = r.cfg;
+  const std::size_t gx = c.cpml_cells_x, gy = c.cpml_cells_y;
+  const std::size_t x0 = gx, x1 = c.nx - gx, y0 = gy, y1 = c.ny - gy;
+  std::vector<std::pair<std::size_t, std::size_t>> target;
+  for (std::size_t i = x0; i <= x1; ++i) {
+    target.push_back({i, y0});
+    target.push_back({i, y1});
+  }
+  for (std::size_t j = y0 + 1; j < y1; ++j) {
+    target.push_back({x0, j});
+    target.push_back({x1, j});
+  }
+  struct Header {
+    std::uint64_t tag, version, nx, ny, nz, gx, gy, count;
+    double dx, dy, dz, dt, beta;
+  };
+  const bool binomial3 = c.shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+  const Header h{0x4150524c53555246ULL, binomial3 ? 2ULL : 1ULL, c.nx, c.ny, c.reference_nz,
+                 gx, gy, target.size(), c.dx, c.dy, c.dz, c.dt, 0.0};
+  char name[] = "/tmp/aprl-surface-XXXXXX";
+  const int fd = ::mkstemp(name);
+  if (fd < 0) throw std::runtime_error("Cannot create reference surface-current file");
+  std::vector<double> values(target.size());
+  const auto& bx = r.reference[3];
+  const auto& by = r.reference[4];
+  const auto* sx = r.referenceShape[3];
+  const auto* sy = r.referenceShape[4];
+  bool ok = ::write(fd, &h, sizeof h) == (ssize_t)sizeof h;
+  for (std::size_t k = 0; ok && k < c.reference_nz; ++k) {
+    for (std::size_t p = 0; p < target.size(); ++p) {
+      const std::size_t i = target[p].first, j = target[p].second;
+      const double dby = by.at((k * sy[1] + j) * sy[0] + i) - by.at((k * sy[1] + j) * sy[0] + i - 1);
+      const double dbx = bx.at((k * sx[1] + j) * sx[0] + i) - bx.at((k * sx[1] + j - 1) * sx[0] + i);
+      values[p] = (dby / c.dx - dbx / c.dy) / SI::mu0;
+      if (!std::isfinite(values[p])) {
+        ::close(fd);
+        ::unlink(name);
+        throw std::runtime_error("Nonfinite equivalent boundary current");
+      }
+    }
+    const ssize_t bytes = (ssize_t)(values.size() * sizeof(double));
+    ok = ::write(fd, values.data(), values.size() * sizeof(double)) == bytes;
+  }
+  const std::uint64_t complete = 0x434f4d504c455445ULL;
+  ok = ok && ::write(fd, &complete, sizeof complete) == (ssize_t)sizeof complete;
+  ::close(fd);
+  if (!ok) {
+    ::unlink(name);
+    throw std::runtime_error("Cannot write reference surface current");
+  }
+  r.surfaceFile = name;
+  const EBGridGeometry g(c.nx, c.ny, c.reference_nz, c.dx, c.dy, c.dz, c.dt,
+                         EBMaxwellSolver::CowanZ);
+  const std::size_t guards[3] = {gx, gy, 0};
+  r.surface.reset(new aprl::TransverseReferenceCurrent(name, g, guards, 0.0, "", binomial3));
+}
+
+void apply_surface(ref_run& r) {
+  if (!r.cfg.reference_surface_current) return;
+  prepare_surface(r);
+  r.surface->apply(*r.fields, r.offset, r.step, r.cfg.translation_beta, false);
+}
+
+void finish_surface(ref_run& r) {
+  if (r.cfg.reference_surface_current && r.surface) r.surface->finish(*r.fields);
+}
+
 aprl_status ref_run_coupling_trial(ref_run* r, double residual[4]) {
   return guarded([&] {
     if (r->stage != 2 && r->stage != 3) throw std::logic_error("Coupling trial requires a previewed electric field");
@@ -668,6 +757,9 @@ aprl_status ref_run_coupling_trial(ref_run* r, double residual[4]) {
     r->coupling->exchangeCandidate();
     pushDepositAndMigrate(*r);
     r->coupling->completeCurrent();
+    // src/simulation_source_coupling.cpp:44
+    apply_surface(*r);
+    finish_surface(*r);
     r->coupling->applyCurrentSource(-1.);
     r->coupling->exchangeCandidate();
     const auto res = r->coupling->localResidual();
@@ -689,10 +781,14 @@ aprl_status ref_run_commit_electric(ref_run* r) {
     r->coupling->completeCurrent();
     r->coupling->setReplay(false);
     r->coupling->finish(r->step + 1, r->lastIterations, r->lastForce, r->lastWork);
+    // applyMovingTransverseReferenceCurrent before the commit, finish after
+    // (src/simulation.cpp:548-549, 560-561)
+    apply_surface(*r);
     r->coupling->swapElectric();
     r->window->undoPreviewElectricBoundary(*r->fields);
     r->coupling->applyCurrentSource(-1.);
     r->window->commitPreparedElectricBoundary(*r->fields);
+    finish_surface(*r);
     r->stage = 4;
   });
 }
