@@ -495,110 +495,6 @@ struct ElectricVisitor {
         }
     }
   }
-
-  // Two pieces [f0, l0] and [f1, l1] of one chord in z-neighbouring cells of
-  // one (i, j) column, gathered over the union of their stencils: each node's
-  // two weights are added first and the node is read once (82 reads instead
-  // of 128).  The weights are binomialXZSegment's; only the order of the
-  // additions changes.  Returns false (and gathers nothing) when the pieces
-  // are not such a pair or the union leaves the interior.
-  __device__ __forceinline__ bool f3_pair(const GridT<F>& G, const double s[3],
-                                          const double d[3], double f0, double l0, double f1,
-                                          double l1) {
-    long long cell[2][3];
-    double mid[2][3];
-    const double first[2] = {f0, f1}, last[2] = {l0, l1};
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const double m = (first[q] + last[q]) * 0.5;
-      for (int a = 0; a < 3; ++a) {
-        mid[q][a] = s[a] + m * d[a];
-        cell[q][a] = (long long)floor(mid[q][a]);
-      }
-      if (cell[q][0] == (long long)G.nx) --cell[q][0];
-      if (cell[q][1] == (long long)G.ny) --cell[q][1];
-    }
-    if (cell[0][0] != cell[1][0] || cell[0][1] != cell[1][1]) return false;
-    int lo;
-    if (cell[1][2] == cell[0][2] + 1) lo = 0;
-    else if (cell[0][2] == cell[1][2] + 1) lo = 1;
-    else return false;
-    const int up = 1 - lo;
-    const long long i = cell[lo][0], j = cell[lo][1], k = cell[lo][2];
-    if (!(i >= 2 && i <= G.nx - 3 && j >= 1 && j <= G.ny - 2 && k >= 2 && k <= G.nz - 4))
-      return false;
-    const W edge[3] = {W(0.25), W(0.5), W(0.25)};
-    const W slope[4] = {W(-0.25), W(-0.25), W(0.25), W(0.25)};
-    const W sy[2] = {W(-1.), W(1.)};
-    W wx[2][4], wz[2][4], wy[2][2], width[2], xy[2], xz[2], yz[2];
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int q = t == 0 ? lo : up;
-      width[t] = W(last[q] - first[q]);
-      node_weights(W(mid[q][0] - i), wx[t]);
-      node_weights(W(mid[q][2] - cell[q][2]), wz[t]);
-      wy[t][0] = W(1.) - W(mid[q][1] - j);
-      wy[t][1] = W(mid[q][1] - j);
-      const W curvature = width[t] * width[t] / W(12.);
-      xy[t] = curvature * W(d[0]) * W(d[1]);
-      xz[t] = curvature * W(d[0]) * W(d[2]);
-      yz[t] = curvature * W(d[1]) * W(d[2]);
-    }
-    const int I = (int)i, J = (int)j, K = (int)k;
-    // Ex: z levels K-1 .. K+3 (the lower piece's c = zz, the upper's zz - 1)
-    {
-      const int nxc = G.nx, nyc = G.ny + 1, nzc = G.nz + 1;
-#pragma unroll
-      for (int zz = 0; zz < 5; ++zz) {
-        const size_t plane = (size_t)ring(K - 1 + zz, G.zb_e[0], nzc) * nyc;
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          W weight = W(0.);
-          if (zz < 4) weight += width[0] * (wy[0][b] * wz[0][zz] + yz[0] * sy[b] * slope[zz]);
-          if (zz >= 1)
-            weight += width[1] * (wy[1][b] * wz[1][zz - 1] + yz[1] * sy[b] * slope[zz - 1]);
-          const size_t n0 = (plane + J + b) * nxc + (I - 1);
-#pragma unroll
-          for (int a = 0; a < 3; ++a) r[0] += term(0, n0 + a, 0, weight * edge[a]);
-        }
-      }
-    }
-    // Ey: z levels K-1 .. K+3
-    {
-      const int nxc = G.nx + 1, nyc = G.ny, nzc = G.nz + 1;
-#pragma unroll
-      for (int zz = 0; zz < 5; ++zz) {
-        const size_t n0 = ((size_t)ring(K - 1 + zz, G.zb_e[1], nzc) * nyc + J) * nxc + (I - 1);
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          W weight = W(0.);
-          if (zz < 4) weight += width[0] * (wx[0][a] * wz[0][zz] + xz[0] * slope[a] * slope[zz]);
-          if (zz >= 1)
-            weight += width[1] * (wx[1][a] * wz[1][zz - 1] + xz[1] * slope[a] * slope[zz - 1]);
-          r[1] += term(1, n0 + a, 0, weight);
-        }
-      }
-    }
-    // Ez: z levels K-1 .. K+2 (each piece smoothed over its own three)
-    {
-      const int nxc = G.nx + 1, nyc = G.ny + 1, nzc = G.nz;
-#pragma unroll
-      for (int b = 0; b < 2; ++b)
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const W wl = width[0] * (wx[0][a] * wy[0][b] + xy[0] * slope[a] * sy[b]);
-          const W wu = width[1] * (wx[1][a] * wy[1][b] + xy[1] * slope[a] * sy[b]);
-          const W level[4] = {wl * edge[0], wl * edge[1] + wu * edge[0],
-                              wl * edge[2] + wu * edge[1], wu * edge[2]};
-#pragma unroll
-          for (int zz = 0; zz < 4; ++zz) {
-            const size_t plane = (size_t)ring(K - 1 + zz, G.zb_e[2], nzc) * nyc;
-            r[2] += term(2, (plane + J + b) * nxc + (I - 1 + a), 0, level[zz]);
-          }
-        }
-    }
-    return true;
-  }
 };
 
 template <class W, class F>
@@ -695,11 +591,7 @@ __device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const Ptr3
 }
 
 // Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
-// Pair: a linear-binomial3 chord of exactly two pieces in z-neighbouring
-// cells is gathered over the union of their stencils (ElectricVisitor::
-// f3_pair); the residual's re-gather uses it, the first trial's guess gather
-// keeps the reference's per-piece order.
-template <int S, bool Pair = false, class W, class F>
+template <int S, class W, class F>
 __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g,
                                                     const double a[3], const double b[3],
                                                     const Ptr3<W>& orbit, double out[3]) {
@@ -707,17 +599,7 @@ __device__ __forceinline__ unsigned gather_electric(const GridT<F>& g,
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
   ElectricVisitor<W, F> v{&g, orbit, {W(0.), W(0.), W(0.)}};
-  bool done = false;
-  if constexpr (Pair && S == 0) {
-    const double h[3] = {g.dx, g.dy, g.dz};
-    CutWalker w;
-    if (w.init(path.begin, path.end, g.origin, h)) {
-      double f0, l0, f1, l1, fx, lx;
-      if (w.advance(f0, l0) && w.advance(f1, l1) && !w.advance(fx, lx))
-        done = v.f3_pair(g, w.x, w.v, f0, l0, f1, l1);
-    }
-  }
-  if (!done && shape_weights<S>(g, path.begin, path.end, v) < 0) return kErrCrossingBudget;
+  if (shape_weights<S>(g, path.begin, path.end, v) < 0) return kErrCrossingBudget;
   const double fraction = path.last - path.first;
   for (int d = 0; d < 3; ++d) out[d] = double(v.r[d]) * fraction;
   return kErrNone;
@@ -1850,7 +1732,7 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]),
                         static_cast<const W*>(a.bgather[1]),
                         static_cast<const W*>(a.bgather[2])}};
-    unsigned err = gather_electric<S, APRL_RESIDUAL_PAIR != 0>(a.g, first, last, orbit, ne);
+    unsigned err = gather_electric<S>(a.g, first, last, orbit, ne);
     if (!err) err = gather_magnetic<S>(a.g, first, last, bsrc, nb);
     if (err) {
       raise_error(a.status, err, (unsigned long long)n);

@@ -194,10 +194,6 @@ struct ChordArgs {
 #ifndef APRL_GATHER_MIN_BLOCKS
 #define APRL_GATHER_MIN_BLOCKS 6
 #endif
-// The residual's re-gather over a chord-pair union (ElectricVisitor::f3_pair).
-#ifndef APRL_RESIDUAL_PAIR
-#define APRL_RESIDUAL_PAIR 1
-#endif
 #ifndef APRL_CHORD_MIN_BLOCKS
 #define APRL_CHORD_MIN_BLOCKS 0
 #endif

@@ -198,8 +198,10 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
         return 9 * 8 * n_cells
     if kernel == "electric_commit":     # read E* and J, write E
         return 9 * 8 * n_cells
-    if kernel == "push_deposit":        # read x,u,q,m,nextE/B; write x1,u1,usedE/B,work,flags
-        return particles * (64 + 48 + 48 + 48 + 8 + 2)
+    if kernel == "push_deposit":        # read x,u,q,m,nextE/B; write x1,u1,usedE/B,work,flags,
+        return particles * (64 + 48 + 48 + 48 + 8 + 2 + 49)   # and the chord (b, e, mode)
+    if kernel == "chord_deposit":       # read the chord (b, e), q, mode; J updates are L2 reductions
+        return particles * (48 + 8 + 1)
     if kernel == "residual":            # read x0,x1,q,m,usedE/B,work; write nextE/B
         return particles * (48 + 16 + 48 + 8 + 48)
     if kernel == "guess_gather":        # read x,u,flags; write nextE/B
@@ -220,9 +222,10 @@ MEASURED_TRAFFIC = {"push_deposit": ("particle", 349.0),
                     "orbit_sum": ("launch", 788.7e6)}
 
 
-# L2 reduction sectors per particle of one push_deposit launch (ncu
-# lts__t_sectors_op_red of the 250k-particle dipole capture: 22.6 M).
-RED_SECTORS_PER_PARTICLE = 90.4
+# L2 reduction sectors per particle of one chord_deposit launch: ncu
+# lts__t_sectors_srcunit_tex_op_red on the dipole workload (the unmerged
+# one-reduction-per-visit deposit of the same chords took 90.4 at 250k).
+RED_SECTORS_PER_PARTICLE = {250_000: 45.5}
 
 
 PROBE_SOURCE = os.path.join(REPO, "bench_probe.cu")
@@ -455,23 +458,34 @@ def run_ours(args):
                     "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
                     "launches": count}
     atomic_roofline = None
-    if "push_deposit" in profile and world == 1:
-        ms, count = profile["push_deposit"]
+    if "chord_deposit" in profile and world == 1:
+        ms, count = profile["chord_deposit"]
         per_launch_ms = ms / max(count, 1)
-        sectors = RED_SECTORS_PER_PARTICLE * particle_steps / max(K, 1)
-        achieved_atomic = sectors / (per_launch_ms * 1e-3) / 1e9
-        peak_atomic = atomic_peak()
+        mean_particles = particle_steps / max(K, 1)
+        # sectors per particle measured nearest this particle count
+        key = min(RED_SECTORS_PER_PARTICLE, key=lambda n: abs(math.log(n / max(mean_particles, 1))))
+        per_particle = RED_SECTORS_PER_PARTICLE[key]
+        achieved_atomic = per_particle * mean_particles / (per_launch_ms * 1e-3) / 1e9
+        peak_atomic = atomic_peak(integer=bool(args.deterministic))
         atomic_roofline = {
-            "kernel": "push_deposit", "bound": "l2-fp64-atomics",
+            "kernel": "chord_deposit",
+            "bound": "l2-int64-atomics" if args.deterministic else "l2-fp64-atomics",
             "achieved": achieved_atomic, "peak": peak_atomic, "unit": "G reductions/s",
             "frac": achieved_atomic / peak_atomic if peak_atomic else None,
-            "peak_source": "measured here: one FP64 reduction per lane per 32-byte sector, "
+            "peak_source": "measured here: one reduction per lane per 32-byte sector, "
                            "neighbouring sectors, 16 MB window (bench_probe.cu)",
-            "reductions_per_particle": RED_SECTORS_PER_PARTICLE,
-            "note": "whole push_deposit launch time, push arithmetic included"}
-    kernels = {k: {"ms": v[0], "launches": v[1],
-                   "share": v[0] / max(sum(x[0] for x in profile.values()), 1e-12)}
-               for k, v in profile.items()}
+            "reductions_per_particle": per_particle,
+            "reductions_measured_at_particles": key,
+            "note": "whole chord_deposit launch time"}
+    total_ms = max(sum(x[0] for x in profile.values()), 1e-12)
+    kernels = {}
+    for k, v in profile.items():
+        entry = {"ms": v[0], "launches": v[1], "share": v[0] / total_ms}
+        algo = algorithmic_bytes(k, cfg, particle_steps / max(K, 1), stats["carriers"])
+        if algo and v[1]:
+            gbs = algo / (v[0] / v[1] * 1e-3) / 1e9
+            entry.update({"bytes_per_launch": algo, "achieved_gbs": gbs, "hbm_frac": gbs / peak})
+        kernels[k] = entry
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s",
         "n_gpus": world, "steps": K, "warmup": W,
