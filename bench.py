@@ -216,16 +216,19 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # one ncu capture of this workload's grid with 250k particles, cold L2: per
 # particle for the particle kernels, per launch for the grid passes.
-MEASURED_TRAFFIC = {"push_deposit": ("particle", 349.0),
-                    "residual": ("particle", 473.0),
+MEASURED_TRAFFIC = {"chord_deposit": ("particle", 229.0),
+                    "push_deposit": ("particle", 217.0),
+                    "residual": ("particle", 567.0),
+                    "guess_gather": ("particle", 454.0),
                     "cowan_magnetic": ("launch", 669.9e6),
-                    "orbit_sum": ("launch", 788.7e6)}
+                    "orbit_sum": ("launch", 792.0e6),
+                    "electric_preview": ("launch", 844.2e6)}
 
 
 # L2 reduction sectors per particle of one chord_deposit launch: ncu
 # lts__t_sectors_srcunit_tex_op_red on the dipole workload (the unmerged
 # one-reduction-per-visit deposit of the same chords took 90.4 at 250k).
-RED_SECTORS_PER_PARTICLE = {250_000: 45.5}
+RED_SECTORS_PER_PARTICLE = {250_000: 45.5, 1_000_000: 21.3}
 
 
 PROBE_SOURCE = os.path.join(REPO, "bench_probe.cu")
@@ -453,8 +456,9 @@ def run_ours(args):
                     "frac": (achieved / peak) if achieved else None,
                     "peak_source": peak_kind,
                     "traffic": measured_traffic(name, mean_particles),
-                    "traffic_source": "ncu DRAM bytes of the 250k-particle capture of this "
-                                      "grid, scaled per particle for particle kernels",
+                    "traffic_source": "ncu DRAM bytes of one-kernel captures of this grid "
+                                      "with 250k particles, scaled per particle for particle "
+                                      "kernels (profiles/dram_traffic_*)",
                     "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
                     "launches": count}
     atomic_roofline = None

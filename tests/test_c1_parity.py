@@ -91,3 +91,19 @@ def test_drift_full_size_matches_reference_for_20_steps():
             compare(gpu, ref, f"FP64 atomics, step {step}")
             compare(det, ref, f"fixed-point sum, step {step}")
     assert ref.stats()["step"] == STEPS and ref.stats()["particles"] > 0
+
+
+QUINTIC_STEPS = 10
+
+
+def test_drift_full_size_quintic_matches_reference_for_10_steps():
+    """The same configuration with the quintic-compensated shape (its 12-node
+    z stencils and four-point Gauss quadrature per cut piece), 10 steps."""
+    w = workloads.drift_c1(steps=QUINTIC_STEPS + 2, shape="quintic-compensated")
+    ref = checkers.run(reference_binding(), w)
+    gpu = native.Run(native.load(), w.config).load_workload(w)
+    for step in range(1, QUINTIC_STEPS + 1):
+        ref.step(1)
+        gpu.step(1)
+        if step in (1, 5, QUINTIC_STEPS):
+            compare(gpu, ref, f"quintic, step {step}")
