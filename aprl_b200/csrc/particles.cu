@@ -213,21 +213,36 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
 // longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with
 // smoothX = (shape == linear-binomial3).  Returns the segment count, or -1
 // when the chord exceeds the 64-cut crossing budget.
+// lattice_shape_weights takes the chord in lattice units: start
+// x = (begin - origin)/h and extent v = (end - begin)/h per axis.
 template <int S, class F, class V>
-__device__ int shape_weights(const GridT<F>& g, const double begin[3], const double end[3],
-                             V& visit) {
+__device__ int lattice_shape_weights(const GridT<F>& g, const double x[3], const double v[3],
+                                     V& visit);
+
+template <int S, class F, class V>
+__device__ __forceinline__ int shape_weights(const GridT<F>& g, const double begin[3],
+                                             const double end[3], V& visit) {
   const double h[3] = {g.dx, g.dy, g.dz};
+  double x[3], v[3];
+  for (int a = 0; a < 3; ++a) {
+    x[a] = (begin[a] - g.origin[a]) / h[a];
+    v[a] = (end[a] - begin[a]) / h[a];
+  }
+  return lattice_shape_weights<S>(g, x, v, visit);
+}
+
+template <int S, class F, class V>
+__device__ __forceinline__ int lattice_shape_weights(const GridT<F>& g, const double x[3],
+                                                     const double v[3], V& visit) {
   // The cell-boundary cuts of the chord, ascending.  Along each axis the cuts
   // (j - x)/v of the crossed lattice planes j are already monotone, so a
   // three-way merge yields the sorted cut sequence of the reference (same
   // values, ties give zero-width pieces) without a cut array.
-  double x[3], v[3], next[3];
+  double next[3];
   long long plane[3], left[3];
   int dir[3];
   long long total = 0;
   for (int a = 0; a < 3; ++a) {
-    x[a] = (begin[a] - g.origin[a]) / h[a];
-    v[a] = (end[a] - begin[a]) / h[a];
     left[a] = 0;
     if (v[a] != 0.) {
       const double lo = fmin(x[a], x[a] + v[a]), hi = fmax(x[a], x[a] + v[a]);
@@ -517,12 +532,15 @@ template <class W, class F>
 __device__ __forceinline__ void binomial_xz_magnetic(const GridT<F>& g, const Ptr3<W>& bsrc,
                                                      const double p[3], double value[3]) {
   const double h[3] = {g.dx, g.dy, g.dz};
+  // the point in lattice units, shared by the three components' staggerings
+  double lattice[3];
+  for (int d = 0; d < 3; ++d) lattice[d] = (p[d] - g.origin[d]) / h[d];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     long long cell[3];
     double fraction[3];
     for (int d = 0; d < 3; ++d) {
-      const double pos = (p[d] - g.origin[d]) / h[d] - (a == d ? 0. : 0.5);
+      const double pos = lattice[d] - (a == d ? 0. : 0.5);
       cell[d] = (long long)floor(pos);
       fraction[d] = pos - cell[d];
     }
@@ -590,35 +608,28 @@ __device__ __forceinline__ void trilinear_magnetic(const GridT<F>& g, const Ptr3
   }
 }
 
-// Impl::electric(a, b, open=true) for wide shapes (src/source_coupling.cpp:31-39).
+// Impl::electric(a, b, open=true) for wide shapes and Impl::magnetic
+// (src/source_coupling.cpp:31-51) of one chord a -> b: both clip the chord
+// with clipOpenOrbit, which is done once here; the electric error (crossing
+// budget) skips the magnetic gather, as the reference's call order does.
 template <int S, class W, class F>
-__device__ __forceinline__ unsigned gather_electric(const GridT<F>& g,
-                                                    const double a[3], const double b[3],
-                                                    const Ptr3<W>& orbit, double out[3]) {
-  OpenOrbit path;
-  if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
-  if (!path.valid) return kErrOrbitOutside;
-  ElectricVisitor<W, F> v{&g, orbit, {W(0.), W(0.), W(0.)}};
-  if (shape_weights<S>(g, path.begin, path.end, v) < 0) return kErrCrossingBudget;
-  const double fraction = path.last - path.first;
-  for (int d = 0; d < 3; ++d) out[d] = double(v.r[d]) * fraction;
-  return kErrNone;
-}
-
-// Impl::magnetic (src/source_coupling.cpp:40-51).
-template <int S, class W, class F>
-__device__ __forceinline__ unsigned gather_magnetic(const GridT<F>& g,
-                                                    const double a[3], const double b[3],
-                                                    const Ptr3<W>& bsrc, double out[3]) {
+__device__ __forceinline__ unsigned gather_fields(const GridT<F>& g, const double a[3],
+                                                  const double b[3], const Ptr3<W>& orbit,
+                                                  const Ptr3<W>& bsrc, double e_out[3],
+                                                  double b_out[3]) {
   OpenOrbit path;
   if (!clip_open_orbit(g, a, b, path)) return kErrNonFinite;
   if (!path.valid) return kErrOrbitOutside;
   double middle[3];
   for (int d = 0; d < 3; ++d) middle[d] = (path.begin[d] + path.end[d]) * .5;
+  const double fraction = path.last - path.first;
+  ElectricVisitor<W, F> ev{&g, orbit, {W(0.), W(0.), W(0.)}};
+  if (shape_weights<S>(g, path.begin, path.end, ev) < 0) return kErrCrossingBudget;
+  for (int d = 0; d < 3; ++d) e_out[d] = double(ev.r[d]) * fraction;
   if constexpr (S == 0)
-    binomial_xz_magnetic(g, bsrc, middle, out);
+    binomial_xz_magnetic(g, bsrc, middle, b_out);
   else
-    trilinear_magnetic(g, bsrc, middle, out);
+    trilinear_magnetic(g, bsrc, middle, b_out);
   return kErrNone;
 }
 
@@ -1153,8 +1164,7 @@ __global__ void APRL_GATHER_BOUNDS guess_gather_kernel(PushArgs<F> a) {
                        static_cast<const W*>(a.orbit[2])}};
   const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]), static_cast<const W*>(a.bgather[1]),
                       static_cast<const W*>(a.bgather[2])}};
-  unsigned err = gather_electric<S>(a.g, s.start, guess, orbit, ne);
-  if (!err) err = gather_magnetic<S>(a.g, s.start, guess, bsrc, nb);
+  const unsigned err = gather_fields<S>(a.g, s.start, guess, orbit, bsrc, ne, nb);
   if (err) raise_error(a.status, err, (unsigned long long)n);
   double* next_e = const_cast<double*>(a.next_e);
   double* next_b = const_cast<double*>(a.next_b);
@@ -1732,8 +1742,7 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
     const Ptr3<W> bsrc{{static_cast<const W*>(a.bgather[0]),
                         static_cast<const W*>(a.bgather[1]),
                         static_cast<const W*>(a.bgather[2])}};
-    unsigned err = gather_electric<S>(a.g, first, last, orbit, ne);
-    if (!err) err = gather_magnetic<S>(a.g, first, last, bsrc, nb);
+    const unsigned err = gather_fields<S>(a.g, first, last, orbit, bsrc, ne, nb);
     if (err) {
       raise_error(a.status, err, (unsigned long long)n);
       for (int d = 0; d < 3; ++d) ne[d] = nb[d] = 0.0;
