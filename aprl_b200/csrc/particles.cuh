@@ -179,14 +179,15 @@ struct ChordArgs {
 // Occupancy knobs of the hot particle kernels (blocks of 128 threads
 // that must fit one SM; 0 leaves the register count to the compiler).
 // Measured on the 128x128x512 dipole grid with 1M particles, with the
-// kernels built per shape: push_deposit at 8 blocks (64 registers, with
-// spills) beats 4, 10, 12 and 16 blocks on the binomial3, quintic,
-// FP32-mixed and drift workloads -- its FP64 reductions want many warps in
-// flight; the residual and the guess gather at 6 blocks (80 registers) beat
-// 4, 5 and 8 (dipole step 4.47 -> 4.44 ms, FP32-mixed 3.44 -> 3.35 ms,
-// quintic 15.99 -> 15.62 ms).
+// kernels built per shape: push_deposit at 6 blocks (80 registers) beats 5,
+// 7 and 8 on the binomial3, FP32-mixed and drift workloads and ties on
+// quintic (binomial3 launch 0.133 -> 0.120 ms against 8 blocks, whose
+// 64 registers spilled; with the main chords still deposited inside it, 8
+// had been best); the residual and the guess gather at 6 blocks (80
+// registers) beat 4, 5, 7 and 8 (dipole step 4.47 -> 4.44 ms, FP32-mixed
+// 3.44 -> 3.35 ms, quintic 15.99 -> 15.62 ms).
 #ifndef APRL_PUSH_MIN_BLOCKS
-#define APRL_PUSH_MIN_BLOCKS 8
+#define APRL_PUSH_MIN_BLOCKS 6
 #endif
 #ifndef APRL_RESIDUAL_MIN_BLOCKS
 #define APRL_RESIDUAL_MIN_BLOCKS 6
