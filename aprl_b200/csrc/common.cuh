@@ -293,22 +293,11 @@ struct Basis {
 
 // basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54): the
 // cell in binary64, the B-spline and compensation arithmetic in F on the
-// cell-relative offset.
+// cell-relative offset.  The compensation of the degree-`degree` spline
+// values n[0..degree]:
 template <class F>
-__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) {
-  const unsigned degree = edge ? 4 : 5;
-  const double cell = floor(z);
-  const F f = F(z - cell);
-  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
-  for (unsigned j = 1; j <= degree; ++j) {
-    F saved = F(0.);
-    for (unsigned k = 0; k < j; ++k) {
-      const F t = n[k] / F(j);
-      n[k] = saved + (F(k + 1) - f) * t;
-      saved = (f + F(j) - F(k) - F(1)) * t;
-    }
-    n[j] = saved;
-  }
+__device__ __forceinline__ void quintic_compensate(const F* n, unsigned degree, double cell,
+                                                   Basis<F>& r) {
   const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
                d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
   const F c[7] = {F(-d / 64.), F(b / 16. + 3 * d / 32.), F(-a / 4. - b / 4. - 15 * d / 64.),
@@ -319,6 +308,52 @@ __device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) 
   for (int q = 0; q < 12; ++q) r.v[q] = F(0.);
   for (unsigned j = 0; j <= degree; ++j)
     for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
+}
+
+// The B-spline recursion on f = z - floor(z) up to `degree`.
+template <class F>
+__device__ __forceinline__ void quintic_spline_level(F n[6], F f, unsigned j) {
+  F saved = F(0.);
+  for (unsigned k = 0; k < j; ++k) {
+    const F t = n[k] / F(j);
+    n[k] = saved + (F(k + 1) - f) * t;
+    saved = (f + F(j) - F(k) - F(1)) * t;
+  }
+  n[j] = saved;
+}
+
+template <class F>
+__device__ __forceinline__ void quintic_basis(double z, bool edge, Basis<F>& r) {
+  const unsigned degree = edge ? 4 : 5;
+  const double cell = floor(z);
+  const F f = F(z - cell);
+  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
+  for (unsigned j = 1; j <= degree; ++j) quintic_spline_level(n, f, j);
+  quintic_compensate(n, degree, cell, r);
+}
+
+// Both spline sets of one point: the edge basis (degree 4) is the node
+// basis's recursion (degree 5) stopped after its fourth level, so one pass
+// yields the values quintic_basis computes for either.
+template <class F>
+struct QuinticSplines {
+  double cell;
+  F edge[5];
+  F node[6];
+};
+
+template <class F>
+__device__ __forceinline__ void quintic_splines(double z, QuinticSplines<F>& s) {
+  s.cell = floor(z);
+  const F f = F(z - s.cell);
+  F n[6] = {F(1.), F(0.), F(0.), F(0.), F(0.), F(0.)};
+#pragma unroll
+  for (unsigned j = 1; j <= 4; ++j) quintic_spline_level(n, f, j);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) s.edge[q] = n[q];
+  quintic_spline_level(n, f, 5);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) s.node[q] = n[q];
 }
 
 // BoostFrameTransform::gammaFromProperVelocity (src/boostframe.cpp:74-87).

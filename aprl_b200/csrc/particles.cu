@@ -138,6 +138,7 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
   F factor[4], fx[4], fy[4];
   long long i = 0, j = 0, kz = 0;
   bool same = true;
+#pragma unroll
   for (int t = 0; t < 4; ++t) {
     const double u = .5 * (upper + lower + width * q[t]), xx = x[0] + u * v[0],
                  yy = x[1] + u * v[1];
@@ -161,6 +162,11 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
     quintic_segment(g, x, v, lower, upper, width, visit);
     return;
   }
+  // Each Gauss point's spline recursion once; the compensated bases below
+  // are formed from these values exactly as quintic_basis forms them.
+  QuinticSplines<F> spline[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) quintic_splines(zz[t], spline[t]);
   Basis<F> b;
   // Jx at (i, j + c) and Jy at (i + c, j): node basis, 12 nodes.
   for (int axis = 0; axis < 2; ++axis)
@@ -170,7 +176,7 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
       long long first = 0;
       for (int k = 0; k < 12; ++k) acc[k] = F(0.);
       for (int t = 0; t < 4; ++t) {
-        quintic_basis(zz[t], false, b);
+        quintic_compensate(spline[t].node, 5, spline[t].cell, b);
         first = b.first;
         const F side = axis == 0 ? (c ? fy[t] : F(1.) - fy[t]) : (c ? fx[t] : F(1.) - fx[t]);
         for (int k = 0; k < b.count; ++k) {
@@ -196,7 +202,7 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
       long long first = 0;
       for (int k = 0; k < 12; ++k) acc[k] = F(0.);
       for (int t = 0; t < 4; ++t) {
-        quintic_basis(zz[t], true, b);
+        quintic_compensate(spline[t].edge, 4, spline[t].cell, b);
         first = b.first;
         for (int k = 0; k < b.count; ++k) {
           const F w = factor[t] * b.v[k];
