@@ -97,9 +97,11 @@ __device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double 
     if (i == (long long)g.nx) --i;
     if (j == (long long)g.ny) --j;
     const F fx = F(xx - i), fy = F(yy - j);
+    QuinticSplines<F> spline;
+    quintic_splines(zz, spline);
     Basis<F> nodes, edge;
-    quintic_basis(zz, false, nodes);
-    quintic_basis(zz, true, edge);
+    quintic_compensate(spline.node, 5, spline.cell, nodes);
+    quintic_compensate(spline.edge, 4, spline.cell, edge);
     for (int k = 0; k < nodes.count; ++k) {
       const F w = factor * nodes.v[k];
       if (w == F(0.)) continue;
@@ -121,8 +123,11 @@ __device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double 
 // the same cell, so the 4 x 92 node visits fall on 92 nodes; each node's four
 // weights are summed first and visited once (a quarter of the atomics).  The
 // weights are quintic_segment's; only their summation order changes.  Per
-// component and transverse corner the Gauss points' bases are recomputed,
-// which keeps the accumulators to one z column (12 values).  A piece whose
+// component and transverse corner the Gauss points' compensated bases are
+// re-formed from their spline values (one recursion per point, done once),
+// which keeps the accumulators to one z column (12 values); two corners per
+// pass would hold 24 live sums, and at the kernels' 80 registers they spill
+// several times more.  A piece whose
 // Gauss points straddle a cell (only possible through rounding at a cut) is
 // visited point by point.
 template <class G, class V>

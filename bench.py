@@ -194,10 +194,10 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
     n_cells = cfg.nx * cfg.ny * cfg.nz
     if kernel == "cowan_magnetic":      # read 3 E, read+write 3 B
         return 9 * 8 * n_cells
-    if kernel == "electric_preview":    # read 3 E^n and 3 B, write 3 E*
-        return 9 * 8 * n_cells
-    if kernel == "electric_commit":     # read E* and J, write E
-        return 9 * 8 * n_cells
+    if kernel == "electric_preview":    # read 3 E^n and 3 B, write 3 E* and, with particles
+        return (12 if particles else 9) * 8 * n_cells   # in the window, the orbit sum E* + E^n
+    if kernel == "electric_commit":     # read J; E* += -dt/eps0 J only where J != 0
+        return 3 * 8 * n_cells          # (that part depends on the bunch; not counted)
     if kernel == "push_deposit":        # read x,u,q,m,nextE/B; write x1,u1,usedE/B,work,flags,
         return particles * (64 + 48 + 48 + 48 + 8 + 2 + 49)   # and the chord (b, e, mode)
     if kernel == "chord_deposit":       # read the chord (b, e), q, mode; J updates are L2 reductions
@@ -214,15 +214,18 @@ def algorithmic_bytes(kernel, cfg, particles, carriers):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# one ncu capture of this workload's grid with 250k particles, cold L2: per
-# particle for the particle kernels, per launch for the grid passes.
-MEASURED_TRAFFIC = {"chord_deposit": ("particle", 229.0),
-                    "push_deposit": ("particle", 217.0),
-                    "residual": ("particle", 567.0),
-                    "guess_gather": ("particle", 454.0),
-                    "cowan_magnetic": ("launch", 669.9e6),
-                    "orbit_sum": ("launch", 792.0e6),
-                    "electric_preview": ("launch", 844.2e6)}
+# one-kernel ncu captures of the default workload -- dipole, 128x128x512
+# cells, 1M particles, linear-binomial3, FP64 -- with a cold L2.  The grid
+# passes move the same bytes for any bunch on this grid; the particle
+# kernels' traffic is mostly the fields over the bunch's region, which does
+# not grow with the particle count, so they have a figure only at 1M.
+GRID_TRAFFIC = {"cowan_magnetic": 669_778_944, "orbit_sum": 791_749_632,
+                "electric_preview": 845_800_448, "electric_commit": 280_096_512}
+PARTICLE_TRAFFIC = {"chord_deposit": 118_682_624, "push_deposit": 252_511_232,
+                    "residual": 287_908_096, "guess_gather": 191_039_744}
+PARTICLE_TRAFFIC_CONFIG = {"workload": "dipole", "shape": "linear-binomial3",
+                           "precision": "fp64", "particles": 1_000_000,
+                           "deterministic": False}
 
 
 # L2 reduction sectors per particle of one chord_deposit launch: ncu
@@ -264,11 +267,17 @@ def atomic_peak(integer=False):
     return rate.value / 1e9
 
 
-def measured_traffic(kernel, particles):
-    kind, value = MEASURED_TRAFFIC.get(kernel, (None, None))
-    if kind == "particle":
-        return value * particles
-    return value
+def measured_traffic(kernel, args):
+    """Measured DRAM bytes of one launch of `kernel` on this run's
+    configuration, or None where none was measured."""
+    if args.workload != "dipole":
+        return None
+    if kernel in GRID_TRAFFIC:
+        return GRID_TRAFFIC[kernel]
+    if kernel in PARTICLE_TRAFFIC and all(
+            getattr(args, key) == value for key, value in PARTICLE_TRAFFIC_CONFIG.items()):
+        return PARTICLE_TRAFFIC[kernel]
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -455,10 +464,10 @@ def run_ours(args):
                     "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": (achieved / peak) if achieved else None,
                     "peak_source": peak_kind,
-                    "traffic": measured_traffic(name, mean_particles),
-                    "traffic_source": "ncu DRAM bytes of one-kernel captures of this grid "
-                                      "with 250k particles, scaled per particle for particle "
-                                      "kernels (profiles/dram_traffic_*)",
+                    "traffic": measured_traffic(name, args),
+                    "traffic_source": "ncu DRAM bytes of a one-kernel capture of this "
+                                      "workload at 1M particles, cold L2 "
+                                      "(profiles/dram_traffic_dipole_128x128x512_1M.md)",
                     "bytes_per_launch": algo, "ms_per_launch": per_launch_ms,
                     "launches": count}
     atomic_roofline = None
@@ -489,6 +498,11 @@ def run_ours(args):
         if algo and v[1]:
             gbs = algo / (v[0] / v[1] * 1e-3) / 1e9
             entry.update({"bytes_per_launch": algo, "achieved_gbs": gbs, "hbm_frac": gbs / peak})
+        traffic = measured_traffic(k, args)
+        if traffic and v[1]:
+            # DRAM bytes one launch moved (ncu) over its mean launch time here
+            entry.update({"dram_bytes_per_launch": traffic,
+                          "dram_gbs": traffic / (v[0] / v[1] * 1e-3) / 1e9})
         kernels[k] = entry
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s",
