@@ -194,7 +194,12 @@ class SelfFieldConfig(C.Structure):
         ("maximum_mean_transverse_beta", C.c_double),
         ("maximum_iterations", C.c_uint64),
         ("guard_cells", C.c_uint64 * 3),
+        ("source_shape", C.c_int32),
+        ("reserved", C.c_int32),
     ]
+
+
+SOURCE_SHAPES = {"cic": 0, "run-shape": 1}
 
 
 class SelfFieldReport(C.Structure):
@@ -221,12 +226,16 @@ class SelfFieldReport(C.Structure):
 def self_field_config(run_config, model="cowan-relativistic-poisson", tolerance=1e-10,
                       maximum_iterations=20000, maximum_mean_transverse_beta=0.05,
                       include_transverse_cpml_particles=False,
-                      hold_transverse_until_activation=False, solver="cg"):
+                      hold_transverse_until_activation=False, solver="cg",
+                      source_shape="cic"):
     """The initializer controls with the CPML cells as the static guard;
     solver "cg" (the reference's initializer) or "modal" (transverse sine
-    modes and a tridiagonal solve along z per mode)."""
+    modes and a tridiagonal solve along z per mode); source_shape "cic"
+    (the initializer's charge) or "run-shape" (the shaped source of the
+    moving window's prepared reference)."""
     c = SelfFieldConfig()
     c.solver = {"cg": 0, "modal": 1}[solver]
+    c.source_shape = SOURCE_SHAPES[source_shape]
     c.model = SELF_FIELD_MODELS[model]
     c.include_transverse_cpml_particles = int(include_transverse_cpml_particles)
     c.hold_transverse_until_activation = int(hold_transverse_until_activation)

@@ -57,6 +57,9 @@ enum DeviceError : unsigned {
   kErrFixedRange = 22,        // deterministic deposit: contribution beyond the fixed-point range
   kErrBounds = 23,            // bounds-checked build: an index outside its array
   kErrSurfaceCurrent = 24,    // non-finite equivalent boundary current of the reference
+  kErrReferenceSupport = 25,  // shaped reference source on or outside the zero-potential box
+  kErrReferenceSource = 26,   // shaped reference source: non-finite longitudinal coordinate
+  kErrReferenceCharge = 27,   // shaped reference source: non-finite charge
   kErrCount
 };
 

@@ -108,6 +108,9 @@ const char* device_error_text(unsigned code) {
     case kErrFixedRange:
       return "Deposit contribution beyond the deterministic fixed-point range";
     case kErrSurfaceCurrent: return "Nonfinite equivalent boundary current";
+    case kErrReferenceSupport: return "Reference charge support touches Dirichlet surface";
+    case kErrReferenceSource: return "Nonfinite quintic reference source";
+    case kErrReferenceCharge: return "Nonfinite quintic reference charge";
     case kErrBounds:
       return "Array index outside its array (bounds-checked build)";
   }
@@ -120,6 +123,8 @@ aprl_status device_error_status(unsigned code) {
     case kErrSupportY: case kErrStartInCpml: case kErrStartOutside:
     case kErrReferenceRange: case kErrBounds:
       return APRL_ERR_OUT_OF_RANGE;
+    case kErrReferenceSupport: case kErrReferenceSource: case kErrReferenceCharge:
+      return APRL_ERR_INVALID_ARGUMENT;
     default:
       return APRL_ERR_RUNTIME;
   }
@@ -3172,6 +3177,13 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
     return fail(APRL_ERR_INVALID_ARGUMENT,
                 "Transverse CPML-source initialization requires at least two physical guard "
                 "cells in x and y");
+  if (cfg->source_shape != APRL_SOURCE_SHAPE_CIC &&
+      cfg->source_shape != APRL_SOURCE_SHAPE_RUN_SHAPE)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Unknown initial self-field source shape");
+  const bool shaped = cfg->source_shape == APRL_SOURCE_SHAPE_RUN_SHAPE;
+  if (shaped && include)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "The shaped reference source has no transverse CPML-source padding");
   const bool cowan = cfg->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON;
   const bool relativistic = cfg->model == APRL_SELF_FIELD_RELATIVISTIC_POISSON || cowan;
   const int pad = include ? 2 : 0;
@@ -3353,10 +3365,16 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
                          (size_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1) * sizeof(double) +
                          (pad ? rho_count * sizeof(double) : 0);
 
-  // The CIC charge and the Poisson source (src/eb_initial_field.cpp:979-1027)
+  // The CIC charge (or the shaped reference source) and the Poisson source
+  // (src/eb_initial_field.cpp:979-1027)
   const DGrid g = make_grid<double>(r);
-  TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
-             buf.rho, L.lx, L.ly, pad, r->d_status));
+  const int binomial = c.shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+  if (shaped)
+    TRY(launch(r, kSfDeposit, sf_shaped_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
+               P, g, buf.rho, L.lx, L.ly, L, binomial, r->d_status));
+  else
+    TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
+               buf.rho, L.lx, L.ly, pad, r->d_status));
   const DD vertex_volume = ledger_product(ledger_product(c.dx, c.dy), c.dz);
   TRY(launch(r, kSfSource, sf_source_kernel, tile_grid, tile_block, A, vertex_volume));
   TRY(launch(r, kSfFinish, sf_finish_kernel, dim3(1), dim3(kSelfFieldThreads),
@@ -3484,12 +3502,18 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
       TRY(launch(r, kSfClear, sf_clear_outside_kernel, dim3(fblocks), dim3(256), A, comp,
                  (int)cfg->guard_cells[0], (int)cfg->guard_cells[1], (int)cfg->guard_cells[2]));
 
-  // validateGauss on the unpadded CIC charge (src/eb_initial_field.cpp:1083-1091)
+  // validateGauss on the unpadded charge the potential was solved for
+  // (src/eb_initial_field.cpp:1083-1091): CIC, or the shaped reference source
+  // (whose lattice has no padding)
   const int vx = (int)c.nx + 1, vy = (int)c.ny + 1;
   CUDA_TRY(cudaMemsetAsync(buf.rho, 0, (size_t)vx * vy * (c.nz + 1) * sizeof(double), r->stream));
   CUDA_TRY(cudaMemsetAsync(buf.max_bits, 0, sizeof(unsigned long long), r->stream));
-  TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
-             buf.rho, vx, vy, 0, r->d_status));
+  if (shaped)
+    TRY(launch(r, kSfDeposit, sf_shaped_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256),
+               P, g, buf.rho, vx, vy, L, binomial, r->d_status));
+  else
+    TRY(launch(r, kSfDeposit, sf_deposit_kernel, dim3(blocks_for(r->np, 256)), dim3(256), P, g,
+               buf.rho, vx, vy, 0, r->d_status));
   const int gblocks = (int)std::min<size_t>(kSelfFieldBlocks,
                                             blocks_for((size_t)vx * vy * c.nz, kSelfFieldThreads));
   TRY(launch(r, kSfGauss, sf_gauss_kernel, dim3(gblocks), dim3(kSelfFieldThreads), A,

@@ -186,6 +186,87 @@ __global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, i
       }
 }
 
+// BlockedCowanReference::depositQuintic (src/blocked_cowan_reference.cpp:
+// 559-592): the shaped source with which the moving window prepares its
+// reference (the mesh shape, src/simulation_moving_window.cpp:145-148).  Per
+// particle x = (p - origin)/h; for linear-binomial3 the binomial3
+// transverse x weights over nodes floor(x)-1 .. floor(x)+2
+// (src/transverse_source_shape.h:8-10) and the binomial3 node basis in z,
+// for quintic-compensated linear x weights and the quintic node basis; y is
+// linear.  Each nonzero contribution ((q/(dx dy dz)) wx) wy wz must land on
+// an interior node of L's zero-potential box, else the reference's
+// "Reference charge support touches Dirichlet surface".  Binary64 atomics:
+// the same terms as the reference's serial sum, in another order.
+__global__ void sf_shaped_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly,
+                                         SfLattice L, int binomial, DeviceStatus* status) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= p.n) return;
+  const double q = p.q[n];
+  if (!isfinite(q)) {
+    raise_error(status, kErrReferenceCharge, (unsigned long long)n);
+    return;
+  }
+  const double x = (p.x[n] - g.origin[0]) / g.dx, y = (p.y[n] - g.origin[1]) / g.dy,
+               z = (p.z[n] - g.origin[2]) / g.dz;
+  if (!isfinite(z)) {
+    raise_error(status, kErrReferenceSource, (unsigned long long)n);
+    return;
+  }
+  if (!isfinite(x) || !isfinite(y)) {  // no node of such a support is interior
+    raise_error(status, kErrReferenceSupport, (unsigned long long)n);
+    return;
+  }
+  const double cx = floor(x), cy = floor(y);
+  const long long ix = (long long)cx, iy = (long long)cy;
+  const double fx = x - cx, fy = y - cy, scale = q / (g.dx * g.dy * g.dz);
+  double wz[12];
+  long long zfirst;
+  int zcount;
+  if (binomial) {
+    // basis(z, false, LinearBinomial3) (src/longitudinal_shape.h:26-36)
+    const double cell = floor(z), f = z - cell;
+    const double c3[3] = {0.25, 0.5, 0.25};
+    for (int t = 0; t < 4; ++t) wz[t] = 0.0;
+    for (int s = 0; s < 3; ++s) {
+      wz[s] += c3[s] * (1.0 - f);
+      wz[s + 1] += c3[s] * f;
+    }
+    zfirst = (long long)cell - 1;
+    zcount = 4;
+  } else {
+    Basis<double> b;
+    quintic_basis<double>(z, false, b);
+    for (int t = 0; t < 12; ++t) wz[t] = b.v[t];
+    zfirst = b.first;
+    zcount = b.count;
+  }
+  double wx[4] = {1.0 - fx, fx, 0.0, 0.0};
+  if (binomial) {
+    wx[0] = 0.25 * (1.0 - fx);
+    wx[1] = 0.5 - 0.25 * fx;
+    wx[2] = 0.25 + 0.25 * fx;
+    wx[3] = 0.25 * fx;
+  }
+  const long long xfirst = ix - (binomial ? 1 : 0);
+  const int xcount = binomial ? 4 : 2;
+  for (int c = 0; c < zcount; ++c) {
+    const long long k = zfirst + c;
+    if (wz[c] == 0.0) continue;
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < xcount; ++i) {
+        const double value = scale * wx[i] * (j ? fy : 1.0 - fy) * wz[c];
+        if (value == 0.0) continue;
+        const long long nx = xfirst + i, ny = iy + j;
+        if (!(nx > L.lo[0] && nx < L.hi[0] && ny > L.lo[1] && ny < L.hi[1] && k > L.lo[2] &&
+              k < L.hi[2])) {
+          raise_error(status, kErrReferenceSupport, (unsigned long long)n);
+          return;
+        }
+        atomicAdd(&rho[((size_t)k * ly + (size_t)ny) * lx + (size_t)nx], value);
+      }
+  }
+}
+
 // The Poisson source rho/eps0 at the interior vertices (into the residual
 // and the first direction), with partial sums of the interior charge and of
 // the source norm (src/eb_initial_field.cpp:991-1027).

@@ -75,6 +75,10 @@ __global__ void sf_moments_kernel(SfParticles p, DD* partial);
 __global__ void sf_finish_kernel(const DD* partial, int blocks, int quantities, DD* out);
 __global__ void sf_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly, int pad,
                                   DeviceStatus* status);
+// The moving window's shaped reference source (BlockedCowanReference::
+// depositQuintic) into an unpadded lattice; binomial selects linear-binomial3.
+__global__ void sf_shaped_deposit_kernel(SfParticles p, DGrid g, double* rho, int lx, int ly,
+                                         SfLattice L, int binomial, DeviceStatus* status);
 __global__ void sf_source_kernel(SfArgs a, DD volume);
 // One CG iteration is three launches: apply (its last block forms alpha),
 // update (its last block forms the relative residual, the stopping test and

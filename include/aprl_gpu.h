@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define APRL_GPU_ABI_VERSION 2
+#define APRL_GPU_ABI_VERSION 3
 
 typedef enum {
   APRL_OK = 0,
@@ -509,6 +509,24 @@ typedef enum {
   APRL_SELF_FIELD_SOLVER_MODAL = 1
 } aprl_self_field_solver;
 
+/* The charge the potential is solved for.  CIC: the cloud-in-cell charge of
+ * EBGaussFieldInitializer (ChargeConservingCurrentDepositor::depositCharge,
+ * src/eb_deposition.cpp:168-193).  RUN_SHAPE: the shaped source with which
+ * the moving window prepares its inlet reference
+ * (BlockedCowanReference::depositQuintic, src/blocked_cowan_reference.cpp:
+ * 559-592, selected by the mesh shape at src/simulation_moving_window.cpp:
+ * 145-148 and src/config.cpp:1084-1112): for linear-binomial3 the
+ * binomial3 transverse weights in x (src/transverse_source_shape.h:8-10),
+ * linear in y and the binomial3 node basis in z; for quintic-compensated
+ * linear in x and y and the quintic node basis in z.  Its support must lie
+ * inside the zero-potential box ("Reference charge support touches Dirichlet
+ * surface") and it has no transverse CPML-source padding
+ * (include_transverse_cpml_particles must be 0). */
+typedef enum {
+  APRL_SOURCE_SHAPE_CIC = 0,
+  APRL_SOURCE_SHAPE_RUN_SHAPE = 1
+} aprl_source_shape;
+
 typedef struct {
   int32_t model;                      /* aprl_self_field_model */
   int32_t include_transverse_cpml_particles;
@@ -518,6 +536,8 @@ typedef struct {
   double maximum_mean_transverse_beta;
   uint64_t maximum_iterations;
   uint64_t guard_cells[3];            /* staticFieldGuardCells: the CPML cells per axis */
+  int32_t source_shape;               /* aprl_source_shape */
+  int32_t reserved;                   /* zero */
 } aprl_self_field_config;
 
 /* EBGaussInitializationReport (src/eb_initial_field.h:17-34). */
@@ -557,12 +577,17 @@ aprl_status aprl_run_initialize_self_field(aprl_run* run, const aprl_self_field_
  * and its fill of MovingWindowReference): the Cowan initial self-field
  * (aprl_run_initialize_self_field with `config`) of the given particles on
  * the reference grid (nx, ny, reference_nz cells from reference_origin),
- * whose E and B become the run's six reference tables.  The reference
- * checks that the blocked modal solve reproduces this initializer on the
- * same grid to its CG tolerance (verification/blocked_cowan_reference_checks.cpp:61-130);
- * here the initializer itself is the solve.  Particles in box coordinates
- * at box time 0; ids are not needed.  Allocates a temporary run of the
- * reference grid's size for the solve.  Before the first step. */
+ * whose E and B become the run's six reference tables.  With
+ * config->source_shape = APRL_SOURCE_SHAPE_RUN_SHAPE the charge is the
+ * shaped source the moving window uses for its reference (the run's own
+ * shape, BlockedCowanReference::depositQuintic), with
+ * config->solver = APRL_SELF_FIELD_SOLVER_MODAL the blocked reference's
+ * sine-mode and tridiagonal solve; CIC and CG are the initializer's.  The
+ * reference's own check holds its blocked solve to the initializer to the
+ * CG tolerance (verification/blocked_cowan_reference_checks.cpp:61-130).
+ * Particles in box coordinates at box time 0; ids are not needed.
+ * Allocates a temporary run of the reference grid's size for the solve.
+ * Before the first step. */
 aprl_status aprl_run_prepare_reference(aprl_run* run, size_t count, const double* x,
                                        const double* y, const double* z, const double* ux,
                                        const double* uy, const double* uz,

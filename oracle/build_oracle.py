@@ -4,7 +4,9 @@
   always built.
 * oracle/_ref/libaprl_ref.so -- the reference's own hot-path translation
   units, compiled straight from the APRL sources with a single-rank MPI
-  stand-in (oracle/ref/mpi_shim) and the driver in oracle/ref/ref_harness.cpp.
+  stand-in (oracle/ref/mpi_shim), a stand-in for the three FFTW calls of the
+  blocked Cowan reference (oracle/ref/fftw_shim: the type-I sine transform
+  by direct sums) and the driver in oracle/ref/ref_harness.cpp.
   Built only where the APRL source tree is present; the built library then
   travels with the repository copy.
 
@@ -33,7 +35,7 @@ REFERENCE_UNITS = [
     "eb_field", "eb_cpml", "eb_deposition", "eb_particles", "boostframe",
     "eb_sources", "compute_threads", "source_coupling",
     "moving_window_fields", "particle_boundary", "pending_particle_queue",
-    "eb_initial_field", "transverse_reference_current",
+    "eb_initial_field", "transverse_reference_current", "blocked_cowan_reference",
 ]
 
 
@@ -69,8 +71,9 @@ def build_reference(reference_src):
     objdir = os.path.join(outdir, "obj")
     os.makedirs(objdir, exist_ok=True)
     shim = os.path.join(HERE, "ref", "mpi_shim")
+    fftw = os.path.join(HERE, "ref", "fftw_shim")
     flags = ["-std=c++14", "-O2", "-fopenmp", "-DAPRL_HAS_OPENMP=1",
-             "-DAPRL_HAS_MOVING_WINDOW=1", "-fPIC", "-I", shim,
+             "-DAPRL_HAS_MOVING_WINDOW=1", "-fPIC", "-I", shim, "-I", fftw,
              "-I", reference_src, "-I", os.path.join(REPO, "include")]
     objects = []
     headers = [os.path.join(reference_src, f) for f in os.listdir(reference_src)
@@ -82,9 +85,10 @@ def build_reference(reference_src):
             run(["g++"] + flags + ["-c", src, "-o", obj])
         objects.append(obj)
     for src in [os.path.join(HERE, "ref", "ref_harness.cpp"),
-                os.path.join(shim, "mpi_shim.cpp")]:
+                os.path.join(shim, "mpi_shim.cpp"),
+                os.path.join(fftw, "fftw_shim.cpp")]:
         obj = os.path.join(objdir, os.path.basename(src).replace(".cpp", ".o"))
-        if newer(obj, [src, os.path.join(shim, "mpi.h"),
+        if newer(obj, [src, os.path.join(shim, "mpi.h"), os.path.join(fftw, "fftw3.h"),
                        os.path.join(REPO, "include", "aprl_gpu.h")] + headers):
             run(["g++"] + flags + ["-c", src, "-o", obj])
         objects.append(obj)

@@ -3280,6 +3280,51 @@ static aprl_status sf_deposit(const oracle_run* r, double* rho, size_t lx, size_
   return APRL_OK;
 }
 
+/* The moving window's shaped reference source, BlockedCowanReference::
+ * depositQuintic (src/blocked_cowan_reference.cpp:559-592): per particle
+ * x = (p - origin)/h, the transverse x weights (src/transverse_source_shape.h:
+ * 8-10, nodes floor(x)-1 .. floor(x)+2) for linear-binomial3 or linear ones,
+ * linear y weights and the run shape's node basis in z; each nonzero
+ * contribution q/(dx dy dz) wx wy wz must land on an interior node of the
+ * zero-potential box `d`.  The reference adds a node's contributions in the
+ * order of its z-block source buckets, this restatement in particle order:
+ * the same terms, summed in another order. */
+static aprl_status sf_shaped_deposit(const oracle_run* r, double* rho, size_t lx, size_t ly,
+                                     const sdomain_t* d) {
+  const aprl_run_config* g = &r->cfg;
+  const int binomial = g->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+  for (size_t n = 0; n < r->np; ++n) {
+    const particle_t* p = &r->p[n];
+    if (!isfinite(p->q)) return fail(APRL_ERR_INVALID_ARGUMENT, "Nonfinite quintic reference charge");
+    const double x = (p->pos[0] - r->origin[0]) / g->dx, y = (p->pos[1] - r->origin[1]) / g->dy,
+                 z = (p->pos[2] - r->origin[2]) / g->dz;
+    if (!isfinite(z)) return fail(APRL_ERR_INVALID_ARGUMENT, "Nonfinite quintic reference source");
+    const long long ix = (long long)floor(x), iy = (long long)floor(y);
+    const double fx = x - ix, fy = y - iy, scale = p->q / (g->dx * g->dy * g->dz);
+    const basis_t weights = shape_basis(z, 0, g->shape);
+    double wx[4] = {1. - fx, fx, 0., 0.};
+    if (binomial) node_weights(fx, wx);
+    const long long first_x = ix - (binomial ? 1 : 0);
+    const unsigned count_x = binomial ? 4 : 2;
+    for (unsigned c = 0; c < weights.count; ++c) {
+      const long long k = weights.first + c;
+      if (weights.v[c] == 0.) continue;
+      for (unsigned j = 0; j < 2; ++j)
+        for (unsigned i = 0; i < count_x; ++i) {
+          const double value = scale * wx[i] * (j ? fy : 1. - fy) * weights.v[c];
+          if (value == 0.) continue;
+          const long long node_x = first_x + i, node_y = iy + j;
+          if (k < 0 || node_x < 0 || node_y < 0 ||
+              !sf_interior((size_t)node_x, (size_t)node_y, (size_t)k, d))
+            return fail(APRL_ERR_INVALID_ARGUMENT,
+                        "Reference charge support touches Dirichlet surface");
+          rho[((size_t)k * ly + (size_t)node_y) * lx + (size_t)node_x] += value;
+        }
+    }
+  }
+  return APRL_OK;
+}
+
 static long double sf_dot(const slab_t* a, const slab_t* b, const sdomain_t* d, size_t nz) {
   long double local = 0.0L;
   for (size_t p = 1; p <= nz; ++p) {
@@ -3388,6 +3433,12 @@ aprl_status oracle_run_initialize_self_field(oracle_run* r, const aprl_self_fiel
     return fail(APRL_ERR_INVALID_ARGUMENT,
                 "Transverse CPML-source initialization requires at least two physical guard "
                 "cells in x and y");
+  if (cfg->source_shape != APRL_SOURCE_SHAPE_CIC && cfg->source_shape != APRL_SOURCE_SHAPE_RUN_SHAPE)
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Unknown initial self-field source shape");
+  const int shaped = cfg->source_shape == APRL_SOURCE_SHAPE_RUN_SHAPE;
+  if (shaped && include)
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "The shaped reference source has no transverse CPML-source padding");
   const int cowan = cfg->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON;
   const int relativistic = cfg->model == APRL_SELF_FIELD_RELATIVISTIC_POISSON || cowan;
   const size_t pad = include ? 2 : 0;
@@ -3489,7 +3540,8 @@ aprl_status oracle_run_initialize_self_field(oracle_run* r, const aprl_self_fiel
                          (g->nx + 1) * (g->ny + 1) * (g->nz + 1) * sizeof(double) +
                          (pad ? lx * ly * (g->nz + 1) * sizeof(double) : 0);
   double* rho = (double*)calloc(lx * ly * (g->nz + 1), sizeof(double));
-  aprl_status st = sf_deposit(r, rho, lx, ly, pad);
+  aprl_status st = shaped ? sf_shaped_deposit(r, rho, lx, ly, &domain)
+                          : sf_deposit(r, rho, lx, ly, pad);
   if (st != APRL_OK) {
     free(rho);
     sf_free(s, 4);
@@ -3670,11 +3722,12 @@ aprl_status oracle_run_initialize_self_field(oracle_run* r, const aprl_self_fiel
           }
     }
   }
-  /* validateGauss (src/eb_initial_field.cpp:743-806) on the unpadded CIC charge */
+  /* validateGauss (src/eb_initial_field.cpp:743-806) on the unpadded charge
+   * the potential was solved for (CIC, or the shaped reference source) */
   {
     const size_t vx = g->nx + 1, vy = g->ny + 1;
     double* vrho = (double*)calloc(vx * vy * (g->nz + 1), sizeof(double));
-    st = sf_deposit(r, vrho, vx, vy, 0);
+    st = shaped ? sf_shaped_deposit(r, vrho, vx, vy, &physical) : sf_deposit(r, vrho, vx, vy, 0);
     if (st != APRL_OK) {
       free(vrho);
       return st;

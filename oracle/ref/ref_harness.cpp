@@ -74,15 +74,6 @@ aprl_status guarded(F f) {
 }
 }  // namespace
 
-// The blocked modal reference needs FFTW, which this image lacks; the
-// harness writes the surface-current file itself (below), so the only caller
-// of this member, TransverseReferenceCurrent::prepare, is never reached.
-namespace aprl { namespace verification {
-Double BlockedCowanReference::field(unsigned, std::size_t, std::size_t, std::size_t) {
-  throw std::runtime_error("BlockedCowanReference is not built here");
-}
-}}  // namespace aprl::verification
-
 struct ref_run {
   aprl_run_config cfg;
   // The reference's own TransverseReferenceCurrent over a file the harness
@@ -1058,6 +1049,65 @@ aprl_status ref_run_energy_ledger(ref_run* r, aprl_energy_ledger* out) {
 }
 
 // EBGaussFieldInitializer::initialize at one rank on the run's particles.
+// The reference's own BlockedCowanReference (src/blocked_cowan_reference.h:
+// 59-130), built here over the FFTW stand-in of fftw_shim/, on a reference
+// grid of config->nx x ny x reference_nz cells from reference_origin: its
+// charge deposit, transverse-mode solve and native E/B, read back with
+// field() into the six tables (x fastest, the layout of
+// aprl_run_set_reference).  shape 0 deposits CIC; shape 1 the run's own
+// shape as the moving window prepares its reference
+// (src/simulation_moving_window.cpp:145-148 with src/config.cpp:1084-1112):
+// linear-binomial3 in z with the binomial3 transverse x weights, or the
+// quintic-compensated node basis in z.  `directory` must not exist: the
+// reference creates it, and its files are removed afterwards.  report:
+// source charge, deposited charge, minimum Thomas pivot, minimum mode
+// eigenvalue.
+aprl_status ref_blocked_reference(const aprl_run_config* config, size_t n, const double* x,
+                                  const double* y, const double* z, const double* charge,
+                                  double beta, const uint64_t guards[3], uint64_t block_layers,
+                                  int shape, const char* directory, double* const tables[6],
+                                  double report[4]) {
+  return guarded([&] {
+    const EBGridGeometry g(config->nx, config->ny, config->reference_nz, config->dx, config->dy,
+                           config->dz, config->dt, EBMaxwellSolver::CowanZ);
+    Vec origin;
+    for (unsigned a = 0; a < 3; ++a) origin[a] = config->reference_origin[a];
+    std::vector<RelativisticParticleSI> particles(n);
+    for (size_t i = 0; i < n; ++i) {
+      particles[i].position[0] = x[i];
+      particles[i].position[1] = y[i];
+      particles[i].position[2] = z[i];
+      particles[i].charge = charge[i];
+      particles[i].id = i;
+    }
+    const bool shaped = shape != 0;
+    const bool binomial = config->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+    const std::size_t guard[3] = {guards[0], guards[1], guards[2]};
+    const std::string dir(directory);
+    {
+      verification::BlockedCowanReference ref(
+          g, origin, particles, beta, guard, block_layers, dir, MPI_COMM_SELF,
+          shaped && !binomial, false, shaped && binomial, shaped && binomial, false);
+      const std::size_t nx[6] = {g.nx, g.nx + 1, g.nx + 1, g.nx + 1, g.nx, g.nx};
+      const std::size_t ny[6] = {g.ny + 1, g.ny, g.ny + 1, g.ny, g.ny + 1, g.ny};
+      const std::size_t nz[6] = {g.nz + 1, g.nz + 1, g.nz, g.nz, g.nz, g.nz + 1};
+      for (unsigned c = 0; c < 6; ++c)
+        for (std::size_t k = 0; k < nz[c]; ++k)
+          for (std::size_t j = 0; j < ny[c]; ++j)
+            for (std::size_t i = 0; i < nx[c]; ++i)
+              tables[c][(k * ny[c] + j) * nx[c] + i] = ref.field(c, i, j, k);
+      const auto& rep = ref.report();
+      report[0] = rep.sourceCharge;
+      report[1] = rep.depositedCharge;
+      report[2] = rep.minimumPivot;
+      report[3] = rep.minimumModeEigenvalue;
+    }
+    for (const char* name : {"/rho.bin", "/checkpoints.bin", "/phi.bin", "/metadata.txt"})
+      (void)::unlink((dir + name).c_str());
+    (void)::rmdir(dir.c_str());
+  });
+}
+
 aprl_status ref_run_initialize_self_field(ref_run* r, const aprl_self_field_config* c,
                                           aprl_self_field_report* out) {
   return guarded([&] {

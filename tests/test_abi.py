@@ -28,11 +28,13 @@ def test_library_exports_every_declared_function():
 
 def test_abi_version_and_struct_layout():
     b = native.load()
-    assert b.fn["abi_version"]() == 2
+    assert b.fn["abi_version"]() == 3
     # Layout of the plain-data structs as the C compiler sees them.
     assert C.sizeof(abi.Magnet) == 8 + 3 * 8 + 10 * 8
     assert abi.RunConfig.magnets.offset % 8 == 0
     assert C.sizeof(abi.StepStats) % 8 == 0
+    assert C.sizeof(abi.SelfFieldConfig) == 4 * 4 + 3 * 8 + 3 * 8 + 2 * 4
+    assert abi.SelfFieldConfig.source_shape.offset == 64
 
 
 def test_cowan_coefficients_need_no_device():

@@ -3,13 +3,15 @@
 The reference prepares its inlet supply with BlockedCowanReference, a modal
 solve of the Cowan relativistic Poisson problem on the whole reference grid
 that its own check holds to the Cowan initializer on the same grid within
-the CG tolerance (verification/blocked_cowan_reference_checks.cpp:61-130);
-its translation unit needs FFTW and is not built here.  The GPU path runs the
-initializer itself on the reference grid.  Its tables must equal the
-oracle's initializer on that grid (pinned bit for bit to the reference's
-EBGaussFieldInitializer, tests/test_self_field.py) to the tolerance of the
-self-field tests, and a run stepping on them must follow the oracle stepping
-on the oracle's tables.
+the CG tolerance (verification/blocked_cowan_reference_checks.cpp:61-130).
+Its translation unit is built into oracle/_ref over a stand-in for the three
+FFTW calls it makes (oracle/ref/fftw_shim: the type-I sine transform by
+direct sums), so the oracle's initializer is held to the reference's own
+blocked solve here, with the CIC source and with the shaped source the
+moving window uses (the run's shape).  The GPU path runs the initializer
+(CG or the same modal solve) on the reference grid; its tables must equal
+the oracle's to the tolerance of the self-field tests, and a run stepping on
+them must follow the oracle stepping on the oracle's tables.
 """
 import numpy as np
 import pytest
@@ -37,12 +39,46 @@ def reference_grid(cfg):
     return big
 
 
-def oracle_tables(w):
+def oracle_tables(w, source_shape="cic"):
     big = reference_grid(w.config)
     run = native.Run(checkers.oracle(), big)
     run.set_particles(w.particles)
-    report = run.initialize_self_field(abi.self_field_config(big))
+    report = run.initialize_self_field(abi.self_field_config(big, source_shape=source_shape))
     return [run.get_field(a) for a in range(6)], report
+
+
+def blocked_tables(w, report, shaped, directory):
+    """The reference's own BlockedCowanReference on the same reference grid,
+    with the initializer's mean beta_z and guards (as the moving window
+    prepares it, src/simulation_moving_window.cpp:145-148)."""
+    big = reference_grid(w.config)
+    sf = abi.self_field_config(big)
+    return checkers.blocked_reference(w.config, w.particles, report["mean_beta_z"],
+                                      [sf.guard_cells[a] for a in range(3)], 8, shaped,
+                                      str(directory))
+
+
+def support_touching_case(shape):
+    """The covering case with one particle whose shaped support reaches a
+    zero-potential face while its CIC support stays inside: the binomial3
+    x weights (nodes floor(x)-1 ..) reach the face x = guard, the quintic
+    z basis (nodes floor(z)-5 ..) the lower z face."""
+    w = covering_case()
+    cfg = w.config
+    cfg.shape = shape
+    w.particles = dict(w.particles)
+    if shape == abi.SHAPE_LINEAR_BINOMIAL3:
+        x = np.array(w.particles["x"], dtype=np.float64)
+        x[0] = cfg.reference_origin[0] + (cfg.cpml_cells_x + 1.5) * cfg.dx
+        w.particles["x"] = x
+    else:
+        z = np.array(w.particles["z"], dtype=np.float64)
+        z[0] = cfg.reference_origin[2] + 3.5 * cfg.dz
+        w.particles["z"] = z
+    return w
+
+
+SHAPES = [abi.SHAPE_LINEAR_BINOMIAL3, abi.SHAPE_QUINTIC_COMPENSATED]
 
 
 def test_reference_grid_holds_the_window():
@@ -73,3 +109,82 @@ def test_gpu_prepared_reference_matches_the_oracle_and_steps():
     for a in range(6):
         assert checkers.max_relative(g.get_field(a), o.get_field(a)) <= BOUND
     assert g.stats()["particles"] == o.stats()["particles"]
+
+
+@pytest.mark.skipif(not checkers.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("source", ["cic", "run-shape"])
+def test_oracle_prepared_reference_matches_the_references_blocked_solve(shape, source, tmp_path):
+    """The reference's BlockedCowanReference (its deposit, sine-mode and
+    Thomas solve and native E/B, built over the FFTW stand-in) against the
+    oracle's initializer with the same source, to the CG tolerance as the
+    reference's own check holds them (verification/
+    blocked_cowan_reference_checks.cpp:61-130)."""
+    w = covering_case()
+    w.config.shape = shape
+    tables, report = oracle_tables(w, source)
+    directory = tmp_path / "blocked"
+    blocked, summary = blocked_tables(w, report, source != "cic", directory)
+    for a in range(6):
+        assert checkers.max_relative(blocked[a], tables[a]) <= BOUND, a
+    assert summary[2] > 0.0 and summary[3] > 0.0  # positive Thomas pivots and modes
+    assert abs(summary[1] - summary[0]) <= 1e-12 * abs(summary[0])  # charge conserved
+    assert not directory.exists()
+
+
+@pytest.mark.skipif(not checkers.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("shape", SHAPES)
+def test_shaped_source_touching_the_guard_is_refused_like_the_reference(shape, tmp_path):
+    w = support_touching_case(shape)
+    big = reference_grid(w.config)
+    run = native.Run(checkers.oracle(), big)
+    run.set_particles(w.particles)
+    with pytest.raises(native.AprlError) as oracle_error:
+        run.initialize_self_field(abi.self_field_config(big, source_shape="run-shape"))
+    with pytest.raises(native.AprlError) as reference_error:
+        blocked_tables(w, {"mean_beta_z": 0.5}, True, tmp_path / "blocked")
+    for e in (oracle_error.value, reference_error.value):
+        assert e.status == abi.APRL_ERR_INVALID_ARGUMENT
+        assert e.message.startswith("Reference charge support touches Dirichlet surface")
+    # the CIC source of the same bunch stays inside the box
+    run.initialize_self_field(abi.self_field_config(big))
+
+
+def test_shaped_source_has_no_cpml_padding():
+    w = covering_case()
+    big = reference_grid(w.config)
+    run = native.Run(checkers.oracle(), big)
+    run.set_particles(w.particles)
+    with pytest.raises(native.AprlError) as e:
+        run.initialize_self_field(abi.self_field_config(
+            big, source_shape="run-shape", include_transverse_cpml_particles=True))
+    assert e.value.status == abi.APRL_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("solver", ["cg", "modal"])
+def test_gpu_shaped_prepared_reference_matches_the_oracle(shape, solver):
+    w = covering_case()
+    cfg = w.config
+    cfg.shape = shape
+    tables, expected = oracle_tables(w, "run-shape")
+    g = native.Run(native.load(), cfg)
+    g.set_particles(w.particles)
+    g.prepare_reference(w.particles, abi.self_field_config(cfg, solver=solver,
+                                                           source_shape="run-shape"))
+    for a in range(6):
+        assert checkers.max_relative(g.get_reference(a), tables[a]) <= BOUND, a
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", SHAPES)
+def test_gpu_shaped_source_touching_the_guard_is_refused(shape):
+    w = support_touching_case(shape)
+    g = native.Run(native.load(), w.config)
+    g.set_particles(w.particles)
+    with pytest.raises(native.AprlError) as e:
+        g.prepare_reference(w.particles, abi.self_field_config(w.config,
+                                                               source_shape="run-shape"))
+    assert e.value.status == abi.APRL_ERR_INVALID_ARGUMENT
+    assert e.value.message.startswith("Reference charge support touches Dirichlet surface")
