@@ -195,7 +195,7 @@ class SelfFieldConfig(C.Structure):
         ("maximum_iterations", C.c_uint64),
         ("guard_cells", C.c_uint64 * 3),
         ("source_shape", C.c_int32),
-        ("reserved", C.c_int32),
+        ("open_transverse", C.c_int32),
     ]
 
 
@@ -227,15 +227,18 @@ def self_field_config(run_config, model="cowan-relativistic-poisson", tolerance=
                       maximum_iterations=20000, maximum_mean_transverse_beta=0.05,
                       include_transverse_cpml_particles=False,
                       hold_transverse_until_activation=False, solver="cg",
-                      source_shape="cic"):
+                      source_shape="cic", open_transverse=False):
     """The initializer controls with the CPML cells as the static guard;
     solver "cg" (the reference's initializer) or "modal" (transverse sine
     modes and a tridiagonal solve along z per mode); source_shape "cic"
     (the initializer's charge) or "run-shape" (the shaped source of the
-    moving window's prepared reference)."""
+    moving window's prepared reference); open_transverse: the potential
+    extends to the outer transverse faces, held there at the free-space
+    potential of the charge (needs solver "modal")."""
     c = SelfFieldConfig()
     c.solver = {"cg": 0, "modal": 1}[solver]
     c.source_shape = SOURCE_SHAPES[source_shape]
+    c.open_transverse = int(open_transverse)
     c.model = SELF_FIELD_MODELS[model]
     c.include_transverse_cpml_particles = int(include_transverse_cpml_particles)
     c.hold_transverse_until_activation = int(hold_transverse_until_activation)

@@ -63,7 +63,7 @@ enum Kernel : unsigned {
   kSfMoments, kSfFinish, kSfDeposit, kSfSource, kSfApply, kSfUpdate,
   kSfDirection, kSfSmooth, kSfElectric, kSfMagnetic, kSfClear, kSfGauss, kSfEnergy,
   kInletHalo, kInletCharge, kInletComplete, kRadixCount, kPermuteParticles,
-  kCurrentConvert, kFixedConvert, kChordDeposit, kSfModal, kSurfaceCurrent, kKernelCount
+  kCurrentConvert, kFixedConvert, kChordDeposit, kSfModal, kSurfaceCurrent, kSfOpen, kKernelCount
 };
 
 const char* kKernelNames[kKernelCount] = {
@@ -77,7 +77,7 @@ const char* kKernelNames[kKernelCount] = {
   "trial_verdict", "sf_moments", "sf_finish", "sf_deposit", "sf_source", "sf_apply",
   "sf_update", "sf_direction", "sf_smooth", "sf_electric", "sf_magnetic",
   "sf_clear", "sf_gauss", "sf_energy", "inlet_halo", "inlet_charge", "inlet_complete",
-  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit", "sf_modal", "surface_current"};
+  "radix_count", "permute_particles", "current_convert", "fixed_convert", "chord_deposit", "sf_modal", "surface_current", "sf_open"};
 
 const char* device_error_text(unsigned code) {
   switch (code) {
@@ -3140,9 +3140,11 @@ struct SfBuffers {
   DD *partial = nullptr, *out = nullptr;
   SfState* state = nullptr;
   unsigned long long* max_bits = nullptr;
+  double* side = nullptr;  // the open-transverse-wall table
   ~SfBuffers() {
     for (double* p : slab) device_free(r, p);
     device_free(r, rho);
+    device_free(r, side);
     device_free(r, partial);
     device_free(r, out);
     device_free(r, state);
@@ -3153,6 +3155,200 @@ struct SfBuffers {
 aprl_status sf_read(aprl_run* r, const DD* device, DD* host, int count) {
   CUDA_TRY(cudaMemcpyAsync(host, device, count * sizeof(DD), cudaMemcpyDeviceToHost, r->stream));
   CUDA_TRY(cudaStreamSynchronize(r->stream));
+  return APRL_OK;
+}
+
+// The free-space potential of the open-wall sources at a batch of targets
+// (coordinates relative to the grid origin, z stretched), on the GPU.
+struct OpenSources {
+  aprl_run* r;
+  long long count = 0;
+  double* device = nullptr;  // x, y, z, q, each `count` long
+  ~OpenSources() { device_free(r, device); }
+
+  aprl_status potential(const std::vector<double>& tx, const std::vector<double>& ty,
+                        const std::vector<double>& tz, std::vector<double>& out) {
+    const size_t n = tx.size();
+    out.assign(n, 0.0);
+    if (n == 0) return APRL_OK;
+    double* t = nullptr;
+    TRY(device_alloc(r, &t, 4 * n));
+    aprl_status s = APRL_OK;
+    if (run_copy(r, t, tx.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        run_copy(r, t + n, ty.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        run_copy(r, t + 2 * n, tz.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      s = fail(APRL_ERR_CUDA, "cudaMemcpyAsync failed");
+    if (s == APRL_OK)
+      s = launch(r, kSfOpen, sf_coulomb_kernel, dim3((unsigned)std::min<size_t>(n, 1u << 20)),
+                 dim3(256), (const double*)t, (const double*)(t + n),
+                 (const double*)(t + 2 * n), (long long)n, (const double*)device,
+                 (const double*)(device + count), (const double*)(device + 2 * count),
+                 (const double*)(device + 3 * count), count, t + 3 * n);
+    if (s == APRL_OK &&
+        (run_copy(r, out.data(), t + 3 * n, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+         cudaStreamSynchronize(r->stream) != cudaSuccess))
+      s = fail(APRL_ERR_CUDA, "open-wall potential read-back failed");
+    device_free(r, t);
+    return s;
+  }
+};
+
+// OpenTransverseTrace's 8-point Lagrange interpolation of a coarse table
+// (src/open_transverse_trace.h:214-232), weights formed as the reference does.
+struct OpenInterpolation {
+  int first = 0;
+  double w[8] = {};
+  double eval(const double* v, int stride) const {
+    double sum = 0.;
+    for (int j = 0; j < 8; ++j) sum += w[j] * v[(first + j) * stride];
+    return sum;
+  }
+};
+
+std::vector<OpenInterpolation> open_weights(int count, int stride, int coarse) {
+  std::vector<OpenInterpolation> out(count);
+  for (int i = 0; i < count; ++i) {
+    const double x = double(i) / stride + 3.;
+    OpenInterpolation& s = out[i];
+    s.first = std::max(0, std::min(coarse - 8, int(x) - 3));
+    for (int j = 0; j < 8; ++j) {
+      double v = 1.;
+      for (int l = 0; l < 8; ++l)
+        if (l != j) v *= (x - (s.first + l)) / (j - l);
+      s.w[j] = v;
+    }
+  }
+  return out;
+}
+
+// The open-transverse-wall table (OpenTransverseTrace::build,
+// src/open_transverse_trace.h:65-190) of the charge in `rho` (an unpadded
+// (nx+1) x (ny+1) x (nz+1) vertex lattice, charge per volume), with the
+// sources of BlockedCowanReference::openSources (src/blocked_cowan_reference.cpp:
+// 662-681): every nonzero interior vertex, at (i dx, j dy, k dz gamma) with
+// charge rho gamma dx dy dz / (4 pi eps0), gamma = 1/sqrt(1 - translation).
+// For each of the eight faces (x = -dx, 0, nx dx, (nx+1) dx, then in y) the
+// potential is sampled on a coarse grid, interpolated to the native nodes,
+// compared with direct sums at 99 points, and evaluated directly at every
+// native node where the interpolation misses by more than 2e-7.  The
+// potential sums run on the GPU; the rest is the reference's host logic.
+aprl_status open_wall_trace(aprl_run* r, const aprl_run_config& c, const double* rho_device,
+                            double translation, const uint64_t guards[3],
+                            std::vector<double>& values) {
+  const int nx = (int)c.nx, ny = (int)c.ny, nz = (int)c.nz;
+  const size_t lx = c.nx + 1, ly = c.ny + 1;
+  std::vector<double> rho(lx * ly * (c.nz + 1));
+  CUDA_TRY(run_copy(r, rho.data(), rho_device, rho.size() * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaStreamSynchronize(r->stream));
+  const double gamma = 1. / std::sqrt(1. - translation);
+  const double scale = gamma * c.dx * c.dy * c.dz / (4. * std::acos(-1.) * kEpsilon0);
+  std::vector<double> sx, sy, sz, sq;
+  for (int k = 1; k < nz; ++k)
+    for (int j = 1; j < ny; ++j)
+      for (int i = 1; i < nx; ++i) {
+        const double density = rho[((size_t)k * ly + j) * lx + i];
+        if (density == 0.) continue;
+        if (i <= (int)guards[0] || i >= nx - (int)guards[0] || j <= (int)guards[1] ||
+            j >= ny - (int)guards[1])
+          return fail(APRL_ERR_RUNTIME, "Open reference charge overlaps original deposition guard");
+        sx.push_back(i * c.dx);
+        sy.push_back(j * c.dy);
+        sz.push_back(k * c.dz * gamma);
+        sq.push_back(density * scale);
+      }
+  const size_t width = 4 * ((size_t)nx + 3 + ny + 3);
+  values.assign(width * (c.nz + 1), 0.);
+  if (sq.empty()) return APRL_OK;
+  if (!(gamma > 0.) || !std::isfinite(gamma))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Invalid open trace gamma");
+  for (size_t s = 0; s < sq.size(); ++s)
+    if (!std::isfinite(sx[s]) || !std::isfinite(sy[s]) || !std::isfinite(sz[s]) ||
+        !std::isfinite(sq[s]))
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Nonfinite open trace source");
+  OpenSources src{r};
+  src.count = (long long)sq.size();
+  TRY(device_alloc(r, &src.device, 4 * sq.size()));
+  const std::vector<double>* columns[4] = {&sx, &sy, &sz, &sq};
+  for (int a = 0; a < 4; ++a)
+    CUDA_TRY(run_copy(r, src.device + a * sq.size(), columns[a]->data(), sq.size() * 8,
+                      cudaMemcpyHostToDevice));
+  const double hz = c.dz * gamma;
+  std::vector<double> tx, ty, tz, coarse, rows, exact, native;
+  for (int tile = 0; tile < 8; ++tile) {
+    const bool fixed_x = tile < 4;
+    const int t = tile % 4;
+    const int n = fixed_x ? nx : ny, ns = fixed_x ? ny : nx;
+    const double hf = fixed_x ? c.dx : c.dy, hs = fixed_x ? c.dy : c.dx;
+    const double fixed = (t < 2 ? t - 1 : n + t - 2) * hf;
+    const std::vector<double>& coords = fixed_x ? sx : sy;
+    const auto extremes = std::minmax_element(coords.begin(), coords.end());
+    const double dist = t < 2 ? *extremes.first - fixed : fixed - *extremes.second;
+    if (!(dist > 0.))
+      return fail(APRL_ERR_INVALID_ARGUMENT, "Beam support must be inside each open outer face");
+    // about 13 samples per closest-source distance, or every native node
+    const int ds = std::max(1, static_cast<int>(std::min(0.075 * dist / hs, (ns + 2) / 7.)));
+    const int dz = std::max(1, static_cast<int>(std::min(0.075 * dist / hz, nz / 7.)));
+    const int cs = (ns + 2 + ds - 1) / ds + 8, cz = (nz + dz - 1) / dz + 8;
+    const auto place = [&](double tangent, double z) {
+      tx.push_back(fixed_x ? fixed : tangent);
+      ty.push_back(fixed_x ? tangent : fixed);
+      tz.push_back(z);
+    };
+    tx.clear(), ty.clear(), tz.clear();
+    for (int k = 0; k < cz; ++k)
+      for (int p = 0; p < cs; ++p) place(((p - 3) * ds - 1) * hs, (k - 3) * dz * hz);
+    TRY(src.potential(tx, ty, tz, coarse));
+    const size_t offset = fixed_x ? (size_t)t * (ny + 3) : 4 * ((size_t)ny + 3) + (size_t)t * (nx + 3);
+    const auto sp = open_weights(ns + 3, ds, cs), zp = open_weights(nz + 1, dz, cz);
+    rows.assign((size_t)(ns + 3) * cz, 0.);
+    for (int k = 0; k < cz; ++k)
+      for (int p = 0; p < ns + 3; ++p) rows[(size_t)k * (ns + 3) + p] = sp[p].eval(&coarse[(size_t)k * cs], 1);
+    for (int k = 1; k < nz; ++k)
+      for (int p = 0; p < ns + 3; ++p)
+        values[(size_t)k * width + offset + p] = zp[k].eval(&rows[p], ns + 3);
+    // direct checks away from the interpolation nodes, near sources too
+    const auto zlimits = std::minmax_element(sz.begin(), sz.end());
+    const std::vector<double>& other = fixed_x ? sy : sx;
+    const auto slimits = std::minmax_element(other.begin(), other.end());
+    const auto check_index = [&](int a, int b, int& k, int& p) {
+      const double znear = (*zlimits.first + *zlimits.second) * 0.5 / hz;
+      const double snear = (*slimits.first + *slimits.second) * 0.5 / hs;
+      k = a < 7 ? int(znear + (a - 3) * dist / (3. * hz) + 0.4 * dz) : int((a - 6.4) * nz / 4.2);
+      p = b < 5 ? int(snear + (b - 2) * dist / (3. * hs) + 0.35 * ds) + 1
+                : int((b - 4.6) * (ns + 2) / 3.6);
+      k = std::max(1, std::min(nz - 1, k));
+      p = std::max(0, std::min(ns + 2, p));
+    };
+    tx.clear(), ty.clear(), tz.clear();
+    for (int index = 0; index < 99; ++index) {
+      int k, p;
+      check_index(index / 9, index % 9, k, p);
+      place((p - 1) * hs, k * hz);
+    }
+    TRY(src.potential(tx, ty, tz, exact));
+    double tile_error = 0.;
+    for (int a = 0; a < 11; ++a)
+      for (int b = 0; b < 9; ++b) {
+        int k, p;
+        check_index(a, b, k, p);
+        const double want = exact[a * 9 + b], got = values[(size_t)k * width + offset + p];
+        if (!std::isfinite(want) || !std::isfinite(got))
+          return fail(APRL_ERR_RUNTIME, "Nonfinite open wall trace");
+        if (want != 0.)
+          tile_error = std::max(tile_error, std::abs((got - want) / want));
+        else if (got != 0.)
+          tile_error = std::numeric_limits<double>::infinity();
+      }
+    if (tile_error > 2.e-7) {
+      tx.clear(), ty.clear(), tz.clear();
+      for (int k = 1; k < nz; ++k)
+        for (int p = 0; p < ns + 3; ++p) place((p - 1) * hs, k * hz);
+      TRY(src.potential(tx, ty, tz, native));
+      for (int k = 1; k < nz; ++k)
+        for (int p = 0; p < ns + 3; ++p)
+          values[(size_t)k * width + offset + p] = native[(size_t)(k - 1) * (ns + 3) + p];
+    }
+  }
   return APRL_OK;
 }
 
@@ -3184,6 +3380,17 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
   if (shaped && include)
     return fail(APRL_ERR_INVALID_ARGUMENT,
                 "The shaped reference source has no transverse CPML-source padding");
+  // The open-transverse-wall reference (BlockedCowanReference::configure,
+  // src/blocked_cowan_reference.cpp:314-329): its solve reaches the outer
+  // transverse faces, where the wall table holds the potential.
+  const bool open = cfg->open_transverse != 0;
+  if (open && (cfg->guard_cells[2] != 0 || cfg->guard_cells[0] == 0 || cfg->guard_cells[1] == 0))
+    return fail(APRL_ERR_INVALID_ARGUMENT, "Open transverse reference requires only transverse CPML");
+  if (open && (cfg->solver != APRL_SELF_FIELD_SOLVER_MODAL ||
+               cfg->model != APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON || include))
+    return fail(APRL_ERR_INVALID_ARGUMENT,
+                "The open transverse reference is the Cowan relativistic-Poisson modal solve "
+                "without transverse CPML-source padding");
   const bool cowan = cfg->model == APRL_SELF_FIELD_COWAN_RELATIVISTIC_POISSON;
   const bool relativistic = cfg->model == APRL_SELF_FIELD_RELATIVISTIC_POISSON || cowan;
   const int pad = include ? 2 : 0;
@@ -3197,7 +3404,7 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
                   "Initial static-field guard leaves fewer than two physical cells");
     physical_lo[a] = (int)cfg->guard_cells[a];
     physical_hi[a] = (int)(cells[a] - cfg->guard_cells[a]);
-    L.lo[a] = include && a < 2 ? 0 : (int)cfg->guard_cells[a];
+    L.lo[a] = (include || open) && a < 2 ? 0 : (int)cfg->guard_cells[a];
     L.hi[a] = (int)(pcells[a] - L.lo[a]);
   }
   L.lx = (int)pcells[0] + 1;
@@ -3392,6 +3599,15 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
                 "physical mesh padding");
   if (!(sums[1].hi > 0.0) || !std::isfinite(sums[1].hi))
     return fail(APRL_ERR_RUNTIME, "Initial particle charge produced an invalid Poisson source norm");
+  SfOpenSide side{nullptr, (int)c.nx, (int)c.ny, (int)c.nz,
+                  4 * ((long long)c.nx + 3 + (long long)c.ny + 3)};
+  if (open) {
+    std::vector<double> values;
+    TRY(open_wall_trace(r, c, buf.rho, A.translation, cfg->guard_cells, values));
+    TRY(device_alloc(r, &buf.side, values.size()));
+    CUDA_TRY(run_copy(r, buf.side, values.data(), values.size() * 8, cudaMemcpyHostToDevice));
+    side.values = buf.side;
+  }
 
   SfState state{};
   if (cfg->solver == APRL_SELF_FIELD_SOLVER_MODAL) {
@@ -3430,6 +3646,9 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
     double* work = A.residual;
     const unsigned blocks = blocks_for(count, 256);
     TRY(launch(r, kSfModal, sf_modal_gather_kernel, dim3(blocks), dim3(256), A, w0, ix, iy, iz));
+    if (open)
+      TRY(launch(r, kSfOpen, sf_open_lift_kernel, dim3(blocks), dim3(256), A, side, w0, ix, iy,
+                 iz));
     TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
                (const double*)w0, w1, (const double*)tx, 0, ix, iy, iz, 1.0));
     TRY(launch(r, kSfModal, sf_modal_transform_kernel, dim3(blocks), dim3(256),
@@ -3442,6 +3661,8 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
                (const double*)w1, w0, (const double*)tx, 0, ix, iy, iz, 2.0 / (ix + 1)));
     TRY(launch(r, kSfModal, sf_modal_scatter_kernel, dim3(blocks), dim3(256), A,
                (const double*)w0, ix, iy, iz));
+    if (open)
+      TRY(launch(r, kSfOpen, sf_open_wall_fill_kernel, dim3(64), dim3(256), A, side));
     device_free(r, tables);
     state.done = 1;
     rep->iterations = 0;
@@ -3482,6 +3703,8 @@ aprl_status aprl_run_initialize_self_field(aprl_run* r, const aprl_self_field_co
     for (int axis = 0; axis < 3; ++axis) {
       CUDA_TRY(cudaMemsetAsync(A.image, 0, slab * sizeof(double), r->stream));
       TRY(launch(r, kSfSmooth, sf_smooth_kernel, tile_grid, tile_block, A, axis));
+      if (open)
+        TRY(launch(r, kSfOpen, sf_open_wall_smooth_kernel, dim3(64), dim3(256), A, side, axis));
       TRY(launch(r, kSfElectric, sf_electric_kernel, dim3(fblocks), dim3(256), A, axis, 1.0, 1));
     }
   } else {

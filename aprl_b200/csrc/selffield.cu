@@ -430,6 +430,130 @@ __global__ void sf_smooth_kernel(SfArgs a, int axis) {
   }
 }
 
+// ---- the open-transverse-wall reference ----------------------------------
+// OpenTransverseTrace::at (src/open_transverse_trace.h:52-58): zero on the
+// longitudinal end planes; a point with x on or outside a face in x reads
+// that face's row (corners included), else the face in y.
+__device__ __forceinline__ double open_at(const SfOpenSide& s, int i, int j, int k) {
+  if (k <= 0 || k >= s.nz) return 0.0;
+  const int tx = i <= 0 ? i + 1 : (i >= s.nx ? i - s.nx + 2 : -1);
+  if (tx >= 0) return s.values[(long long)k * s.width + tx * (s.ny + 3) + j + 1];
+  const int ty = j <= 0 ? j + 1 : j - s.ny + 2;
+  return s.values[(long long)k * s.width + 4 * (s.ny + 3) + ty * (s.nx + 3) + i + 1];
+}
+
+// OpenTransverseTrace::Sources::potential (src/open_transverse_trace.h:25-34)
+// at each target: a block per target, its threads over the sources, then a
+// block sum (another summation order than the reference's loop).
+__global__ void __launch_bounds__(256) sf_coulomb_kernel(const double* tx, const double* ty,
+                                                         const double* tz, long long targets,
+                                                         const double* sx, const double* sy,
+                                                         const double* sz, const double* sq,
+                                                         long long sources, double* out) {
+  __shared__ double warp_sums[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long t = blockIdx.x; t < targets; t += gridDim.x) {
+    const double x = tx[t], y = ty[t], z = tz[t];
+    double sum = 0.0;
+    for (long long s = threadIdx.x; s < sources; s += blockDim.x) {
+      const double dx = x - sx[s], dy = y - sy[s], dz = z - sz[s];
+      sum += sq[s] / sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) warp_sums[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += warp_sums[w];
+      out[t] = total;
+    }
+    __syncthreads();
+  }
+}
+
+// BlockedCowanReference::liftOpenSides (src/blocked_cowan_reference.cpp:
+// 694-706) on the compact interior array of the modal solve (x fastest,
+// vertices lo+1 .. hi-1 with the transverse lo = 0): each node next to a
+// face subtracts the sum of the elliptic stencil's weights times the face
+// potentials it reaches, summed over dz, dy, dx as the reference does.
+__global__ void sf_open_lift_kernel(SfArgs a, SfOpenSide side, double* rhs, int ix, int iy,
+                                    int iz) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (long long)ix * iy * iz) return;
+  const SfLattice& L = a.L;
+  const int i = L.lo[0] + 1 + (int)(n % ix), j = L.lo[1] + 1 + (int)((n / ix) % iy),
+            k = L.lo[2] + 1 + (int)(n / ((long long)ix * iy));
+  if (!(i == 1 || i == side.nx - 1 || j == 1 || j == side.ny - 1)) return;
+  double value = 0.0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = i + dx, y = j + dy;
+        if (x == 0 || x == side.nx || y == 0 || y == side.ny)
+          value += a.stencil[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] * open_at(side, x, y, k + dz);
+      }
+  rhs[n] -= value;
+}
+
+// The face node m of a plane: x faces first (j = 0 .. ny at i = 0, then at
+// i = nx), then the y faces' inner nodes (i = 1 .. nx-1 at j = 0, then ny).
+__device__ __forceinline__ void open_face_node(const SfOpenSide& s, int m, int& i, int& j) {
+  if (m < 2 * (s.ny + 1)) {
+    i = m < s.ny + 1 ? 0 : s.nx;
+    j = m % (s.ny + 1);
+  } else {
+    m -= 2 * (s.ny + 1);
+    j = m < s.nx - 1 ? 0 : s.ny;
+    i = 1 + m % (s.nx - 1);
+  }
+}
+
+// The face potentials of planes 1 .. nz-1 into the potential lattice
+// (ensureField's phi fill, src/blocked_cowan_reference.cpp:872-877).
+__global__ void sf_open_wall_fill_kernel(SfArgs a, SfOpenSide side) {
+  const int per = 2 * (side.ny + 1) + 2 * (side.nx - 1);
+  const long long count = (long long)per * (side.nz - 1);
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int k = 1 + (int)(n / per);
+    int i, j;
+    open_face_node(side, (int)(n % per), i, j);
+    a.potential[sf_at(a.L, i, j, k + 1)] = open_at(side, i, j, k);
+  }
+}
+
+// smoothOnWall (src/blocked_cowan_reference.cpp:842-858) at the face nodes of
+// planes 1 .. nz-1: the nine transverse-plane terms in the reference's order
+// (a outer, b inner), the face table for every point on or outside a face,
+// minus the translation term on the longitudinal axis.
+__global__ void sf_open_wall_smooth_kernel(SfArgs a, SfOpenSide side, int axis) {
+  const int ta = (axis + 1) % 3, tb = (axis + 2) % 3;
+  const int per = 2 * (side.ny + 1) + 2 * (side.nx - 1);
+  const long long count = (long long)per * (side.nz - 1);
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < count;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int k = 1 + (int)(n / per);
+    int i, j;
+    open_face_node(side, (int)(n % per), i, j);
+    double value = 0.0;
+    for (int u = -1; u <= 1; ++u)
+      for (int v = -1; v <= 1; ++v) {
+        int d[3] = {0, 0, 0};
+        d[ta] = u;
+        d[tb] = v;
+        const int x = i + d[0], y = j + d[1], z = k + d[2];
+        const double p = (x <= 0 || y <= 0 || x >= side.nx || y >= side.ny)
+                             ? open_at(side, x, y, z)
+                             : a.potential[sf_at(a.L, x, y, z + 1)];
+        const double w = u == 0 ? (v == 0 ? a.alpha[axis] : a.beta[tb])
+                                : (v == 0 ? a.beta[ta] : a.delta[axis]);
+        value += w * p;
+      }
+    a.image[sf_at(a.L, i, j, k + 1)] =
+        value - (axis == 2 ? a.translation * open_at(side, i, j, k) : 0.0);
+  }
+}
+
 // One E component from the potential (or its smoothed form) by a forward
 // difference, E = -(coefficient * difference) / spacing
 // (fieldsFromPotential and fieldsFromCowanPotential,

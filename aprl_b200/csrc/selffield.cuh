@@ -101,6 +101,28 @@ __global__ void sf_modal_transform_kernel(const double* in, double* out, const d
 __global__ void sf_modal_z_kernel(SfArgs a, double* data, double* work, const double* cos_x,
                                   const double* cos_y, int ix, int iy, int iz);
 
+// The open-transverse-wall reference (src/open_transverse_trace.h:20-235):
+// the wall table in OpenTransverseTrace's layout, width = 4 (nx+3+ny+3)
+// values per plane: the faces x = -dx, 0, nx dx, (nx+1) dx (ny+3 values
+// each, j = -1 .. ny+1), then the faces in y (nx+3 values each).
+struct SfOpenSide {
+  const double* values;
+  int nx, ny, nz;
+  long long width;
+};
+// Free-space potential sum_s q_s / |t - s| at each target (one block each).
+__global__ void sf_coulomb_kernel(const double* tx, const double* ty, const double* tz,
+                                  long long targets, const double* sx, const double* sy,
+                                  const double* sz, const double* sq, long long sources,
+                                  double* out);
+// liftOpenSides: the compact modal right-hand side minus the stencil's wall terms.
+__global__ void sf_open_lift_kernel(SfArgs a, SfOpenSide side, double* rhs, int ix, int iy,
+                                    int iz);
+// The wall potentials into the potential lattice (interior planes).
+__global__ void sf_open_wall_fill_kernel(SfArgs a, SfOpenSide side);
+// smoothOnWall: the Cowan smoothing of `axis` at the wall nodes into image.
+__global__ void sf_open_wall_smooth_kernel(SfArgs a, SfOpenSide side, int axis);
+
 // Host helpers: the double-double quotient and square root rounded to binary64.
 double sf_ratio(DD a, DD b);
 long double sf_long(DD a);

@@ -537,7 +537,17 @@ typedef struct {
   uint64_t maximum_iterations;
   uint64_t guard_cells[3];            /* staticFieldGuardCells: the CPML cells per axis */
   int32_t source_shape;               /* aprl_source_shape */
-  int32_t reserved;                   /* zero */
+  /* Nonzero: the open-transverse-wall reference (BlockedCowanReference with
+   * openTransverse, src/blocked_cowan_reference.cpp:662-701, src/
+   * open_transverse_trace.h:20-190; mesh.moving_window.open_transverse_reference).
+   * The potential extends through the transverse CPML to the outer faces,
+   * where it takes the free-space Coulomb potential of the deposited charge
+   * (sampled coarsely and interpolated, checked against direct sums, direct
+   * everywhere where the check fails), lifted into the solve and used by
+   * the field reconstruction at the faces.  guard_cells must be the CPML
+   * cells in x and y and 0 in z, the solver MODAL, and
+   * include_transverse_cpml_particles 0. */
+  int32_t open_transverse;
 } aprl_self_field_config;
 
 /* EBGaussInitializationReport (src/eb_initial_field.h:17-34). */

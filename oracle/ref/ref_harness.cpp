@@ -1058,15 +1058,18 @@ aprl_status ref_run_energy_ledger(ref_run* r, aprl_energy_ledger* out) {
 // shape as the moving window prepares its reference
 // (src/simulation_moving_window.cpp:145-148 with src/config.cpp:1084-1112):
 // linear-binomial3 in z with the binomial3 transverse x weights, or the
-// quintic-compensated node basis in z.  `directory` must not exist: the
-// reference creates it, and its files are removed afterwards.  report:
-// source charge, deposited charge, minimum Thomas pivot, minimum mode
-// eigenvalue.
+// quintic-compensated node basis in z.  open: the open-transverse-wall
+// variant (openTransverse; guards must then be the CPML cells in x and y and
+// 0 in z).  `directory` must not exist: the reference creates it, and its
+// files are removed afterwards.  report: source charge, deposited charge,
+// minimum Thomas pivot, minimum mode eigenvalue, and for the open variant
+// the wall table's largest checked interpolation error and its fallback
+// tiles.
 aprl_status ref_blocked_reference(const aprl_run_config* config, size_t n, const double* x,
                                   const double* y, const double* z, const double* charge,
                                   double beta, const uint64_t guards[3], uint64_t block_layers,
-                                  int shape, const char* directory, double* const tables[6],
-                                  double report[4]) {
+                                  int shape, int open, const char* directory,
+                                  double* const tables[6], double report[6]) {
   return guarded([&] {
     const EBGridGeometry g(config->nx, config->ny, config->reference_nz, config->dx, config->dy,
                            config->dz, config->dt, EBMaxwellSolver::CowanZ);
@@ -1087,7 +1090,7 @@ aprl_status ref_blocked_reference(const aprl_run_config* config, size_t n, const
     {
       verification::BlockedCowanReference ref(
           g, origin, particles, beta, guard, block_layers, dir, MPI_COMM_SELF,
-          shaped && !binomial, false, shaped && binomial, shaped && binomial, false);
+          shaped && !binomial, false, shaped && binomial, shaped && binomial, open != 0);
       const std::size_t nx[6] = {g.nx, g.nx + 1, g.nx + 1, g.nx + 1, g.nx, g.nx};
       const std::size_t ny[6] = {g.ny + 1, g.ny, g.ny + 1, g.ny, g.ny + 1, g.ny};
       const std::size_t nz[6] = {g.nz + 1, g.nz + 1, g.nz, g.nz, g.nz, g.nz + 1};
@@ -1101,8 +1104,11 @@ aprl_status ref_blocked_reference(const aprl_run_config* config, size_t n, const
       report[1] = rep.depositedCharge;
       report[2] = rep.minimumPivot;
       report[3] = rep.minimumModeEigenvalue;
+      report[4] = rep.openTraceMaxRelativeError;
+      report[5] = (double)rep.openTraceFallbackTiles;
     }
-    for (const char* name : {"/rho.bin", "/checkpoints.bin", "/phi.bin", "/metadata.txt"})
+    for (const char* name :
+         {"/rho.bin", "/checkpoints.bin", "/phi.bin", "/metadata.txt", "/side-potential.bin"})
       (void)::unlink((dir + name).c_str());
     (void)::rmdir(dir.c_str());
   });

@@ -74,26 +74,30 @@ def reference():
         f = lib.ref_blocked_reference
         f.restype = C.c_int
         f.argtypes = [C.POINTER(abi.RunConfig), C.c_size_t] + [C.POINTER(C.c_double)] * 4 + \
-            [C.c_double, C.POINTER(C.c_uint64), C.c_uint64, C.c_int, C.c_char_p,
+            [C.c_double, C.POINTER(C.c_uint64), C.c_uint64, C.c_int, C.c_int, C.c_char_p,
              C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_double)]
     return _reference
 
 
-def blocked_reference(cfg, particles, beta, guards, block_layers, shaped, directory):
+def blocked_reference(cfg, particles, beta, guards, block_layers, shaped, directory,
+                      open_transverse=False):
     """The reference's own BlockedCowanReference (built over the FFTW
     stand-in) on cfg's reference grid: the six native tables and its report
     (source charge, deposited charge, minimum pivot, minimum mode
-    eigenvalue).  shaped: deposit with the run's own shape instead of CIC."""
+    eigenvalue, open-wall interpolation error, open-wall fallback tiles).
+    shaped: deposit with the run's own shape instead of CIC;
+    open_transverse: the open-transverse-wall variant."""
     lib = reference()
     n = len(particles["x"])
     cols = [np.ascontiguousarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "charge")]
     tables = [np.zeros(abi.reference_shape(cfg, a)[::-1]) for a in range(6)]
     ptrs = (C.POINTER(C.c_double) * 6)(*[t.ctypes.data_as(C.POINTER(C.c_double)) for t in tables])
     g = (C.c_uint64 * 3)(*guards)
-    report = (C.c_double * 4)()
+    report = (C.c_double * 6)()
     lib.check(lib.lib.ref_blocked_reference(
         C.byref(cfg), n, *[c.ctypes.data_as(C.POINTER(C.c_double)) for c in cols],
-        float(beta), g, int(block_layers), 1 if shaped else 0, directory.encode(), ptrs, report))
+        float(beta), g, int(block_layers), 1 if shaped else 0, 1 if open_transverse else 0,
+        directory.encode(), ptrs, report))
     return tables, list(report)
 
 

@@ -8,7 +8,8 @@ Its translation unit is built into oracle/_ref over a stand-in for the three
 FFTW calls it makes (oracle/ref/fftw_shim: the type-I sine transform by
 direct sums), so the oracle's initializer is held to the reference's own
 blocked solve here, with the CIC source and with the shaped source the
-moving window uses (the run's shape).  The GPU path runs the initializer
+moving window uses (the run's shape), and the GPU's open-transverse-wall
+reference is held to the reference's own open solve.  The GPU path runs the initializer
 (CG or the same modal solve) on the reference grid; its tables must equal
 the oracle's to the tolerance of the self-field tests, and a run stepping on
 them must follow the oracle stepping on the oracle's tables.
@@ -20,6 +21,10 @@ import checkers
 from aprl_b200 import abi, native, workloads
 
 BOUND = 1e-9
+# GPU against the reference's own open-wall solve: both are direct solves of
+# the same lifted problem (sine sums against FFTW's transform stand-in,
+# block sums against serial Coulomb sums), so only rounding separates them.
+OPEN_BOUND = 1e-11
 
 
 def covering_case():
@@ -47,7 +52,7 @@ def oracle_tables(w, source_shape="cic"):
     return [run.get_field(a) for a in range(6)], report
 
 
-def blocked_tables(w, report, shaped, directory):
+def blocked_tables(w, report, shaped, directory, open_transverse=False):
     """The reference's own BlockedCowanReference on the same reference grid,
     with the initializer's mean beta_z and guards (as the moving window
     prepares it, src/simulation_moving_window.cpp:145-148)."""
@@ -55,7 +60,18 @@ def blocked_tables(w, report, shaped, directory):
     sf = abi.self_field_config(big)
     return checkers.blocked_reference(w.config, w.particles, report["mean_beta_z"],
                                       [sf.guard_cells[a] for a in range(3)], 8, shaped,
-                                      str(directory))
+                                      str(directory), open_transverse=open_transverse)
+
+
+def wide_case():
+    """A 48 x 48 x 64 grid with the bunch near its axis: about 20 cells from
+    the outer transverse faces, the open-wall table is sampled on a coarse
+    grid and interpolated (the reference's checked error about 1e-11), not
+    evaluated at every node."""
+    w = workloads.self_field_case(8.84e6, nx=48, ny=48, nz=64, particles=2000)
+    w.config.reference_nz = w.config.initial_offset + w.config.nz + 4
+    w.reference = []
+    return w
 
 
 def support_touching_case(shape):
@@ -188,3 +204,61 @@ def test_gpu_shaped_source_touching_the_guard_is_refused(shape):
                                                                source_shape="run-shape"))
     assert e.value.status == abi.APRL_ERR_INVALID_ARGUMENT
     assert e.value.message.startswith("Reference charge support touches Dirichlet surface")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not checkers.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("source", ["cic", "run-shape"])
+def test_gpu_open_transverse_reference_matches_the_references_blocked_solve(shape, source,
+                                                                           tmp_path):
+    """The open-transverse-wall reference (mesh.moving_window.
+    open_transverse_reference): the GPU's wall table, lifted modal solve and
+    face smoothing against the reference's own BlockedCowanReference with
+    openTransverse on the same grid, source and beta."""
+    w = covering_case()
+    cfg = w.config
+    cfg.shape = shape
+    g = native.Run(native.load(), cfg)
+    g.set_particles(w.particles)
+    report = g.prepare_reference(w.particles, abi.self_field_config(
+        cfg, solver="modal", source_shape=source, open_transverse=True))
+    directory = tmp_path / "blocked"
+    blocked, summary = blocked_tables(w, report, source != "cic", directory, open_transverse=True)
+    for a in range(6):
+        assert checkers.max_relative(g.get_reference(a), blocked[a]) <= OPEN_BOUND, a
+    assert not directory.exists()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not checkers.reference_available(), reason="oracle/_ref not built")
+def test_gpu_open_transverse_reference_interpolated_wall_matches(tmp_path):
+    w = wide_case()
+    cfg = w.config
+    g = native.Run(native.load(), cfg)
+    g.set_particles(w.particles)
+    report = g.prepare_reference(w.particles, abi.self_field_config(
+        cfg, solver="modal", source_shape="run-shape", open_transverse=True))
+    blocked, summary = blocked_tables(w, report, True, tmp_path / "blocked",
+                                      open_transverse=True)
+    assert 0.0 < summary[4] < 2e-7 and summary[5] == 0  # interpolated, no direct fallback
+    for a in range(6):
+        assert checkers.max_relative(g.get_reference(a), blocked[a]) <= OPEN_BOUND, a
+
+
+@pytest.mark.gpu
+def test_gpu_open_transverse_reference_refuses_what_the_reference_refuses():
+    w = covering_case()
+    cfg = w.config
+    g = native.Run(native.load(), cfg)
+    g.set_particles(w.particles)
+    for kwargs in ({"solver": "cg"}, {"solver": "modal", "include_transverse_cpml_particles": True}):
+        with pytest.raises(native.AprlError) as e:
+            g.prepare_reference(w.particles, abi.self_field_config(cfg, open_transverse=True,
+                                                                   **kwargs))
+        assert e.value.status == abi.APRL_ERR_INVALID_ARGUMENT
+    c = abi.self_field_config(cfg, solver="modal", open_transverse=True)
+    c.guard_cells[2] = 1
+    with pytest.raises(native.AprlError) as e:
+        g.prepare_reference(w.particles, c)
+    assert e.value.message == "Open transverse reference requires only transverse CPML"
