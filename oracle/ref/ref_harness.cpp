@@ -29,6 +29,8 @@
 #include <vector>
 #include <unistd.h>
 
+#include <fstream>
+
 #include "aprl_gpu.h"
 #include "boostframe.h"
 #include "charge_matched_inlet.h"
@@ -665,13 +667,15 @@ aprl_status ref_run_preview_electric(ref_run* r) {
   });
 }
 
-// TransverseReferenceCurrent::prepare's file (src/transverse_reference_current.cpp:
-// 17-18, 29-33, 46-63) written from the in-memory reference tables: the
-// header, curl_z(B_ref)/mu0 at the points() targets for every reference
-// plane, and the completion marker; then the reference's class opens it.
-void prepare_surface(ref_run& r) {
-  if (r.surface) return;
-  const aprl_run_config& c = r.cfg;
+// TransverseReferenceCurrent::prepare's values (src/transverse_reference_current.cpp:
+// 19-27, 46-63) from in-memory Bx and By tables of a reference grid of
+// nz planes: curl_z(B_ref)/mu0 at the points() targets of every plane, plane
+// by plane.  prepare_surface writes them in the reference's file format;
+// ref_surface_current_pin holds them to the reference's own prepare.
+std::vector<double> surface_values(const aprl_run_config& c, std::size_t nz,
+                                   const std::vector<double>& bx, const std::size_t sx[3],
+                                   const std::vector<double>& by, const std::size_t sy[3],
+                                   std::size_t& count) {
   const std::size_t gx = c.cpml_cells_x, gy = c.cpml_cells_y;
   const std::size_t x0 = gx, x1 = c.nx - gx, y0 = gy, y1 = c.ny - gy;
   std::vector<std::pair<std::size_t, std::size_t>> target;
@@ -683,37 +687,44 @@ void prepare_surface(ref_run& r) {
     target.push_back({x0, j});
     target.push_back({x1, j});
   }
+  count = target.size();
+  std::vector<double> values(nz * count);
+  for (std::size_t k = 0; k < nz; ++k)
+    for (std::size_t p = 0; p < count; ++p) {
+      const std::size_t i = target[p].first, j = target[p].second;
+      const double dby = by.at((k * sy[1] + j) * sy[0] + i) - by.at((k * sy[1] + j) * sy[0] + i - 1);
+      const double dbx = bx.at((k * sx[1] + j) * sx[0] + i) - bx.at((k * sx[1] + j - 1) * sx[0] + i);
+      values[k * count + p] = (dby / c.dx - dbx / c.dy) / SI::mu0;
+      if (!std::isfinite(values[k * count + p]))
+        throw std::runtime_error("Nonfinite equivalent boundary current");
+    }
+  return values;
+}
+
+// The file of TransverseReferenceCurrent::prepare (header, the values, the
+// completion marker) written from the run's reference tables; then the
+// reference's class opens it.
+void prepare_surface(ref_run& r) {
+  if (r.surface) return;
+  const aprl_run_config& c = r.cfg;
+  const std::size_t gx = c.cpml_cells_x, gy = c.cpml_cells_y;
+  std::size_t count = 0;
+  const std::vector<double> values = surface_values(c, c.reference_nz, r.reference[3],
+                                                    r.referenceShape[3], r.reference[4],
+                                                    r.referenceShape[4], count);
   struct Header {
     std::uint64_t tag, version, nx, ny, nz, gx, gy, count;
     double dx, dy, dz, dt, beta;
   };
   const bool binomial3 = c.shape == APRL_SHAPE_LINEAR_BINOMIAL3;
   const Header h{0x4150524c53555246ULL, binomial3 ? 2ULL : 1ULL, c.nx, c.ny, c.reference_nz,
-                 gx, gy, target.size(), c.dx, c.dy, c.dz, c.dt, 0.0};
+                 gx, gy, count, c.dx, c.dy, c.dz, c.dt, 0.0};
   char name[] = "/tmp/aprl-surface-XXXXXX";
   const int fd = ::mkstemp(name);
   if (fd < 0) throw std::runtime_error("Cannot create reference surface-current file");
-  std::vector<double> values(target.size());
-  const auto& bx = r.reference[3];
-  const auto& by = r.reference[4];
-  const auto* sx = r.referenceShape[3];
-  const auto* sy = r.referenceShape[4];
   bool ok = ::write(fd, &h, sizeof h) == (ssize_t)sizeof h;
-  for (std::size_t k = 0; ok && k < c.reference_nz; ++k) {
-    for (std::size_t p = 0; p < target.size(); ++p) {
-      const std::size_t i = target[p].first, j = target[p].second;
-      const double dby = by.at((k * sy[1] + j) * sy[0] + i) - by.at((k * sy[1] + j) * sy[0] + i - 1);
-      const double dbx = bx.at((k * sx[1] + j) * sx[0] + i) - bx.at((k * sx[1] + j - 1) * sx[0] + i);
-      values[p] = (dby / c.dx - dbx / c.dy) / SI::mu0;
-      if (!std::isfinite(values[p])) {
-        ::close(fd);
-        ::unlink(name);
-        throw std::runtime_error("Nonfinite equivalent boundary current");
-      }
-    }
-    const ssize_t bytes = (ssize_t)(values.size() * sizeof(double));
-    ok = ::write(fd, values.data(), values.size() * sizeof(double)) == bytes;
-  }
+  const ssize_t bytes = (ssize_t)(values.size() * sizeof(double));
+  ok = ok && ::write(fd, values.data(), values.size() * sizeof(double)) == bytes;
   const std::uint64_t complete = 0x434f4d504c455445ULL;
   ok = ok && ::write(fd, &complete, sizeof complete) == (ssize_t)sizeof complete;
   ::close(fd);
@@ -1109,6 +1120,66 @@ aprl_status ref_blocked_reference(const aprl_run_config* config, size_t n, const
     }
     for (const char* name :
          {"/rho.bin", "/checkpoints.bin", "/phi.bin", "/metadata.txt", "/side-potential.bin"})
+      (void)::unlink((dir + name).c_str());
+    (void)::rmdir(dir.c_str());
+  });
+}
+
+// The reference's own TransverseReferenceCurrent::prepare
+// (src/transverse_reference_current.cpp:46-63) over its own
+// BlockedCowanReference of the bunch (shaped source, guards = the CPML
+// cells, as src/simulation_moving_window.cpp:145-157 prepares both), and the
+// values surface_values forms from that reference's Bx and By tables, each
+// `count` points per plane over reference_nz planes.
+aprl_status ref_surface_current_pin(const aprl_run_config* config, size_t n, const double* x,
+                                    const double* y, const double* z, const double* charge,
+                                    double beta, uint64_t block_layers, const char* directory,
+                                    double* from_reference, double* from_tables,
+                                    size_t capacity, size_t* count) {
+  return guarded([&] {
+    const EBGridGeometry g(config->nx, config->ny, config->reference_nz, config->dx, config->dy,
+                           config->dz, config->dt, EBMaxwellSolver::CowanZ);
+    Vec origin;
+    for (unsigned a = 0; a < 3; ++a) origin[a] = config->reference_origin[a];
+    std::vector<RelativisticParticleSI> particles(n);
+    for (size_t i = 0; i < n; ++i) {
+      particles[i].position[0] = x[i];
+      particles[i].position[1] = y[i];
+      particles[i].position[2] = z[i];
+      particles[i].charge = charge[i];
+      particles[i].id = i;
+    }
+    const bool binomial = config->shape == APRL_SHAPE_LINEAR_BINOMIAL3;
+    const std::size_t guard[3] = {config->cpml_cells_x, config->cpml_cells_y, 0};
+    const std::string dir(directory), file = dir + "/transverse-current.bin";
+    {
+      verification::BlockedCowanReference ref(g, origin, particles, beta, guard, block_layers,
+                                               dir, MPI_COMM_SELF, !binomial, false, binomial,
+                                               binomial, false);
+      TransverseReferenceCurrent::prepare(file, ref, g, guard, beta, binomial);
+      std::vector<double> bx, by;
+      const std::size_t sx[3] = {g.nx + 1, g.ny, g.nz}, sy[3] = {g.nx, g.ny + 1, g.nz};
+      bx.resize(sx[0] * sx[1] * sx[2]);
+      by.resize(sy[0] * sy[1] * sy[2]);
+      for (std::size_t k = 0; k < g.nz; ++k)
+        for (std::size_t j = 0; j < g.ny + 1; ++j)
+          for (std::size_t i = 0; i < g.nx + 1; ++i) {
+            if (j < g.ny) bx[(k * sx[1] + j) * sx[0] + i] = ref.field(3, i, j, k);
+            if (i < g.nx) by[(k * sy[1] + j) * sy[0] + i] = ref.field(4, i, j, k);
+          }
+      std::size_t points = 0;
+      const std::vector<double> mine = surface_values(*config, g.nz, bx, sx, by, sy, points);
+      *count = points;
+      if (mine.size() > capacity) throw std::invalid_argument("surface-current capacity too small");
+      std::copy(mine.begin(), mine.end(), from_tables);
+      // the reference's file: header (8 words + 5 doubles), values, marker
+      std::ifstream in(file, std::ios::binary);
+      in.seekg(13 * 8);
+      in.read(reinterpret_cast<char*>(from_reference), (std::streamsize)(mine.size() * 8));
+      if (!in) throw std::runtime_error("Cannot read the reference's surface-current file");
+    }
+    for (const char* name : {"/transverse-current.bin", "/rho.bin", "/checkpoints.bin",
+                             "/phi.bin", "/metadata.txt"})
       (void)::unlink((dir + name).c_str());
     (void)::rmdir(dir.c_str());
   });

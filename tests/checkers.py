@@ -76,7 +76,32 @@ def reference():
         f.argtypes = [C.POINTER(abi.RunConfig), C.c_size_t] + [C.POINTER(C.c_double)] * 4 + \
             [C.c_double, C.POINTER(C.c_uint64), C.c_uint64, C.c_int, C.c_int, C.c_char_p,
              C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_double)]
+        f = lib.ref_surface_current_pin
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(abi.RunConfig), C.c_size_t] + [C.POINTER(C.c_double)] * 4 + \
+            [C.c_double, C.c_uint64, C.c_char_p, C.POINTER(C.c_double),
+             C.POINTER(C.c_double), C.c_size_t, C.POINTER(C.c_size_t)]
     return _reference
+
+
+def surface_current_pin(cfg, particles, beta, directory):
+    """The equivalent surface current per reference plane and point from the
+    reference's own TransverseReferenceCurrent::prepare over its own
+    BlockedCowanReference, and from the harness's writer fed that
+    reference's Bx, By tables: (from_reference, from_tables), each
+    [plane][point]."""
+    lib = reference()
+    cols = [np.ascontiguousarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "charge")]
+    capacity = (cfg.reference_nz + 1) * 2 * (cfg.nx + cfg.ny + 2)
+    a = np.zeros(capacity)
+    b = np.zeros(capacity)
+    count = C.c_size_t()
+    lib.check(lib.lib.ref_surface_current_pin(
+        C.byref(cfg), len(cols[0]), *[c.ctypes.data_as(C.POINTER(C.c_double)) for c in cols],
+        float(beta), 8, directory.encode(), a.ctypes.data_as(C.POINTER(C.c_double)),
+        b.ctypes.data_as(C.POINTER(C.c_double)), capacity, C.byref(count)))
+    n = cfg.reference_nz * count.value
+    return a[:n].reshape(cfg.reference_nz, -1), b[:n].reshape(cfg.reference_nz, -1)
 
 
 def blocked_reference(cfg, particles, beta, guards, block_layers, shaped, directory,

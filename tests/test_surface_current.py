@@ -86,3 +86,22 @@ def test_gpu_refuses_a_reference_shorter_than_the_window():
         g.step(1)
     assert info.value.status == abi.APRL_ERR_OUT_OF_RANGE
     assert info.value.message.startswith("Reference surface-current query outside domain")
+
+
+@pytest.mark.skipif(not checkers.reference_available(),
+                    reason="reference translation units not built")
+@pytest.mark.parametrize("shape", SHAPES)
+def test_file_writer_matches_the_references_own_prepare(shape, tmp_path):
+    """The harness writes the prepared surface current from reference
+    tables; the reference's own TransverseReferenceCurrent::prepare reads
+    its BlockedCowanReference.  Over the same blocked reference of a bunch
+    (the run's shaped source, as the moving window prepares both) the two
+    give the same values bit for bit."""
+    import test_prepared_reference as prepared
+    w = prepared.covering_case()
+    w.config.shape = abi.SHAPES[shape]
+    reference, tables = checkers.surface_current_pin(w.config, w.particles, 0.5,
+                                                     str(tmp_path / "blocked"))
+    assert reference.shape == tables.shape and np.abs(reference).max() > 0.0
+    assert np.array_equal(reference, tables)
+    assert not (tmp_path / "blocked").exists()
