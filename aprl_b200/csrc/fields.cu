@@ -179,6 +179,10 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
   PlaneSlots ps = {{0, 1, 2}};
   load_plane(t, a, k0 - 1, ps.s[0], i0, j0);
   load_plane(t, a, k0, ps.s[1], i0, j0);
+  // The column's CPML slots are the same on every plane of the march.
+  const bool column = i <= g.nx && j <= g.ny;
+  const int slot_x = column && i < g.nx ? a.mx.ordinal[i] : -1;
+  const int slot_y = column && j < g.ny ? a.my.ordinal[j] : -1;
   for (int k = k0; k < k1; ++k) {
     load_plane(t, a, k + 1, ps.s[2], i0, j0);
     __syncthreads();
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
                              tile_smoothed(t, a, 1, 2, li, lj, 0, ps);
         double* bx = &g.b[0][b_index(g, 0, i, j, k)];
         double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
-        const int s = a.my.ordinal[j];
+        const int s = slot_y;
         if (s >= 0)
           v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
                                              history_at(a.h[0], s, k, g.zb_b[0], i, g.status));
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
                              tile_smoothed(t, a, 2, 0, li, lj, 0, ps);
         double* by = &g.b[1][b_index(g, 1, i, j, k)];
         double v = *by - (dtdz * dExDz - dtdx * dEzDx);
-        const int s = a.mx.ordinal[i];
+        const int s = slot_x;
         if (s >= 0)
           v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
                                             history_at(a.h[1], s, k, g.zb_b[1], j, g.status));
@@ -216,11 +220,11 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
                              tile_smoothed(t, a, 0, 1, li, lj, 0, ps);
         double* bz = &g.b[2][b_index(g, 2, i, j, k)];
         double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
-        const int sx = a.mx.ordinal[i];
+        const int sx = slot_x;
         if (sx >= 0)
           v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,
                                              history_at(a.h[2], sx, k, g.zb_b[2], j, g.status));
-        const int sy = a.my.ordinal[j];
+        const int sy = slot_y;
         if (sy >= 0)
           v += 1.0 * dtdy * cpml_correction(a.my, j, dExDy,
                                             history_at(a.h[3], sy, k, g.zb_b[2], i, g.status));

@@ -563,28 +563,42 @@ def other_configs(args, stream):
     """Device-resident step rates of the other single-GPU configurations,
     W warm-up and K timed steps each (CUDA events on the run's stream): the
     plain FP64 drift (64x64x256, 100k), the dipole workload with the
-    quintic-compensated shape, and the dipole workload in the bit-reproducible
-    current mode."""
+    quintic-compensated shape, in FP64 and FP32-mixed, the dipole workload
+    in the bit-reproducible current mode, and the planar-undulator workload
+    (128x128x2048, 4M, FP32-mixed, from its Cowan self-field, with the
+    energy ledger)."""
     import torch
     K, W = args.steps, args.warmup
+    quintic = lambda: workloads.dipole_c2(steps=W + K + 4, particles=args.particles,
+                                          shape="quintic-compensated", seed=17)
     cases = {
-        "drift_64x64x256_100k_binomial3_fp64": lambda: workloads.drift_c1(
-            steps=W + K + 4, particles=100_000, seed=17),
-        "dipole_128x128x512_1M_quintic_fp64": lambda: workloads.dipole_c2(
-            steps=W + K + 4, particles=args.particles, shape="quintic-compensated", seed=17),
-        "dipole_128x128x512_1M_binomial3_fp64_deterministic": lambda: workloads.dipole_c2(
-            steps=W + K + 4, particles=args.particles, seed=17),
+        "drift_64x64x256_100k_binomial3_fp64": (lambda: workloads.drift_c1(
+            steps=W + K + 4, particles=100_000, seed=17), {}),
+        "dipole_128x128x512_1M_quintic_fp64": (quintic, {}),
+        "dipole_128x128x512_1M_quintic_fp32_mixed": (quintic, {"precision": "fp32-mixed"}),
+        "dipole_128x128x512_1M_binomial3_fp64_deterministic": (lambda: workloads.dipole_c2(
+            steps=W + K + 4, particles=args.particles, seed=17), {"deterministic": True}),
+        "undulator_128x128x2048_4M_binomial3_fp32_mixed": (lambda: workloads.undulator_c3(
+            steps=W + K + 4, particles=4_000_000, seed=17, precision="fp32-mixed"),
+            {"self_field": True, "ledger": True}),
     }
     out = {}
     lib = native.load()
-    for name, make in cases.items():
+    for name, (make, options) in cases.items():
         w = make()
         cfg = w.config
-        if name.endswith("deterministic"):
+        if options.get("deterministic"):
             cfg = workloads.with_determinism(cfg)
+        if options.get("precision"):
+            cfg = workloads.with_precision(cfg, options["precision"])
         run = native.Run(lib, cfg, stream=stream.cuda_stream)
         run.set_reference(w.reference)
         run.set_particles(w.particles)
+        if options.get("self_field"):
+            run.initialize_self_field(abi.self_field_config(
+                cfg, hold_transverse_until_activation=True))
+        if options.get("ledger"):
+            run.enable_energy_ledger()
         for _ in range(W):
             run.step(1)
         run.synchronize()
@@ -606,6 +620,11 @@ def other_configs(args, stream):
                      "cells": list(w.description["cells"]),
                      "particles": int(w.particles["x"].size),
                      "fixed_point_trials_mean": stats["total_iterations"] / max(K, 1)}
+        if options.get("self_field"):
+            out[name]["initial_fields"] = "cowan-relativistic-poisson self-field"
+        if options.get("ledger"):
+            out[name]["energy_ledger"] = True
+        del w, run
     return out
 
 
