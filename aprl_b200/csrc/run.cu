@@ -370,6 +370,7 @@ struct aprl_run {
   double time = 0.0;
   double origin[3]{};
   int stage = 0;
+  bool step_open = false;  // aprl_run_step_begin without its aprl_run_step_end yet
   unsigned trials = 0;
   uint32_t last_iterations = 0, max_iterations = 0;
   uint64_t total_iterations = 0;
@@ -2722,31 +2723,45 @@ aprl_status aprl_run_set_carriers(aprl_run* r, size_t n, const double* pos, cons
   return APRL_OK;
 }
 
+// The seams and whole-step calls refuse to run inside a step opened with
+// aprl_run_step_begin: its trials are in flight and step_finish reads them.
+static aprl_status no_open_step(const aprl_run* r) {
+  if (r->step_open)
+    return fail(APRL_ERR_RUNTIME,
+                "A step begun with aprl_run_step_begin is open; end it with aprl_run_step_end");
+  return APRL_OK;
+}
+
 aprl_status aprl_run_advance_magnetic(aprl_run* r) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
   TRY(do_advance_magnetic(r));
   return check_device(r);
 }
 
 aprl_status aprl_run_preview_electric(aprl_run* r) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
   TRY(do_preview_electric(r));
   return check_device(r);
 }
 
 aprl_status aprl_run_coupling_trial(aprl_run* r, double residual[4]) {
   if (!r || !residual) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
+  TRY(no_open_step(r));
   return do_trial(r, residual);
 }
 
 aprl_status aprl_run_commit_electric(aprl_run* r) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
   TRY(do_commit(r));
   return check_device(r);
 }
 
 aprl_status aprl_run_shift(aprl_run* r) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
   return do_shift(r);
 }
 
@@ -2842,6 +2857,7 @@ extern "C" {
 
 aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
   if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
   for (uint32_t n = 0; n < steps; ++n) {
     TRY(step_enqueue(r));
     TRY(step_finish(r));
@@ -2849,11 +2865,30 @@ aprl_status aprl_run_step(aprl_run* r, uint32_t steps) {
   return check_device(r);
 }
 
+aprl_status aprl_run_step_begin(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  TRY(no_open_step(r));
+  TRY(step_enqueue(r));
+  r->step_open = true;
+  return APRL_OK;
+}
+
+aprl_status aprl_run_step_end(aprl_run* r) {
+  if (!r) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+  if (!r->step_open)
+    return fail(APRL_ERR_RUNTIME, "No step begun with aprl_run_step_begin is open");
+  r->step_open = false;
+  TRY(step_finish(r));
+  return check_device(r);
+}
+
 aprl_status aprl_runs_step(aprl_run* const* runs, size_t count, uint32_t steps,
                            aprl_status* statuses) {
   if (count && !runs) return fail(APRL_ERR_INVALID_ARGUMENT, "null argument");
-  for (size_t i = 0; i < count; ++i)
+  for (size_t i = 0; i < count; ++i) {
     if (!runs[i]) return fail(APRL_ERR_INVALID_ARGUMENT, "null run");
+    TRY(no_open_step(runs[i]));
+  }
   std::vector<aprl_status> status(count, APRL_OK);
   std::string first_error;
   auto note = [&](size_t i, aprl_status st) {

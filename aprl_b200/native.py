@@ -53,6 +53,8 @@ _SIGNATURES = {
     "run_commit_electric": (C.c_int, [_H]),
     "run_shift": (C.c_int, [_H]),
     "run_step": (C.c_int, [_H, C.c_uint32]),
+    "run_step_begin": (C.c_int, [_H]),
+    "run_step_end": (C.c_int, [_H]),
     "run_get_stats": (C.c_int, [_H, C.POINTER(abi.StepStats)]),
     "run_tuning": (C.c_int, [_H, C.POINTER(abi.Tuning)]),
     "run_enable_energy_ledger": (C.c_int, [_H, C.c_int]),
@@ -338,6 +340,15 @@ class Run:
 
     def step(self, steps=1):
         self.b("run_step", self.handle, steps)
+
+    def step_begin(self):
+        """Queue one step's magnetic update, preview and first trials and
+        return without waiting (aprl_run_step_begin)."""
+        self.b("run_step_begin", self.handle)
+
+    def step_end(self):
+        """Finish the step begun by step_begin (aprl_run_step_end)."""
+        self.b("run_step_end", self.handle)
 
     def tuning(self):
         t = abi.Tuning()

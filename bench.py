@@ -395,10 +395,11 @@ def run_ours(args):
     run, _ = start_run()
     # The inlet reference table lives in pinned host memory (48 MB on the
     # dipole grid); each step uploads the native planes that step's inlet
-    # queries touch.  Step k+1's planes are issued right after step k is
-    # enqueued, so their host-side finiteness check overlaps step k's tail;
-    # the copy is stream-ordered behind step k.  K steps, K uploads, all
-    # inside the timed region (the first one before the loop).
+    # queries touch.  Step k+1's planes are uploaded between
+    # aprl_run_step_begin and aprl_run_step_end of step k, so their host-side
+    # finiteness check runs while step k's trials run on the GPU; the copy is
+    # stream-ordered behind those trials.  K steps, K uploads, all inside the
+    # timed region (the first one before the loop).
     pinned_ref = []
     for table in w.reference:
         host = torch.empty(table.shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -434,14 +435,19 @@ def run_ours(args):
     inside = [False, False]
     for i in range(K):
         e2e_particle_steps += run.particle_count()
-        run.step(1)
+        # Step i runs between begin and end; meanwhile the host checks and
+        # queues step i+1's planes.  Step i-1's detector plane is complete
+        # once step_end has read step i's trials back (its copy ran before
+        # them on the stream).
+        run.step_begin()
+        if i + 1 < K:
+            h2d += upload(step0 + i + 1)
+        run.step_end()
         if i > 0 and inside[(i - 1) % 2]:
             planes_finite &= bool(np.isfinite(detectors[(i - 1) % 2]).all())
             planes_read += 1
         inside[i % 2] = run.sample_field_plane_async(detector_lab_z, detectors[i % 2])
         d2h += detectors[0].nbytes + 8 * 24  # plane + stats block
-        if i + 1 < K:
-            h2d += upload(step0 + i + 1)
         run.stats()
     run.synchronize()
     if inside[(K - 1) % 2]:

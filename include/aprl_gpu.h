@@ -352,6 +352,19 @@ aprl_status aprl_run_shift(aprl_run* run);
  * window and conservative-source coupling (src/simulation.cpp:493-613). */
 aprl_status aprl_run_step(aprl_run* run, uint32_t steps);
 
+/* One aprl_run_step in two halves (no counterpart in the reference), so that
+ * the host can work while the step runs.  aprl_run_step_begin queues the
+ * step's magnetic update, preview and the fixed-point trials issued ahead on
+ * the run's stream and returns without waiting.  aprl_run_step_end waits for
+ * their residuals, runs any further trials the stopping rule asks for, and
+ * queues the commit and the shift; the result is exactly aprl_run_step's.
+ * Between the two, reference planes may be uploaded
+ * (aprl_run_set_reference_planes: stream-ordered after the trials, so the
+ * step's commit and shift already see them) and host-side queries made; the
+ * seam calls and the whole-step calls are refused until the step ends. */
+aprl_status aprl_run_step_begin(aprl_run* run);
+aprl_status aprl_run_step_end(aprl_run* run);
+
 /* `steps` coupled steps of `count` independent runs in lock step (no
  * counterpart in the reference, which steps one Simulation per job): each
  * step of every run is queued -- begin, magnetic update, preview and the

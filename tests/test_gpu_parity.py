@@ -205,3 +205,34 @@ def test_held_trial_residual_counts_pushed_slots():
     assert rg[3] == ro[3] < g.particle_count()
     for x, y in zip(rg[:3], ro[:3]):
         assert abs(x - y) <= 1e-12 * max(abs(y), 1e-300)
+
+
+@pytest.mark.gpu
+def test_split_step_matches_whole_steps_bit_for_bit():
+    """aprl_run_step_begin / aprl_run_step_end give exactly aprl_run_step's
+    result (bit-reproducible mode, so two runs can be compared bitwise), with
+    reference planes uploaded between the halves; seam and whole-step calls
+    are refused while a step is open."""
+    w = workloads.small_case(steps=4)
+    cfg = workloads.with_determinism(w.config)
+    whole = native.Run(native.load(), cfg)
+    split = native.Run(native.load(), cfg)
+    for r in (whole, split):
+        r.set_reference(w.reference)
+        r.set_particles(w.particles)
+    whole.step(w.steps)
+    for _ in range(w.steps):
+        split.step_begin()
+        split.set_reference_planes(2, 0, w.reference[2][:3])
+        with pytest.raises(native.AprlError):
+            split.step(1)
+        with pytest.raises(native.AprlError):
+            split.b("run_shift", split.handle)
+        split.step_end()
+    with pytest.raises(native.AprlError):
+        split.step_end()
+    for a in range(6):
+        assert np.array_equal(split.get_field(a), whole.get_field(a)), a
+    assert split.stats()["particles"] == whole.stats()["particles"]
+    whole.close()
+    split.close()
