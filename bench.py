@@ -436,23 +436,24 @@ def run_ours(args):
     for i in range(K):
         e2e_particle_steps += run.particle_count()
         # Step i runs between begin and end; meanwhile the host checks and
-        # queues step i+1's planes.  Step i-1's detector plane is complete
-        # once step_end has read step i's trials back (its copy ran before
-        # them on the stream).
+        # queues step i+1's planes and reads step i-2's detector plane (its
+        # copy completed before step i-1's trials were read back; its buffer
+        # is refilled only by step i's plane, queued after step_end).
         run.step_begin()
         if i + 1 < K:
             h2d += upload(step0 + i + 1)
-        run.step_end()
-        if i > 0 and inside[(i - 1) % 2]:
-            planes_finite &= bool(np.isfinite(detectors[(i - 1) % 2]).all())
+        if i > 1 and inside[i % 2]:
+            planes_finite &= bool(np.isfinite(detectors[i % 2]).all())
             planes_read += 1
+        run.step_end()
         inside[i % 2] = run.sample_field_plane_async(detector_lab_z, detectors[i % 2])
         d2h += detectors[0].nbytes + 8 * 24  # plane + stats block
         run.stats()
     run.synchronize()
-    if inside[(K - 1) % 2]:
-        planes_finite &= bool(np.isfinite(detectors[(K - 1) % 2]).all())
-        planes_read += 1
+    for last in (K - 2, K - 1):  # the two planes the loop has not read yet
+        if last >= 0 and inside[last % 2]:
+            planes_finite &= bool(np.isfinite(detectors[last % 2]).all())
+            planes_read += 1
     e_stop.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e_start.elapsed_time(e_stop)
