@@ -294,6 +294,40 @@ struct Basis {
   F v[12];
 };
 
+// The seven compensation coefficients of the p = 5 spline
+// (src/longitudinal_shape.h:48-54), each formed in binary64 and rounded once
+// to the arithmetic type.
+namespace quintic_detail {
+constexpr double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
+                 d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
+constexpr double c[7] = {-d / 64.,
+                         b / 16. + 3 * d / 32.,
+                         -a / 4. - b / 4. - 15 * d / 64.,
+                         1 + a / 2. + 3 * b / 8. + 5 * d / 16.,
+                         -a / 4. - b / 4. - 15 * d / 64.,
+                         b / 16. + 3 * d / 32.,
+                         -d / 64.};
+}  // namespace quintic_detail
+
+static __constant__ double kQuinticC64[7] = {
+    quintic_detail::c[0], quintic_detail::c[1], quintic_detail::c[2], quintic_detail::c[3],
+    quintic_detail::c[4], quintic_detail::c[5], quintic_detail::c[6]};
+static __constant__ float kQuinticC32[7] = {
+    float(quintic_detail::c[0]), float(quintic_detail::c[1]), float(quintic_detail::c[2]),
+    float(quintic_detail::c[3]), float(quintic_detail::c[4]), float(quintic_detail::c[5]),
+    float(quintic_detail::c[6])};
+
+template <class F>
+__device__ __forceinline__ F quintic_coefficient(int k);
+template <>
+__device__ __forceinline__ double quintic_coefficient<double>(int k) {
+  return kQuinticC64[k];
+}
+template <>
+__device__ __forceinline__ float quintic_coefficient<float>(int k) {
+  return kQuinticC32[k];
+}
+
 // basis(z, edge, QuinticCompensated) (src/longitudinal_shape.h:48-54): the
 // cell in binary64, the B-spline and compensation arithmetic in F on the
 // cell-relative offset.  The compensation of the degree-`degree` spline
@@ -301,16 +335,23 @@ struct Basis {
 template <class F>
 __device__ __forceinline__ void quintic_compensate(const F* n, unsigned degree, double cell,
                                                    Basis<F>& r) {
-  const double p = 5., a = p / 6., b = 3 * p / 40. + p * (p - 1) / 72.,
-               d = 5 * p / 112. + p * (p - 1) / 80. + p * (p - 1) * (p - 2) / 1296.;
-  const F c[7] = {F(-d / 64.), F(b / 16. + 3 * d / 32.), F(-a / 4. - b / 4. - 15 * d / 64.),
-                  F(1 + a / 2. + 3 * b / 8. + 5 * d / 16.),
-                  F(-a / 4. - b / 4. - 15 * d / 64.), F(b / 16. + 3 * d / 32.), F(-d / 64.)};
   r.first = (long long)cell - 5;
   r.count = degree + 7;
   for (int q = 0; q < 12; ++q) r.v[q] = F(0.);
   for (unsigned j = 0; j <= degree; ++j)
-    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * c[k];
+    for (unsigned k = 0; k < 7; ++k) r.v[j + k] += n[j] * quintic_coefficient<F>(k);
+}
+
+// Node q of quintic_compensate's result alone: the same products, summed in
+// the same order (spline index j rising), so the value is bit for bit
+// quintic_compensate's r.v[q].
+template <class F>
+__device__ __forceinline__ F quintic_compensated_at(const F* n, int degree, int q) {
+  F v = F(0.);
+#pragma unroll
+  for (int j = 0; j <= 5; ++j)
+    if (j <= degree && q - j >= 0 && q - j < 7) v += n[j] * quintic_coefficient<F>(q - j);
+  return v;
 }
 
 // The B-spline recursion on f = z - floor(z) up to `degree`.

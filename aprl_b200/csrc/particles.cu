@@ -122,14 +122,13 @@ __device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double 
 // quintic_segment for a deposit: every Gauss point of a cut piece lies in
 // the same cell, so the 4 x 92 node visits fall on 92 nodes; each node's four
 // weights are summed first and visited once (a quarter of the atomics).  The
-// weights are quintic_segment's; only their summation order changes.  Per
-// component and transverse corner the Gauss points' compensated bases are
-// re-formed from their spline values (one recursion per point, done once),
-// which keeps the accumulators to one z column (12 values); two corners per
-// pass would hold 24 live sums, and at the kernels' 80 registers they spill
-// several times more.  A piece whose
-// Gauss points straddle a cell (only possible through rounding at a cut) is
-// visited point by point.
+// weights are quintic_segment's; only their summation order changes.  The
+// walk is node by node: a Gauss point's compensated value at a node is formed
+// once (quintic_compensated_at, the same sums as quintic_compensate) and
+// shared by the component's transverse corners, so a node keeps four live
+// sums and the 12-node loop stays rolled.  A piece whose Gauss points
+// straddle a cell (only possible through rounding at a cut) is visited point
+// by point.
 template <class G, class V>
 __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const double x[3],
                                                        const double v[3], double lower,
@@ -167,58 +166,54 @@ __device__ __forceinline__ void quintic_segment_summed(const GridT<G>& g, const 
     quintic_segment(g, x, v, lower, upper, width, visit);
     return;
   }
-  // Each Gauss point's spline recursion once; the compensated bases below
-  // are formed from these values exactly as quintic_basis forms them.
+  // Each Gauss point's spline recursion once.
   QuinticSplines<F> spline[4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) quintic_splines(zz[t], spline[t]);
-  Basis<F> b;
+  const long long first = (long long)spline[0].cell - 5;
   // Jx at (i, j + c) and Jy at (i + c, j): node basis, 12 nodes.
-  for (int axis = 0; axis < 2; ++axis)
-    for (int c = 0; c < 2; ++c) {
-      F acc[12];
-      unsigned hit = 0;
-      long long first = 0;
-      for (int k = 0; k < 12; ++k) acc[k] = F(0.);
-      for (int t = 0; t < 4; ++t) {
-        quintic_compensate(spline[t].node, 5, spline[t].cell, b);
-        first = b.first;
-        const F side = axis == 0 ? (c ? fy[t] : F(1.) - fy[t]) : (c ? fx[t] : F(1.) - fx[t]);
-        for (int k = 0; k < b.count; ++k) {
-          const F w = factor[t] * b.v[k];
-          if (w == F(0.)) continue;
-          acc[k] += w * side;
-          hit |= 1u << k;
-        }
-      }
-      for (int k = 0; k < 12; ++k)
-        if (hit & (1u << k)) {
-          if (axis == 0)
-            visit(0, i, j + c, first + k, acc[k]);
-          else
-            visit(1, i + c, j, first + k, acc[k]);
-        }
+#pragma unroll 1
+  for (int k = 0; k < 12; ++k) {
+    F acc[4] = {F(0.), F(0.), F(0.), F(0.)};
+    bool hit = false;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const F w = factor[t] * quintic_compensated_at(spline[t].node, 5, k);
+      if (w == F(0.)) continue;
+      hit = true;
+      acc[0] += w * (F(1.) - fy[t]);
+      acc[1] += w * fy[t];
+      acc[2] += w * (F(1.) - fx[t]);
+      acc[3] += w * fx[t];
     }
+    if (!hit) continue;
+    visit(0, i, j, first + k, acc[0]);
+    visit(0, i, j + 1, first + k, acc[1]);
+    visit(1, i, j, first + k, acc[2]);
+    visit(1, i + 1, j, first + k, acc[3]);
+  }
   // Jz at (i + a, j + c): edge basis, 11 nodes.
-  for (int c = 0; c < 2; ++c)
-    for (int a = 0; a < 2; ++a) {
-      F acc[12];
-      unsigned hit = 0;
-      long long first = 0;
-      for (int k = 0; k < 12; ++k) acc[k] = F(0.);
-      for (int t = 0; t < 4; ++t) {
-        quintic_compensate(spline[t].edge, 4, spline[t].cell, b);
-        first = b.first;
-        for (int k = 0; k < b.count; ++k) {
-          const F w = factor[t] * b.v[k];
-          if (w == F(0.)) continue;
-          acc[k] += w * (a ? fx[t] : F(1.) - fx[t]) * (c ? fy[t] : F(1.) - fy[t]);
-          hit |= 1u << k;
-        }
-      }
-      for (int k = 0; k < 12; ++k)
-        if (hit & (1u << k)) visit(2, i + a, j + c, first + k, acc[k]);
+#pragma unroll 1
+  for (int k = 0; k < 11; ++k) {
+    F acc[4] = {F(0.), F(0.), F(0.), F(0.)};
+    bool hit = false;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const F w = factor[t] * quintic_compensated_at(spline[t].edge, 4, k);
+      if (w == F(0.)) continue;
+      hit = true;
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+          acc[2 * c + a] += w * (a ? fx[t] : F(1.) - fx[t]) * (c ? fy[t] : F(1.) - fy[t]);
     }
+    if (!hit) continue;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int a = 0; a < 2; ++a) visit(2, i + a, j + c, first + k, acc[2 * c + a]);
+  }
 }
 
 // longitudinal_shape::weights (src/longitudinal_shape.h:97-117) with

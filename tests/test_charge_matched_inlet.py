@@ -81,8 +81,14 @@ def test_aperture_without_interior_is_rejected():
 
 
 def compare(g, o):
-    for a, (x, y) in enumerate(zip(fields(g), fields(o))):
-        assert checkers.max_relative(x, y) <= RTOL, f"field {a}"
+    # Each component is held to RTOL of its field's peak (E's for Ex, Ey, Ez;
+    # B's for Bx, By, Bz).  In the held-injection beam Bz peaks near 2.5e-3
+    # beside Bx near 7: relative to Bz's own peak, the run-to-run spread of
+    # the FP64 atomic sums alone reaches about 1.4e-12, which is 5e-16 of |B|.
+    got, want = fields(g), fields(o)
+    for a in range(6):
+        scale = max(np.abs(f).max() for f in want[3 * (a // 3):3 * (a // 3) + 3])
+        assert np.abs(got[a] - want[a]).max() <= RTOL * scale, f"field {a}"
     pg, po = g.get_particles(), o.get_particles()
     np.testing.assert_array_equal(pg["id"], po["id"])
     for k in ("x", "y", "z", "ux", "uy", "uz"):
