@@ -119,10 +119,11 @@ __device__ __forceinline__ void quintic_segment(const GridT<G>& g, const double 
   }
 }
 
-// quintic_segment for a deposit: every Gauss point of a cut piece lies in
-// the same cell, so the 4 x 92 node visits fall on 92 nodes; each node's four
-// weights are summed first and visited once (a quarter of the atomics).  The
-// weights are quintic_segment's; only their summation order changes.  The
+// quintic_segment for the deposit and the electric gather: every Gauss point
+// of a cut piece lies in the same cell, so the 4 x 92 node visits fall on 92
+// nodes; each node's four weights are summed first and visited once (a
+// quarter of the atomics or S reads).  The weights are quintic_segment's;
+// only their summation order changes.  The
 // walk is node by node: a Gauss point's compensated value at a node is formed
 // once (quintic_compensated_at, the same sums as quintic_compensate) and
 // shared by the component's transverse corners, so a node keeps four live
