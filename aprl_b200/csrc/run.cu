@@ -259,6 +259,22 @@ struct aprl_run {
   // short, latency-bound launch overlaps the particles' push.
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // Reference planes set with aprl_run_set_reference_planes cross PCIe on
+  // `upload`, into a staging buffer, as soon as they are given; the run's
+  // stream then copies them device to device into the table at the call's
+  // place in its own order (after the slot's `staged` event), so the
+  // transfer overlaps the work already queued.  Two slots per component
+  // take turns; `drained` marks the stream's copy out of a slot, which the
+  // next transfer into that slot waits for.
+  struct Stage {
+    double* data = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t staged = nullptr, drained = nullptr;
+    bool used = false;
+  };
+  cudaStream_t upload = nullptr;
+  Stage staging[6][2];
+  int staging_next[6] = {};
   double coeff[12]{};
   // E, B and J are binary64 in both modes (`fes`: J element size); the
   // FP32-mixed mode runs the gathers in binary32.
@@ -2257,6 +2273,13 @@ aprl_status aprl_run_create(const aprl_run_config* config, void* stream, aprl_ru
       cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&r->join, cudaEventDisableTiming) != cudaSuccess)
     return cleanup(fail(APRL_ERR_CUDA, "side stream creation failed"));
+  if (cudaStreamCreateWithFlags(&r->upload, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(APRL_ERR_CUDA, "upload stream creation failed"));
+  for (auto& component : r->staging)
+    for (auto& st : component)
+      if (cudaEventCreateWithFlags(&st.staged, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&st.drained, cudaEventDisableTiming) != cudaSuccess)
+        return cleanup(fail(APRL_ERR_CUDA, "upload event creation failed"));
   r->h_sums = r->h_sums_slots;
   r->h_counters = r->h_counters_slots;
   r->offset = c.initial_offset;
@@ -2278,6 +2301,16 @@ aprl_status aprl_run_destroy(aprl_run* r) {
   }
   if (r->fork) cudaEventDestroy(r->fork);
   if (r->join) cudaEventDestroy(r->join);
+  if (r->upload) {
+    cudaStreamSynchronize(r->upload);
+    cudaStreamDestroy(r->upload);
+  }
+  for (auto& component : r->staging)
+    for (auto& st : component) {
+      if (st.staged) cudaEventDestroy(st.staged);
+      if (st.drained) cudaEventDestroy(st.drained);
+      device_free(r, st.data);
+    }
   for (auto& t : r->pending) {
     cudaEventDestroy(t.start);
     cudaEventDestroy(t.stop);
@@ -2389,8 +2422,30 @@ aprl_status aprl_run_set_reference_planes(aprl_run* r, unsigned a, uint64_t firs
   const size_t plane = s[0] * s[1];
   if (!all_finite(host, planes * plane))
     return fail(APRL_ERR_RUNTIME, "Non-finite moving-window inlet");
-  CUDA_TRY(cudaMemcpyAsync(r->ref[a] + first * plane, host, planes * plane * 8,
-                           cudaMemcpyHostToDevice, r->stream));
+  const size_t bytes = planes * plane * 8;
+  if (bytes) {
+    aprl_run::Stage& st = r->staging[a][r->staging_next[a]];
+    if (st.bytes < bytes) {
+      // The old block's last reader is the stream's copy out of it, which
+      // the stream-ordered free follows; the new block is ready for every
+      // stream once device_alloc_bytes returns.
+      device_free(r, st.data);
+      st.data = nullptr;
+      st.bytes = 0;
+      st.used = false;
+      TRY(device_alloc(r, &st.data, bytes / 8));
+      st.bytes = bytes;
+    }
+    r->staging_next[a] ^= 1;
+    if (st.used) CUDA_TRY(cudaStreamWaitEvent(r->upload, st.drained, 0));
+    CUDA_TRY(cudaMemcpyAsync(st.data, host, bytes, cudaMemcpyHostToDevice, r->upload));
+    CUDA_TRY(cudaEventRecord(st.staged, r->upload));
+    CUDA_TRY(cudaStreamWaitEvent(r->stream, st.staged, 0));
+    CUDA_TRY(cudaMemcpyAsync(r->ref[a] + first * plane, st.data, bytes,
+                             cudaMemcpyDeviceToDevice, r->stream));
+    CUDA_TRY(cudaEventRecord(st.drained, r->stream));
+    st.used = true;
+  }
   if (a == 3 || a == 4) r->surface_ready = false;
   return APRL_OK;
 }

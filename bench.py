@@ -397,9 +397,10 @@ def run_ours(args):
     # dipole grid); each step uploads the native planes that step's inlet
     # queries touch.  Step k+1's planes are uploaded between
     # aprl_run_step_begin and aprl_run_step_end of step k, so their host-side
-    # finiteness check runs while step k's trials run on the GPU; the copy is
-    # stream-ordered behind those trials.  K steps, K uploads, all inside the
-    # timed region (the first one before the loop).
+    # finiteness check and their PCIe transfer (on the run's copy stream) run
+    # while step k's trials run on the GPU; the planes take effect in stream
+    # order behind those trials.  K steps, K uploads, all inside the timed
+    # region (the first one before the loop).
     pinned_ref = []
     for table in w.reference:
         host = torch.empty(table.shape, dtype=torch.float64, pin_memory=True).numpy()

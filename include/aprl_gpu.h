@@ -257,7 +257,15 @@ aprl_status aprl_run_set_reference(aprl_run* run, unsigned component,
  * bounded block reader (src/blocked_cowan_reference.h:59-98): when
  * aprl_run_set_reference was given host == NULL the table is allocated
  * zero-filled, and this call overwrites `planes` native z planes starting at
- * `first_plane` of one component (host holds planes*nx_c*ny_c doubles). */
+ * `first_plane` of one component (host holds planes*nx_c*ny_c doubles).
+ * The planes take effect at this call's place in the run's stream order:
+ * work queued before it reads the old values, work queued after it the new.
+ * Their host-to-device transfer starts at once on a copy stream of the run,
+ * beside the work already queued (for instance between aprl_run_step_begin
+ * and aprl_run_step_end), into a staging buffer from which the run's stream
+ * copies them.  From page-locked memory the call returns before the
+ * transfer ends: keep `host` unchanged until the run's stream has passed
+ * this call. */
 aprl_status aprl_run_set_reference_planes(aprl_run* run, unsigned component,
                                           uint64_t first_plane, uint64_t planes,
                                           const double* host);
