@@ -183,6 +183,10 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
   const bool column = i <= g.nx && j <= g.ny;
   const int slot_x = column && i < g.nx ? a.mx.ordinal[i] : -1;
   const int slot_y = column && j < g.ny ? a.my.ordinal[j] : -1;
+  // The z differences smooth within one plane (x and y neighbours), so the
+  // smoothed Ey and Ex of plane k+1 are, bit for bit, the plane-k operands
+  // of the next step: carried in registers instead of evaluated again.
+  double ey_above = 0.0, ex_above = 0.0;
   for (int k = k0; k < k1; ++k) {
     load_plane(t, a, k + 1, ps.s[2], i0, j0);
     __syncthreads();
@@ -190,8 +194,9 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
       if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
         const double dEzDy = tile_smoothed(t, a, 2, 1, li, lj + 1, 0, ps) -
                              tile_smoothed(t, a, 2, 1, li, lj, 0, ps);
-        const double dEyDz = tile_smoothed(t, a, 1, 2, li, lj, 1, ps) -
-                             tile_smoothed(t, a, 1, 2, li, lj, 0, ps);
+        const double ey_here = k > k0 ? ey_above : tile_smoothed(t, a, 1, 2, li, lj, 0, ps);
+        ey_above = tile_smoothed(t, a, 1, 2, li, lj, 1, ps);
+        const double dEyDz = ey_above - ey_here;
         double* bx = &g.b[0][b_index(g, 0, i, j, k)];
         double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
         const int s = slot_y;
@@ -201,8 +206,9 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         *bx = v;
       }
       if (i < g.nx && k < g.nz) {  // By (nx, ny+1, nz)
-        const double dExDz = tile_smoothed(t, a, 0, 2, li, lj, 1, ps) -
-                             tile_smoothed(t, a, 0, 2, li, lj, 0, ps);
+        const double ex_here = k > k0 ? ex_above : tile_smoothed(t, a, 0, 2, li, lj, 0, ps);
+        ex_above = tile_smoothed(t, a, 0, 2, li, lj, 1, ps);
+        const double dExDz = ex_above - ex_here;
         const double dEzDx = tile_smoothed(t, a, 2, 0, li + 1, lj, 0, ps) -
                              tile_smoothed(t, a, 2, 0, li, lj, 0, ps);
         double* by = &g.b[1][b_index(g, 1, i, j, k)];
