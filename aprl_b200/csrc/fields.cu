@@ -272,17 +272,38 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
   if (i > g.nx || j > g.ny || k > g.nz) return;
   const double curl = g.dt / (kMu0 * kEpsilon0);
   const double cx = curl / g.dx, cy = curl / g.dy, cz = curl / g.dz;
-  if (i < g.nx) {  // Ex (nx, ny+1, nz+1)
-    const size_t n = e_index(g, 0, i, j, k);
-    const double old = g.e_old[0][n];
-    double v = old;
-    if (k >= 1 && k < g.nz && j >= 1 && j < g.ny)
-      v += cy * (bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k)) -
-           cz * (bval(g, 1, i, j, k) - bval(g, 1, i, j, k - 1));
-    if (j >= 1 && j < g.ny) {
+  // Every E and B read of the node is issued before its first store (the
+  // stores may alias them as far as the compiler knows), so their latencies
+  // overlap; each difference below is formed from the same two values as
+  // before, in the same order.
+  const bool has_x = i < g.nx, has_y = j < g.ny, has_z = k < g.nz;
+  const bool x_row = has_x && j >= 1 && j < g.ny;     // Ex: y difference of Bz
+  const bool x_curl = x_row && k >= 1 && k < g.nz;    // Ex: the whole curl
+  const bool y_row = has_y && i >= 1 && i < g.nx;     // Ey: x difference of Bz
+  const bool y_curl = y_row && k >= 1 && k < g.nz;    // Ey: the whole curl
+  const bool z_inner = has_z && i >= 1 && i < g.nx && j >= 1 && j < g.ny;
+  const size_t n0 = has_x ? e_index(g, 0, i, j, k) : 0;
+  const size_t n1 = has_y ? e_index(g, 1, i, j, k) : 0;
+  const size_t n2 = has_z ? e_index(g, 2, i, j, k) : 0;
+  const double old0 = has_x ? g.e_old[0][n0] : 0.0;
+  const double old1 = has_y ? g.e_old[1][n1] : 0.0;
+  const double old2 = has_z ? g.e_old[2][n2] : 0.0;
+  const double bz = x_row || y_row ? bval(g, 2, i, j, k) : 0.0;
+  const double bz_j = x_row ? bval(g, 2, i, j - 1, k) : 0.0;
+  const double bz_i = y_row ? bval(g, 2, i - 1, j, k) : 0.0;
+  const double by = x_curl || z_inner ? bval(g, 1, i, j, k) : 0.0;
+  const double by_k = x_curl ? bval(g, 1, i, j, k - 1) : 0.0;
+  const double by_i = z_inner ? bval(g, 1, i - 1, j, k) : 0.0;
+  const double bx = y_curl || z_inner ? bval(g, 0, i, j, k) : 0.0;
+  const double bx_k = y_curl ? bval(g, 0, i, j, k - 1) : 0.0;
+  const double bx_j = z_inner ? bval(g, 0, i, j - 1, k) : 0.0;
+  if (has_x) {  // Ex (nx, ny+1, nz+1)
+    double v = old0;
+    if (x_curl) v += cy * (bz - bz_j) - cz * (by - by_k);
+    if (x_row) {
       const int s = a.ey_prof.ordinal[j];
       if (s >= 0) {
-        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i, j - 1, k);
+        const double diff = bz - bz_j;
         v += 1.0 * cy * cpml_correction(a.ey_prof, j, diff,
                                         history_at(a.h[0], s, k, g.zb_e[0], i, g.status));
       }
@@ -293,20 +314,16 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
         a.pre_inlet[0][APRL_BOUNDED(g.status, (size_t)j * g.nx + i, (size_t)g.nx * (g.ny + 1), 22)] = v;
       v = inlet_value(a.inlet, 0, i, j);
     }
-    g.e_star[0][n] = v;
-    if (a.orbit[0]) preview_orbit(a, 0, n, v, old);
+    g.e_star[0][n0] = v;
+    if (a.orbit[0]) preview_orbit(a, 0, n0, v, old0);
   }
-  if (j < g.ny) {  // Ey (nx+1, ny, nz+1)
-    const size_t n = e_index(g, 1, i, j, k);
-    const double old = g.e_old[1][n];
-    double v = old;
-    if (k >= 1 && k < g.nz && i >= 1 && i < g.nx)
-      v += cz * (bval(g, 0, i, j, k) - bval(g, 0, i, j, k - 1)) -
-           cx * (bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k));
-    if (i >= 1 && i < g.nx) {
+  if (has_y) {  // Ey (nx+1, ny, nz+1)
+    double v = old1;
+    if (y_curl) v += cz * (bx - bx_k) - cx * (bz - bz_i);
+    if (y_row) {
       const int s = a.ex_prof.ordinal[i];
       if (s >= 0) {
-        const double diff = bval(g, 2, i, j, k) - bval(g, 2, i - 1, j, k);
+        const double diff = bz - bz_i;
         v += -1.0 * cx * cpml_correction(a.ex_prof, i, diff,
                                          history_at(a.h[1], s, k, g.zb_e[1], j, g.status));
       }
@@ -318,34 +335,29 @@ __global__ void electric_preview_kernel(PreviewArgs<F> a) {
                                     (size_t)(g.nx + 1) * g.ny, 23)] = v;
       v = inlet_value(a.inlet, 1, i, j);
     }
-    g.e_star[1][n] = v;
-    if (a.orbit[0]) preview_orbit(a, 1, n, v, old);
+    g.e_star[1][n1] = v;
+    if (a.orbit[0]) preview_orbit(a, 1, n1, v, old1);
   }
-  if (k < g.nz) {  // Ez (nx+1, ny+1, nz)
-    const size_t n = e_index(g, 2, i, j, k);
-    const double old = g.e_old[2][n];
-    double v = old;
-    const bool inner = i >= 1 && i < g.nx && j >= 1 && j < g.ny;
-    if (inner)
-      v += cx * (bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k)) -
-           cy * (bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k));
-    if (inner) {
+  if (has_z) {  // Ez (nx+1, ny+1, nz)
+    double v = old2;
+    if (z_inner) v += cx * (by - by_i) - cy * (bx - bx_j);
+    if (z_inner) {
       const int sx = a.ex_prof.ordinal[i];
       if (sx >= 0) {
-        const double diff = bval(g, 1, i, j, k) - bval(g, 1, i - 1, j, k);
+        const double diff = by - by_i;
         v += 1.0 * cx * cpml_correction(a.ex_prof, i, diff,
                                         history_at(a.h[2], sx, k, g.zb_e[2], j, g.status));
       }
       const int sy = a.ey_prof.ordinal[j];
       if (sy >= 0) {
-        const double diff = bval(g, 0, i, j, k) - bval(g, 0, i, j - 1, k);
+        const double diff = bx - bx_j;
         v += -1.0 * cy * cpml_correction(a.ey_prof, j, diff,
                                          history_at(a.h[3], sy, k, g.zb_e[2], i, g.status));
       }
     }
     if (i == 0 || i == g.nx || j == 0 || j == g.ny) v = 0.0;
-    g.e_star[2][n] = v;
-    if (a.orbit[0]) preview_orbit(a, 2, n, v, old);
+    g.e_star[2][n2] = v;
+    if (a.orbit[0]) preview_orbit(a, 2, n2, v, old2);
   }
 }
 
@@ -358,16 +370,23 @@ __global__ void electric_commit_kernel(GridT<F> g) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
   if (i > g.nx || j > g.ny || k > g.nz) return;
+  // The three J reads are issued before the first update of E* (which may
+  // alias them as far as the compiler knows), so their latencies overlap.
+  F jc[3];
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
-    if (!current_mask(g, c, i, j, k)) continue;
-    const F jc = g.j[c][j_index(g, c, i, j, k)];
-    if (jc != F(0.)) {
+    jc[c] = F(0.);
+    if (i < e_nx(g, c) && j < e_ny(g, c) && k < e_nz(g, c) && current_mask(g, c, i, j, k))
+      jc[c] = g.j[c][j_index(g, c, i, j, k)];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (jc[c] != F(0.)) {
       // binary64 J: g.jcoef is -dt/eps0 itself.  A binary32 J is widened and
       // scaled by the binary64 coefficient.
       const double jcoef =
           sizeof(F) == sizeof(double) ? (double)g.jcoef : -1. * g.dt / kEpsilon0;
-      g.e_star[c][e_index(g, c, i, j, k)] += jcoef * (double)jc;
+      g.e_star[c][e_index(g, c, i, j, k)] += jcoef * (double)jc[c];
     }
   }
 }
@@ -451,15 +470,27 @@ __global__ void orbit_sum_kernel(GridT<double> g, W* s0, W* s1, W* s2, int with_
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
   W* s[3] = {s0, s1, s2};
+  // Every read of the node is issued before its first store (which may
+  // alias them as far as the compiler knows), so their latencies overlap.
+  bool in[3];
+  size_t n[3];
+  double star[3], old[3], jc[3];
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if (i >= e_nx(g, c) || j >= e_ny(g, c) || k >= e_nz(g, c)) continue;
-    const size_t n = e_index(g, c, i, j, k);
-    double v = g.e_star[c][n];
-    if (with_current && current_mask(g, c, i, j, k)) {
-      const double jc = g.j[c][j_index(g, c, i, j, k)];
-      if (jc != 0.) v += g.jcoef * jc;
-    }
-    s[c][n] = W(v + g.e_old[c][n]);
+    in[c] = i < e_nx(g, c) && j < e_ny(g, c) && k < e_nz(g, c);
+    n[c] = in[c] ? e_index(g, c, i, j, k) : 0;
+    star[c] = in[c] ? g.e_star[c][n[c]] : 0.;
+    old[c] = in[c] ? g.e_old[c][n[c]] : 0.;
+    jc[c] = in[c] && with_current && current_mask(g, c, i, j, k)
+                ? g.j[c][j_index(g, c, i, j, k)]
+                : 0.;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!in[c]) continue;
+    double v = star[c];
+    if (jc[c] != 0.) v += g.jcoef * jc[c];
+    s[c][n[c]] = W(v + old[c]);
   }
 }
 
