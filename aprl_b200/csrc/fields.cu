@@ -189,6 +189,17 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
   double ey_above = 0.0, ex_above = 0.0;
   for (int k = k0; k < k1; ++k) {
     load_plane(t, a, k + 1, ps.s[2], i0, j0);
+    // The node's three B values are read before the first B store (which
+    // may alias them as far as the compiler knows).
+    const bool has_bx = column && j < g.ny && k < g.nz;
+    const bool has_by = column && i < g.nx && k < g.nz;
+    const bool has_bz = column && i < g.nx && j < g.ny;
+    double* const bx = has_bx ? &g.b[0][b_index(g, 0, i, j, k)] : nullptr;
+    double* const by = has_by ? &g.b[1][b_index(g, 1, i, j, k)] : nullptr;
+    double* const bz = has_bz ? &g.b[2][b_index(g, 2, i, j, k)] : nullptr;
+    const double bx_old = has_bx ? *bx : 0.0;
+    const double by_old = has_by ? *by : 0.0;
+    const double bz_old = has_bz ? *bz : 0.0;
     __syncthreads();
     if (i <= g.nx && j <= g.ny) {
       if (j < g.ny && k < g.nz) {  // Bx (nx+1, ny, nz)
@@ -197,8 +208,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         const double ey_here = k > k0 ? ey_above : tile_smoothed(t, a, 1, 2, li, lj, 0, ps);
         ey_above = tile_smoothed(t, a, 1, 2, li, lj, 1, ps);
         const double dEyDz = ey_above - ey_here;
-        double* bx = &g.b[0][b_index(g, 0, i, j, k)];
-        double v = *bx - (dtdy * dEzDy - dtdz * dEyDz);
+        double v = bx_old - (dtdy * dEzDy - dtdz * dEyDz);
         const int s = slot_y;
         if (s >= 0)
           v += -1.0 * dtdy * cpml_correction(a.my, j, dEzDy,
@@ -211,8 +221,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
         const double dExDz = ex_above - ex_here;
         const double dEzDx = tile_smoothed(t, a, 2, 0, li + 1, lj, 0, ps) -
                              tile_smoothed(t, a, 2, 0, li, lj, 0, ps);
-        double* by = &g.b[1][b_index(g, 1, i, j, k)];
-        double v = *by - (dtdz * dExDz - dtdx * dEzDx);
+        double v = by_old - (dtdz * dExDz - dtdx * dEzDx);
         const int s = slot_x;
         if (s >= 0)
           v += 1.0 * dtdx * cpml_correction(a.mx, i, dEzDx,
@@ -224,8 +233,7 @@ __global__ void __launch_bounds__(kTX * kTY, APRL_COWAN_MIN_BLOCKS)
                              tile_smoothed(t, a, 1, 0, li, lj, 0, ps);
         const double dExDy = tile_smoothed(t, a, 0, 1, li, lj + 1, 0, ps) -
                              tile_smoothed(t, a, 0, 1, li, lj, 0, ps);
-        double* bz = &g.b[2][b_index(g, 2, i, j, k)];
-        double v = *bz - (dtdx * dEyDx - dtdy * dExDy);
+        double v = bz_old - (dtdx * dEyDx - dtdy * dExDy);
         const int sx = slot_x;
         if (sx >= 0)
           v += -1.0 * dtdx * cpml_correction(a.mx, i, dEyDx,

@@ -1920,14 +1920,20 @@ __global__ void gather_particles_kernel(DParticles out, DParticles src, const do
   const long long slot = compact_slot(flag, want, n, block_offset, selected);
   const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
   if (!selected) return;
-  out.x[slot] = x1[i]; out.y[slot] = y1[i]; out.z[slot] = z1[i];
-  out.ux[slot] = ux1[i]; out.uy[slot] = uy1[i]; out.uz[slot] = uz1[i];
-  out.q[slot] = src.q[i];
-  out.m[slot] = src.m[i];
-  out.id[slot] = src.id[i];
-  out.order[slot] = src.order[i];
-  out.frozen[slot] = frozen1[i];
-  out.beta[slot] = src.beta[i];
+  // Every read before the first store (which may alias them as far as the
+  // compiler knows), so the reads' latencies overlap.
+  const double x = x1[i], y = y1[i], z = z1[i], ux = ux1[i], uy = uy1[i], uz = uz1[i];
+  const double q = src.q[i], m = src.m[i], beta = src.beta[i];
+  const unsigned long long id = src.id[i], order = src.order[i];
+  const unsigned char frozen = frozen1[i];
+  out.x[slot] = x; out.y[slot] = y; out.z[slot] = z;
+  out.ux[slot] = ux; out.uy[slot] = uy; out.uz[slot] = uz;
+  out.q[slot] = q;
+  out.m[slot] = m;
+  out.id[slot] = id;
+  out.order[slot] = order;
+  out.frozen[slot] = frozen;
+  out.beta[slot] = beta;
 }
 
 __global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsigned char* flag,
@@ -1938,11 +1944,15 @@ __global__ void gather_carriers_kernel(DCarriers out, DCarriers src, const unsig
   const long long slot = compact_slot(flag, want, n, block_offset, selected) + (long long)base;
   const long long i = (long long)blockIdx.x * kScanBlock + threadIdx.x;
   if (!selected) return;
-  out.px[slot] = src.px[i]; out.py[slot] = src.py[i]; out.pz[slot] = src.pz[i];
-  out.vx[slot] = src.vx[i]; out.vy[slot] = src.vy[i]; out.vz[slot] = src.vz[i];
-  out.q[slot] = src.q[i];
-  out.w[slot] = src.w[i];
-  out.key[slot] = src.key[i];
+  const double px = src.px[i], py = src.py[i], pz = src.pz[i];
+  const double vx = src.vx[i], vy = src.vy[i], vz = src.vz[i];
+  const double q = src.q[i], w = src.w[i];
+  const unsigned long long key = src.key[i];
+  out.px[slot] = px; out.py[slot] = py; out.pz[slot] = pz;
+  out.vx[slot] = vx; out.vy[slot] = vy; out.vz[slot] = vz;
+  out.q[slot] = q;
+  out.w[slot] = w;
+  out.key[slot] = key;
 }
 
 // ---------------------------------------------------------------------------
@@ -2034,14 +2044,20 @@ __global__ void permute_particles_kernel(DParticles out, DParticles src, long lo
   const long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= n) return;
   const long long i = index[d];
-  out.x[d] = src.x[i]; out.y[d] = src.y[i]; out.z[d] = src.z[i];
-  out.ux[d] = src.ux[i]; out.uy[d] = src.uy[i]; out.uz[d] = src.uz[i];
-  out.q[d] = src.q[i];
-  out.m[d] = src.m[i];
-  out.id[d] = src.id[i];
-  out.order[d] = src.order[i];
-  out.frozen[d] = src.frozen[i];
-  out.beta[d] = src.beta[i];
+  // Every read before the first store, as in gather_particles_kernel.
+  const double x = src.x[i], y = src.y[i], z = src.z[i];
+  const double ux = src.ux[i], uy = src.uy[i], uz = src.uz[i];
+  const double q = src.q[i], m = src.m[i], beta = src.beta[i];
+  const unsigned long long id = src.id[i], order = src.order[i];
+  const unsigned char frozen = src.frozen[i];
+  out.x[d] = x; out.y[d] = y; out.z[d] = z;
+  out.ux[d] = ux; out.uy[d] = uy; out.uz[d] = uz;
+  out.q[d] = q;
+  out.m[d] = m;
+  out.id[d] = id;
+  out.order[d] = order;
+  out.frozen[d] = frozen;
+  out.beta[d] = beta;
 }
 
 // Exclusive scan of 1024-element chunks; chunk totals go to chunk_sum.
