@@ -1754,14 +1754,21 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
       raise_error(a.status, err, (unsigned long long)n);
       for (int d = 0; d < 3; ++d) ne[d] = nb[d] = 0.0;
     }
+    // The trial's reads, issued together before the first store (which may
+    // alias them as far as the compiler knows).
+    double used_e[3], used_b[3];
+    for (int d = 0; d < 3; ++d) {
+      used_e[d] = a.used_e[3 * n + d];
+      used_b[d] = a.used_b[3 * n + d];
+    }
+    const double q = a.p.q[n], m = a.p.m[n], abs_work = a.abs_grid_work[n];
     double de[3], db[3];
     for (int d = 0; d < 3; ++d) {
       a.next_e[3 * n + d] = ne[d];
       a.next_b[3 * n + d] = nb[d];
-      de[d] = ne[d] - a.used_e[3 * n + d];
-      db[d] = nb[d] - a.used_b[3 * n + d];
+      de[d] = ne[d] - used_e[d];
+      db[d] = nb[d] - used_b[d];
     }
-    const double q = a.p.q[n], m = a.p.m[n];
     force = fabs(q / m) * dt / kC *
             (sqrt(de[0] * de[0] + de[1] * de[1] + de[2] * de[2]) +
              kC * sqrt(db[0] * db[0] + db[1] * db[1] + db[2] * db[2]));
@@ -1771,7 +1778,7 @@ __global__ void APRL_RESIDUAL_BOUNDS residual_kernel(ResidualArgs<F> a) {
       wn += q * ne[d] * (last[d] - first[d]);
     }
     defect = fabs(wd);
-    scale = a.abs_grid_work[n] + fabs(wn);
+    scale = abs_work + fabs(wn);
   }
   __shared__ unsigned s_calls[32];
   const unsigned calls = __popc(__ballot_sync(0xffffffffu, seen != 0));
