@@ -2427,13 +2427,19 @@ aprl_status aprl_run_set_reference_planes(aprl_run* r, unsigned a, uint64_t firs
     aprl_run::Stage& st = r->staging[a][r->staging_next[a]];
     if (st.bytes < bytes) {
       // The old block's last reader is the stream's copy out of it, which
-      // the stream-ordered free follows; the new block is ready for every
-      // stream once device_alloc_bytes returns.
+      // the stream-ordered free follows.  The new block is allocated in the
+      // upload stream's order, without a wait: the transfer into it follows
+      // on that stream, and the run's stream reads it only after `staged`.
       device_free(r, st.data);
       st.data = nullptr;
       st.bytes = 0;
       st.used = false;
-      TRY(device_alloc(r, &st.data, bytes / 8));
+      void* block = nullptr;
+      const cudaError_t e = cudaMallocFromPoolAsync(&block, bytes, r->pool, r->upload);
+      if (e != cudaSuccess)
+        return fail(APRL_ERR_CUDA, "device allocation of %zu bytes failed: %s", bytes,
+                    cudaGetErrorString(e));
+      st.data = static_cast<double*>(block);
       st.bytes = bytes;
     }
     r->staging_next[a] ^= 1;
